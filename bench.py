@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Stieltjes-transform hot path.
+
+Workload (default): the exact-kernel scale-up case -- p = 1,000,000
+eigenvalues drawn i.i.d. from the Marchenko-Pastur law (c = 0.5,
+sigma^2 = 1) by inverse CDF on a 2^20-point grid, sorted, f64 storage,
+eta = 1/sqrt(p), all p targets -- with the mixed-precision exact kernel
+(FP32 compensated far field, FP64 near field).  One "step" is one full
+transform of that spectrum.  Metric: pair evaluations per second
+(p_targets * p_sources / t) and ms per transform.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+For N > 1 the driver launches one process per GPU with torch.distributed;
+every rank transforms its own spectrum (weak scaling, no data-path
+collective), timing is the max over ranks.  ``--impl reference`` times the
+reference algorithm's CPU implementation (the C++ restatement of the
+crate's parallel route, run with every host thread) on a bounded sample of
+the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Stieltjes pairs/s & ms @p=50k/1M, mixed vs FP64 at stated err; fwd+adj ms"
+UNIT = "pairs/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--p", type=int, default=1_000_000)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target duration of one CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# --------------------------------------------------------------- clocks --
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+
+        def reader():
+            for line in self.proc.stdout:
+                self.rows.append([x.strip() for x in line.split(",")])
+
+        self.thread = threading.Thread(target=reader, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ reference --
+def cpu_baseline_sample(ev, eta, seconds):
+    """Time the reference's parallel all-points route (C++ restatement of
+    cacheblock.rs:1454-1513, every host thread) on a target sample sized to
+    about `seconds` of work; returns pairs/s and the sample description."""
+    from oracle import oracle as O
+
+    O.build()
+    p = ev.size
+    probe = min(p, 64)
+    t0 = time.perf_counter()
+    O.tiled_targets(ev[:probe], ev, eta)
+    rate = probe * p / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(p, max(probe, rate * seconds / p)))
+    idx = np.linspace(0, p - 1, n).astype(np.int64)
+    t0 = time.perf_counter()
+    O.tiled_targets(ev[idx], ev, eta)
+    dt = time.perf_counter() - t0
+    return n * p / dt, n, dt, O.num_threads()
+
+
+def run_reference(args, world, rank):
+    from shrinkers_b200 import spectra
+
+    if rank != 0:
+        return
+    p = args.p
+    ev = spectra.config2(p)
+    eta = 1.0 / math.sqrt(p)
+    vals, samples = [], []
+    for i in range(args.warmup + args.steps):
+        rate, n, dt, cores = cpu_baseline_sample(ev, eta, args.cpu_seconds / max(1, args.steps))
+        if i >= args.warmup:
+            vals.append(rate)
+            samples.append((n, dt))
+    value = float(np.median(vals))
+    n, dt = samples[-1]
+    ms = p * p / value * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"exact all-points transform, MP(c=0.5) p={p}, eta=1/sqrt(p)",
+                   "p": p, "route": "reference parallel all-points route (tiled full square)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{n} targets x {p} sources per step ({dt:.1f} s); "
+                                   "ms_per_step extrapolated to all p targets"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours --
+def run_ours(args, world, rank, local):
+    import torch
+    import shrinkers_b200 as rk
+    from shrinkers_b200 import _native, spectra
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+    L = _native.load()
+    p = args.p
+    prec = {"mixed": 1, "f64": 0}[args.precision]
+    ev_h = spectra.config2(p, seed=2 + rank)
+    eta = 1.0 / math.sqrt(p)
+    ev = torch.from_numpy(ev_h).to(dev)
+    re = torch.empty(p, dtype=torch.float64, device=dev)
+    im = torch.empty_like(re)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+    stream = torch.cuda.current_stream(dev)
+
+    def step(precision=prec, out=(re, im)):
+        st = L.shrk_stieltjes_all_dev(ev.data_ptr(), p, eta, 2, precision, float("nan"), 0,
+                                      out[0].data_ptr(), out[1].data_ptr(), stream.cuda_stream)
+        _native.check(st, "stieltjes_all_dev")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    L.shrk_timing_reset()
+    L.shrk_timing_enable(1)
+    clocks = ClockSampler(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)  # L2 flush between timed iterations (outside the events)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    launches = int(L.shrk_launch_count())
+    L.shrk_timing_enable(0)
+    import ctypes as C
+    kname = b"pair_sum_mixed" if prec == 1 else b"pair_sum_f64"
+    kn, kms = C.c_int64(), C.c_double()
+    L.shrk_timing_read(kname, C.byref(kn), C.byref(kms))
+    total_ms = float(np.sum(times))
+    if pg:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    value = world * p * p / (ms * 1e-3)
+
+    # ---- end-to-end through the public C ABI with host buffers
+    ev_pin = torch.from_numpy(ev_h).pin_memory()
+    ore = torch.empty(p, dtype=torch.float64).pin_memory()
+    oim = torch.empty(p, dtype=torch.float64).pin_memory()
+    _D = C.POINTER(C.c_double)
+
+    def e2e_call():
+        st = L.shrk_stieltjes_all(C.cast(ev_pin.data_ptr(), _D), p, eta, 2, prec, float("nan"), 0,
+                                  C.cast(ore.data_ptr(), _D), C.cast(oim.data_ptr(), _D))
+        _native.check(st, "stieltjes_all")
+
+    e2e_call()
+    e2e_times = []
+    for _ in range(max(2, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        e2e_call()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(e2e_times))
+    if pg:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * p * p / e2e_s
+
+    extras = {}
+    roof = None
+    cpu = None
+    if rank == 0:
+        # ---- roofline of the dominant kernel (library CUDA-event timing)
+        f32r, f64r = C.c_double(), C.c_double()
+        _native.check(L.shrk_measure_pipe_rates(C.byref(f32r), C.byref(f64r)))
+        k_avg_s = kms.value / max(kn.value, 1) * 1e-3
+        ops_per_pair = 6.0 if prec == 1 else 7.0
+        peak = f32r.value if prec == 1 else f64r.value
+        achieved = p * p * ops_per_pair / k_avg_s
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get(kname.decode())
+        roof = {"bound": "fp32" if prec == 1 else "fp64", "achieved": achieved / 1e12,
+                "peak": peak / 1e12, "unit": "Tops/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": kname.decode(),
+                "kernel_ms": k_avg_s * 1e3, "kernel_launches": kn.value,
+                "basis": (f"{ops_per_pair:g} pipe lane-ops per pair evaluation x p^2 pairs per "
+                          "launch / CUDA-event kernel time; peak = measured FMA lane-op rate "
+                          "of this GPU (shrk_measure_pipe_rates)")}
+        if not args.no_extras:
+            extras = secondary(args, L, dev, ev, ev_h, eta, p, stream)
+        cpu_rate, n, dt, cores = cpu_baseline_sample(ev_h, eta, args.cpu_seconds)
+        cpu = {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{n} of {p} targets x {p} sources, {dt:.1f} s, reference parallel "
+                         "route restated in C++ (OpenMP)"}
+
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if prec == 1 else "f64", "data": "synthetic",
+        "config": {"workload": f"exact all-points transform, MP(c=0.5) p={p}, eta=1/sqrt(p), "
+                               f"{args.precision} kernel",
+                   "p": p, "eta": eta, "precision": args.precision,
+                   "l2": "flushed between timed iterations (256 MiB write)",
+                   "parallelism": f"{world} GPU(s), one transform per GPU"},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * p,
+                "d2h_bytes_per_step": 16 * p, "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "extras": extras,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def secondary(args, L, dev, ev, ev_h, eta, p, stream):
+    """FP64 vs mixed at p (speed + error), p = 50k both kernels, and the
+    forward + adjoint cost at p = 20k."""
+    import torch
+    from shrinkers_b200 import _native, spectra
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {}
+    r64 = torch.empty(p, dtype=torch.float64, device=dev)
+    i64 = torch.empty_like(r64)
+    rmx = torch.empty_like(r64)
+    imx = torch.empty_like(r64)
+
+    def run(prec, a, b, evt=ev, pp=p, e=eta):
+        _native.check(L.shrk_stieltjes_all_dev(evt.data_ptr(), pp, e, 2, prec, float("nan"), 0,
+                                               a.data_ptr(), b.data_ptr(), stream.cuda_stream))
+
+    out["fp64_ms"] = timed(lambda: run(0, r64, i64), 2)
+    out["mixed_ms"] = timed(lambda: run(1, rmx, imx), 3)
+    out["mixed_speedup_vs_fp64"] = out["fp64_ms"] / out["mixed_ms"]
+    a64 = torch.complex(r64, i64)
+    amx = torch.complex(rmx, imx)
+    rel = (torch.abs(amx - a64) / torch.abs(a64)).cpu().numpy()
+    out["mixed_vs_fp64_rel_err_median"] = float(np.median(rel))
+    out["mixed_vs_fp64_rel_err_max"] = float(np.max(rel))
+    out["mixed_pairs_per_s"] = p * p / (out["mixed_ms"] * 1e-3)
+    out["fp64_pairs_per_s"] = p * p / (out["fp64_ms"] * 1e-3)
+    # p = 50k
+    p2 = 50_000
+    ev2 = torch.from_numpy(spectra.config2(p2)).to(dev)
+    e2 = 1.0 / math.sqrt(p2)
+    a = torch.empty(p2, dtype=torch.float64, device=dev)
+    b = torch.empty_like(a)
+    out["p50k_fp64_ms"] = timed(lambda: run(0, a, b, ev2, p2, e2), 10)
+    out["p50k_mixed_ms"] = timed(lambda: run(1, a, b, ev2, p2, e2), 10)
+    # forward + adjoint at p = 20k (exact)
+    p3 = 20_000
+    ev3 = torch.from_numpy(spectra.config5(p3)).to(dev)
+    e3 = 1.0 / math.sqrt(p3)
+    g = torch.randn(2, p3, dtype=torch.float64, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
+    fr = torch.empty(p3, dtype=torch.float64, device=dev)
+    fi = torch.empty_like(fr)
+    gr = torch.empty_like(fr)
+    for prec, name in [(0, "f64"), (1, "mixed")]:
+        f_ms = timed(lambda: run(prec, fr, fi, ev3, p3, e3), 10)
+
+        def fa():
+            run(prec, fr, fi, ev3, p3, e3)
+            _native.check(L.shrk_stieltjes_adjoint_dev(ev3.data_ptr(), p3, e3, g[0].data_ptr(),
+                                                       g[1].data_ptr(), prec, gr.data_ptr(),
+                                                       stream.cuda_stream))
+        fa_ms = timed(fa, 10)
+        out[f"p20k_{name}_fwd_ms"] = f_ms
+        out[f"p20k_{name}_fwd_adj_ms"] = fa_ms
+        out[f"p20k_{name}_fwd_adj_over_fwd"] = fa_ms / f_ms
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,200 @@
+/*
+ * shrinkers_b200 -- C ABI of the B200 Stieltjes-transform hot path.
+ *
+ * Drop-in boundary for the `stieltjes` dispatcher of the shrinkers crate
+ * (alexisrosuel/shrinkers).  Every entry point below names the reference
+ * function it replaces (path:line inside the crate).  Plain pointers and
+ * sizes only; no allocation is visible to the caller (device scratch is
+ * cached per device inside the library); every function returns a status
+ * code and never aborts.  Host-pointer entry points copy the inputs to the
+ * device, run on a library-owned stream and copy the outputs back; `_dev`
+ * entry points take device pointers and a cudaStream_t (as void*; NULL = the
+ * legacy default stream) and are
+ * stream-ordered (no host synchronisation unless stated).
+ *
+ * Conventions (identical to the reference):
+ *   raw sum   S(x) = sum_j 1/((x - ev_j) - i*eta)       (src/stieltjes/term.rs:26-31)
+ *             Re = sum d/(d^2+eta^2), Im = sum eta/(d^2+eta^2) > 0, d = x - ev_j;
+ *   all-points entry points return S(ev_i)/p (mod.rs:601-790 scale_soa/aos);
+ *   at-points entry points return raw sums (mod.rs:394-494).
+ *   The diagonal term i = j is included (it contributes i/eta).
+ */
+#ifndef SHRINKERS_B200_H
+#define SHRINKERS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status -- */
+typedef enum {
+  SHRK_OK = 0,
+  SHRK_EINVAL = 1,   /* invalid argument (message via shrk_last_error)        */
+  SHRK_ECUDA = 2,    /* CUDA runtime error or no usable device                */
+  SHRK_ETIMEOUT = 3, /* a bounded device-side wait gave up                    */
+  SHRK_ENOTIMPL = 4, /* method outside the GPU path (see shrk_method)         */
+  SHRK_ENOMEM = 5    /* device allocation failed                              */
+} shrk_status;
+
+/* Method identifiers: same names and order as StieltjesMethod
+ * (src/config.rs:19-89).  Exact family (NAIVE .. BLOCKED_HYBRID) -> GPU exact
+ * kernels; CHEBCODE* -> GPU treecode with the same ChebPreset; NUFFT -> GPU
+ * coarse-grid NUFFT; AUTO/SPEED_AUTO/ACCURACY_AUTO -> resolved exactly as
+ * config::resolve_auto_method.  ADAPTIVE, FFT5/3/2, TREECODE, EWALD, DST and
+ * HODLR return SHRK_ENOTIMPL (no CPU fallback). */
+typedef enum {
+  SHRK_M_NAIVE = 0, SHRK_M_AUTOVEC, SHRK_M_BLOCKED, SHRK_M_BLOCKED_AUTOVEC,
+  SHRK_M_BLOCKED_TILED, SHRK_M_BLOCKED_WINDOWED, SHRK_M_BLOCKED_HYBRID,
+  SHRK_M_ADAPTIVE, SHRK_M_FFT5, SHRK_M_FFT3, SHRK_M_FFT2, SHRK_M_NUFFT,
+  SHRK_M_TREECODE, SHRK_M_CHEBCODE, SHRK_M_CHEBCODE_FAST, SHRK_M_CHEBCODE_XTREME,
+  SHRK_M_CHEBCODE_BALANCED, SHRK_M_EWALD, SHRK_M_DST, SHRK_M_AUTO, SHRK_M_HODLR,
+  SHRK_M_SPEED_AUTO, SHRK_M_ACCURACY_AUTO
+} shrk_method;
+
+/* Arithmetic of the exact kernels.  F64: every pair in FP64.  MIXED: pairs
+ * farther apart than shrk_mixed_near_k()*eta in FP32 with compensated
+ * accumulation, nearer pairs and all reductions in FP64.  (The reference's
+ * own `precision="f32"` path is shrk_stieltjes_all_f32.) */
+typedef enum { SHRK_PREC_F64 = 0, SHRK_PREC_MIXED = 1 } shrk_precision;
+
+/* Parallelism of the reference (config.rs:200-226).  The GPU computes the
+ * same sums whatever the value; it only selects which reference route the
+ * auto policy and the parity tests follow. */
+typedef enum { SHRK_PAR_SEQUENTIAL = 0, SHRK_PAR_PARALLEL = 1, SHRK_PAR_AUTO = 2 } shrk_parallelism;
+
+/* ------------------------------------------------------- diagnostics -- */
+/* Copies the last error message of the calling thread (NUL-terminated). */
+size_t shrk_last_error(char* buf, size_t len);
+/* Library version string, e.g. "0.1.0". */
+const char* shrk_version(void);
+/* Number of visible CUDA devices (0 when none); never fails. */
+int shrk_device_count(void);
+
+/* ---------------------------------------------------- method policy -- */
+/* python.rs:321-350 parse_method (all aliases).  SHRK_EINVAL on unknown. */
+shrk_status shrk_parse_method(const char* name, int* method_out);
+/* config.rs:92-118 StieltjesMethod::name. */
+const char* shrk_method_name(int method);
+/* config.rs:543-555 resolve_auto_method (+ pareto_autogen.rs:22-86). */
+int shrk_resolve_auto_method(int method, int parallel, size_t p);
+/* config.rs:565-585 grid_appropriate. */
+int shrk_grid_appropriate(int method, size_t p, size_t nq);
+/* Near-field radius (in units of eta) of the MIXED exact kernel. */
+double shrk_mixed_near_k(void);
+
+/* ------------------------------------------------------ transforms -- */
+/* mod.rs:601-790 compute_all_stieltjes: S(ev_i)/p for every i.
+ * cutoff_ratio: NaN = CutoffConfig::Disabled, else Enabled{ratio}. */
+shrk_status shrk_stieltjes_all(const double* ev, size_t p, double eta, int method,
+                               int precision, double cutoff_ratio, int parallelism,
+                               double* out_re, double* out_im);
+/* Device-pointer form of shrk_stieltjes_all (ev, out_* on the device). */
+shrk_status shrk_stieltjes_all_dev(const double* d_ev, size_t p, double eta, int method,
+                                   int precision, double cutoff_ratio, int parallelism,
+                                   double* d_re, double* d_im, void* stream);
+/* mod.rs:805-848 compute_all_stieltjes_f32 (precision="f32",
+ * python.rs:820-829): FP32 full-square sum scaled by 1/p in FP32. */
+shrk_status shrk_stieltjes_all_f32(const float* ev, size_t p, float eta, int method,
+                                   double cutoff_ratio, float* out_re, float* out_im);
+/* mod.rs:394-494 compute_stieltjes_at_points: RAW sums at nq query points. */
+shrk_status shrk_stieltjes_at_points(const double* q, size_t nq, const double* ev, size_t p,
+                                     double eta, int method, int precision, double cutoff_ratio,
+                                     int parallelism, double* raw_re, double* raw_im);
+shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const double* d_ev,
+                                         size_t p, double eta, int method, int precision,
+                                         double cutoff_ratio, int parallelism, double* d_re,
+                                         double* d_im, void* stream);
+/* autovec.rs:38-77 compute_all_stieltjes_with_deriv (python.rs:758-781):
+ * RAW value and derivative w.r.t. the query point at every eigenvalue. */
+shrk_status shrk_stieltjes_with_deriv(const double* ev, size_t p, double eta, double* re,
+                                      double* im, double* dre, double* dim);
+
+/* Batched uneven spectra (no reference counterpart; replaces a host loop of
+ * compute_all_stieltjes calls): spectrum s is ev[offsets[s] .. offsets[s+1]),
+ * evaluated at its own eta[s]; outputs are scaled by 1/p_s and laid out like
+ * the input.  One persistent launch pulls (spectrum, target tile, source
+ * split) items from a device queue. */
+shrk_status shrk_stieltjes_batched(const double* ev, const int64_t* offsets, size_t n_spectra,
+                                   const double* eta, int precision, double* out_re,
+                                   double* out_im);
+shrk_status shrk_stieltjes_batched_dev(const double* d_ev, const int64_t* d_offsets,
+                                       size_t n_spectra, const double* d_eta, int precision,
+                                       double* d_re, double* d_im, void* stream);
+
+/* Adjoint of m(z_j) = (1/p) sum_i 1/(ev_i - z_j), z_j = ev_j + i*eta (the
+ * -conj(S)/p convention; no reference counterpart).  Given cotangents
+ * g_j = g_re[j] + i g_im[j] of L = sum_j Re(conj(g_j) m_j), writes
+ * grad[k] = dL/d ev_k including the dependence of z_k on ev_k. */
+shrk_status shrk_stieltjes_adjoint(const double* ev, size_t p, double eta, const double* g_re,
+                                   const double* g_im, int precision, double* grad);
+shrk_status shrk_stieltjes_adjoint_dev(const double* d_ev, size_t p, double eta,
+                                       const double* d_g_re, const double* d_g_im, int precision,
+                                       double* d_grad, void* stream);
+
+/* ------------------------------------------------------- consumers -- */
+/* shrinkage.rs:22-34 shrinkage_factor (pure host arithmetic). */
+double shrk_shrinkage_factor(double lambda, double c, double m_re, double m_im);
+/* estimation.rs:48-56 inverse_bbp; estimation.rs:37-39 bbp_threshold. */
+double shrk_inverse_bbp(double lambda_hat, double gamma, double sigma2);
+double shrk_bbp_threshold(double gamma, double sigma2);
+/* detection.rs:75-83 mp_median_factor. */
+double shrk_mp_median_factor(double gamma);
+/* detection.rs:134-153 detect_spikes_bema on an ASCENDING spectrum.
+ * spike_indices must hold p entries; *k receives the count. */
+shrk_status shrk_detect_spikes_bema(const double* sorted, size_t p, double gamma, double margin,
+                                    size_t* k, int64_t* spike_indices, double* bulk_edge,
+                                    double* sigma2);
+/* estimation.rs:75-90 ledoit_wolf_shrinkage: xi_i from the GPU transform
+ * with the LW map fused into the FP64 reduction epilogue.  eta NaN ->
+ * 0.4/sqrt(p) (mod.rs:150-153).  Input order preserved. */
+shrk_status shrk_ledoit_wolf_shrinkage(const double* ev, size_t p, double c, int method,
+                                       int precision, int parallelism, double eta, double* xi);
+/* shrinkage.rs:60-84 rie_shrinkage (trace-rescaled). */
+shrk_status shrk_rie_shrinkage(const double* ev, size_t p, double c, int method, int precision,
+                               int parallelism, double* xi);
+/* deconvolution/mod.rs:116-259 spectral_deconvolution with the MP inversion
+ * fused into the grid transform's epilogue.  eta/lambda_min/lambda_max NaN =
+ * None.  out7 holds 7*n_points doubles: lambda_grid, density, w_re,
+ * sample_stieltjes_real/imag, population_stieltjes_real/imag. */
+shrk_status shrk_spectral_deconvolution(const double* ev, size_t p, double c, size_t n_points,
+                                        double eta, double lambda_min, double lambda_max,
+                                        int method, int precision, int parallelism,
+                                        double cutoff_ratio, double* out7);
+/* population.rs:72-116 estimate_population_eigenvalues (RmtConfig::new:
+ * Blocked, sequential, eta = 0.4/sqrt(p_bulk)).  spikes/spike_sample hold p
+ * entries (descending on return), bulk_population/bulk_sample p entries
+ * (p - k written, ascending in the sample eigenvalue). */
+shrk_status shrk_estimate_population_eigenvalues(const double* ev, size_t p, double c,
+                                                 double margin, int precision, size_t* k,
+                                                 double* spikes, double* spike_sample,
+                                                 double* bulk_edge, double* sigma2,
+                                                 double* bulk_population, double* bulk_sample);
+/* hybrid.rs:96-138 deconvolve_spiked (eta NaN -> 0.1/sqrt(p_bulk)). */
+shrk_status shrk_deconvolve_spiked(const double* ev, size_t p, double c, size_t n_points,
+                                   double eta, double margin, int method, int precision,
+                                   int parallelism, double cutoff_ratio, size_t* k,
+                                   double* spikes, double* spike_sample, double* bulk_edge,
+                                   double* sigma2, double* out7);
+
+/* ------------------------------------------------------- profiling -- */
+/* Per-kernel CUDA-event timing of the library's own launches (off by
+ * default).  shrk_timing_read returns the number of launches of the kernel
+ * family `name` since the last reset and their summed duration (ms). */
+void shrk_timing_enable(int on);
+void shrk_timing_reset(void);
+shrk_status shrk_timing_read(const char* name, int64_t* launches, double* total_ms);
+/* Number of kernels the library launched since the last reset. */
+int64_t shrk_launch_count(void);
+/* Measured FMA issue rates of the current device (lane-operations per
+ * second, one FMA = one op) for FP32 and FP64: the roofline denominators of
+ * the exact kernels.  Runs two short probe kernels. */
+shrk_status shrk_measure_pipe_rates(double* fp32_ops_per_s, double* fp64_ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHRINKERS_B200_H */

@@ -1,0 +1,389 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front-end of the CPU restatement.
+
+The oracle restates the shrinkers crate's Stieltjes-transform algorithms in
+C++ (``oracle_*.cpp``, each function citing the reference file:line it
+follows) and is used as the parity checker for the CUDA path and as the
+timed CPU baseline.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import this module; the product package
+``shrinkers_b200`` never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "_build", "liboracle.so")
+
+# Method identifiers: declaration order of StieltjesMethod (src/config.rs:19-89).
+METHODS = [
+    "naive", "autovec", "blocked", "blocked_autovec", "blocked_tiled",
+    "blocked_windowed", "blocked_hybrid", "adaptive", "fft5", "fft3", "fft2",
+    "nufft", "treecode", "chebcode", "chebcode_fast", "chebcode_xtreme",
+    "chebcode_balanced", "ewald", "dst", "auto", "hodlr", "speed_auto",
+    "accuracy_auto",
+]
+M = {name: i for i, name in enumerate(METHODS)}
+
+_D = C.POINTER(C.c_double)
+_F = C.POINTER(C.c_float)
+_I64 = C.POINTER(C.c_int64)
+_SZ = C.c_size_t
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    if force or not os.path.exists(_SO):
+        subprocess.run(["make", "-C", _HERE, "-s"], check=True)
+    return _SO
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(_SO)
+        sig = {
+            "orc_resolve_auto_method": (C.c_int, [C.c_int, C.c_int, _SZ]),
+            "orc_grid_appropriate": (C.c_int, [C.c_int, _SZ, _SZ]),
+            "orc_term": (None, [C.c_double, C.c_double, C.c_double, _D, _D]),
+            "orc_term_hoisted": (None, [C.c_double, C.c_double, C.c_double, _D, _D]),
+            "orc_naive_sum": (None, [C.c_double, _D, _SZ, C.c_double, _D, _D]),
+            "orc_autovec_sum": (None, [C.c_double, _D, _SZ, C.c_double, _D, _D]),
+            "orc_symmetric_sweep": (None, [_D, _SZ, C.c_double, _D, _D]),
+            "orc_tiled_full_square": (None, [_D, _SZ, C.c_double, _D, _D]),
+            "orc_blocked_at_points": (None, [_D, _SZ, _D, _SZ, C.c_double, C.c_double, _D, _D]),
+            "orc_compute_all": (C.c_int, [_D, _SZ, C.c_double, C.c_int, C.c_double, C.c_int, _D, _D]),
+            "orc_compute_at_points": (C.c_int, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, C.c_double, C.c_int, _D, _D]),
+            "orc_tiled_targets": (None, [_D, _SZ, _D, _SZ, C.c_double, _D, _D]),
+            "orc_all_f32": (None, [_F, _SZ, C.c_float, _F, _F]),
+            "orc_with_deriv": (None, [_D, _SZ, C.c_double, _D, _D, _D, _D]),
+            "orc_truth_points": (None, [_D, _SZ, _D, _SZ, C.c_double, _D, _D]),
+            "orc_adjoint_direct": (None, [_D, _SZ, C.c_double, _D, _D, C.POINTER(C.c_long), _SZ, _D]),
+            "orc_num_threads": (C.c_int, []),
+            "orc_set_num_threads": (None, [C.c_int]),
+            "orc_chebcode_points": (None, [_D, _SZ, _D, _SZ, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, _D, _D]),
+            "orc_grid_leaf_cap": (_SZ, [_SZ, _SZ, _SZ, _SZ]),
+            "orc_chebtree_export": (_SZ, [_D, _SZ, C.c_int, C.c_double, _SZ, _D, _D, _I64, _I64, C.POINTER(C.c_int32), _D, _D]),
+            "orc_nufft_grid_size": (_SZ, [C.c_double, C.c_double]),
+            "orc_nufft_points": (None, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, _D, _D]),
+            "orc_nufft_grid": (_SZ, [_D, _SZ, C.c_double, _D, _D, _D, _D]),
+            "orc_fft": (None, [_D, _SZ, C.c_int]),
+            "orc_lagrange4": (None, [C.c_double, _D]),
+            "orc_shrinkage_factor": (C.c_double, [C.c_double] * 4),
+            "orc_inverse_bbp": (C.c_double, [C.c_double] * 3),
+            "orc_bbp_threshold": (C.c_double, [C.c_double] * 2),
+            "orc_mp_median_factor": (C.c_double, [C.c_double]),
+            "orc_bema": (_SZ, [_D, _SZ, C.c_double, C.c_double, _I64, _D, _D]),
+            "orc_ledoit_wolf": (C.c_int, [_D, _SZ, C.c_double, C.c_int, C.c_int, C.c_double, _D]),
+            "orc_rie": (C.c_int, [_D, _SZ, C.c_double, C.c_int, C.c_int, _D]),
+            "orc_spectral_deconvolution": (C.c_int, [_D, _SZ, C.c_double, _SZ, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _D]),
+            "orc_estimate_population": (C.c_int, [_D, _SZ, C.c_double, C.c_double, C.POINTER(_SZ), _D, _D, _D, _D, _D, _D]),
+            "orc_deconvolve_spiked": (C.c_int, [_D, _SZ, C.c_double, _SZ, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.POINTER(_SZ), _D, _D, _D, _D, _D]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_D)
+
+
+def _arr(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def _nan(x):
+    return float("nan") if x is None else float(x)
+
+
+def method_id(m) -> int:
+    return m if isinstance(m, int) else M[m]
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_num_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+# ----------------------------------------------------------------- exact --
+def term(li, lj, eta):
+    r, i = C.c_double(), C.c_double()
+    lib().orc_term(li, lj, eta, C.byref(r), C.byref(i))
+    return r.value, i.value
+
+
+def naive_sum(x, ev, eta):
+    ev = _arr(ev)
+    r, i = C.c_double(), C.c_double()
+    lib().orc_naive_sum(x, _d(ev), ev.size, eta, C.byref(r), C.byref(i))
+    return r.value, i.value
+
+
+def autovec_sum(x, ev, eta):
+    ev = _arr(ev)
+    r, i = C.c_double(), C.c_double()
+    lib().orc_autovec_sum(x, _d(ev), ev.size, eta, C.byref(r), C.byref(i))
+    return r.value, i.value
+
+
+def symmetric_sweep(ev, eta):
+    ev = _arr(ev)
+    re, im = np.empty_like(ev), np.empty_like(ev)
+    lib().orc_symmetric_sweep(_d(ev), ev.size, eta, _d(re), _d(im))
+    return re, im
+
+
+def tiled_full_square(ev, eta):
+    ev = _arr(ev)
+    re, im = np.empty_like(ev), np.empty_like(ev)
+    lib().orc_tiled_full_square(_d(ev), ev.size, eta, _d(re), _d(im))
+    return re, im
+
+
+def tiled_targets(targets, ev, eta):
+    """Parallel all-points route of the reference for a subset of targets (raw)."""
+    t, ev = _arr(targets), _arr(ev)
+    re, im = np.empty_like(t), np.empty_like(t)
+    lib().orc_tiled_targets(_d(t), t.size, _d(ev), ev.size, eta, _d(re), _d(im))
+    return re, im
+
+
+def compute_all(ev, eta, method="blocked", cutoff=None, parallel=False):
+    """compute_all_stieltjes (src/stieltjes/mod.rs:601-790), scaled by 1/p."""
+    ev = _arr(ev)
+    re, im = np.empty_like(ev), np.empty_like(ev)
+    st = lib().orc_compute_all(_d(ev), ev.size, eta, method_id(method), _nan(cutoff),
+                               int(bool(parallel)), _d(re), _d(im))
+    if st:
+        raise NotImplementedError(f"oracle does not restate method {method!r}")
+    return re, im
+
+
+def compute_at_points(q, ev, eta, method="blocked", cutoff=None, parallel=False):
+    """compute_stieltjes_at_points (src/stieltjes/mod.rs:394-494), raw sums."""
+    q, ev = _arr(q), _arr(ev)
+    re, im = np.empty_like(q), np.empty_like(q)
+    st = lib().orc_compute_at_points(_d(q), q.size, _d(ev), ev.size, eta, method_id(method),
+                                     _nan(cutoff), int(bool(parallel)), _d(re), _d(im))
+    if st:
+        raise NotImplementedError(f"oracle does not restate method {method!r}")
+    return re, im
+
+
+def all_f32(ev, eta):
+    ev = np.ascontiguousarray(np.asarray(ev, dtype=np.float32))
+    re, im = np.empty_like(ev), np.empty_like(ev)
+    lib().orc_all_f32(ev.ctypes.data_as(_F), ev.size, np.float32(eta),
+                      re.ctypes.data_as(_F), im.ctypes.data_as(_F))
+    return re, im
+
+
+def with_deriv(ev, eta):
+    ev = _arr(ev)
+    out = [np.empty_like(ev) for _ in range(4)]
+    lib().orc_with_deriv(_d(ev), ev.size, eta, *[_d(o) for o in out])
+    return tuple(out)
+
+
+def truth_points(q, ev, eta):
+    """Raw sums in double-double arithmetic (the error-statistics truth)."""
+    q, ev = _arr(q), _arr(ev)
+    re, im = np.empty_like(q), np.empty_like(q)
+    lib().orc_truth_points(_d(q), q.size, _d(ev), ev.size, eta, _d(re), _d(im))
+    return re, im
+
+
+def adjoint_direct(ev, eta, w, v, idx=None):
+    ev, w, v = _arr(ev), _arr(w), _arr(v)
+    if idx is None:
+        n, ip = ev.size, None
+    else:
+        idxa = np.ascontiguousarray(np.asarray(idx, dtype=np.int64))
+        n, ip = idxa.size, idxa.ctypes.data_as(C.POINTER(C.c_long))
+    g = np.empty(n)
+    lib().orc_adjoint_direct(_d(ev), ev.size, eta, _d(w), _d(v), ip, n, _d(g))
+    return g
+
+
+# --------------------------------------------------------------- chebcode --
+PRESETS = {  # src/stieltjes/chebcode.rs:939-972
+    "chebcode": (0.5, 11, 32, False),
+    "chebcode_fast": (1.0, 8, 32, True),
+    "chebcode_xtreme": (0.25, 11, 16, False),
+    "chebcode_balanced": (0.55, 11, 32, False),
+}
+
+
+def chebcode_points(q, ev, eta, theta, n, leaf_cap, f32, parallel=True):
+    q, ev = _arr(q), _arr(ev)
+    re, im = np.empty_like(q), np.empty_like(q)
+    lib().orc_chebcode_points(_d(q), q.size, _d(ev), ev.size, eta, theta, n, leaf_cap,
+                              int(f32), int(parallel), _d(re), _d(im))
+    return re, im
+
+
+def grid_leaf_cap(n, p, nq, preset_leaf):
+    return int(lib().orc_grid_leaf_cap(n, p, nq, preset_leaf))
+
+
+def chebtree(sorted_ev, n, theta, leaf_cap):
+    s = _arr(sorted_ev)
+    L = lib()
+    nn = L.orc_chebtree_export(_d(s), s.size, n, theta, leaf_cap, None, None, None, None, None,
+                               None, None)
+    lo, hi = np.empty(nn), np.empty(nn)
+    li, hi_i = np.empty(nn, np.int64), np.empty(nn, np.int64)
+    right = np.empty(nn, np.int32)
+    nodes, w = np.empty(nn * n), np.empty(nn * n)
+    L.orc_chebtree_export(_d(s), s.size, n, theta, leaf_cap, _d(lo), _d(hi),
+                          li.ctypes.data_as(_I64), hi_i.ctypes.data_as(_I64),
+                          right.ctypes.data_as(C.POINTER(C.c_int32)), _d(nodes), _d(w))
+    return dict(lo=lo, hi=hi, lo_idx=li, hi_idx=hi_i, right=right,
+                nodes=nodes.reshape(nn, n), w=w.reshape(nn, n))
+
+
+# ------------------------------------------------------------------ nufft --
+def nufft_grid_size(raw_range, eta):
+    return int(lib().orc_nufft_grid_size(raw_range, eta))
+
+
+def nufft_points(q, ev, eta, parallel=False):
+    q, ev = _arr(q), _arr(ev)
+    re, im = np.empty_like(q), np.empty_like(q)
+    lib().orc_nufft_points(_d(q), q.size, _d(ev), ev.size, eta, int(parallel), _d(re), _d(im))
+    return re, im
+
+
+def nufft_grid(ev, eta):
+    ev = _arr(ev)
+    L = lib()
+    raw = float(ev[-1] - ev[0])
+    m = nufft_grid_size(raw, eta)
+    dens, packed = np.empty(m), np.empty(2 * m)
+    lo, dx = C.c_double(), C.c_double()
+    L.orc_nufft_grid(_d(ev), ev.size, eta, _d(dens), _d(packed), C.byref(lo), C.byref(dx))
+    return dict(m=m, density=dens, packed=packed[0::2] + 1j * packed[1::2], lo=lo.value,
+                dx=dx.value)
+
+
+def fft(x, sign=-1):
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.complex128)).copy()
+    lib().orc_fft(a.view(np.float64).ctypes.data_as(_D), a.size, int(sign))
+    return a
+
+
+def lagrange4(t):
+    w = np.empty(4)
+    lib().orc_lagrange4(t, _d(w))
+    return w
+
+
+# -------------------------------------------------------------- consumers --
+def shrinkage_factor(li, c, mr, mi):
+    return lib().orc_shrinkage_factor(li, c, mr, mi)
+
+
+def inverse_bbp(lh, gamma, sigma2=1.0):
+    return lib().orc_inverse_bbp(lh, gamma, sigma2)
+
+
+def bbp_threshold(gamma, sigma2):
+    return lib().orc_bbp_threshold(gamma, sigma2)
+
+
+def mp_median_factor(g):
+    return lib().orc_mp_median_factor(g)
+
+
+def bema(sorted_ev, gamma, margin=1.0):
+    s = _arr(sorted_ev)
+    idx = np.empty(max(s.size, 1), np.int64)
+    edge, s2 = C.c_double(), C.c_double()
+    k = lib().orc_bema(_d(s), s.size, gamma, margin, idx.ctypes.data_as(_I64), C.byref(edge),
+                       C.byref(s2))
+    return dict(k=int(k), spike_indices=idx[:k].copy(), bulk_edge=edge.value, sigma2=s2.value)
+
+
+def ledoit_wolf(ev, c, method="blocked", parallel=False, eta=None):
+    ev = _arr(ev)
+    out = np.empty_like(ev)
+    st = lib().orc_ledoit_wolf(_d(ev), ev.size, c, method_id(method), int(parallel), _nan(eta),
+                               _d(out))
+    if st:
+        raise NotImplementedError(method)
+    return out
+
+
+def rie(ev, c, method="blocked", parallel=False):
+    ev = _arr(ev)
+    out = np.empty_like(ev)
+    st = lib().orc_rie(_d(ev), ev.size, c, method_id(method), int(parallel), _d(out))
+    if st:
+        raise NotImplementedError(method)
+    return out
+
+
+_DECONV_KEYS = ["lambda_grid", "density", "w_re", "sample_stieltjes_real",
+                "sample_stieltjes_imag", "population_stieltjes_real",
+                "population_stieltjes_imag"]
+
+
+def spectral_deconvolution(ev, c, n_points=200, eta=None, lmin=None, lmax=None,
+                           method="blocked", parallel=False, cutoff=None):
+    ev = _arr(ev)
+    out = np.empty(7 * n_points)
+    st = lib().orc_spectral_deconvolution(_d(ev), ev.size, c, n_points, _nan(eta), _nan(lmin),
+                                          _nan(lmax), method_id(method), int(parallel),
+                                          _nan(cutoff), _d(out))
+    if st:
+        raise NotImplementedError(method)
+    o = out.reshape(7, n_points)
+    return {k: o[i].copy() for i, k in enumerate(_DECONV_KEYS)}
+
+
+def estimate_population_eigenvalues(ev, c, margin=1.0):
+    ev = _arr(ev)
+    p = ev.size
+    k = C.c_size_t()
+    sp, ss = np.empty(max(p, 1)), np.empty(max(p, 1))
+    bp, bs = np.empty(max(p, 1)), np.empty(max(p, 1))
+    edge, s2 = C.c_double(), C.c_double()
+    st = lib().orc_estimate_population(_d(ev), p, c, margin, C.byref(k), _d(sp), _d(ss),
+                                       C.byref(edge), C.byref(s2), _d(bp), _d(bs))
+    assert st == 0
+    kk = k.value
+    return dict(k=kk, spikes=sp[:kk].copy(), spike_sample=ss[:kk].copy(), bulk_edge=edge.value,
+                sigma2=s2.value, bulk_population=bp[:p - kk].copy(), bulk_sample=bs[:p - kk].copy())
+
+
+def deconvolve_spiked(ev, c, n_points=200, eta=None, margin=1.0, method="auto", parallel=False,
+                      cutoff=None):
+    ev = _arr(ev)
+    p = ev.size
+    k = C.c_size_t()
+    sp, ss = np.empty(max(p, 1)), np.empty(max(p, 1))
+    edge, s2 = C.c_double(), C.c_double()
+    out = np.empty(7 * n_points)
+    st = lib().orc_deconvolve_spiked(_d(ev), p, c, n_points, _nan(eta), margin, method_id(method),
+                                     int(parallel), _nan(cutoff), C.byref(k), _d(sp), _d(ss),
+                                     C.byref(edge), C.byref(s2), _d(out))
+    if st:
+        raise NotImplementedError(method)
+    kk = k.value
+    o = out.reshape(7, n_points)
+    return dict(k=kk, spikes=sp[:kk].copy(), spike_sample=ss[:kk].copy(), bulk_edge=edge.value,
+                sigma2=s2.value, bulk={key: o[i].copy() for i, key in enumerate(_DECONV_KEYS)})

@@ -1,0 +1,249 @@
+// TEST INFRASTRUCTURE ONLY (see oracle.h): restatement of the coarse-grid
+// NUFFT of src/stieltjes/nufft.rs (grid policy 33-126, entry points
+// 164-220) over the dual-convolution core of src/stieltjes/fft5.rs
+// (lagrange_weights 136-164, splat 175-185, interp_at 191-211,
+// fft_convolution 325-432, interpolate_grid 440-476) and the packing helpers
+// of src/stieltjes/fftplan.rs:43-76.
+//
+// The reference's transforms come from rustfft 6.4.1 (Cargo.lock), which is
+// not vendored.  Its published contract -- unnormalised DFT, forward sign
+// e^{-2 pi i jk/m}, inverse e^{+2 pi i jk/m} -- is restated here with an
+// iterative radix-2 decimation-in-time FFT of our own; the rounding of
+// rustfft's mixed-radix plans is not reproduced, so FFT-level parity with the
+// reference is by tolerance only.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <vector>
+#include <omp.h>
+
+namespace orc {
+
+typedef std::complex<double> cplx;
+
+// nufft.rs:33-58
+static const double PAD_ETA_MULT = 2000.0, PAD_RANGE_FRAC = 0.75, RESOLUTION = 5.0;
+static const size_t MIN_GRID = 8192, MAX_GRID = 65536;
+
+static size_t next_pow2(size_t n) {  // mod.rs:529-535
+  size_t p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+// nufft.rs:106-126 grid_size_for_range.
+size_t nufft_grid_size(double raw_range, double eta) {
+  double pad = std::max(PAD_ETA_MULT * eta, PAD_RANGE_FRAC * raw_range);
+  double range = raw_range + 2.0 * pad;
+  size_t max_grid = std::max(std::max(MAX_GRID, MIN_GRID), (size_t)2);
+  double target = RESOLUTION * range / eta;
+  target = std::isfinite(target) ? std::min(target, (double)max_grid) : (double)max_grid;
+  return std::min(next_pow2(std::max((size_t)std::ceil(target), MIN_GRID)), max_grid);
+}
+
+// fft5.rs:136-164 lagrange_weights<N>.
+template <int N>
+static inline void lagrange_weights(double t, double* w) {
+  const double q = (double)(N / 2);
+  double pref[N], suf[N], acc = 1.0;
+  for (int j = 0; j < N; ++j) {
+    pref[j] = acc;
+    acc *= t - (double)j + q - 1.0;
+  }
+  acc = 1.0;
+  for (int j = N - 1; j >= 0; --j) {
+    suf[j] = acc;
+    acc *= t - (double)j + q - 1.0;
+  }
+  for (int j = 0; j < N; ++j) {
+    double den = 1.0;
+    for (int l = 0; l < N; ++l)
+      if (l != j) den *= (double)(j - l);
+    w[j] = pref[j] * suf[j] / den;
+  }
+}
+
+// fft5.rs:175-185 splat<4> (Cubic, the NUFFT default).
+static inline void splat4(double* density, size_t m, double pos) {
+  double fl = std::floor(pos);
+  long i0 = (long)fl;
+  double t = pos - (double)i0;
+  double w[4];
+  lagrange_weights<4>(t, w);
+  const long off0 = -4 / 2 + 1;
+  for (int j = 0; j < 4; ++j) {
+    long cell = std::min(std::max(i0 + off0 + j, 0L), (long)m - 1);
+    density[cell] += w[j];
+  }
+}
+
+// Radix-2 iterative DFT, unnormalised; sign = -1 forward, +1 inverse.
+void fft_radix2(cplx* a, size_t m, int sign) {
+  for (size_t i = 1, j = 0; i < m; ++i) {
+    size_t bit = m >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  std::vector<cplx> tw(m / 2);
+  for (size_t k = 0; k < m / 2; ++k) {
+    double ang = 2.0 * M_PI * (double)k / (double)m;
+    tw[k] = cplx(std::cos(ang), sign * std::sin(ang));
+  }
+  for (size_t len = 2; len <= m; len <<= 1) {
+    size_t step = m / len;
+    for (size_t i = 0; i < m; i += len) {
+      for (size_t k = 0; k < len / 2; ++k) {
+        cplx u = a[i + k], v = a[i + k + len / 2] * tw[k * step];
+        a[i + k] = u + v;
+        a[i + k + len / 2] = u - v;
+      }
+    }
+  }
+}
+
+struct Grid { std::vector<cplx> out; double lo, dx; size_t m; };
+
+// fft5.rs:325-432 fft_convolution with the NUFFT options (Cubic stencil,
+// m = grid_size, pad = max(2000 eta, 0.75 raw_range)).
+static void convolution(const double* ev, size_t p, double eta, bool parallel, Grid& G) {
+  double lo_raw = ev[0], hi_raw = ev[p - 1];
+  double raw_range = hi_raw - lo_raw;
+  size_t m = std::max(nufft_grid_size(raw_range, eta), (size_t)2);
+  double pad = std::max(PAD_ETA_MULT * eta, PAD_RANGE_FRAC * raw_range);
+  double lo = lo_raw - pad, hi = hi_raw + pad;
+  double range = hi - lo;
+  double dx = range / (double)m;
+  size_t half = m / 2;
+
+  std::vector<double> density(m, 0.0);
+  if (parallel && p >= 4096) {  // fft5.rs:259-292 per-worker buffers + reduce
+    int nt = omp_get_max_threads();
+    std::vector<std::vector<double>> bufs(nt, std::vector<double>(m, 0.0));
+    size_t chunk = (p + nt - 1) / nt;
+#pragma omp parallel num_threads(nt)
+    {
+      int t = omp_get_thread_num();
+      size_t a = std::min(p, (size_t)t * chunk), b = std::min(p, a + chunk);
+      for (size_t k = a; k < b; ++k) splat4(bufs[t].data(), m, (ev[k] - lo) / dx);
+    }
+    for (int t = 0; t < nt; ++t)
+      for (size_t i = 0; i < m; ++i) density[i] += bufs[t][i];
+  } else {
+    for (size_t k = 0; k < p; ++k) splat4(density.data(), m, (ev[k] - lo) / dx);
+  }
+
+  std::vector<cplx> packed(m);
+  const double mf = (double)m;
+  for (size_t i = 0; i < m; ++i) {
+    double sd = (i <= half) ? (double)i : (double)i - mf;
+    double x = sd * dx;
+    double denom = x * x + eta * eta;
+    packed[i] = cplx(density[i], x / denom);
+  }
+  fft_radix2(packed.data(), m, -1);
+  // fftplan.rs:43-54 unpack_packed_real_pair
+  std::vector<cplx> D(m), K(m);
+  for (size_t k = 0; k < m; ++k) {
+    cplx ck = packed[k], cnk = std::conj(packed[(m - k) % m]);
+    cplx s = ck + cnk, df = ck - cnk;
+    D[k] = cplx(0.5 * s.real(), 0.5 * s.imag());
+    // (-0.5 i) * df
+    K[k] = cplx(0.5 * df.imag(), -0.5 * df.real());
+  }
+  // fft5.rs:404-416 analytic even kernel
+  double r = std::exp(-2.0 * M_PI * eta / ((double)m * dx));
+  double ke0 = M_PI / dx;
+  std::vector<double> ke(m);
+  double pw = 1.0;
+  for (size_t k = 0; k <= half; ++k) { ke[k] = ke0 * pw; pw *= r; }
+  pw = r;
+  for (size_t k = m - 1; k > half; --k) { ke[k] = ke0 * pw; pw *= r; }
+  // fftplan.rs:62-76 pack_dual_product
+  G.out.resize(m);
+  for (size_t k = 0; k < m; ++k) {
+    cplx d = D[k];
+    double ih_re = d.real() * ke[k], ih_im = d.imag() * ke[k];
+    cplx rh = d * K[k];
+    G.out[k] = cplx(ih_re - rh.imag(), ih_im + rh.real());
+  }
+  fft_radix2(G.out.data(), m, +1);
+  G.lo = lo;
+  G.dx = dx;
+  G.m = m;
+}
+
+// fft5.rs:191-211 interp_at<4> + 440-476 interpolate_grid.
+static void interpolate(const Grid& G, const double* q, size_t nq, bool parallel, double* re,
+                        double* im) {
+  const double inv_m = 1.0 / (double)G.m;
+#pragma omp parallel for schedule(static) if (parallel && nq >= 4096)
+  for (long k = 0; k < (long)nq; ++k) {
+    double pos = (q[k] - G.lo) / G.dx;
+    long i0 = (long)std::floor(pos);
+    double t = pos - (double)i0, w[4];
+    lagrange_weights<4>(t, w);
+    double ra = 0.0, ia = 0.0;
+    for (int j = 0; j < 4; ++j) {
+      long cell = std::min(std::max(i0 - 1 + j, 0L), (long)G.m - 1);
+      ia += G.out[cell].real() * w[j];
+      ra += G.out[cell].imag() * w[j];
+    }
+    re[k] = ra * inv_m;
+    im[k] = ia * inv_m;
+  }
+}
+
+// nufft.rs:164-220 (raw sums; `sorted_ev` follows the reference's contract
+// that the first/last entries bound the spectrum).
+void nufft_points(const double* q, size_t nq, const double* ev, size_t p, double eta,
+                  bool parallel, double* re, double* im) {
+  if (p == 0 || nq == 0) return;
+  Grid G;
+  convolution(ev, p, eta, parallel, G);
+  interpolate(G, q, nq, parallel, re, im);
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+size_t orc_nufft_grid_size(double raw_range, double eta) { return nufft_grid_size(raw_range, eta); }
+
+void orc_nufft_points(const double* q, size_t nq, const double* ev, size_t p, double eta,
+                      int parallel, double* re, double* im) {
+  nufft_points(q, nq, ev, p, eta, parallel != 0, re, im);
+}
+
+// Grid-level export for kernel-by-kernel parity: density after the splat
+// (m doubles) and the packed grid after the inverse FFT (2m doubles,
+// interleaved re/im, before the 1/m scaling).  Returns m.
+size_t orc_nufft_grid(const double* ev, size_t p, double eta, double* density_out,
+                      double* packed_out, double* lo_out, double* dx_out) {
+  Grid G;
+  convolution(ev, p, eta, false, G);
+  if (density_out) {
+    std::fill(density_out, density_out + G.m, 0.0);
+    for (size_t k = 0; k < p; ++k) splat4(density_out, G.m, (ev[k] - G.lo) / G.dx);
+  }
+  if (packed_out)
+    for (size_t k = 0; k < G.m; ++k) {
+      packed_out[2 * k] = G.out[k].real();
+      packed_out[2 * k + 1] = G.out[k].imag();
+    }
+  if (lo_out) *lo_out = G.lo;
+  if (dx_out) *dx_out = G.dx;
+  return G.m;
+}
+
+void orc_fft(double* interleaved, size_t m, int sign) {
+  fft_radix2(reinterpret_cast<std::complex<double>*>(interleaved), m, sign);
+}
+
+void orc_lagrange4(double t, double* w) { lagrange_weights<4>(t, w); }
+
+}  // extern "C"

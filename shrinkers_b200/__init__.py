@@ -1,0 +1,432 @@
+"""shrinkers_b200 -- the shrinkers Stieltjes-transform hot path on NVIDIA B200.
+
+A drop-in for the Python face of the ``shrinkers`` crate (its PyO3 module,
+src/python.rs:1048-1071) restricted to the functions that run the empirical
+Stieltjes transform and the estimators that consume it:
+
+    stieltjes_transform, stieltjes_transform_with_deriv, deconvolve_spiked,
+    estimate_population_eigenvalues, ledoit_wolf_shrinkage,
+    shrink_eigenvalues, detect_spikes_bema, inverse_bbp
+
+Same names, keyword arguments, defaults, return dictionaries and error
+messages as the reference; the transforms run in hand-written sm_100a CUDA
+kernels behind the C ABI of ``include/shrinkers_b200.h``.  Additions with no
+reference counterpart: ``precision="mixed"`` (FP32 far field + FP64 near
+field), :func:`stieltjes_transform_batched`, :func:`stieltjes_adjoint`, and
+the PyTorch autograd binding in :mod:`shrinkers_b200.autograd`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import numbers
+
+import numpy as np
+
+from . import _native
+
+__version__ = "0.1.0"
+
+__all__ = [
+    "stieltjes_transform", "stieltjes_transform_with_deriv", "deconvolve_spiked",
+    "estimate_population_eigenvalues", "ledoit_wolf_shrinkage", "shrink_eigenvalues",
+    "detect_spikes_bema", "inverse_bbp", "stieltjes_at_points", "stieltjes_transform_batched",
+    "stieltjes_adjoint", "parse_method", "method_name",
+]
+
+_D = C.POINTER(C.c_double)
+_PREC = {"f64": 0, "mixed": 1}
+_PAR_SEQ, _PAR_PAR, _PAR_AUTO = 0, 1, 2
+
+
+def _lib():
+    return _native.load()
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+# ------------------------------------------------------------ parsing --
+class _Inferred:
+    pass
+
+
+INFERRED = "inferred"
+
+
+def _inferred_f64(value, what: str):
+    """InferredF64 extraction (python.rs:97-134): float, None or "inferred"."""
+    if isinstance(value, str):
+        if value == "inferred":
+            return None
+        raise ValueError("expected a float, None, or the string 'inferred'")
+    if value is None:
+        return None
+    try:
+        return float(value)
+    except (TypeError, ValueError):
+        raise ValueError("expected a float, None, or the string 'inferred'") from None
+
+
+def _require_positive_finite(v: float, what: str) -> float:
+    """python.rs:146-153."""
+    if not (math.isfinite(v) and v > 0.0):
+        raise ValueError(f"{what} must be a positive finite number, got {_fmt(v)}")
+    return v
+
+
+def _fmt(v: float) -> str:
+    if math.isnan(v):
+        return "NaN"
+    if math.isinf(v):
+        return "inf" if v > 0 else "-inf"
+    return repr(float(v))
+
+
+def _owned_f64_vec(array, what: str = "eigenvalues") -> np.ndarray:
+    """python.rs:186-191: a 1-D float64 ndarray, contiguous, copied."""
+    if not isinstance(array, np.ndarray) or array.ndim != 1 or array.dtype != np.float64:
+        raise TypeError(
+            f"argument '{what}': expected a 1-D numpy.ndarray of float64, got "
+            f"{type(array).__name__}"
+            + (f" of dtype {array.dtype} and ndim {array.ndim}" if isinstance(array, np.ndarray) else ""))
+    if not array.flags["C_CONTIGUOUS"]:
+        raise ValueError(f"{what} must be contiguous")
+    return np.array(array, dtype=np.float64, copy=True)
+
+
+def _require_finite(ev: np.ndarray, what: str) -> None:
+    """python.rs:135-144."""
+    if not np.all(np.isfinite(ev)):
+        raise ValueError(f"{what} must be finite (found NaN or infinity)")
+
+
+def _sanitize_positive(ev: np.ndarray, what: str = "eigenvalues") -> None:
+    """python.rs:292-308: clamp round-off dust, reject meaningful negatives."""
+    _require_finite(ev, what)
+    scale = max(1.0, float(np.max(np.abs(ev)))) if ev.size else 1.0
+    tol = 1e-10 * scale
+    neg = np.nonzero(ev < 0.0)[0]
+    for i in neg:
+        v = float(ev[i])
+        if v < -tol:
+            raise ValueError(
+                f"{what} must be non-negative (found {v}, tolerance {tol:.3e}); "
+                "covariance eigenvalues cannot be significantly negative")
+        ev[i] = 0.0
+
+
+def _require_concentration(c) -> float:
+    """python.rs:311-318."""
+    c = float(c)
+    if not math.isfinite(c) or c <= 0.0 or c > 1.0:
+        raise ValueError(f"c (concentration ratio p/n) must satisfy 0 < c <= 1, got {_fmt(c)}")
+    return c
+
+
+def _owned_positive_spectrum(array, c) -> tuple[np.ndarray, float]:
+    """python.rs:194-199."""
+    ev = _owned_f64_vec(array, "eigenvalues")
+    _sanitize_positive(ev, "eigenvalues")
+    return ev, _require_concentration(c)
+
+
+def _parse_parallel(parallel) -> int:
+    """python.rs:367-373 (Option<bool>; anything else is a TypeError)."""
+    if parallel is None:
+        return _PAR_AUTO
+    if isinstance(parallel, (bool, np.bool_)):
+        return _PAR_PAR if bool(parallel) else _PAR_SEQ
+    raise TypeError(f"argument 'parallel': '{type(parallel).__name__}' object cannot be "
+                    "converted to 'PyBool'")
+
+
+def parse_method(method: str) -> int:
+    """python.rs:321-350 parse_method: every alias of the reference."""
+    if not isinstance(method, str):
+        raise TypeError(f"argument 'method': '{type(method).__name__}' object cannot be "
+                        "converted to 'PyString'")
+    out = C.c_int()
+    st = _lib().shrk_parse_method(method.encode(), C.byref(out))
+    if st != _native.SHRK_OK:
+        raise ValueError(f"unknown method '{method}'")
+    return out.value
+
+
+def method_name(method_id: int) -> str:
+    return _lib().shrk_method_name(int(method_id)).decode()
+
+
+def _usize(v, what: str) -> int:
+    if isinstance(v, (bool, np.bool_)) or not isinstance(v, numbers.Integral):
+        raise TypeError(f"argument '{what}': '{type(v).__name__}' object cannot be "
+                        "interpreted as an integer")
+    v = int(v)
+    if v < 0:
+        raise OverflowError(f"argument '{what}': can't convert negative int to unsigned")
+    return v
+
+
+def _cutoff(cutoff) -> float:
+    """python.rs:277-284: None/"inferred" disable it (NaN on the ABI)."""
+    v = _inferred_f64(cutoff, "cutoff")
+    if v is None:
+        return float("nan")
+    return _require_positive_finite(v, "cutoff ratio")
+
+
+# --------------------------------------------------------- transforms --
+def stieltjes_transform(eigenvalues, eta=INFERRED, method="blocked", precision="f64",
+                        cutoff=INFERRED, parallel=False):
+    """python.rs:783-837: S(lambda_i)/p for every eigenvalue.
+
+    Returns {"real", "imag"} (float64; float32 for precision="f32"), Im > 0.
+    ``precision="mixed"`` selects the B200 mixed-precision exact kernel.
+    """
+    ev = _owned_f64_vec(eigenvalues, "eigenvalues")
+    _require_finite(ev, "eigenvalues")
+    if ev.size == 0:
+        raise ValueError("eigenvalues must be non-empty")
+    p = ev.size
+    eta_v = _inferred_f64(eta, "eta")
+    eta_v = _require_positive_finite(0.1 / math.sqrt(p) if eta_v is None else eta_v, "eta")
+    m = parse_method(method)
+    par = _parse_parallel(parallel)
+    cut = _cutoff(cutoff)
+    L = _lib()
+    if precision in ("f64", "mixed"):
+        re, im = np.empty(p), np.empty(p)
+        st = L.shrk_stieltjes_all(_dp(ev), p, eta_v, m, _PREC[precision], cut, par, _dp(re), _dp(im))
+        _native.check(st, "stieltjes_transform")
+        return {"real": re, "imag": im}
+    if precision == "f32":
+        ev32 = ev.astype(np.float32)
+        re, im = np.empty(p, np.float32), np.empty(p, np.float32)
+        fp = C.POINTER(C.c_float)
+        st = L.shrk_stieltjes_all_f32(ev32.ctypes.data_as(fp), p, np.float32(eta_v), m, cut,
+                                      re.ctypes.data_as(fp), im.ctypes.data_as(fp))
+        _native.check(st, "stieltjes_transform(f32)")
+        return {"real": re, "imag": im}
+    raise ValueError(f"unknown precision '{precision}' (expected 'f64' or 'f32')")
+
+
+def stieltjes_transform_with_deriv(eigenvalues, eta=INFERRED):
+    """python.rs:758-781: raw value and analytic derivative at every eigenvalue."""
+    ev = _owned_f64_vec(eigenvalues, "eigenvalues")
+    _require_finite(ev, "eigenvalues")
+    if ev.size == 0:
+        raise ValueError("eigenvalues must be non-empty")
+    p = ev.size
+    eta_v = _inferred_f64(eta, "eta")
+    eta_v = _require_positive_finite(0.1 / math.sqrt(p) if eta_v is None else eta_v, "eta")
+    out = [np.empty(p) for _ in range(4)]
+    st = _lib().shrk_stieltjes_with_deriv(_dp(ev), p, eta_v, *[_dp(o) for o in out])
+    _native.check(st, "stieltjes_transform_with_deriv")
+    return dict(zip(["real", "imag", "deriv_real", "deriv_imag"], out))
+
+
+def stieltjes_at_points(query_points, eigenvalues, eta, method="blocked", precision="f64",
+                        cutoff=None, parallel=False):
+    """Raw sums at arbitrary query points (compute_stieltjes_at_points,
+    src/stieltjes/mod.rs:394-494; not exported by the reference's module)."""
+    q = np.ascontiguousarray(np.asarray(query_points, dtype=np.float64))
+    ev = np.ascontiguousarray(np.asarray(eigenvalues, dtype=np.float64))
+    re, im = np.empty(q.size), np.empty(q.size)
+    st = _lib().shrk_stieltjes_at_points(_dp(q), q.size, _dp(ev), ev.size, float(eta),
+                                         parse_method(method), _PREC[precision], _cutoff(cutoff),
+                                         _parse_parallel(parallel), _dp(re), _dp(im))
+    _native.check(st, "stieltjes_at_points")
+    return {"real": re, "imag": im}
+
+
+def stieltjes_transform_batched(spectra, eta=None, precision="mixed"):
+    """Many spectra of uneven length in one persistent launch.
+
+    ``spectra``: a sequence of 1-D float64 arrays, or a tuple
+    ``(values, offsets)`` with spectrum s = values[offsets[s]:offsets[s+1]].
+    ``eta``: None (1/sqrt(p_s) per spectrum), a float, or one value per
+    spectrum.  Returns a list of {"real", "imag"} dicts scaled by 1/p_s.
+    """
+    if isinstance(spectra, tuple) and len(spectra) == 2 and np.ndim(spectra[1]) == 1 \
+            and np.asarray(spectra[1]).dtype.kind in "iu":
+        vals = np.ascontiguousarray(np.asarray(spectra[0], dtype=np.float64))
+        offs = np.ascontiguousarray(np.asarray(spectra[1], dtype=np.int64))
+    else:
+        arrs = [np.asarray(s, dtype=np.float64).ravel() for s in spectra]
+        offs = np.zeros(len(arrs) + 1, np.int64)
+        offs[1:] = np.cumsum([a.size for a in arrs])
+        vals = np.ascontiguousarray(np.concatenate(arrs) if arrs else np.empty(0))
+    n = offs.size - 1
+    sizes = np.diff(offs)
+    if n <= 0:
+        return []
+    if np.any(sizes <= 0):
+        raise ValueError("eigenvalues must be non-empty")
+    _require_finite(vals, "eigenvalues")
+    if eta is None:
+        etas = 1.0 / np.sqrt(sizes.astype(np.float64))
+    else:
+        etas = np.broadcast_to(np.asarray(eta, dtype=np.float64), (n,)).copy()
+    for e in etas:
+        _require_positive_finite(float(e), "eta")
+    etas = np.ascontiguousarray(etas)
+    re, im = np.empty(vals.size), np.empty(vals.size)
+    st = _lib().shrk_stieltjes_batched(_dp(vals), offs.ctypes.data_as(C.POINTER(C.c_int64)), n,
+                                       _dp(etas), _PREC[precision], _dp(re), _dp(im))
+    _native.check(st, "stieltjes_transform_batched")
+    return [{"real": re[offs[s]:offs[s + 1]], "imag": im[offs[s]:offs[s + 1]]} for s in range(n)]
+
+
+def stieltjes_adjoint(eigenvalues, g_real, g_imag, eta=None, precision="f64"):
+    """dL/d lambda for L = sum_j Re(conj(g_j) m_j), m_j = (1/p) sum_i 1/(lambda_i - z_j),
+    z_j = lambda_j + i eta (eta default 1/sqrt(p)).  Includes the dependence
+    of z_j on lambda_j."""
+    ev = np.ascontiguousarray(np.asarray(eigenvalues, dtype=np.float64))
+    gr = np.ascontiguousarray(np.asarray(g_real, dtype=np.float64))
+    gi = np.ascontiguousarray(np.asarray(g_imag, dtype=np.float64))
+    if ev.size == 0:
+        raise ValueError("eigenvalues must be non-empty")
+    if gr.shape != ev.shape or gi.shape != ev.shape:
+        raise ValueError("cotangents must have the shape of eigenvalues")
+    _require_finite(ev, "eigenvalues")
+    eta_v = 1.0 / math.sqrt(ev.size) if eta is None else _require_positive_finite(float(eta), "eta")
+    grad = np.empty(ev.size)
+    st = _lib().shrk_stieltjes_adjoint(_dp(ev), ev.size, eta_v, _dp(gr), _dp(gi), _PREC[precision],
+                                       _dp(grad))
+    _native.check(st, "stieltjes_adjoint")
+    return grad
+
+
+# ---------------------------------------------------------- estimators --
+_BULK_KEYS = ["lambda_grid", "density", "w_re", "sample_stieltjes_real",
+              "sample_stieltjes_imag", "population_stieltjes_real",
+              "population_stieltjes_imag"]
+
+
+def deconvolve_spiked(eigenvalues, c, n_points=200, eta=INFERRED, margin=1.0, *, method="auto",
+                      parallel=False, cutoff=INFERRED, precision="f64"):
+    """python.rs:428-475 deconvolve_spiked (BEMA + inverse BBP + El Karoui)."""
+    ev, c = _owned_positive_spectrum(eigenvalues, c)
+    n_points = _usize(n_points, "n_points")
+    if n_points == 0:
+        raise ValueError("n_points must be >= 1")
+    margin = _require_positive_finite(float(margin), "margin")
+    eta_v = _inferred_f64(eta, "eta")
+    eta_arg = float("nan") if eta_v is None else _require_positive_finite(eta_v, "eta")
+    m = parse_method(method)
+    par = _parse_parallel(parallel)
+    cut = _cutoff(cutoff)
+    p = ev.size
+    k = C.c_size_t()
+    sp, ss = np.empty(max(p, 1)), np.empty(max(p, 1))
+    edge, s2 = C.c_double(), C.c_double()
+    out = np.zeros(7 * n_points)
+    st = _lib().shrk_deconvolve_spiked(_dp(ev), p, c, n_points, eta_arg, margin, m,
+                                       _PREC[precision], par, cut, C.byref(k), _dp(sp), _dp(ss),
+                                       C.byref(edge), C.byref(s2), _dp(out))
+    _native.check(st, "deconvolve_spiked")
+    kk = int(k.value)
+    o = out.reshape(7, n_points)
+    if p - kk == 0:
+        o = np.zeros((7, 0))
+    return {
+        "k": kk,
+        "spikes": sp[:kk].copy(),
+        "spike_sample": ss[:kk].copy(),
+        "bulk_edge": float(edge.value),
+        "sigma2": float(s2.value),
+        "bulk": {key: o[i].copy() for i, key in enumerate(_BULK_KEYS)},
+    }
+
+
+def estimate_population_eigenvalues(eigenvalues, c, margin=1.0, *, precision="f64"):
+    """python.rs:974-1000 estimate_population_eigenvalues."""
+    ev, c = _owned_positive_spectrum(eigenvalues, c)
+    margin = _require_positive_finite(float(margin), "margin")
+    p = ev.size
+    k = C.c_size_t()
+    sp, ss = np.empty(max(p, 1)), np.empty(max(p, 1))
+    bp, bs = np.empty(max(p, 1)), np.empty(max(p, 1))
+    edge, s2 = C.c_double(), C.c_double()
+    st = _lib().shrk_estimate_population_eigenvalues(_dp(ev), p, c, margin, _PREC[precision],
+                                                     C.byref(k), _dp(sp), _dp(ss), C.byref(edge),
+                                                     C.byref(s2), _dp(bp), _dp(bs))
+    _native.check(st, "estimate_population_eigenvalues")
+    kk = int(k.value)
+    return {
+        "k": kk,
+        "spikes": sp[:kk].copy(),
+        "spike_sample": ss[:kk].copy(),
+        "bulk_edge": float(edge.value),
+        "sigma2": float(s2.value),
+        "bulk_population": bp[:p - kk].copy(),
+        "bulk_sample": bs[:p - kk].copy(),
+    }
+
+
+def ledoit_wolf_shrinkage(eigenvalues, c, *, precision="f64"):
+    """python.rs:1007-1019: raw Ledoit-Wolf xi (RmtConfig::new: Blocked, sequential)."""
+    ev, c = _owned_positive_spectrum(eigenvalues, c)
+    out = np.empty(ev.size)
+    if ev.size == 0:
+        return out
+    st = _lib().shrk_ledoit_wolf_shrinkage(_dp(ev), ev.size, c, 2, _PREC[precision], _PAR_SEQ,
+                                           float("nan"), _dp(out))
+    _native.check(st, "ledoit_wolf_shrinkage")
+    return out
+
+
+def shrink_eigenvalues(eigenvalues, c, *, method="auto", parallel=False, precision="f64"):
+    """python.rs:1021-1042: trace-preserving RIE shrinkage."""
+    ev = _owned_f64_vec(eigenvalues, "eigenvalues")
+    _require_finite(ev, "eigenvalues")
+    c = _require_concentration(c)
+    m = parse_method(method)
+    par = _parse_parallel(parallel)
+    out = np.empty(ev.size)
+    if ev.size == 0:
+        return out
+    st = _lib().shrk_rie_shrinkage(_dp(ev), ev.size, c, m, _PREC[precision], par, _dp(out))
+    _native.check(st, "shrink_eigenvalues")
+    return out
+
+
+def detect_spikes_bema(eigenvalues, c, margin=1.0):
+    """python.rs:856-874 detect_spikes_bema (host arithmetic, bit-exact)."""
+    ev, c = _owned_positive_spectrum(eigenvalues, c)
+    ev = np.sort(ev, kind="stable")
+    margin = _require_positive_finite(float(margin), "margin")
+    k = C.c_size_t()
+    idx = np.empty(max(ev.size, 1), np.int64)
+    edge, s2 = C.c_double(), C.c_double()
+    st = _lib().shrk_detect_spikes_bema(_dp(ev), ev.size, c, margin, C.byref(k),
+                                        idx.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(edge),
+                                        C.byref(s2))
+    _native.check(st, "detect_spikes_bema")
+    kk = int(k.value)
+    return {"k": kk, "spike_indices": idx[:kk].copy(), "bulk_edge": float(edge.value),
+            "sigma2": float(s2.value)}
+
+
+def _checked_lambda_hat(x: float) -> float:
+    """python.rs:155-169."""
+    if not math.isfinite(x):
+        raise ValueError("lambda_hat must be finite (found NaN or infinity)")
+    if x <= 0.0:
+        raise ValueError("lambda_hat must be positive (sample spikes cannot be ≤ 0)")
+    return x
+
+
+def inverse_bbp(lambda_hat, c, sigma2=1.0):
+    """python.rs:931-942: scalar -> float, 1-D array -> ndarray."""
+    c = _require_concentration(c)
+    sigma2 = _require_positive_finite(float(sigma2), "sigma2")
+    L = _lib()
+    if isinstance(lambda_hat, (numbers.Real, np.floating)) and not isinstance(lambda_hat, bool):
+        return float(L.shrk_inverse_bbp(_checked_lambda_hat(float(lambda_hat)), c, sigma2))
+    try:
+        arr = [float(x) for x in np.asarray(lambda_hat, dtype=np.float64).ravel()]
+    except (TypeError, ValueError):
+        raise ValueError("expected a float or a 1-D array of floats") from None
+    return np.array([L.shrk_inverse_bbp(_checked_lambda_hat(x), c, sigma2) for x in arr])

@@ -1,0 +1,54 @@
+"""Build recipe of libshrinkers_b200.so (nvcc, sm_100a, in-tree)."""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libshrinkers_b200.so")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    # The epilogues restate the reference's operation order; every FMA in the
+    # kernels is written explicitly.
+    "--fmad=false",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+    "-shared", "-cudart", "static",
+]
+
+
+def sources() -> list[str]:
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+    deps.append(os.path.join(HERE, "..", "include", "shrinkers_b200.h"))
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
+    if not force and not needs_build():
+        return LIB
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    cmd = [nvcc, *NVCC_FLAGS, *(extra or []), "-o", LIB + ".tmp", *sources()]
+    # nvcc must use the system host compiler (the image's CXX lacks OpenMP/libs).
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    env.pop("CC", None)
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True, env=env)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    import sys
+    build(force=True, verbose=True, extra=sys.argv[1:])

@@ -1,0 +1,885 @@
+// C ABI of libshrinkers_b200 (include/shrinkers_b200.h): argument checks,
+// method policy, per-device state, host<->device staging, and the host-side
+// pieces of the estimators (sort, BEMA, inverse BBP) that the reference also
+// runs on the host.  All heavy arithmetic runs in the kernels of exact.cu,
+// nufft.cu, chebcode.cu and batched.cu; there is no CPU fallback.
+#include "common.cuh"
+#include "internal.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace shrk {
+
+// ------------------------------------------------------------ errors --
+static thread_local std::string t_last_error;
+
+void set_error(const std::string& msg) { t_last_error = msg; }
+
+shrk_status cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) return SHRK_ENOMEM;
+  return SHRK_ECUDA;
+}
+
+static shrk_status einval(const std::string& msg) {
+  set_error(msg);
+  return SHRK_EINVAL;
+}
+
+// ------------------------------------------------------ device state --
+struct DeviceState {
+  bool init = false;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  Scratch slots[16];
+  int* err = nullptr;
+};
+
+static std::mutex g_mu;  // serialises library calls (state + scratch reuse)
+static std::map<int, DeviceState> g_dev;
+
+static shrk_status current_state(DeviceState** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  DeviceState& st = g_dev[dev];
+  if (!st.init) {
+    SHRK_CUDA(cudaDeviceGetAttribute(&st.sms, cudaDevAttrMultiProcessorCount, dev));
+    SHRK_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
+    SHRK_CUDA(cudaMalloc(&st.err, sizeof(int)));
+    SHRK_CUDA(cudaMemset(st.err, 0, sizeof(int)));
+    st.init = true;
+  }
+  *out = &st;
+  return SHRK_OK;
+}
+
+static DeviceState* g_cur = nullptr;  // valid while g_mu is held
+
+shrk_status scratch_get(int slot, size_t bytes, void** out) {
+  Scratch& s = g_cur->slots[slot];
+  if (s.bytes < bytes) {
+    if (s.ptr) {
+      cudaError_t e = cudaFree(s.ptr);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaFree(scratch)");
+    }
+    s.ptr = nullptr;
+    s.bytes = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&s.ptr, want);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(scratch)");
+    s.bytes = want;
+  }
+  *out = s.ptr;
+  return SHRK_OK;
+}
+
+int* device_error_word() { return g_cur->err; }
+int sm_count() { return g_cur ? g_cur->sms : 148; }
+cudaStream_t library_stream() { return g_cur->stream; }
+
+shrk_status check_device_error(cudaStream_t s) {
+  int h = 0;
+  SHRK_CUDA(cudaMemcpyAsync(&h, g_cur->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  if (h != DEV_ERR_NONE) {
+    SHRK_CUDA(cudaMemsetAsync(g_cur->err, 0, sizeof(int), s));
+    SHRK_CUDA(cudaStreamSynchronize(s));
+    if (h == DEV_ERR_TIMEOUT) {
+      set_error("a bounded device-side wait gave up (timeout)");
+      return SHRK_ETIMEOUT;
+    }
+    set_error("a device-side self-check failed (code " + std::to_string(h) + ")");
+    return SHRK_ECUDA;
+  }
+  return SHRK_OK;
+}
+
+// ------------------------------------------------------------ timing --
+static std::atomic<int64_t> g_launches{0};
+static bool g_timing = false;
+struct TimedLaunch { std::string family; cudaEvent_t a, b; };
+static std::vector<TimedLaunch> g_timed;
+
+LaunchScope::LaunchScope(const char* fam, cudaStream_t s) : family(fam), stream(s) {
+  g_launches.fetch_add(1);
+  if (g_timing) {
+    cudaEventCreate(&start);
+    cudaEventCreate(&stop);
+    cudaEventRecord(start, s);
+  }
+}
+LaunchScope::~LaunchScope() {
+  if (start) {
+    cudaEventRecord(stop, stream);
+    g_timed.push_back({family, start, stop});
+  }
+}
+
+// ----------------------------------------------------------- helpers --
+static bool is_auto(int m) {
+  return m == SHRK_M_AUTO || m == SHRK_M_SPEED_AUTO || m == SHRK_M_ACCURACY_AUTO;
+}
+static bool is_exact_family(int m) {
+  return m == SHRK_M_NAIVE || m == SHRK_M_AUTOVEC || m == SHRK_M_BLOCKED ||
+         m == SHRK_M_BLOCKED_AUTOVEC || m == SHRK_M_BLOCKED_TILED ||
+         m == SHRK_M_BLOCKED_WINDOWED || m == SHRK_M_BLOCKED_HYBRID;
+}
+static bool is_cheb(int m) {
+  return m == SHRK_M_CHEBCODE || m == SHRK_M_CHEBCODE_FAST || m == SHRK_M_CHEBCODE_XTREME ||
+         m == SHRK_M_CHEBCODE_BALANCED;
+}
+
+static shrk_status check_common(size_t p, double eta, int method, int precision) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (!(std::isfinite(eta) && eta > 0.0)) return einval("eta must be a positive finite number");
+  if (method < 0 || method > SHRK_M_ACCURACY_AUTO) return einval("unknown method id");
+  if (precision != SHRK_PREC_F64 && precision != SHRK_PREC_MIXED)
+    return einval("unknown precision id");
+  return SHRK_OK;
+}
+
+static shrk_status check_cutoff(double cutoff) {
+  if (std::isnan(cutoff)) return SHRK_OK;
+  if (!(std::isfinite(cutoff) && cutoff > 0.0))
+    return einval("cutoff ratio must be a positive finite number");
+  return SHRK_OK;
+}
+
+static shrk_status not_impl(int m) {
+  set_error(std::string("method '") + shrk_method_name(m) +
+            "' has no GPU implementation in shrinkers_b200 (no CPU fallback)");
+  return SHRK_ENOTIMPL;
+}
+
+static shrk_status h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  SHRK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+  return SHRK_OK;
+}
+static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  SHRK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+  return SHRK_OK;
+}
+
+// Scratch slot map: 0 split partials, 1 block bounds, 2 adjoint partials,
+// 3 input spectrum, 4/5 outputs, 6 query points, 7 raw sums (2 arrays),
+// 8 sorted copy / tree, 9.. method-private.
+
+// Raw (or scaled) sums of `method` at targets d_tgt against d_src, written
+// through `epi`.  `h_src` (may be null) is a host copy of the sources, used
+// by the treecode build.  The method must already be resolved.
+static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* d_src,
+                                 const double* h_src, int64_t ns, double eta, int method,
+                                 int precision, double cutoff, const Epilogue& epi,
+                                 cudaStream_t s) {
+  const bool cut = !std::isnan(cutoff);
+  if (is_exact_family(method)) {
+    const bool windowed_re = cut && (method == SHRK_M_BLOCKED || method == SHRK_M_BLOCKED_TILED ||
+                                     method == SHRK_M_BLOCKED_WINDOWED ||
+                                     method == SHRK_M_BLOCKED_AUTOVEC);
+    const bool windowed_im = windowed_re || (cut && method == SHRK_M_BLOCKED_HYBRID);
+    if (!windowed_re && !windowed_im)
+      return exact_pair_sums(d_tgt, nt, d_src, ns, eta, precision, epi, s);
+    void* raw = nullptr;
+    SHRK_TRY(scratch_get(7, sizeof(double) * 2 * nt, &raw));
+    double* rre = (double*)raw;
+    double* rim = rre + nt;
+    if (windowed_re) {
+      SHRK_TRY(windowed_sums(d_tgt, nt, d_src, ns, eta, cutoff * eta, 1.0, rre, rim, s));
+    } else {  // hybrid: exact real part, windowed imaginary part
+      void* tmp = nullptr;
+      SHRK_TRY(scratch_get(9, sizeof(double) * nt, &tmp));
+      Epilogue e1;
+      e1.mode = EPI_SUMS;
+      e1.scale = 1.0;
+      e1.out_re = rre;
+      e1.out_im = (double*)tmp;
+      SHRK_TRY(exact_pair_sums(d_tgt, nt, d_src, ns, eta, precision, e1, s));
+      void* tmp2 = nullptr;
+      SHRK_TRY(scratch_get(10, sizeof(double) * nt, &tmp2));
+      SHRK_TRY(windowed_sums(d_tgt, nt, d_src, ns, eta, cutoff * eta, 1.0, (double*)tmp2, rim, s));
+    }
+    return apply_epilogue(d_tgt, rre, rim, nt, epi, s);
+  }
+  if (method == SHRK_M_NUFFT || is_cheb(method)) {
+    void* raw = nullptr;
+    SHRK_TRY(scratch_get(7, sizeof(double) * 2 * nt, &raw));
+    double* rre = (double*)raw;
+    double* rim = rre + nt;
+    if (method == SHRK_M_NUFFT) {
+      double lo = 0.0, hi = 0.0;
+      if (h_src) {
+        lo = h_src[0];
+        hi = h_src[ns - 1];
+      } else {
+        SHRK_TRY(d2h(&lo, d_src, sizeof(double), s));
+        SHRK_TRY(d2h(&hi, d_src + ns - 1, sizeof(double), s));
+        SHRK_CUDA(cudaStreamSynchronize(s));
+      }
+      SHRK_TRY(nufft_points(d_tgt, nt, d_src, ns, lo, hi, eta, rre, rim, s));
+    } else {
+      ChebParams prm;
+      cheb_preset(method, &prm);
+      if (epi.mode == EPI_MP)  // grid path: mod.rs:475-489 relaxes the leaf cap
+        prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nt, prm.leaf_cap);
+      std::vector<double> host;
+      if (!h_src) {
+        host.resize(ns);
+        SHRK_TRY(d2h(host.data(), d_src, sizeof(double) * ns, s));
+        SHRK_CUDA(cudaStreamSynchronize(s));
+        h_src = host.data();
+      }
+      // The tree is built over the ascending copy (chebcode.rs:1088-1097).
+      std::vector<double> sorted;
+      const double* hs = h_src;
+      const double* ds = d_src;
+      bool sorted_in = true;
+      for (int64_t i = 1; i < ns; ++i)
+        if (!(h_src[i - 1] <= h_src[i])) { sorted_in = false; break; }
+      if (!sorted_in) {
+        sorted.assign(h_src, h_src + ns);
+        std::sort(sorted.begin(), sorted.end());
+        void* dsb = nullptr;
+        SHRK_TRY(scratch_get(8, sizeof(double) * ns, &dsb));
+        SHRK_TRY(h2d(dsb, sorted.data(), sizeof(double) * ns, s));
+        hs = sorted.data();
+        ds = (const double*)dsb;
+      }
+      SHRK_TRY(chebcode_points(d_tgt, nt, hs, ds, ns, eta, prm, rre, rim, s));
+      SHRK_CUDA(cudaStreamSynchronize(s));  // `sorted` / `host` are read by the build
+    }
+    return apply_epilogue(d_tgt, rre, rim, nt, epi, s);
+  }
+  return not_impl(method);
+}
+
+static int resolve(int method, int parallelism, size_t p) {
+  return shrk_resolve_auto_method(method, parallelism == SHRK_PAR_PARALLEL ? 1 : 0, p);
+}
+
+// ------------------------------------------------ host estimators -- //
+// detection.rs:75-83
+static double mp_median_factor(double gamma) {
+  double g = std::min(std::max(gamma, 0.0), 1.0);
+  return 0.999995823 - 0.333211332 * g - 0.0106766617 * g * g - 0.000758816762 * g * g * g -
+         0.00256753402 * g * g * g * g;
+}
+// estimation.rs:37-39
+static double bbp_threshold(double gamma, double sigma2) {
+  double s = 1.0 + std::sqrt(gamma);
+  return sigma2 * (s * s);
+}
+// estimation.rs:48-56
+static double inverse_bbp(double lh, double gamma, double sigma2) {
+  double x = lh / sigma2;
+  double a = x + 1.0 - gamma;
+  double disc = a * a - 4.0 * x;
+  if (disc <= 0.0) return bbp_threshold(gamma, sigma2);
+  double ell = ((x + 1.0 - gamma) + std::sqrt(disc)) / 2.0;
+  return ell * sigma2;
+}
+
+struct SpikeSplit {
+  size_t k = 0;
+  double edge = 0.0, sigma2 = 0.0;
+  std::vector<size_t> idx;
+  std::vector<double> sorted, spikes, spike_sample, bulk;
+};
+
+// detection.rs:134-153 (median 111-121, scan_above 49-63) on a sorted copy.
+static void bema(const double* sorted, size_t p, double gamma, double margin, SpikeSplit& out) {
+  out.idx.clear();
+  if (p == 0) return;
+  double med = (p % 2 == 0) ? (sorted[p / 2 - 1] + sorted[p / 2]) / 2.0 : sorted[p / 2];
+  double sigma2 = med / mp_median_factor(gamma);
+  double edge = bbp_threshold(gamma, sigma2);
+  double thr = edge * std::max(margin, 1.0);
+  for (size_t i = p; i-- > 0;) {
+    if (sorted[i] > thr) out.idx.push_back(i);
+    else break;
+  }
+  std::reverse(out.idx.begin(), out.idx.end());
+  out.k = out.idx.size();
+  out.edge = edge;
+  out.sigma2 = sigma2;
+}
+
+// spiked/mod.rs:54-91 detect_debias_split (spikes returned descending).
+static void detect_debias_split(const double* ev, size_t p, double gamma, double margin,
+                                SpikeSplit& s) {
+  s.sorted.assign(ev, ev + p);
+  std::stable_sort(s.sorted.begin(), s.sorted.end());
+  bema(s.sorted.data(), p, gamma, margin, s);
+  s.spikes.clear();
+  s.spike_sample.clear();
+  for (size_t i : s.idx) {
+    s.spike_sample.push_back(s.sorted[i]);
+    s.spikes.push_back(inverse_bbp(s.sorted[i], gamma, s.sigma2));
+  }
+  std::reverse(s.spikes.begin(), s.spikes.end());
+  std::reverse(s.spike_sample.begin(), s.spike_sample.end());
+  s.bulk.clear();
+  size_t q = 0;
+  for (size_t i = 0; i < p; ++i) {
+    if (q < s.idx.size() && s.idx[q] == i) { ++q; continue; }
+    s.bulk.push_back(s.sorted[i]);
+  }
+}
+
+// Ledoit-Wolf xi on the device for host ev (estimation.rs:75-90).
+static shrk_status lw_device(const double* ev, size_t p, double c, int method, int precision,
+                             int parallelism, double eta, double* xi) {
+  DeviceState* st = g_cur;
+  cudaStream_t s = st->stream;
+  int m = resolve(method, parallelism, p);
+  if (std::isnan(eta)) eta = 0.4 / std::sqrt((double)p);  // mod.rs:150-153
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * p, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  Epilogue epi;
+  epi.mode = EPI_LW;
+  epi.scale = 1.0 / (double)p;
+  epi.c = c;
+  epi.out_re = (double*)out;
+  SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, ev, (int64_t)p, eta,
+                         m, precision, NAN, epi, s));
+  SHRK_TRY(d2h(xi, out, sizeof(double) * p, s));
+  return check_device_error(s);
+}
+
+// deconvolution/mod.rs:116-259 with the inversion fused into the epilogue.
+static shrk_status deconv_device(const double* ev, size_t p, double c, size_t n_points, double eta,
+                                 double lmin, double lmax, int method, int precision,
+                                 int parallelism, double cutoff, double* out7) {
+  if (p == 0) return SHRK_OK;
+  cudaStream_t s = g_cur->stream;
+  double eta_val = std::isnan(eta) ? 0.1 / std::sqrt((double)p) : eta;
+  double mn = INFINITY, mx = -INFINITY;
+  for (size_t i = 0; i < p; ++i) {
+    mn = std::min(mn, ev[i]);
+    mx = std::max(mx, ev[i]);
+  }
+  double range = (mx - mn) > 0.0 ? mx - mn : 1.0;
+  double margin = 0.2 * range;
+  double lo = std::isnan(lmin) ? std::max(mn - margin, 0.0) : lmin;
+  double hi = std::isnan(lmax) ? mx + margin : lmax;
+  double step = n_points > 1 ? (hi - lo) / ((double)n_points - 1.0) : 0.0;
+  double* grid = out7;
+  for (size_t k = 0; k < n_points; ++k) grid[k] = lo + step * (double)k;
+  // config.rs:507-516 resolve_auto_at_points (parallelism Auto -> Sequential)
+  const bool par = parallelism == SHRK_PAR_PARALLEL;
+  int m = method;
+  if (is_auto(m)) m = shrk_grid_appropriate(shrk_resolve_auto_method(m, par, p), p, n_points);
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* dq = nullptr;
+  SHRK_TRY(scratch_get(6, sizeof(double) * n_points, &dq));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 6 * n_points, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  SHRK_TRY(h2d(dq, grid, sizeof(double) * n_points, s));
+  Epilogue epi;
+  epi.mode = EPI_MP;
+  epi.scale = 1.0 / (double)p;
+  epi.c = c;
+  epi.eta = eta_val;
+  for (int i = 0; i < 6; ++i) epi.out[i] = (double*)out + i * n_points;
+  SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)n_points, (const double*)dev, ev, (int64_t)p,
+                         eta_val, m, precision, cutoff, epi, s));
+  SHRK_TRY(d2h(out7 + n_points, out, sizeof(double) * 6 * n_points, s));
+  return check_device_error(s);
+}
+
+struct Guard {
+  std::lock_guard<std::mutex> lk;
+  shrk_status st;
+  Guard() : lk(g_mu) { st = current_state(&g_cur); }
+};
+
+}  // namespace shrk
+
+using namespace shrk;
+
+// ===================================================================== ABI
+
+extern "C" {
+
+size_t shrk_last_error(char* buf, size_t len) {
+  const std::string& e = t_last_error;
+  if (buf && len) {
+    size_t n = std::min(len - 1, e.size());
+    std::memcpy(buf, e.data(), n);
+    buf[n] = '\0';
+  }
+  return e.size();
+}
+
+const char* shrk_version(void) { return "0.1.0"; }
+
+int shrk_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+// config.rs:92-118
+const char* shrk_method_name(int m) {
+  static const char* names[] = {
+      "naive", "autovec", "blocked", "blocked_autovec", "blocked_tiled", "blocked_windowed",
+      "blocked_hybrid", "adaptive", "fft5", "fft3", "fft2", "nufft", "fmm", "chebcode",
+      "chebcode_fast", "chebcode_xtreme", "chebcode_balanced", "ewald", "dst", "auto", "hodlr",
+      "speed_auto", "accuracy_auto"};
+  if (m < 0 || m > SHRK_M_ACCURACY_AUTO) return "?";
+  return names[m];
+}
+
+// python.rs:321-350
+shrk_status shrk_parse_method(const char* name, int* out) {
+  static const struct { const char* n; int m; } tab[] = {
+      {"naive", SHRK_M_NAIVE}, {"autovec", SHRK_M_AUTOVEC}, {"blocked", SHRK_M_BLOCKED},
+      {"blocked_autovec", SHRK_M_BLOCKED_AUTOVEC}, {"blocked_tiled", SHRK_M_BLOCKED_TILED},
+      {"blocked_windowed", SHRK_M_BLOCKED_WINDOWED}, {"blocked_hybrid", SHRK_M_BLOCKED_HYBRID},
+      {"adaptive", SHRK_M_ADAPTIVE}, {"fft5", SHRK_M_FFT5}, {"fft3", SHRK_M_FFT3},
+      {"fft2", SHRK_M_FFT2}, {"nufft", SHRK_M_NUFFT}, {"fft_fast", SHRK_M_NUFFT},
+      {"fmm", SHRK_M_TREECODE}, {"treecode", SHRK_M_TREECODE}, {"chebcode", SHRK_M_CHEBCODE},
+      {"chebyshev", SHRK_M_CHEBCODE}, {"chebcode_fast", SHRK_M_CHEBCODE_FAST},
+      {"chebf", SHRK_M_CHEBCODE_FAST}, {"chebcode_xtreme", SHRK_M_CHEBCODE_XTREME},
+      {"chebx", SHRK_M_CHEBCODE_XTREME}, {"chebcode_balanced", SHRK_M_CHEBCODE_BALANCED},
+      {"chebb", SHRK_M_CHEBCODE_BALANCED}, {"ewald", SHRK_M_EWALD}, {"dst", SHRK_M_DST},
+      {"auto", SHRK_M_AUTO}, {"hodlr", SHRK_M_HODLR}, {"speed_auto", SHRK_M_SPEED_AUTO},
+      {"speed", SHRK_M_SPEED_AUTO}, {"accuracy_auto", SHRK_M_ACCURACY_AUTO},
+      {"accuracy", SHRK_M_ACCURACY_AUTO}};
+  if (!name || !out) return einval("null argument");
+  for (auto& e : tab)
+    if (std::strcmp(e.n, name) == 0) {
+      *out = e.m;
+      return SHRK_OK;
+    }
+  return einval(std::string("unknown method '") + name + "'");
+}
+
+// config.rs:543-555 + pareto_autogen.rs:22-86
+int shrk_resolve_auto_method(int m, int parallel, size_t p) {
+  struct Bin { size_t p_max; int ss, sp, as, ap; };
+  static const Bin bins[] = {
+      {1000, SHRK_M_CHEBCODE_FAST, SHRK_M_CHEBCODE_FAST, SHRK_M_BLOCKED_TILED, SHRK_M_BLOCKED},
+      {2000, SHRK_M_CHEBCODE_FAST, SHRK_M_CHEBCODE_FAST, SHRK_M_BLOCKED_TILED, SHRK_M_AUTOVEC},
+      {5000, SHRK_M_CHEBCODE_FAST, SHRK_M_CHEBCODE_FAST, SHRK_M_BLOCKED_TILED, SHRK_M_AUTOVEC},
+      {10000, SHRK_M_CHEBCODE_FAST, SHRK_M_CHEBCODE_FAST, SHRK_M_BLOCKED, SHRK_M_BLOCKED_TILED},
+      {20000, SHRK_M_CHEBCODE_FAST, SHRK_M_CHEBCODE_FAST, SHRK_M_BLOCKED, SHRK_M_BLOCKED},
+      {50000, SHRK_M_CHEBCODE_FAST, SHRK_M_CHEBCODE_FAST, SHRK_M_BLOCKED_TILED, SHRK_M_BLOCKED},
+      {SIZE_MAX, SHRK_M_NUFFT, SHRK_M_NUFFT, SHRK_M_BLOCKED_TILED, SHRK_M_BLOCKED},
+  };
+  if (!is_auto(m)) return m;
+  const Bin* b = &bins[6];
+  for (const Bin& x : bins)
+    if (p <= x.p_max) { b = &x; break; }
+  if (m != SHRK_M_ACCURACY_AUTO) return parallel ? b->sp : b->ss;
+  return parallel ? b->ap : b->as;
+}
+
+// config.rs:565-585
+int shrk_grid_appropriate(int m, size_t p, size_t nq) {
+  if (nq > SIZE_MAX / 4 || nq * 4 >= p) return m;
+  if (m == SHRK_M_NUFFT && p >= 300000) return m;
+  switch (m) {
+    case SHRK_M_FFT5: case SHRK_M_FFT3: case SHRK_M_FFT2: case SHRK_M_NUFFT:
+    case SHRK_M_ADAPTIVE: case SHRK_M_DST:
+      return SHRK_M_CHEBCODE_FAST;
+    default:
+      return m;
+  }
+}
+
+double shrk_mixed_near_k(void) { return mixed_near_k(); }
+
+shrk_status shrk_stieltjes_all_dev(const double* d_ev, size_t p, double eta, int method,
+                                   int precision, double cutoff, int parallelism, double* d_re,
+                                   double* d_im, void* stream) {
+  SHRK_TRY(check_common(p, eta, method, precision));
+  SHRK_TRY(check_cutoff(cutoff));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
+  int m = resolve(method, parallelism, p);
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = 1.0 / (double)p;
+  epi.out_re = d_re;
+  epi.out_im = d_im;
+  return sums_dispatch(d_ev, (int64_t)p, d_ev, nullptr, (int64_t)p, eta, m, precision, cutoff,
+                       epi, s);
+}
+
+shrk_status shrk_stieltjes_all(const double* ev, size_t p, double eta, int method, int precision,
+                               double cutoff, int parallelism, double* out_re, double* out_im) {
+  SHRK_TRY(check_common(p, eta, method, precision));
+  SHRK_TRY(check_cutoff(cutoff));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  int m = resolve(method, parallelism, p);
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = 1.0 / (double)p;
+  epi.out_re = (double*)out;
+  epi.out_im = (double*)out + p;
+  SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, ev, (int64_t)p, eta,
+                         m, precision, cutoff, epi, s));
+  SHRK_TRY(d2h(out_re, out, sizeof(double) * p, s));
+  SHRK_TRY(d2h(out_im, (double*)out + p, sizeof(double) * p, s));
+  return check_device_error(s);
+}
+
+shrk_status shrk_stieltjes_all_f32(const float* ev, size_t p, float eta, int method,
+                                   double cutoff, float* out_re, float* out_im) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (!(std::isfinite(eta) && eta > 0.0f)) return einval("eta must be a positive finite number");
+  SHRK_TRY(check_cutoff(cutoff));
+  // mod.rs:818-847: Blocked/BlockedTiled/Auto without a cutoff run the f32
+  // kernel; every other combination runs the f64 path and rounds.
+  if (!(method == SHRK_M_BLOCKED || method == SHRK_M_BLOCKED_TILED || method == SHRK_M_AUTO) ||
+      !std::isnan(cutoff)) {
+    std::vector<double> e64(ev, ev + p), r(p), i(p);
+    // Parallelism::Sequential (mod.rs:836-845)
+    SHRK_TRY(shrk_stieltjes_all(e64.data(), p, (double)eta, method, SHRK_PREC_F64, cutoff,
+                                SHRK_PAR_SEQUENTIAL, r.data(), i.data()));
+    for (size_t k = 0; k < p; ++k) {
+      out_re[k] = (float)r[k];
+      out_im[k] = (float)i[k];
+    }
+    return SHRK_OK;
+  }
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(float) * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(float) * 2 * p, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(float) * p, s));
+  SHRK_TRY(all_f32((const float*)dev, (int64_t)p, eta, (float*)out, (float*)out + p, s));
+  SHRK_TRY(d2h(out_re, out, sizeof(float) * p, s));
+  SHRK_TRY(d2h(out_im, (float*)out + p, sizeof(float) * p, s));
+  return check_device_error(s);
+}
+
+shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const double* d_ev, size_t p,
+                                         double eta, int method, int precision, double cutoff,
+                                         int parallelism, double* d_re, double* d_im,
+                                         void* stream) {
+  SHRK_TRY(check_common(p, eta, method, precision));
+  SHRK_TRY(check_cutoff(cutoff));
+  if (nq == 0) return SHRK_OK;
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
+  const bool par = parallelism == SHRK_PAR_PARALLEL;
+  int m = method;
+  if (is_auto(m)) m = shrk_grid_appropriate(shrk_resolve_auto_method(m, par, p), p, nq);
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = 1.0;
+  epi.out_re = d_re;
+  epi.out_im = d_im;
+  return sums_dispatch(d_q, (int64_t)nq, d_ev, nullptr, (int64_t)p, eta, m, precision, cutoff,
+                       epi, s);
+}
+
+shrk_status shrk_stieltjes_at_points(const double* q, size_t nq, const double* ev, size_t p,
+                                     double eta, int method, int precision, double cutoff,
+                                     int parallelism, double* raw_re, double* raw_im) {
+  SHRK_TRY(check_common(p, eta, method, precision));
+  SHRK_TRY(check_cutoff(cutoff));
+  if (nq == 0) return SHRK_OK;
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  const bool par = parallelism == SHRK_PAR_PARALLEL;
+  int m = method;
+  if (is_auto(m)) m = shrk_grid_appropriate(shrk_resolve_auto_method(m, par, p), p, nq);
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* dq = nullptr;
+  SHRK_TRY(scratch_get(6, sizeof(double) * nq, &dq));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 2 * nq, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  SHRK_TRY(h2d(dq, q, sizeof(double) * nq, s));
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = 1.0;
+  epi.out_re = (double*)out;
+  epi.out_im = (double*)out + nq;
+  SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)nq, (const double*)dev, ev, (int64_t)p, eta,
+                         m, precision, cutoff, epi, s));
+  SHRK_TRY(d2h(raw_re, out, sizeof(double) * nq, s));
+  SHRK_TRY(d2h(raw_im, (double*)out + nq, sizeof(double) * nq, s));
+  return check_device_error(s);
+}
+
+shrk_status shrk_stieltjes_with_deriv(const double* ev, size_t p, double eta, double* re,
+                                      double* im, double* dre, double* dim) {
+  SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, SHRK_PREC_F64));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 4 * p, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  double* o = (double*)out;
+  SHRK_TRY(with_deriv((const double*)dev, (int64_t)p, eta, o, o + p, o + 2 * p, o + 3 * p, s));
+  SHRK_TRY(d2h(re, o, sizeof(double) * p, s));
+  SHRK_TRY(d2h(im, o + p, sizeof(double) * p, s));
+  SHRK_TRY(d2h(dre, o + 2 * p, sizeof(double) * p, s));
+  SHRK_TRY(d2h(dim, o + 3 * p, sizeof(double) * p, s));
+  return check_device_error(s);
+}
+
+shrk_status shrk_stieltjes_batched_dev(const double* d_ev, const int64_t* d_offsets,
+                                       size_t n_spectra, const double* d_eta, int precision,
+                                       double* d_re, double* d_im, void* stream) {
+  if (n_spectra == 0) return SHRK_OK;
+  if (precision != SHRK_PREC_F64 && precision != SHRK_PREC_MIXED)
+    return einval("unknown precision id");
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
+  return batched(d_ev, d_offsets, nullptr, (int64_t)n_spectra, d_eta, precision, d_re, d_im, s);
+}
+
+shrk_status shrk_stieltjes_batched(const double* ev, const int64_t* offsets, size_t n_spectra,
+                                   const double* eta, int precision, double* out_re,
+                                   double* out_im) {
+  if (n_spectra == 0) return SHRK_OK;
+  if (offsets[0] != 0) return einval("offsets[0] must be 0");
+  for (size_t i = 0; i < n_spectra; ++i) {
+    if (offsets[i + 1] <= offsets[i]) return einval("every spectrum must be non-empty");
+    if (!(std::isfinite(eta[i]) && eta[i] > 0.0))
+      return einval("eta must be a positive finite number");
+  }
+  if (precision != SHRK_PREC_F64 && precision != SHRK_PREC_MIXED)
+    return einval("unknown precision id");
+  const size_t total = (size_t)offsets[n_spectra];
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * total, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 2 * total, &out));
+  void* doff = nullptr;
+  SHRK_TRY(scratch_get(6, sizeof(int64_t) * (n_spectra + 1) + sizeof(double) * n_spectra, &doff));
+  double* deta = (double*)((int64_t*)doff + n_spectra + 1);
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * total, s));
+  SHRK_TRY(h2d(doff, offsets, sizeof(int64_t) * (n_spectra + 1), s));
+  SHRK_TRY(h2d(deta, eta, sizeof(double) * n_spectra, s));
+  SHRK_TRY(batched((const double*)dev, (const int64_t*)doff, offsets, (int64_t)n_spectra, deta,
+                   precision, (double*)out, (double*)out + total, s));
+  SHRK_TRY(d2h(out_re, out, sizeof(double) * total, s));
+  SHRK_TRY(d2h(out_im, (double*)out + total, sizeof(double) * total, s));
+  return check_device_error(s);
+}
+
+shrk_status shrk_stieltjes_adjoint_dev(const double* d_ev, size_t p, double eta,
+                                       const double* d_gre, const double* d_gim, int precision,
+                                       double* d_grad, void* stream) {
+  SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, precision));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
+  return adjoint(d_ev, (int64_t)p, eta, d_gre, d_gim, precision, d_grad, s);
+}
+
+shrk_status shrk_stieltjes_adjoint(const double* ev, size_t p, double eta, const double* g_re,
+                                   const double* g_im, int precision, double* grad) {
+  SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, precision));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * 3 * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * p, &out));
+  double* d = (double*)dev;
+  SHRK_TRY(h2d(d, ev, sizeof(double) * p, s));
+  SHRK_TRY(h2d(d + p, g_re, sizeof(double) * p, s));
+  SHRK_TRY(h2d(d + 2 * p, g_im, sizeof(double) * p, s));
+  SHRK_TRY(adjoint(d, (int64_t)p, eta, d + p, d + 2 * p, precision, (double*)out, s));
+  SHRK_TRY(d2h(grad, out, sizeof(double) * p, s));
+  return check_device_error(s);
+}
+
+// ------------------------------------------------------- consumers --
+double shrk_shrinkage_factor(double li, double c, double mr, double mi) {
+  double tr = c * li * mr, ti = c * li * mi;
+  double dr = 1.0 - c + tr, di = ti;
+  double n2 = dr * dr + di * di;
+  return n2 > 0.0 ? li / n2 : li;
+}
+double shrk_inverse_bbp(double lh, double gamma, double sigma2) {
+  return inverse_bbp(lh, gamma, sigma2);
+}
+double shrk_bbp_threshold(double gamma, double sigma2) { return bbp_threshold(gamma, sigma2); }
+double shrk_mp_median_factor(double gamma) { return mp_median_factor(gamma); }
+
+shrk_status shrk_detect_spikes_bema(const double* sorted, size_t p, double gamma, double margin,
+                                    size_t* k, int64_t* idx, double* edge, double* sigma2) {
+  SpikeSplit s;
+  bema(sorted, p, gamma, margin, s);
+  *k = s.k;
+  for (size_t i = 0; i < s.k; ++i) idx[i] = (int64_t)s.idx[i];
+  *edge = s.edge;
+  *sigma2 = s.sigma2;
+  return SHRK_OK;
+}
+
+shrk_status shrk_ledoit_wolf_shrinkage(const double* ev, size_t p, double c, int method,
+                                       int precision, int parallelism, double eta, double* xi) {
+  if (p == 0) return SHRK_OK;
+  if (!std::isnan(eta)) SHRK_TRY(check_common(p, eta, method, precision));
+  Guard g;
+  SHRK_TRY(g.st);
+  return lw_device(ev, p, c, method, precision, parallelism, eta, xi);
+}
+
+shrk_status shrk_rie_shrinkage(const double* ev, size_t p, double c, int method, int precision,
+                               int parallelism, double* xi) {
+  if (p == 0) return SHRK_OK;
+  {
+    Guard g;
+    SHRK_TRY(g.st);
+    SHRK_TRY(lw_device(ev, p, c, method, precision, parallelism, NAN, xi));
+  }
+  double tr = 0.0, sh = 0.0;
+  for (size_t i = 0; i < p; ++i) tr += ev[i];
+  for (size_t i = 0; i < p; ++i) sh += xi[i];
+  double scale = sh > 0.0 ? tr / sh : 1.0;  // shrinkage.rs:37-44
+  for (size_t i = 0; i < p; ++i) xi[i] *= scale;
+  return SHRK_OK;
+}
+
+shrk_status shrk_spectral_deconvolution(const double* ev, size_t p, double c, size_t n_points,
+                                        double eta, double lmin, double lmax, int method,
+                                        int precision, int parallelism, double cutoff,
+                                        double* out7) {
+  SHRK_TRY(check_cutoff(cutoff));
+  if (p == 0 || n_points == 0) return SHRK_OK;
+  Guard g;
+  SHRK_TRY(g.st);
+  return deconv_device(ev, p, c, n_points, eta, lmin, lmax, method, precision, parallelism, cutoff,
+                       out7);
+}
+
+shrk_status shrk_estimate_population_eigenvalues(const double* ev, size_t p, double c,
+                                                 double margin, int precision, size_t* k,
+                                                 double* spikes, double* spike_sample,
+                                                 double* bulk_edge, double* sigma2,
+                                                 double* bulk_population, double* bulk_sample) {
+  *k = 0;
+  *bulk_edge = 0.0;
+  *sigma2 = 0.0;
+  if (p == 0) return SHRK_OK;
+  SpikeSplit sp;
+  detect_debias_split(ev, p, c, margin, sp);
+  *k = sp.k;
+  *bulk_edge = sp.edge;
+  *sigma2 = sp.sigma2;
+  std::copy(sp.spikes.begin(), sp.spikes.end(), spikes);
+  std::copy(sp.spike_sample.begin(), sp.spike_sample.end(), spike_sample);
+  std::copy(sp.bulk.begin(), sp.bulk.end(), bulk_sample);
+  if (sp.bulk.empty()) return SHRK_OK;
+  Guard g;
+  SHRK_TRY(g.st);
+  // RmtConfig::new(c): Blocked, Sequential, eta = 0.4/sqrt(p_bulk)
+  return lw_device(sp.bulk.data(), sp.bulk.size(), c, SHRK_M_BLOCKED, precision,
+                   SHRK_PAR_SEQUENTIAL, NAN, bulk_population);
+}
+
+shrk_status shrk_deconvolve_spiked(const double* ev, size_t p, double c, size_t n_points,
+                                   double eta, double margin, int method, int precision,
+                                   int parallelism, double cutoff, size_t* k, double* spikes,
+                                   double* spike_sample, double* bulk_edge, double* sigma2,
+                                   double* out7) {
+  SHRK_TRY(check_cutoff(cutoff));
+  *k = 0;
+  *bulk_edge = 0.0;
+  *sigma2 = 0.0;
+  if (p == 0) return SHRK_OK;
+  SpikeSplit sp;
+  detect_debias_split(ev, p, c, margin, sp);
+  *k = sp.k;
+  *bulk_edge = sp.edge;
+  *sigma2 = sp.sigma2;
+  std::copy(sp.spikes.begin(), sp.spikes.end(), spikes);
+  std::copy(sp.spike_sample.begin(), sp.spike_sample.end(), spike_sample);
+  if (sp.bulk.empty()) return SHRK_OK;
+  Guard g;
+  SHRK_TRY(g.st);
+  return deconv_device(sp.bulk.data(), sp.bulk.size(), c, n_points, eta, NAN, NAN, method,
+                       precision, parallelism, cutoff, out7);
+}
+
+// ------------------------------------------------------- profiling --
+void shrk_timing_enable(int on) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_timing = on != 0;
+}
+
+void shrk_timing_reset(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (auto& t : g_timed) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  g_timed.clear();
+  g_launches.store(0);
+}
+
+shrk_status shrk_timing_read(const char* name, int64_t* launches, double* total_ms) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int64_t n = 0;
+  double ms = 0.0;
+  for (auto& t : g_timed) {
+    if (name && t.family != name) continue;
+    float f = 0.0f;
+    cudaError_t e = cudaEventSynchronize(t.b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&f, t.a, t.b);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
+    ++n;
+    ms += f;
+  }
+  *launches = n;
+  *total_ms = ms;
+  return SHRK_OK;
+}
+
+int64_t shrk_launch_count(void) { return g_launches.load(); }
+
+shrk_status shrk_measure_pipe_rates(double* fp32, double* fp64) {
+  Guard g;
+  SHRK_TRY(g.st);
+  return measure_pipe_rates(fp32, fp64);
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Internal (C++) interfaces between the C-ABI layer and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "../../include/shrinkers_b200.h"
+
+namespace shrk {
+
+// What the FP64 reduction epilogue of the pair-sum kernels writes.
+enum EpilogueMode : int {
+  EPI_SUMS = 0,    // out_re/out_im = raw sums * scale
+  EPI_LW = 1,      // out_re = shrinkage_factor(x, c, re*scale, im*scale)
+  EPI_MP = 2,      // El Karoui inversion on a grid: 6 arrays (see exact.cu)
+  EPI_DERIV = 3,   // value + derivative (4 arrays), E7
+};
+
+struct Epilogue {
+  int mode = EPI_SUMS;
+  double scale = 1.0;      // 1/p for the all-points convention
+  double c = 0.0;          // concentration ratio (LW, MP)
+  double eta = 0.0;        // imaginary part of z (MP)
+  double* out_re = nullptr;
+  double* out_im = nullptr;
+  double* out[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+// Exact O(nt * ns) pair sums S(x_t) = sum_j 1/((x_t - s_j) - i eta), on the
+// device, with the epilogue fused into the deterministic split reduction.
+// precision: SHRK_PREC_F64 or SHRK_PREC_MIXED.
+shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src, int64_t ns,
+                            double eta, int precision, const Epilogue& epi, cudaStream_t s);
+
+// Windowed sums: only pairs with |x_t - s_j| <= window are included (sorted
+// sources).  which: bit 0 = real part, bit 1 = imaginary part.
+shrk_status windowed_sums(const double* d_tgt, int64_t nt, const double* d_src, int64_t ns,
+                          double eta, double window, double scale, double* d_re, double* d_im,
+                          cudaStream_t s);
+
+// E7: raw value + derivative at every source point.
+shrk_status with_deriv(const double* d_ev, int64_t p, double eta, double* d_re, double* d_im,
+                       double* d_dre, double* d_dim, cudaStream_t s);
+
+// E6: FP32 full-square sums scaled by 1/p in FP32.
+shrk_status all_f32(const float* d_ev, int64_t p, float eta, float* d_re, float* d_im,
+                    cudaStream_t s);
+
+// Adjoint of the all-points transform (see shrk_stieltjes_adjoint).
+shrk_status adjoint(const double* d_ev, int64_t p, double eta, const double* d_gre,
+                    const double* d_gim, int precision, double* d_grad, cudaStream_t s);
+
+// Batched uneven spectra.
+shrk_status batched(const double* d_ev, const int64_t* d_offsets, const int64_t* h_offsets,
+                    int64_t n_spectra, const double* d_eta, int precision, double* d_re,
+                    double* d_im, cudaStream_t s);
+
+// Epilogue over precomputed raw sums (n targets), same arithmetic as the
+// fused reduction of exact_pair_sums.
+shrk_status apply_epilogue(const double* d_tgt, const double* d_raw_re, const double* d_raw_im,
+                           int64_t n, const Epilogue& epi, cudaStream_t s);
+
+// Coarse-grid NUFFT: raw sums at nq points.  lo_raw/hi_raw are the first and
+// last source values (the reference's sortedness contract).
+shrk_status nufft_points(const double* d_q, int64_t nq, const double* d_src, int64_t ns,
+                         double lo_raw, double hi_raw, double eta, double* d_re, double* d_im,
+                         cudaStream_t s);
+size_t nufft_grid_size(double raw_range, double eta);
+
+// Chebyshev treecode (raw sums at nq points).
+struct ChebParams { double theta; int n; int leaf_cap; bool f32; };
+bool cheb_preset(int method, ChebParams* out);
+size_t grid_leaf_cap(size_t n, size_t p, size_t nq, size_t preset_leaf);
+shrk_status chebcode_points(const double* d_q, int64_t nq, const double* h_sorted_src,
+                            const double* d_sorted_src, int64_t ns, double eta,
+                            const ChebParams& prm, double* d_re, double* d_im, cudaStream_t s);
+
+double mixed_near_k();
+shrk_status measure_pipe_rates(double* fp32, double* fp64);
+
+}  // namespace shrk

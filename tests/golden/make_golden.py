@@ -1,0 +1,156 @@
+"""Extract the reference's golden vectors and known answers into a fixture.
+
+Reads the shrinkers crate's own test modules AS TEXT (the crate itself
+cannot be compiled here: no Rust toolchain) and writes
+``reference_vectors.json`` next to this script.  Run it where the
+reference checkout is available:
+
+    python tests/golden/make_golden.py /path/to/shrinkers
+
+Every entry records the file:line range it came from.  The JSON is
+committed; tests never read the reference checkout at run time.
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+
+def _floats(block: str) -> list[float]:
+    return [float(x.replace("_", "")) for x in re.findall(r"-?\d[\d_]*\.\d[\d_]*(?:e-?\d+)?", block)]
+
+
+def _vec_after(text: str, name: str) -> list[float]:
+    m = re.search(r"let %s: Vec<f64> = vec!\[(.*?)\];" % re.escape(name), text, re.S)
+    if not m:
+        raise SystemExit(f"golden vector {name} not found")
+    return _floats(m.group(1))
+
+
+def _line_of(text: str, needle: str) -> int:
+    return text[: text.index(needle)].count("\n") + 1
+
+
+def main(root: str) -> None:
+    src = os.path.join(root, "src")
+    out: dict = {}
+
+    # ---- El Karoui golden master: src/deconvolution/mod.rs ----
+    path = os.path.join(src, "deconvolution", "mod.rs")
+    text = open(path).read()
+    start = _line_of(text, "fn test_golden_master_regression")
+    gm = text[text.index("fn test_golden_master_regression"):]
+    gm = gm[: gm.index("// ── Convention tests")]
+    evals = _floats(re.search(r"let evals = vec!\[(.*?)\];", gm, re.S).group(1))
+    c = float(re.search(r"let c = ([\d.]+);", gm).group(1))
+    n_points = int(re.search(r"let n_points = (\d+);", gm).group(1))
+    eta = float(re.search(r"let eta = ([\d.]+);", gm).group(1))
+    out["golden_master"] = {
+        "source": f"src/deconvolution/mod.rs:{start}-{start + gm.count(chr(10))}",
+        "evals": evals, "c": c, "n_points": n_points, "eta": eta, "method": "blocked",
+        "epsilon": 1e-14,
+        "density": _vec_after(gm, "expected_density"),
+        "w_re": _vec_after(gm, "expected_w_re"),
+        "sample_stieltjes_imag": _vec_after(gm, "expected_si"),
+        "population_stieltjes_imag": _vec_after(gm, "expected_pi"),
+    }
+
+    # ---- known answer: convention A at z = 2 + 0.1i (mod.rs test_empirical_stieltjes_simple)
+    i0 = text.index("fn test_empirical_stieltjes_simple")
+    blk = text[i0: i0 + 1500]
+    num = float(re.search(r"let expected_ga_imag = -([\d.]+)_f64 / 3\.0;", blk).group(1))
+    out["empirical_at_point"] = {
+        "source": f"src/deconvolution/mod.rs:{_line_of(text, 'fn test_empirical_stieltjes_simple')}",
+        "evals": [1.0, 2.0, 3.0], "z": [2.0, 0.1], "ga_imag": -num / 3.0, "ga_real": 0.0,
+    }
+
+    # ---- term.rs known answer
+    path = os.path.join(src, "stieltjes", "term.rs")
+    text = open(path).read()
+    ln = _line_of(text, "fn test_term_basic")
+    m = re.search(r"stieltjes_term\(([\d.]+), ([\d.]+), ([\d.]+)\)", text[text.index("fn test_term_basic"):])
+    out["term_basic"] = {"source": f"src/stieltjes/term.rs:{ln}",
+                         "args": [float(m.group(1)), float(m.group(2)), float(m.group(3))],
+                         "expected": [1.0 / 1.01, 0.1 / 1.01], "tol": 1e-15}
+
+    # ---- cacheblock.rs: unsorted 7-value sym case, p = 1 case
+    path = os.path.join(src, "stieltjes", "cacheblock.rs")
+    text = open(path).read()
+    i0 = text.index("fn test_symmetric_all_points_matches_reference")
+    blk = text[i0: i0 + 3000]
+    evals7 = _floats(re.search(r"let evals = vec!\[(.*?)\];", blk, re.S).group(1))
+    eta7 = float(re.search(r"let eta = ([\d.]+);", blk).group(1))
+    m1 = re.search(r"compute_all_stieltjes_blocked_tiled\(&\[([\d.]+)\], ([\d.]+)", blk)
+    out["symmetric_small"] = {
+        "source": f"src/stieltjes/cacheblock.rs:{_line_of(text, 'fn test_symmetric_all_points_matches_reference')}",
+        "evals": evals7, "eta": eta7, "tol": 1e-12,
+        "p1": {"lambda": float(m1.group(1)), "eta": float(m1.group(2)), "re": 0.0,
+               "im": 1.0 / float(m1.group(2))},
+        "big": {"n": 1000, "rule": "((i*7919) % 9973)/9973*4-2 sorted", "eta": 0.11, "tol": 1e-12},
+    }
+
+    # ---- estimation.rs: inverse BBP round trip and threshold
+    path = os.path.join(src, "spiked", "estimation.rs")
+    text = open(path).read()
+    i0 = text.index("fn test_inverse_bbp_roundtrip")
+    blk = text[i0: i0 + 800]
+    ells = _floats(re.search(r"for ell in \[(.*?)\]", blk).group(1))
+    gamma = float(re.search(r"let gamma = ([\d.]+);", blk).group(1))
+    out["inverse_bbp_roundtrip"] = {
+        "source": f"src/spiked/estimation.rs:{_line_of(text, 'fn test_inverse_bbp_roundtrip')}",
+        "gamma": gamma, "sigma2": 1.0, "ells": ells, "tol": 1e-10,
+    }
+    out["bbp_threshold"] = {
+        "source": f"src/spiked/estimation.rs:{_line_of(text, 'fn test_bbp_threshold_formula')}",
+        "gamma": 0.25, "sigma2": 2.0, "expected": 4.5, "tol": 1e-12,
+    }
+
+    # ---- detection.rs: BEMA known counts
+    path = os.path.join(src, "spiked", "detection.rs")
+    text = open(path).read()
+    out["bema_known"] = {
+        "source": f"src/spiked/detection.rs:{_line_of(text, 'fn test_detect_spikes_bema_known')}",
+        "bulk": {"n": 100, "start": 0.5, "step": 0.015}, "spikes": [5.0, 7.0, 10.0],
+        "gamma": 0.25, "margin": 1.0, "k": 3,
+    }
+    out["bema_none"] = {
+        "source": f"src/spiked/detection.rs:{_line_of(text, 'fn test_detect_spikes_bema_no_spikes')}",
+        "bulk": {"n": 100, "start": 0.5, "step": 0.01}, "gamma": 0.25, "margin": 1.0, "k": 0,
+    }
+    out["mp_median_factor"] = {
+        "source": f"src/spiked/detection.rs:{_line_of(text, 'fn test_mp_median_factor')}",
+        "points": [[0.0, 1.0, 1e-3], [0.25, 0.916, 0.01], [1.0, 0.653, 0.01]],
+    }
+
+    # ---- nufft.rs: grid sizing pins
+    path = os.path.join(src, "stieltjes", "nufft.rs")
+    text = open(path).read()
+    out["nufft_grid"] = {
+        "source": f"src/stieltjes/nufft.rs:{_line_of(text, 'fn grid_size_is_capped_and_independent_of_p')}",
+        "cases": [[4.0, 1e-4, 65536], [2.0, 0.01, 32768], [2.0, 1e-300, 65536]],
+    }
+
+    # ---- config.rs: auto-resolution pins
+    path = os.path.join(src, "config.rs")
+    text = open(path).read()
+    i0 = text.index("fn test_auto_resolution_is_parallelism_aware")
+    blk = text[i0: i0 + 3000]
+    cases = []
+    for par, p, meth in re.findall(
+            r"Parallelism::(\w+),\s*([\d_]+)usize,\s*StieltjesMethod::(\w+)", blk):
+        cases.append([par == "Parallel", int(p.replace("_", "")), meth])
+    out["auto_resolution"] = {
+        "source": f"src/config.rs:{_line_of(text, 'fn test_auto_resolution_is_parallelism_aware')}",
+        "cases": cases,
+    }
+
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {dst}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

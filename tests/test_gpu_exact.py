@@ -1,0 +1,233 @@
+"""Parity of the exact CUDA kernels with the oracle (GPU; through the C ABI).
+
+Bars: FP64 path <= 1e-12 relative (normwise rel-L2 and per point with the
+reference's floor scale = max(|re|, |im|, 1e-12), mod.rs:1024-1029);
+MIXED path <= 1e-9 median relative error vs the double-double truth.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from shrinkers_b200 import _native, spectra
+
+pytestmark = pytest.mark.gpu
+
+F64, MIXED = 0, 1
+NAN = float("nan")
+_D = C.POINTER(C.c_double)
+
+
+def dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def gpu_all(ev, eta, method="blocked", precision=F64, cutoff=NAN, parallel=0):
+    L = _native.load()
+    ev = np.ascontiguousarray(ev, dtype=np.float64)
+    re, im = np.empty(ev.size), np.empty(ev.size)
+    m = C.c_int()
+    assert L.shrk_parse_method(method.encode(), C.byref(m)) == 0
+    st = L.shrk_stieltjes_all(dp(ev), ev.size, eta, m.value, precision, cutoff, parallel, dp(re), dp(im))
+    _native.check(st, "stieltjes_all")
+    return re, im
+
+
+def gpu_points(q, ev, eta, method="blocked", precision=F64, cutoff=NAN):
+    L = _native.load()
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    ev = np.ascontiguousarray(ev, dtype=np.float64)
+    re, im = np.empty(q.size), np.empty(q.size)
+    m = C.c_int()
+    L.shrk_parse_method(method.encode(), C.byref(m))
+    st = L.shrk_stieltjes_at_points(dp(q), q.size, dp(ev), ev.size, eta, m.value, precision,
+                                    cutoff, 0, dp(re), dp(im))
+    _native.check(st, "stieltjes_at_points")
+    return re, im
+
+
+def rel_err_pointwise(re, im, ref_re, ref_im):
+    scale = np.maximum(np.maximum(np.abs(ref_re), np.abs(ref_im)), 1e-12)
+    return (np.abs(re - ref_re) + np.abs(im - ref_im)) / scale
+
+
+def rel_l2(re, im, ref_re, ref_im):
+    return math.sqrt(np.sum((re - ref_re) ** 2 + (im - ref_im) ** 2) /
+                     np.sum(ref_re ** 2 + ref_im ** 2))
+
+
+SIZES = [1, 2, 3, 5, 63, 64, 65, 255, 257, 1023, 1024, 1025, 2001, 4099, 12347]
+
+
+@pytest.mark.parametrize("p", SIZES)
+def test_f64_all_points_matches_oracle(oracle, p):
+    ev = spectra.config2(p, seed=p) if p > 5 else np.sort(np.random.default_rng(p).uniform(0, 3, p))
+    eta = 1.0 / math.sqrt(p)
+    re, im = gpu_all(ev, eta)
+    for par in (False, True):
+        o_re, o_im = oracle.compute_all(ev, eta, "blocked", parallel=par)
+        assert np.max(rel_err_pointwise(re, im, o_re, o_im)) < 1e-12
+        assert rel_l2(re, im, o_re, o_im) < 1e-12
+
+
+def test_p1_is_pure_diagonal():
+    """cacheblock.rs:1604-1607: p = 1 gives (0, 1/eta) before the 1/p scale."""
+    re, im = gpu_all(np.array([2.0]), 0.5)
+    assert re[0] == 0.0 and abs(im[0] - 2.0) < 1e-15
+
+
+def test_unsorted_seven_values(oracle, golden):
+    """cacheblock.rs:1580-1602: unsorted input, 1e-12 vs the per-row sum."""
+    g = golden["symmetric_small"]
+    ev = np.array(g["evals"])
+    re, im = gpu_all(ev, g["eta"])
+    for i, li in enumerate(ev):
+        r, m = oracle.autovec_sum(li, ev, g["eta"])
+        assert abs(re[i] * ev.size - r) < g["tol"] and abs(im[i] * ev.size - m) < g["tol"]
+
+
+def test_unsorted_large_matches_sorted(oracle):
+    p = 5000
+    ev = spectra.config2(p)
+    perm = np.random.default_rng(11).permutation(p)
+    eta = 1.0 / math.sqrt(p)
+    re, im = gpu_all(ev[perm], eta)
+    o_re, o_im = oracle.compute_all(ev[perm], eta, "blocked", parallel=True)
+    assert np.max(rel_err_pointwise(re, im, o_re, o_im)) < 1e-12
+    # MIXED on unsorted input: every CTA's targets are spread over the whole
+    # spectrum, so the kernel keeps those pairs in FP64; both orders stay
+    # within the mixed bar of the FP64 result.
+    for order in (perm, np.arange(p)):
+        r2, i2 = gpu_all(ev[order], eta, precision=MIXED)
+        err = np.hypot(r2 - o_re[np.argsort(perm)][order], i2 - o_im[np.argsort(perm)][order])
+        err /= np.hypot(o_re[np.argsort(perm)][order], o_im[np.argsort(perm)][order])
+        assert np.median(err) <= 1e-9 and np.max(err) <= 1e-6
+
+
+@pytest.mark.parametrize("method", ["naive", "autovec", "blocked", "blocked_autovec",
+                                    "blocked_tiled", "blocked_windowed", "blocked_hybrid"])
+def test_every_exact_alias_matches_naive(oracle, method):
+    """mod.rs:858-913 on the GPU: every exact method name, p = 50, 1e-13."""
+    ev = np.log1p((np.arange(50) + 0.5) * 0.2)
+    eta = 0.05
+    ref = np.array([oracle.naive_sum(li, ev, eta) for li in ev]) / 50.0
+    re, im = gpu_all(ev, eta, method)
+    assert np.max(np.abs(re - ref[:, 0])) < 1e-13
+    assert np.max(np.abs(im - ref[:, 1])) < 1e-13
+
+
+def test_golden_master_through_gpu(golden):
+    """deconvolution/mod.rs:281-399 golden master via shrk_spectral_deconvolution."""
+    g = golden["golden_master"]
+    L = _native.load()
+    ev = np.array(g["evals"])
+    n = g["n_points"]
+    out = np.zeros(7 * n)
+    st = L.shrk_spectral_deconvolution(dp(ev), ev.size, g["c"], n, g["eta"], NAN, NAN, 2, F64, 0,
+                                       NAN, dp(out))
+    _native.check(st)
+    o = out.reshape(7, n)
+    np.testing.assert_allclose(o[1], g["density"], rtol=0, atol=g["epsilon"])
+    np.testing.assert_allclose(o[2], g["w_re"], rtol=0, atol=g["epsilon"])
+    np.testing.assert_allclose(o[4], g["sample_stieltjes_imag"], rtol=0, atol=g["epsilon"])
+    np.testing.assert_allclose(o[6], g["population_stieltjes_imag"], rtol=0, atol=g["epsilon"])
+
+
+@pytest.mark.parametrize("nq,p", [(1, 1000), (200, 1000), (200, 50000), (4097, 3001)])
+def test_at_points_matches_oracle(oracle, nq, p):
+    ev = spectra.config2(p, seed=nq)
+    eta = 0.1 / math.sqrt(p)
+    q = np.linspace(ev[0] - 0.1, ev[-1] + 0.1, nq)
+    re, im = gpu_points(q, ev, eta)
+    o_re, o_im = oracle.compute_at_points(q, ev, eta, "blocked")
+    assert np.max(rel_err_pointwise(re, im, o_re, o_im)) < 1e-12
+
+
+@pytest.mark.parametrize("p", [1000, 20000])
+def test_mixed_precision_error_vs_truth(oracle, p):
+    ev = spectra.config2(p)
+    eta = 1.0 / math.sqrt(p)
+    re, im = gpu_all(ev, eta, precision=MIXED)
+    t_re, t_im = oracle.truth_points(ev, ev, eta)
+    err = np.hypot(re - t_re / p, im - t_im / p) / np.hypot(t_re / p, t_im / p)
+    assert np.median(err) <= 1e-9, np.median(err)
+    assert np.max(err) <= 1e-6, np.max(err)
+
+
+def test_cutoff_windowed_matches_oracle(oracle):
+    """mod.rs:998-1033: with a cutoff the exact family runs the windowed sums."""
+    p = 8000
+    ev = spectra.log_spectrum(p)
+    eta = 0.1 / math.sqrt(p)
+    for method in ["blocked", "blocked_windowed", "blocked_hybrid"]:
+        re, im = gpu_all(ev, eta, method, cutoff=10.0)
+        o_re, o_im = oracle.compute_all(ev, eta, method, cutoff=10.0)
+        assert np.max(rel_err_pointwise(re, im, o_re, o_im)) < 1e-10, method
+
+
+def test_with_deriv_matches_oracle(oracle):
+    """autovec.rs:38-77 value + derivative."""
+    L = _native.load()
+    p = 3000
+    ev = spectra.log_spectrum(p)
+    eta = 0.05 / math.sqrt(p)
+    out = [np.empty(p) for _ in range(4)]
+    _native.check(L.shrk_stieltjes_with_deriv(dp(ev), p, eta, *[dp(o) for o in out]))
+    ref = oracle.with_deriv(ev, eta)
+    for a, b in zip(out, ref):
+        np.testing.assert_allclose(a, b, rtol=1e-11, atol=1e-11 * np.max(np.abs(b)))
+
+
+def test_f32_precision_matches_oracle(oracle):
+    """cacheblock.rs:1525-1572: f32 path, rtol 5e-2 vs f64 (test_python_api.py:484-489)."""
+    L = _native.load()
+    p = 3000
+    ev = spectra.config2(p).astype(np.float32)
+    eta = np.float32(1.0 / math.sqrt(p))
+    re, im = np.empty(p, np.float32), np.empty(p, np.float32)
+    fp = C.POINTER(C.c_float)
+    _native.check(L.shrk_stieltjes_all_f32(ev.ctypes.data_as(fp), p, eta, 2, NAN,
+                                           re.ctypes.data_as(fp), im.ctypes.data_as(fp)))
+    o_re, o_im = oracle.all_f32(ev, eta)
+    np.testing.assert_allclose(re, o_re, rtol=1e-3, atol=1e-3 * np.max(np.abs(o_re)))
+    np.testing.assert_allclose(im, o_im, rtol=1e-3)
+    f_re, f_im = gpu_all(ev.astype(np.float64), float(eta))
+    np.testing.assert_allclose(re, f_re, rtol=5e-2, atol=5e-2 * np.max(np.abs(f_re)))
+
+
+def test_full_size_properties():
+    """p = 1e6 (BASELINE scale-up workload): size-independent checks.
+    * antisymmetry: sum_i Re S(lambda_i) = 0 up to rounding;
+    * MIXED vs FP64 on the device: median relative difference <= 1e-9;
+    * a sample of targets against the double-double truth on the host."""
+    from oracle import oracle as O
+    p = 1_000_000
+    ev = spectra.config2(p)
+    eta = 1.0 / math.sqrt(p)
+    r64, i64 = gpu_all(ev, eta, precision=F64)
+    rmx, imx = gpu_all(ev, eta, precision=MIXED)
+    assert abs(np.sum(r64)) / np.sum(np.abs(r64)) < 1e-12
+    d = np.hypot(rmx - r64, imx - i64) / np.hypot(r64, i64)
+    assert np.median(d) <= 1e-9, np.median(d)
+    idx = np.random.default_rng(0).choice(p, 48, replace=False)
+    t_re, t_im = O.truth_points(ev[idx], ev, eta)
+    e64 = np.hypot(r64[idx] - t_re / p, i64[idx] - t_im / p) / np.hypot(t_re / p, t_im / p)
+    assert np.max(e64) < 1e-12
+    emx = np.hypot(rmx[idx] - t_re / p, imx[idx] - t_im / p) / np.hypot(t_re / p, t_im / p)
+    assert np.median(emx) <= 1e-9
+
+
+@pytest.mark.parametrize("p", [1000, 3001])
+def test_adjoint_matches_direct_gradient(oracle, p):
+    L = _native.load()
+    ev = spectra.config5(p)
+    eta = 1.0 / math.sqrt(p)
+    rng = np.random.default_rng(5)
+    w, v = rng.standard_normal(p), rng.standard_normal(p)
+    ref = oracle.adjoint_direct(ev, eta, w, v)
+    for prec, tol in [(F64, 1e-11), (MIXED, 1e-7)]:
+        g = np.empty(p)
+        _native.check(L.shrk_stieltjes_adjoint(dp(ev), p, eta, dp(w), dp(v), prec, dp(g)))
+        err = np.abs(g - ref) / (np.abs(ref) + 1e-3 * np.max(np.abs(ref)))
+        assert np.median(err) < tol * 1e-2 and np.max(err) < tol, (prec, np.max(err))

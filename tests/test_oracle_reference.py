@@ -1,0 +1,266 @@
+"""The oracle pinned against the reference's own golden vectors, known
+answers and tolerance suite (CPU only).
+
+Fixtures come from tests/golden/reference_vectors.json (extracted from the
+crate's test modules by tests/golden/make_golden.py); tolerances are the
+reference's own, cited per test.
+"""
+import numpy as np
+import pytest
+
+from shrinkers_b200 import spectra
+
+
+def rel_l2(a_re, a_im, b_re, b_im):
+    num = np.sqrt(np.sum((a_re - b_re) ** 2 + (a_im - b_im) ** 2))
+    return num / np.sqrt(np.sum(b_re ** 2 + b_im ** 2))
+
+
+# ---------------------------------------------------------------- golden --
+def test_golden_master_regression(oracle, golden):
+    """deconvolution/mod.rs:281-399: El Karoui inversion at epsilon 1e-14."""
+    g = golden["golden_master"]
+    r = oracle.spectral_deconvolution(np.array(g["evals"]), g["c"], g["n_points"], eta=g["eta"],
+                                      method="blocked")
+    for key in ["density", "w_re", "sample_stieltjes_imag", "population_stieltjes_imag"]:
+        np.testing.assert_allclose(r[key], g[key], rtol=0, atol=g["epsilon"])
+
+
+def test_empirical_at_point_known_answer(oracle, golden):
+    """deconvolution/mod.rs:646-665: Im g_A(2+0.1i) = -10.198.../3 for {1,2,3}."""
+    g = golden["empirical_at_point"]
+    re, im = oracle.compute_at_points([g["z"][0]], g["evals"], g["z"][1], method="naive")
+    p = len(g["evals"])
+    # convention A = -S/p (mod.rs:67-84)
+    assert abs(-re[0] / p - g["ga_real"]) < 1e-12
+    assert abs(-im[0] / p - g["ga_imag"]) < 1e-10
+
+
+def test_term_basic(oracle, golden):
+    """term.rs:52-57."""
+    g = golden["term_basic"]
+    r, i = oracle.term(*g["args"])
+    assert abs(r - g["expected"][0]) < g["tol"]
+    assert abs(i - g["expected"][1]) < g["tol"]
+
+
+def test_symmetric_sweep_known_cases(oracle, golden):
+    """cacheblock.rs:1580-1624: unsorted 7 values, p = 1, sym vs full square."""
+    g = golden["symmetric_small"]
+    ev = np.array(g["evals"])
+    re, im = oracle.symmetric_sweep(ev, g["eta"])
+    for i, li in enumerate(ev):
+        r, m = oracle.autovec_sum(li, ev, g["eta"])
+        assert abs(re[i] - r) < g["tol"] and abs(im[i] - m) < g["tol"]
+    r1, i1 = oracle.symmetric_sweep([g["p1"]["lambda"]], g["p1"]["eta"])
+    assert r1[0] == 0.0
+    assert abs(i1[0] - g["p1"]["im"]) < 1e-15
+    big = np.sort([((i * 7919) % 9973) / 9973.0 * 4.0 - 2.0 for i in range(g["big"]["n"])])
+    sr, si = oracle.symmetric_sweep(big, g["big"]["eta"])
+    pr, pi = oracle.tiled_full_square(big, g["big"]["eta"])
+    scale = np.maximum(np.maximum(np.abs(sr), np.abs(si)), 1e-12)
+    assert np.max((np.abs(pr - sr) + np.abs(pi - si)) / scale) < g["big"]["tol"]
+
+
+def test_inverse_bbp_roundtrip(oracle, golden):
+    """estimation.rs:98-108 (+ threshold 120-126)."""
+    g = golden["inverse_bbp_roundtrip"]
+    for ell in g["ells"]:
+        lh = ell * (1.0 + g["gamma"] / (ell - 1.0))
+        assert abs(oracle.inverse_bbp(lh, g["gamma"], g["sigma2"]) - ell) < g["tol"]
+    t = golden["bbp_threshold"]
+    assert abs(oracle.bbp_threshold(t["gamma"], t["sigma2"]) - t["expected"]) < t["tol"]
+    edge = oracle.bbp_threshold(0.5, 1.0)
+    assert abs(oracle.inverse_bbp(edge, 0.5, 1.0) - edge) < 1e-10
+
+
+def test_bema_known_counts(oracle, golden):
+    """detection.rs:286-311."""
+    g = golden["bema_known"]
+    b = g["bulk"]
+    ev = np.sort(np.concatenate([b["start"] + b["step"] * np.arange(b["n"]), g["spikes"]]))
+    r = oracle.bema(ev, g["gamma"], g["margin"])
+    assert r["k"] == g["k"]
+    assert 2.0 < r["bulk_edge"] < 5.0
+    g = golden["bema_none"]
+    b = g["bulk"]
+    ev = b["start"] + b["step"] * np.arange(b["n"])
+    assert oracle.bema(ev, g["gamma"], g["margin"])["k"] == g["k"]
+    for gam, want, tol in golden["mp_median_factor"]["points"]:
+        assert abs(oracle.mp_median_factor(gam) - want) < tol
+
+
+def test_nufft_grid_pins(oracle, golden):
+    """nufft.rs:229-250."""
+    for raw, eta, m in golden["nufft_grid"]["cases"]:
+        assert oracle.nufft_grid_size(raw, eta) == m
+
+
+def test_auto_resolution_pins(oracle, golden):
+    """config.rs:592-658 + at-points redirect 661-713."""
+    for par, p, meth in golden["auto_resolution"]["cases"]:
+        name = {"ChebCodeFast": "chebcode_fast", "Nufft": "nufft"}[meth]
+        assert oracle.lib().orc_resolve_auto_method(oracle.M["auto"], int(par), p) == oracle.M[name]
+    ga = oracle.lib().orc_grid_appropriate
+    assert ga(oracle.M["nufft"], 200_000, 200) == oracle.M["chebcode_fast"]
+    assert ga(oracle.M["nufft"], 300_000, 200) == oracle.M["nufft"]
+    assert ga(oracle.M["fft5"], 50_000, 200) == oracle.M["chebcode_fast"]
+    assert ga(oracle.M["chebcode"], 50_000, 200) == oracle.M["chebcode"]
+
+
+# ------------------------------------------------------ tolerance suite --
+def test_all_exact_methods_agree(oracle):
+    """mod.rs:858-913: every exact method vs naive at p=50, 1e-13."""
+    ev = np.log1p((np.arange(50) + 0.5) * 0.2)
+    eta = 0.05
+    ref = np.array([oracle.naive_sum(li, ev, eta) for li in ev]) / 50.0
+    for m in ["naive", "autovec", "blocked", "blocked_tiled", "blocked_windowed",
+              "blocked_hybrid"]:
+        re, im = oracle.compute_all(ev, eta, m)
+        assert np.max(np.abs(re - ref[:, 0])) < 1e-13, m
+        assert np.max(np.abs(im - ref[:, 1])) < 1e-13, m
+
+
+@pytest.mark.parametrize("p", [300, 2001, 2002, 2003, 4001])
+def test_tiled_parallel_matches_sequential(oracle, p):
+    """mod.rs:1035-1085: includes p % 4 != 0 (the remainder-bug class), 1e-12."""
+    ev = spectra.log_spectrum(p)
+    eta = 0.1 / np.sqrt(p)
+    s_re, s_im = oracle.compute_all(ev, eta, "blocked", parallel=False)
+    p_re, p_im = oracle.compute_all(ev, eta, "blocked", parallel=True)
+    scale = np.maximum(np.maximum(np.abs(s_re), np.abs(s_im)), 1e-12)
+    assert np.max((np.abs(p_re - s_re) + np.abs(p_im - s_im)) / scale) < 1e-12
+
+
+def test_with_deriv_matches_finite_difference(oracle):
+    """autovec.rs:115-148."""
+    p = 300
+    ev = spectra.log_spectrum(p)
+    eta = 0.05 / np.sqrt(p)
+    re, im, dre, dim = oracle.with_deriv(ev, eta)
+    for i in range(0, p, 37):
+        r, m = oracle.autovec_sum(ev[i], ev, eta)
+        assert abs(re[i] - r) < 1e-10 and abs(im[i] - m) < 1e-10
+    for i in [0, 1, p // 3, p - 1]:
+        h = min(1e-5, max(abs(ev[i]), 1.0) * 1e-5)
+        rp, ip = oracle.autovec_sum(ev[i] + h, ev, eta)
+        rm, imm = oracle.autovec_sum(ev[i] - h, ev, eta)
+        fd = ((rp - rm) / (2 * h), (ip - imm) / (2 * h))
+        tol = 8e-2 if i == 0 else 5e-4
+        assert abs(dre[i] - fd[0]) < tol * (abs(fd[0]) + 1.0)
+        assert abs(dim[i] - fd[1]) < tol * (abs(fd[1]) + 1.0)
+
+
+@pytest.mark.parametrize("p", [512, 2000, 8000])
+def test_chebcode_default_accuracy(oracle, p):
+    """chebcode.rs:1401-1419: DEFAULT preset max rel < 1e-2."""
+    ev = spectra.log_spectrum(p)
+    eta = 0.1 / np.sqrt(p)
+    ex_re, ex_im = oracle.compute_all(ev, eta, "blocked", parallel=True)
+    cr, ci = oracle.compute_all(ev, eta, "chebcode", parallel=True)
+    scale = np.maximum(np.abs(ex_re) + np.abs(ex_im), 1e-12)
+    assert np.max((np.abs(cr - ex_re) + np.abs(ci - ex_im)) / scale) < 1e-2
+
+
+def test_chebcode_presets_error_classes(oracle):
+    """Preset error classes (chebcode.rs:939-972, RESULT.md) on an MP spectrum."""
+    p = 8000
+    ev = spectra.config2(p)
+    eta = 1.0 / np.sqrt(p)
+    ex_re, ex_im = oracle.compute_all(ev, eta, "blocked", parallel=True)
+    for name, tol in [("chebcode_fast", 5e-5), ("chebcode", 5e-8), ("chebcode_balanced", 5e-8),
+                      ("chebcode_xtreme", 1e-10)]:
+        r, i = oracle.compute_all(ev, eta, name, parallel=True)
+        assert rel_l2(r, i, ex_re, ex_im) < tol, name
+
+
+def test_chebcode_unsorted_input(oracle):
+    """chebcode.rs:1366-1399: shuffled input, results in input order."""
+    p = 512
+    ev = spectra.log_spectrum(p)
+    perm = np.random.default_rng(7).permutation(p)
+    r1, i1 = oracle.compute_all(ev, 0.05, "chebcode")
+    r2, i2 = oracle.compute_all(ev[perm], 0.05, "chebcode")
+    np.testing.assert_allclose(r2, r1[perm], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(i2, i1[perm], rtol=0, atol=1e-12)
+
+
+def test_nufft_matches_exact_and_parallel(oracle):
+    """nufft.rs:252-318: rel-L2 < 1e-4 at p=8192, eta=1/sqrt(p), seq/par < 1e-9."""
+    p = 8192
+    ev = spectra.log_spectrum(p)
+    eta = 1.0 / np.sqrt(p)
+    ex_re, ex_im = oracle.compute_all(ev, eta, "blocked", parallel=True)
+    got = oracle.nufft_points(ev, ev, eta, parallel=False)
+    assert rel_l2(got[0] / p, got[1] / p, ex_re, ex_im) < 1e-4
+    par = oracle.nufft_points(ev, ev, eta, parallel=True)
+    assert np.max(np.maximum(np.abs(got[0] - par[0]), np.abs(got[1] - par[1]))) < 1e-9
+    grid = ev[0] + (ev[-1] - ev[0]) * np.arange(200) / 199.0
+    eg = oracle.compute_at_points(grid, ev, eta, "blocked", parallel=True)
+    gg = oracle.nufft_points(grid, ev, eta)
+    assert rel_l2(gg[0], gg[1], eg[0], eg[1]) < 1e-4
+
+
+def test_fft_matches_dft(oracle):
+    """The oracle's own radix-2 FFT against a direct DFT (rustfft contract)."""
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(256) + 1j * rng.standard_normal(256)
+    np.testing.assert_allclose(oracle.fft(x, -1), np.fft.fft(x), rtol=0, atol=1e-11)
+    np.testing.assert_allclose(oracle.fft(x, +1), np.fft.ifft(x) * 256, rtol=0, atol=1e-11)
+
+
+def test_lagrange_partition_of_unity(oracle):
+    """fft5.rs:774-804."""
+    for t in np.linspace(0, 0.999, 17):
+        assert abs(oracle.lagrange4(t).sum() - 1.0) < 1e-14
+
+
+def test_truth_matches_exact(oracle):
+    """The double-double truth agrees with the FP64 sums to ~1e-14."""
+    ev = spectra.config2(2000)
+    eta = 1.0 / np.sqrt(2000)
+    tr, ti = oracle.truth_points(ev, ev, eta)
+    er, ei = oracle.compute_all(ev, eta, "blocked")
+    assert rel_l2(tr / 2000, ti / 2000, er, ei) < 1e-13
+
+
+def test_adjoint_direct_matches_finite_difference(oracle):
+    """FP64 direct-sum gradient vs central differences (h = 1e-6)."""
+    p = 400
+    ev = spectra.config5(p)
+    eta = 1.0 / np.sqrt(p)
+    rng = np.random.default_rng(5)
+    w, v = rng.standard_normal(p), rng.standard_normal(p)
+    idx = np.random.default_rng(6).choice(p, 16, replace=False)
+    g = oracle.adjoint_direct(ev, eta, w, v, idx)
+
+    def loss(x):
+        # m = -conj(S)/p: Re m = -Re S/p, Im m = Im S/p (truth in double-double)
+        re, im = oracle.truth_points(x, x, eta)
+        return np.sum(w * (-re / p) + v * (im / p))
+
+    h = 1e-6
+    for t, k in enumerate(idx):
+        xp, xm = ev.copy(), ev.copy()
+        xp[k] += h
+        xm[k] -= h
+        fd = (loss(xp) - loss(xm)) / (2 * h)
+        assert abs(fd - g[t]) < 1e-5 * max(1.0, abs(g[t])), (k, fd, g[t])
+
+
+def test_lw_and_population_pipeline_shapes(oracle):
+    """population.rs:126-169 and hybrid.rs:150-200 behaviours on the oracle."""
+    bulk = 0.5 + 0.015 * np.arange(100)
+    ev = np.concatenate([bulk, [5.0, 7.0, 10.0]])
+    r = oracle.estimate_population_eigenvalues(ev, 0.25)
+    assert r["k"] == 3 and len(r["bulk_population"]) == 100
+    assert r["spikes"][0] > r["spikes"][1] > r["spikes"][2]
+    assert np.all(r["spikes"] < r["spike_sample"])
+    d = oracle.deconvolve_spiked(ev, 0.25, 100, eta=0.1, method="blocked")
+    assert d["k"] == 3 and np.all(np.isfinite(d["bulk"]["density"]))
+    lw = oracle.ledoit_wolf(bulk, 0.25)
+    np.testing.assert_allclose(r["bulk_population"][:0], lw[:0])
+    # no-spike path delegates to plain LW (population.rs:131-145)
+    ev0 = 0.5 + 0.01 * np.arange(100)
+    r0 = oracle.estimate_population_eigenvalues(ev0, 0.25)
+    np.testing.assert_allclose(r0["bulk_population"], oracle.ledoit_wolf(ev0, 0.25), atol=1e-12)
