@@ -39,7 +39,7 @@ struct DeviceState {
   bool init = false;
   int sms = 0;
   cudaStream_t stream = nullptr;
-  Scratch slots[16];
+  Scratch slots[24];
   int* err = nullptr;
 };
 
@@ -171,7 +171,8 @@ static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
 
 // Scratch slot map: 0 split partials, 1 block bounds, 2 adjoint partials,
 // 3 input spectrum, 4/5 outputs, 6 query points, 7 raw sums (2 arrays),
-// 8 sorted copy / tree, 9.. method-private.
+// 8 sorted copy of the sources, 9/10 hybrid temporaries, 11 NUFFT grids,
+// 15 probe sink, 16..21 treecode.
 
 // Raw (or scaled) sums of `method` at targets d_tgt against d_src, written
 // through `epi`.  `h_src` (may be null) is a host copy of the sources, used
@@ -210,53 +211,43 @@ static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* 
     return apply_epilogue(d_tgt, rre, rim, nt, epi, s);
   }
   if (method == SHRK_M_NUFFT || is_cheb(method)) {
-    void* raw = nullptr;
-    SHRK_TRY(scratch_get(7, sizeof(double) * 2 * nt, &raw));
-    double* rre = (double*)raw;
-    double* rim = rre + nt;
+    // Both methods need the sources in ascending order on the device: the
+    // treecode builds over the sorted copy (chebcode.rs:1088-1097) and the
+    // NUFFT splat gathers contiguous source runs per grid cell.  A host copy
+    // decides sortedness (and feeds the tree build).
+    std::vector<double> host, sorted;
+    if (!h_src) {
+      host.resize(ns);
+      SHRK_TRY(d2h(host.data(), d_src, sizeof(double) * ns, s));
+      SHRK_CUDA(cudaStreamSynchronize(s));
+      h_src = host.data();
+    }
+    const double* hs = h_src;
+    const double* ds = d_src;
+    bool sorted_in = true;
+    for (int64_t i = 1; i < ns; ++i)
+      if (!(h_src[i - 1] <= h_src[i])) { sorted_in = false; break; }
+    if (!sorted_in) {
+      sorted.assign(h_src, h_src + ns);
+      std::sort(sorted.begin(), sorted.end());
+      void* dsb = nullptr;
+      SHRK_TRY(scratch_get(8, sizeof(double) * ns, &dsb));
+      SHRK_TRY(h2d(dsb, sorted.data(), sizeof(double) * ns, s));
+      hs = sorted.data();
+      ds = (const double*)dsb;
+    }
     if (method == SHRK_M_NUFFT) {
-      double lo = 0.0, hi = 0.0;
-      if (h_src) {
-        lo = h_src[0];
-        hi = h_src[ns - 1];
-      } else {
-        SHRK_TRY(d2h(&lo, d_src, sizeof(double), s));
-        SHRK_TRY(d2h(&hi, d_src + ns - 1, sizeof(double), s));
-        SHRK_CUDA(cudaStreamSynchronize(s));
-      }
-      SHRK_TRY(nufft_points(d_tgt, nt, d_src, ns, lo, hi, eta, rre, rim, s));
+      SHRK_TRY(nufft_points(d_tgt, nt, ds, ns, h_src[0], h_src[ns - 1], eta, epi, s));
     } else {
       ChebParams prm;
       cheb_preset(method, &prm);
-      if (epi.mode == EPI_MP)  // grid path: mod.rs:475-489 relaxes the leaf cap
-        prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nt, prm.leaf_cap);
-      std::vector<double> host;
-      if (!h_src) {
-        host.resize(ns);
-        SHRK_TRY(d2h(host.data(), d_src, sizeof(double) * ns, s));
-        SHRK_CUDA(cudaStreamSynchronize(s));
-        h_src = host.data();
-      }
-      // The tree is built over the ascending copy (chebcode.rs:1088-1097).
-      std::vector<double> sorted;
-      const double* hs = h_src;
-      const double* ds = d_src;
-      bool sorted_in = true;
-      for (int64_t i = 1; i < ns; ++i)
-        if (!(h_src[i - 1] <= h_src[i])) { sorted_in = false; break; }
-      if (!sorted_in) {
-        sorted.assign(h_src, h_src + ns);
-        std::sort(sorted.begin(), sorted.end());
-        void* dsb = nullptr;
-        SHRK_TRY(scratch_get(8, sizeof(double) * ns, &dsb));
-        SHRK_TRY(h2d(dsb, sorted.data(), sizeof(double) * ns, s));
-        hs = sorted.data();
-        ds = (const double*)dsb;
-      }
-      SHRK_TRY(chebcode_points(d_tgt, nt, hs, ds, ns, eta, prm, rre, rim, s));
-      SHRK_CUDA(cudaStreamSynchronize(s));  // `sorted` / `host` are read by the build
+      // At arbitrary query points (targets are not the sources) the leaf
+      // capacity is relaxed by the grid rule (mod.rs:475-489).
+      if (d_tgt != d_src) prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nt, prm.leaf_cap);
+      SHRK_TRY(chebcode_points(d_tgt, nt, hs, ds, ns, eta, prm, epi, s));
     }
-    return apply_epilogue(d_tgt, rre, rim, nt, epi, s);
+    if (!sorted.empty()) SHRK_CUDA(cudaStreamSynchronize(s));  // h2d reads `sorted`
+    return SHRK_OK;
   }
   return not_impl(method);
 }

@@ -24,6 +24,7 @@
 // compensated (TwoSum hi/lo) accumulator.  Every other pair -- the near
 // field, where d cancels -- is summed in FP64, as are all reductions.
 #include "common.cuh"
+#include "epilogue.cuh"
 #include "internal.h"
 
 #include <algorithm>
@@ -40,15 +41,14 @@ constexpr int WT = 32 * R;     // targets per warp
 constexpr int CH = 1024;       // sources per staged chunk
 constexpr int SUB = 256;       // sources per near/far classification block
 // FP32 far-field arithmetic of the MIXED kernel (compile-time choices; the
-// defaults are the measured best, see the design notes):
-//   SHRK_RCP  0: one rcp.approx per pair
-//             1: one rcp.approx per pair + one Newton step
-//             2: one rcp.approx per TWO pairs (1/a = b/(ab), 1/b = a/(ab))
-//                + one Newton step on 1/(ab)
+// defaults are the measured best):
+//   SHRK_RCP  0: rcp.approx alone (biased: ~1.5e-9 median error at p = 1e6)
+//             1: rcp.approx + one Newton step (unbiased)
 //   SHRK_FOLDMODE 0: FP32 partials folded into a TwoSum hi/lo FP32 pair
 //                 1: FP32 partials folded into the FP64 accumulators
+//   SHRK_FOLD: sources per FP32 partial (two interleaved chains)
 #ifndef SHRK_RCP
-#define SHRK_RCP 2
+#define SHRK_RCP 1
 #endif
 #ifndef SHRK_FOLDMODE
 #define SHRK_FOLDMODE 1
@@ -70,6 +70,7 @@ struct PairArgs {
   const double* src;
   int64_t ns;
   const double2* bounds;  // per SUB block of sources: (min, max)
+  const double2* gminmax; // (min, max) over all sources
   double eta;
   double near_dist;
   int64_t n_tiles;
@@ -81,6 +82,23 @@ struct PairArgs {
   int use_tma;
 };
 
+// Power of two u >= ulp_float(M): the grid on which target offsets are
+// snapped so that (xh - mh) is exact for every |mh| <= M.  IEEE-754 bit
+// layout only (exponent field of M, shifted by the 23 fraction bits).
+__device__ __forceinline__ double snap_unit(double M) {
+  const long long bits = __double_as_longlong(M) & 0x7FF0000000000000LL;
+  return __longlong_as_double(bits) * 0x1p-23;
+}
+
+// Split x - c into xh + xl with xh a multiple of u (exact in float while
+// |x - c| < 2^23 u, which the caller guarantees).
+__device__ __forceinline__ void split_target(double x, double c, double u, float& xh, float& xl) {
+  const double xo = x - c;
+  const double h = rint(xo / u) * u;
+  xh = (float)h;
+  xl = (float)(xo - h);
+}
+
 __device__ __forceinline__ void pair64(double x, double s, double eta2, double& re, double& iv) {
   const double d = x - s;
   const double inv = rcp_f64(fma(d, d, eta2));
@@ -88,37 +106,36 @@ __device__ __forceinline__ void pair64(double x, double s, double eta2, double& 
   iv = iv + inv;
 }
 
-__device__ __forceinline__ void pair32(float xh, float xl, float mu, float eta2f, float& re,
-                                       float& iv) {
-  const float d = (xh - mu) + xl;
-  const float den = fmaf(d, d, eta2f);
-  float inv = rcp_f32(den);
-#if SHRK_RCP == 1
-  inv = fmaf(inv, fmaf(-den, inv, 1.0f), inv);  // Newton: removes the seed's bias
-#endif
-  re = fmaf(d, inv, re);
-  iv = iv + inv;
+// FP32 separation of a target and a source, both split around the CTA
+// centre c: x - c = xh + xl and s - c = mh + ml, with xh a multiple of a
+// power of two u >= ulp(max |s - c|).  Then xh - mh is exact (or rounds on
+// mh's own bits), and the final rounding of (xh - mh) + (xl - ml) depends on
+// the source's low bits ml -- the errors of different pairs are independent.
+// (Rounding a FIXED target offset onto each source's float grid instead
+// shifts the target coherently by up to half an ulp of d: a systematic error
+// that no accumulation scheme can remove.)
+__device__ __forceinline__ float sep32(float xh, float xl, float mh, float ml) {
+  return (xh - mh) + (xl - ml);
 }
 
-// Two pairs sharing one MUFU reciprocal: r ~ 1/(a b) refined by one Newton
-// step, then 1/a = b r and 1/b = a r.  The denominators of far pairs lie in
-// [(K eta)^2, range^2], so a*b stays a normal float for every spectrum the
-// far path accepts (checked on the host).
-__device__ __forceinline__ void pair32x2(float xh0, float xl0, float xh1, float xl1, float mu,
-                                         float eta2f, float& re0, float& iv0, float& re1,
-                                         float& iv1) {
-  const float d0 = (xh0 - mu) + xl0;
-  const float d1 = (xh1 - mu) + xl1;
-  const float a = fmaf(d0, d0, eta2f);
-  const float b = fmaf(d1, d1, eta2f);
-  const float ab = a * b;
-  float r = rcp_f32(ab);
-  r = fmaf(r, fmaf(-ab, r, 1.0f), r);
-  const float i0 = b * r, i1 = a * r;
-  re0 = fmaf(d0, i0, re0);
-  iv0 = iv0 + i0;
-  re1 = fmaf(d1, i1, re1);
-  iv1 = iv1 + i1;
+// Unbiased FP32 reciprocal: the MUFU seed's error has a nonzero mean (a
+// few 1e-9 relative, measured), which would add coherently over a far field
+// of ~1e6 same-signed terms; one Newton step r + r (1 - a r) removes it.
+__device__ __forceinline__ float rcp32_unbiased(float a) {
+  const float r = rcp_f32(a);
+#if SHRK_RCP == 1
+  return fmaf(r, fmaf(-a, r, 1.0f), r);
+#else
+  return r;
+#endif
+}
+
+__device__ __forceinline__ void pair32(float xh, float xl, float mh, float ml, float eta2f,
+                                       float& re, float& iv) {
+  const float d = sep32(xh, xl, mh, ml);
+  const float inv = rcp32_unbiased(fmaf(d, d, eta2f));
+  re = fmaf(d, inv, re);
+  iv = iv + inv;
 }
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -135,7 +152,8 @@ __device__ __forceinline__ double warp_min(double v) {
 template <bool MIXED>
 __global__ void __launch_bounds__(NT, 2) pair_sum_kernel(const PairArgs a) {
   __shared__ __align__(16) double sbuf[2][CH];
-  __shared__ __align__(16) float smu[MIXED ? CH : 4];
+  __shared__ __align__(16) float smu[MIXED ? CH : 4];   // high part of s - c
+  __shared__ __align__(16) float smul[MIXED ? CH : 4];  // low part of s - c
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ double red[NT / 32];
 
@@ -185,10 +203,7 @@ __global__ void __launch_bounds__(NT, 2) pair_sum_kernel(const PairArgs a) {
       double spread = 0.0, mn = x[0], mx = x[0];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const double xo = x[r] - c;
-        xh[r] = (float)xo;
-        xl[r] = (float)(xo - (double)xh[r]);
-        spread = fmax(spread, fabs(xo));
+        spread = fmax(spread, fabs(x[r] - c));
         mn = fmin(mn, x[r]);
         mx = fmax(mx, x[r]);
       }
@@ -200,7 +215,12 @@ __global__ void __launch_bounds__(NT, 2) pair_sum_kernel(const PairArgs a) {
       double w = 0.0;
 #pragma unroll
       for (int i = 0; i < NT / 32; ++i) w = fmax(w, red[i]);
-      thr = fmax(a.near_dist, w);
+      const double2 g = *a.gminmax;
+      const double u = snap_unit(fmax(fmax(g.y - c, c - g.x), w));
+      // The far path needs the targets' snapped offsets to stay exact floats.
+      thr = (w < 0x1p22 * u) ? fmax(a.near_dist, w) : INFINITY;
+#pragma unroll
+      for (int r = 0; r < R; ++r) split_target(x[r], c, u, xh[r], xl[r]);
     }
 
     auto chunk_is_tma = [&](int k) -> bool {
@@ -242,7 +262,12 @@ __global__ void __launch_bounds__(NT, 2) pair_sum_kernel(const PairArgs a) {
         return;
       }
       if (MIXED) {
-        for (int i = tid; i < len; i += NT) smu[i] = (float)(sbuf[b][i] - c);
+        for (int i = tid; i < len; i += NT) {
+          const double so = sbuf[b][i] - c;
+          const float h = (float)so;
+          smu[i] = h;
+          smul[i] = (float)(so - (double)h);
+        }
         __syncthreads();
       }
 
@@ -259,35 +284,38 @@ __global__ void __launch_bounds__(NT, 2) pair_sum_kernel(const PairArgs a) {
         }
         if (MIXED && far32) {
           const float* mp = &smu[sub];
+          const float* lp = &smul[sub];
           for (int j = 0; j < SUB; j += FOLD) {
-            float pr[R], pv[R];
+            // Two interleaved FP32 chains per target (even / odd sources)
+            // halve the partials' accumulation error at no extra work.
+            float pr[2][R], pv[2][R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) { pr[r] = 0.0f; pv[r] = 0.0f; }
+            for (int r = 0; r < R; ++r) {
+              pr[0][r] = pv[0][r] = 0.0f;
+              pr[1][r] = pv[1][r] = 0.0f;
+            }
 #pragma unroll
             for (int q = 0; q < FOLD; q += 4) {
               const float4 m4 = *reinterpret_cast<const float4*>(mp + j + q);
+              const float4 l4 = *reinterpret_cast<const float4*>(lp + j + q);
               const float ms[4] = {m4.x, m4.y, m4.z, m4.w};
+              const float ls[4] = {l4.x, l4.y, l4.z, l4.w};
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
-#if SHRK_RCP == 2
 #pragma unroll
-                for (int r = 0; r < R; r += 2)
-                  pair32x2(xh[r], xl[r], xh[r + 1], xl[r + 1], ms[u], eta2f, pr[r], pv[r],
-                           pr[r + 1], pv[r + 1]);
-#else
-#pragma unroll
-                for (int r = 0; r < R; ++r) pair32(xh[r], xl[r], ms[u], eta2f, pr[r], pv[r]);
-#endif
+                for (int r = 0; r < R; ++r)
+                  pair32(xh[r], xl[r], ms[u], ls[u], eta2f, pr[u & 1][r], pv[u & 1][r]);
               }
             }
 #pragma unroll
             for (int r = 0; r < R; ++r) {
+              const float sr = pr[0][r] + pr[1][r], sv = pv[0][r] + pv[1][r];
 #if SHRK_FOLDMODE == 1
-              re64[r] += (double)pr[r];
-              iv64[r] += (double)pv[r];
+              re64[r] += (double)sr;
+              iv64[r] += (double)sv;
 #else
-              two_sum_acc(hr[r], lr[r], pr[r]);
-              two_sum_acc(hv[r], lv[r], pv[r]);
+              two_sum_acc(hr[r], lr[r], sr);
+              two_sum_acc(hv[r], lv[r], sv);
 #endif
             }
           }
@@ -336,6 +364,29 @@ __global__ void __launch_bounds__(NT, 2) pair_sum_kernel(const PairArgs a) {
   }
 }
 
+// (min, max) over the block bounds, written after them (one CTA).
+__global__ void __launch_bounds__(1024) minmax_kernel(double2* __restrict__ bounds, int64_t nblocks) {
+  __shared__ double smin[32], smax[32];
+  double mn = INFINITY, mx = -INFINITY;
+  for (int64_t i = threadIdx.x; i < nblocks; i += blockDim.x) {
+    mn = fmin(mn, bounds[i].x);
+    mx = fmax(mx, bounds[i].y);
+  }
+  mn = warp_min(mn);
+  mx = warp_max(mx);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { smin[w] = mn; smax[w] = mx; }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    mn = lane < nw ? smin[lane] : INFINITY;
+    mx = lane < nw ? smax[lane] : -INFINITY;
+    mn = warp_min(mn);
+    mx = warp_max(mx);
+    if (lane == 0) bounds[nblocks] = make_double2(mn, mx);
+  }
+}
+
 // (min, max) of every SUB-block of sources.
 __global__ void block_bounds_kernel(const double* __restrict__ src, int64_t ns,
                                     double2* __restrict__ out, int64_t nblocks) {
@@ -374,34 +425,7 @@ __global__ void reduce_kernel(const ReduceArgs a) {
     re += a.part_re[(int64_t)s * a.nt + t];
     im += a.part_im[(int64_t)s * a.nt + t];
   }
-  const Epilogue& e = a.epi;
-  if (e.mode == EPI_SUMS) {
-    e.out_re[t] = re * e.scale;
-    e.out_im[t] = im * e.scale;
-  } else if (e.mode == EPI_LW) {
-    // shrinkage.rs:22-34 on the scaled pair (mod.rs:216-237 map_stieltjes)
-    const double li = a.tgt[t], c = e.c;
-    const double mr = re * e.scale, mi = im * e.scale;
-    const double tr = c * li * mr, ti = c * li * mi;
-    const double dr = 1.0 - c + tr, di = ti;
-    const double n2 = dr * dr + di * di;
-    e.out_re[t] = n2 > 0.0 ? li / n2 : li;
-  } else if (e.mode == EPI_MP) {
-    // deconvolution/mod.rs:206-248 on the raw grid sums
-    const double zr = a.tgt[t], zi = e.eta, c = e.c, inv_p = e.scale;
-    const double gr = -re * inv_p, gi = im * inv_p;
-    const double zgr = zr * gr - zi * gi, zgi = zr * gi + zi * gr;
-    const double ar = 1.0 - c - c * zgr, ai = -c * zgi;
-    const double an = ar * ar + ai * ai;
-    const double wr = an > 0.0 ? (zr * ar + zi * ai) / an : zr;
-    const double mr = ar * gr - ai * gi, mi = ar * gi + ai * gr;
-    e.out[0][t] = mi / 3.141592653589793;
-    e.out[1][t] = wr;
-    e.out[2][t] = gr;
-    e.out[3][t] = gi;
-    e.out[4][t] = mr;
-    e.out[5][t] = mi;
-  }
+  epi_store(a.epi, t, a.tgt[t], re, im);
 }
 
 // --------------------------------------------------------------- E7 ----
@@ -513,6 +537,7 @@ struct AdjArgs {
   const double* v;
   int64_t p;
   const double2* bounds;
+  const double2* gminmax;
   double eta;
   double near_dist;
   int64_t n_tiles;
@@ -525,7 +550,8 @@ template <bool MIXED>
 __global__ void __launch_bounds__(NT, 2) adjoint_kernel(const AdjArgs a) {
   constexpr int ACH = 512;
   __shared__ __align__(16) double sl[ACH], sw[ACH], sv[ACH];
-  __shared__ __align__(16) float fmu[MIXED ? ACH : 4], fw[MIXED ? ACH : 4], fv[MIXED ? ACH : 4];
+  __shared__ __align__(16) float fmu[MIXED ? ACH : 4], fml[MIXED ? ACH : 4];
+  __shared__ __align__(16) float fw[MIXED ? ACH : 4], fv[MIXED ? ACH : 4];
   __shared__ double red[NT / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double eta = a.eta, eta2 = eta * eta, teta = 2.0 * eta;
@@ -556,10 +582,7 @@ __global__ void __launch_bounds__(NT, 2) adjoint_kernel(const AdjArgs a) {
       double spread = 0.0, mn = x[0], mx = x[0];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const double xo = x[r] - c;
-        xh[r] = (float)xo;
-        xl[r] = (float)(xo - (double)xh[r]);
-        spread = fmax(spread, fabs(xo));
+        spread = fmax(spread, fabs(x[r] - c));
         mn = fmin(mn, x[r]);
         mx = fmax(mx, x[r]);
       }
@@ -570,7 +593,11 @@ __global__ void __launch_bounds__(NT, 2) adjoint_kernel(const AdjArgs a) {
       __syncthreads();
       double wd = 0.0;
       for (int i = 0; i < NT / 32; ++i) wd = fmax(wd, red[i]);
-      thr = fmax(a.near_dist, wd);
+      const double2 g = *a.gminmax;
+      const double u = snap_unit(fmax(fmax(g.y - c, c - g.x), wd));
+      thr = (wd < 0x1p22 * u) ? fmax(a.near_dist, wd) : INFINITY;
+#pragma unroll
+      for (int r = 0; r < R; ++r) split_target(x[r], c, u, xh[r], xl[r]);
     }
     const int64_t s0 = (int64_t)split * a.split_len, s1 = min(a.p, s0 + a.split_len);
     for (int64_t cs = s0; cs < s1; cs += ACH) {
@@ -581,7 +608,10 @@ __global__ void __launch_bounds__(NT, 2) adjoint_kernel(const AdjArgs a) {
         sw[i] = a.w[cs + i];
         sv[i] = a.v[cs + i];
         if (MIXED) {
-          fmu[i] = (float)(sl[i] - c);
+          const double so = sl[i] - c;
+          const float h = (float)so;
+          fmu[i] = h;
+          fml[i] = (float)(so - (double)h);
           fw[i] = (float)sw[i];
           fv[i] = (float)sv[i];
         }
@@ -604,12 +634,12 @@ __global__ void __launch_bounds__(NT, 2) adjoint_kernel(const AdjArgs a) {
               for (int q = 0; q < 4; ++q) pp[r][q] = 0.0f;
 #pragma unroll 4
             for (int jj = j; jj < j + FOLD; ++jj) {
-              const float mu = fmu[jj], wj = fw[jj], vj = fv[jj];
+              const float mh = fmu[jj], ml = fml[jj], wj = fw[jj], vj = fv[jj];
 #pragma unroll
               for (int r = 0; r < R; ++r) {
-                const float d = (xh[r] - mu) + xl[r];
+                const float d = sep32(xh[r], xl[r], mh, ml);
                 const float d2 = d * d;
-                const float inv = rcp_f32(d2 + eta2f);
+                const float inv = rcp32_unbiased(d2 + eta2f);
                 const float i2 = inv * inv;
                 const float A = (d2 - eta2f) * i2;
                 const float B = tetaf * d * i2;
@@ -696,6 +726,22 @@ SplitPlan plan_splits(int64_t nt, int64_t ns, int chunk) {
 
 double mixed_near_k() { return g_near_k; }
 
+// Block bounds of the sources and, after them, the global (min, max).
+static shrk_status source_bounds(const double* d_src, int64_t ns, int64_t nblocks,
+                                 double2* bounds, cudaStream_t s) {
+  {
+    LaunchScope ls("block_bounds", s);
+    block_bounds_kernel<<<(unsigned)((nblocks + 7) / 8), 256, 0, s>>>(d_src, ns, bounds, nblocks);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  {
+    LaunchScope ls("block_bounds", s);
+    minmax_kernel<<<1, 1024, 0, s>>>(bounds, nblocks);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  return SHRK_OK;
+}
+
 shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src, int64_t ns,
                             double eta, int precision, const Epilogue& epi, cudaStream_t s) {
   if (nt <= 0) return SHRK_OK;
@@ -711,11 +757,9 @@ shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src
   const int64_t nblocks = (ns + SUB - 1) / SUB;
   if (mixed) {
     void* b = nullptr;
-    SHRK_TRY(scratch_get(1, sizeof(double2) * (size_t)nblocks, &b));
+    SHRK_TRY(scratch_get(1, sizeof(double2) * (size_t)(nblocks + 1), &b));
     bounds = (double2*)b;
-    LaunchScope ls("block_bounds", s);
-    block_bounds_kernel<<<(unsigned)((nblocks + 7) / 8), 256, 0, s>>>(d_src, ns, bounds, nblocks);
-    SHRK_CUDA(cudaGetLastError());
+    SHRK_TRY(source_bounds(d_src, ns, nblocks, bounds, s));
   }
   PairArgs a;
   a.tgt = d_tgt;
@@ -723,6 +767,7 @@ shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src
   a.src = d_src;
   a.ns = ns;
   a.bounds = bounds;
+  a.gminmax = bounds ? bounds + nblocks : nullptr;
   a.eta = eta;
   a.near_dist = std::max(g_near_k * eta, 1e-9);
   a.n_tiles = pl.n_tiles;
@@ -790,14 +835,12 @@ shrk_status adjoint(const double* d_ev, int64_t p, double eta, const double* d_g
   void* part = nullptr;
   SHRK_TRY(scratch_get(2, sizeof(double) * 4 * (size_t)pl.n_splits * (size_t)p, &part));
   double2* bounds = nullptr;
+  const int64_t nblocks = (p + SUB - 1) / SUB;
   if (mixed) {
-    const int64_t nblocks = (p + SUB - 1) / SUB;
     void* b = nullptr;
-    SHRK_TRY(scratch_get(1, sizeof(double2) * (size_t)nblocks, &b));
+    SHRK_TRY(scratch_get(1, sizeof(double2) * (size_t)(nblocks + 1), &b));
     bounds = (double2*)b;
-    LaunchScope ls("block_bounds", s);
-    block_bounds_kernel<<<(unsigned)((nblocks + 7) / 8), 256, 0, s>>>(d_ev, p, bounds, nblocks);
-    SHRK_CUDA(cudaGetLastError());
+    SHRK_TRY(source_bounds(d_ev, p, nblocks, bounds, s));
   }
   AdjArgs a;
   a.ev = d_ev;
@@ -805,6 +848,7 @@ shrk_status adjoint(const double* d_ev, int64_t p, double eta, const double* d_g
   a.v = d_gim;
   a.p = p;
   a.bounds = bounds;
+  a.gminmax = bounds ? bounds + nblocks : nullptr;
   a.eta = eta;
   a.near_dist = std::max(g_near_k * eta, 1e-9);
   a.n_tiles = pl.n_tiles;

@@ -60,20 +60,22 @@ shrk_status batched(const double* d_ev, const int64_t* d_offsets, const int64_t*
 shrk_status apply_epilogue(const double* d_tgt, const double* d_raw_re, const double* d_raw_im,
                            int64_t n, const Epilogue& epi, cudaStream_t s);
 
-// Coarse-grid NUFFT: raw sums at nq points.  lo_raw/hi_raw are the first and
-// last source values (the reference's sortedness contract).
-shrk_status nufft_points(const double* d_q, int64_t nq, const double* d_src, int64_t ns,
-                         double lo_raw, double hi_raw, double eta, double* d_re, double* d_im,
+// Coarse-grid NUFFT at nq points, epilogue fused into the interpolation.
+// d_sorted_src holds the sources in ascending order; lo_raw/hi_raw are the
+// first and last source values IN THE CALLER'S ORDER (the reference takes
+// the grid bounds from the first and last entries, nufft.rs:139-146).
+shrk_status nufft_points(const double* d_q, int64_t nq, const double* d_sorted_src, int64_t ns,
+                         double lo_raw, double hi_raw, double eta, const Epilogue& epi,
                          cudaStream_t s);
 size_t nufft_grid_size(double raw_range, double eta);
 
-// Chebyshev treecode (raw sums at nq points).
+// Chebyshev treecode at nq points, epilogue fused into the evaluation.
 struct ChebParams { double theta; int n; int leaf_cap; bool f32; };
 bool cheb_preset(int method, ChebParams* out);
 size_t grid_leaf_cap(size_t n, size_t p, size_t nq, size_t preset_leaf);
 shrk_status chebcode_points(const double* d_q, int64_t nq, const double* h_sorted_src,
                             const double* d_sorted_src, int64_t ns, double eta,
-                            const ChebParams& prm, double* d_re, double* d_im, cudaStream_t s);
+                            const ChebParams& prm, const Epilogue& epi, cudaStream_t s);
 
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);

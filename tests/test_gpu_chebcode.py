@@ -1,0 +1,100 @@
+"""ChebCode treecode on the GPU vs the oracle (bit for bit) and vs the exact
+sums (the presets' documented error classes, chebcode.rs:1401-1441,
+mod.rs:1198-1254)."""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from shrinkers_b200 import _native, spectra
+
+pytestmark = pytest.mark.gpu
+NAN = float("nan")
+_D = C.POINTER(C.c_double)
+PRESET_IDS = {"chebcode": 13, "chebcode_fast": 14, "chebcode_xtreme": 15, "chebcode_balanced": 16}
+
+
+def dp(a):
+    return a.ctypes.data_as(_D)
+
+
+def gpu_all(ev, eta, method):
+    L = _native.load()
+    ev = np.ascontiguousarray(ev, dtype=np.float64)
+    re, im = np.empty(ev.size), np.empty(ev.size)
+    _native.check(L.shrk_stieltjes_all(dp(ev), ev.size, eta, PRESET_IDS[method], 0, NAN, 0,
+                                       dp(re), dp(im)))
+    return re, im
+
+
+def gpu_points(q, ev, eta, method):
+    L = _native.load()
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    ev = np.ascontiguousarray(ev, dtype=np.float64)
+    re, im = np.empty(q.size), np.empty(q.size)
+    _native.check(L.shrk_stieltjes_at_points(dp(q), q.size, dp(ev), ev.size, eta,
+                                             PRESET_IDS[method], 0, NAN, 0, dp(re), dp(im)))
+    return re, im
+
+
+@pytest.mark.parametrize("method", list(PRESET_IDS))
+@pytest.mark.parametrize("p", [1, 2, 31, 33, 1000, 20011])
+def test_treecode_bit_exact_vs_oracle(oracle, method, p):
+    ev = spectra.config2(p, seed=p) if p > 2 else np.array([0.7, 1.3][:p])
+    eta = 1.0 / math.sqrt(p)
+    re, im = gpu_all(ev, eta, method)
+    o_re, o_im = oracle.compute_all(ev, eta, method, parallel=True)
+    np.testing.assert_array_equal(re, o_re)
+    np.testing.assert_array_equal(im, o_im)
+
+
+@pytest.mark.parametrize("method", ["chebcode", "chebcode_fast"])
+def test_treecode_unsorted_bit_exact(oracle, method):
+    p = 4096
+    ev = spectra.config3(p)
+    perm = np.random.default_rng(9).permutation(p)
+    eta = 1.0 / math.sqrt(p)
+    re, im = gpu_all(ev[perm], eta, method)
+    o_re, o_im = oracle.compute_all(ev[perm], eta, method, parallel=True)
+    np.testing.assert_array_equal(re, o_re)
+    np.testing.assert_array_equal(im, o_im)
+
+
+@pytest.mark.parametrize("method", list(PRESET_IDS))
+def test_treecode_grid_path_bit_exact(oracle, method):
+    """At-points path (deconvolution grid): raw sums, leaf cap relaxed by
+    grid_leaf_cap (mod.rs:361-370, 475-489)."""
+    p = 30000
+    ev = spectra.config2(p)
+    eta = 0.1 / math.sqrt(p)
+    q = np.linspace(ev[0] - 0.05, ev[-1] + 0.05, 200)
+    re, im = gpu_points(q, ev, eta, method)
+    o_re, o_im = oracle.compute_at_points(q, ev, eta, method)
+    np.testing.assert_array_equal(re, o_re)
+    np.testing.assert_array_equal(im, o_im)
+
+
+@pytest.mark.parametrize("p", [512, 2000, 8000])
+def test_default_preset_accuracy(oracle, p):
+    """chebcode.rs:1401-1419: DEFAULT preset max relative error < 1e-2."""
+    ev = spectra.log_spectrum(p)
+    eta = 0.1 / math.sqrt(p)
+    ex_re, ex_im = oracle.compute_all(ev, eta, "blocked", parallel=True)
+    re, im = gpu_all(ev, eta, "chebcode")
+    scale = np.maximum(np.abs(ex_re) + np.abs(ex_im), 1e-12)
+    assert np.max((np.abs(re - ex_re) + np.abs(im - ex_im)) / scale) < 1e-2
+
+
+def test_preset_error_classes_full_size(oracle):
+    """p = 1e6 MP + 20 spikes: each preset's error vs the double-double truth
+    on a target sample stays in its documented class."""
+    p = 1_000_000
+    ev = spectra.config3(p)
+    eta = 1.0 / math.sqrt(p)
+    idx = np.random.default_rng(2).choice(p, 24, replace=False)
+    t_re, t_im = oracle.truth_points(ev[idx], ev, eta)
+    for method, tol in [("chebcode_fast", 2e-4), ("chebcode", 1e-7)]:
+        re, im = gpu_all(ev, eta, method)
+        err = np.hypot(re[idx] * p - t_re, im[idx] * p - t_im) / np.hypot(t_re, t_im)
+        assert np.median(err) < tol, (method, np.median(err))
