@@ -1,0 +1,454 @@
+// Exact O(nt*ns) Stieltjes pair sums on sm_100a (forward transform).
+//
+// Replaces the exact family of the shrinkers crate: symmetric_sweep
+// (src/stieltjes/cacheblock.rs:841-954), the tiled full-square kernels
+// (cacheblock.rs:1286-1513) and the at-points kernel (cacheblock.rs:167-437).
+// The pair term is term.rs:26-31:
+//     1/((x - s) - i eta) = (d + i eta)/(d^2 + eta^2),  d = x - s.
+//
+// Work decomposition: a CTA of 256 threads owns a tile of 256*R targets (R
+// per thread, 32*R consecutive targets per warp) and one split of the
+// sources.  Source chunks of 1024 doubles are staged into shared memory by
+// TMA bulk copies (cp.async.bulk + mbarrier, double-buffered) and read by all
+// threads as broadcasts.  Each (tile, split) item writes partial sums to a
+// scratch slab; a second kernel reduces the splits in a fixed order in FP64
+// (deterministic) and applies the fused epilogue.
+//
+// F64 (R = 4): every pair in FP64, reciprocal = hardware seed + one
+// third-order Newton step.
+//
+// MIXED (R = 4): a source block of 256 whose interval lies at least
+// max(K*eta, W) from the warp's targets (W = spread of the CTA's targets
+// around their centre) is summed in FP32 with the packed f32x2 pipe -- two
+// targets per instruction, separation scheme of pairs.cuh, unbiased
+// reciprocal, two interleaved FP32 chains per target folded into FP64
+// every 16 sources.  Every other pair (the near field, where d cancels) is
+// summed in FP64, as are all reductions.
+#include "common.cuh"
+#include "epilogue.cuh"
+#include "internal.h"
+#include "pairs.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace shrk {
+
+namespace {
+
+#ifndef SHRK_R_MIXED
+#define SHRK_R_MIXED 4
+#endif
+#ifndef SHRK_CHAINS
+#define SHRK_CHAINS 2
+#endif
+#ifndef SHRK_MIXED_CTAS
+#define SHRK_MIXED_CTAS 2
+#endif
+
+constexpr int NT = 256;   // threads per CTA
+constexpr int CH = 1024;  // sources per staged chunk
+constexpr int FOLD = 16;  // sources per FP32 partial before the FP64 fold
+constexpr int R_F64 = 4;
+constexpr int R_MIXED = SHRK_R_MIXED;
+constexpr int CHAINS = SHRK_CHAINS;  // interleaved FP32 chains per target
+
+double g_near_k = SHRK_NEAR_K;
+
+struct PairArgs {
+  const double* tgt;
+  int64_t nt;
+  const double* src;
+  int64_t ns;
+  const double2* bounds;   // per SUB block of sources: (min, max)
+  const double2* gminmax;  // (min, max) over all sources
+  double eta;
+  double near_dist;
+  int64_t n_tiles;
+  int n_splits;
+  int64_t split_len;       // multiple of CH
+  double* part_re;         // [n_splits][nt]
+  double* part_im;
+  int* err;
+  int use_tma;
+};
+
+template <bool MIXED, int R>
+__global__ void __launch_bounds__(NT, MIXED ? SHRK_MIXED_CTAS : 2) pair_sum_kernel(const PairArgs a) {
+  constexpr int TT = NT * R, WT = 32 * R, R2 = R / 2;
+  __shared__ __align__(16) double sbuf[2][CH];
+  __shared__ __align__(16) float4 sm4[MIXED ? CH : 1];  // {mh, mh, ml, ml} per source
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ double red[NT / 32];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t phase = 0u;    // bit b: expected parity of bar[b]
+  uint32_t pending = 0u;  // bit b: thread 0 has a copy in flight into sbuf[b]
+
+  const double eta = a.eta, eta2 = eta * eta;
+  const float eta2f = (float)eta2;
+  const u64 ETA2 = pk2(eta2f, eta2f), ONE = pk2(1.0f, 1.0f);
+  const int64_t n_items = a.n_tiles * (int64_t)a.n_splits;
+
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int64_t tile = item / a.n_splits;
+    const int split = (int)(item % a.n_splits);
+    const int64_t tile0 = tile * TT;
+    const int64_t wbase = tile0 + (int64_t)warp * WT;
+    const double x0 = a.tgt[tile0];
+    double x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t idx = wbase + r * 32 + lane;
+      x[r] = idx < a.nt ? a.tgt[idx] : x0;
+    }
+    const int64_t s0 = (int64_t)split * a.split_len;
+    const int64_t s1 = min(a.ns, s0 + a.split_len);
+    const int nchunks = (int)((s1 - s0 + CH - 1) / CH);
+
+    double re64[R], iv64[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) re64[r] = iv64[r] = 0.0;
+    u64 XH[MIXED ? R2 : 1], XL[MIXED ? R2 : 1];
+    const double c = x0;
+    double wlo = 0.0, whi = 0.0, thr = INFINITY;
+    if (MIXED) {
+      double spread = 0.0, mn = x[0], mx = x[0];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        spread = fmax(spread, fabs(x[r] - c));
+        mn = fmin(mn, x[r]);
+        mx = fmax(mx, x[r]);
+      }
+      wlo = warp_min(mn);
+      whi = warp_max(mx);
+      spread = warp_max(spread);
+      if (lane == 0) red[warp] = spread;
+      __syncthreads();
+      double w = 0.0;
+#pragma unroll
+      for (int i = 0; i < NT / 32; ++i) w = fmax(w, red[i]);
+      const double2 g = *a.gminmax;
+      const double u = snap_unit(fmax(fmax(g.y - c, c - g.x), w));
+      // The far path needs the targets' snapped offsets to stay exact floats.
+      thr = (w < 0x1p22 * u) ? fmax(a.near_dist, w) : INFINITY;
+#pragma unroll
+      for (int k = 0; k < R2; ++k) {
+        float h0, l0, h1, l1;
+        split_target(x[2 * k], c, u, h0, l0);
+        split_target(x[2 * k + 1], c, u, h1, l1);
+        XH[k] = pk2(h0, h1);
+        XL[k] = pk2(l0, l1);
+      }
+    }
+
+    auto chunk_is_tma = [&](int k) -> bool {
+      const int64_t cs = s0 + (int64_t)k * CH;
+      return a.use_tma && k < nchunks && (s1 - cs) >= CH;
+    };
+    if (tid == 0) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        if (chunk_is_tma(k)) {
+          mbar_arrive_expect_tx(&bar[k], CH * 8);
+          bulk_g2s(sbuf[k], a.src + s0 + (int64_t)k * CH, CH * 8, &bar[k]);
+          pending |= 1u << k;
+        }
+      }
+    }
+
+    for (int k = 0; k < nchunks; ++k) {
+      const int b = k & 1;
+      const int64_t cs = s0 + (int64_t)k * CH;
+      const int len = (int)min((int64_t)CH, s1 - cs);
+      bool ok = true;
+      if (chunk_is_tma(k)) {
+        ok = mbar_wait(&bar[b], (phase >> b) & 1u);
+        phase ^= 1u << b;
+        pending &= ~(1u << b);
+      } else {
+        for (int i = tid; i < len; i += NT) sbuf[b][i] = a.src[cs + i];
+      }
+      if (!__syncthreads_and(ok)) {
+        // A bulk copy never completed: record it, drain what thread 0 still
+        // has in flight (bounded), and leave the kernel uniformly.
+        if (tid == 0) {
+          atomicExch(a.err, DEV_ERR_TIMEOUT);
+          for (int q = 0; q < 2; ++q)
+            if ((pending >> q) & 1u) mbar_wait(&bar[q], (phase >> q) & 1u, 200000000LL);
+        }
+        return;
+      }
+      if (MIXED) {
+        for (int i = tid; i < len; i += NT) {
+          float mh, ml;
+          split_source(sbuf[b][i], c, mh, ml);
+          sm4[i] = make_float4(mh, mh, ml, ml);
+        }
+        __syncthreads();
+      }
+
+      for (int sub = 0; sub < len; sub += SUB) {
+        const int slen = min(SUB, len - sub);
+        bool far32 = false;
+        if (MIXED && slen == SUB) {
+          const double2 bd = a.bounds[(cs + sub) / SUB];
+          const double gap = fmax(fmax(bd.x - whi, wlo - bd.y), 0.0);
+          const double span = fmax(bd.y - wlo, whi - bd.x);
+          far32 = gap >= thr && span <= 1e9;
+        }
+        if (MIXED && far32) {
+          const float4* sp = &sm4[sub];
+          const u64 ETA2_ = ETA2, ONE_ = ONE;
+          for (int j = 0; j < SUB; j += FOLD) {
+            // two interleaved chains (even / odd sources) halve the FP32
+            // partials' accumulation error
+            u64 RE[CHAINS][R2], IV[CHAINS][R2];
+#pragma unroll
+            for (int ch = 0; ch < CHAINS; ++ch)
+#pragma unroll
+              for (int kk = 0; kk < R2; ++kk) RE[ch][kk] = IV[ch][kk] = 0ull;
+#pragma unroll
+            for (int q = 0; q < FOLD; ++q) {
+              const float4 s4 = sp[j + q];
+              const u64 MH = pk2(s4.x, s4.y), ML = pk2(s4.z, s4.w);
+#pragma unroll
+              for (int kk = 0; kk < R2; ++kk)
+                pair32x2(MH, ML, XH[kk], XL[kk], ETA2_, ONE_, RE[q % CHAINS][kk],
+                         IV[q % CHAINS][kk]);
+            }
+#pragma unroll
+            for (int kk = 0; kk < R2; ++kk) {
+              float r0, r1, v0, v1;
+              u64 sr = RE[0][kk], sv = IV[0][kk];
+#pragma unroll
+              for (int ch = 1; ch < CHAINS; ++ch) {
+                sr = fadd2(sr, RE[ch][kk]);
+                sv = fadd2(sv, IV[ch][kk]);
+              }
+              upk2(sr, r0, r1);
+              upk2(sv, v0, v1);
+              re64[2 * kk] += (double)r0;
+              re64[2 * kk + 1] += (double)r1;
+              iv64[2 * kk] -= (double)v0;
+              iv64[2 * kk + 1] -= (double)v1;
+            }
+          }
+        } else {
+          const double* sp = &sbuf[b][sub];
+          int j = 0;
+#pragma unroll 2
+          for (; j + 2 <= slen; j += 2) {
+            const double2 l2 = *reinterpret_cast<const double2*>(sp + j);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              pair64(x[r], l2.x, eta2, re64[r], iv64[r]);
+              pair64(x[r], l2.y, eta2, re64[r], iv64[r]);
+            }
+          }
+          if (j < slen) {
+            const double l = sp[j];
+#pragma unroll
+            for (int r = 0; r < R; ++r) pair64(x[r], l, eta2, re64[r], iv64[r]);
+          }
+        }
+      }
+      __syncthreads();
+      if (tid == 0 && chunk_is_tma(k + 2)) {
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&bar[b], CH * 8);
+        bulk_g2s(sbuf[b], a.src + s0 + (int64_t)(k + 2) * CH, CH * 8, &bar[b]);
+        pending |= 1u << b;
+      }
+    }
+
+    double* pre = a.part_re + (int64_t)split * a.nt;
+    double* pim = a.part_im + (int64_t)split * a.nt;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t idx = wbase + r * 32 + lane;
+      if (idx < a.nt) {
+        pre[idx] = re64[r];
+        pim[idx] = eta * iv64[r];
+      }
+    }
+  }
+}
+
+__global__ void block_bounds_kernel(const double* __restrict__ src, int64_t ns,
+                                    double2* __restrict__ out, int64_t nblocks) {
+  const int64_t blk = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (blk >= nblocks) return;
+  const int64_t b0 = blk * SUB, b1 = min(ns, b0 + SUB);
+  double mn = INFINITY, mx = -INFINITY;
+  for (int64_t i = b0 + lane; i < b1; i += 32) {
+    const double v = src[i];
+    mn = fmin(mn, v);
+    mx = fmax(mx, v);
+  }
+  mn = warp_min(mn);
+  mx = warp_max(mx);
+  if (lane == 0) out[blk] = make_double2(mn, mx);
+}
+
+__global__ void __launch_bounds__(1024) minmax_kernel(double2* __restrict__ bounds,
+                                                      int64_t nblocks) {
+  __shared__ double smin[32], smax[32];
+  double mn = INFINITY, mx = -INFINITY;
+  for (int64_t i = threadIdx.x; i < nblocks; i += blockDim.x) {
+    mn = fmin(mn, bounds[i].x);
+    mx = fmax(mx, bounds[i].y);
+  }
+  mn = warp_min(mn);
+  mx = warp_max(mx);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    smin[w] = mn;
+    smax[w] = mx;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    mn = lane < nw ? smin[lane] : INFINITY;
+    mx = lane < nw ? smax[lane] : -INFINITY;
+    mn = warp_min(mn);
+    mx = warp_max(mx);
+    if (lane == 0) bounds[nblocks] = make_double2(mn, mx);
+  }
+}
+
+struct ReduceArgs {
+  const double* part_re;
+  const double* part_im;
+  int n_splits;
+  int64_t nt;
+  const double* tgt;
+  Epilogue epi;
+};
+
+// Fixed-order FP64 reduction of the split partials + fused epilogue.
+__global__ void reduce_kernel(const ReduceArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.nt) return;
+  double re = 0.0, im = 0.0;
+  for (int s = 0; s < a.n_splits; ++s) {
+    re += a.part_re[(int64_t)s * a.nt + t];
+    im += a.part_im[(int64_t)s * a.nt + t];
+  }
+  epi_store(a.epi, t, a.tgt[t], re, im);
+}
+
+}  // namespace
+
+double mixed_near_k() { return g_near_k; }
+
+SplitPlan plan_splits(int64_t nt, int64_t ns, int tile, int chunk, int ctas_per_sm) {
+  SplitPlan pl;
+  pl.n_tiles = (nt + tile - 1) / tile;
+  const int ctas = std::max(1, sm_count() * ctas_per_sm);
+  const int64_t max_splits = std::max<int64_t>(1, (ns + chunk - 1) / chunk);
+  int64_t want = (8LL * ctas + pl.n_tiles - 1) / pl.n_tiles;
+  want = std::min(std::max<int64_t>(want, 1), max_splits);
+  const int64_t per = (ns + want - 1) / want;
+  pl.split_len = ((per + chunk - 1) / chunk) * chunk;
+  pl.n_splits = (int)((ns + pl.split_len - 1) / pl.split_len);
+  pl.grid = (int)std::min<int64_t>(pl.n_tiles * pl.n_splits, ctas);
+  return pl;
+}
+
+shrk_status source_bounds(const double* d_src, int64_t ns, int64_t nblocks, double2* bounds,
+                          cudaStream_t s) {
+  {
+    LaunchScope ls("block_bounds", s);
+    block_bounds_kernel<<<(unsigned)((nblocks + 7) / 8), 256, 0, s>>>(d_src, ns, bounds, nblocks);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  {
+    LaunchScope ls("block_bounds", s);
+    minmax_kernel<<<1, 1024, 0, s>>>(bounds, nblocks);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  return SHRK_OK;
+}
+
+shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src, int64_t ns,
+                            double eta, int precision, const Epilogue& epi, cudaStream_t s) {
+  if (nt <= 0) return SHRK_OK;
+  if (ns <= 0) {
+    set_error("exact_pair_sums: empty source set");
+    return SHRK_EINVAL;
+  }
+  const bool mixed = (precision == SHRK_PREC_MIXED);
+  const int R = mixed ? R_MIXED : R_F64;
+  const SplitPlan pl = plan_splits(nt, ns, NT * R, CH, mixed ? SHRK_MIXED_CTAS : 2);
+  void* part = nullptr;
+  SHRK_TRY(scratch_get(0, sizeof(double) * 2 * (size_t)pl.n_splits * (size_t)nt, &part));
+  double2* bounds = nullptr;
+  const int64_t nblocks = (ns + SUB - 1) / SUB;
+  if (mixed) {
+    void* b = nullptr;
+    SHRK_TRY(scratch_get(1, sizeof(double2) * (size_t)(nblocks + 1), &b));
+    bounds = (double2*)b;
+    SHRK_TRY(source_bounds(d_src, ns, nblocks, bounds, s));
+  }
+  PairArgs a;
+  a.tgt = d_tgt;
+  a.nt = nt;
+  a.src = d_src;
+  a.ns = ns;
+  a.bounds = bounds;
+  a.gminmax = bounds ? bounds + nblocks : nullptr;
+  a.eta = eta;
+  a.near_dist = std::max(g_near_k * eta, 1e-9);
+  a.n_tiles = pl.n_tiles;
+  a.n_splits = pl.n_splits;
+  a.split_len = pl.split_len;
+  a.part_re = (double*)part;
+  a.part_im = (double*)part + (size_t)pl.n_splits * nt;
+  a.err = device_error_word();
+  a.use_tma = ((uintptr_t)d_src % 16 == 0) ? 1 : 0;
+  {
+    LaunchScope ls(mixed ? "pair_sum_mixed" : "pair_sum_f64", s);
+    if (mixed) pair_sum_kernel<true, R_MIXED><<<pl.grid, NT, 0, s>>>(a);
+    else pair_sum_kernel<false, R_F64><<<pl.grid, NT, 0, s>>>(a);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  ReduceArgs ra;
+  ra.part_re = a.part_re;
+  ra.part_im = a.part_im;
+  ra.n_splits = pl.n_splits;
+  ra.nt = nt;
+  ra.tgt = d_tgt;
+  ra.epi = epi;
+  {
+    LaunchScope ls("split_reduce", s);
+    reduce_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(ra);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  return SHRK_OK;
+}
+
+shrk_status apply_epilogue(const double* d_tgt, const double* d_raw_re, const double* d_raw_im,
+                           int64_t n, const Epilogue& epi, cudaStream_t s) {
+  if (n <= 0) return SHRK_OK;
+  ReduceArgs ra;
+  ra.part_re = d_raw_re;
+  ra.part_im = d_raw_im;
+  ra.n_splits = 1;
+  ra.nt = n;
+  ra.tgt = d_tgt;
+  ra.epi = epi;
+  LaunchScope ls("epilogue", s);
+  reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ra);
+  SHRK_CUDA(cudaGetLastError());
+  return SHRK_OK;
+}
+
+}  // namespace shrk
