@@ -106,22 +106,45 @@ __device__ __forceinline__ u64 fsub2(u64 a, u64 b) {
   return d;
 }
 
-// Two FP32 far-field pairs (two targets, one source) in packed form.  All
-// quantities are carried negated so no negation is needed on the packed
-// pipe: ND = s - x, NR = -1/(d^2+eta^2) refined by one Newton step.
-//   re += d * r   ==  RE += ND * NR
-//   iv += r       ==  IVN += NR          (IVN accumulates -iv)
-__device__ __forceinline__ void pair32x2(u64 MH, u64 ML, u64 XH, u64 XL, u64 ETA2, u64 ONE,
-                                         u64& RE, u64& IVN) {
-  const u64 ND = fadd2(fsub2(MH, XH), fsub2(ML, XL));
-  const u64 DEN = ffma2(ND, ND, ETA2);
+__device__ __forceinline__ u64 fmul2(u64 a, u64 b) {
+  u64 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// Four FP32 far-field pairs: two targets (the packed lanes) x two sources
+// s1, s2 of one 256-source block with centre cb.
+//   TH + TL = x - cb   (TH = float(x - cb), TL = the rounding remainder)
+//   SM      = float(s1 - cb),  DL = float(s1 - s2)
+//   d1 = TH - (SM - TL) = x - s1,   d2 = d1 + DL = x - s2
+// The remainder TL keeps the block-wide target offset exact.  It must enter
+// through SM, whose ulp is far finer than TH's: (TH - SM) + TL would round
+// TL away (TH - SM already sits on TH's ulp grid) and leave a coherent
+// offset of up to half an ulp on every pair of the block.  In this order the
+// one rounding at ulp(d) depends on each source's low bits, so the
+// separation errors of different pairs are independent.
+// One reciprocal serves both sources:
+//   e_k = d_k^2 + eta^2,  r = 1/(e1 e2) (MUFU seed + one Newton step, which
+//   removes the seed's nonzero mean error),
+//   d1/e1 + d2/e2 = (d1 e2 + d2 e1) r,   1/e1 + 1/e2 = (e1 + e2) r.
+// r is carried negated (NR = -r) so the packed pipe needs no negation:
+// RE and IVN accumulate -sum d/e and -sum 1/e.  The caller keeps e1 e2
+// inside the FP32 normal range (block span <= 1e9, gap >= 1e-9).
+__device__ __forceinline__ void pairs32x4(u64 SM, u64 DL, u64 TH, u64 TL, u64 ETA2, u64 ONE,
+                                          u64& RE, u64& IVN) {
+  const u64 D1 = fsub2(TH, fsub2(SM, TL));
+  const u64 D2 = fadd2(D1, DL);
+  const u64 E1 = ffma2(D1, D1, ETA2);
+  const u64 E2 = ffma2(D2, D2, ETA2);
+  const u64 P = fmul2(E1, E2);
   float a0, a1;
-  upk2(DEN, a0, a1);
+  upk2(P, a0, a1);
   const u64 NR0 = pk2(rcp_f32(-a0), rcp_f32(-a1));
-  const u64 E = ffma2(DEN, NR0, ONE);  // 1 - den * r
-  const u64 NR = ffma2(NR0, E, NR0);   // -(r + r e)
-  RE = ffma2(ND, NR, RE);
-  IVN = fadd2(IVN, NR);
+  const u64 E = ffma2(P, NR0, ONE);   // 1 - P r
+  const u64 NR = ffma2(NR0, E, NR0);  // -(r + r e)
+  const u64 NUM = ffma2(D1, E2, fmul2(D2, E1));
+  RE = ffma2(NUM, NR, RE);
+  IVN = ffma2(fadd2(E1, E2), NR, IVN);
 }
 
 // Host: (min, max) of every SUB-block of d_src into bounds[0..nblocks) and the

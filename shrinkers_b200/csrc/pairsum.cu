@@ -18,12 +18,11 @@
 // third-order Newton step.
 //
 // MIXED (R = 4): a source block of 256 whose interval lies at least
-// max(K*eta, W) from the warp's targets (W = spread of the CTA's targets
-// around their centre) is summed in FP32 with the packed f32x2 pipe -- two
-// targets per instruction, separation scheme of pairs.cuh, unbiased
-// reciprocal, two interleaved FP32 chains per target folded into FP64
-// every 16 sources.  Every other pair (the near field, where d cancels) is
-// summed in FP64, as are all reductions.
+// max(K*eta, 1e-9) from all of the warp's targets is summed in FP32 on the
+// packed f32x2 pipe -- two targets x two sources per step, one unbiased
+// reciprocal per two sources (pairs32x4 in pairs.cuh), FP32 partials folded
+// into FP64 every 16 sources.  Every other pair (the near field, where the
+// terms are large and d cancels) is summed in FP64, as are all reductions.
 #include "common.cuh"
 #include "epilogue.cuh"
 #include "internal.h"
@@ -39,9 +38,6 @@ namespace {
 #ifndef SHRK_R_MIXED
 #define SHRK_R_MIXED 4
 #endif
-#ifndef SHRK_CHAINS
-#define SHRK_CHAINS 2
-#endif
 #ifndef SHRK_MIXED_CTAS
 #define SHRK_MIXED_CTAS 2
 #endif
@@ -51,7 +47,6 @@ constexpr int CH = 1024;  // sources per staged chunk
 constexpr int FOLD = 16;  // sources per FP32 partial before the FP64 fold
 constexpr int R_F64 = 4;
 constexpr int R_MIXED = SHRK_R_MIXED;
-constexpr int CHAINS = SHRK_CHAINS;  // interleaved FP32 chains per target
 
 double g_near_k = SHRK_NEAR_K;
 
@@ -61,7 +56,6 @@ struct PairArgs {
   const double* src;
   int64_t ns;
   const double2* bounds;   // per SUB block of sources: (min, max)
-  const double2* gminmax;  // (min, max) over all sources
   double eta;
   double near_dist;
   int64_t n_tiles;
@@ -77,9 +71,8 @@ template <bool MIXED, int R>
 __global__ void __launch_bounds__(NT, MIXED ? SHRK_MIXED_CTAS : 2) pair_sum_kernel(const PairArgs a) {
   constexpr int TT = NT * R, WT = 32 * R, R2 = R / 2;
   __shared__ __align__(16) double sbuf[2][CH];
-  __shared__ __align__(16) float4 sm4[MIXED ? CH : 1];  // {mh, mh, ml, ml} per source
+  __shared__ __align__(16) float4 sm4[MIXED ? CH / 2 : 1];  // {sm, sm, dl, dl} per source pair
   __shared__ __align__(8) uint64_t bar[2];
-  __shared__ double red[NT / 32];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) {
@@ -115,37 +108,18 @@ __global__ void __launch_bounds__(NT, MIXED ? SHRK_MIXED_CTAS : 2) pair_sum_kern
     double re64[R], iv64[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) re64[r] = iv64[r] = 0.0;
-    u64 XH[MIXED ? R2 : 1], XL[MIXED ? R2 : 1];
-    const double c = x0;
-    double wlo = 0.0, whi = 0.0, thr = INFINITY;
+    // Range of this warp's targets: a source block is summed in FP32 only if
+    // it lies at least near_dist from all of them.
+    double wlo = 0.0, whi = 0.0;
     if (MIXED) {
-      double spread = 0.0, mn = x[0], mx = x[0];
+      double mn = x[0], mx = x[0];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        spread = fmax(spread, fabs(x[r] - c));
         mn = fmin(mn, x[r]);
         mx = fmax(mx, x[r]);
       }
       wlo = warp_min(mn);
       whi = warp_max(mx);
-      spread = warp_max(spread);
-      if (lane == 0) red[warp] = spread;
-      __syncthreads();
-      double w = 0.0;
-#pragma unroll
-      for (int i = 0; i < NT / 32; ++i) w = fmax(w, red[i]);
-      const double2 g = *a.gminmax;
-      const double u = snap_unit(fmax(fmax(g.y - c, c - g.x), w));
-      // The far path needs the targets' snapped offsets to stay exact floats.
-      thr = (w < 0x1p22 * u) ? fmax(a.near_dist, w) : INFINITY;
-#pragma unroll
-      for (int k = 0; k < R2; ++k) {
-        float h0, l0, h1, l1;
-        split_target(x[2 * k], c, u, h0, l0);
-        split_target(x[2 * k + 1], c, u, h1, l1);
-        XH[k] = pk2(h0, h1);
-        XL[k] = pk2(l0, l1);
-      }
     }
 
     auto chunk_is_tma = [&](int k) -> bool {
@@ -186,10 +160,18 @@ __global__ void __launch_bounds__(NT, MIXED ? SHRK_MIXED_CTAS : 2) pair_sum_kern
         return;
       }
       if (MIXED) {
-        for (int i = tid; i < len; i += NT) {
-          float mh, ml;
-          split_source(sbuf[b][i], c, mh, ml);
-          sm4[i] = make_float4(mh, mh, ml, ml);
+        // Source pairs of each full 256-block: (s1, s2) = (src[k], src[k+128])
+        // as {SM, SM, DL, DL} relative to the block's first source.  Pairing
+        // sources half a block apart keeps e1 = d1^2+eta^2 and e2 well apart:
+        // adjacent sorted sources give e1 e2 ~ a square, and the rounded
+        // reciprocal of a near-square carries a small systematic error
+        // (~2e-11 relative, measured) that adds up coherently at large p.
+        for (int i = tid; i < (len / SUB) * (SUB / 2); i += NT) {
+          const int blk = i / (SUB / 2) * SUB, k = i % (SUB / 2);
+          const double cb = sbuf[b][blk];
+          const double s1 = sbuf[b][blk + k], s2 = sbuf[b][blk + k + SUB / 2];
+          const float sm = (float)(s1 - cb), dl = (float)(s1 - s2);
+          sm4[i] = make_float4(sm, sm, dl, dl);
         }
         __syncthreads();
       }
@@ -201,41 +183,41 @@ __global__ void __launch_bounds__(NT, MIXED ? SHRK_MIXED_CTAS : 2) pair_sum_kern
           const double2 bd = a.bounds[(cs + sub) / SUB];
           const double gap = fmax(fmax(bd.x - whi, wlo - bd.y), 0.0);
           const double span = fmax(bd.y - wlo, whi - bd.x);
-          far32 = gap >= thr && span <= 1e9;
+          far32 = gap >= a.near_dist && span <= 1e9;
         }
         if (MIXED && far32) {
-          const float4* sp = &sm4[sub];
+          // Block-wide target offsets x - cb = TH + TL.
+          const double cb = sbuf[b][sub];
+          u64 TH[R2], TL[R2];
+#pragma unroll
+          for (int kk = 0; kk < R2; ++kk) {
+            const double o0 = x[2 * kk] - cb, o1 = x[2 * kk + 1] - cb;
+            const float h0 = (float)o0, h1 = (float)o1;
+            TH[kk] = pk2(h0, h1);
+            TL[kk] = pk2((float)(o0 - (double)h0), (float)(o1 - (double)h1));
+          }
+          const float4* sp = &sm4[sub / 2];
           const u64 ETA2_ = ETA2, ONE_ = ONE;
-          for (int j = 0; j < SUB; j += FOLD) {
-            // two interleaved chains (even / odd sources) halve the FP32
-            // partials' accumulation error
-            u64 RE[CHAINS][R2], IV[CHAINS][R2];
+          for (int j = 0; j < SUB / 2; j += FOLD / 2) {
+            u64 RE[R2], IV[R2];
 #pragma unroll
-            for (int ch = 0; ch < CHAINS; ++ch)
+            for (int kk = 0; kk < R2; ++kk) RE[kk] = IV[kk] = 0ull;
 #pragma unroll
-              for (int kk = 0; kk < R2; ++kk) RE[ch][kk] = IV[ch][kk] = 0ull;
-#pragma unroll
-            for (int q = 0; q < FOLD; ++q) {
+            for (int q = 0; q < FOLD / 2; ++q) {
               const float4 s4 = sp[j + q];
-              const u64 MH = pk2(s4.x, s4.y), ML = pk2(s4.z, s4.w);
+              const u64 SM = pk2(s4.x, s4.y), DL = pk2(s4.z, s4.w);
 #pragma unroll
               for (int kk = 0; kk < R2; ++kk)
-                pair32x2(MH, ML, XH[kk], XL[kk], ETA2_, ONE_, RE[q % CHAINS][kk],
-                         IV[q % CHAINS][kk]);
+                pairs32x4(SM, DL, TH[kk], TL[kk], ETA2_, ONE_, RE[kk], IV[kk]);
             }
+            // FP32 partials of FOLD sources are folded into FP64 (negated).
 #pragma unroll
             for (int kk = 0; kk < R2; ++kk) {
               float r0, r1, v0, v1;
-              u64 sr = RE[0][kk], sv = IV[0][kk];
-#pragma unroll
-              for (int ch = 1; ch < CHAINS; ++ch) {
-                sr = fadd2(sr, RE[ch][kk]);
-                sv = fadd2(sv, IV[ch][kk]);
-              }
-              upk2(sr, r0, r1);
-              upk2(sv, v0, v1);
-              re64[2 * kk] += (double)r0;
-              re64[2 * kk + 1] += (double)r1;
+              upk2(RE[kk], r0, r1);
+              upk2(IV[kk], v0, v1);
+              re64[2 * kk] -= (double)r0;
+              re64[2 * kk + 1] -= (double)r1;
               iv64[2 * kk] -= (double)v0;
               iv64[2 * kk + 1] -= (double)v1;
             }
@@ -404,7 +386,6 @@ shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src
   a.src = d_src;
   a.ns = ns;
   a.bounds = bounds;
-  a.gminmax = bounds ? bounds + nblocks : nullptr;
   a.eta = eta;
   a.near_dist = std::max(g_near_k * eta, 1e-9);
   a.n_tiles = pl.n_tiles;
