@@ -107,6 +107,29 @@ shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const dou
                                          size_t p, double eta, int method, int precision,
                                          double cutoff_ratio, int parallelism, double* d_re,
                                          double* d_im, void* stream);
+/* Allocation-free form of shrk_stieltjes_at_points_dev for the exact method
+ * (no counterpart in the reference): the same RAW sums, FP64 or MIXED, with
+ * every device temporary taken from one static array of
+ * SHRK_NOALLOC_SCRATCH_BYTES inside the library, for callers that cannot let
+ * a library allocate or free device memory (a framework holding the device
+ * in its own pool, latency-bound loops, fixed-footprint services).
+ *   - Limits: nq <= SHRK_NOALLOC_MAX_POINTS, p <= SHRK_NOALLOC_MAX_EIGS;
+ *     larger sizes return SHRK_EINVAL with a message naming the limit.
+ *   - The first call on each device does a one-time setup (it looks up the
+ *     array's device address, which may also load the module onto the
+ *     device); make that first call before any stream capture.
+ *   - Every call on a device shares the array.  Calls that overlap -- on
+ *     different streams, or enqueued concurrently from several host threads
+ *     -- race on it and corrupt each other's results; serialise them (for
+ *     instance one stream, one thread at a time).
+ *   - Stream-ordered, no host synchronisation: if a bounded device-side wait
+ *     gives up, every output of that call is NaN. */
+#define SHRK_NOALLOC_SCRATCH_BYTES (8u << 20)
+#define SHRK_NOALLOC_MAX_POINTS 262144
+#define SHRK_NOALLOC_MAX_EIGS 16777216
+shrk_status shrk_stieltjes_at_points_noalloc(const double* d_q, size_t nq, const double* d_ev,
+                                             size_t p, double eta, int precision, double* d_re,
+                                             double* d_im, void* stream);
 /* autovec.rs:38-77 compute_all_stieltjes_with_deriv (python.rs:758-781):
  * RAW value and derivative w.r.t. the query point at every eigenvalue. */
 shrk_status shrk_stieltjes_with_deriv(const double* ev, size_t p, double eta, double* re,

@@ -38,6 +38,7 @@ SIGNATURES = {
     "shrk_stieltjes_all_f32": (_ST, [_F, _SZ, C.c_float, C.c_int, C.c_double, _F, _F]),
     "shrk_stieltjes_at_points": (_ST, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, _D, _D]),
     "shrk_stieltjes_at_points_dev": (_ST, [_P, _SZ, _P, _SZ, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, _P, _P, _P]),
+    "shrk_stieltjes_at_points_noalloc": (_ST, [_P, _SZ, _P, _SZ, C.c_double, C.c_int, _P, _P, _P]),
     "shrk_stieltjes_with_deriv": (_ST, [_D, _SZ, C.c_double, _D, _D, _D, _D]),
     "shrk_stieltjes_batched": (_ST, [_D, _I64, _SZ, _D, C.c_int, _D, _D]),
     "shrk_stieltjes_batched_dev": (_ST, [_P, _P, _SZ, _P, C.c_int, _P, _P, _P]),

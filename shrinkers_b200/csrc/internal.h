@@ -32,6 +32,16 @@ struct Epilogue {
 shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src, int64_t ns,
                             double eta, int precision, const Epilogue& epi, cudaStream_t s);
 
+// The same raw sums (no epilogue) with every temporary in caller-provided
+// device memory and no library state touched: `part` holds part_capacity
+// (re, im) split partials (>= nt), `bounds` ns/256 + 2 double2 (MIXED only),
+// `err` a device int the caller has zeroed on stream s.  If a bounded wait
+// gives up, every output is NaN.  sms = multiprocessor count of the device.
+shrk_status exact_pair_sums_fixed(const double* d_tgt, int64_t nt, const double* d_src,
+                                  int64_t ns, double eta, int precision, double* d_re,
+                                  double* d_im, double* part, int64_t part_capacity,
+                                  double2* bounds, int* err, int sms, cudaStream_t s);
+
 // Windowed sums: only pairs with |x_t - s_j| <= window are included (sorted
 // sources).  which: bit 0 = real part, bit 1 = imaginary part.
 shrk_status windowed_sums(const double* d_tgt, int64_t nt, const double* d_src, int64_t ns,

@@ -432,4 +432,83 @@ shrk_status apply_epilogue(const double* d_tgt, const double* d_raw_re, const do
   return SHRK_OK;
 }
 
+namespace {
+
+// Split reduction for the caller-scratch launcher: raw sums, or NaN in every
+// output when the pair kernel recorded a failed bounded wait (the caller is
+// not synchronised, so the failure is reported through the values).
+__global__ void reduce_flagged_kernel(const double* part_re, const double* part_im, int n_splits,
+                                      int64_t nt, const int* err, double* out_re,
+                                      double* out_im) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  if (*err != DEV_ERR_NONE) {
+    out_re[t] = NAN;
+    out_im[t] = NAN;
+    return;
+  }
+  double re = 0.0, im = 0.0;
+  for (int s = 0; s < n_splits; ++s) {
+    re += part_re[(int64_t)s * nt + t];
+    im += part_im[(int64_t)s * nt + t];
+  }
+  out_re[t] = re;
+  out_im[t] = im;
+}
+
+}  // namespace
+
+shrk_status exact_pair_sums_fixed(const double* d_tgt, int64_t nt, const double* d_src,
+                                  int64_t ns, double eta, int precision, double* d_re,
+                                  double* d_im, double* part, int64_t part_capacity,
+                                  double2* bounds, int* err, int sms, cudaStream_t s) {
+  if (nt <= 0) return SHRK_OK;
+  if (ns <= 0 || part_capacity < nt) {
+    set_error("exact_pair_sums_fixed: empty source set or scratch smaller than one split");
+    return SHRK_EINVAL;
+  }
+  const bool mixed = (precision == SHRK_PREC_MIXED);
+  const int R = mixed ? R_MIXED : R_F64;
+  const int ctas = std::max(1, sms * (mixed ? SHRK_MIXED_CTAS : 2));
+  const int64_t n_tiles = (nt + NT * R - 1) / (NT * R);
+  // Same split rule as plan_splits, additionally capped by the scratch.
+  const int64_t max_splits =
+      std::max<int64_t>(1, std::min<int64_t>((ns + CH - 1) / CH, part_capacity / nt));
+  int64_t want = (8LL * ctas + n_tiles - 1) / n_tiles;
+  want = std::min(std::max<int64_t>(want, 1), max_splits);
+  const int64_t per = (ns + want - 1) / want;
+  const int64_t split_len = ((per + CH - 1) / CH) * CH;
+  const int n_splits = (int)((ns + split_len - 1) / split_len);
+  const int grid = (int)std::min<int64_t>(n_tiles * n_splits, ctas);
+  const int64_t nblocks = (ns + SUB - 1) / SUB;
+  if (mixed) {
+    block_bounds_kernel<<<(unsigned)((nblocks + 7) / 8), 256, 0, s>>>(d_src, ns, bounds, nblocks);
+    SHRK_CUDA(cudaGetLastError());
+    minmax_kernel<<<1, 1024, 0, s>>>(bounds, nblocks);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  PairArgs a;
+  a.tgt = d_tgt;
+  a.nt = nt;
+  a.src = d_src;
+  a.ns = ns;
+  a.bounds = mixed ? bounds : nullptr;
+  a.eta = eta;
+  a.near_dist = std::max(g_near_k * eta, 1e-9);
+  a.n_tiles = n_tiles;
+  a.n_splits = n_splits;
+  a.split_len = split_len;
+  a.part_re = part;
+  a.part_im = part + (size_t)n_splits * nt;
+  a.err = err;
+  a.use_tma = ((uintptr_t)d_src % 16 == 0) ? 1 : 0;
+  if (mixed) pair_sum_kernel<true, R_MIXED><<<grid, NT, 0, s>>>(a);
+  else pair_sum_kernel<false, R_F64><<<grid, NT, 0, s>>>(a);
+  SHRK_CUDA(cudaGetLastError());
+  reduce_flagged_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(
+      a.part_re, a.part_im, n_splits, nt, err, d_re, d_im);
+  SHRK_CUDA(cudaGetLastError());
+  return SHRK_OK;
+}
+
 }  // namespace shrk
