@@ -146,6 +146,14 @@ shrk_status shrk_stieltjes_batched(const double* ev, const int64_t* offsets, siz
 shrk_status shrk_stieltjes_batched_dev(const double* d_ev, const int64_t* d_offsets,
                                        size_t n_spectra, const double* d_eta, int precision,
                                        double* d_re, double* d_im, void* stream);
+/* Autotuner of the batched launch (no reference counterpart).  For each
+ * p-bucket [2^8,2^9), ..., [2^14,2^15), [2^15,inf) it times every candidate
+ * (targets per thread R in {2,4}, source split SL in {1024,...,8192}) on a
+ * synthetic batch of that bucket and keeps the fastest; table receives
+ * (R, SL) per bucket, 16 ints.  Runs once per device and precision (the
+ * first batched call runs it implicitly), again when force != 0.  Spectra
+ * of the batched entry points hold at most 16 777 216 values each. */
+shrk_status shrk_batched_autotune(int precision, int force, int32_t* table);
 
 /* Adjoint of m(z_j) = (1/p) sum_i 1/(ev_i - z_j), z_j = ev_j + i*eta (the
  * -conj(S)/p convention; no reference counterpart).  Given cotangents

@@ -109,6 +109,8 @@ static bool g_timing = false;
 struct TimedLaunch { std::string family; cudaEvent_t a, b; };
 static std::vector<TimedLaunch> g_timed;
 
+void add_launches(int64_t n) { g_launches.fetch_add(n); }
+
 LaunchScope::LaunchScope(const char* fam, cudaStream_t s) : family(fam), stream(s) {
   g_launches.fetch_add(1);
   if (g_timing) {
@@ -690,6 +692,18 @@ shrk_status shrk_stieltjes_batched(const double* ev, const int64_t* offsets, siz
   SHRK_TRY(d2h(out_re, out, sizeof(double) * total, s));
   SHRK_TRY(d2h(out_im, (double*)out + total, sizeof(double) * total, s));
   return check_device_error(s);
+}
+
+shrk_status shrk_batched_autotune(int precision, int force, int32_t* table) {
+  if (precision != SHRK_PREC_F64 && precision != SHRK_PREC_MIXED)
+    return einval("unknown precision id");
+  Guard g;
+  SHRK_TRY(g.st);
+  int t[16];
+  SHRK_TRY(batched_tune(precision, force != 0, t, g_cur->stream));
+  if (table)
+    for (int i = 0; i < 16; ++i) table[i] = t[i];
+  return check_device_error(g_cur->stream);
 }
 
 shrk_status shrk_stieltjes_adjoint_dev(const double* d_ev, size_t p, double eta,

@@ -48,6 +48,10 @@ struct LaunchScope {
   cudaEvent_t start = nullptr, stop = nullptr;
 };
 
+// Adds kernels launched outside a LaunchScope (inside a CUDA graph) to the
+// library's launch count.
+void add_launches(int64_t n);
+
 // Read back and clear the device error word; maps a set word to a status.
 shrk_status check_device_error(cudaStream_t s);
 

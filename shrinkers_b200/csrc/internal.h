@@ -60,10 +60,15 @@ shrk_status all_f32(const float* d_ev, int64_t p, float eta, float* d_re, float*
 shrk_status adjoint(const double* d_ev, int64_t p, double eta, const double* d_gre,
                     const double* d_gim, int precision, double* d_grad, cudaStream_t s);
 
-// Batched uneven spectra.
+// Batched uneven spectra (batched.cu).  h_offsets may be null (then the
+// offsets and etas are read back from the device to build the plan).
 shrk_status batched(const double* d_ev, const int64_t* d_offsets, const int64_t* h_offsets,
                     int64_t n_spectra, const double* d_eta, int precision, double* d_re,
                     double* d_im, cudaStream_t s);
+// Runs the batched autotuner for `precision` on the current device (if it has
+// not run yet, or if force) and writes (R, SL) for the 8 p-buckets into
+// table[16] (may be null).
+shrk_status batched_tune(int precision, bool force, int* table, cudaStream_t s);
 
 // Epilogue over precomputed raw sums (n targets), same arithmetic as the
 // fused reduction of exact_pair_sums.

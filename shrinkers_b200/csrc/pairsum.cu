@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "epilogue.cuh"
 #include "internal.h"
+#include "pair_item.cuh"
 #include "pairs.cuh"
 
 #include <algorithm>
@@ -42,9 +43,8 @@ namespace {
 #define SHRK_MIXED_CTAS 2
 #endif
 
-constexpr int NT = 256;   // threads per CTA
-constexpr int CH = 1024;  // sources per staged chunk
-constexpr int FOLD = 16;  // sources per FP32 partial before the FP64 fold
+constexpr int NT = PAIR_NT;
+constexpr int CH = PAIR_CH;
 constexpr int R_F64 = 4;
 constexpr int R_MIXED = SHRK_R_MIXED;
 
@@ -69,197 +69,29 @@ struct PairArgs {
 
 template <bool MIXED, int R>
 __global__ void __launch_bounds__(NT, MIXED ? SHRK_MIXED_CTAS : 2) pair_sum_kernel(const PairArgs a) {
-  constexpr int TT = NT * R, WT = 32 * R, R2 = R / 2;
-  __shared__ __align__(16) double sbuf[2][CH];
-  __shared__ __align__(16) float4 sm4[MIXED ? CH / 2 : 1];  // {sm, sm, dl, dl} per source pair
-  __shared__ __align__(8) uint64_t bar[2];
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  uint32_t phase = 0u;    // bit b: expected parity of bar[b]
-  uint32_t pending = 0u;  // bit b: thread 0 has a copy in flight into sbuf[b]
-
-  const double eta = a.eta, eta2 = eta * eta;
-  const float eta2f = (float)eta2;
-  const u64 ETA2 = pk2(eta2f, eta2f), ONE = pk2(1.0f, 1.0f);
+  __shared__ PairStage st;
+  pair_stage_init(st);
+  uint32_t phase = 0u;    // bit b: expected parity of st.bar[b]
+  uint32_t pending = 0u;  // bit b: thread 0 has a copy in flight into st.sbuf[b]
   const int64_t n_items = a.n_tiles * (int64_t)a.n_splits;
-
   for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int64_t tile = item / a.n_splits;
     const int split = (int)(item % a.n_splits);
-    const int64_t tile0 = tile * TT;
-    const int64_t wbase = tile0 + (int64_t)warp * WT;
-    const double x0 = a.tgt[tile0];
-    double x[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int64_t idx = wbase + r * 32 + lane;
-      x[r] = idx < a.nt ? a.tgt[idx] : x0;
-    }
-    const int64_t s0 = (int64_t)split * a.split_len;
-    const int64_t s1 = min(a.ns, s0 + a.split_len);
-    const int nchunks = (int)((s1 - s0 + CH - 1) / CH);
-
-    double re64[R], iv64[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) re64[r] = iv64[r] = 0.0;
-    // Range of this warp's targets: a source block is summed in FP32 only if
-    // it lies at least near_dist from all of them.
-    double wlo = 0.0, whi = 0.0;
-    if (MIXED) {
-      double mn = x[0], mx = x[0];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        mn = fmin(mn, x[r]);
-        mx = fmax(mx, x[r]);
-      }
-      wlo = warp_min(mn);
-      whi = warp_max(mx);
-    }
-
-    auto chunk_is_tma = [&](int k) -> bool {
-      const int64_t cs = s0 + (int64_t)k * CH;
-      return a.use_tma && k < nchunks && (s1 - cs) >= CH;
-    };
-    if (tid == 0) {
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        if (chunk_is_tma(k)) {
-          mbar_arrive_expect_tx(&bar[k], CH * 8);
-          bulk_g2s(sbuf[k], a.src + s0 + (int64_t)k * CH, CH * 8, &bar[k]);
-          pending |= 1u << k;
-        }
-      }
-    }
-
-    for (int k = 0; k < nchunks; ++k) {
-      const int b = k & 1;
-      const int64_t cs = s0 + (int64_t)k * CH;
-      const int len = (int)min((int64_t)CH, s1 - cs);
-      bool ok = true;
-      if (chunk_is_tma(k)) {
-        ok = mbar_wait(&bar[b], (phase >> b) & 1u);
-        phase ^= 1u << b;
-        pending &= ~(1u << b);
-      } else {
-        for (int i = tid; i < len; i += NT) sbuf[b][i] = a.src[cs + i];
-      }
-      if (!__syncthreads_and(ok)) {
-        // A bulk copy never completed: record it, drain what thread 0 still
-        // has in flight (bounded), and leave the kernel uniformly.
-        if (tid == 0) {
-          atomicExch(a.err, DEV_ERR_TIMEOUT);
-          for (int q = 0; q < 2; ++q)
-            if ((pending >> q) & 1u) mbar_wait(&bar[q], (phase >> q) & 1u, 200000000LL);
-        }
-        return;
-      }
-      if (MIXED) {
-        // Source pairs of each full 256-block: (s1, s2) = (src[k], src[k+128])
-        // as {SM, SM, DL, DL} relative to the block's first source.  Pairing
-        // sources half a block apart keeps e1 = d1^2+eta^2 and e2 well apart:
-        // adjacent sorted sources give e1 e2 ~ a square, and the rounded
-        // reciprocal of a near-square carries a small systematic error
-        // (~2e-11 relative, measured) that adds up coherently at large p.
-        for (int i = tid; i < (len / SUB) * (SUB / 2); i += NT) {
-          const int blk = i / (SUB / 2) * SUB, k = i % (SUB / 2);
-          const double cb = sbuf[b][blk];
-          const double s1 = sbuf[b][blk + k], s2 = sbuf[b][blk + k + SUB / 2];
-          const float sm = (float)(s1 - cb), dl = (float)(s1 - s2);
-          sm4[i] = make_float4(sm, sm, dl, dl);
-        }
-        __syncthreads();
-      }
-
-      for (int sub = 0; sub < len; sub += SUB) {
-        const int slen = min(SUB, len - sub);
-        bool far32 = false;
-        if (MIXED && slen == SUB) {
-          const double2 bd = a.bounds[(cs + sub) / SUB];
-          const double gap = fmax(fmax(bd.x - whi, wlo - bd.y), 0.0);
-          const double span = fmax(bd.y - wlo, whi - bd.x);
-          far32 = gap >= a.near_dist && span <= 1e9;
-        }
-        if (MIXED && far32) {
-          // Block-wide target offsets x - cb = TH + TL.
-          const double cb = sbuf[b][sub];
-          u64 TH[R2], TL[R2];
-#pragma unroll
-          for (int kk = 0; kk < R2; ++kk) {
-            const double o0 = x[2 * kk] - cb, o1 = x[2 * kk + 1] - cb;
-            const float h0 = (float)o0, h1 = (float)o1;
-            TH[kk] = pk2(h0, h1);
-            TL[kk] = pk2((float)(o0 - (double)h0), (float)(o1 - (double)h1));
-          }
-          const float4* sp = &sm4[sub / 2];
-          const u64 ETA2_ = ETA2, ONE_ = ONE;
-          for (int j = 0; j < SUB / 2; j += FOLD / 2) {
-            u64 RE[R2], IV[R2];
-#pragma unroll
-            for (int kk = 0; kk < R2; ++kk) RE[kk] = IV[kk] = 0ull;
-#pragma unroll
-            for (int q = 0; q < FOLD / 2; ++q) {
-              const float4 s4 = sp[j + q];
-              const u64 SM = pk2(s4.x, s4.y), DL = pk2(s4.z, s4.w);
-#pragma unroll
-              for (int kk = 0; kk < R2; ++kk)
-                pairs32x4(SM, DL, TH[kk], TL[kk], ETA2_, ONE_, RE[kk], IV[kk]);
-            }
-            // FP32 partials of FOLD sources are folded into FP64 (negated).
-#pragma unroll
-            for (int kk = 0; kk < R2; ++kk) {
-              float r0, r1, v0, v1;
-              upk2(RE[kk], r0, r1);
-              upk2(IV[kk], v0, v1);
-              re64[2 * kk] -= (double)r0;
-              re64[2 * kk + 1] -= (double)r1;
-              iv64[2 * kk] -= (double)v0;
-              iv64[2 * kk + 1] -= (double)v1;
-            }
-          }
-        } else {
-          const double* sp = &sbuf[b][sub];
-          int j = 0;
-#pragma unroll 2
-          for (; j + 2 <= slen; j += 2) {
-            const double2 l2 = *reinterpret_cast<const double2*>(sp + j);
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              pair64(x[r], l2.x, eta2, re64[r], iv64[r]);
-              pair64(x[r], l2.y, eta2, re64[r], iv64[r]);
-            }
-          }
-          if (j < slen) {
-            const double l = sp[j];
-#pragma unroll
-            for (int r = 0; r < R; ++r) pair64(x[r], l, eta2, re64[r], iv64[r]);
-          }
-        }
-      }
-      __syncthreads();
-      if (tid == 0 && chunk_is_tma(k + 2)) {
-        fence_proxy_async();
-        mbar_arrive_expect_tx(&bar[b], CH * 8);
-        bulk_g2s(sbuf[b], a.src + s0 + (int64_t)(k + 2) * CH, CH * 8, &bar[b]);
-        pending |= 1u << b;
-      }
-    }
-
-    double* pre = a.part_re + (int64_t)split * a.nt;
-    double* pim = a.part_im + (int64_t)split * a.nt;
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int64_t idx = wbase + r * 32 + lane;
-      if (idx < a.nt) {
-        pre[idx] = re64[r];
-        pim[idx] = eta * iv64[r];
-      }
-    }
+    PairItem it;
+    it.tgt = a.tgt;
+    it.nt = a.nt;
+    it.src = a.src;
+    it.s0 = (int64_t)split * a.split_len;
+    it.s1 = min(a.ns, it.s0 + a.split_len);
+    it.tile0 = tile * (NT * R);
+    it.eta = a.eta;
+    it.near_dist = a.near_dist;
+    it.bounds = a.bounds;
+    it.out_re = a.part_re + (int64_t)split * a.nt;
+    it.out_im = a.part_im + (int64_t)split * a.nt;
+    it.err = a.err;
+    it.use_tma = a.use_tma != 0;
+    if (!pair_item<MIXED, R>(it, st, phase, pending)) return;
   }
 }
 
