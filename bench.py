@@ -317,8 +317,9 @@ def run_ours(args, world, rank, local):
 
 
 def secondary(args, L, dev, ev, ev_h, eta, p, stream):
-    """FP64 vs mixed at p (speed + error), p = 50k both kernels, and the
-    forward + adjoint cost at p = 20k."""
+    """FP64 vs mixed at p (speed + error), p = 50k both kernels, the forward +
+    adjoint cost at p = 20k and 200k, and the batched launch on 4096 uneven
+    spectra."""
     import torch
     from shrinkers_b200 import _native, spectra
 
@@ -382,6 +383,38 @@ def secondary(args, L, dev, ev, ev_h, eta, p, stream):
         out[f"p20k_{name}_fwd_ms"] = f_ms
         out[f"p20k_{name}_fwd_adj_ms"] = fa_ms
         out[f"p20k_{name}_fwd_adj_over_fwd"] = fa_ms / f_ms
+    # forward + adjoint at p = 200k (exact kernels)
+    p4 = 200_000
+    ev4 = torch.from_numpy(spectra.config5(p4)).to(dev)
+    e4 = 1.0 / math.sqrt(p4)
+    g4 = torch.randn(2, p4, dtype=torch.float64, device=dev,
+                     generator=torch.Generator(device=dev).manual_seed(5))
+    f4r = torch.empty(p4, dtype=torch.float64, device=dev)
+    f4i = torch.empty_like(f4r)
+    g4o = torch.empty_like(f4r)
+    for prec, name in [(0, "f64"), (1, "mixed")]:
+        f_ms = timed(lambda: run(prec, f4r, f4i, ev4, p4, e4), 3)
+        a_ms = timed(lambda: _native.check(L.shrk_stieltjes_adjoint_dev(
+            ev4.data_ptr(), p4, e4, g4[0].data_ptr(), g4[1].data_ptr(), prec, g4o.data_ptr(),
+            stream.cuda_stream)), 3)
+        out[f"p200k_{name}_fwd_ms"] = f_ms
+        out[f"p200k_{name}_adj_ms"] = a_ms
+        out[f"p200k_{name}_fwd_adj_over_fwd"] = (f_ms + a_ms) / f_ms
+    # batched: 4096 spectra, p log-uniform in [256, 16384], eta = 1/sqrt(p)
+    vals, offs, etas = spectra.config4()
+    n = offs.size - 1
+    bv = torch.from_numpy(vals).to(dev)
+    bo = torch.from_numpy(offs).to(dev)
+    be = torch.from_numpy(etas).to(dev)
+    br = torch.empty_like(bv)
+    bi = torch.empty_like(bv)
+    out["batched_pairs"] = float(np.sum(np.diff(offs).astype(np.float64) ** 2))
+    for prec, name in [(0, "f64"), (1, "mixed")]:
+        b_ms = timed(lambda: _native.check(L.shrk_stieltjes_batched_dev(
+            bv.data_ptr(), bo.data_ptr(), n, be.data_ptr(), prec, br.data_ptr(), bi.data_ptr(),
+            stream.cuda_stream)), 3)
+        out[f"batched_{name}_ms"] = b_ms
+        out[f"batched_{name}_pairs_per_s"] = out["batched_pairs"] / (b_ms * 1e-3)
     return out
 
 

@@ -305,15 +305,6 @@ struct GraphCache {
 };
 GraphCache g_graph[kMaxDev];
 
-uint64_t fnv(const int64_t* v, int64_t n) {
-  uint64_t h = 1469598103934665603ull;
-  for (int64_t i = 0; i < n; ++i) {
-    h ^= (uint64_t)v[i];
-    h *= 1099511628211ull;
-  }
-  return h;
-}
-
 int current_device() {
   int d = 0;
   cudaGetDevice(&d);
