@@ -39,7 +39,7 @@ struct DeviceState {
   bool init = false;
   int sms = 0;
   cudaStream_t stream = nullptr;
-  Scratch slots[24];
+  Scratch slots[32];
   int* err = nullptr;
 };
 
@@ -174,13 +174,14 @@ static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
 // Scratch slot map: 0 split partials, 1 block bounds, 2 adjoint partials,
 // 3 input spectrum, 4/5 outputs, 6 query points, 7 raw sums (2 arrays),
 // 8 sorted copy of the sources, 9/10 hybrid temporaries, 11 NUFFT grids,
-// 15 probe sink, 16..21 treecode.
+// 12/13/14/22/23 batched path (its cached graph reads 12, 13, 14 and 22, so
+// no other path may write them), 15 probe sink, 16..21 treecode,
+// 24 NUFFT stencil weights.
 
 // Raw (or scaled) sums of `method` at targets d_tgt against d_src, written
-// through `epi`.  `h_src` (may be null) is a host copy of the sources, used
-// by the treecode build.  The method must already be resolved.
+// through `epi`.  The method must already be resolved.
 static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* d_src,
-                                 const double* h_src, int64_t ns, double eta, int method,
+                                 int64_t ns, double eta, int method,
                                  int precision, double cutoff, const Epilogue& epi,
                                  cudaStream_t s) {
   const bool cut = !std::isnan(cutoff);
@@ -213,42 +214,19 @@ static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* 
     return apply_epilogue(d_tgt, rre, rim, nt, epi, s);
   }
   if (method == SHRK_M_NUFFT || is_cheb(method)) {
-    // Both methods need the sources in ascending order on the device: the
-    // treecode builds over the sorted copy (chebcode.rs:1088-1097) and the
-    // NUFFT splat gathers contiguous source runs per grid cell.  A host copy
-    // decides sortedness (and feeds the tree build).
-    std::vector<double> host, sorted;
-    if (!h_src) {
-      host.resize(ns);
-      SHRK_TRY(d2h(host.data(), d_src, sizeof(double) * ns, s));
-      SHRK_CUDA(cudaStreamSynchronize(s));
-      h_src = host.data();
-    }
-    const double* hs = h_src;
-    const double* ds = d_src;
-    bool sorted_in = true;
-    for (int64_t i = 1; i < ns; ++i)
-      if (!(h_src[i - 1] <= h_src[i])) { sorted_in = false; break; }
-    if (!sorted_in) {
-      sorted.assign(h_src, h_src + ns);
-      std::sort(sorted.begin(), sorted.end());
-      void* dsb = nullptr;
-      SHRK_TRY(scratch_get(8, sizeof(double) * ns, &dsb));
-      SHRK_TRY(h2d(dsb, sorted.data(), sizeof(double) * ns, s));
-      hs = sorted.data();
-      ds = (const double*)dsb;
-    }
+    const double* ds = nullptr;
+    double first = 0.0, last = 0.0;
+    SHRK_TRY(sorted_sources(d_src, ns, &ds, &first, &last, s));
     if (method == SHRK_M_NUFFT) {
-      SHRK_TRY(nufft_points(d_tgt, nt, ds, ns, h_src[0], h_src[ns - 1], eta, epi, s));
+      SHRK_TRY(nufft_points(d_tgt, nt, ds, ns, first, last, eta, epi, s));
     } else {
       ChebParams prm;
       cheb_preset(method, &prm);
       // At arbitrary query points (targets are not the sources) the leaf
       // capacity is relaxed by the grid rule (mod.rs:475-489).
       if (d_tgt != d_src) prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nt, prm.leaf_cap);
-      SHRK_TRY(chebcode_points(d_tgt, nt, hs, ds, ns, eta, prm, epi, s));
+      SHRK_TRY(chebcode_points(d_tgt, nt, ds, ns, eta, prm, epi, s));
     }
-    if (!sorted.empty()) SHRK_CUDA(cudaStreamSynchronize(s));  // h2d reads `sorted`
     return SHRK_OK;
   }
   return not_impl(method);
@@ -344,7 +322,7 @@ static shrk_status lw_device(const double* ev, size_t p, double c, int method, i
   epi.scale = 1.0 / (double)p;
   epi.c = c;
   epi.out_re = (double*)out;
-  SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, ev, (int64_t)p, eta,
+  SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, (int64_t)p, eta,
                          m, precision, NAN, epi, s));
   SHRK_TRY(d2h(xi, out, sizeof(double) * p, s));
   return check_device_error(s);
@@ -387,7 +365,7 @@ static shrk_status deconv_device(const double* ev, size_t p, double c, size_t n_
   epi.c = c;
   epi.eta = eta_val;
   for (int i = 0; i < 6; ++i) epi.out[i] = (double*)out + i * n_points;
-  SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)n_points, (const double*)dev, ev, (int64_t)p,
+  SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)n_points, (const double*)dev, (int64_t)p,
                          eta_val, m, precision, cutoff, epi, s));
   SHRK_TRY(d2h(out7 + n_points, out, sizeof(double) * 6 * n_points, s));
   return check_device_error(s);
@@ -513,7 +491,7 @@ shrk_status shrk_stieltjes_all_dev(const double* d_ev, size_t p, double eta, int
   epi.scale = 1.0 / (double)p;
   epi.out_re = d_re;
   epi.out_im = d_im;
-  return sums_dispatch(d_ev, (int64_t)p, d_ev, nullptr, (int64_t)p, eta, m, precision, cutoff,
+  return sums_dispatch(d_ev, (int64_t)p, d_ev, (int64_t)p, eta, m, precision, cutoff,
                        epi, s);
 }
 
@@ -535,7 +513,7 @@ shrk_status shrk_stieltjes_all(const double* ev, size_t p, double eta, int metho
   epi.scale = 1.0 / (double)p;
   epi.out_re = (double*)out;
   epi.out_im = (double*)out + p;
-  SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, ev, (int64_t)p, eta,
+  SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, (int64_t)p, eta,
                          m, precision, cutoff, epi, s));
   SHRK_TRY(d2h(out_re, out, sizeof(double) * p, s));
   SHRK_TRY(d2h(out_im, (double*)out + p, sizeof(double) * p, s));
@@ -593,7 +571,7 @@ shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const dou
   epi.scale = 1.0;
   epi.out_re = d_re;
   epi.out_im = d_im;
-  return sums_dispatch(d_q, (int64_t)nq, d_ev, nullptr, (int64_t)p, eta, m, precision, cutoff,
+  return sums_dispatch(d_q, (int64_t)nq, d_ev, (int64_t)p, eta, m, precision, cutoff,
                        epi, s);
 }
 
@@ -622,7 +600,7 @@ shrk_status shrk_stieltjes_at_points(const double* q, size_t nq, const double* e
   epi.scale = 1.0;
   epi.out_re = (double*)out;
   epi.out_im = (double*)out + nq;
-  SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)nq, (const double*)dev, ev, (int64_t)p, eta,
+  SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)nq, (const double*)dev, (int64_t)p, eta,
                          m, precision, cutoff, epi, s));
   SHRK_TRY(d2h(raw_re, out, sizeof(double) * nq, s));
   SHRK_TRY(d2h(raw_im, (double*)out + nq, sizeof(double) * nq, s));

@@ -2,10 +2,11 @@
 //
 // Replaces src/stieltjes/chebcode.rs: the flat pre-order tree of
 // FlatChebTree::build (242-572: midpoint split, barycentric leaf fill,
-// reverse-order parent merge, f32 mirrors) is built on the host in C++; the
+// reverse-order parent merge, f32 mirrors) is built on the GPU, breadth
+// first, with every weight accumulated in the reference's order; the
 // per-query evaluation (contribution_f64 607-711, contribution_fast32
-// 722-828) runs on the GPU, one thread per query, queries in their given
-// order (ascending queries keep a warp's traversals coherent).
+// 722-828) runs one thread per query, queries in their given order
+// (ascending queries keep a warp's traversals coherent).
 //
 // The evaluation reproduces the reference's x86 arithmetic operation by
 // operation: two-lane leaf accumulation with a scalar tail, unfused lane
@@ -36,104 +37,162 @@ struct NodeF32 {
   int32_t right;
 };
 
-struct HostTree {
-  std::vector<double> lo, hi, accept_hw, nodes, w;
-  std::vector<int64_t> lo_idx, hi_idx;
-  std::vector<int32_t> right;
-  int n = 0;
-  double theta_sq = 0.0;
+// --------------------------------------------------- tree (device) --
+// FlatChebTree::build (chebcode.rs:509-572) on the GPU, breadth first:
+//   1. split: every node of a level with more than leaf_cap sources (and
+//      depth < 48) splits at the midpoint of its value range (upper_bound of
+//      mid, or the index midpoint when one side would be empty,
+//      chebcode.rs:347-388); children take slots from an atomic counter and
+//      are linked explicitly, so slot order does not matter;
+//   2. subtree sizes bottom-up, pre-order indices top-down (node, left
+//      subtree, right subtree -- the reference's flat layout);
+//   3. flat arrays at the pre-order indices: bounds, acceptance radius,
+//      Chebyshev nodes c + l cos(j pi/(n-1)) (set_node_positions 268-278);
+//   4. P2M: one thread per leaf adds the barycentric rows of its sources in
+//      index order (fill_leaves 401-460);
+//   5. M2M: level by level from the deepest, one thread per internal node
+//      merges the left then the right child's node masses
+//      (merge_all_weights 474-506).
+// Every weight is accumulated in the reference's order with the same
+// operations (IEEE division, fused fma where it uses mul_add), so the tree is
+// identical to the sequential build.
+
+struct ChebConsts {
+  double sm1[MAX_N];  // cos(j pi / (n - 1)), computed on the host
+  double lam[MAX_N];  // barycentric weights of the 2nd-kind nodes
+  int n;
 };
 
 // chebcode.rs:309-337 barycentric_row.
-void bary_row(double x, const double* t, const double* lam, double* w, double* v, int n,
-              double mass) {
+__device__ __forceinline__ void bary_row_dev(double x, const double* t, const ChebConsts& k,
+                                             double* w, double mass) {
+  double v[MAX_N];
   double s = 0.0;
-  int hit = -1;
-  for (int j = 0; j < n; ++j) {
-    double d = x - t[j];
+  for (int j = 0; j < k.n; ++j) {
+    const double d = x - t[j];
     if (d == 0.0) {
-      hit = j;
-      break;
+      w[j] += mass;
+      return;
     }
-    double q = lam[j] / d;
+    const double q = k.lam[j] / d;
     v[j] = q;
     s += q;
   }
-  if (hit >= 0) {
-    w[hit] += mass;
+  const double m = mass * (1.0 / s);
+  for (int j = 0; j < k.n; ++j) w[j] = fma(m, v[j], w[j]);
+}
+
+struct BuildArrays {
+  int64_t* blo;  // BFS slot -> source index range [blo, bhi)
+  int64_t* bhi;
+  int32_t* lc;   // children (-1: leaf)
+  int32_t* rc;
+  int32_t* size;
+  int32_t* pre;  // pre-order index
+  int* counter;  // next free BFS slot
+};
+
+__global__ void tree_split_kernel(const double* __restrict__ sorted, BuildArrays b, int begin,
+                                  int end, int depth, int64_t leaf_cap) {
+  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= end) return;
+  const int64_t lo_idx = b.blo[i], hi_idx = b.bhi[i];
+  if (hi_idx - lo_idx <= leaf_cap || depth >= MAX_TREE_DEPTH) {
+    b.lc[i] = b.rc[i] = -1;
     return;
   }
-  double m = mass * (1.0 / s);
-  for (int j = 0; j < n; ++j) w[j] = std::fma(m, v[j], w[j]);
-}
-
-// chebcode.rs:347-388 build_topology (+ set_node_positions 268-278).
-int32_t build_topology(HostTree& T, const double* sorted, const std::vector<double>& sm1,
-                       int64_t lo_idx, int64_t hi_idx, int64_t leaf_cap, int depth) {
-  int32_t idx = (int32_t)T.lo.size();
-  int64_t count = hi_idx - lo_idx;
-  double lo = sorted[lo_idx], hi = sorted[hi_idx - 1];
-  T.lo.push_back(lo);
-  T.hi.push_back(hi);
-  double hw = 0.5 * (hi - lo);
-  T.accept_hw.push_back(hw * hw / T.theta_sq);
-  T.lo_idx.push_back(lo_idx);
-  T.hi_idx.push_back(hi_idx);
-  double c = 0.5 * (lo + hi), l = 0.5 * (hi - lo);
-  for (int j = 0; j < T.n; ++j) {
-    T.nodes.push_back(c + l * sm1[j]);
-    T.w.push_back(0.0);
+  const double lo = sorted[lo_idx], hi = sorted[hi_idx - 1];
+  const double mid = lo + 0.5 * (hi - lo);
+  int64_t a = lo_idx, e = hi_idx;  // upper_bound: first element > mid
+  while (a < e) {
+    const int64_t m = (a + e) >> 1;
+    if (mid < sorted[m]) e = m;
+    else a = m + 1;
   }
-  T.right.push_back(-1);
-  if (count <= leaf_cap || depth >= MAX_TREE_DEPTH) return idx;
-  double mid = lo + 0.5 * (hi - lo);
-  int64_t split = (int64_t)(std::upper_bound(sorted + lo_idx, sorted + hi_idx, mid) - sorted);
+  int64_t split = a;
   if (split == lo_idx || split == hi_idx) split = (lo_idx + hi_idx) / 2;
-  build_topology(T, sorted, sm1, lo_idx, split, leaf_cap, depth + 1);
-  int32_t ri = build_topology(T, sorted, sm1, split, hi_idx, leaf_cap, depth + 1);
-  T.right[idx] = ri;
-  return idx;
+  const int slot = atomicAdd(b.counter, 2);
+  b.blo[slot] = lo_idx;
+  b.bhi[slot] = split;
+  b.blo[slot + 1] = split;
+  b.bhi[slot + 1] = hi_idx;
+  b.lc[i] = slot;
+  b.rc[i] = slot + 1;
 }
 
-// chebcode.rs:509-572 FlatChebTree::build (weights: fill_leaves 401-460,
-// merge_all_weights 474-506).
-void build_tree(HostTree& T, const double* sorted, int64_t p, int n, double theta,
-                int64_t leaf_cap) {
-  T.n = n;
-  T.theta_sq = theta * theta;
-  std::vector<double> sm1(n), lam(n);
-  for (int j = 0; j < n; ++j) {
-    sm1[j] = std::cos((double)j * M_PI / (double)(n - 1));
-    double sign = (j % 2 == 0) ? 1.0 : -1.0;
-    lam[j] = (j == 0 || j == n - 1) ? 0.5 * sign : sign;
+__global__ void tree_size_kernel(BuildArrays b, int begin, int end) {
+  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= end) return;
+  b.size[i] = b.lc[i] < 0 ? 1 : 1 + b.size[b.lc[i]] + b.size[b.rc[i]];
+}
+
+__global__ void tree_pre_kernel(BuildArrays b, int begin, int end) {
+  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= end || b.lc[i] < 0) return;
+  b.pre[b.lc[i]] = b.pre[i] + 1;
+  b.pre[b.rc[i]] = b.pre[i] + 1 + b.size[b.lc[i]];
+}
+
+struct FlatTree {
+  double* lo;
+  double* hi;
+  double* accept_hw;
+  int64_t* lo_idx;
+  int64_t* hi_idx;
+  int32_t* right;
+  double* nodes;  // [nn][n]
+  double* w;      // [nn][n]
+};
+
+__global__ void tree_fill_kernel(const double* __restrict__ sorted, BuildArrays b, int nn,
+                                 FlatTree f, ChebConsts k, double theta_sq) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= nn) return;
+  const int idx = b.pre[i];
+  const int64_t lo_idx = b.blo[i], hi_idx = b.bhi[i];
+  const double lo = sorted[lo_idx], hi = sorted[hi_idx - 1];
+  f.lo[idx] = lo;
+  f.hi[idx] = hi;
+  const double hw = 0.5 * (hi - lo);
+  f.accept_hw[idx] = hw * hw / theta_sq;
+  f.lo_idx[idx] = lo_idx;
+  f.hi_idx[idx] = hi_idx;
+  f.right[idx] = b.lc[i] < 0 ? -1 : b.pre[b.rc[i]];
+  const double c = 0.5 * (lo + hi), l = 0.5 * (hi - lo);
+  for (int j = 0; j < k.n; ++j) f.nodes[(int64_t)idx * k.n + j] = c + l * k.sm1[j];
+}
+
+__global__ void tree_p2m_kernel(const double* __restrict__ sorted, BuildArrays b, int nn,
+                                FlatTree f, ChebConsts k) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= nn || b.lc[i] >= 0) return;
+  const int idx = b.pre[i];
+  double t[MAX_N], w[MAX_N];
+  for (int j = 0; j < k.n; ++j) {
+    t[j] = f.nodes[(int64_t)idx * k.n + j];
+    w[j] = 0.0;
   }
-  const size_t est = (size_t)std::max<int64_t>(1, std::min<int64_t>(4 * p / std::max<int64_t>(leaf_cap, 1) + 32, 2 * p));
-  T.lo.reserve(est); T.hi.reserve(est); T.accept_hw.reserve(est);
-  T.lo_idx.reserve(est); T.hi_idx.reserve(est); T.right.reserve(est);
-  T.nodes.reserve(est * n); T.w.reserve(est * n);
-  build_topology(T, sorted, sm1, 0, p, leaf_cap, 0);
-  const size_t nn = T.lo.size();
-  std::vector<double> v(n);
-  for (size_t i = 0; i < nn; ++i) {
-    if (T.right[i] >= 0) continue;
-    double* w = &T.w[i * n];
-    for (int j = 0; j < n; ++j) w[j] = 0.0;
-    for (int64_t k = T.lo_idx[i]; k < T.hi_idx[i]; ++k)
-      bary_row(sorted[k], &T.nodes[i * n], lam.data(), w, v.data(), n, 1.0);
+  for (int64_t q = b.blo[i]; q < b.bhi[i]; ++q) bary_row_dev(sorted[q], t, k, w, 1.0);
+  for (int j = 0; j < k.n; ++j) f.w[(int64_t)idx * k.n + j] = w[j];
+}
+
+__global__ void tree_m2m_kernel(BuildArrays b, int begin, int end, FlatTree f, ChebConsts k) {
+  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= end || b.lc[i] < 0) return;
+  const int idx = b.pre[i];
+  double t[MAX_N], w[MAX_N];
+  for (int j = 0; j < k.n; ++j) {
+    t[j] = f.nodes[(int64_t)idx * k.n + j];
+    w[j] = 0.0;
   }
-  for (size_t pi = nn; pi-- > 0;) {
-    if (T.right[pi] < 0) continue;
-    double* pw = &T.w[pi * n];
-    for (int j = 0; j < n; ++j) pw[j] = 0.0;
-    const double* t = &T.nodes[pi * n];
-    const int32_t kids[2] = {(int32_t)pi + 1, T.right[pi]};
-    for (int32_t ci : kids)
-      for (int ti = 0; ti < n; ++ti) {
-        double m = T.w[(size_t)ci * n + ti];
-        if (m == 0.0) continue;
-        bary_row(T.nodes[(size_t)ci * n + ti], t, lam.data(), pw, v.data(), n, m);
-      }
-  }
+  const int kids[2] = {b.pre[b.lc[i]], b.pre[b.rc[i]]};
+  for (int c = 0; c < 2; ++c)
+    for (int ti = 0; ti < k.n; ++ti) {
+      const double m = f.w[(int64_t)kids[c] * k.n + ti];
+      if (m == 0.0) continue;
+      bary_row_dev(f.nodes[(int64_t)kids[c] * k.n + ti], t, k, w, m);
+    }
+  for (int j = 0; j < k.n; ++j) f.w[(int64_t)idx * k.n + j] = w[j];
 }
 
 // ----------------------------------------------------------- device --
@@ -312,13 +371,114 @@ __global__ void __launch_bounds__(128) cheb_eval_f32(const EvalArgs a) {
   epi_store(a.epi, t, lambda, leaf_re + (double)hr, leaf_im + eta * (double)hi);
 }
 
-template <typename T>
-shrk_status upload(int slot_base, int slot, const std::vector<T>& v, T** out, cudaStream_t s) {
-  void* p = nullptr;
-  SHRK_TRY(scratch_get(slot_base + slot, sizeof(T) * std::max<size_t>(v.size(), 1), &p));
-  if (!v.empty())
-    SHRK_CUDA(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
-  *out = (T*)p;
+__global__ void tree_init_kernel(BuildArrays b, int64_t ns) {
+  b.blo[0] = 0;
+  b.bhi[0] = ns;
+  b.pre[0] = 0;
+  *b.counter = 1;
+}
+
+// F32 mirror of the flat tree for the fast preset (NodeF32 + node panels).
+__global__ void tree_f32_kernel(FlatTree f, int nn, int n, NodeF32* nf, float* panel) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= nn) return;
+  nf[i] = {(float)f.lo[i], (float)f.hi[i], (float)f.accept_hw[i], (uint32_t)f.lo_idx[i],
+           (uint32_t)f.hi_idx[i], f.right[i]};
+  for (int j = 0; j < n; ++j) {
+    panel[(int64_t)i * 2 * n + j] = (float)f.nodes[(int64_t)i * n + j];
+    panel[(int64_t)i * 2 * n + n + j] = (float)f.w[(int64_t)i * n + j];
+  }
+}
+
+unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// Builds the flat tree of d_sorted (ascending) into the TREE_SLOTS scratch.
+// Scratch slots 25/26 hold the breadth-first build arrays.
+shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams& prm,
+                           FlatTree& f, int& nn_out, cudaStream_t s) {
+  const int64_t cap = std::max<int64_t>(2 * ns, 2);
+  if (cap > (int64_t)INT32_MAX / 2) {
+    set_error("chebcode: too many eigenvalues for the tree build");
+    return SHRK_EINVAL;
+  }
+  ChebConsts k;
+  k.n = prm.n;
+  for (int j = 0; j < prm.n; ++j) {
+    k.sm1[j] = std::cos((double)j * M_PI / (double)(prm.n - 1));
+    const double sign = (j % 2 == 0) ? 1.0 : -1.0;
+    k.lam[j] = (j == 0 || j == prm.n - 1) ? 0.5 * sign : sign;
+  }
+  void* p64 = nullptr;
+  void* p32 = nullptr;
+  SHRK_TRY(scratch_get(25, sizeof(int64_t) * 2 * (size_t)cap, &p64));
+  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (4 * (size_t)cap + 64), &p32));
+  BuildArrays b;
+  b.blo = (int64_t*)p64;
+  b.bhi = b.blo + cap;
+  b.lc = (int32_t*)p32;
+  b.rc = b.lc + cap;
+  b.size = b.rc + cap;
+  b.pre = b.size + cap;
+  b.counter = (int*)(b.pre + cap);
+  constexpr int BS = 256;
+  {
+    LaunchScope ls("cheb_build", s);
+    tree_init_kernel<<<1, 1, 0, s>>>(b, ns);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  // 1. split, level by level (each level's children fill the next slots)
+  std::vector<int> lb{0}, le{1};
+  for (int depth = 0;; ++depth) {
+    const int begin = lb.back(), end = le.back();
+    tree_split_kernel<<<blocks_for(end - begin, BS), BS, 0, s>>>(d_sorted, b, begin, end, depth,
+                                                                  (int64_t)prm.leaf_cap);
+    SHRK_CUDA(cudaGetLastError());
+    add_launches(1);
+    int next = 0;
+    SHRK_CUDA(cudaMemcpyAsync(&next, b.counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SHRK_CUDA(cudaStreamSynchronize(s));
+    if (next == end) break;
+    lb.push_back(end);
+    le.push_back(next);
+  }
+  const int nn = le.back();
+  const int levels = (int)lb.size();
+  // 2. subtree sizes bottom-up, pre-order indices top-down
+  for (int L = levels - 1; L >= 0; --L) {
+    tree_size_kernel<<<blocks_for(le[L] - lb[L], BS), BS, 0, s>>>(b, lb[L], le[L]);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  for (int L = 0; L < levels; ++L) {
+    tree_pre_kernel<<<blocks_for(le[L] - lb[L], BS), BS, 0, s>>>(b, lb[L], le[L]);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  add_launches(2 * levels);
+  // 3. flat arrays
+  void* q = nullptr;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 0, sizeof(double) * 3 * (size_t)nn, &q));
+  f.lo = (double*)q;
+  f.hi = f.lo + nn;
+  f.accept_hw = f.hi + nn;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 1, sizeof(int64_t) * 2 * (size_t)nn, &q));
+  f.lo_idx = (int64_t*)q;
+  f.hi_idx = f.lo_idx + nn;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 2, sizeof(int32_t) * (size_t)nn, &q));
+  f.right = (int32_t*)q;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 3, sizeof(double) * 2 * (size_t)nn * prm.n, &q));
+  f.nodes = (double*)q;
+  f.w = f.nodes + (size_t)nn * prm.n;
+  tree_fill_kernel<<<blocks_for(nn, BS), BS, 0, s>>>(d_sorted, b, nn, f, k,
+                                                     prm.theta * prm.theta);
+  SHRK_CUDA(cudaGetLastError());
+  // 4. P2M at the leaves; 5. M2M from the deepest internal level up
+  tree_p2m_kernel<<<blocks_for(nn, 128), 128, 0, s>>>(d_sorted, b, nn, f, k);
+  SHRK_CUDA(cudaGetLastError());
+  for (int L = levels - 2; L >= 0; --L) {
+    tree_m2m_kernel<<<blocks_for(le[L] - lb[L], 128), 128, 0, s>>>(b, lb[L], le[L], f, k);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  add_launches(2 + std::max(levels - 1, 0));
+  nn_out = nn;
   return SHRK_OK;
 }
 
@@ -345,17 +505,17 @@ size_t grid_leaf_cap(size_t n, size_t p, size_t nq, size_t preset_leaf) {
   return std::min(std::max(r, preset_leaf), hi);
 }
 
-shrk_status chebcode_points(const double* d_q, int64_t nq, const double* h_sorted_src,
-                            const double* d_sorted_src, int64_t ns, double eta,
-                            const ChebParams& prm, const Epilogue& epi, cudaStream_t s) {
+shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorted_src, int64_t ns,
+                            double eta, const ChebParams& prm, const Epilogue& epi,
+                            cudaStream_t s) {
   if (nq <= 0 || ns <= 0) return SHRK_OK;
   if (prm.n < 2 || prm.n > MAX_N) {
     set_error("chebcode: interpolation order must be in [2, 16]");
     return SHRK_EINVAL;
   }
-  HostTree T;
-  build_tree(T, h_sorted_src, ns, prm.n, prm.theta, prm.leaf_cap);
-  const size_t nn = T.lo.size();
+  FlatTree f;
+  int nn = 0;
+  SHRK_TRY(build_tree_gpu(d_sorted_src, ns, prm, f, nn, s));
   EvalArgs a;
   a.q = d_q;
   a.nq = nq;
@@ -367,63 +527,34 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* h_sorte
   a.nf = nullptr;
   a.panel = nullptr;
   if (!prm.f32) {
-    double *lo, *hi, *acc, *nodes, *w;
-    int64_t *li, *hix;
-    int32_t* right;
-    SHRK_TRY(upload(TREE_SLOTS, 0, T.lo, &lo, s));
-    SHRK_TRY(upload(TREE_SLOTS, 1, T.hi, &hi, s));
-    SHRK_TRY(upload(TREE_SLOTS, 2, T.accept_hw, &acc, s));
-    std::vector<int64_t> idx(2 * nn);
-    for (size_t i = 0; i < nn; ++i) {
-      idx[i] = T.lo_idx[i];
-      idx[nn + i] = T.hi_idx[i];
-    }
-    int64_t* didx;
-    SHRK_TRY(upload(TREE_SLOTS, 3, idx, &didx, s));
-    li = didx;
-    hix = didx + nn;
-    SHRK_TRY(upload(TREE_SLOTS, 4, T.right, &right, s));
-    std::vector<double> nw(2 * nn * prm.n);
-    std::copy(T.nodes.begin(), T.nodes.end(), nw.begin());
-    std::copy(T.w.begin(), T.w.end(), nw.begin() + nn * prm.n);
-    double* dnw;
-    SHRK_TRY(upload(TREE_SLOTS, 5, nw, &dnw, s));
-    nodes = dnw;
-    w = dnw + nn * prm.n;
-    a.t.lo = lo;
-    a.t.hi = hi;
-    a.t.accept_hw = acc;
-    a.t.lo_idx = li;
-    a.t.hi_idx = hix;
-    a.t.right = right;
-    a.t.nodes = nodes;
-    a.t.w = w;
+    a.t.lo = f.lo;
+    a.t.hi = f.hi;
+    a.t.accept_hw = f.accept_hw;
+    a.t.lo_idx = f.lo_idx;
+    a.t.hi_idx = f.hi_idx;
+    a.t.right = f.right;
+    a.t.nodes = f.nodes;
+    a.t.w = f.w;
     LaunchScope ls("cheb_eval_f64", s);
     cheb_eval_f64<<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   } else {
-    std::vector<NodeF32> nf(nn);
-    std::vector<float> panel(nn * 2 * prm.n);
-    for (size_t i = 0; i < nn; ++i) {
-      nf[i] = {(float)T.lo[i], (float)T.hi[i], (float)T.accept_hw[i], (uint32_t)T.lo_idx[i],
-               (uint32_t)T.hi_idx[i], T.right[i]};
-      for (int j = 0; j < prm.n; ++j) {
-        panel[i * 2 * prm.n + j] = (float)T.nodes[i * prm.n + j];
-        panel[i * 2 * prm.n + prm.n + j] = (float)T.w[i * prm.n + j];
-      }
+    void* q = nullptr;
+    SHRK_TRY(scratch_get(TREE_SLOTS + 4, sizeof(NodeF32) * (size_t)nn, &q));
+    NodeF32* nf = (NodeF32*)q;
+    SHRK_TRY(scratch_get(TREE_SLOTS + 5, sizeof(float) * 2 * (size_t)nn * prm.n, &q));
+    float* panel = (float*)q;
+    {
+      LaunchScope ls("cheb_build", s);
+      tree_f32_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(f, nn, prm.n, nf, panel);
+      SHRK_CUDA(cudaGetLastError());
     }
-    NodeF32* dnf;
-    float* dpanel;
-    SHRK_TRY(upload(TREE_SLOTS, 0, nf, &dnf, s));
-    SHRK_TRY(upload(TREE_SLOTS, 1, panel, &dpanel, s));
-    a.nf = dnf;
-    a.panel = dpanel;
+    a.nf = nf;
+    a.panel = panel;
     LaunchScope ls("cheb_eval_f32", s);
     cheb_eval_f32<<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   }
-  // The host vectors feeding the uploads must outlive the copies.
-  SHRK_CUDA(cudaStreamSynchronize(s));
   return SHRK_OK;
 }
 

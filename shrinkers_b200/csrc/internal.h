@@ -88,9 +88,15 @@ size_t nufft_grid_size(double raw_range, double eta);
 struct ChebParams { double theta; int n; int leaf_cap; bool f32; };
 bool cheb_preset(int method, ChebParams* out);
 size_t grid_leaf_cap(size_t n, size_t p, size_t nq, size_t preset_leaf);
-shrk_status chebcode_points(const double* d_q, int64_t nq, const double* h_sorted_src,
-                            const double* d_sorted_src, int64_t ns, double eta,
-                            const ChebParams& prm, const Epilogue& epi, cudaStream_t s);
+shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorted_src, int64_t ns,
+                            double eta, const ChebParams& prm, const Epilogue& epi,
+                            cudaStream_t s);
+
+// Sources in ascending order on the device (d_src itself when already
+// sorted, else a sorted copy in library scratch) and the first / last entry
+// of d_src in the caller's order (sources.cu).
+shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sorted,
+                           double* first, double* last, cudaStream_t s);
 
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);

@@ -3,16 +3,18 @@
 // Replaces src/stieltjes/nufft.rs (grid policy 33-126, entry points 164-220)
 // and the dual-convolution core of src/stieltjes/fft5.rs (splat 175-185 /
 // 259-318, fft_convolution 325-432, interpolate_grid 440-476) with the
-// packing helpers of src/stieltjes/fftplan.rs:43-76.  Pipeline (7 kernels,
+// packing helpers of src/stieltjes/fftplan.rs:43-76.  Pipeline (8 kernels,
 // all FP64):
 //
-//   1. splat_pack   one thread per grid cell GATHERS the 4-point Cubic
-//                   Lagrange weights of the sources whose stencil covers it
-//                   (sources ascending, so each cell's sources are one
-//                   contiguous run found by binary search) and writes
-//                   packed[c] = density[c] + i * x_c/(x_c^2 + eta^2).  Each
-//                   cell sums its sources in ascending order -- the order of
-//                   the reference's sequential splat -- with no atomics.
+//   1. splat        one thread per source computes its stencil cell and
+//                   4-point Cubic Lagrange weights; then one warp per grid
+//                   cell GATHERS the weights of the sources whose stencil
+//                   covers it (sources ascending, so they are one contiguous
+//                   run, found by a 32-way search) and writes packed[c] =
+//                   density[c] + i * x_c/(x_c^2 + eta^2).  Fixed-order warp
+//                   sums: deterministic, no atomics (the reference's
+//                   sequential and per-worker splats differ from each other
+//                   by rounding; its tests pin the NUFFT by tolerance).
 //   2. fft (x2)     four-step FFT m = m1*m2 (m1, m2 <= 256): column FFTs of
 //                   length m1 in shared memory with the inter-pass twiddle,
 //                   then row FFTs of length m2.  Twiddles and the analytic
@@ -78,6 +80,8 @@ struct GridArgs {
   int64_t ns;
   double lo, dx, eta;
   int64_t m;
+  int* cell;          // per source: floor((src - lo)/dx), clamped to [-4, m + 4]
+  double* w;          // per source: the 4 stencil weights, SoA [4][ns]
   double2* packed;
 };
 
@@ -88,57 +92,81 @@ __device__ __forceinline__ int64_t cell0_of(double v, double lo, double dx, doub
   return (int64_t)fl;
 }
 
-// First source index j with floor((src[j]-lo)/dx) >= key (sources ascending).
-__device__ int64_t first_with_cell_ge(const GridArgs& a, int64_t key) {
-  int64_t lo = 0, hi = a.ns;
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    double t;
-    if (cell0_of(a.src[mid], a.lo, a.dx, &t) < key) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
+// Per source: stencil cell i0 = floor((v - lo)/dx) and the 4-point Cubic
+// Lagrange weights of t = pos - i0 (fft5.rs:175-185).  Clamping i0 to
+// [-4, m + 4] keeps the edge-cell mapping (every slot of such a source lands
+// on the same edge cell) and the order of the sorted sources.
+__global__ void splat_weights_kernel(const GridArgs a) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.ns) return;
+  double t;
+  const int64_t i0 = cell0_of(a.src[j], a.lo, a.dx, &t);
+  double w[4];
+  lagrange4(t, w);
+  a.cell[j] = (int)(i0 < -4 ? -4 : (i0 > a.m + 4 ? a.m + 4 : i0));
+#pragma unroll
+  for (int k = 0; k < 4; ++k) a.w[(int64_t)k * a.ns + j] = w[k];
 }
 
-// Steps 1+pack: gather-splat of cell c, then packed[c] (fft5.rs:259-318, 364-376).
+// First source index j with cell[j] >= key (ns if none), cell[] non-
+// decreasing: a 32-way search where every lane probes one point per round.
+__device__ int64_t warp_first_ge(const int* __restrict__ cell, int64_t ns, int key, int lane) {
+  int64_t lo = 0, hi = ns;  // the answer lies in [lo, hi]
+  while (hi - lo > 32) {
+    const int64_t step = (hi - lo + 31) / 32;
+    const int64_t q = lo + (int64_t)lane * step;
+    const bool less = q < hi && cell[q] < key;
+    const int cnt = __popc(__ballot_sync(0xffffffffu, less));
+    const int64_t nlo = cnt > 0 ? lo + (int64_t)(cnt - 1) * step + 1 : lo;
+    hi = min(hi, lo + (int64_t)cnt * step);
+    lo = nlo;
+  }
+  const int64_t q = lo + lane;
+  const bool less = q < hi && cell[q] < key;
+  return lo + __popc(__ballot_sync(0xffffffffu, less));
+}
+
+// Steps 1+pack: one warp per grid cell gathers the stencil weights of the
+// sources covering it (fft5.rs:259-318), then packed[c] = density[c] +
+// i x_c/(x_c^2 + eta^2) (fft5.rs:364-376).  Lanes stride the cell's source
+// run and a fixed butterfly adds the lane sums: deterministic, no atomics.
 __global__ void splat_pack_kernel(const GridArgs a) {
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.m) return;
-  double dens = 0.0;
+  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= a.m) return;  // whole warps exit together
   const int64_t m = a.m;
+  double dens = 0.0;
   if (c > 0 && c < m - 1) {
     // interior cell: exactly one stencil slot k = c + 1 - i0 per source
-    int64_t j = first_with_cell_ge(a, c - 2);
-    for (; j < a.ns; ++j) {
-      double t;
-      const int64_t i0 = cell0_of(a.src[j], a.lo, a.dx, &t);
-      if (i0 > c + 1) break;
-      double w[4];
-      lagrange4(t, w);
-      dens += w[c + 1 - i0];
+    const int64_t j0 = warp_first_ge(a.cell, a.ns, (int)c - 2, lane);
+    const int64_t j1 = warp_first_ge(a.cell, a.ns, (int)c + 2, lane);
+    for (int64_t j = j0 + lane; j < j1; j += 32) {
+      const int k = (int)c + 1 - a.cell[j];
+      dens += a.w[(int64_t)k * a.ns + j];
     }
   } else {
-    // edge cell: every slot whose clamped index lands here, sources in order
-    const int64_t j0 = (c == 0) ? 0 : first_with_cell_ge(a, m - 3);
-    const int64_t j1 = (c == 0) ? first_with_cell_ge(a, 2) : a.ns;
-    for (int64_t j = j0; j < j1; ++j) {
-      double t;
-      const int64_t i0 = cell0_of(a.src[j], a.lo, a.dx, &t);
-      double w[4];
-      lagrange4(t, w);
+    // edge cell: every slot whose clamped index lands here
+    const int64_t j0 = (c == 0) ? 0 : warp_first_ge(a.cell, a.ns, (int)m - 3, lane);
+    const int64_t j1 = (c == 0) ? warp_first_ge(a.cell, a.ns, 2, lane) : a.ns;
+    for (int64_t j = j0 + lane; j < j1; j += 32) {
+      const int i0 = a.cell[j];
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        int64_t cell = i0 - 1 + k;
+        int64_t cell = (int64_t)i0 - 1 + k;
         cell = cell < 0 ? 0 : (cell > m - 1 ? m - 1 : cell);
-        if (cell == c) dens += w[k];
+        if (cell == c) dens += a.w[(int64_t)k * a.ns + j];
       }
     }
   }
-  const int64_t half = m / 2;
-  const double sd = (c <= half) ? (double)c : (double)c - (double)m;
-  const double x = sd * a.dx;
-  const double denom = x * x + a.eta * a.eta;
-  a.packed[c] = make_double2(dens, x / denom);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) dens += __shfl_xor_sync(0xffffffffu, dens, o);
+  if (lane == 0) {
+    const int64_t half = m / 2;
+    const double sd = (c <= half) ? (double)c : (double)c - (double)m;
+    const double x = sd * a.dx;
+    const double denom = x * x + a.eta * a.eta;
+    a.packed[c] = make_double2(dens, x / denom);
+  }
 }
 
 // ---------------------------------------------------------------- FFT --
@@ -385,10 +413,19 @@ shrk_status nufft_points(const double* d_q, int64_t nq, const double* d_src, int
   double2* A = (double2*)w;
   double2* B = A + m;
   double2* Tmp = B + m;
-  GridArgs ga{d_src, ns, lo, dx, eta, m, A};
+  void* sw = nullptr;
+  SHRK_TRY(scratch_get(24, (sizeof(int) + 4 * sizeof(double)) * (size_t)ns + 256, &sw));
+  double* wts = (double*)sw;
+  int* cell = (int*)(wts + 4 * ns);
+  GridArgs ga{d_src, ns, lo, dx, eta, m, cell, wts, A};
   {
     LaunchScope ls("nufft_splat", s);
-    splat_pack_kernel<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(ga);
+    splat_weights_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(ga);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  {
+    LaunchScope ls("nufft_splat", s);
+    splat_pack_kernel<<<(unsigned)((m * 32 + 255) / 256), 256, 0, s>>>(ga);
     SHRK_CUDA(cudaGetLastError());
   }
   SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, s));

@@ -1,0 +1,63 @@
+// Sources in ascending order on the device, for the methods that need them
+// (the treecode builds over the sorted spectrum, chebcode.rs:1088-1097; the
+// NUFFT splat gathers contiguous source runs per grid cell).  Sortedness is
+// checked on the device; only unsorted input is sorted (CUB radix sort into
+// library scratch).  The first and last entries IN THE CALLER'S ORDER are
+// returned too: the NUFFT takes its grid bounds from them (nufft.rs:139-146).
+#include "common.cuh"
+#include "internal.h"
+
+#include <cub/device/device_radix_sort.cuh>
+
+namespace shrk {
+namespace {
+
+__global__ void unsorted_kernel(const double* __restrict__ src, int64_t n, int* flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (i < n && !(src[i - 1] <= src[i])) *flag = 1;
+}
+
+}  // namespace
+
+// Scratch: slot 27 the flag, slot 8 the sorted copy, slot 28 CUB's temporary.
+shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sorted,
+                           double* first, double* last, cudaStream_t s) {
+  void* f = nullptr;
+  SHRK_TRY(scratch_get(27, 256, &f));
+  int* flag = (int*)f;
+  SHRK_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+  if (ns > 1) {
+    LaunchScope ls("sources_check", s);
+    unsorted_kernel<<<(unsigned)((ns - 1 + 255) / 256), 256, 0, s>>>(d_src, ns, flag);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  int h_flag = 0;
+  SHRK_CUDA(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaMemcpyAsync(first, d_src, sizeof(double), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaMemcpyAsync(last, d_src + (ns - 1), sizeof(double), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  if (!h_flag) {
+    *d_sorted = d_src;
+    return SHRK_OK;
+  }
+  if (ns > (int64_t)INT32_MAX) {
+    set_error("unsorted input larger than 2^31 values: sort it before the call");
+    return SHRK_EINVAL;
+  }
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(8, sizeof(double) * (size_t)ns, &out));
+  size_t temp_bytes = 0;
+  SHRK_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, d_src, (double*)out, (int)ns, 0,
+                                           64, s));
+  void* temp = nullptr;
+  SHRK_TRY(scratch_get(28, std::max<size_t>(temp_bytes, 256), &temp));
+  {
+    LaunchScope ls("sources_sort", s);
+    SHRK_CUDA(cub::DeviceRadixSort::SortKeys(temp, temp_bytes, d_src, (double*)out, (int)ns, 0,
+                                             64, s));
+  }
+  *d_sorted = (const double*)out;
+  return SHRK_OK;
+}
+
+}  // namespace shrk
