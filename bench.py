@@ -44,7 +44,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--p", type=int, default=1_000_000)
+    ap.add_argument("--spectra", type=int, default=4096,
+                    help="batched workload: number of spectra")
+    ap.add_argument("--p", type=int, default=None,
+                    help="spectrum size (default: the workload's own size)")
+    ap.add_argument("--workload", default="exact",
+                    choices=["exact", "adjoint", "batched", "chebcode_fast", "chebcode",
+                             "chebcode_xtreme", "nufft"],
+                    help="exact (default, the headline): all-points exact transform at p=1M; "
+                         "adjoint: the adjoint kernel at p=20000; batched: 4096 uneven "
+                         "spectra; chebcode*/nufft: the method at p=1M on the spiked "
+                         "spectrum")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
@@ -316,10 +326,254 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+METHOD_IDS = {"chebcode": 13, "chebcode_fast": 14, "chebcode_xtreme": 15, "nufft": 11}
+CHEB_PRESETS = {"chebcode": (0.5, 11, 32, False), "chebcode_fast": (1.0, 8, 32, True),
+                "chebcode_xtreme": (0.25, 11, 16, False)}
+
+
+def run_path(args, world, rank, local):
+    """One JSON line for a secondary workload: the adjoint, the batched launch,
+    a treecode preset or the NUFFT.  Same timing rules as the headline
+    (device-resident input, CUDA events on the launching stream, L2 flushed
+    between steps, max over ranks); e2e goes through the host-pointer entry
+    point; the CPU baseline is the oracle's restatement of the reference's
+    parallel route on a bounded sample."""
+    import ctypes as C
+    import torch
+    from shrinkers_b200 import _native, spectra
+    from oracle import oracle as O
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    L = _native.load()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    prec = {"mixed": 1, "f64": 0}[args.precision]
+    wl = args.workload
+    p = args.p
+    _D = C.POINTER(C.c_double)
+    _I64 = C.POINTER(C.c_int64)
+
+    def dptr(t):
+        return C.cast(t.data_ptr(), _D)
+
+    roof = None
+    if wl == "adjoint":
+        ev_h = spectra.config5(p, seed=5 + rank)
+        eta = 1.0 / math.sqrt(p)
+        ev = torch.from_numpy(ev_h).to(dev)
+        g = torch.randn(2, p, dtype=torch.float64, device=dev,
+                        generator=torch.Generator(device=dev).manual_seed(5 + rank))
+        out = torch.empty(p, dtype=torch.float64, device=dev)
+        units = float(p) * p
+        family = b"adjoint_mixed" if prec == 1 else b"adjoint_f64"
+        desc = f"adjoint of the all-points transform, MP(c=0.3)+5 spikes p={p}, eta=1/sqrt(p)"
+
+        def step():
+            _native.check(L.shrk_stieltjes_adjoint_dev(ev.data_ptr(), p, eta, g[0].data_ptr(),
+                                                       g[1].data_ptr(), prec, out.data_ptr(), sp))
+        gh = g.cpu().pin_memory()
+        evp = torch.from_numpy(ev_h).pin_memory()
+        oh = torch.empty(p, dtype=torch.float64).pin_memory()
+
+        def e2e():
+            _native.check(L.shrk_stieltjes_adjoint(dptr(evp), p, eta, dptr(gh[0]), dptr(gh[1]),
+                                                   prec, dptr(oh)))
+        io = (24 * p, 8 * p)
+
+        def cpu():
+            w, v = gh[0].numpy(), gh[1].numpy()
+            t0 = time.perf_counter()
+            O.adjoint_direct(ev_h, eta, w, v)
+            dt = time.perf_counter() - t0
+            return float(p) * p / dt, f"direct-sum gradient at all {p} points, {dt:.2f} s"
+    elif wl == "batched":
+        vals, offs, etas = spectra.config4(n_spectra=args.spectra, seed=4 + rank)
+        n = offs.size - 1
+        bv = torch.from_numpy(vals).to(dev)
+        bo = torch.from_numpy(offs).to(dev)
+        be = torch.from_numpy(etas).to(dev)
+        br = torch.empty_like(bv)
+        bi = torch.empty_like(bv)
+        units = float(np.sum(np.diff(offs).astype(np.float64) ** 2))
+        family = b"batched"
+        desc = (f"batched exact transform, {n} spectra, p log-uniform in [256, 16384], "
+                f"eta=1/sqrt(p) per spectrum, {args.precision} kernel")
+
+        def step():
+            _native.check(L.shrk_stieltjes_batched_dev(bv.data_ptr(), bo.data_ptr(), n,
+                                                       be.data_ptr(), prec, br.data_ptr(),
+                                                       bi.data_ptr(), sp))
+        vp = torch.from_numpy(vals).pin_memory()
+        op = torch.from_numpy(offs).pin_memory()
+        ep = torch.from_numpy(etas).pin_memory()
+        rp = torch.empty(vals.size, dtype=torch.float64).pin_memory()
+        ip = torch.empty(vals.size, dtype=torch.float64).pin_memory()
+
+        def e2e():
+            _native.check(L.shrk_stieltjes_batched(dptr(vp), C.cast(op.data_ptr(), _I64), n,
+                                                   dptr(ep), prec, dptr(rp), dptr(ip)))
+        io = (8 * vals.size + 8 * (n + 1) + 8 * n, 16 * vals.size)
+
+        def cpu():
+            pairs, t0 = 0.0, time.perf_counter()
+            for s_ in range(0, n, max(1, n // 64)):
+                a = vals[offs[s_]:offs[s_ + 1]]
+                O.compute_all(a, float(etas[s_]), "blocked", parallel=True)
+                pairs += float(a.size) ** 2
+            dt = time.perf_counter() - t0
+            return pairs / dt, f"every {max(1, n // 64)}th spectrum, {dt:.2f} s"
+    else:
+        ev_h = spectra.config3(p, seed=3 + rank)
+        eta = 1.0 / math.sqrt(p)
+        ev = torch.from_numpy(ev_h).to(dev)
+        xr = torch.empty(p, dtype=torch.float64, device=dev)
+        xi = torch.empty_like(xr)
+        mid = METHOD_IDS[wl]
+        units = float(p) * p
+        family = b"nufft_splat" if wl == "nufft" else (
+            b"cheb_eval_f32" if wl == "chebcode_fast" else b"cheb_eval_f64")
+        desc = (f"{wl} all-points transform (tree build / grid included), MP(c=0.1)+20 spikes "
+                f"in [3,50] p={p}, eta=1/sqrt(p)")
+
+        def step():
+            _native.check(L.shrk_stieltjes_all_dev(ev.data_ptr(), p, eta, mid, 0, float("nan"),
+                                                   0, xr.data_ptr(), xi.data_ptr(), sp))
+        evp = torch.from_numpy(ev_h).pin_memory()
+        rp = torch.empty(p, dtype=torch.float64).pin_memory()
+        ip = torch.empty(p, dtype=torch.float64).pin_memory()
+
+        def e2e():
+            _native.check(L.shrk_stieltjes_all(dptr(evp), p, eta, mid, 0, float("nan"), 0,
+                                               dptr(rp), dptr(ip)))
+        io = (8 * p, 16 * p)
+
+        def cpu():
+            t0 = time.perf_counter()
+            if wl == "nufft":
+                O.nufft_points(ev_h, ev_h, eta, parallel=True)
+            else:
+                th, nn_, leaf, f32 = CHEB_PRESETS[wl]
+                O.chebcode_points(ev_h, ev_h, eta, th, nn_, leaf, f32, parallel=True)
+            dt = time.perf_counter() - t0
+            return units / dt, f"full transform (tree build / grid included), {dt:.2f} s"
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    L.shrk_timing_reset()
+    L.shrk_timing_enable(1)
+    clocks = ClockSampler(local)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = int(L.shrk_launch_count())
+    L.shrk_timing_enable(0)
+    kn, kms = C.c_int64(), C.c_double()
+    L.shrk_timing_read(family, C.byref(kn), C.byref(kms))
+    total_ms = float(np.sum(times))
+    if pg:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    value = world * units / (ms * 1e-3)
+    e2e()
+    te = []
+    for _ in range(max(2, min(args.steps, 5))):
+        t0 = time.perf_counter()
+        e2e()
+        te.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(te))
+    if pg:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    cpu_line = None
+    if rank == 0:
+        k_s = kms.value / max(kn.value, 1) * 1e-3
+        if wl in ("adjoint", "batched") and kn.value:
+            f32r, f64r = C.c_double(), C.c_double()
+            _native.check(L.shrk_measure_pipe_rates(C.byref(f32r), C.byref(f64r)))
+            # adjoint: 15 ops per unordered pair = 7.5 per ordered pair
+            ops = (7.5 if wl == "adjoint" else (6.0 if prec == 1 else 7.0))
+            peak = f32r.value if prec == 1 else f64r.value
+            ach = units * ops / k_s
+            roof = {"bound": "fp32" if prec == 1 else "fp64", "achieved": ach / 1e12,
+                    "peak": peak / 1e12, "unit": "Tops/s", "frac": ach / peak, "traffic": None,
+                    "kernel": family.decode(), "kernel_ms": k_s * 1e3,
+                    "basis": f"{ops:g} pipe lane-ops per pair evaluation; peak = measured FMA "
+                             "lane-op rate of this GPU"}
+        elif wl == "nufft" and kn.value:
+            m = 65536
+            alg = 8 * p + 4 * 16 * m  # splat: read sources, write the grid
+            roof = {"bound": "hbm", "achieved": alg / k_s / 1e9,
+                    "peak": _measured_hbm(), "unit": "GB/s",
+                    "frac": alg / k_s / 1e9 / _measured_hbm(), "traffic": None,
+                    "kernel": "nufft_splat", "kernel_ms": k_s * 1e3,
+                    "basis": "splat: 8 B per source read + 64 B per grid cell written"}
+        rate, sample = cpu()
+        cpu_line = {"value": rate, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                    "sample": sample}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": ("f32+f64" if prec == 1 else "f64")
+        if wl in ("adjoint", "batched") else ("f32+f64" if wl == "chebcode_fast" else "f64"),
+        "data": "synthetic",
+        "config": {"workload": desc, "p": p if wl != "batched" else None,
+                   "l2": "flushed between timed iterations (256 MiB)",
+                   "parallelism": f"{world} GPU(s), one workload per GPU",
+                   "units": "pair evaluations (effective p^2 for the treecode and NUFFT)"},
+        "roofline": roof, "cpu_baseline": cpu_line,
+        "e2e": {"value": world * units / e2e_s, "unit": UNIT, "h2d_bytes_per_step": io[0],
+                "d2h_bytes_per_step": io[1], "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _measured_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        for k in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if k in d:
+                return float(d[k])
+    except (OSError, ValueError):
+        pass
+    return 6650.0
+
+
 def secondary(args, L, dev, ev, ev_h, eta, p, stream):
     """FP64 vs mixed at p (speed + error), p = 50k both kernels, the forward +
-    adjoint cost at p = 20k and 200k, and the batched launch on 4096 uneven
-    spectra."""
+    adjoint cost at p = 20k and 200k, the batched launch on 4096 uneven
+    spectra, and the treecode presets and NUFFT at p = 1M."""
     import torch
     from shrinkers_b200 import _native, spectra
 
@@ -415,14 +669,45 @@ def secondary(args, L, dev, ev, ev_h, eta, p, stream):
             stream.cuda_stream)), 3)
         out[f"batched_{name}_ms"] = b_ms
         out[f"batched_{name}_pairs_per_s"] = out["batched_pairs"] / (b_ms * 1e-3)
+    # treecode presets and NUFFT at p = 1M (MP c = 0.1 + 20 spikes in [3, 50]),
+    # eta = 1/sqrt(p): whole call on device-resident input (tree build
+    # included), error vs the FP64 exact kernel
+    p5 = 1_000_000
+    ev5 = torch.from_numpy(spectra.config3(p5)).to(dev)
+    e5 = 1.0 / math.sqrt(p5)
+    x5r = torch.empty(p5, dtype=torch.float64, device=dev)
+    x5i = torch.empty_like(x5r)
+    run(0, x5r, x5i, ev5, p5, e5)
+    ex5 = torch.complex(x5r, x5i)
+    for name, mid in [("chebcode_fast", 14), ("chebcode", 13), ("chebcode_xtreme", 15),
+                      ("nufft", 11)]:
+        def call(mid=mid):
+            _native.check(L.shrk_stieltjes_all_dev(ev5.data_ptr(), p5, e5, mid, 0, float("nan"), 0,
+                                                   x5r.data_ptr(), x5i.data_ptr(),
+                                                   stream.cuda_stream))
+        ms = timed(call, 5)
+        rel = torch.abs(torch.complex(x5r, x5i) - ex5) / torch.abs(ex5)
+        out[f"p1m_{name}_ms"] = ms
+        out[f"p1m_{name}_rel_err_median"] = float(rel.median())
     return out
 
 
 def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
+    if args.p is None:
+        args.p = {"adjoint": 20_000}.get(args.workload, 1_000_000)
     if args.impl == "reference":
+        if args.workload != "exact":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference arm times the headline workload only; "
+                                  "secondary workload lines carry their own cpu_baseline"}))
+            return
         run_reference(args, world, rank)
+        return
+    if args.workload != "exact":
+        run_path(args, world, rank, local)
         return
     run_ours(args, world, rank, local)
 

@@ -151,8 +151,10 @@ shrk_status shrk_stieltjes_batched_dev(const double* d_ev, const int64_t* d_offs
  * (targets per thread R in {2,4}, source split SL in {1024,...,8192}) on a
  * synthetic batch of that bucket and keeps the fastest; table receives
  * (R, SL) per bucket, 16 ints.  Runs once per device and precision (the
- * first batched call runs it implicitly), again when force != 0.  Spectra
- * of the batched entry points hold at most 16 777 216 values each. */
+ * first batched call runs it implicitly, unless the environment variable
+ * SHRK_BATCHED_AUTOTUNE=0 selects the fixed default table), again when
+ * force != 0.  Spectra of the batched entry points hold at most 16 777 216
+ * values each. */
 shrk_status shrk_batched_autotune(int precision, int force, int32_t* table);
 
 /* Adjoint of m(z_j) = (1/p) sum_i 1/(ev_i - z_j), z_j = ev_j + i*eta (the

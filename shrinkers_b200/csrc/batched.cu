@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -433,7 +434,17 @@ shrk_status batched(const double* d_ev, const int64_t* d_offsets, const int64_t*
     return SHRK_EINVAL;
   }
   Tune& t = g_tune[dev][precision];
-  if (!t.tuned) SHRK_TRY(autotune(precision, t, s));
+  if (!t.tuned) {
+    // SHRK_BATCHED_AUTOTUNE=0: keep the default table (plans, and so the
+    // split summation order, then do not depend on timing).
+    const char* env = std::getenv("SHRK_BATCHED_AUTOTUNE");
+    if (env && std::strcmp(env, "0") == 0) {
+      default_tune(t);
+      t.tuned = true;
+    } else {
+      SHRK_TRY(autotune(precision, t, s));
+    }
+  }
 
   // Replay the cached graph when the plan (offsets, precision, tuning) and
   // every buffer it references are unchanged.
