@@ -166,6 +166,17 @@ shrk_status shrk_stieltjes_adjoint(const double* ev, size_t p, double eta, const
 shrk_status shrk_stieltjes_adjoint_dev(const double* d_ev, size_t p, double eta,
                                        const double* d_g_re, const double* d_g_im, int precision,
                                        double* d_grad, void* stream);
+/* The same gradient with every source sum evaluated by the ChebCode tree of
+ * `method` (CHEBCODE, CHEBCODE_FAST, CHEBCODE_XTREME, CHEBCODE_BALANCED:
+ * the presets of chebcode.rs:926-998; no reference counterpart): leaves are
+ * summed exactly, accepted nodes through Chebyshev node weights of the
+ * charges 1, g_re and g_im.  FP64 throughout. */
+shrk_status shrk_stieltjes_adjoint_treecode(const double* ev, size_t p, double eta,
+                                            const double* g_re, const double* g_im, int method,
+                                            double* grad);
+shrk_status shrk_stieltjes_adjoint_treecode_dev(const double* d_ev, size_t p, double eta,
+                                                const double* d_g_re, const double* d_g_im,
+                                                int method, double* d_grad, void* stream);
 
 /* ------------------------------------------------------- consumers -- */
 /* shrinkage.rs:22-34 shrinkage_factor (pure host arithmetic). */

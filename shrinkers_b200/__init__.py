@@ -278,10 +278,13 @@ def stieltjes_transform_batched(spectra, eta=None, precision="mixed"):
     return [{"real": re[offs[s]:offs[s + 1]], "imag": im[offs[s]:offs[s + 1]]} for s in range(n)]
 
 
-def stieltjes_adjoint(eigenvalues, g_real, g_imag, eta=None, precision="f64"):
+def stieltjes_adjoint(eigenvalues, g_real, g_imag, eta=None, precision="f64", method="exact"):
     """dL/d lambda for L = sum_j Re(conj(g_j) m_j), m_j = (1/p) sum_i 1/(lambda_i - z_j),
     z_j = lambda_j + i eta (eta default 1/sqrt(p)).  Includes the dependence
-    of z_j on lambda_j."""
+    of z_j on lambda_j.  ``method``: "exact" (every pair; ``precision`` f64 or
+    mixed) or a ChebCode preset name ("chebcode", "chebcode_xtreme",
+    "chebcode_balanced", "chebcode_fast"), whose tree evaluates the source
+    sums in FP64."""
     ev = np.ascontiguousarray(np.asarray(eigenvalues, dtype=np.float64))
     gr = np.ascontiguousarray(np.asarray(g_real, dtype=np.float64))
     gi = np.ascontiguousarray(np.asarray(g_imag, dtype=np.float64))
@@ -292,8 +295,12 @@ def stieltjes_adjoint(eigenvalues, g_real, g_imag, eta=None, precision="f64"):
     _require_finite(ev, "eigenvalues")
     eta_v = 1.0 / math.sqrt(ev.size) if eta is None else _require_positive_finite(float(eta), "eta")
     grad = np.empty(ev.size)
-    st = _lib().shrk_stieltjes_adjoint(_dp(ev), ev.size, eta_v, _dp(gr), _dp(gi), _PREC[precision],
-                                       _dp(grad))
+    if method == "exact":
+        st = _lib().shrk_stieltjes_adjoint(_dp(ev), ev.size, eta_v, _dp(gr), _dp(gi),
+                                           _PREC[precision], _dp(grad))
+    else:
+        st = _lib().shrk_stieltjes_adjoint_treecode(_dp(ev), ev.size, eta_v, _dp(gr), _dp(gi),
+                                                    parse_method(method), _dp(grad))
     _native.check(st, "stieltjes_adjoint")
     return grad
 

@@ -1,15 +1,19 @@
 """PyTorch autograd over the GPU transform and its hand-written adjoint.
 
-``stieltjes_m(ev, eta=None, precision="f64")`` returns
+``stieltjes_m(ev, eta=None, precision="f64", method="exact")`` returns
 
     m_j = (1/p) sum_i 1/(ev_i - z_j),   z_j = ev_j + i*eta,
 
 as a complex128 CUDA tensor, differentiable with respect to ``ev``
-(including the dependence of z_j on ev_j).  The forward pass is the exact
-all-points kernel (``shrk_stieltjes_all_dev``; m = -conj(S)/p in terms of
+(including the dependence of z_j on ev_j).  The forward pass is the
+all-points transform (``shrk_stieltjes_all_dev``; m = -conj(S)/p in terms of
 the reference's raw sum S(x) = sum_i 1/((x - ev_i) - i*eta), term.rs:26-31);
 the backward pass is the adjoint kernel (``shrk_stieltjes_adjoint_dev``),
-which recomputes the pair terms instead of storing them.  Both run on the
+which recomputes the pair terms instead of storing them.  With a ChebCode
+preset as ``method`` both passes use that preset's tree (forward:
+``shrk_stieltjes_all_dev`` with the preset; backward:
+``shrk_stieltjes_adjoint_treecode_dev``); the gradient is then the treecode
+evaluation of the exact adjoint, to the preset's accuracy.  Both run on the
 caller's current CUDA stream with device pointers: no host copies.
 
 For a real loss L, PyTorch hands backward the cotangent
@@ -28,6 +32,7 @@ from . import _native
 
 _PREC = {"f64": 0, "mixed": 1}
 _BLOCKED = 2  # StieltjesMethod::Blocked
+_CHEB = {"chebcode": 13, "chebcode_fast": 14, "chebcode_xtreme": 15, "chebcode_balanced": 16}
 
 
 def _check_input(ev: torch.Tensor) -> None:
@@ -45,21 +50,23 @@ class StieltjesTransform(torch.autograd.Function):
     """m(z_j) at z_j = ev_j + i*eta for every j (see the module docstring)."""
 
     @staticmethod
-    def forward(ctx, ev: torch.Tensor, eta: float, precision: str):
+    def forward(ctx, ev: torch.Tensor, eta: float, precision: str, method: str = "exact"):
         L = _native.load()
         prec = _PREC[precision]
+        mid = _BLOCKED if method == "exact" else _CHEB[method]
         ev_c = ev.detach().contiguous()
         p = ev_c.numel()
         re = torch.empty_like(ev_c)
         im = torch.empty_like(ev_c)
         with torch.cuda.device(ev_c.device):
             stream = torch.cuda.current_stream(ev_c.device).cuda_stream
-            st = L.shrk_stieltjes_all_dev(ev_c.data_ptr(), p, eta, _BLOCKED, prec, float("nan"), 0,
+            st = L.shrk_stieltjes_all_dev(ev_c.data_ptr(), p, eta, mid, prec, float("nan"), 0,
                                           re.data_ptr(), im.data_ptr(), stream)
         _native.check(st, "stieltjes_all_dev")
         ctx.save_for_backward(ev_c)
         ctx.eta = eta
         ctx.prec = prec
+        ctx.method = mid
         # S/p -> m = -conj(S)/p
         return torch.complex(-re, im)
 
@@ -73,18 +80,28 @@ class StieltjesTransform(torch.autograd.Function):
         grad = torch.empty_like(ev)
         with torch.cuda.device(ev.device):
             stream = torch.cuda.current_stream(ev.device).cuda_stream
-            st = L.shrk_stieltjes_adjoint_dev(ev.data_ptr(), ev.numel(), ctx.eta, g_re.data_ptr(),
-                                              g_im.data_ptr(), ctx.prec, grad.data_ptr(), stream)
+            if ctx.method == _BLOCKED:
+                st = L.shrk_stieltjes_adjoint_dev(ev.data_ptr(), ev.numel(), ctx.eta,
+                                                  g_re.data_ptr(), g_im.data_ptr(), ctx.prec,
+                                                  grad.data_ptr(), stream)
+            else:
+                st = L.shrk_stieltjes_adjoint_treecode_dev(ev.data_ptr(), ev.numel(), ctx.eta,
+                                                           g_re.data_ptr(), g_im.data_ptr(),
+                                                           ctx.method, grad.data_ptr(), stream)
         _native.check(st, "stieltjes_adjoint_dev")
-        return grad, None, None
+        return grad, None, None, None
 
 
-def stieltjes_m(ev: torch.Tensor, eta: float | None = None, precision: str = "f64") -> torch.Tensor:
-    """Differentiable m(z_j), z_j = ev_j + i*eta (eta default 1/sqrt(p))."""
+def stieltjes_m(ev: torch.Tensor, eta: float | None = None, precision: str = "f64",
+                method: str = "exact") -> torch.Tensor:
+    """Differentiable m(z_j), z_j = ev_j + i*eta (eta default 1/sqrt(p));
+    method "exact" or a ChebCode preset name."""
     _check_input(ev)
     if precision not in _PREC:
         raise ValueError(f"unknown precision '{precision}' (expected 'f64' or 'mixed')")
+    if method != "exact" and method not in _CHEB:
+        raise ValueError(f"unknown method '{method}' (expected 'exact' or a chebcode preset)")
     eta_v = 1.0 / math.sqrt(ev.numel()) if eta is None else float(eta)
     if not (math.isfinite(eta_v) and eta_v > 0.0):
         raise ValueError("eta must be a positive finite number")
-    return StieltjesTransform.apply(ev, eta_v, precision)
+    return StieltjesTransform.apply(ev, eta_v, precision, method)

@@ -694,6 +694,47 @@ shrk_status shrk_stieltjes_adjoint_dev(const double* d_ev, size_t p, double eta,
   return adjoint(d_ev, (int64_t)p, eta, d_gre, d_gim, precision, d_grad, s);
 }
 
+static shrk_status check_cheb_method(int method, ChebParams* prm) {
+  if (!is_cheb(method) || !cheb_preset(method, prm))
+    return einval("the treecode adjoint takes a ChebCode method (chebcode, chebcode_fast, "
+                  "chebcode_xtreme, chebcode_balanced)");
+  return SHRK_OK;
+}
+
+shrk_status shrk_stieltjes_adjoint_treecode_dev(const double* d_ev, size_t p, double eta,
+                                                const double* d_gre, const double* d_gim,
+                                                int method, double* d_grad, void* stream) {
+  SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, SHRK_PREC_F64));
+  ChebParams prm;
+  SHRK_TRY(check_cheb_method(method, &prm));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
+  return chebcode_adjoint(d_ev, (int64_t)p, eta, d_gre, d_gim, prm, d_grad, s);
+}
+
+shrk_status shrk_stieltjes_adjoint_treecode(const double* ev, size_t p, double eta,
+                                            const double* g_re, const double* g_im, int method,
+                                            double* grad) {
+  SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, SHRK_PREC_F64));
+  ChebParams prm;
+  SHRK_TRY(check_cheb_method(method, &prm));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * 3 * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * p, &out));
+  double* d = (double*)dev;
+  SHRK_TRY(h2d(d, ev, sizeof(double) * p, s));
+  SHRK_TRY(h2d(d + p, g_re, sizeof(double) * p, s));
+  SHRK_TRY(h2d(d + 2 * p, g_im, sizeof(double) * p, s));
+  SHRK_TRY(chebcode_adjoint(d, (int64_t)p, eta, d + p, d + 2 * p, prm, (double*)out, s));
+  SHRK_TRY(d2h(grad, out, sizeof(double) * p, s));
+  return check_device_error(s);
+}
+
 shrk_status shrk_stieltjes_adjoint(const double* ev, size_t p, double eta, const double* g_re,
                                    const double* g_im, int precision, double* grad) {
   SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, precision));

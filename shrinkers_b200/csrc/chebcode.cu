@@ -90,12 +90,11 @@ struct BuildArrays {
   int32_t* size;
   int32_t* pre;  // pre-order index
   int* counter;  // next free BFS slot
+  int* levels;   // level L = BFS slots [levels[2L], levels[2L+1])
 };
 
-__global__ void tree_split_kernel(const double* __restrict__ sorted, BuildArrays b, int begin,
-                                  int end, int depth, int64_t leaf_cap) {
-  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= end) return;
+__device__ __forceinline__ void tree_split_node(const double* __restrict__ sorted, BuildArrays b,
+                                                int i, int depth, int64_t leaf_cap) {
   const int64_t lo_idx = b.blo[i], hi_idx = b.bhi[i];
   if (hi_idx - lo_idx <= leaf_cap || depth >= MAX_TREE_DEPTH) {
     b.lc[i] = b.rc[i] = -1;
@@ -119,6 +118,23 @@ __global__ void tree_split_kernel(const double* __restrict__ sorted, BuildArrays
   b.lc[i] = slot;
   b.rc[i] = slot + 1;
 }
+
+// Splits the nodes of level `depth` (its slot range read from b.levels, so
+// successive levels launch without host round trips).
+__global__ void tree_split_kernel(const double* __restrict__ sorted, BuildArrays b, int depth,
+                                  int64_t leaf_cap) {
+  const int begin = b.levels[2 * depth], end = b.levels[2 * depth + 1];
+  for (int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x); i < end;
+       i += (int)(gridDim.x * blockDim.x))
+    tree_split_node(sorted, b, i, depth, leaf_cap);
+}
+
+// The next level holds exactly the children allocated while splitting this one.
+__global__ void tree_level_advance_kernel(BuildArrays b, int depth) {
+  b.levels[2 * depth + 2] = b.levels[2 * depth + 1];
+  b.levels[2 * depth + 3] = *b.counter;
+}
+
 
 __global__ void tree_size_kernel(BuildArrays b, int begin, int end) {
   const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -162,8 +178,11 @@ __global__ void tree_fill_kernel(const double* __restrict__ sorted, BuildArrays 
   for (int j = 0; j < k.n; ++j) f.nodes[(int64_t)idx * k.n + j] = c + l * k.sm1[j];
 }
 
-__global__ void tree_p2m_kernel(const double* __restrict__ sorted, BuildArrays b, int nn,
-                                FlatTree f, ChebConsts k) {
+// charges: per sorted source (null = unit masses, the reference's P2M);
+// wout: the node-weight array [nn][n] to fill.
+__global__ void tree_p2m_kernel(const double* __restrict__ sorted,
+                                const double* __restrict__ charges, BuildArrays b, int nn,
+                                FlatTree f, double* wout, ChebConsts k) {
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= nn || b.lc[i] >= 0) return;
   const int idx = b.pre[i];
@@ -172,11 +191,13 @@ __global__ void tree_p2m_kernel(const double* __restrict__ sorted, BuildArrays b
     t[j] = f.nodes[(int64_t)idx * k.n + j];
     w[j] = 0.0;
   }
-  for (int64_t q = b.blo[i]; q < b.bhi[i]; ++q) bary_row_dev(sorted[q], t, k, w, 1.0);
-  for (int j = 0; j < k.n; ++j) f.w[(int64_t)idx * k.n + j] = w[j];
+  for (int64_t q = b.blo[i]; q < b.bhi[i]; ++q)
+    bary_row_dev(sorted[q], t, k, w, charges ? charges[q] : 1.0);
+  for (int j = 0; j < k.n; ++j) wout[(int64_t)idx * k.n + j] = w[j];
 }
 
-__global__ void tree_m2m_kernel(BuildArrays b, int begin, int end, FlatTree f, ChebConsts k) {
+__global__ void tree_m2m_kernel(BuildArrays b, int begin, int end, FlatTree f, double* wts,
+                                ChebConsts k) {
   const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= end || b.lc[i] < 0) return;
   const int idx = b.pre[i];
@@ -188,11 +209,11 @@ __global__ void tree_m2m_kernel(BuildArrays b, int begin, int end, FlatTree f, C
   const int kids[2] = {b.pre[b.lc[i]], b.pre[b.rc[i]]};
   for (int c = 0; c < 2; ++c)
     for (int ti = 0; ti < k.n; ++ti) {
-      const double m = f.w[(int64_t)kids[c] * k.n + ti];
+      const double m = wts[(int64_t)kids[c] * k.n + ti];
       if (m == 0.0) continue;
       bary_row_dev(f.nodes[(int64_t)kids[c] * k.n + ti], t, k, w, m);
     }
-  for (int j = 0; j < k.n; ++j) f.w[(int64_t)idx * k.n + j] = w[j];
+  for (int j = 0; j < k.n; ++j) wts[(int64_t)idx * k.n + j] = w[j];
 }
 
 // ----------------------------------------------------------- device --
@@ -376,6 +397,8 @@ __global__ void tree_init_kernel(BuildArrays b, int64_t ns) {
   b.bhi[0] = ns;
   b.pre[0] = 0;
   *b.counter = 1;
+  b.levels[0] = 0;
+  b.levels[1] = 1;
 }
 
 // F32 mirror of the flat tree for the fast preset (NodeF32 + node panels).
@@ -392,10 +415,38 @@ __global__ void tree_f32_kernel(FlatTree f, int nn, int n, NodeF32* nf, float* p
 
 unsigned blocks_for(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// A built tree: the flat arrays plus what further weight sets need (the
+// breadth-first arrays stay valid in scratch until the next build).
+struct TreeBuild {
+  FlatTree f;
+  int nn = 0;
+  std::vector<int> lb, le;  // breadth-first level ranges
+  BuildArrays b;
+  ChebConsts k;
+};
+
+// Node weights of `charges` (per sorted source; null = unit masses) into
+// wout: P2M at the leaves, then M2M from the deepest internal level up.
+shrk_status tree_weights(const TreeBuild& tb, const double* d_sorted, const double* charges,
+                         double* wout, cudaStream_t s) {
+  tree_p2m_kernel<<<blocks_for(tb.nn, 128), 128, 0, s>>>(d_sorted, charges, tb.b, tb.nn, tb.f,
+                                                          wout, tb.k);
+  SHRK_CUDA(cudaGetLastError());
+  const int levels = (int)tb.lb.size();
+  for (int L = levels - 2; L >= 0; --L) {
+    tree_m2m_kernel<<<blocks_for(tb.le[L] - tb.lb[L], 128), 128, 0, s>>>(tb.b, tb.lb[L], tb.le[L],
+                                                                       tb.f, wout, tb.k);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  add_launches(1 + std::max(levels - 1, 0));
+  return SHRK_OK;
+}
+
 // Builds the flat tree of d_sorted (ascending) into the TREE_SLOTS scratch.
 // Scratch slots 25/26 hold the breadth-first build arrays.
 shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams& prm,
-                           FlatTree& f, int& nn_out, cudaStream_t s) {
+                           TreeBuild& tb, cudaStream_t s) {
+  FlatTree& f = tb.f;
   const int64_t cap = std::max<int64_t>(2 * ns, 2);
   if (cap > (int64_t)INT32_MAX / 2) {
     set_error("chebcode: too many eigenvalues for the tree build");
@@ -411,7 +462,8 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   void* p64 = nullptr;
   void* p32 = nullptr;
   SHRK_TRY(scratch_get(25, sizeof(int64_t) * 2 * (size_t)cap, &p64));
-  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (4 * (size_t)cap + 64), &p32));
+  constexpr int NLEV = MAX_TREE_DEPTH + 2;  // levels 0..48 split, level 49 is empty
+  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (4 * (size_t)cap + 8 + 2 * NLEV), &p32));
   BuildArrays b;
   b.blo = (int64_t*)p64;
   b.bhi = b.blo + cap;
@@ -420,26 +472,42 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   b.size = b.rc + cap;
   b.pre = b.size + cap;
   b.counter = (int*)(b.pre + cap);
+  b.levels = b.counter + 8;
   constexpr int BS = 256;
   {
     LaunchScope ls("cheb_build", s);
     tree_init_kernel<<<1, 1, 0, s>>>(b, ns);
     SHRK_CUDA(cudaGetLastError());
   }
-  // 1. split, level by level (each level's children fill the next slots)
-  std::vector<int> lb{0}, le{1};
-  for (int depth = 0;; ++depth) {
-    const int begin = lb.back(), end = le.back();
-    tree_split_kernel<<<blocks_for(end - begin, BS), BS, 0, s>>>(d_sorted, b, begin, end, depth,
-                                                                  (int64_t)prm.leaf_cap);
-    SHRK_CUDA(cudaGetLastError());
-    add_launches(1);
-    int next = 0;
-    SHRK_CUDA(cudaMemcpyAsync(&next, b.counter, sizeof(int), cudaMemcpyDeviceToHost, s));
+  // 1. split, level by level (each level's children fill the next slots);
+  //    levels run in batches of 8 with one read-back of the level table per
+  //    batch to see whether a level came out empty.
+  const int split_grid = std::max(1, sm_count() * 4);
+  int h_lev[2 * NLEV];
+  int last = -1;  // first empty level
+  for (int L0 = 0; last < 0;) {
+    const int L1 = std::min(L0 + 8, NLEV - 1);
+    for (int L = L0; L < L1; ++L) {
+      tree_split_kernel<<<split_grid, BS, 0, s>>>(d_sorted, b, L, (int64_t)prm.leaf_cap);
+      SHRK_CUDA(cudaGetLastError());
+      tree_level_advance_kernel<<<1, 1, 0, s>>>(b, L);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    add_launches(2 * (L1 - L0));
+    SHRK_CUDA(cudaMemcpyAsync(h_lev, b.levels, sizeof(h_lev), cudaMemcpyDeviceToHost, s));
     SHRK_CUDA(cudaStreamSynchronize(s));
-    if (next == end) break;
-    lb.push_back(end);
-    le.push_back(next);
+    for (int L = L0 + 1; L <= L1; ++L)
+      if (h_lev[2 * L] == h_lev[2 * L + 1]) {
+        last = L;
+        break;
+      }
+    if (last < 0 && L1 == NLEV - 1) last = L1;  // cannot happen: depth 48 never splits
+    L0 = L1;
+  }
+  std::vector<int> lb, le;
+  for (int L = 0; L < last; ++L) {
+    lb.push_back(h_lev[2 * L]);
+    le.push_back(h_lev[2 * L + 1]);
   }
   const int nn = le.back();
   const int levels = (int)lb.size();
@@ -470,16 +538,109 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   tree_fill_kernel<<<blocks_for(nn, BS), BS, 0, s>>>(d_sorted, b, nn, f, k,
                                                      prm.theta * prm.theta);
   SHRK_CUDA(cudaGetLastError());
+  add_launches(1);
+  tb.nn = nn;
+  tb.lb = lb;
+  tb.le = le;
+  tb.b = b;
+  tb.k = k;
   // 4. P2M at the leaves; 5. M2M from the deepest internal level up
-  tree_p2m_kernel<<<blocks_for(nn, 128), 128, 0, s>>>(d_sorted, b, nn, f, k);
-  SHRK_CUDA(cudaGetLastError());
-  for (int L = levels - 2; L >= 0; --L) {
-    tree_m2m_kernel<<<blocks_for(le[L] - lb[L], 128), 128, 0, s>>>(b, lb[L], le[L], f, k);
-    SHRK_CUDA(cudaGetLastError());
+  return tree_weights(tb, d_sorted, nullptr, f.w, s);
+}
+
+// ------------------------------------------------ treecode adjoint --
+// Gradient of L = sum_j (w_j Re m_j + v_j Im m_j) (the adjoint of the
+// all-points transform, no reference counterpart) with the source sums of
+// the squared kernel K2(a) = 1/(a - i eta)^2 = (A + iB), a = x_k - y_j,
+//   A = (a^2 - eta^2)/D^2 = r - 2 eta^2 r^2,  B = 2 a eta/D^2,  r = 1/D,
+// evaluated by the same tree: grad_k = (1/p)[w_k Re T1 - Re Tw - v_k Im T1
+// - Im Tv] with T_c = sum_j c_j K2(x_k - y_j) for the charges c = 1, w, v.
+// Leaves sum exactly; an accepted node (the forward's acceptance test)
+// contributes sum_i W^c_i K2(x_k - t_i) with its Chebyshev node weights of
+// charge c (P2M with masses c_j, then M2M).
+struct AdjEvalArgs {
+  const double* x;   // targets = the eigenvalues, caller's order
+  const double* w;   // cotangents, caller's order
+  const double* v;
+  int64_t p;
+  const double* sorted;
+  const double* cw;  // charges in sorted order
+  const double* cv;
+  double eta;
+  DevTreeF64 t;      // t.w: unit-mass node weights
+  const double* ww;  // node weights of charges w
+  const double* wv;  // node weights of charges v
+  double* grad;
+  int* err;
+};
+
+__device__ __forceinline__ void k2_terms(double d, double eta2, double m2e2, double teta,
+                                         double& A, double& B) {
+  const double r = rcp_f64(fma(d, d, eta2));
+  const double r2 = r * r;
+  A = fma(m2e2, r2, r);
+  B = teta * d * r2;
+}
+
+__global__ void __launch_bounds__(128) cheb_adjoint_f64(const AdjEvalArgs a) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.p) return;
+  const DevTreeF64& T = a.t;
+  const int n = T.n;
+  const double x = a.x[k], eta = a.eta, eta2 = eta * eta;
+  const double m2e2 = -2.0 * eta2, teta = 2.0 * eta;
+  int32_t stack[MAX_TREE_DEPTH + 2];
+  int top = 0;
+  stack[top++] = 0;
+  double s1r = 0.0, s1i = 0.0, swr = 0.0, svi = 0.0;
+  while (top > 0) {
+    const int32_t node = stack[--top];
+    const int32_t rt = T.right[node];
+    if (rt < 0) {
+      for (int64_t q = T.lo_idx[node]; q < T.hi_idx[node]; ++q) {
+        double A, B;
+        k2_terms(x - a.sorted[q], eta2, m2e2, teta, A, B);
+        s1r += A;
+        s1i += B;
+        swr = fma(a.cw[q], A, swr);
+        svi = fma(a.cv[q], B, svi);
+      }
+      continue;
+    }
+    const double lo = T.lo[node], hi = T.hi[node];
+    const double cl = fmax(fmax(lo - x, x - hi), 0.0);
+    if (T.accept_hw[node] < fma(cl, cl, eta2)) {
+      const int64_t base = (int64_t)node * n;
+      for (int j = 0; j < n; ++j) {
+        double A, B;
+        k2_terms(x - T.nodes[base + j], eta2, m2e2, teta, A, B);
+        const double w1 = T.w[base + j];
+        s1r = fma(w1, A, s1r);
+        s1i = fma(w1, B, s1i);
+        swr = fma(a.ww[base + j], A, swr);
+        svi = fma(a.wv[base + j], B, svi);
+      }
+    } else {
+      if (top + 2 > MAX_TREE_DEPTH + 2) {  // cannot happen for a depth-capped tree
+        atomicExch(a.err, DEV_ERR_BOUNDS);
+        break;
+      }
+      stack[top++] = rt;
+      stack[top++] = node + 1;
+    }
   }
-  add_launches(2 + std::max(levels - 1, 0));
-  nn_out = nn;
-  return SHRK_OK;
+  a.grad[k] = (a.w[k] * s1r - swr - a.v[k] * s1i - svi) / (double)a.p;
+}
+
+// Charges in sorted order: out[i] = c[perm[i]] (perm null: identity).
+__global__ void gather_charges_kernel(const double* __restrict__ gw, const double* __restrict__ gv,
+                                      const int* __restrict__ perm, int64_t n, double* cw,
+                                      double* cv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t j = perm ? perm[i] : i;
+  cw[i] = gw[j];
+  cv[i] = gv[j];
 }
 
 }  // namespace
@@ -513,9 +674,10 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     set_error("chebcode: interpolation order must be in [2, 16]");
     return SHRK_EINVAL;
   }
-  FlatTree f;
-  int nn = 0;
-  SHRK_TRY(build_tree_gpu(d_sorted_src, ns, prm, f, nn, s));
+  TreeBuild tb;
+  SHRK_TRY(build_tree_gpu(d_sorted_src, ns, prm, tb, s));
+  const FlatTree& f = tb.f;
+  const int nn = tb.nn;
   EvalArgs a;
   a.q = d_q;
   a.nq = nq;
@@ -555,6 +717,62 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     cheb_eval_f32<<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   }
+  return SHRK_OK;
+}
+
+shrk_status chebcode_adjoint(const double* d_ev, int64_t p, double eta, const double* d_gre,
+                             const double* d_gim, const ChebParams& prm, double* d_grad,
+                             cudaStream_t s) {
+  if (p <= 0) return SHRK_OK;
+  if (prm.n < 2 || prm.n > MAX_N) {
+    set_error("chebcode: interpolation order must be in [2, 16]");
+    return SHRK_EINVAL;
+  }
+  const double* ds = nullptr;
+  const int* perm = nullptr;
+  SHRK_TRY(sorted_sources_perm(d_ev, p, &ds, &perm, s));
+  // Scratch slot 30: the charges in sorted order; slot 31: their node weights.
+  void* q = nullptr;
+  SHRK_TRY(scratch_get(30, sizeof(double) * 2 * (size_t)p, &q));
+  double* cw = (double*)q;
+  double* cv = cw + p;
+  {
+    LaunchScope ls("cheb_build", s);
+    gather_charges_kernel<<<blocks_for(p, 256), 256, 0, s>>>(d_gre, d_gim, perm, p, cw, cv);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  TreeBuild tb;
+  SHRK_TRY(build_tree_gpu(ds, p, prm, tb, s));
+  SHRK_TRY(scratch_get(31, sizeof(double) * 2 * (size_t)tb.nn * prm.n, &q));
+  double* ww = (double*)q;
+  double* wv = ww + (size_t)tb.nn * prm.n;
+  SHRK_TRY(tree_weights(tb, ds, cw, ww, s));
+  SHRK_TRY(tree_weights(tb, ds, cv, wv, s));
+  AdjEvalArgs a;
+  a.x = d_ev;
+  a.w = d_gre;
+  a.v = d_gim;
+  a.p = p;
+  a.sorted = ds;
+  a.cw = cw;
+  a.cv = cv;
+  a.eta = eta;
+  a.t.lo = tb.f.lo;
+  a.t.hi = tb.f.hi;
+  a.t.accept_hw = tb.f.accept_hw;
+  a.t.lo_idx = tb.f.lo_idx;
+  a.t.hi_idx = tb.f.hi_idx;
+  a.t.right = tb.f.right;
+  a.t.nodes = tb.f.nodes;
+  a.t.w = tb.f.w;
+  a.t.n = prm.n;
+  a.ww = ww;
+  a.wv = wv;
+  a.grad = d_grad;
+  a.err = device_error_word();
+  LaunchScope ls("cheb_adjoint", s);
+  cheb_adjoint_f64<<<blocks_for(p, 128), 128, 0, s>>>(a);
+  SHRK_CUDA(cudaGetLastError());
   return SHRK_OK;
 }
 

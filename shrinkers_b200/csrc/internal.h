@@ -97,6 +97,16 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
 // of d_src in the caller's order (sources.cu).
 shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sorted,
                            double* first, double* last, cudaStream_t s);
+// The same, plus the permutation: d_sorted[i] = d_src[perm[i]]; *d_perm is
+// null when d_src is already sorted (the identity).
+shrk_status sorted_sources_perm(const double* d_src, int64_t ns, const double** d_sorted,
+                                const int** d_perm, cudaStream_t s);
+
+// Treecode adjoint (chebcode.cu): the gradient of shrk_stieltjes_adjoint
+// with every source sum evaluated by the ChebCode tree of preset `prm`.
+shrk_status chebcode_adjoint(const double* d_ev, int64_t p, double eta, const double* d_gre,
+                             const double* d_gim, const ChebParams& prm, double* d_grad,
+                             cudaStream_t s);
 
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);

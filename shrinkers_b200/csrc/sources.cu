@@ -17,11 +17,15 @@ __global__ void unsorted_kernel(const double* __restrict__ src, int64_t n, int* 
   if (i < n && !(src[i - 1] <= src[i])) *flag = 1;
 }
 
-}  // namespace
+__global__ void iota_kernel(int* v, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = (int)i;
+}
 
-// Scratch: slot 27 the flag, slot 8 the sorted copy, slot 28 CUB's temporary.
-shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sorted,
-                           double* first, double* last, cudaStream_t s) {
+// Device-side sortedness check (scratch slot 27 holds the flag) and the
+// first / last entries, read back with one synchronisation.
+shrk_status check_sorted(const double* d_src, int64_t ns, bool* sorted, double* first,
+                         double* last, cudaStream_t s) {
   void* f = nullptr;
   SHRK_TRY(scratch_get(27, 256, &f));
   int* flag = (int*)f;
@@ -36,13 +40,24 @@ shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sor
   SHRK_CUDA(cudaMemcpyAsync(first, d_src, sizeof(double), cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaMemcpyAsync(last, d_src + (ns - 1), sizeof(double), cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
-  if (!h_flag) {
-    *d_sorted = d_src;
-    return SHRK_OK;
-  }
-  if (ns > (int64_t)INT32_MAX) {
+  *sorted = h_flag == 0;
+  if (!*sorted && ns > (int64_t)INT32_MAX) {
     set_error("unsorted input larger than 2^31 values: sort it before the call");
     return SHRK_EINVAL;
+  }
+  return SHRK_OK;
+}
+
+}  // namespace
+
+// Scratch: slot 8 the sorted copy, slot 28 CUB's temporary.
+shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sorted,
+                           double* first, double* last, cudaStream_t s) {
+  bool sorted = true;
+  SHRK_TRY(check_sorted(d_src, ns, &sorted, first, last, s));
+  if (sorted) {
+    *d_sorted = d_src;
+    return SHRK_OK;
   }
   void* out = nullptr;
   SHRK_TRY(scratch_get(8, sizeof(double) * (size_t)ns, &out));
@@ -57,6 +72,42 @@ shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sor
                                              64, s));
   }
   *d_sorted = (const double*)out;
+  return SHRK_OK;
+}
+
+// As sorted_sources, with the source index of every sorted entry (scratch
+// slot 29 holds the identity and the permutation).
+shrk_status sorted_sources_perm(const double* d_src, int64_t ns, const double** d_sorted,
+                                const int** d_perm, cudaStream_t s) {
+  bool sorted = true;
+  double first = 0.0, last = 0.0;
+  SHRK_TRY(check_sorted(d_src, ns, &sorted, &first, &last, s));
+  *d_perm = nullptr;
+  if (sorted) {
+    *d_sorted = d_src;
+    return SHRK_OK;
+  }
+  void* pv = nullptr;
+  SHRK_TRY(scratch_get(29, sizeof(int) * 2 * (size_t)ns, &pv));
+  int* ids = (int*)pv;
+  int* perm = ids + ns;
+  iota_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(ids, ns);
+  SHRK_CUDA(cudaGetLastError());
+  add_launches(1);
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(8, sizeof(double) * (size_t)ns, &out));
+  size_t temp_bytes = 0;
+  SHRK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, d_src, (double*)out, ids, perm,
+                                            (int)ns, 0, 64, s));
+  void* temp = nullptr;
+  SHRK_TRY(scratch_get(28, std::max<size_t>(temp_bytes, 256), &temp));
+  {
+    LaunchScope ls("sources_sort", s);
+    SHRK_CUDA(cub::DeviceRadixSort::SortPairs(temp, temp_bytes, d_src, (double*)out, ids, perm,
+                                              (int)ns, 0, 64, s));
+  }
+  *d_sorted = (const double*)out;
+  *d_perm = perm;
   return SHRK_OK;
 }
 

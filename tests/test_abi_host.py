@@ -191,3 +191,15 @@ def test_non_ndarray_input_is_type_error(rk):
         rk.stieltjes_transform([1.0, 2.0, 3.0])
     with pytest.raises(TypeError):
         rk.stieltjes_transform(np.arange(5, dtype=np.float32))
+
+
+def test_treecode_adjoint_rejects_non_treecode_methods(rk):
+    """The method check runs on the host before any device work."""
+    import ctypes as C
+    L = _native.load()
+    x = np.ones(4)
+    D = C.POINTER(C.c_double)
+    st = L.shrk_stieltjes_adjoint_treecode(x.ctypes.data_as(D), 4, 0.5, x.ctypes.data_as(D),
+                                           x.ctypes.data_as(D), 2, x.ctypes.data_as(D))
+    assert st == _native.SHRK_EINVAL
+    assert "ChebCode" in _native.last_error()
