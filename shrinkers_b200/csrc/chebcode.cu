@@ -63,24 +63,6 @@ struct ChebConsts {
   int n;
 };
 
-// chebcode.rs:309-337 barycentric_row.
-__device__ __forceinline__ void bary_row_dev(double x, const double* t, const ChebConsts& k,
-                                             double* w, double mass) {
-  double v[MAX_N];
-  double s = 0.0;
-  for (int j = 0; j < k.n; ++j) {
-    const double d = x - t[j];
-    if (d == 0.0) {
-      w[j] += mass;
-      return;
-    }
-    const double q = k.lam[j] / d;
-    v[j] = q;
-    s += q;
-  }
-  const double m = mass * (1.0 / s);
-  for (int j = 0; j < k.n; ++j) w[j] = fma(m, v[j], w[j]);
-}
 
 struct BuildArrays {
   int64_t* blo;  // BFS slot -> source index range [blo, bhi)
@@ -178,42 +160,65 @@ __global__ void tree_fill_kernel(const double* __restrict__ sorted, BuildArrays 
   for (int j = 0; j < k.n; ++j) f.nodes[(int64_t)idx * k.n + j] = c + l * k.sm1[j];
 }
 
-// charges: per sorted source (null = unit masses, the reference's P2M);
-// wout: the node-weight array [nn][n] to fill.
+// chebcode.rs:309-337 barycentric_row, one warp wide: lane j < n owns node j
+// and its weight w.  The n divisions run in parallel; s is summed in the
+// sequential order (q_0 + q_1) + q_2 + ... through shuffles, an exact hit goes
+// to the first node with d == 0 (as the sequential loop's break does), and
+// each weight takes the same fma -- the result equals the sequential row bit
+// for bit.
+__device__ __forceinline__ void bary_row_warp(double x, double t, double lam, int n, int lane,
+                                              double& w, double mass) {
+  const double d = x - t;
+  const unsigned hit = __ballot_sync(0xffffffffu, lane < n && d == 0.0);
+  if (hit) {
+    if (lane == __ffs(hit) - 1) w += mass;
+    return;
+  }
+  const double q = lane < n ? lam / d : 0.0;
+  double sum = 0.0;
+  for (int j = 0; j < n; ++j) sum += __shfl_sync(0xffffffffu, q, j);
+  const double m = mass * (1.0 / sum);
+  if (lane < n) w = fma(m, q, w);
+}
+
+// P2M, one warp per leaf.  charges: per sorted source (null = unit masses,
+// the reference's P2M); wout: the node-weight array [nn][n] to fill.
 __global__ void tree_p2m_kernel(const double* __restrict__ sorted,
                                 const double* __restrict__ charges, BuildArrays b, int nn,
                                 FlatTree f, double* wout, ChebConsts k) {
-  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= nn || b.lc[i] >= 0) return;
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= nn || b.lc[i] >= 0) return;  // whole warps leave together
   const int idx = b.pre[i];
-  double t[MAX_N], w[MAX_N];
-  for (int j = 0; j < k.n; ++j) {
-    t[j] = f.nodes[(int64_t)idx * k.n + j];
-    w[j] = 0.0;
-  }
+  const int n = k.n;
+  const double t = lane < n ? f.nodes[(int64_t)idx * n + lane] : 0.0;
+  const double lam = lane < n ? k.lam[lane] : 0.0;
+  double w = 0.0;
   for (int64_t q = b.blo[i]; q < b.bhi[i]; ++q)
-    bary_row_dev(sorted[q], t, k, w, charges ? charges[q] : 1.0);
-  for (int j = 0; j < k.n; ++j) wout[(int64_t)idx * k.n + j] = w[j];
+    bary_row_warp(sorted[q], t, lam, n, lane, w, charges ? charges[q] : 1.0);
+  if (lane < n) wout[(int64_t)idx * n + lane] = w;
 }
 
+// M2M, one warp per internal node of a level: the left then the right
+// child's node masses, in node order.
 __global__ void tree_m2m_kernel(BuildArrays b, int begin, int end, FlatTree f, double* wts,
                                 ChebConsts k) {
-  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= end || b.lc[i] < 0) return;
+  const int i = begin + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= end || b.lc[i] < 0) return;  // whole warps leave together
   const int idx = b.pre[i];
-  double t[MAX_N], w[MAX_N];
-  for (int j = 0; j < k.n; ++j) {
-    t[j] = f.nodes[(int64_t)idx * k.n + j];
-    w[j] = 0.0;
-  }
+  const int n = k.n;
+  const double t = lane < n ? f.nodes[(int64_t)idx * n + lane] : 0.0;
+  const double lam = lane < n ? k.lam[lane] : 0.0;
+  double w = 0.0;
   const int kids[2] = {b.pre[b.lc[i]], b.pre[b.rc[i]]};
   for (int c = 0; c < 2; ++c)
-    for (int ti = 0; ti < k.n; ++ti) {
-      const double m = wts[(int64_t)kids[c] * k.n + ti];
+    for (int ti = 0; ti < n; ++ti) {
+      const double m = wts[(int64_t)kids[c] * n + ti];
       if (m == 0.0) continue;
-      bary_row_dev(f.nodes[(int64_t)kids[c] * k.n + ti], t, k, w, m);
+      bary_row_warp(f.nodes[(int64_t)kids[c] * n + ti], t, lam, n, lane, w, m);
     }
-  for (int j = 0; j < k.n; ++j) wts[(int64_t)idx * k.n + j] = w[j];
+  if (lane < n) wts[(int64_t)idx * n + lane] = w;
 }
 
 // ----------------------------------------------------------- device --
@@ -429,13 +434,13 @@ struct TreeBuild {
 // wout: P2M at the leaves, then M2M from the deepest internal level up.
 shrk_status tree_weights(const TreeBuild& tb, const double* d_sorted, const double* charges,
                          double* wout, cudaStream_t s) {
-  tree_p2m_kernel<<<blocks_for(tb.nn, 128), 128, 0, s>>>(d_sorted, charges, tb.b, tb.nn, tb.f,
-                                                          wout, tb.k);
+  tree_p2m_kernel<<<blocks_for((int64_t)tb.nn * 32, 128), 128, 0, s>>>(d_sorted, charges, tb.b,
+                                                                       tb.nn, tb.f, wout, tb.k);
   SHRK_CUDA(cudaGetLastError());
   const int levels = (int)tb.lb.size();
   for (int L = levels - 2; L >= 0; --L) {
-    tree_m2m_kernel<<<blocks_for(tb.le[L] - tb.lb[L], 128), 128, 0, s>>>(tb.b, tb.lb[L], tb.le[L],
-                                                                       tb.f, wout, tb.k);
+    tree_m2m_kernel<<<blocks_for((int64_t)(tb.le[L] - tb.lb[L]) * 32, 128), 128, 0, s>>>(
+        tb.b, tb.lb[L], tb.le[L], tb.f, wout, tb.k);
     SHRK_CUDA(cudaGetLastError());
   }
   add_launches(1 + std::max(levels - 1, 0));
