@@ -178,7 +178,23 @@ shrk_status shrk_stieltjes_adjoint_treecode_dev(const double* d_ev, size_t p, do
                                                 const double* d_g_re, const double* d_g_im,
                                                 int method, double* d_grad, void* stream);
 
+/* mod.rs:304-319 compute_stieltjes_scaled_ray: RAW sums at z_i = ev_i(1 + i*scale),
+ * i.e. every point has its own eta_i = scale*ev_i.  Exact FP64 pair sums (the
+ * reference takes the exact per-point route for every method here). */
+shrk_status shrk_stieltjes_scaled_ray(const double* ev, size_t p, double scale, double* raw_re,
+                                      double* raw_im);
+shrk_status shrk_stieltjes_scaled_ray_dev(const double* d_ev, size_t p, double scale,
+                                          double* d_re, double* d_im, void* stream);
+
 /* ------------------------------------------------------- consumers -- */
+/* deconvolution/inverse.rs:156-269 inverse_nonlinear_shrinkage (RmtConfig::new:
+ * exact sums): method 0 QIS, 1 LIS, 2 GIS.  precision_ev / covariance_ev hold
+ * p entries in input order; *smoothing receives the bandwidth h; theta and
+ * htheta (p entries each) may be NULL.  Eigenvalues must be strictly positive
+ * and c in (0, 1]. */
+shrk_status shrk_inverse_nonlinear_shrinkage(const double* ev, size_t p, double c, int method,
+                                             double* precision_ev, double* covariance_ev,
+                                             double* smoothing, double* theta, double* htheta);
 /* shrinkage.rs:22-34 shrinkage_factor (pure host arithmetic). */
 double shrk_shrinkage_factor(double lambda, double c, double m_re, double m_im);
 /* estimation.rs:48-56 inverse_bbp; estimation.rs:37-39 bbp_threshold. */

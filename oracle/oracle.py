@@ -86,6 +86,8 @@ def lib():
             "orc_spectral_deconvolution": (C.c_int, [_D, _SZ, C.c_double, _SZ, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, _D]),
             "orc_estimate_population": (C.c_int, [_D, _SZ, C.c_double, C.c_double, C.POINTER(_SZ), _D, _D, _D, _D, _D, _D]),
             "orc_deconvolve_spiked": (C.c_int, [_D, _SZ, C.c_double, _SZ, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.POINTER(_SZ), _D, _D, _D, _D, _D]),
+            "orc_scaled_ray": (None, [_D, _SZ, C.c_double, _D, _D]),
+            "orc_inverse_shrinkage": (None, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -387,3 +389,27 @@ def deconvolve_spiked(ev, c, n_points=200, eta=None, margin=1.0, method="auto", 
     o = out.reshape(7, n_points)
     return dict(k=kk, spikes=sp[:kk].copy(), spike_sample=ss[:kk].copy(), bulk_edge=edge.value,
                 sigma2=s2.value, bulk={key: o[i].copy() for i, key in enumerate(_DECONV_KEYS)})
+
+
+# ------------------------------------------------------- inverse shrinkage --
+def scaled_ray(ev, scale):
+    """compute_stieltjes_scaled_ray (src/stieltjes/mod.rs:304-319): RAW sums at
+    z_i = ev_i (1 + i scale)."""
+    ev = _arr(ev)
+    re, im = np.empty_like(ev), np.empty_like(ev)
+    lib().orc_scaled_ray(_d(ev), ev.size, scale, _d(re), _d(im))
+    return re, im
+
+
+INVERSE_METHODS = {"qis": 0, "lis": 1, "gis": 2}
+
+
+def inverse_shrinkage(ev, c, method="qis"):
+    """inverse_nonlinear_shrinkage (src/deconvolution/inverse.rs:156-269)."""
+    ev = _arr(ev)
+    out = [np.empty_like(ev) for _ in range(4)]
+    h = C.c_double()
+    lib().orc_inverse_shrinkage(_d(ev), ev.size, c, INVERSE_METHODS[method], *[_d(o) for o in out],
+                                C.byref(h))
+    return dict(precision_eigenvalues=out[0], covariance_eigenvalues=out[1], theta=out[2],
+                htheta=out[3], smoothing=h.value)

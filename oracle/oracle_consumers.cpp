@@ -7,6 +7,8 @@
 // (src/deconvolution/population.rs:72-116, hybrid.rs:96-138).
 #include "oracle.h"
 
+#include <cfloat>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -145,6 +147,79 @@ static int spectral_deconvolution(const double* ev, size_t p, double c, size_t n
   return 0;
 }
 
+// mod.rs:304-319 compute_stieltjes_scaled_ray with RmtConfig::new(c)'s
+// Blocked method and no cutoff: stieltjes_sum_for_one -> the autovec sum
+// (mod.rs:244-262, cacheblock.rs:124-134) at z_i = lambda_i (1 + i scale);
+// RAW sums.  The parallel route maps the same per-point sums.
+void scaled_ray(const double* ev, size_t p, double scale, double* re, double* im) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < (long)p; ++i) {
+    const double eta = scale * ev[i];
+    autovec_sum(ev[i], ev, p, eta, &re[i], &im[i]);
+  }
+}
+
+static double safe_reciprocal(double x) {  // inverse.rs safe_reciprocal
+  return (x > 0.0 && std::isfinite(x)) ? 1.0 / x : DBL_MAX;
+}
+
+// deconvolution/inverse.rs:156-269 inverse_nonlinear_shrinkage.
+// method: 0 QIS, 1 LIS, 2 GIS.
+void inverse_shrinkage(const double* ev, size_t p, double c, int method, double* prec,
+                       double* cov, double* theta, double* htheta, double* smoothing) {
+  if (p == 0) {
+    *smoothing = 0.0;
+    return;
+  }
+  const double p_f = (double)p;
+  const double inv_p = 1.0 / p_f;
+  const double h = std::pow(std::min(c * c, 1.0 / (c * c)), 0.35) / std::pow(p_f, 0.35);
+  *smoothing = h;
+  std::vector<double> re(p), im(p), inv_lambda(p), delta(p), omega(p);
+  scaled_ray(ev, p, h, re.data(), im.data());
+  double min_inv = INFINITY, trace = 0.0;
+  for (size_t i = 0; i < p; ++i) {
+    const double li = ev[i];
+    theta[i] = li * re[i] * inv_p;
+    htheta[i] = li * im[i] * inv_p;
+    const double x = 1.0 / li;
+    inv_lambda[i] = x;
+    min_inv = std::min(min_inv, x);
+    trace += li;
+  }
+  const double omc = 1.0 - c;
+  for (size_t i = 0; i < p; ++i) {
+    const double x = inv_lambda[i];
+    const double th = theta[i];
+    const double amp2 = theta[i] * theta[i] + htheta[i] * htheta[i];
+    const double denom = omc * omc * x + 2.0 * c * omc * x * th + c * c * x * amp2;
+    delta[i] = (denom > 0.0 && std::isfinite(denom)) ? 1.0 / denom : ev[i];
+    const double lis = omc * x + 2.0 * c * x * th;
+    omega[i] = lis > min_inv ? lis : min_inv;
+  }
+  if (method == 0) {
+    double sum = 0.0;
+    for (size_t i = 0; i < p; ++i) sum += delta[i];
+    const double scale = (sum > 0.0 && std::isfinite(sum)) ? trace / sum : 1.0;
+    for (size_t i = 0; i < p; ++i) {
+      cov[i] = delta[i] * scale;
+      prec[i] = safe_reciprocal(cov[i]);
+    }
+  } else if (method == 1) {
+    for (size_t i = 0; i < p; ++i) {
+      cov[i] = safe_reciprocal(omega[i]);
+      prec[i] = omega[i];
+    }
+  } else {
+    for (size_t i = 0; i < p; ++i) {
+      const double ratio = omega[i] / delta[i];
+      prec[i] = (ratio > 0.0 && std::isfinite(ratio)) ? std::sqrt(ratio)
+                                                      : safe_reciprocal(ev[i]);
+      cov[i] = safe_reciprocal(prec[i]);
+    }
+  }
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -232,6 +307,15 @@ int orc_deconvolve_spiked(const double* ev, size_t p, double c, size_t n_points,
   }
   return orc_spectral_deconvolution(s.bulk.data(), s.bulk.size(), c, n_points, eta, NAN, NAN,
                                     method, parallel, cutoff, out7);
+}
+
+void orc_scaled_ray(const double* ev, size_t p, double scale, double* re, double* im) {
+  scaled_ray(ev, p, scale, re, im);
+}
+
+void orc_inverse_shrinkage(const double* ev, size_t p, double c, int method, double* prec,
+                           double* cov, double* theta, double* htheta, double* smoothing) {
+  inverse_shrinkage(ev, p, c, method, prec, cov, theta, htheta, smoothing);
 }
 
 }  // extern "C"

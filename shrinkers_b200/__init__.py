@@ -31,7 +31,8 @@ __all__ = [
     "stieltjes_transform", "stieltjes_transform_with_deriv", "deconvolve_spiked",
     "estimate_population_eigenvalues", "ledoit_wolf_shrinkage", "shrink_eigenvalues",
     "detect_spikes_bema", "inverse_bbp", "stieltjes_at_points", "stieltjes_transform_batched",
-    "stieltjes_adjoint", "parse_method", "method_name",
+    "stieltjes_adjoint", "parse_method", "method_name", "inverse_nonlinear_shrinkage",
+    "stieltjes_scaled_ray",
 ]
 
 _D = C.POINTER(C.c_double)
@@ -382,6 +383,53 @@ def ledoit_wolf_shrinkage(eigenvalues, c, *, precision="f64"):
                                            float("nan"), _dp(out))
     _native.check(st, "ledoit_wolf_shrinkage")
     return out
+
+
+_INVERSE = {"qis": 0, "quadratic": 0, "quadratic_inverse": 0,
+            "lis": 1, "linear": 1, "linear_inverse": 1,
+            "gis": 2, "geometric": 2, "geometric_inverse": 2}
+
+
+def _parse_inverse_method(method: str) -> int:
+    """inverse.rs:98-105 InverseShrinkageMethod::parse (python.rs:353-359)."""
+    key = method.lower() if isinstance(method, str) else None
+    if key not in _INVERSE:
+        raise ValueError(f"unknown inverse shrinkage method '{method}' "
+                         "(expected 'qis', 'lis' or 'gis')")
+    return _INVERSE[key]
+
+
+def stieltjes_scaled_ray(eigenvalues, scale):
+    """RAW sums at z_i = lambda_i (1 + i*scale) (mod.rs:304-319), as
+    {"real", "imag"}; every point has its own eta_i = scale*lambda_i."""
+    ev = _owned_f64_vec(eigenvalues, "eigenvalues")
+    if ev.size == 0:
+        raise ValueError("eigenvalues must be non-empty")
+    _require_finite(ev, "eigenvalues")
+    s = _require_positive_finite(float(scale), "scale")
+    re, im = np.empty(ev.size), np.empty(ev.size)
+    _native.check(_lib().shrk_stieltjes_scaled_ray(_dp(ev), ev.size, s, _dp(re), _dp(im)),
+                  "stieltjes_scaled_ray")
+    return {"real": re, "imag": im}
+
+
+def inverse_nonlinear_shrinkage(eigenvalues, c, *, method="qis", parallel=False):
+    """python.rs:562-591 inverse_nonlinear_shrinkage (Ledoit & Wolf 2022):
+    precision-matrix eigenvalues by QIS / LIS / GIS.  Returns
+    {"precision_eigenvalues", "covariance_eigenvalues", "smoothing"}."""
+    ev, c = _owned_positive_spectrum(eigenvalues, c)
+    bad = ev[ev <= 0.0]
+    if bad.size:
+        raise ValueError("eigenvalues must be strictly positive for inverse shrinkage "
+                         f"(found {_fmt(float(bad[0]))})")
+    m = _parse_inverse_method(method)
+    _parse_parallel(parallel)
+    prec, cov = np.empty(ev.size), np.empty(ev.size)
+    h = C.c_double()
+    _native.check(_lib().shrk_inverse_nonlinear_shrinkage(_dp(ev), ev.size, c, m, _dp(prec),
+                                                          _dp(cov), C.byref(h), None, None),
+                  "inverse_nonlinear_shrinkage")
+    return {"precision_eigenvalues": prec, "covariance_eigenvalues": cov, "smoothing": h.value}
 
 
 def shrink_eigenvalues(eigenvalues, c, *, method="auto", parallel=False, precision="f64"):

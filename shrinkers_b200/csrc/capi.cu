@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -785,6 +786,108 @@ shrk_status shrk_ledoit_wolf_shrinkage(const double* ev, size_t p, double c, int
   Guard g;
   SHRK_TRY(g.st);
   return lw_device(ev, p, c, method, precision, parallelism, eta, xi);
+}
+
+shrk_status shrk_stieltjes_scaled_ray_dev(const double* d_ev, size_t p, double scale,
+                                          double* d_re, double* d_im, void* stream) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (!(std::isfinite(scale) && scale > 0.0))
+    return einval("scale must be a positive finite number");
+  Guard g;
+  SHRK_TRY(g.st);
+  return scaled_ray_sums(d_ev, (int64_t)p, scale, d_re, d_im, (cudaStream_t)stream);
+}
+
+shrk_status shrk_stieltjes_scaled_ray(const double* ev, size_t p, double scale, double* raw_re,
+                                      double* raw_im) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (!(std::isfinite(scale) && scale > 0.0))
+    return einval("scale must be a positive finite number");
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  SHRK_TRY(scaled_ray_sums((const double*)dev, (int64_t)p, scale, (double*)out,
+                           (double*)out + p, s));
+  SHRK_TRY(d2h(raw_re, out, sizeof(double) * p, s));
+  SHRK_TRY(d2h(raw_im, (double*)out + p, sizeof(double) * p, s));
+  return check_device_error(s);
+}
+
+// inverse.rs safe_reciprocal: 1/x, or the largest double for x <= 0 or
+// non-finite.
+static double safe_reciprocal(double x) {
+  return (x > 0.0 && std::isfinite(x)) ? 1.0 / x : std::numeric_limits<double>::max();
+}
+
+shrk_status shrk_inverse_nonlinear_shrinkage(const double* ev, size_t p, double c, int method,
+                                             double* precision_ev, double* covariance_ev,
+                                             double* smoothing, double* theta_out,
+                                             double* htheta_out) {
+  *smoothing = 0.0;
+  if (p == 0) return SHRK_OK;
+  if (!(std::isfinite(c) && c > 0.0 && c <= 1.0))
+    return einval("concentration ratio c must be in (0, 1]");
+  if (method < 0 || method > 2)
+    return einval("unknown inverse shrinkage method (expected 0 qis, 1 lis or 2 gis)");
+  for (size_t i = 0; i < p; ++i)
+    if (!(std::isfinite(ev[i]) && ev[i] > 0.0))
+      return einval("eigenvalues must be strictly positive for inverse shrinkage (found " +
+                    std::to_string(ev[i]) + ")");
+  // Ledoit-Wolf bandwidth (inverse.rs:170), then theta + i Htheta = ev_i m(z_i)
+  // on the ray z_i = ev_i (1 + i h) from the GPU.
+  const double p_f = (double)p, inv_p = 1.0 / p_f;
+  const double h = std::pow(std::min(c * c, 1.0 / (c * c)), 0.35) / std::pow(p_f, 0.35);
+  *smoothing = h;
+  std::vector<double> re(p), im(p);
+  SHRK_TRY(shrk_stieltjes_scaled_ray(ev, p, h, re.data(), im.data()));
+  // inverse.rs:183-259, in the reference's evaluation order.
+  std::vector<double> theta(p), htheta(p), inv_lambda(p), delta(p), omega(p);
+  double min_inv = INFINITY, trace = 0.0;
+  for (size_t i = 0; i < p; ++i) {
+    theta[i] = ev[i] * re[i] * inv_p;
+    htheta[i] = ev[i] * im[i] * inv_p;
+    inv_lambda[i] = 1.0 / ev[i];
+    min_inv = std::min(min_inv, inv_lambda[i]);
+    trace += ev[i];
+  }
+  const double omc = 1.0 - c;
+  for (size_t i = 0; i < p; ++i) {
+    const double x = inv_lambda[i], th = theta[i];
+    const double amp2 = theta[i] * theta[i] + htheta[i] * htheta[i];
+    const double denom = omc * omc * x + 2.0 * c * omc * x * th + c * c * x * amp2;
+    delta[i] = (denom > 0.0 && std::isfinite(denom)) ? 1.0 / denom : ev[i];
+    const double lis = omc * x + 2.0 * c * x * th;
+    omega[i] = lis > min_inv ? lis : min_inv;
+  }
+  if (method == 0) {  // QIS: trace-preserving rescale of the covariance
+    double sum = 0.0;
+    for (size_t i = 0; i < p; ++i) sum += delta[i];
+    const double scale = (sum > 0.0 && std::isfinite(sum)) ? trace / sum : 1.0;
+    for (size_t i = 0; i < p; ++i) {
+      covariance_ev[i] = delta[i] * scale;
+      precision_ev[i] = safe_reciprocal(covariance_ev[i]);
+    }
+  } else if (method == 1) {  // LIS
+    for (size_t i = 0; i < p; ++i) {
+      covariance_ev[i] = safe_reciprocal(omega[i]);
+      precision_ev[i] = omega[i];
+    }
+  } else {  // GIS: geometric mean of the QIS and LIS covariance estimates
+    for (size_t i = 0; i < p; ++i) {
+      const double ratio = omega[i] / delta[i];
+      precision_ev[i] = (ratio > 0.0 && std::isfinite(ratio)) ? std::sqrt(ratio)
+                                                              : safe_reciprocal(ev[i]);
+      covariance_ev[i] = safe_reciprocal(precision_ev[i]);
+    }
+  }
+  if (theta_out) std::copy(theta.begin(), theta.end(), theta_out);
+  if (htheta_out) std::copy(htheta.begin(), htheta.end(), htheta_out);
+  return SHRK_OK;
 }
 
 shrk_status shrk_rie_shrinkage(const double* ev, size_t p, double c, int method, int precision,

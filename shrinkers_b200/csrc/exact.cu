@@ -1,9 +1,11 @@
 // Smaller exact kernels: the value+derivative sum (src/stieltjes/autovec.rs:
-// 38-77), the f32 full-square kernel (src/stieltjes/cacheblock.rs:1525-1572)
-// and the windowed cutoff sums (cacheblock.rs:452-577).  The forward
+// 38-77), the f32 full-square kernel (src/stieltjes/cacheblock.rs:1525-1572),
+// the windowed cutoff sums (cacheblock.rs:452-577) and the scaled-ray sums of
+// inverse nonlinear shrinkage (src/stieltjes/mod.rs:304-319).  The forward
 // pair-sum kernels live in pairsum.cu, the adjoint in adjoint.cu.
 #include "common.cuh"
 #include "internal.h"
+#include "pairs.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -110,7 +112,99 @@ __global__ void windowed_kernel(const double* __restrict__ tgt, int64_t nt,
   im_o[t] = si * scale;
 }
 
+// ------------------------------------------------------ scaled ray ----
+// mod.rs:304-319 compute_stieltjes_scaled_ray: RAW sums at z_t = x_t (1 + i h),
+// i.e. every target has its own eta_t = h x_t.  FP64 pairs; a CTA of 256
+// threads holds 4 targets per thread (and their eta^2), source chunks of
+// 1024 are staged in shared memory; source splits write partial slabs that
+// ray_reduce_kernel adds in a fixed order.
+constexpr int RAY_NT = 256, RAY_R = 4, RAY_CH = 1024;
+
+__global__ void __launch_bounds__(RAY_NT, 2) ray_kernel(const double* __restrict__ ev, int64_t p,
+                                                       double scale, int64_t n_tiles,
+                                                       int n_splits, int64_t split_len,
+                                                       double* part_re, double* part_im) {
+  __shared__ double sb[RAY_CH];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t n_items = n_tiles * n_splits;
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int64_t tile = item / n_splits;
+    const int split = (int)(item % n_splits);
+    const int64_t wbase = tile * RAY_NT * RAY_R + (int64_t)warp * 32 * RAY_R;
+    double x[RAY_R], eta2[RAY_R], re[RAY_R], iv[RAY_R];
+#pragma unroll
+    for (int r = 0; r < RAY_R; ++r) {
+      const int64_t idx = wbase + r * 32 + lane;
+      x[r] = idx < p ? ev[idx] : ev[0];
+      const double eta = scale * x[r];
+      eta2[r] = eta * eta;
+      re[r] = iv[r] = 0.0;
+    }
+    const int64_t s0 = (int64_t)split * split_len, s1 = min(p, s0 + split_len);
+    for (int64_t cs = s0; cs < s1; cs += RAY_CH) {
+      const int len = (int)min((int64_t)RAY_CH, s1 - cs);
+      __syncthreads();
+      for (int i = threadIdx.x; i < len; i += RAY_NT) sb[i] = ev[cs + i];
+      __syncthreads();
+#pragma unroll 4
+      for (int j = 0; j < len; ++j) {
+        const double l = sb[j];
+#pragma unroll
+        for (int r = 0; r < RAY_R; ++r) {
+          const double d = x[r] - l;
+          const double inv = rcp_f64(fma(d, d, eta2[r]));
+          re[r] = fma(d, inv, re[r]);
+          iv[r] += inv;
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < RAY_R; ++r) {
+      const int64_t idx = wbase + r * 32 + lane;
+      if (idx < p) {
+        part_re[(int64_t)split * p + idx] = re[r];
+        part_im[(int64_t)split * p + idx] = scale * x[r] * iv[r];
+      }
+    }
+  }
+}
+
+__global__ void ray_reduce_kernel(const double* __restrict__ part_re,
+                                  const double* __restrict__ part_im, int n_splits, int64_t p,
+                                  double* out_re, double* out_im) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p) return;
+  double re = 0.0, im = 0.0;
+  for (int k = 0; k < n_splits; ++k) {
+    re += part_re[(int64_t)k * p + t];
+    im += part_im[(int64_t)k * p + t];
+  }
+  out_re[t] = re;
+  out_im[t] = im;
+}
+
 }  // namespace
+
+shrk_status scaled_ray_sums(const double* d_ev, int64_t p, double scale, double* d_re,
+                            double* d_im, cudaStream_t s) {
+  if (p <= 0) return SHRK_OK;
+  const SplitPlan pl = plan_splits(p, p, RAY_NT * RAY_R, RAY_CH, 2);
+  void* part = nullptr;
+  SHRK_TRY(scratch_get(0, sizeof(double) * 2 * (size_t)pl.n_splits * (size_t)p, &part));
+  double* pre = (double*)part;
+  double* pim = pre + (size_t)pl.n_splits * p;
+  {
+    LaunchScope ls("scaled_ray", s);
+    ray_kernel<<<pl.grid, RAY_NT, 0, s>>>(d_ev, p, scale, pl.n_tiles, pl.n_splits, pl.split_len,
+                                          pre, pim);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  LaunchScope ls("split_reduce", s);
+  ray_reduce_kernel<<<(unsigned)((p + 255) / 256), 256, 0, s>>>(pre, pim, pl.n_splits, p, d_re,
+                                                                d_im);
+  SHRK_CUDA(cudaGetLastError());
+  return SHRK_OK;
+}
 
 shrk_status windowed_sums(const double* d_tgt, int64_t nt, const double* d_src, int64_t ns,
                           double eta, double window, double scale, double* d_re, double* d_im,

@@ -52,6 +52,10 @@ shrk_status windowed_sums(const double* d_tgt, int64_t nt, const double* d_src, 
 shrk_status with_deriv(const double* d_ev, int64_t p, double eta, double* d_re, double* d_im,
                        double* d_dre, double* d_dim, cudaStream_t s);
 
+// mod.rs:304-319: RAW sums at z_t = ev_t (1 + i scale) (eta_t = scale ev_t).
+shrk_status scaled_ray_sums(const double* d_ev, int64_t p, double scale, double* d_re,
+                            double* d_im, cudaStream_t s);
+
 // E6: FP32 full-square sums scaled by 1/p in FP32.
 shrk_status all_f32(const float* d_ev, int64_t p, float eta, float* d_re, float* d_im,
                     cudaStream_t s);

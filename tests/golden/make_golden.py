@@ -146,6 +146,27 @@ def main(root: str) -> None:
         "cases": cases,
     }
 
+    # ---- inverse nonlinear shrinkage: QIS golden master (deconvolution/inverse.rs)
+    path = os.path.join(src, "deconvolution", "inverse.rs")
+    text = open(path).read()
+    i0 = text.index("fn qis_golden_master")
+    blk = text[i0: text.index("\n    }\n", i0)]
+    sp = text[text.index("fn spectrum(p: usize)"):]
+    sp = sp[: sp.index("}")]
+    fl = _floats(sp)  # lambda_i = base + (i + 1.0) * step
+    base, step = fl[0], fl[2]
+    rows = re.findall(r"\((\d+),\s*(-?[\d_.e-]+),\s*(-?[\d_.e-]+)\)", blk)
+    out["qis_golden"] = {
+        "source": f"src/deconvolution/inverse.rs:{_line_of(text, 'fn qis_golden_master')}",
+        "spectrum": {"base": base, "step": step,
+                     "p": int(re.search(r"spectrum\((\d+)\)", blk).group(1))},
+        "c": float(re.search(r"let c = ([\d.]+);", blk).group(1)),
+        "smoothing": _floats(re.search(r"nls\.smoothing, ([\d_.]+)", blk).group(1))[0],
+        "rows": [[int(i), float(t.replace("_", "")), float(w.replace("_", ""))]
+                 for i, t, w in rows],
+        "max_relative": 1e-11,
+    }
+
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)

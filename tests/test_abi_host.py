@@ -203,3 +203,13 @@ def test_treecode_adjoint_rejects_non_treecode_methods(rk):
                                            x.ctypes.data_as(D), 2, x.ctypes.data_as(D))
     assert st == _native.SHRK_EINVAL
     assert "ChebCode" in _native.last_error()
+
+
+def test_inverse_shrinkage_validation(rk):
+    """python.rs:202-216 and 353-359 messages; checked before any device work."""
+    with pytest.raises(ValueError, match="strictly positive"):
+        rk.inverse_nonlinear_shrinkage(np.array([0.0, 1.0, 2.0]), c=0.3)
+    with pytest.raises(ValueError, match="unknown inverse shrinkage"):
+        rk.inverse_nonlinear_shrinkage(np.array([1.0, 2.0]), c=0.3, method="nope")
+    with pytest.raises(ValueError):
+        rk.inverse_nonlinear_shrinkage(np.array([1.0, 2.0]), c=1.5)

@@ -264,3 +264,54 @@ def test_lw_and_population_pipeline_shapes(oracle):
     ev0 = 0.5 + 0.01 * np.arange(100)
     r0 = oracle.estimate_population_eigenvalues(ev0, 0.25)
     np.testing.assert_allclose(r0["bulk_population"], oracle.ledoit_wolf(ev0, 0.25), atol=1e-12)
+
+
+def _qis_spectrum(g):
+    sp = g["spectrum"]
+    return sp["base"] + (np.arange(sp["p"]) + 1.0) * sp["step"]
+
+
+def test_inverse_shrinkage_qis_golden_master(oracle, golden):
+    """inverse.rs:426 qis_golden_master: smoothing, theta and precision pins."""
+    g = golden["qis_golden"]
+    r = oracle.inverse_shrinkage(_qis_spectrum(g), g["c"], "qis")
+    assert abs(r["smoothing"] / g["smoothing"] - 1.0) <= 1e-12
+    for i, theta, prec in g["rows"]:
+        assert abs(r["theta"][i] / theta - 1.0) <= g["max_relative"]
+        assert abs(r["precision_eigenvalues"][i] / prec - 1.0) <= g["max_relative"]
+
+
+def test_scaled_ray_is_theta_by_definition(oracle, golden):
+    """theta_i + i Htheta_i = lambda_i m(lambda_i (1 + i h)): the ray sums equal
+    the inverse-shrinkage shrinkers written in the inverse eigenvalues
+    x = 1/lambda (1e-12 absolute, as inverse.rs:308-320)."""
+    g = golden["qis_golden"]
+    lam = _qis_spectrum(g)
+    r = oracle.inverse_shrinkage(lam, g["c"], "qis")
+    h, p = r["smoothing"], lam.size
+    x = 1.0 / lam
+    diff = x[None, :] - x[:, None]            # x_j - x_i
+    den = diff ** 2 + (x[None, :] * h) ** 2
+    theta = np.sum(x[None, :] * diff / den, axis=1) / p
+    htheta = np.sum(x[None, :] ** 2 * h / den, axis=1) / p
+    np.testing.assert_allclose(r["theta"], theta, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(r["htheta"], htheta, rtol=0, atol=1e-12)
+
+
+def test_inverse_shrinkage_properties(oracle, golden):
+    """QIS preserves the trace; GIS is the geometric mean of QIS (unscaled)
+    and LIS (inverse.rs:323-399)."""
+    g = golden["qis_golden"]
+    lam = _qis_spectrum(g)
+    c = 0.45
+    q = oracle.inverse_shrinkage(lam, c, "qis")
+    np.testing.assert_allclose(q["covariance_eigenvalues"].sum(), lam.sum(), rtol=1e-12)
+    np.testing.assert_allclose(q["precision_eigenvalues"], 1.0 / q["covariance_eigenvalues"],
+                               rtol=1e-12)
+    lis = oracle.inverse_shrinkage(lam, c, "lis")
+    gis = oracle.inverse_shrinkage(lam, c, "gis")
+    x = 1.0 / lam
+    a2 = q["theta"] ** 2 + q["htheta"] ** 2
+    raw_qis = 1.0 / ((1 - c) ** 2 * x + 2 * c * (1 - c) * x * q["theta"] + c * c * x * a2)
+    np.testing.assert_allclose(gis["covariance_eigenvalues"],
+                               np.sqrt(raw_qis * lis["covariance_eigenvalues"]), rtol=1e-12)
