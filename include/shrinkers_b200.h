@@ -178,6 +178,20 @@ shrk_status shrk_stieltjes_adjoint_treecode_dev(const double* d_ev, size_t p, do
                                                 const double* d_g_re, const double* d_g_im,
                                                 int method, double* d_grad, void* stream);
 
+/* chebcode.rs:1312-1361 ChebCodeBatch::evaluate_many (gamma sweeps): one tree
+ * built for the preset `method` (CHEBCODE*: its theta, order and leaf
+ * capacity; the far field is FP64 whatever the preset), then RAW sums at
+ * every eigenvalue for each of the n_eta etas, evaluated two etas per
+ * traversal (chebcode.rs:836-915: a node is accepted only when both etas
+ * accept it).  out_re / out_im: n_eta x p, row-major, input order; etas must
+ * be positive and finite. */
+shrk_status shrk_chebcode_evaluate_many(const double* ev, size_t p, const double* etas,
+                                        size_t n_eta, int method, double* out_re,
+                                        double* out_im);
+shrk_status shrk_chebcode_evaluate_many_dev(const double* d_ev, size_t p, const double* d_etas,
+                                            size_t n_eta, int method, double* d_re, double* d_im,
+                                            void* stream);
+
 /* mod.rs:304-319 compute_stieltjes_scaled_ray: RAW sums at z_i = ev_i(1 + i*scale),
  * i.e. every point has its own eta_i = scale*ev_i.  Exact FP64 pair sums (the
  * reference takes the exact per-point route for every method here). */

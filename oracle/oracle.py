@@ -87,6 +87,7 @@ def lib():
             "orc_estimate_population": (C.c_int, [_D, _SZ, C.c_double, C.c_double, C.POINTER(_SZ), _D, _D, _D, _D, _D, _D]),
             "orc_deconvolve_spiked": (C.c_int, [_D, _SZ, C.c_double, _SZ, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double, C.POINTER(_SZ), _D, _D, _D, _D, _D]),
             "orc_scaled_ray": (None, [_D, _SZ, C.c_double, _D, _D]),
+            "orc_evaluate_many": (None, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, C.c_int, _D, _D]),
             "orc_inverse_shrinkage": (None, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
         }
         for name, (res, args) in sig.items():
@@ -235,6 +236,17 @@ def chebcode_points(q, ev, eta, theta, n, leaf_cap, f32, parallel=True):
     re, im = np.empty_like(q), np.empty_like(q)
     lib().orc_chebcode_points(_d(q), q.size, _d(ev), ev.size, eta, theta, n, leaf_cap,
                               int(f32), int(parallel), _d(re), _d(im))
+    return re, im
+
+
+def evaluate_many(ev, etas, theta, n, leaf_cap):
+    """ChebCodeBatch::evaluate_many (src/stieltjes/chebcode.rs:1312-1361): RAW
+    sums at every eigenvalue for each eta, as (n_eta, p) arrays."""
+    ev = _arr(ev)
+    et = _arr(etas)
+    re = np.empty((et.size, ev.size))
+    im = np.empty_like(re)
+    lib().orc_evaluate_many(_d(ev), ev.size, _d(et), et.size, theta, n, leaf_cap, _d(re), _d(im))
     return re, im
 
 

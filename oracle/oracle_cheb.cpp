@@ -323,6 +323,89 @@ void chebcode_points(const double* q, size_t nq, const double* ev, size_t p, dou
   }
 }
 
+// chebcode.rs:836-915 contribution_x2: two etas per traversal, one per lane
+// (x86 lanes: unfused multiply-adds, true division).  A node is accepted
+// only when half_w^2 < theta^2 (cl^2 + min(eta)^2), the reference's own form.
+static void contribution_x2(const Tree& T, double x, double e0, double e1, double* r0,
+                            double* i0, double* r1, double* i1) {
+  const int n = T.n;
+  const double e2a = e0 * e0, e2b = e1 * e1;
+  const double e_min = std::min(e0, e1);
+  int32_t stack[MAX_TREE_DEPTH + 2];
+  int top = 0;
+  stack[top++] = 0;
+  double ar0 = 0.0, ar1 = 0.0, ai0 = 0.0, ai1 = 0.0;
+  while (top > 0) {
+    const int32_t node = stack[--top];
+    const size_t ni = (size_t)node;
+    if (T.right[ni] < 0) {
+      for (size_t k = T.lo_idx[ni]; k < T.hi_idx[ni]; ++k) {
+        const double d = x - T.sorted[k];
+        const double dd = d * d;
+        const double inv0 = 1.0 / (e2a + dd), inv1 = 1.0 / (e2b + dd);
+        ar0 = ar0 + d * inv0;
+        ar1 = ar1 + d * inv1;
+        ai0 = ai0 + e0 * inv0;
+        ai1 = ai1 + e1 * inv1;
+      }
+      continue;
+    }
+    const double lo = T.lo[ni], hi = T.hi[ni];
+    const double cl = x < lo ? lo - x : (x > hi ? x - hi : 0.0);
+    const double d_sq = cl * cl + e_min * e_min;
+    const double half_w = 0.5 * (hi - lo);
+    if (half_w * half_w < T.theta_sq * d_sq) {
+      for (int j = 0; j < n; ++j) {
+        const double dj = x - T.nodes[ni * n + j];
+        const double wj = T.w[ni * n + j];
+        const double dd = dj * dj;
+        const double inv0 = 1.0 / (e2a + dd), inv1 = 1.0 / (e2b + dd);
+        const double wd = wj * dj;
+        ar0 = ar0 + wd * inv0;
+        ar1 = ar1 + wd * inv1;
+        ai0 = ai0 + (wj * e0) * inv0;
+        ai1 = ai1 + (wj * e1) * inv1;
+      }
+    } else {
+      const int32_t r = T.right[ni];
+      if (r >= 0) {
+        stack[top++] = r;
+        stack[top++] = node + 1;
+      }
+    }
+  }
+  *r0 = ar0;
+  *i0 = ai0;
+  *r1 = ar1;
+  *i1 = ai1;
+}
+
+// chebcode.rs:1312-1361 ChebCodeBatch::evaluate_many: RAW sums at every
+// eigenvalue (input order) for each eta; etas taken in pairs (an odd last
+// eta is paired with itself).  out_re/out_im: n_eta x p row-major.
+void evaluate_many(const double* ev, size_t p, const double* etas, size_t n_eta, double theta,
+                   int n, int leaf_cap, double* out_re, double* out_im) {
+  if (p == 0 || n_eta == 0) return;
+  std::vector<double> sorted(ev, ev + p);
+  if (!is_sorted_ascending(ev, p)) std::sort(sorted.begin(), sorted.end());
+  Tree T;
+  build_tree(T, sorted.data(), p, n, theta, (size_t)leaf_cap);
+  for (size_t k = 0; k < n_eta; k += 2) {
+    const double e0 = etas[k], e1 = (k + 1 < n_eta) ? etas[k + 1] : etas[k];
+#pragma omp parallel for schedule(dynamic, 128)
+    for (long i = 0; i < (long)p; ++i) {
+      double r0, i0, r1, i1;
+      contribution_x2(T, ev[i], e0, e1, &r0, &i0, &r1, &i1);
+      out_re[k * p + i] = r0;
+      out_im[k * p + i] = i0;
+      if (k + 1 < n_eta) {
+        out_re[(k + 1) * p + i] = r1;
+        out_im[(k + 1) * p + i] = i1;
+      }
+    }
+  }
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -333,6 +416,11 @@ void orc_chebcode_points(const double* q, size_t nq, const double* ev, size_t p,
                          double theta, int n, int leaf_cap, int f32, int parallel, double* re,
                          double* im) {
   chebcode_points(q, nq, ev, p, eta, theta, n, leaf_cap, f32 != 0, parallel != 0, re, im);
+}
+
+void orc_evaluate_many(const double* ev, size_t p, const double* etas, size_t n_eta,
+                       double theta, int n, int leaf_cap, double* out_re, double* out_im) {
+  evaluate_many(ev, p, etas, n_eta, theta, n, leaf_cap, out_re, out_im);
 }
 
 size_t orc_grid_leaf_cap(size_t n, size_t p, size_t nq, size_t preset_leaf) {

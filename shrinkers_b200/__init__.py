@@ -32,7 +32,7 @@ __all__ = [
     "estimate_population_eigenvalues", "ledoit_wolf_shrinkage", "shrink_eigenvalues",
     "detect_spikes_bema", "inverse_bbp", "stieltjes_at_points", "stieltjes_transform_batched",
     "stieltjes_adjoint", "parse_method", "method_name", "inverse_nonlinear_shrinkage",
-    "stieltjes_scaled_ray",
+    "stieltjes_scaled_ray", "chebcode_evaluate_many",
 ]
 
 _D = C.POINTER(C.c_double)
@@ -410,6 +410,26 @@ def stieltjes_scaled_ray(eigenvalues, scale):
     re, im = np.empty(ev.size), np.empty(ev.size)
     _native.check(_lib().shrk_stieltjes_scaled_ray(_dp(ev), ev.size, s, _dp(re), _dp(im)),
                   "stieltjes_scaled_ray")
+    return {"real": re, "imag": im}
+
+
+def chebcode_evaluate_many(eigenvalues, etas, method="chebcode"):
+    """ChebCodeBatch::evaluate_many (chebcode.rs:1312-1361): one tree for the
+    ChebCode preset ``method``, RAW sums at every eigenvalue for each eta.
+    Returns {"real", "imag"} arrays of shape (len(etas), p), input order."""
+    ev = _owned_f64_vec(eigenvalues, "eigenvalues")
+    if ev.size == 0:
+        raise ValueError("eigenvalues must be non-empty")
+    _require_finite(ev, "eigenvalues")
+    et = np.ascontiguousarray(np.asarray(etas, dtype=np.float64).ravel())
+    for e in et:
+        _require_positive_finite(float(e), "eta")
+    re = np.empty((et.size, ev.size))
+    im = np.empty_like(re)
+    if et.size:
+        _native.check(_lib().shrk_chebcode_evaluate_many(_dp(ev), ev.size, _dp(et), et.size,
+                                                         parse_method(method), _dp(re), _dp(im)),
+                      "chebcode_evaluate_many")
     return {"real": re, "imag": im}
 
 

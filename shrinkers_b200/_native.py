@@ -47,6 +47,8 @@ SIGNATURES = {
     "shrk_stieltjes_adjoint_dev": (_ST, [_P, _SZ, C.c_double, _P, _P, C.c_int, _P, _P]),
     "shrk_stieltjes_adjoint_treecode": (_ST, [_D, _SZ, C.c_double, _D, _D, C.c_int, _D]),
     "shrk_stieltjes_adjoint_treecode_dev": (_ST, [_P, _SZ, C.c_double, _P, _P, C.c_int, _P, _P]),
+    "shrk_chebcode_evaluate_many": (_ST, [_D, _SZ, _D, _SZ, C.c_int, _D, _D]),
+    "shrk_chebcode_evaluate_many_dev": (_ST, [_P, _SZ, _P, _SZ, C.c_int, _P, _P, _P]),
     "shrk_stieltjes_scaled_ray": (_ST, [_D, _SZ, C.c_double, _D, _D]),
     "shrk_stieltjes_scaled_ray_dev": (_ST, [_P, _SZ, C.c_double, _P, _P, _P]),
     "shrk_inverse_nonlinear_shrinkage": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),

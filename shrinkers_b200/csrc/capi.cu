@@ -702,6 +702,47 @@ static shrk_status check_cheb_method(int method, ChebParams* prm) {
   return SHRK_OK;
 }
 
+shrk_status shrk_chebcode_evaluate_many_dev(const double* d_ev, size_t p, const double* d_etas,
+                                            size_t n_eta, int method, double* d_re, double* d_im,
+                                            void* stream) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (n_eta == 0) return SHRK_OK;
+  ChebParams prm;
+  SHRK_TRY(check_cheb_method(method, &prm));
+  Guard g;
+  SHRK_TRY(g.st);
+  return chebcode_evaluate_many(d_ev, (int64_t)p, d_etas, (int64_t)n_eta, prm, d_re, d_im,
+                                (cudaStream_t)stream);
+}
+
+shrk_status shrk_chebcode_evaluate_many(const double* ev, size_t p, const double* etas,
+                                        size_t n_eta, int method, double* out_re,
+                                        double* out_im) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (n_eta == 0) return SHRK_OK;
+  for (size_t k = 0; k < n_eta; ++k)
+    if (!(std::isfinite(etas[k]) && etas[k] > 0.0))
+      return einval("eta must be a positive finite number");
+  ChebParams prm;
+  SHRK_TRY(check_cheb_method(method, &prm));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * (p + n_eta), &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p * n_eta, &out));
+  double* d = (double*)dev;
+  SHRK_TRY(h2d(d, ev, sizeof(double) * p, s));
+  SHRK_TRY(h2d(d + p, etas, sizeof(double) * n_eta, s));
+  double* o = (double*)out;
+  SHRK_TRY(chebcode_evaluate_many(d, (int64_t)p, d + p, (int64_t)n_eta, prm, o, o + p * n_eta,
+                                  s));
+  SHRK_TRY(d2h(out_re, o, sizeof(double) * p * n_eta, s));
+  SHRK_TRY(d2h(out_im, o + p * n_eta, sizeof(double) * p * n_eta, s));
+  return check_device_error(s);
+}
+
 shrk_status shrk_stieltjes_adjoint_treecode_dev(const double* d_ev, size_t p, double eta,
                                                 const double* d_gre, const double* d_gim,
                                                 int method, double* d_grad, void* stream) {

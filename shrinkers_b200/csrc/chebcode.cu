@@ -553,6 +553,90 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   return tree_weights(tb, d_sorted, nullptr, f.w, s);
 }
 
+// ------------------------------------------------------ multi-eta --
+// chebcode.rs:836-915 contribution_x2: two etas per traversal (the
+// reference's F64x2 lanes; on its x86 target lane multiply-adds are unfused
+// and the reciprocal is a true division -- both reproduced here, the build
+// contracts nothing).  A node is accepted when half_w^2 < theta^2 (cl^2 +
+// min(eta)^2), i.e. only if both lanes would accept it.  One thread per
+// (point, eta pair); results bit-exact with the reference algorithm.
+struct ManyArgs {
+  const double* x;       // evaluation points (the eigenvalues, caller's order)
+  int64_t p;
+  const double* sorted;
+  const double* etas;
+  int64_t n_eta;
+  DevTreeF64 t;
+  double theta_sq;
+  double* out_re;        // [n_eta][p]
+  double* out_im;
+  int* err;
+};
+
+__global__ void __launch_bounds__(128) cheb_eval_x2(const ManyArgs a) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t n_pairs = (a.n_eta + 1) / 2;
+  if (g >= a.p * n_pairs) return;
+  const int64_t i = g % a.p, k = (g / a.p) * 2;
+  const bool two = k + 1 < a.n_eta;
+  const double e0 = a.etas[k], e1 = two ? a.etas[k + 1] : e0;
+  const double e2a = e0 * e0, e2b = e1 * e1, e_min = fmin(e0, e1);
+  const DevTreeF64& T = a.t;
+  const int n = T.n;
+  const double x = a.x[i];
+  int32_t stack[MAX_TREE_DEPTH + 2];
+  int top = 0;
+  stack[top++] = 0;
+  double ar0 = 0.0, ar1 = 0.0, ai0 = 0.0, ai1 = 0.0;
+  while (top > 0) {
+    const int32_t node = stack[--top];
+    const int32_t rt = T.right[node];
+    if (rt < 0) {
+      for (int64_t q = T.lo_idx[node]; q < T.hi_idx[node]; ++q) {
+        const double d = x - a.sorted[q];
+        const double dd = d * d;
+        const double inv0 = 1.0 / (e2a + dd), inv1 = 1.0 / (e2b + dd);
+        ar0 = ar0 + d * inv0;
+        ar1 = ar1 + d * inv1;
+        ai0 = ai0 + e0 * inv0;
+        ai1 = ai1 + e1 * inv1;
+      }
+      continue;
+    }
+    const double lo = T.lo[node], hi = T.hi[node];
+    const double cl = x < lo ? lo - x : (x > hi ? x - hi : 0.0);
+    const double d_sq = cl * cl + e_min * e_min;
+    const double half_w = 0.5 * (hi - lo);
+    if (half_w * half_w < a.theta_sq * d_sq) {
+      const int64_t base = (int64_t)node * n;
+      for (int j = 0; j < n; ++j) {
+        const double dj = x - T.nodes[base + j];
+        const double wj = T.w[base + j];
+        const double dd = dj * dj;
+        const double inv0 = 1.0 / (e2a + dd), inv1 = 1.0 / (e2b + dd);
+        const double wd = wj * dj;
+        ar0 = ar0 + wd * inv0;
+        ar1 = ar1 + wd * inv1;
+        ai0 = ai0 + (wj * e0) * inv0;
+        ai1 = ai1 + (wj * e1) * inv1;
+      }
+    } else {
+      if (top + 2 > MAX_TREE_DEPTH + 2) {  // cannot happen for a depth-capped tree
+        atomicExch(a.err, DEV_ERR_BOUNDS);
+        break;
+      }
+      stack[top++] = rt;
+      stack[top++] = node + 1;
+    }
+  }
+  a.out_re[k * a.p + i] = ar0;
+  a.out_im[k * a.p + i] = ai0;
+  if (two) {
+    a.out_re[(k + 1) * a.p + i] = ar1;
+    a.out_im[(k + 1) * a.p + i] = ai1;
+  }
+}
+
 // ------------------------------------------------ treecode adjoint --
 // Gradient of L = sum_j (w_j Re m_j + v_j Im m_j) (the adjoint of the
 // all-points transform, no reference counterpart) with the source sums of
@@ -777,6 +861,44 @@ shrk_status chebcode_adjoint(const double* d_ev, int64_t p, double eta, const do
   a.err = device_error_word();
   LaunchScope ls("cheb_adjoint", s);
   cheb_adjoint_f64<<<blocks_for(p, 128), 128, 0, s>>>(a);
+  SHRK_CUDA(cudaGetLastError());
+  return SHRK_OK;
+}
+
+shrk_status chebcode_evaluate_many(const double* d_ev, int64_t p, const double* d_etas,
+                                   int64_t n_eta, const ChebParams& prm, double* d_re,
+                                   double* d_im, cudaStream_t s) {
+  if (p <= 0 || n_eta <= 0) return SHRK_OK;
+  if (prm.n < 2 || prm.n > MAX_N) {
+    set_error("chebcode: interpolation order must be in [2, 16]");
+    return SHRK_EINVAL;
+  }
+  const double* ds = nullptr;
+  double first = 0.0, last = 0.0;
+  SHRK_TRY(sorted_sources(d_ev, p, &ds, &first, &last, s));
+  TreeBuild tb;
+  SHRK_TRY(build_tree_gpu(ds, p, prm, tb, s));
+  ManyArgs a;
+  a.x = d_ev;
+  a.p = p;
+  a.sorted = ds;
+  a.etas = d_etas;
+  a.n_eta = n_eta;
+  a.t.lo = tb.f.lo;
+  a.t.hi = tb.f.hi;
+  a.t.accept_hw = tb.f.accept_hw;
+  a.t.lo_idx = tb.f.lo_idx;
+  a.t.hi_idx = tb.f.hi_idx;
+  a.t.right = tb.f.right;
+  a.t.nodes = tb.f.nodes;
+  a.t.w = tb.f.w;
+  a.t.n = prm.n;
+  a.theta_sq = prm.theta * prm.theta;
+  a.out_re = d_re;
+  a.out_im = d_im;
+  a.err = device_error_word();
+  LaunchScope ls("cheb_eval_x2", s);
+  cheb_eval_x2<<<blocks_for(p * ((n_eta + 1) / 2), 128), 128, 0, s>>>(a);
   SHRK_CUDA(cudaGetLastError());
   return SHRK_OK;
 }

@@ -112,6 +112,12 @@ shrk_status chebcode_adjoint(const double* d_ev, int64_t p, double eta, const do
                              const double* d_gim, const ChebParams& prm, double* d_grad,
                              cudaStream_t s);
 
+// chebcode.rs:1312-1361 ChebCodeBatch::evaluate_many on the GPU: RAW sums at
+// every eigenvalue for each of n_eta etas (device array), [n_eta][p].
+shrk_status chebcode_evaluate_many(const double* d_ev, int64_t p, const double* d_etas,
+                                   int64_t n_eta, const ChebParams& prm, double* d_re,
+                                   double* d_im, cudaStream_t s);
+
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);
 

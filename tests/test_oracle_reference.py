@@ -315,3 +315,21 @@ def test_inverse_shrinkage_properties(oracle, golden):
     raw_qis = 1.0 / ((1 - c) ** 2 * x + 2 * c * (1 - c) * x * q["theta"] + c * c * x * a2)
     np.testing.assert_allclose(gis["covariance_eigenvalues"],
                                np.sqrt(raw_qis * lis["covariance_eigenvalues"]), rtol=1e-12)
+
+
+def test_evaluate_many_matches_single_eta(oracle):
+    """chebcode.rs:1370-1400: the two-eta traversal equals per-eta single
+    calls within 5e-8 (1 + |re|) (a node accepted for both etas can differ
+    from one eta's own traversal at acceptance boundaries), also for
+    unsorted input."""
+    p = 512
+    ev = np.log(np.arange(1, p + 1, dtype=np.float64))
+    shuffled = ev[np.random.default_rng(7).permutation(p)]
+    etas = [0.02, 0.05, 0.11]
+    for inp in (ev, shuffled):
+        re, im = oracle.evaluate_many(inp, etas, 0.5, 11, 32)
+        for k, eta in enumerate(etas):
+            sr, si = oracle.compute_all(inp, eta, "chebcode")
+            sr, si = sr * p, si * p
+            assert np.all(np.abs(re[k] - sr) <= 5e-8 * (1.0 + np.abs(sr)))
+            assert np.all(np.abs(im[k] - si) <= 5e-8)
