@@ -200,6 +200,24 @@ shrk_status shrk_stieltjes_scaled_ray(const double* ev, size_t p, double scale, 
 shrk_status shrk_stieltjes_scaled_ray_dev(const double* d_ev, size_t p, double scale,
                                           double* d_re, double* d_im, void* stream);
 
+/* fft5.rs:568-590 compute_all_stieltjes_fft5_with_options: RAW sums (not
+ * scaled by 1/p) at every eigenvalue from the fft5 grid convolution with the
+ * Fft5Options knobs (fft5.rs:213-249): order = stencil nodes, 2/4/6/8 for
+ * Linear/Cubic/Quintic/Heptic (the methods "fft5"/"fft3"/"fft2" use 8);
+ * m_override = forced grid size, 0 for the rule dx <= eta/8, m >= 8p, at
+ * most 2^20; pad = max(pad_eta_mult*eta, pad_range_frac*raw_range) (defaults
+ * 1000 and 0.75).  The first and last entries bound the grid, as in the
+ * reference (ascending input expected).  SHRK_ENOTIMPL when the grid size is
+ * not a power of two no larger than 2^22. */
+shrk_status shrk_stieltjes_fft5_with_options(const double* ev, size_t p, double eta, int order,
+                                             size_t m_override, double pad_eta_mult,
+                                             double pad_range_frac, double* raw_re,
+                                             double* raw_im);
+shrk_status shrk_stieltjes_fft5_with_options_dev(const double* d_ev, size_t p, double eta,
+                                                 int order, size_t m_override,
+                                                 double pad_eta_mult, double pad_range_frac,
+                                                 double* d_re, double* d_im, void* stream);
+
 /* ------------------------------------------------------- consumers -- */
 /* deconvolution/inverse.rs:156-269 inverse_nonlinear_shrinkage (RmtConfig::new:
  * exact sums): method 0 QIS, 1 LIS, 2 GIS.  precision_ev / covariance_ev hold

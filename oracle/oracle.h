@@ -69,4 +69,13 @@ size_t nufft_grid_size(double raw_range, double eta);
 void nufft_points(const double* q, size_t nq, const double* sorted_ev, size_t p, double eta,
                   bool parallel, double* re, double* im);
 
+// fft5 grid convolution (src/stieltjes/fft5.rs), raw sums.  order = stencil
+// nodes (2/4/6/8), m_override 0 = the adaptive grid rule.  Returns 4 when the
+// grid size is not a power of two.
+size_t fft5_grid_size(double lo_raw, double hi_raw, size_t p, double eta, double pad_eta_mult,
+                      double pad_range_frac);
+int fft5_points(const double* q, size_t nq, const double* ev, size_t p, double eta, int order,
+                size_t m_override, double pad_eta_mult, double pad_range_frac, double* re,
+                double* im);
+
 }  // namespace orc

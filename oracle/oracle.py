@@ -76,6 +76,9 @@ def lib():
             "orc_nufft_grid": (_SZ, [_D, _SZ, C.c_double, _D, _D, _D, _D]),
             "orc_fft": (None, [_D, _SZ, C.c_int]),
             "orc_lagrange4": (None, [C.c_double, _D]),
+            "orc_lagrange": (None, [C.c_int, C.c_double, _D]),
+            "orc_fft5_grid_size": (_SZ, [C.c_double, C.c_double, _SZ, C.c_double, C.c_double, C.c_double]),
+            "orc_fft5_points": (C.c_int, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, _SZ, C.c_double, C.c_double, _D, _D]),
             "orc_shrinkage_factor": (C.c_double, [C.c_double] * 4),
             "orc_inverse_bbp": (C.c_double, [C.c_double] * 3),
             "orc_bbp_threshold": (C.c_double, [C.c_double] * 2),
@@ -292,6 +295,30 @@ def nufft_grid(ev, eta):
     L.orc_nufft_grid(_d(ev), ev.size, eta, _d(dens), _d(packed), C.byref(lo), C.byref(dx))
     return dict(m=m, density=dens, packed=packed[0::2] + 1j * packed[1::2], lo=lo.value,
                 dx=dx.value)
+
+
+# ------------------------------------------------------------------- fft5 --
+def fft5_grid_size(ev, eta, pad_eta_mult=1000.0, pad_range_frac=0.75):
+    ev = _arr(ev)
+    return int(lib().orc_fft5_grid_size(float(ev[0]), float(ev[-1]), ev.size, eta, pad_eta_mult,
+                                        pad_range_frac))
+
+
+def fft5_points(q, ev, eta, order=8, m=None, pad_eta_mult=1000.0, pad_range_frac=0.75):
+    """fft5.rs:559-625: RAW sums of the fft5 grid convolution at q."""
+    q, ev = _arr(q), _arr(ev)
+    re, im = np.empty_like(q), np.empty_like(q)
+    st = lib().orc_fft5_points(_d(q), q.size, _d(ev), ev.size, eta, int(order), int(m or 0),
+                               pad_eta_mult, pad_range_frac, _d(re), _d(im))
+    if st:
+        raise ValueError("fft5 oracle: the grid size must be a power of two")
+    return re, im
+
+
+def lagrange(n, t):
+    w = np.empty(n)
+    lib().orc_lagrange(int(n), float(t), _d(w))
+    return w
 
 
 def fft(x, sign=-1):

@@ -383,6 +383,24 @@ int compute_all(const double* ev, size_t p, double eta, int method, double cutof
     case NUFFT:
       nufft_points(ev, p, ev, p, eta, parallel, re, im);
       break;
+    case FFT5:
+    case FFT3:
+    case FFT2:  // mod.rs:634-641: one dual-convolution kernel for all three names
+      if (fft5_points(ev, p, ev, p, eta, 8, 0, 1000.0, 0.75, re, im)) return 4;
+      break;
+    case ADAPTIVE:
+    case DST: {
+      // adaptive.rs:43-68 / mod.rs:672-690: fft5 real part, windowed
+      // imaginary part (adaptive: ratio 10 by default; dst: the caller's
+      // cutoff, the exact blocked sums without one).
+      std::vector<double> tmp(p);
+      if (fft5_points(ev, p, ev, p, eta, 8, 0, 1000.0, 0.75, re, tmp.data())) return 4;
+      double cut = cutoff;
+      if (method == ADAPTIVE && std::isnan(cut)) cut = 10.0;
+      if (std::isnan(cut)) symmetric_sweep(ev, p, eta, tmp.data(), im);
+      else windowed(ev, p, eta, cut, tmp.data(), im);
+      break;
+    }
     default:
       return 4;
   }
@@ -423,7 +441,12 @@ int compute_at_points(const double* q, size_t nq, const double* ev, size_t p, do
 #pragma omp parallel for schedule(dynamic, 16) if (parallel)
       for (long k = 0; k < (long)nq; ++k) naive_sum(q[k], ev, p, eta, &re[k], &im[k]);
       return 0;
+    case FFT5: case FFT3: case FFT2:  // mod.rs:447-453
+      return fft5_points(q, nq, ev, p, eta, 8, 0, 1000.0, 0.75, re, im);
     case AUTOVEC:
+    // mod.rs:265-287: the remaining grid methods evaluate single points with
+    // the autovec sum.
+    case ADAPTIVE: case DST: case TREECODE: case EWALD: case HODLR:
 #pragma omp parallel for schedule(dynamic, 16) if (parallel)
       for (long k = 0; k < (long)nq; ++k) autovec_sum(q[k], ev, p, eta, &re[k], &im[k]);
       return 0;

@@ -1,9 +1,10 @@
-// TEST INFRASTRUCTURE ONLY (see oracle.h): restatement of the coarse-grid
-// NUFFT of src/stieltjes/nufft.rs (grid policy 33-126, entry points
-// 164-220) over the dual-convolution core of src/stieltjes/fft5.rs
-// (lagrange_weights 136-164, splat 175-185, interp_at 191-211,
-// fft_convolution 325-432, interpolate_grid 440-476) and the packing helpers
-// of src/stieltjes/fftplan.rs:43-76.
+// TEST INFRASTRUCTURE ONLY (see oracle.h): restatement of the FFT grid
+// convolution of src/stieltjes/fft5.rs (Fft5Options 213-249, lagrange_weights
+// 136-164, splat 175-185, splat_chunk 295-318, fft_convolution 325-432,
+// interp_at 191-211, interpolate_grid 440-476, entry points 559-625) with the
+// packing helpers of src/stieltjes/fftplan.rs:43-76, and of the coarse-grid
+// NUFFT policy over it (src/stieltjes/nufft.rs: grid policy 33-126, entry
+// points 164-220).
 //
 // The reference's transforms come from rustfft 6.4.1 (Cargo.lock), which is
 // not vendored.  Its published contract -- unnormalised DFT, forward sign
@@ -65,17 +66,32 @@ static inline void lagrange_weights(double t, double* w) {
   }
 }
 
-// fft5.rs:175-185 splat<4> (Cubic, the NUFFT default).
-static inline void splat4(double* density, size_t m, double pos) {
+// fft5.rs:175-185 splat<N>: one unit mass at grid position pos.
+template <int N>
+static inline void splat(double* density, size_t m, double pos) {
   double fl = std::floor(pos);
   long i0 = (long)fl;
   double t = pos - (double)i0;
-  double w[4];
-  lagrange_weights<4>(t, w);
-  const long off0 = -4 / 2 + 1;
-  for (int j = 0; j < 4; ++j) {
+  double w[N];
+  lagrange_weights<N>(t, w);
+  const long off0 = -N / 2 + 1;
+  for (int j = 0; j < N; ++j) {
     long cell = std::min(std::max(i0 + off0 + j, 0L), (long)m - 1);
     density[cell] += w[j];
+  }
+}
+
+// fft5.rs:295-318 splat_chunk: dispatch on the stencil width.
+static void splat_chunk(const double* ev, size_t a, size_t b, double* density, size_t m,
+                        double lo, double dx, int order) {
+  for (size_t k = a; k < b; ++k) {
+    const double pos = (ev[k] - lo) / dx;
+    switch (order) {
+      case 2: splat<2>(density, m, pos); break;
+      case 4: splat<4>(density, m, pos); break;
+      case 6: splat<6>(density, m, pos); break;
+      default: splat<8>(density, m, pos); break;
+    }
   }
 }
 
@@ -106,13 +122,40 @@ void fft_radix2(cplx* a, size_t m, int sign) {
 
 struct Grid { std::vector<cplx> out; double lo, dx; size_t m; };
 
-// fft5.rs:325-432 fft_convolution with the NUFFT options (Cubic stencil,
-// m = grid_size, pad = max(2000 eta, 0.75 raw_range)).
-static void convolution(const double* ev, size_t p, double eta, bool parallel, Grid& G) {
+// fft5.rs:213-249 Fft5Options.
+struct Opts {
+  int order;          // stencil nodes: 2, 4, 6 or 8
+  size_t m_override;  // 0 = the adaptive rule
+  double pad_eta_mult, pad_range_frac;
+};
+
+// Rust's saturating float -> usize cast (NaN -> 0, negative -> 0).
+static size_t sat_usize(double v) {
+  if (!(v > 0.0)) return 0;
+  if (v >= 18446744073709551616.0) return SIZE_MAX;
+  return (size_t)v;
+}
+
+// fft5.rs:339-361: the fft5 grid rule dx <= eta/8 and m >= 8p, capped at 2^20.
+size_t fft5_grid_size(double lo_raw, double hi_raw, size_t p, double eta, double pad_eta_mult,
+                      double pad_range_frac) {
+  const double raw_range = hi_raw - lo_raw;
+  const double pad = std::max(pad_eta_mult * eta, pad_range_frac * raw_range);
+  const double lo = lo_raw - pad, hi = hi_raw + pad;
+  const double range = hi - lo;
+  size_t min_grid = sat_usize(std::ceil(8.0 * range / eta));
+  min_grid = std::min(std::max(min_grid, 8 * p), (size_t)1024 * 1024);
+  return std::max(next_pow2(min_grid), (size_t)2);
+}
+
+// fft5.rs:325-432 fft_convolution: grid (lo, dx, m) from the first/last
+// entries, order-N splat, packed forward FFT, analytic even kernel, packed
+// product, inverse FFT.  m must be a power of two (the radix-2 restatement).
+static void convolution(const double* ev, size_t p, double eta, const Opts& o, size_t m,
+                        bool parallel, Grid& G) {
   double lo_raw = ev[0], hi_raw = ev[p - 1];
   double raw_range = hi_raw - lo_raw;
-  size_t m = std::max(nufft_grid_size(raw_range, eta), (size_t)2);
-  double pad = std::max(PAD_ETA_MULT * eta, PAD_RANGE_FRAC * raw_range);
+  double pad = std::max(o.pad_eta_mult * eta, o.pad_range_frac * raw_range);
   double lo = lo_raw - pad, hi = hi_raw + pad;
   double range = hi - lo;
   double dx = range / (double)m;
@@ -127,12 +170,12 @@ static void convolution(const double* ev, size_t p, double eta, bool parallel, G
     {
       int t = omp_get_thread_num();
       size_t a = std::min(p, (size_t)t * chunk), b = std::min(p, a + chunk);
-      for (size_t k = a; k < b; ++k) splat4(bufs[t].data(), m, (ev[k] - lo) / dx);
+      splat_chunk(ev, a, b, bufs[t].data(), m, lo, dx, o.order);
     }
     for (int t = 0; t < nt; ++t)
       for (size_t i = 0; i < m; ++i) density[i] += bufs[t][i];
   } else {
-    for (size_t k = 0; k < p; ++k) splat4(density.data(), m, (ev[k] - lo) / dx);
+    splat_chunk(ev, 0, p, density.data(), m, lo, dx, o.order);
   }
 
   std::vector<cplx> packed(m);
@@ -175,35 +218,67 @@ static void convolution(const double* ev, size_t p, double eta, bool parallel, G
   G.m = m;
 }
 
-// fft5.rs:191-211 interp_at<4> + 440-476 interpolate_grid.
-static void interpolate(const Grid& G, const double* q, size_t nq, bool parallel, double* re,
-                        double* im) {
+// fft5.rs:191-211 interp_at<N>: re <- .im, im <- .re, times 1/m.
+template <int N>
+static inline void interp_at(const Grid& G, double q, double inv_m, double* re, double* im) {
+  double pos = (q - G.lo) / G.dx;
+  long i0 = (long)std::floor(pos);
+  double t = pos - (double)i0, w[N];
+  lagrange_weights<N>(t, w);
+  const long off0 = -N / 2 + 1;
+  double ra = 0.0, ia = 0.0;
+  for (int j = 0; j < N; ++j) {
+    long cell = std::min(std::max(i0 + off0 + j, 0L), (long)G.m - 1);
+    ia += G.out[cell].real() * w[j];
+    ra += G.out[cell].imag() * w[j];
+  }
+  *re = ra * inv_m;
+  *im = ia * inv_m;
+}
+
+// fft5.rs:440-476 interpolate_grid.
+static void interpolate(const Grid& G, const double* q, size_t nq, int order, bool parallel,
+                        double* re, double* im) {
   const double inv_m = 1.0 / (double)G.m;
 #pragma omp parallel for schedule(static) if (parallel && nq >= 4096)
   for (long k = 0; k < (long)nq; ++k) {
-    double pos = (q[k] - G.lo) / G.dx;
-    long i0 = (long)std::floor(pos);
-    double t = pos - (double)i0, w[4];
-    lagrange_weights<4>(t, w);
-    double ra = 0.0, ia = 0.0;
-    for (int j = 0; j < 4; ++j) {
-      long cell = std::min(std::max(i0 - 1 + j, 0L), (long)G.m - 1);
-      ia += G.out[cell].real() * w[j];
-      ra += G.out[cell].imag() * w[j];
+    switch (order) {
+      case 2: interp_at<2>(G, q[k], inv_m, &re[k], &im[k]); break;
+      case 4: interp_at<4>(G, q[k], inv_m, &re[k], &im[k]); break;
+      case 6: interp_at<6>(G, q[k], inv_m, &re[k], &im[k]); break;
+      default: interp_at<8>(G, q[k], inv_m, &re[k], &im[k]); break;
     }
-    re[k] = ra * inv_m;
-    im[k] = ia * inv_m;
   }
 }
 
-// nufft.rs:164-220 (raw sums; `sorted_ev` follows the reference's contract
-// that the first/last entries bound the spectrum).
+static Opts nufft_opts() { return Opts{4, 0, PAD_ETA_MULT, PAD_RANGE_FRAC}; }
+
+// nufft.rs:164-220 (raw sums; the first/last entries bound the spectrum).
 void nufft_points(const double* q, size_t nq, const double* ev, size_t p, double eta,
                   bool parallel, double* re, double* im) {
   if (p == 0 || nq == 0) return;
   Grid G;
-  convolution(ev, p, eta, parallel, G);
-  interpolate(G, q, nq, parallel, re, im);
+  const size_t m = std::max(nufft_grid_size(ev[p - 1] - ev[0], eta), (size_t)2);
+  convolution(ev, p, eta, nufft_opts(), m, parallel, G);
+  interpolate(G, q, nq, 4, parallel, re, im);
+}
+
+// fft5.rs:559-625 compute_all_stieltjes_fft5_with_options /
+// compute_stieltjes_fft_at_points (raw sums, sequential).  Returns 0, or 4
+// when the grid size is not a power of two.
+int fft5_points(const double* q, size_t nq, const double* ev, size_t p, double eta, int order,
+                size_t m_override, double pad_eta_mult, double pad_range_frac, double* re,
+                double* im) {
+  if (p == 0 || nq == 0) return 0;
+  const Opts o{order, m_override, pad_eta_mult, pad_range_frac};
+  const size_t m = m_override ? std::max(m_override, (size_t)2)
+                              : fft5_grid_size(ev[0], ev[p - 1], p, eta, pad_eta_mult,
+                                               pad_range_frac);
+  if ((m & (m - 1)) != 0) return 4;
+  Grid G;
+  convolution(ev, p, eta, o, m, false, G);
+  interpolate(G, q, nq, order, false, re, im);
+  return 0;
 }
 
 }  // namespace orc
@@ -225,10 +300,11 @@ void orc_nufft_points(const double* q, size_t nq, const double* ev, size_t p, do
 size_t orc_nufft_grid(const double* ev, size_t p, double eta, double* density_out,
                       double* packed_out, double* lo_out, double* dx_out) {
   Grid G;
-  convolution(ev, p, eta, false, G);
+  const size_t m = std::max(nufft_grid_size(ev[p - 1] - ev[0], eta), (size_t)2);
+  convolution(ev, p, eta, nufft_opts(), m, false, G);
   if (density_out) {
     std::fill(density_out, density_out + G.m, 0.0);
-    for (size_t k = 0; k < p; ++k) splat4(density_out, G.m, (ev[k] - G.lo) / G.dx);
+    splat_chunk(ev, 0, p, density_out, G.m, G.lo, G.dx, 4);
   }
   if (packed_out)
     for (size_t k = 0; k < G.m; ++k) {
@@ -245,5 +321,26 @@ void orc_fft(double* interleaved, size_t m, int sign) {
 }
 
 void orc_lagrange4(double t, double* w) { lagrange_weights<4>(t, w); }
+
+// Lagrange weights of an n-node stencil (n = 2, 4, 6, 8).
+void orc_lagrange(int n, double t, double* w) {
+  switch (n) {
+    case 2: lagrange_weights<2>(t, w); break;
+    case 4: lagrange_weights<4>(t, w); break;
+    case 6: lagrange_weights<6>(t, w); break;
+    default: lagrange_weights<8>(t, w); break;
+  }
+}
+
+size_t orc_fft5_grid_size(double lo_raw, double hi_raw, size_t p, double eta, double pad_eta_mult,
+                          double pad_range_frac) {
+  return fft5_grid_size(lo_raw, hi_raw, p, eta, pad_eta_mult, pad_range_frac);
+}
+
+int orc_fft5_points(const double* q, size_t nq, const double* ev, size_t p, double eta, int order,
+                    size_t m_override, double pad_eta_mult, double pad_range_frac, double* re,
+                    double* im) {
+  return fft5_points(q, nq, ev, p, eta, order, m_override, pad_eta_mult, pad_range_frac, re, im);
+}
 
 }  // extern "C"

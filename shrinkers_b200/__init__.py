@@ -32,7 +32,7 @@ __all__ = [
     "estimate_population_eigenvalues", "ledoit_wolf_shrinkage", "shrink_eigenvalues",
     "detect_spikes_bema", "inverse_bbp", "stieltjes_at_points", "stieltjes_transform_batched",
     "stieltjes_adjoint", "parse_method", "method_name", "inverse_nonlinear_shrinkage",
-    "stieltjes_scaled_ray", "chebcode_evaluate_many",
+    "stieltjes_scaled_ray", "chebcode_evaluate_many", "stieltjes_fft5_with_options",
 ]
 
 _D = C.POINTER(C.c_double)
@@ -410,6 +410,37 @@ def stieltjes_scaled_ray(eigenvalues, scale):
     re, im = np.empty(ev.size), np.empty(ev.size)
     _native.check(_lib().shrk_stieltjes_scaled_ray(_dp(ev), ev.size, s, _dp(re), _dp(im)),
                   "stieltjes_scaled_ray")
+    return {"real": re, "imag": im}
+
+
+_ORDER = {"linear": 2, "cubic": 4, "quintic": 6, "heptic": 8}
+
+
+def stieltjes_fft5_with_options(eigenvalues, eta, order="heptic", grid_size=None,
+                                pad_eta_mult=1000.0, pad_range_frac=0.75):
+    """compute_all_stieltjes_fft5_with_options (fft5.rs:568-590): RAW sums at
+    every eigenvalue from the fft5 grid convolution, as {"real", "imag"}.
+    order: "linear" / "cubic" / "quintic" / "heptic" (or 2/4/6/8 nodes);
+    grid_size: a forced power-of-two grid (None = dx <= eta/8, m >= 8p);
+    padding max(pad_eta_mult*eta, pad_range_frac*range).  The first and last
+    entries bound the grid (ascending input expected, as in the reference)."""
+    ev = _owned_f64_vec(eigenvalues, "eigenvalues")
+    if ev.size == 0:
+        raise ValueError("eigenvalues must be non-empty")
+    _require_finite(ev, "eigenvalues")
+    e = _require_positive_finite(float(eta), "eta")
+    n = _ORDER.get(order, order) if isinstance(order, str) else int(order)
+    if n not in (2, 4, 6, 8):
+        raise ValueError(f"unknown order {order!r}")
+    m = 0 if grid_size is None else int(grid_size)
+    if m < 0:
+        raise ValueError("grid_size must be positive")
+    re, im = np.empty(ev.size), np.empty(ev.size)
+    _native.check(_lib().shrk_stieltjes_fft5_with_options(_dp(ev), ev.size, e, n, m,
+                                                          float(pad_eta_mult),
+                                                          float(pad_range_frac), _dp(re),
+                                                          _dp(im)),
+                  "stieltjes_fft5_with_options")
     return {"real": re, "imag": im}
 
 

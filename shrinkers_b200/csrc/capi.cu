@@ -2,7 +2,7 @@
 // method policy, per-device state, host<->device staging, and the host-side
 // pieces of the estimators (sort, BEMA, inverse BBP) that the reference also
 // runs on the host.  All heavy arithmetic runs in the kernels of exact.cu,
-// nufft.cu, chebcode.cu and batched.cu; there is no CPU fallback.
+// fftgrid.cu, chebcode.cu and batched.cu; there is no CPU fallback.
 #include "common.cuh"
 #include "internal.h"
 
@@ -174,18 +174,63 @@ static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
 
 // Scratch slot map: 0 split partials, 1 block bounds, 2 adjoint partials,
 // 3 input spectrum, 4/5 outputs, 6 query points, 7 raw sums (2 arrays),
-// 8 sorted copy of the sources, 9/10 hybrid temporaries, 11 NUFFT grids,
+// 8 sorted copy of the sources, 9/10 hybrid temporaries, 11 FFT grids,
 // 12/13/14/22/23 batched path (its cached graph reads 12, 13, 14 and 22, so
 // no other path may write them), 15 probe sink, 16..21 treecode,
-// 24 NUFFT stencil weights.
+// 24 FFT-grid stencil weights.
+
+static bool is_fft5_family(int m) {
+  return m == SHRK_M_FFT5 || m == SHRK_M_FFT3 || m == SHRK_M_FFT2;
+}
 
 // Raw (or scaled) sums of `method` at targets d_tgt against d_src, written
-// through `epi`.  The method must already be resolved.
+// through `epi`.  The method must already be resolved.  all_points: the
+// targets are the sources (compute_all_stieltjes, mod.rs:601-790), else
+// arbitrary query points (compute_stieltjes_at_points, mod.rs:394-494).
 static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* d_src,
                                  int64_t ns, double eta, int method,
                                  int precision, double cutoff, const Epilogue& epi,
-                                 cudaStream_t s) {
+                                 cudaStream_t s, bool all_points) {
   const bool cut = !std::isnan(cutoff);
+  // mod.rs:265-287: at query points, every grid method without a points
+  // path of its own takes the exact per-point sum.
+  if (!all_points && (method == SHRK_M_ADAPTIVE || method == SHRK_M_DST ||
+                      method == SHRK_M_TREECODE || method == SHRK_M_EWALD ||
+                      method == SHRK_M_HODLR))
+    return exact_pair_sums(d_tgt, nt, d_src, ns, eta, precision, epi, s);
+  if (is_fft5_family(method) || method == SHRK_M_ADAPTIVE || method == SHRK_M_DST) {
+    const double* ds = nullptr;
+    double first = 0.0, last = 0.0;
+    SHRK_TRY(sorted_sources(d_src, ns, &ds, &first, &last, s));
+    const Fft5Opts opts;  // fft5.rs:237-249 defaults (heptic)
+    if (is_fft5_family(method))  // mod.rs:634-641 / 447-453: one kernel, three names
+      return fft5_points(d_tgt, nt, ds, ns, first, last, eta, opts, epi, s);
+    // adaptive.rs:43-68, mod.rs:672-690: fft5 real part; imaginary part
+    // windowed (adaptive: ratio 10 by default; dst: the caller's ratio, or the
+    // exact sums without one).
+    void* raw = nullptr;
+    SHRK_TRY(scratch_get(7, sizeof(double) * 2 * nt, &raw));
+    double* rre = (double*)raw;
+    double* rim = rre + nt;
+    void* tmp = nullptr;
+    SHRK_TRY(scratch_get(9, sizeof(double) * nt, &tmp));
+    Epilogue e1;
+    e1.mode = EPI_SUMS;
+    e1.scale = 1.0;
+    e1.out_re = rre;
+    e1.out_im = (double*)tmp;
+    SHRK_TRY(fft5_points(d_tgt, nt, ds, ns, first, last, eta, opts, e1, s));
+    const double ratio = (method == SHRK_M_ADAPTIVE && !cut) ? 10.0 : cutoff;
+    if (std::isnan(ratio)) {
+      Epilogue e2 = e1;  // real part into the scratch, imaginary part kept
+      e2.out_re = (double*)tmp;
+      e2.out_im = rim;
+      SHRK_TRY(exact_pair_sums(d_tgt, nt, d_src, ns, eta, precision, e2, s));
+    } else {
+      SHRK_TRY(windowed_sums(d_tgt, nt, ds, ns, eta, ratio * eta, 1.0, (double*)tmp, rim, s));
+    }
+    return apply_epilogue(d_tgt, rre, rim, nt, epi, s);
+  }
   if (is_exact_family(method)) {
     const bool windowed_re = cut && (method == SHRK_M_BLOCKED || method == SHRK_M_BLOCKED_TILED ||
                                      method == SHRK_M_BLOCKED_WINDOWED ||
@@ -223,9 +268,9 @@ static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* 
     } else {
       ChebParams prm;
       cheb_preset(method, &prm);
-      // At arbitrary query points (targets are not the sources) the leaf
-      // capacity is relaxed by the grid rule (mod.rs:475-489).
-      if (d_tgt != d_src) prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nt, prm.leaf_cap);
+      // At arbitrary query points the leaf capacity is relaxed by the grid
+      // rule (mod.rs:475-489).
+      if (!all_points) prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nt, prm.leaf_cap);
       SHRK_TRY(chebcode_points(d_tgt, nt, ds, ns, eta, prm, epi, s));
     }
     return SHRK_OK;
@@ -324,7 +369,7 @@ static shrk_status lw_device(const double* ev, size_t p, double c, int method, i
   epi.c = c;
   epi.out_re = (double*)out;
   SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, (int64_t)p, eta,
-                         m, precision, NAN, epi, s));
+                         m, precision, NAN, epi, s, true));
   SHRK_TRY(d2h(xi, out, sizeof(double) * p, s));
   return check_device_error(s);
 }
@@ -367,7 +412,7 @@ static shrk_status deconv_device(const double* ev, size_t p, double c, size_t n_
   epi.eta = eta_val;
   for (int i = 0; i < 6; ++i) epi.out[i] = (double*)out + i * n_points;
   SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)n_points, (const double*)dev, (int64_t)p,
-                         eta_val, m, precision, cutoff, epi, s));
+                         eta_val, m, precision, cutoff, epi, s, false));
   SHRK_TRY(d2h(out7 + n_points, out, sizeof(double) * 6 * n_points, s));
   return check_device_error(s);
 }
@@ -493,7 +538,7 @@ shrk_status shrk_stieltjes_all_dev(const double* d_ev, size_t p, double eta, int
   epi.out_re = d_re;
   epi.out_im = d_im;
   return sums_dispatch(d_ev, (int64_t)p, d_ev, (int64_t)p, eta, m, precision, cutoff,
-                       epi, s);
+                       epi, s, true);
 }
 
 shrk_status shrk_stieltjes_all(const double* ev, size_t p, double eta, int method, int precision,
@@ -515,7 +560,7 @@ shrk_status shrk_stieltjes_all(const double* ev, size_t p, double eta, int metho
   epi.out_re = (double*)out;
   epi.out_im = (double*)out + p;
   SHRK_TRY(sums_dispatch((const double*)dev, (int64_t)p, (const double*)dev, (int64_t)p, eta,
-                         m, precision, cutoff, epi, s));
+                         m, precision, cutoff, epi, s, true));
   SHRK_TRY(d2h(out_re, out, sizeof(double) * p, s));
   SHRK_TRY(d2h(out_im, (double*)out + p, sizeof(double) * p, s));
   return check_device_error(s);
@@ -573,7 +618,7 @@ shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const dou
   epi.out_re = d_re;
   epi.out_im = d_im;
   return sums_dispatch(d_q, (int64_t)nq, d_ev, (int64_t)p, eta, m, precision, cutoff,
-                       epi, s);
+                       epi, s, false);
 }
 
 shrk_status shrk_stieltjes_at_points(const double* q, size_t nq, const double* ev, size_t p,
@@ -602,7 +647,7 @@ shrk_status shrk_stieltjes_at_points(const double* q, size_t nq, const double* e
   epi.out_re = (double*)out;
   epi.out_im = (double*)out + nq;
   SHRK_TRY(sums_dispatch((const double*)dq, (int64_t)nq, (const double*)dev, (int64_t)p, eta,
-                         m, precision, cutoff, epi, s));
+                         m, precision, cutoff, epi, s, false));
   SHRK_TRY(d2h(raw_re, out, sizeof(double) * nq, s));
   SHRK_TRY(d2h(raw_im, (double*)out + nq, sizeof(double) * nq, s));
   return check_device_error(s);
@@ -854,6 +899,74 @@ shrk_status shrk_stieltjes_scaled_ray(const double* ev, size_t p, double scale, 
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
   SHRK_TRY(scaled_ray_sums((const double*)dev, (int64_t)p, scale, (double*)out,
                            (double*)out + p, s));
+  SHRK_TRY(d2h(raw_re, out, sizeof(double) * p, s));
+  SHRK_TRY(d2h(raw_im, (double*)out + p, sizeof(double) * p, s));
+  return check_device_error(s);
+}
+
+static shrk_status check_fft5_opts(size_t p, double eta, int order, double pad_eta_mult,
+                                   double pad_range_frac) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (!(std::isfinite(eta) && eta > 0.0)) return einval("eta must be a positive finite number");
+  if (order != 2 && order != 4 && order != 6 && order != 8)
+    return einval("order must be 2, 4, 6 or 8 stencil nodes");
+  if (!std::isfinite(pad_eta_mult) || !std::isfinite(pad_range_frac))
+    return einval("padding multipliers must be finite");
+  return SHRK_OK;
+}
+
+shrk_status shrk_stieltjes_fft5_with_options_dev(const double* d_ev, size_t p, double eta,
+                                                 int order, size_t m_override,
+                                                 double pad_eta_mult, double pad_range_frac,
+                                                 double* d_re, double* d_im, void* stream) {
+  SHRK_TRY(check_fft5_opts(p, eta, order, pad_eta_mult, pad_range_frac));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;
+  const double* ds = nullptr;
+  double first = 0.0, last = 0.0;
+  SHRK_TRY(sorted_sources(d_ev, (int64_t)p, &ds, &first, &last, s));
+  Fft5Opts o;
+  o.order = order;
+  o.m_override = m_override;
+  o.pad_eta_mult = pad_eta_mult;
+  o.pad_range_frac = pad_range_frac;
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = 1.0;
+  epi.out_re = d_re;
+  epi.out_im = d_im;
+  return fft5_points(d_ev, (int64_t)p, ds, (int64_t)p, first, last, eta, o, epi, s);
+}
+
+shrk_status shrk_stieltjes_fft5_with_options(const double* ev, size_t p, double eta, int order,
+                                             size_t m_override, double pad_eta_mult,
+                                             double pad_range_frac, double* raw_re,
+                                             double* raw_im) {
+  SHRK_TRY(check_fft5_opts(p, eta, order, pad_eta_mult, pad_range_frac));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  const double* ds = nullptr;
+  double first = 0.0, last = 0.0;
+  SHRK_TRY(sorted_sources((const double*)dev, (int64_t)p, &ds, &first, &last, s));
+  Fft5Opts o;
+  o.order = order;
+  o.m_override = m_override;
+  o.pad_eta_mult = pad_eta_mult;
+  o.pad_range_frac = pad_range_frac;
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = 1.0;
+  epi.out_re = (double*)out;
+  epi.out_im = (double*)out + p;
+  SHRK_TRY(fft5_points((const double*)dev, (int64_t)p, ds, (int64_t)p, first, last, eta, o, epi,
+                       s));
   SHRK_TRY(d2h(raw_re, out, sizeof(double) * p, s));
   SHRK_TRY(d2h(raw_im, (double*)out + p, sizeof(double) * p, s));
   return check_device_error(s);

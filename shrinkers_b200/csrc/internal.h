@@ -88,6 +88,22 @@ shrk_status nufft_points(const double* d_q, int64_t nq, const double* d_sorted_s
                          cudaStream_t s);
 size_t nufft_grid_size(double raw_range, double eta);
 
+// fft5.rs:213-249 Fft5Options: stencil nodes (2/4/6/8), forced grid size
+// (0 = the adaptive rule dx <= eta/8, m >= 8p), padding multipliers.
+struct Fft5Opts {
+  int order = 8;
+  size_t m_override = 0;
+  double pad_eta_mult = 1000.0;
+  double pad_range_frac = 0.75;
+};
+// fft5 grid convolution at nq points (same source contract as nufft_points);
+// SHRK_ENOTIMPL when the grid size is not a power of two <= 2^22.
+shrk_status fft5_points(const double* d_q, int64_t nq, const double* d_sorted_src, int64_t ns,
+                        double lo_raw, double hi_raw, double eta, const Fft5Opts& o,
+                        const Epilogue& epi, cudaStream_t s);
+size_t fft5_grid_size(double lo_raw, double hi_raw, size_t p, double eta, double pad_eta_mult,
+                      double pad_range_frac);
+
 // Chebyshev treecode at nq points, epilogue fused into the evaluation.
 struct ChebParams { double theta; int n; int leaf_cap; bool f32; };
 bool cheb_preset(int method, ChebParams* out);

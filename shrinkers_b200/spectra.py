@@ -109,3 +109,24 @@ def config5(p: int, seed: int = 5) -> np.ndarray:
 def log_spectrum(p: int) -> np.ndarray:
     """ln(1..p), the reference's canonical test spectrum (testutil.rs:10-12)."""
     return np.log(np.arange(1, p + 1, dtype=np.float64))
+
+
+def harness_spectrum(p: int) -> np.ndarray:
+    """The reference benchmarks' deterministic MP-like spectrum
+    (benches/support/mod.rs:17-35 ``Lcg``, 65-80 ``harness_spectrum``): a
+    c = 0.5 Marchenko-Pastur support filled uniformly by a 64-bit LCG seeded
+    with 42, plus two outliers hi*2.3 and lo*0.35, sorted ascending (p < 3:
+    the first p LCG draws, unsorted)."""
+    c = 0.5
+    lo = (1.0 - float(np.sqrt(c))) ** 2
+    hi = (1.0 + float(np.sqrt(c))) ** 2
+    mask = (1 << 64) - 1
+    state = 42
+    n = p if p < 3 else p - 2
+    out = np.empty(n)
+    for k in range(n):
+        state = (state * 6364136223846793005 + 1442695040888963407) & mask
+        out[k] = lo + ((state >> 11) / float(1 << 53)) * (hi - lo)
+    if p < 3:
+        return out
+    return np.sort(np.concatenate([out, [hi * 2.3, lo * 0.35]]))

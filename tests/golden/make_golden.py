@@ -167,6 +167,27 @@ def main(root: str) -> None:
         "max_relative": 1e-11,
     }
 
+    # ---- fft5 accuracy sweep: the reference's own measured output
+    # (docs/pareto/order_sweep.jsonl, written by examples/measure_fft_order_sweep.rs
+    # on benches/support/mod.rs:65-80 harness_spectrum, eta = 1/sqrt(p),
+    # error = rel-L2 vs the exact sums, support/mod.rs:126-135).
+    path = os.path.join(root, "docs", "pareto", "order_sweep.jsonl")
+    rows = [json.loads(line) for line in open(path) if line.strip()]
+    out["fft5_order_sweep"] = {
+        "source": "docs/pareto/order_sweep.jsonl (examples/measure_fft_order_sweep.rs)",
+        "printed_digits": 4,
+        "rows": [{k: r[k] for k in ("kind", "p", "order", "m", "err", "pad_mult") if k in r}
+                 for r in rows],
+    }
+    ex = os.path.join(src, "stieltjes", "fft5.rs")
+    text = open(ex).read()
+    out["fft5_pipeline_ordering"] = {
+        "source": f"src/stieltjes/fft5.rs:{_line_of(text, 'fn test_heptic_default_not_worse_on_pipeline')}",
+        "p": 5000, "c": 0.5, "m": 8192, "outliers": ["hi*2.3", "lo*0.35"],
+        "bulk_rule": "lo + ((i+0.5)/p)*(hi-lo)", "inv_p": "1/p (p excludes the outliers)",
+        "assert": "e_cubic < e_linear and e_heptic <= e_cubic",
+    }
+
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
     with open(dst, "w") as f:
         json.dump(out, f, indent=1)

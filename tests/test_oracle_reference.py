@@ -210,9 +210,112 @@ def test_fft_matches_dft(oracle):
 
 
 def test_lagrange_partition_of_unity(oracle):
-    """fft5.rs:774-804."""
+    """fft5.rs:774-804: every stencil width, t = s/97 for s in 0..97."""
     for t in np.linspace(0, 0.999, 17):
         assert abs(oracle.lagrange4(t).sum() - 1.0) < 1e-14
+    for n in (2, 4, 6, 8):
+        for s in range(97):
+            w = oracle.lagrange(n, s / 97.0)
+            assert abs(w.sum() - 1.0) < 1e-12
+            assert np.all(np.isfinite(w)) and np.all(np.abs(w) < 10.0)
+
+
+# ------------------------------------------------------------------- fft5 --
+_ORDERS = {"linear": 2, "cubic": 4, "quintic": 6, "heptic": 8}
+
+
+def _harness_exact(oracle, p, cache={}):
+    if p not in cache:
+        ev = spectra.harness_spectrum(p)
+        eta = 1.0 / np.sqrt(p)
+        cache[p] = (ev, eta, *oracle.compute_all(ev, eta, "blocked_tiled", parallel=True))
+    return cache[p]
+
+
+def test_fft5_reproduces_the_reference_order_sweep(oracle, golden):
+    """The reference's own measured fft5 errors (docs/pareto/order_sweep.jsonl,
+    144 rows: p in {1000, 5000, 20000}, 4 stencils, forced and adaptive grids,
+    6 paddings) are reproduced by the restatement to the 4 printed digits."""
+    g = golden["fft5_order_sweep"]
+    worst = 0.0
+    for r in g["rows"]:
+        ev, eta, ere, eim = _harness_exact(oracle, r["p"])
+        kw = dict(order=_ORDERS[r["order"]], m=r["m"])
+        if r["kind"] == "pad":
+            kw["pad_eta_mult"] = float(r["pad_mult"])
+        gre, gim = oracle.fft5_points(ev, ev, eta, **kw)
+        # support/mod.rs:126-135 rel_l2_scaled: raw sums times 1/len
+        err = rel_l2(gre / ev.size, gim / ev.size, ere, eim)
+        worst = max(worst, abs(err - r["err"]) / r["err"])
+    assert worst < 1e-3, worst
+
+
+def test_fft5_adaptive_grid_sizes(oracle, golden):
+    """The adaptive grid (m = null rows) is the forced grid whose error it
+    repeats: 32768 at p = 1000, 65536 at 5000, 262144 at 20000."""
+    rows = golden["fft5_order_sweep"]["rows"]
+    for p, m in [(1000, 32768), (5000, 65536), (20000, 262144)]:
+        ev = spectra.harness_spectrum(p)
+        assert oracle.fft5_grid_size(ev, 1.0 / np.sqrt(p)) == m
+        auto = {r["order"]: r["err"] for r in rows if r["kind"] == "grid" and r["p"] == p
+                and r["m"] is None}
+        forced = {r["order"]: r["err"] for r in rows if r["kind"] == "grid" and r["p"] == p
+                  and r["m"] == m}
+        assert auto == forced
+
+
+def test_fft5_pipeline_ordering(oracle, golden):
+    """fft5.rs:874-925: at a forced m = 8192 the error orders heptic <= cubic
+    < linear (the test's 1/p excludes the two outliers)."""
+    g = golden["fft5_pipeline_ordering"]
+    p, c = g["p"], g["c"]
+    lo, hi = (1 - np.sqrt(c)) ** 2, (1 + np.sqrt(c)) ** 2
+    ev = np.sort(np.concatenate([lo + ((np.arange(p) + 0.5) / p) * (hi - lo),
+                                 [hi * 2.3, lo * 0.35]]))
+    eta = 1.0 / np.sqrt(p)
+    ere, eim = oracle.compute_all(ev, eta, "blocked_tiled")
+    err = {}
+    for n in (2, 4, 8):
+        gre, gim = oracle.fft5_points(ev, ev, eta, order=n, m=g["m"])
+        err[n] = rel_l2(gre / p, gim / p, ere, eim)
+    assert err[4] < err[2] and err[8] <= err[4]
+
+
+def test_fft_family_dispatch(oracle):
+    """mod.rs:634-641 / 672-690, adaptive.rs:43-68: fft5/fft3/fft2 are one
+    kernel; adaptive = fft5 real part + windowed imaginary part (ratio 10 by
+    default); dst = fft5 real part + the caller's window, or the exact
+    imaginary part without one; the single-point fallback of every other grid
+    method is the autovec sum (mod.rs:265-287)."""
+    p = 3000
+    ev = spectra.log_spectrum(p)
+    eta = 0.1 / np.sqrt(p)
+    f5 = oracle.compute_all(ev, eta, "fft5")
+    for name in ("fft3", "fft2"):
+        r = oracle.compute_all(ev, eta, name)
+        np.testing.assert_array_equal(r[0], f5[0])
+        np.testing.assert_array_equal(r[1], f5[1])
+    win = oracle.compute_all(ev, eta, "blocked_windowed", cutoff=10.0)
+    ad = oracle.compute_all(ev, eta, "adaptive")
+    np.testing.assert_array_equal(ad[0], f5[0])
+    np.testing.assert_array_equal(ad[1], win[1])
+    win7 = oracle.compute_all(ev, eta, "blocked_windowed", cutoff=7.0)
+    ds = oracle.compute_all(ev, eta, "dst", cutoff=7.0)
+    np.testing.assert_array_equal(ds[0], f5[0])
+    np.testing.assert_array_equal(ds[1], win7[1])
+    ex = oracle.compute_all(ev, eta, "blocked")
+    ds0 = oracle.compute_all(ev, eta, "dst")
+    np.testing.assert_array_equal(ds0[1], ex[1])
+    # adaptive.rs:76-99: finite everywhere
+    assert np.all(np.isfinite(ad[0])) and np.all(np.isfinite(ad[1]))
+    q = np.linspace(ev[0], ev[-1], 50)
+    av = oracle.compute_at_points(q, ev, eta, "autovec")
+    for name in ("adaptive", "dst", "treecode", "ewald", "hodlr"):
+        r = oracle.compute_at_points(q, ev, eta, name)
+        np.testing.assert_array_equal(r[0], av[0])
+    fq = oracle.compute_at_points(q, ev, eta, "fft5")
+    fp = oracle.fft5_points(q, ev, eta)
+    np.testing.assert_array_equal(fq[0], fp[0])
 
 
 def test_truth_matches_exact(oracle):
