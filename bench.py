@@ -50,10 +50,10 @@ def parse():
                     help="spectrum size (default: the workload's own size)")
     ap.add_argument("--workload", default="exact",
                     choices=["exact", "adjoint", "batched", "chebcode_fast", "chebcode",
-                             "chebcode_xtreme", "nufft"],
+                             "chebcode_xtreme", "nufft", "fft5"],
                     help="exact (default, the headline): all-points exact transform at p=1M; "
                          "adjoint: the adjoint kernel at p=20000; batched: 4096 uneven "
-                         "spectra; chebcode*/nufft: the method at p=1M on the spiked "
+                         "spectra; chebcode*/nufft/fft5: the method at p=1M on the spiked "
                          "spectrum")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
@@ -326,7 +326,9 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
-METHOD_IDS = {"chebcode": 13, "chebcode_fast": 14, "chebcode_xtreme": 15, "nufft": 11}
+METHOD_IDS = {"chebcode": 13, "chebcode_fast": 14, "chebcode_xtreme": 15, "nufft": 11,
+              "fft5": 8}
+FFT5_FAMILIES = (b"fft5_splat", b"fft5_fft", b"fft5_spectral", b"fft5_interp")
 CHEB_PRESETS = {"chebcode": (0.5, 11, 32, False), "chebcode_fast": (1.0, 8, 32, True),
                 "chebcode_xtreme": (0.25, 11, 16, False)}
 
@@ -437,8 +439,8 @@ def run_path(args, world, rank, local):
         xi = torch.empty_like(xr)
         mid = METHOD_IDS[wl]
         units = float(p) * p
-        family = b"nufft_splat" if wl == "nufft" else (
-            b"cheb_eval_f32" if wl == "chebcode_fast" else b"cheb_eval_f64")
+        family = {"nufft": b"nufft_splat", "fft5": b"fft5_fft",
+                  "chebcode_fast": b"cheb_eval_f32"}.get(wl, b"cheb_eval_f64")
         desc = (f"{wl} all-points transform (tree build / grid included), MP(c=0.1)+20 spikes "
                 f"in [3,50] p={p}, eta=1/sqrt(p)")
 
@@ -458,6 +460,8 @@ def run_path(args, world, rank, local):
             t0 = time.perf_counter()
             if wl == "nufft":
                 O.nufft_points(ev_h, ev_h, eta, parallel=True)
+            elif wl == "fft5":  # the reference's fft5 runs sequentially (fft5.rs:589)
+                O.fft5_points(ev_h, ev_h, eta)
             else:
                 th, nn_, leaf, f32 = CHEB_PRESETS[wl]
                 O.chebcode_points(ev_h, ev_h, eta, th, nn_, leaf, f32, parallel=True)
@@ -491,6 +495,14 @@ def run_path(args, world, rank, local):
     L.shrk_timing_enable(0)
     kn, kms = C.c_int64(), C.c_double()
     L.shrk_timing_read(family, C.byref(kn), C.byref(kms))
+    fams = {}
+    if wl == "fft5":  # the dominant launch family of the pipeline
+        for f in FFT5_FAMILIES:
+            n_, ms_ = C.c_int64(), C.c_double()
+            L.shrk_timing_read(f, C.byref(n_), C.byref(ms_))
+            fams[f.decode()] = (n_.value, ms_.value)
+        family = max(FFT5_FAMILIES, key=lambda f: fams[f.decode()][1])
+        kn, kms = C.c_int64(fams[family.decode()][0]), C.c_double(fams[family.decode()][1])
     total_ms = float(np.sum(times))
     if pg:
         t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
@@ -532,6 +544,26 @@ def run_path(args, world, rank, local):
                     "frac": alg / k_s / 1e9 / _measured_hbm(), "traffic": None,
                     "kernel": "nufft_splat", "kernel_ms": k_s * 1e3,
                     "basis": "splat: 8 B per source read + 64 B per grid cell written"}
+        elif wl == "fft5" and kn.value:
+            m = O.fft5_grid_size(ev_h, eta)
+            fam = family.decode()
+            alg_step, basis = {
+                "fft5_splat": (8 * p + 16 * m, "splat (weights + gather launches): 8 B per "
+                               "source read + 16 B per grid cell written, per step"),
+                "fft5_fft": (128 * m, "two transforms of two four-step passes: 16 B per cell "
+                             "read + 16 B written per pass, per step"),
+                "fft5_spectral": (40 * m, "spectral product: 16+8 B per cell read, 16 B "
+                                  "written, per step"),
+                "fft5_interp": (24 * p + 16 * m, "interpolation: 8 B per point read, 16 B "
+                                "written, the grid read once, per step"),
+            }[fam]
+            per_step = kn.value / max(1, args.steps)  # launches of the family per step
+            alg = alg_step / per_step
+            ach = alg / k_s / 1e9
+            roof = {"bound": "hbm", "achieved": ach, "peak": _measured_hbm(), "unit": "GB/s",
+                    "frac": ach / _measured_hbm(), "traffic": None, "kernel": fam,
+                    "kernel_ms": k_s * 1e3, "grid_cells": m, "basis": basis,
+                    "families_ms": {k: v[1] / max(1, args.steps) for k, v in fams.items()}}
         rate, sample = cpu()
         cpu_line = {"value": rate, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
                     "sample": sample}

@@ -11,27 +11,29 @@
 //
 //   1. weights      one thread per source: stencil cell i0 = floor((v-lo)/dx)
 //                   and the N Lagrange weights of t = pos - i0.
-//   2. gather+pack  one thread per grid cell; a CTA of 256 cells finds the
-//                   run of sources whose stencils touch it (two warp-wide
-//                   searches), stages their cells in shared memory, and each
-//                   thread adds its sources' weights in ascending source
-//                   order -- the order of the reference's sequential splat,
-//                   so the density is the same sums, without atomics.  Grids
-//                   with more than two sources per cell (the NUFFT's coarse
-//                   grid) use one warp per cell instead.  Then
+//   2. runs         the last source of each run of equal cells marks it;
+//                   an exclusive max-scan turns the marks into first[key] =
+//                   the first source with cell >= key.
+//   3. gather+pack  one thread per grid cell adds the weights of its sources
+//                   (at most 32) run by run in ascending source order -- the
+//                   order of the reference's sequential splat, so these
+//                   densities are the same sums, without atomics -- and
+//                   queues denser cells for one warp (or one CTA) each.
 //                   packed[c] = density[c] + i x_c/(x_c^2 + eta^2).
-//   3. fft          four-step FFT m = m1*m2 (m1, m2 <= 2048): column FFTs of
+//   4. fft          four-step FFT m = m1*m2 (m1, m2 <= 2048): column FFTs of
 //                   length m1 in shared memory with the inter-pass twiddle,
 //                   then row FFTs of length m2.  Twiddles and the analytic
 //                   even-kernel spectrum are device tables cached per grid.
-//   4. spectral     unpack the two real spectra (conjugate symmetry), form
+//   5. spectral     unpack the two real spectra (conjugate symmetry), form
 //                   Im_hat + i Re_hat = D*K_even + i D*K_odd.
-//   5. fft          inverse transform.
-//   6. interp       N-point interpolation at the query points, 1/m scale,
+//   6. fft          inverse transform.
+//   7. interp       N-point interpolation at the query points, 1/m scale,
 //                   fused FP64 epilogue.
 #include "common.cuh"
 #include "epilogue.cuh"
 #include "internal.h"
+
+#include <cub/cub.cuh>
 
 #include <cmath>
 #include <map>
@@ -116,143 +118,87 @@ struct GridArgs {
   double2* packed;
 };
 
-// Per source: stencil cell and weights (fft5.rs:175-185).  The visiting order
-// makes cell[] non-decreasing.
 template <int N>
-__global__ void splat_weights_kernel(const GridArgs a) {
+__device__ __forceinline__ int clamped_cell(const GridArgs& a, int64_t j, double* t) {
+  const double v = a.rev ? a.src[a.ns - 1 - j] : a.src[j];
+  const int64_t i0 = cell_of<N>(v, a.lo, a.dx, a.m, t);
+  return (int)(i0 < -N ? -N : (i0 > a.m + N ? a.m + N : i0));
+}
+
+// Per source: stencil cell and weights (fft5.rs:175-185).  The visiting order
+// makes cell[] non-decreasing; the last source of each run of equal cells
+// also records last[cell - k_lo] = its index + 1 (k_lo = -N - 1).
+template <int N>
+__global__ void splat_weights_kernel(const GridArgs a, int* __restrict__ last) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.ns) return;
-  const double v = a.rev ? a.src[a.ns - 1 - j] : a.src[j];
-  double t;
-  int64_t i0 = cell_of<N>(v, a.lo, a.dx, a.m, &t);
+  double t, t_next;
+  const int ci = clamped_cell<N>(a, j, &t);
   double w[N];
   lagrange<N>(t, w);
-  i0 = i0 < -N ? -N : (i0 > a.m + N ? a.m + N : i0);
-  a.cell[j] = (int)i0;
+  a.cell[j] = ci;
 #pragma unroll
   for (int k = 0; k < N; ++k) a.w[(int64_t)k * a.ns + j] = w[k];
+  if (j == a.ns - 1 || clamped_cell<N>(a, j + 1, &t_next) != ci) last[ci + N + 1] = (int)(j + 1);
 }
 
-// First source index j with cell[j] >= key (ns if none), cell[] non-
-// decreasing: a 32-way search where every lane probes one point per round.
-__device__ int64_t warp_first_ge(const int* __restrict__ cell, int64_t ns, int key, int lane) {
-  int64_t lo = 0, hi = ns;  // the answer lies in [lo, hi]
-  while (hi - lo > 32) {
-    const int64_t step = (hi - lo + 31) / 32;
-    const int64_t q = lo + (int64_t)lane * step;
-    const bool less = q < hi && cell[q] < key;
-    const int cnt = __popc(__ballot_sync(0xffffffffu, less));
-    const int64_t nlo = cnt > 0 ? lo + (int64_t)(cnt - 1) * step + 1 : lo;
-    hi = min(hi, lo + (int64_t)cnt * step);
-    lo = nlo;
-  }
-  const int64_t q = lo + lane;
-  const bool less = q < hi && cell[q] < key;
-  return lo + __popc(__ballot_sync(0xffffffffu, less));
-}
+constexpr int DENSE_MIN = 32;    // sources above which a cell gets a whole warp
+constexpr int CTA_MIN = 2048;    // ... and above which it gets a whole CTA
 
-// First index in [lo, hi) of a non-decreasing array with value >= key.
-__device__ __forceinline__ int64_t first_ge(const int* __restrict__ v, int64_t lo, int64_t hi,
-                                            int key) {
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (v[mid] < key) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
+struct GatherArgs {
+  GridArgs g;
+  const int* first;  // first[key + N + 1] = #sources with cell < key, key in [-N-1, m+N]
+  int* dense;        // cells left for pack_dense_kernel: [0, m) warp queue, [m, 2m) CTA queue
+  int* n_dense;      // the two queue lengths
+};
 
-constexpr int GATHER_T = 256;     // grid cells per CTA
-constexpr int GATHER_CAP = 4096;  // source cells staged in shared memory
+// Exclusive max-scan operator: first[key] = max over cells below key of last[].
+struct MaxOp {
+  __device__ __forceinline__ int operator()(int x, int y) const { return x > y ? x : y; }
+};
 
-// Steps 1+pack: the density of cell c is the sum of weight k = c + N/2 - 1 - i0
-// over the sources with i0 in [c - N/2, c + N/2 - 1] (fft5.rs:175-185), in
-// ascending source order; the two edge cells also collect every clamped slot.
-// Then packed[c] = density[c] + i x_c/(x_c^2 + eta^2) (fft5.rs:364-376).
-template <int N>
-__global__ void __launch_bounds__(GATHER_T) splat_gather_kernel(const GridArgs a) {
-  constexpr int H = N / 2;
-  __shared__ int s_cell[GATHER_CAP];
-  __shared__ int64_t s_run[2];
-  const int64_t m = a.m;
-  const int64_t c0 = (int64_t)blockIdx.x * GATHER_T;
-  const int64_t c = c0 + threadIdx.x;
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    const int64_t clast = min(c0 + GATHER_T - 1, m - 1);
-    const int64_t jA = warp_first_ge(a.cell, a.ns, (int)(c0 - H), lane);
-    const int64_t jB = warp_first_ge(a.cell, a.ns, (int)(clast + H), lane);
-    if (lane == 0) {
-      s_run[0] = jA;
-      s_run[1] = jB;
-    }
-  }
-  __syncthreads();
-  const int64_t jA = s_run[0], jB = s_run[1];
-  const int64_t n = jB - jA;
-  const bool staged = n <= GATHER_CAP;
-  if (staged)
-    for (int64_t i = threadIdx.x; i < n; i += GATHER_T) s_cell[i] = a.cell[jA + i];
-  __syncthreads();
-  if (c >= m) return;
-  double dens = 0.0;
-  if (c > 0 && c < m - 1) {
-    int64_t j0, j1;
-    if (staged) {
-      j0 = jA + first_ge(s_cell, 0, n, (int)c - H);
-      j1 = jA + first_ge(s_cell, j0 - jA, n, (int)c + H);
-    } else {
-      j0 = first_ge(a.cell, jA, jB, (int)c - H);
-      j1 = first_ge(a.cell, j0, jB, (int)c + H);
-    }
-    for (int64_t j = j0; j < j1; ++j) {
-      const int i0 = staged ? s_cell[j - jA] : a.cell[j];
-      dens += a.w[(int64_t)((int)c + H - 1 - i0) * a.ns + j];
-    }
-  } else {
-    // edge cell: every slot whose clamped index lands here, sources then slots
-    const int64_t j0 = (c == 0) ? 0 : first_ge(a.cell, 0, a.ns, (int)(m - 1 - H));
-    const int64_t j1 = (c == 0) ? first_ge(a.cell, 0, a.ns, H) : a.ns;
-    for (int64_t j = j0; j < j1; ++j) {
-      const int i0 = a.cell[j];
-#pragma unroll
-      for (int k = 0; k < N; ++k) {
-        int64_t cell = (int64_t)i0 - H + 1 + k;
-        cell = cell < 0 ? 0 : (cell > m - 1 ? m - 1 : cell);
-        if (cell == c) dens += a.w[(int64_t)k * a.ns + j];
-      }
-    }
-  }
-  const int64_t half = m / 2;
-  const double sd = (c <= half) ? (double)c : (double)c - (double)m;
+// Steps 1+pack: the density of cell c is the sum of weight k over the run of
+// sources with i0 = c + N/2 - 1 - k, for k = N-1 .. 0 (fft5.rs:175-185): the
+// runs in ascending cell order, i.e. the sources in ascending order -- the
+// order of the reference's sequential splat.  The two edge cells also collect
+// every clamped slot.  One thread per cell adds at most DENSE_MIN sources and
+// queues denser cells for pack_dense_kernel.  packed[c] = density[c] +
+// i x_c/(x_c^2 + eta^2) (fft5.rs:364-376).
+__device__ __forceinline__ void pack_cell(const GridArgs& a, int64_t c, double dens) {
+  const int64_t half = a.m / 2;
+  const double sd = (c <= half) ? (double)c : (double)c - (double)a.m;
   const double x = sd * a.dx;
   const double denom = x * x + a.eta * a.eta;
   a.packed[c] = make_double2(dens, x / denom);
 }
 
-// The same density for grids with many sources per cell (the NUFFT's coarse
-// grid): one warp per cell, lanes stride the cell's source run and a fixed
-// butterfly adds the lane sums (deterministic; the addition order is not the
-// sequential one).
 template <int N>
-__global__ void splat_gather_warp_kernel(const GridArgs a) {
+__global__ void __launch_bounds__(256) pack_sparse_kernel(const GatherArgs ga) {
   constexpr int H = N / 2;
-  const int64_t c = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (c >= a.m) return;  // whole warps exit together
+  const GridArgs& a = ga.g;
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t m = a.m;
+  if (c >= m) return;
+  const int* first = ga.first + N + 1;  // first[key] for key >= -N - 1
   double dens = 0.0;
   if (c > 0 && c < m - 1) {
-    const int64_t j0 = warp_first_ge(a.cell, a.ns, (int)c - H, lane);
-    const int64_t j1 = warp_first_ge(a.cell, a.ns, (int)c + H, lane);
-    for (int64_t j = j0 + lane; j < j1; j += 32) {
-      const int k = (int)c + H - 1 - a.cell[j];
-      dens += a.w[(int64_t)k * a.ns + j];
+    const int cnt = first[c + H] - first[c - H];
+    if (cnt > DENSE_MIN) {
+      const int q = cnt > CTA_MIN ? 1 : 0;
+      ga.dense[q * m + atomicAdd(ga.n_dense + q, 1)] = (int)c;
+      return;
+    }
+#pragma unroll
+    for (int k = N - 1; k >= 0; --k) {
+      const int64_t e = c + H - 1 - k;
+      const double* wk = a.w + (int64_t)k * a.ns;
+      for (int64_t j = first[e], j1 = first[e + 1]; j < j1; ++j) dens += wk[j];
     }
   } else {
-    const int64_t j0 = (c == 0) ? 0 : warp_first_ge(a.cell, a.ns, (int)(m - 1 - H), lane);
-    const int64_t j1 = (c == 0) ? warp_first_ge(a.cell, a.ns, H, lane) : a.ns;
-    for (int64_t j = j0 + lane; j < j1; j += 32) {
+    // edge cell: every slot whose clamped index lands here, sources then slots
+    const int64_t j0 = (c == 0) ? 0 : first[m - 1 - H];
+    const int64_t j1 = (c == 0) ? first[H] : a.ns;
+    for (int64_t j = j0; j < j1; ++j) {
       const int i0 = a.cell[j];
 #pragma unroll
       for (int k = 0; k < N; ++k) {
@@ -262,97 +208,292 @@ __global__ void splat_gather_warp_kernel(const GridArgs a) {
       }
     }
   }
+  pack_cell(a, c, dens);
+}
+
+// The queued cells.  Cells of the CTA queue get one CTA each: threads stride
+// each run and the partial sums are added in a fixed order (warp butterflies,
+// then the warps in order).  Cells of the warp queue get one warp each, lanes
+// striding the runs, a butterfly at the end.  Deterministic, not the
+// sequential order; CTAs and warps stride the queues, whose lengths are read
+// on the device.
+template <int N>
+__device__ __forceinline__ double window_sum(const GatherArgs& ga, const int* first, int c,
+                                             int t, int nt) {
+  constexpr int H = N / 2;
+  double dens = 0.0;
+#pragma unroll
+  for (int k = N - 1; k >= 0; --k) {
+    const int e = c + H - 1 - k;  // the run of cell e feeds slot k
+    const double* wk = ga.g.w + (int64_t)k * ga.g.ns;
+    const int64_t j1 = first[e + 1];
+    for (int64_t j = first[e] + t; j < j1; j += nt) dens += wk[j];
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) dens += __shfl_xor_sync(0xffffffffu, dens, o);
-  if (lane == 0) {
-    const int64_t half = m / 2;
-    const double sd = (c <= half) ? (double)c : (double)c - (double)m;
-    const double x = sd * a.dx;
-    const double denom = x * x + a.eta * a.eta;
-    a.packed[c] = make_double2(dens, x / denom);
+  return dens;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) pack_dense_kernel(const GatherArgs ga) {
+  __shared__ double s_part[8];
+  const int* first = ga.first + N + 1;
+  const int64_t m = ga.g.m;
+  const int n_cta = ga.n_dense[1];
+  for (int i = blockIdx.x; i < n_cta; i += gridDim.x) {
+    const int c = ga.dense[m + i];
+    const double d = window_sum<N>(ga, first, c, threadIdx.x, blockDim.x);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = d;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+      pack_cell(ga.g, c, t);
+    }
+    __syncthreads();
+  }
+  const int n_warp = ga.n_dense[0];
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_warp; i += warps) {
+    const int c = ga.dense[i];
+    const double d = window_sum<N>(ga, first, c, lane, 32);
+    if (lane == 0) pack_cell(ga.g, c, d);
   }
 }
 
 // ---------------------------------------------------------------- FFT --
+// Unnormalised DFT, forward sign e^{-2 pi i jk/m}, inverse e^{+2 pi i jk/m}
+// (the contract of the reference's transform, rustfft).  m = m1*m2 by the
+// four-step method; each row transform of length L (8 <= L <= 2048) runs in
+// shared memory as a mixed-radix Stockham FFT (radix 8, then one radix-4 or
+// radix-2 stage): every thread owns 8 elements per stage, the stage twiddles
+// come from a per-CTA table, and rows are stored with one pad slot per 8
+// elements (and one more per row) so that strided accesses spread over the
+// shared-memory banks.
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+// v * (sign * i)
+__device__ __forceinline__ double2 mul_si(double2 v, double sign) {
+  return make_double2(-sign * v.y, sign * v.x);
+}
+__device__ __forceinline__ int padi(int i) { return i + (i >> 3); }
 
-__device__ __forceinline__ unsigned bitrev(unsigned v, int bits) {
-  return bits == 0 ? 0u : (__brev(v) >> (32 - bits));
+// R-point DFTs in registers, W_R = e^{sign 2 pi i/R}.
+__device__ __forceinline__ void dft2(double2* v) {
+  const double2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+__device__ __forceinline__ void dft4(double2& v0, double2& v1, double2& v2, double2& v3,
+                                     double sign) {
+  const double2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3);
+  const double2 t3 = mul_si(csub(v1, v3), sign);
+  v0 = cadd(t0, t2);
+  v1 = cadd(t1, t3);
+  v2 = csub(t0, t2);
+  v3 = csub(t1, t3);
+}
+__device__ __forceinline__ void dft8(double2* v, double sign) {
+  const double h = 0.70710678118654752440;  // sqrt(1/2)
+  double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4(e0, e1, e2, e3, sign);
+  dft4(o0, o1, o2, o3, sign);
+  o1 = cmul(o1, make_double2(h, sign * h));
+  o2 = mul_si(o2, sign);
+  o3 = cmul(o3, make_double2(-h, sign * h));
+  v[0] = cadd(e0, o0);
+  v[1] = cadd(e1, o1);
+  v[2] = cadd(e2, o2);
+  v[3] = cadd(e3, o3);
+  v[4] = csub(e0, o0);
+  v[5] = csub(e1, o1);
+  v[6] = csub(e2, o2);
+  v[7] = csub(e3, o3);
 }
 
-// Transforms per CTA for length L: G*L <= FFT_MAXL.
-__host__ __device__ __forceinline__ int fft_group(int L) {
-  return L <= 512 ? 4 : (L <= 1024 ? 2 : 1);
-}
-
-// Radix-2 decimation-in-time transform of G rows of length L in shared
-// memory (rows already in bit-reversed order).  tw: table of
-// (cos 2 pi j/m, sin 2 pi j/m), sign -1 forward, +1 inverse.
-__device__ void smem_fft(double2* buf, int G, int L, int64_t m, const double2* tw, double sign) {
-  for (int len = 2; len <= L; len <<= 1) {
-    const int half = len >> 1;
-    const int64_t step = m / len;
-    const int nb = G * (L >> 1);
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int g = b / (L >> 1);
-      const int r = b % (L >> 1);
-      const int grp = r / half, k = r % half;
-      const int i = g * L + grp * len + k;
-      const double2 t = tw[(int64_t)k * step];
-      const double2 w = make_double2(t.x, sign * t.y);
-      const double2 u = buf[i];
-      const double2 v = cmul(buf[i + half], w);
-      buf[i] = make_double2(u.x + v.x, u.y + v.y);
-      buf[i + half] = make_double2(u.x - v.x, u.y - v.y);
+// One radix-R Stockham stage over a row of length L (sub-transform length Ns
+// so far): thread q of the row does the 8/R butterflies j = q + b*L/8.
+template <int R>
+__device__ __forceinline__ void fft_stage(double2* row, const double2* tws, int L, int Ns, int q,
+                                          double sign) {
+  // tws: this stage's twiddles W_{Ns R}^{k r} at [(r - 1) * Ns + k]
+  constexpr int B = 8 / R;
+  const int tpr = L >> 3;
+  double2 v[8];
+#pragma unroll
+  for (int b = 0; b < B; ++b) {
+    const int j = q + b * tpr;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[b * R + r] = row[padi(j + r * (L / R))];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < B; ++b) {
+    const int j = q + b * tpr;
+    const int k = j & (Ns - 1);
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], tws[(r - 1) * Ns + k]);
     }
-    __syncthreads();
+    if (R == 8) dft8(&v[b * R], sign);
+    else if (R == 4) dft4(v[b * R], v[b * R + 1], v[b * R + 2], v[b * R + 3], sign);
+    else dft2(&v[b * R]);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) row[padi(base + r * Ns)] = v[b * R + r];
+  }
+  __syncthreads();
+}
+
+// In-place FFT of a padded row of length L >= 8; every thread of the CTA
+// calls it (the stages hold barriers).
+__device__ void row_fft(double2* row, const double2* tws, int L, int q, double sign) {
+  int Ns = 1, rem = L, off = 0;
+  while (rem >= 8) {
+    fft_stage<8>(row, tws + off, L, Ns, q, sign);
+    if (Ns > 1) off += 7 * Ns;
+    Ns *= 8;
+    rem >>= 3;
+  }
+  if (rem == 4) fft_stage<4>(row, tws + off, L, Ns, q, sign);
+  else if (rem == 2) fft_stage<2>(row, tws + off, L, Ns, q, sign);
+}
+
+// Per-stage twiddles for row_fft: for every stage after the first (Ns > 1,
+// radix R), W_{Ns R}^{k r} = W_m^{k r m/(Ns R)} for r = 1..R-1, k < Ns, laid
+// out [r - 1][k] so that consecutive lanes read consecutive entries; L - 8
+// entries in all.  Taken from the length-m table, sign applied.
+__device__ __forceinline__ void load_stage_twiddles(double2* tws, const double2* __restrict__ tw,
+                                                    int L, int64_t m, double sign) {
+  const int total = L - 8;  // <= 8 * blockDim
+  double2 w[8];
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int idx = threadIdx.x + it * blockDim.x;
+    w[it] = make_double2(1.0, 0.0);
+    if (idx < total) {
+      int off = 0, Ns = 8, rem = L >> 3, R = rem >= 8 ? 8 : rem;
+      while (idx >= off + (R - 1) * Ns) {
+        off += (R - 1) * Ns;
+        Ns *= R;
+        rem /= R;
+        R = rem >= 8 ? 8 : rem;
+      }
+      const int r = (idx - off) / Ns + 1, k = (idx - off) & (Ns - 1);
+      w[it] = tw[(int64_t)k * r * (m / ((int64_t)Ns * R))];
+    }
+  }
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int idx = threadIdx.x + it * blockDim.x;
+    if (idx < total) tws[idx] = make_double2(w[it].x, sign * w[it].y);
   }
 }
 
-// Pass 1: Y[k1*m2 + n2] = W_m^{n2 k1} * sum_n1 x[m2 n1 + n2] W_m1^{n1 k1}.
-__global__ void __launch_bounds__(256) fft_pass1(const double2* __restrict__ x,
-                                                 double2* __restrict__ y, int m1, int b1, int m2,
+// Pass 1: Y[k1*m2 + n2] = W_m^{n2 k1} * sum_n1 x[m2 n1 + n2] W_m1^{n1 k1}, for
+// G columns n2 per CTA (G*m1/8 threads).
+__global__ void __launch_bounds__(256, 4) fft_pass1(const double2* __restrict__ x,
+                                                 double2* __restrict__ y, int m1, int m2,
                                                  int64_t m, const double2* __restrict__ tw,
                                                  double sign) {
-  __shared__ double2 buf[FFT_MAXL];
-  const int G = fft_group(m1);
+  extern __shared__ double2 fsm[];
+  const int L = m1, Lp = L + (L >> 3) + 1, tpr = L >> 3;
+  const int G = blockDim.x / tpr, gl = __ffs(G) - 1;
+  double2* tws = fsm + G * Lp;
+  load_stage_twiddles(tws, tw, L, m, sign);
   const int n2_0 = blockIdx.x * G;
-  for (int e = threadIdx.x; e < G * m1; e += blockDim.x) {
-    const int n1 = e / G, g = e % G;
-    if (n2_0 + g < m2) buf[g * m1 + bitrev((unsigned)n1, b1)] = x[(int64_t)m2 * n1 + n2_0 + g];
+  // G*L = 8*blockDim: every thread moves exactly 8 elements each way
+  double2 v[8];
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = threadIdx.x + it * blockDim.x;
+    const int n1 = e >> gl, g = e & (G - 1);
+    v[it] = n2_0 + g < m2 ? x[(int64_t)m2 * n1 + n2_0 + g] : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = threadIdx.x + it * blockDim.x;
+    fsm[(e & (G - 1)) * Lp + padi(e >> gl)] = v[it];
   }
   __syncthreads();
-  smem_fft(buf, G, m1, m, tw, sign);
-  for (int e = threadIdx.x; e < G * m1; e += blockDim.x) {
-    const int k1 = e / G, g = e % G;
-    const int n2 = n2_0 + g;
-    if (n2 >= m2) continue;
-    const double2 t = tw[((int64_t)n2 * k1) % m];
-    y[(int64_t)k1 * m2 + n2] = cmul(buf[g * m1 + k1], make_double2(t.x, sign * t.y));
+  row_fft(fsm + (threadIdx.x / tpr) * Lp, tws, L, threadIdx.x % tpr, sign);
+  // W_m^a = W_m^{a - a mod 1024} * W_m^{a mod 1024}, both from the table;
+  // two batches of 4 elements keep the loads in flight within 64 registers
+#pragma unroll
+  for (int h = 0; h < 8; h += 4) {
+    double2 wh[4], wl[4];
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int e = threadIdx.x + (h + it) * blockDim.x;
+      const int64_t a = ((int64_t)(n2_0 + (e & (G - 1))) * (e >> gl)) & (m - 1);
+      wh[it] = tw[a & ~(int64_t)1023];
+      wl[it] = tw[a & 1023];
+    }
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int e = threadIdx.x + (h + it) * blockDim.x;
+      const int k1 = e >> gl, g = e & (G - 1);
+      const int n2 = n2_0 + g;
+      const double2 w = cmul(wh[it], wl[it]);
+      if (n2 < m2)
+        y[(int64_t)k1 * m2 + n2] = cmul(fsm[g * Lp + padi(k1)], make_double2(w.x, sign * w.y));
+    }
   }
 }
 
-// Pass 2: X[k1 + m1 k2] = sum_n2 Y[k1*m2 + n2] W_m2^{n2 k2}.
-__global__ void __launch_bounds__(256) fft_pass2(const double2* __restrict__ y,
-                                                 double2* __restrict__ x, int m1, int m2, int b2,
+// Pass 2: X[k1 + m1 k2] = sum_n2 Y[k1*m2 + n2] W_m2^{n2 k2}, G rows per CTA.
+__global__ void __launch_bounds__(256, 4) fft_pass2(const double2* __restrict__ y,
+                                                 double2* __restrict__ x, int m1, int m2,
                                                  int64_t m, const double2* __restrict__ tw,
                                                  double sign) {
-  __shared__ double2 buf[FFT_MAXL];
-  const int G = fft_group(m2);
+  extern __shared__ double2 fsm[];
+  const int L = m2, Lp = L + (L >> 3) + 1, tpr = L >> 3;
+  const int G = blockDim.x / tpr, gl = __ffs(G) - 1, ll = __ffs(L) - 1;
+  double2* tws = fsm + G * Lp;
+  load_stage_twiddles(tws, tw, L, m, sign);
   const int k1_0 = blockIdx.x * G;
-  for (int e = threadIdx.x; e < G * m2; e += blockDim.x) {
-    const int g = e / m2, n2 = e % m2;
-    if (k1_0 + g < m1) buf[g * m2 + bitrev((unsigned)n2, b2)] = y[(int64_t)(k1_0 + g) * m2 + n2];
+  double2 v[8];
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = threadIdx.x + it * blockDim.x;
+    const int g = e >> ll, n2 = e & (L - 1);
+    v[it] = k1_0 + g < m1 ? y[(int64_t)(k1_0 + g) * m2 + n2] : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = threadIdx.x + it * blockDim.x;
+    fsm[(e >> ll) * Lp + padi(e & (L - 1))] = v[it];
   }
   __syncthreads();
-  smem_fft(buf, G, m2, m, tw, sign);
-  for (int e = threadIdx.x; e < G * m2; e += blockDim.x) {
-    const int k2 = e / G, g = e % G;
-    if (k1_0 + g >= m1) continue;
-    x[(int64_t)(k1_0 + g) + (int64_t)m1 * k2] = buf[g * m2 + k2];
+  row_fft(fsm + (threadIdx.x / tpr) * Lp, tws, L, threadIdx.x % tpr, sign);
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = threadIdx.x + it * blockDim.x;
+    const int k2 = e >> gl, g = e & (G - 1);
+    if (k1_0 + g < m1) x[(int64_t)(k1_0 + g) + (int64_t)m1 * k2] = fsm[g * Lp + padi(k2)];
   }
+}
+
+// Transforms shorter than 64 points: direct DFT, one thread per output.
+__global__ void dft_small(const double2* __restrict__ x, double2* __restrict__ y, int m,
+                          const double2* __restrict__ tw, double sign) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int n = 0; n < m; ++n) {
+    const double2 w = tw[((int64_t)n * k) % m];
+    acc = cadd(acc, cmul(x[n], make_double2(w.x, sign * w.y)));
+  }
+  y[k] = acc;
 }
 
 // fftplan.rs:43-76: unpack D (density) and K (odd kernel) from the packed
@@ -481,19 +622,51 @@ int ilog2(int64_t v) {
   return b;
 }
 
+// Rows per CTA for a pass over `rows` transforms of length L: as many as fit
+// 256 threads (8 elements each), but no more than keeps ~2 CTAs per SM.
+int rows_per_cta(int L, int rows) {
+  const int cap = 2048 / L;
+  int g = 1;
+  while (g * 2 <= cap && (int64_t)rows / (g * 2) >= 296) g *= 2;
+  return g;
+}
+
+size_t pass_smem(int L, int G) {
+  return sizeof(double2) * ((size_t)G * (L + (L >> 3) + 1) + L);
+}
+
 shrk_status fft(double2* buf, double2* tmp, int64_t m, const double2* tw, double sign,
                 const char* family, cudaStream_t s) {
-  const int bits = ilog2(m);
-  const int b1 = (bits + 1) / 2, b2 = bits / 2;
-  const int m1 = 1 << b1, m2 = 1 << b2;
-  {
+  if (m < 64) {
     LaunchScope ls(family, s);
-    fft_pass1<<<blocks_for(m2, fft_group(m1)), 256, 0, s>>>(buf, tmp, m1, b1, m2, m, tw, sign);
+    dft_small<<<1, 64, 0, s>>>(buf, tmp, (int)m, tw, sign);
+    SHRK_CUDA(cudaGetLastError());
+    SHRK_CUDA(cudaMemcpyAsync(buf, tmp, sizeof(double2) * m, cudaMemcpyDeviceToDevice, s));
+    return SHRK_OK;
+  }
+  const int bits = ilog2(m);
+  const int m1 = 1 << ((bits + 1) / 2), m2 = 1 << (bits / 2);
+  static bool opted[64] = {false};
+  int dev = 0;
+  SHRK_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && !opted[dev]) {
+    const int big = (int)pass_smem(FFT_MAXL, 1);
+    SHRK_CUDA(cudaFuncSetAttribute(fft_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    SHRK_CUDA(cudaFuncSetAttribute(fft_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    opted[dev] = true;
+  }
+  {
+    const int G = rows_per_cta(m1, m2);
+    LaunchScope ls(family, s);
+    fft_pass1<<<blocks_for(m2, G), G * (m1 >> 3), pass_smem(m1, G), s>>>(buf, tmp, m1, m2, m, tw,
+                                                                        sign);
     SHRK_CUDA(cudaGetLastError());
   }
   {
+    const int G = rows_per_cta(m2, m1);
     LaunchScope ls(family, s);
-    fft_pass2<<<blocks_for(m1, fft_group(m2)), 256, 0, s>>>(tmp, buf, m1, m2, b2, m, tw, sign);
+    fft_pass2<<<blocks_for(m1, G), G * (m2 >> 3), pass_smem(m2, G), s>>>(tmp, buf, m1, m2, m, tw,
+                                                                        sign);
     SHRK_CUDA(cudaGetLastError());
   }
   return SHRK_OK;
@@ -522,22 +695,47 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   double2* A = (double2*)w;
   double2* B = A + m;
   double2* Tmp = B + m;
+  // slot 24: weights [N][ns] | cells [ns] | last [K] | first [K] | queues [2m] |
+  // queue lengths [2] | scan temporaries, K = m + 2N + 2 keys from -N - 1.
+  const int64_t n_keys = m + 2 * N + 2;
+  size_t scan_bytes = 0;
+  SHRK_CUDA(cub::DeviceScan::ExclusiveScan(nullptr, scan_bytes, (const int*)nullptr,
+                                           (int*)nullptr, MaxOp(), 0, (int)n_keys, s));
+  const size_t head = sizeof(double) * N * (size_t)ns +
+                      sizeof(int) * ((size_t)ns + 2 * n_keys + 2 * m + 2);
+  const size_t head_al = (head + 255) & ~(size_t)255;
   void* sw = nullptr;
-  SHRK_TRY(scratch_get(24, (sizeof(int) + N * sizeof(double)) * (size_t)ns + 256, &sw));
+  SHRK_TRY(scratch_get(24, head_al + scan_bytes, &sw));
   double* wts = (double*)sw;
   int* cell = (int*)(wts + (int64_t)N * ns);
+  int* last = cell + ns;
+  int* first = last + n_keys;
+  int* dense = first + n_keys;
+  int* n_dense = dense + 2 * m;
+  void* scan_tmp = (char*)sw + head_al;
   GridArgs ga{d_src, ns, g.dx < 0.0 ? 1 : 0, g.lo, g.dx, eta, m, cell, wts, A};
+  GatherArgs gg{ga, first, dense, n_dense};
+  SHRK_CUDA(cudaMemsetAsync(last, 0, sizeof(int) * n_keys, s));
+  SHRK_CUDA(cudaMemsetAsync(n_dense, 0, 2 * sizeof(int), s));
   {
     LaunchScope ls(g.fam_splat, s);
-    splat_weights_kernel<N><<<blocks_for(ns, 256), 256, 0, s>>>(ga);
+    splat_weights_kernel<N><<<blocks_for(ns, 256), 256, 0, s>>>(ga, last);
     SHRK_CUDA(cudaGetLastError());
   }
   {
     LaunchScope ls(g.fam_splat, s);
-    if (ns > 2 * m)
-      splat_gather_warp_kernel<N><<<blocks_for(m * 32, 256), 256, 0, s>>>(ga);
-    else
-      splat_gather_kernel<N><<<blocks_for(m, GATHER_T), GATHER_T, 0, s>>>(ga);
+    SHRK_CUDA(cub::DeviceScan::ExclusiveScan(scan_tmp, scan_bytes, (const int*)last, first,
+                                             MaxOp(), 0, (int)n_keys, s));
+  }
+  {
+    LaunchScope ls(g.fam_splat, s);
+    pack_sparse_kernel<N><<<blocks_for(m, 256), 256, 0, s>>>(gg);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  {
+    LaunchScope ls(g.fam_splat, s);
+    const unsigned nb = (unsigned)std::min<int64_t>(m, 148 * 16);
+    pack_dense_kernel<N><<<nb, 256, 0, s>>>(gg);
     SHRK_CUDA(cudaGetLastError());
   }
   SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, g.fam_fft, s));

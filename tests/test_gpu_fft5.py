@@ -167,6 +167,17 @@ def test_small_sizes(oracle, p):
         assert close(re, im, o_re, o_im)
 
 
+@pytest.mark.parametrize("m", [2, 8, 32, 64, 128, 512, 2048, 1 << 21, 1 << 22])
+def test_forced_grid_sizes(oracle, m):
+    """Every transform shape: the direct DFT below 64 points, the four-step
+    Stockham passes from 8 x 8 up to 2048 x 2048."""
+    ev = spectra.harness_spectrum(3000)
+    eta = 1.0 / math.sqrt(3000)
+    re, im = gpu_opts(ev, eta, order=4, m=m)
+    o_re, o_im = oracle.fft5_points(ev, ev, eta, order=4, m=m)
+    assert close(re, im, o_re, o_im)
+
+
 def test_forced_grid_errors(rk):
     ev = spectra.log_spectrum(100)
     with pytest.raises(NotImplementedError, match="power of two"):

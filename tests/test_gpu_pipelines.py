@@ -91,6 +91,8 @@ def test_mixed_precision_c1(rk, oracle, c1):
 
 
 def test_out_of_scope_methods_fail_loudly(rk, c1):
-    for method in ["fft5", "adaptive", "fmm", "ewald", "dst", "hodlr"]:
+    """All-points methods without a GPU kernel raise instead of falling back
+    to the CPU (at query points they are the exact per-point sum)."""
+    for method in ["treecode", "fmm", "ewald", "hodlr"]:
         with pytest.raises(NotImplementedError, match="no GPU implementation"):
             rk.stieltjes_transform(c1, method=method)
