@@ -218,6 +218,53 @@ shrk_status shrk_stieltjes_fft5_with_options_dev(const double* d_ev, size_t p, d
                                                  double pad_eta_mult, double pad_range_frac,
                                                  double* d_re, double* d_im, void* stream);
 
+/* --------------------------------------------------- matrix front-end -- */
+/* Matrices are row-major p x p (p <= 46340), eigenvectors are their
+ * columns.  The eigendecomposition is cuSOLVER's syevd on the device (the
+ * reference's symmetric_eigh, pipeline/mod.rs:502-585, is a Jacobi
+ * iteration; eigenvector signs are arbitrary in both).  Output pointers
+ * marked "may be NULL" are skipped when NULL. */
+/* pipeline/mod.rs:502-585 symmetric_eigh: ascending eigenvalues (p) and
+ * the eigenvectors as columns (p x p, may be NULL). */
+shrk_status shrk_symmetric_eigh(const double* matrix, size_t p, double* eigenvalues,
+                                double* eigenvectors);
+/* pipeline/mod.rs:197-242 clean_eigensystem: from a sample eigensystem
+ * (eigenvector columns parallel to `eigenvalues`, any order) and c: the
+ * cleaned covariance (p x p), the eigenvectors with columns sorted by
+ * descending eigenvalue (may be NULL), the RIE eigenvalues (descending),
+ * the squared angular overlaps (overlaps.rs:26-46) and the noise level
+ * sigma2 (MP-median-corrected median, detection.rs:97-104). */
+shrk_status shrk_clean_eigensystem(const double* eigenvectors, const double* eigenvalues,
+                                   size_t p, double c, double* covariance,
+                                   double* sorted_eigenvectors, double* rie_eigenvalues,
+                                   double* overlaps, double* sigma2);
+/* pipeline/mod.rs:244-329 clean_covariance_matrix / clean_correlation_matrix
+ * (one estimator): eigendecompose `matrix`, then clean_eigensystem;
+ * renormalize != 0 rescales the result to unit diagonal
+ * (python.rs:729-731). */
+shrk_status shrk_clean_covariance_matrix(const double* matrix, size_t p, double c,
+                                         int renormalize, double* covariance,
+                                         double* eigenvectors, double* rie_eigenvalues,
+                                         double* overlaps, double* sigma2);
+/* pipeline/mod.rs:331-341 renormalize_to_unit_diagonal: D^-1/2 S D^-1/2, or
+ * S unchanged when a diagonal entry is not positive. */
+shrk_status shrk_renormalize_to_unit_diagonal(const double* matrix, size_t p, double* out);
+/* pipeline/mod.rs:409-464 precision_from_eigensystem: inverse nonlinear
+ * shrinkage (method 0 QIS, 1 LIS, 2 GIS) of the sorted spectrum and
+ * Omega = U diag(precision_ev) U^T; eigenvalues must be strictly positive,
+ * c in (0, 1].  precision_ev / covariance_ev follow the descending sample
+ * eigenvalues. */
+shrk_status shrk_precision_from_eigensystem(const double* eigenvectors, const double* eigenvalues,
+                                            size_t p, double c, int method, double* precision,
+                                            double* sorted_eigenvectors, double* precision_ev,
+                                            double* covariance_ev, double* smoothing);
+/* pipeline/mod.rs:466-478 estimate_precision_matrix: eigendecompose, then
+ * precision_from_eigensystem. */
+shrk_status shrk_estimate_precision_matrix(const double* matrix, size_t p, double c, int method,
+                                           double* precision, double* eigenvectors,
+                                           double* precision_ev, double* covariance_ev,
+                                           double* smoothing);
+
 /* ------------------------------------------------------- consumers -- */
 /* deconvolution/inverse.rs:156-269 inverse_nonlinear_shrinkage (RmtConfig::new:
  * exact sums): method 0 QIS, 1 LIS, 2 GIS.  precision_ev / covariance_ev hold

@@ -92,6 +92,13 @@ def lib():
             "orc_scaled_ray": (None, [_D, _SZ, C.c_double, _D, _D]),
             "orc_evaluate_many": (None, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, C.c_int, _D, _D]),
             "orc_inverse_shrinkage": (None, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
+            "orc_symmetric_eigh": (None, [_D, _SZ, _D, _D]),
+            "orc_angular_overlaps": (None, [_D, _SZ, C.c_double, C.c_double, _D]),
+            "orc_clean_eigensystem": (C.c_int, [_D, _D, _SZ, C.c_double, _D, _D, _D, _D, _D]),
+            "orc_clean_matrix": (C.c_int, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
+            "orc_renormalize": (None, [_D, _SZ, _D]),
+            "orc_precision_from_eigensystem": (None, [_D, _D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
+            "orc_estimate_precision_matrix": (None, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -452,3 +459,80 @@ def inverse_shrinkage(ev, c, method="qis"):
                                 C.byref(h))
     return dict(precision_eigenvalues=out[0], covariance_eigenvalues=out[1], theta=out[2],
                 htheta=out[3], smoothing=h.value)
+
+
+# ---------------------------------------------------------- matrix front --
+def _mat(m):
+    return np.ascontiguousarray(np.asarray(m, dtype=np.float64))
+
+
+def symmetric_eigh(m):
+    """pipeline/mod.rs:502-585 (Jacobi): ascending eigenvalues, eigenvector columns."""
+    m = _mat(m)
+    p = m.shape[0]
+    ev, vec = np.empty(p), np.empty((p, p))
+    lib().orc_symmetric_eigh(_d(m), p, _d(ev), _d(vec))
+    return ev, vec
+
+
+def angular_overlaps(lambda_rie, c, sigma2):
+    l = _arr(lambda_rie)
+    out = np.empty_like(l)
+    lib().orc_angular_overlaps(_d(l), l.size, c, sigma2, _d(out))
+    return out
+
+
+def _clean_out(p):
+    return np.empty((p, p)), np.empty((p, p)), np.empty(p), np.empty(p), C.c_double()
+
+
+def clean_eigensystem(eigenvectors, eigenvalues, c):
+    """pipeline/mod.rs:197-242."""
+    v, e = _mat(eigenvectors), _arr(eigenvalues)
+    p = e.size
+    cov, vec, l, a2, s2 = _clean_out(p)
+    lib().orc_clean_eigensystem(_d(v), _d(e), p, c, _d(cov), _d(vec), _d(l), _d(a2), C.byref(s2))
+    return dict(covariance=cov, eigenvectors=vec, eigenvalues=l, overlaps=a2, sigma2=s2.value)
+
+
+def clean_matrix(m, c, renormalize=False):
+    """pipeline/mod.rs:244-331 (+ python.rs:729-731)."""
+    m = _mat(m)
+    p = m.shape[0]
+    cov, vec, l, a2, s2 = _clean_out(p)
+    lib().orc_clean_matrix(_d(m), p, c, int(renormalize), _d(cov), _d(vec), _d(l), _d(a2),
+                           C.byref(s2))
+    return dict(covariance=cov, eigenvectors=vec, eigenvalues=l, overlaps=a2, sigma2=s2.value)
+
+
+def renormalize_to_unit_diagonal(m):
+    m = _mat(m)
+    out = np.empty_like(m)
+    lib().orc_renormalize(_d(m), m.shape[0], _d(out))
+    return out
+
+
+def _prec_out(p):
+    return np.empty((p, p)), np.empty((p, p)), np.empty(p), np.empty(p), C.c_double()
+
+
+def precision_from_eigensystem(eigenvectors, eigenvalues, c, method="qis"):
+    """pipeline/mod.rs:409-464."""
+    v, e = _mat(eigenvectors), _arr(eigenvalues)
+    p = e.size
+    om, vec, pe, ce, h = _prec_out(p)
+    lib().orc_precision_from_eigensystem(_d(v), _d(e), p, c, INVERSE_METHODS[method], _d(om),
+                                         _d(vec), _d(pe), _d(ce), C.byref(h))
+    return dict(precision=om, eigenvectors=vec, precision_eigenvalues=pe,
+                covariance_eigenvalues=ce, smoothing=h.value)
+
+
+def estimate_precision_matrix(m, c, method="qis"):
+    """pipeline/mod.rs:466-478."""
+    m = _mat(m)
+    p = m.shape[0]
+    om, vec, pe, ce, h = _prec_out(p)
+    lib().orc_estimate_precision_matrix(_d(m), p, c, INVERSE_METHODS[method], _d(om), _d(vec),
+                                        _d(pe), _d(ce), C.byref(h))
+    return dict(precision=om, eigenvectors=vec, precision_eigenvalues=pe,
+                covariance_eigenvalues=ce, smoothing=h.value)

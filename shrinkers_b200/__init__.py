@@ -33,6 +33,9 @@ __all__ = [
     "detect_spikes_bema", "inverse_bbp", "stieltjes_at_points", "stieltjes_transform_batched",
     "stieltjes_adjoint", "parse_method", "method_name", "inverse_nonlinear_shrinkage",
     "stieltjes_scaled_ray", "chebcode_evaluate_many", "stieltjes_fft5_with_options",
+    "clean_correlation_matrix", "clean_covariance_matrix", "estimate_precision_matrix",
+    "clean_eigensystem", "precision_from_eigensystem", "renormalize_to_unit_diagonal",
+    "symmetric_eigh",
 ]
 
 _D = C.POINTER(C.c_double)
@@ -536,3 +539,136 @@ def inverse_bbp(lambda_hat, c, sigma2=1.0):
     except (TypeError, ValueError):
         raise ValueError("expected a float or a 1-D array of floats") from None
     return np.array([L.shrk_inverse_bbp(_checked_lambda_hat(x), c, sigma2) for x in arr])
+
+
+# ------------------------------------------------------- matrix front-end --
+def _owned_symmetric_matrix(matrix, what: str) -> np.ndarray:
+    """python.rs:220-249: a square, finite, symmetric float64 matrix (copied,
+    row-major); symmetry within 1e-12 of the largest magnitude (at least 1)."""
+    if not isinstance(matrix, np.ndarray) or matrix.ndim != 2 or matrix.dtype != np.float64:
+        raise TypeError(f"argument '{what}': expected a 2-D numpy.ndarray of float64")
+    rows, cols = matrix.shape
+    if rows != cols:
+        raise ValueError(f"{what} must be a square matrix")
+    a = np.array(matrix, dtype=np.float64, order="C", copy=True)
+    if not np.all(np.isfinite(a)):
+        raise ValueError(f"{what} must contain only finite values")
+    tol = 1e-12 * max(1.0, float(np.max(np.abs(a)))) if a.size else 0.0
+    if np.any(np.abs(np.triu(a, 1) - np.triu(a.T, 1)) > tol):
+        raise ValueError(f"{what} must be symmetric")
+    if rows == 0:
+        raise ValueError(f"{what} must be non-empty")
+    return a
+
+
+def _clean_dict(p):
+    return (np.empty((p, p)), np.empty((p, p)), np.empty(p), np.empty(p), C.c_double())
+
+
+def _clean_matrix(matrix, what, c, renormalize):
+    a = _owned_symmetric_matrix(matrix, what)
+    c = _require_concentration(c)
+    p = a.shape[0]
+    cov, vec, ev, ov, s2 = _clean_dict(p)
+    _native.check(_lib().shrk_clean_covariance_matrix(_dp(a), p, c, int(bool(renormalize)),
+                                                      _dp(cov), _dp(vec), _dp(ev), _dp(ov),
+                                                      C.byref(s2)), f"clean {what}")
+    return {"covariance": cov, "eigenvectors": vec, "eigenvalues": ev, "overlaps": ov,
+            "sigma2": s2.value}
+
+
+def clean_correlation_matrix(correlation, c, *, renormalize=False):
+    """python.rs:683-741 clean_correlation_matrix (pipeline/mod.rs:308-329):
+    RIE eigenvalue shrinkage + eigenvector angular-overlap correction.
+    Returns {"covariance", "eigenvectors" (columns, descending), "eigenvalues"
+    (RIE, descending), "overlaps", "sigma2"}; renormalize=True rescales the
+    result to unit diagonal."""
+    return _clean_matrix(correlation, "correlation", c, renormalize)
+
+
+def clean_covariance_matrix(covariance, c):
+    """python.rs:647-681 clean_covariance_matrix (pipeline/mod.rs:273-306):
+    the same estimator as clean_correlation_matrix, in covariance units."""
+    return _clean_matrix(covariance, "covariance", c, False)
+
+
+def estimate_precision_matrix(covariance, c, *, method="qis", parallel=False):
+    """python.rs:593-645 estimate_precision_matrix (pipeline/mod.rs:466-478):
+    inverse nonlinear shrinkage of the eigenvalues, Omega = U diag(w) U^T.
+    Returns {"precision", "eigenvectors", "precision_eigenvalues",
+    "covariance_eigenvalues", "smoothing"}."""
+    a = _owned_symmetric_matrix(covariance, "covariance")
+    c = _require_concentration(c)
+    m = _parse_inverse_method(method)
+    _parse_parallel(parallel)
+    p = a.shape[0]
+    om, vec = np.empty((p, p)), np.empty((p, p))
+    pe, ce, h = np.empty(p), np.empty(p), C.c_double()
+    _native.check(_lib().shrk_estimate_precision_matrix(_dp(a), p, c, m, _dp(om), _dp(vec),
+                                                        _dp(pe), _dp(ce), C.byref(h)),
+                  "estimate_precision_matrix")
+    return {"precision": om, "eigenvectors": vec, "precision_eigenvalues": pe,
+            "covariance_eigenvalues": ce, "smoothing": h.value}
+
+
+def _eigensystem(eigenvectors, eigenvalues):
+    v = np.ascontiguousarray(np.asarray(eigenvectors, dtype=np.float64))
+    e = np.ascontiguousarray(np.asarray(eigenvalues, dtype=np.float64).ravel())
+    if v.ndim != 2 or v.shape != (e.size, e.size) or e.size == 0:
+        raise ValueError("eigenvectors must be a non-empty p x p matrix parallel to eigenvalues")
+    if not (np.all(np.isfinite(v)) and np.all(np.isfinite(e))):
+        raise ValueError("eigensystem must contain only finite values")
+    return v, e
+
+
+def clean_eigensystem(eigenvectors, eigenvalues, c):
+    """pipeline/mod.rs:197-242 clean_eigensystem (the reference's Rust entry
+    point for an eigensystem computed elsewhere): same keys as
+    clean_correlation_matrix."""
+    v, e = _eigensystem(eigenvectors, eigenvalues)
+    c = _require_concentration(c)
+    p = e.size
+    cov, vec, ev, ov, s2 = _clean_dict(p)
+    _native.check(_lib().shrk_clean_eigensystem(_dp(v), _dp(e), p, c, _dp(cov), _dp(vec),
+                                                _dp(ev), _dp(ov), C.byref(s2)),
+                  "clean_eigensystem")
+    return {"covariance": cov, "eigenvectors": vec, "eigenvalues": ev, "overlaps": ov,
+            "sigma2": s2.value}
+
+
+def precision_from_eigensystem(eigenvectors, eigenvalues, c, *, method="qis"):
+    """pipeline/mod.rs:409-464 precision_from_eigensystem: same keys as
+    estimate_precision_matrix."""
+    v, e = _eigensystem(eigenvectors, eigenvalues)
+    c = _require_concentration(c)
+    m = _parse_inverse_method(method)
+    p = e.size
+    om, vec = np.empty((p, p)), np.empty((p, p))
+    pe, ce, h = np.empty(p), np.empty(p), C.c_double()
+    _native.check(_lib().shrk_precision_from_eigensystem(_dp(v), _dp(e), p, c, m, _dp(om),
+                                                         _dp(vec), _dp(pe), _dp(ce), C.byref(h)),
+                  "precision_from_eigensystem")
+    return {"precision": om, "eigenvectors": vec, "precision_eigenvalues": pe,
+            "covariance_eigenvalues": ce, "smoothing": h.value}
+
+
+def renormalize_to_unit_diagonal(matrix):
+    """pipeline/mod.rs:331-341: D^-1/2 S D^-1/2 (S unchanged when a diagonal
+    entry is not positive)."""
+    a = np.ascontiguousarray(np.asarray(matrix, dtype=np.float64))
+    if a.ndim != 2 or a.shape[0] != a.shape[1] or a.shape[0] == 0:
+        raise ValueError("matrix must be a non-empty square matrix")
+    out = np.empty_like(a)
+    _native.check(_lib().shrk_renormalize_to_unit_diagonal(_dp(a), a.shape[0], _dp(out)),
+                  "renormalize_to_unit_diagonal")
+    return out
+
+
+def symmetric_eigh(matrix):
+    """pipeline/mod.rs:502-585 symmetric_eigh on the GPU (cuSOLVER syevd):
+    (ascending eigenvalues, eigenvectors as columns)."""
+    a = _owned_symmetric_matrix(matrix, "matrix")
+    p = a.shape[0]
+    ev, vec = np.empty(p), np.empty((p, p))
+    _native.check(_lib().shrk_symmetric_eigh(_dp(a), p, _dp(ev), _dp(vec)), "symmetric_eigh")
+    return ev, vec

@@ -54,6 +54,12 @@ SIGNATURES = {
     "shrk_stieltjes_fft5_with_options": (_ST, [_D, _SZ, C.c_double, C.c_int, _SZ, C.c_double, C.c_double, _D, _D]),
     "shrk_stieltjes_fft5_with_options_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, _SZ, C.c_double, C.c_double, _P, _P, _P]),
     "shrk_inverse_nonlinear_shrinkage": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
+    "shrk_symmetric_eigh": (_ST, [_D, _SZ, _D, _D]),
+    "shrk_clean_eigensystem": (_ST, [_D, _D, _SZ, C.c_double, _D, _D, _D, _D, _D]),
+    "shrk_clean_covariance_matrix": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
+    "shrk_renormalize_to_unit_diagonal": (_ST, [_D, _SZ, _D]),
+    "shrk_precision_from_eigensystem": (_ST, [_D, _D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
+    "shrk_estimate_precision_matrix": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
     "shrk_shrinkage_factor": (C.c_double, [C.c_double] * 4),
     "shrk_inverse_bbp": (C.c_double, [C.c_double] * 3),
     "shrk_bbp_threshold": (C.c_double, [C.c_double] * 2),

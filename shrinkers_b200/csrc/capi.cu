@@ -40,7 +40,7 @@ struct DeviceState {
   bool init = false;
   int sms = 0;
   cudaStream_t stream = nullptr;
-  Scratch slots[32];
+  Scratch slots[40];
   int* err = nullptr;
 };
 
@@ -177,7 +177,8 @@ static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
 // 8 sorted copy of the sources, 9/10 hybrid temporaries, 11 FFT grids,
 // 12/13/14/22/23 batched path (its cached graph reads 12, 13, 14 and 22, so
 // no other path may write them), 15 probe sink, 16..21 treecode,
-// 24 FFT-grid stencil weights.
+// 24 FFT-grid stencil weights, 25..31 (see the kernel files), 32..38 the
+// matrix front-end (matrix.cu).
 
 static bool is_fft5_family(int m) {
   return m == SHRK_M_FFT5 || m == SHRK_M_FFT3 || m == SHRK_M_FFT2;
@@ -422,6 +423,14 @@ struct Guard {
   shrk_status st;
   Guard() : lk(g_mu) { st = current_state(&g_cur); }
 };
+
+shrk_status lib_enter(cudaStream_t* stream) {
+  g_mu.lock();
+  shrk_status st = current_state(&g_cur);
+  *stream = st == SHRK_OK ? g_cur->stream : nullptr;
+  return st;
+}
+void lib_exit() { g_mu.unlock(); }
 
 }  // namespace shrk
 

@@ -134,6 +134,21 @@ shrk_status chebcode_evaluate_many(const double* d_ev, int64_t p, const double* 
                                    int64_t n_eta, const ChebParams& prm, double* d_re,
                                    double* d_im, cudaStream_t s);
 
+// The library lock for code outside the C-ABI file: serialises library
+// calls and selects the calling thread's device state (scratch, stream) for
+// the scope's lifetime.  Not re-entrant: release it before calling a C-ABI
+// entry point.
+shrk_status lib_enter(cudaStream_t* stream);
+void lib_exit();
+struct LibScope {
+  shrk_status st;
+  cudaStream_t stream = nullptr;
+  LibScope() { st = lib_enter(&stream); }
+  ~LibScope() { lib_exit(); }
+  LibScope(const LibScope&) = delete;
+  LibScope& operator=(const LibScope&) = delete;
+};
+
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);
 

@@ -436,3 +436,104 @@ def test_evaluate_many_matches_single_eta(oracle):
             sr, si = sr * p, si * p
             assert np.all(np.abs(re[k] - sr) <= 5e-8 * (1.0 + np.abs(sr)))
             assert np.all(np.abs(im[k] - si) <= 5e-8)
+
+
+# ---------------------------------------------------------- matrix front --
+def _spiked_matrix(p):
+    """pipeline/mod.rs:771-784 symmetric_spiked_matrix."""
+    i = np.arange(p)
+    a = 0.2 / (1.0 + np.abs(i[:, None] - i[None, :]).astype(float))
+    np.fill_diagonal(a, 1.0)
+    return a
+
+
+def test_symmetric_eigh_cases(oracle):
+    """pipeline/mod.rs:602-684: identity, diagonal, and a random symmetric
+    matrix plus a strong rank-1 spike (trace kept to 1e-8, top eigenvalue
+    > 15); the Jacobi eigensystem also matches LAPACK's."""
+    ev, vec = oracle.symmetric_eigh(np.eye(4))
+    np.testing.assert_allclose(ev, 1.0, atol=1e-10)
+    np.testing.assert_allclose(vec.T @ vec, np.eye(4), atol=1e-10)
+    ev, _ = oracle.symmetric_eigh(np.diag([5.0, 4.0, 3.0, 2.0, 1.0]))
+    np.testing.assert_allclose(ev, [1, 2, 3, 4, 5], atol=1e-10)
+    rng = np.random.default_rng(11)
+    p = 20
+    a = rng.uniform(-1, 1, (p, p))
+    a = (a + a.T) / 2
+    v = rng.uniform(-1, 1, p)
+    v /= np.linalg.norm(v)
+    a += 20.0 * np.outer(v, v)
+    ev, vec = oracle.symmetric_eigh(a)
+    assert ev[-1] > 15.0
+    assert abs(ev.sum() - np.trace(a)) < 1e-8
+    np.testing.assert_allclose(ev, np.linalg.eigvalsh(a), atol=1e-12)
+    np.testing.assert_allclose(vec @ np.diag(ev) @ vec.T, a, atol=1e-12)
+
+
+def test_angular_overlaps_known_answers(oracle):
+    """eigenvector_overlaps/mod.rs:27-44."""
+    a2 = oracle.angular_overlaps([5.0, 4.0, 3.0, 2.0], 1e-6, 0.5)
+    np.testing.assert_allclose(a2, 1.0, atol=1e-3)
+    a2 = oracle.angular_overlaps([5.0, 4.0, 3.0, 2.0, 0.5, 0.3], 0.5, 1.0)
+    assert a2[0] > 0 and a2[1] > 0 and a2[4] == 0.0 and a2[5] == 0.0
+
+
+def test_clean_eigensystem_trivial(oracle):
+    """pipeline/mod.rs:625-641: identity eigenvectors give a diagonal result."""
+    r = oracle.clean_eigensystem(np.eye(3), [3.0, 2.0, 1.0], 0.3)
+    s = r["covariance"]
+    assert np.all(np.diag(s) > 0)
+    np.testing.assert_allclose(s - np.diag(np.diag(s)), 0.0, atol=1e-12)
+
+
+def test_precision_identity_basis_and_positive(oracle):
+    """pipeline/mod.rs:686-769."""
+    ev = [2.0, 1.5, 1.0, 0.7, 0.5]
+    r = oracle.precision_from_eigensystem(np.eye(5), ev, 0.2)
+    np.testing.assert_allclose(np.diag(r["precision"]), r["precision_eigenvalues"], rtol=1e-12)
+    off = r["precision"] - np.diag(np.diag(r["precision"]))
+    np.testing.assert_allclose(off, 0.0, atol=1e-12)
+    p = 8
+    cov = np.diag(1.0 + 0.2 * np.arange(p))
+    cov += np.diag(np.full(p - 1, 0.05), 1) + np.diag(np.full(p - 1, 0.05), -1)
+    r = oracle.estimate_precision_matrix(cov, 0.3)
+    om = r["precision"]
+    np.testing.assert_allclose(om, om.T, atol=1e-12)
+    assert np.all(r["precision_eigenvalues"] > 0)
+    np.testing.assert_allclose(np.trace(om), r["precision_eigenvalues"].sum(), rtol=1e-10)
+    v = r["eigenvectors"]
+    np.testing.assert_allclose(om, v @ np.diag(r["precision_eigenvalues"]) @ v.T, atol=1e-10)
+
+
+def test_clean_matrix_paths_and_renormalize(oracle):
+    """pipeline/mod.rs:786-847: covariance and correlation paths agree (one
+    estimator); renormalisation gives a unit diagonal, equals the explicit
+    congruence and stays symmetric; a non-positive diagonal is left alone."""
+    a = _spiked_matrix(9)
+    x = oracle.clean_matrix(a, 0.35)
+    y = oracle.clean_matrix(a, 0.35)
+    np.testing.assert_array_equal(x["covariance"], y["covariance"])
+    s = oracle.clean_matrix(_spiked_matrix(11), 0.4)["covariance"]
+    rn = oracle.renormalize_to_unit_diagonal(s)
+    np.testing.assert_allclose(np.diag(rn), 1.0, atol=1e-12)
+    d = np.sqrt(np.diag(s))
+    np.testing.assert_allclose(rn, s / np.outer(d, d), atol=1e-12)
+    np.testing.assert_allclose(rn, rn.T, atol=1e-14)
+    m = np.array([[0.0, 0.5], [0.5, 4.0]])
+    np.testing.assert_array_equal(oracle.renormalize_to_unit_diagonal(m), m)
+    r2 = oracle.clean_matrix(_spiked_matrix(11), 0.4, renormalize=True)
+    np.testing.assert_array_equal(r2["covariance"], rn)
+
+
+def test_clean_matrix_properties(oracle):
+    """test_python_api.py:168-300 on the restatement: symmetric output,
+    positive diagonal, trace preserved in covariance units."""
+    rng = np.random.default_rng(42)
+    corr = np.corrcoef(rng.standard_normal((400, 60)), rowvar=False)
+    r = oracle.clean_matrix(corr, 60 / 400)
+    np.testing.assert_allclose(r["covariance"], r["covariance"].T, atol=1e-12)
+    assert np.all(np.diag(r["covariance"]) > 0) and r["sigma2"] >= 0
+    rng = np.random.default_rng(3)
+    cov = np.cov(rng.standard_normal((500, 40)), rowvar=False) * 3.0
+    r = oracle.clean_matrix(cov, 40 / 499)
+    assert np.isclose(r["eigenvalues"].sum(), np.trace(cov), rtol=1e-9)
