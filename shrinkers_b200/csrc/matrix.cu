@@ -14,9 +14,11 @@
 // this library's RIE and inverse-shrinkage paths; the per-eigenvalue host
 // arithmetic (noise level, overlaps, bulk level) follows the reference's
 // order.  The reconstructions run on the device: the spiked covariance
-// d I + sum_t s_t v_t v_t^T as an FP64 kernel in the reference's operation
-// order (k is the number of spikes, usually small), the precision matrix
-// U diag(w) U^T as a cuBLAS DGEMM (a plain library GEMM).
+// d I + sum_t s_t v_t v_t^T over the k directions with a positive overlap --
+// an FP64 kernel in the reference's operation order for k <= 16, a cuBLAS
+// DGEMM (a plain library GEMM) above, since the overlap is positive for
+// every cleaned eigenvalue beyond sigma^2 (1 + sqrt(c)) and k can reach a
+// fair share of p -- and the precision matrix U diag(w) U^T as a DGEMM.
 //
 // Layouts: caller matrices are row-major p x p with eigenvectors as columns;
 // the device keeps the eigenvector matrix column-major (column j contiguous),
@@ -50,6 +52,10 @@ constexpr int SLOT_IDX = 35;    // column indices, scales, flags
 constexpr int SLOT_OUT = 36;    // p x p result
 constexpr int SLOT_OUT2 = 37;   // p x p result (renormalised / eigenvectors)
 constexpr int SLOT_TMP = 38;    // p x p staging (input, scaled columns)
+
+// Up to this many active directions the spiked covariance is summed by
+// spiked_reconstruct_kernel in the reference's order; beyond, by a DGEMM.
+constexpr int SMALL_K = 16;
 
 struct Handles {
   cusolverDnHandle_t sol = nullptr;
@@ -142,6 +148,30 @@ __global__ void spiked_reconstruct_kernel(const double* __restrict__ e, int64_t 
   }
 }
 
+// G[t*p + r] = E[cols[t]*p + r] and B[t*p + r] = scales[t] * G[t*p + r]: the
+// k active columns and their scaled copies, operands of the rank-k update.
+__global__ void gather_scaled_kernel(const double* __restrict__ e, int64_t p,
+                                     const int* __restrict__ cols,
+                                     const double* __restrict__ scales, double* __restrict__ g,
+                                     double* __restrict__ b) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = blockIdx.y;
+  if (r >= p) return;
+  const double v = e[(int64_t)cols[t] * p + r];
+  g[t * p + r] = v;
+  b[t * p + r] = scales[t] * v;
+}
+
+// After Sigma = B G^T: copy the upper triangle over the lower one and add d
+// to the diagonal (d + sum_t s_t v_t^2, as the reference's diagonal).
+__global__ void finish_spiked_kernel(double* __restrict__ m, int64_t p, double d) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t r = blockIdx.y;
+  if (c >= p) return;
+  if (c < r) m[r * p + c] = m[c * p + r];
+  else if (c == r) m[r * p + r] = d + m[r * p + r];
+}
+
 // mod.rs:331-341: sc[i] = 1/sqrt(S[i][i]); *bad set when a diagonal entry is
 // not positive (the matrix is then returned unchanged).
 __global__ void diag_scales_kernel(const double* __restrict__ s, int64_t p, double* __restrict__ sc,
@@ -200,13 +230,15 @@ shrk_status syevd(int64_t p, std::vector<double>& w_host, cudaStream_t s) {
   void* work = nullptr;
   SHRK_TRY(scratch_get(SLOT_WORK, sizeof(double) * (size_t)lwork + sizeof(int) + 256, &work));
   info = (char*)work + sizeof(double) * (size_t)lwork;
-  if (cusolverDnDsyevd(H->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)p,
-                       (double*)a, (int)p, (double*)w, (double*)work, lwork, (int*)info) !=
-      CUSOLVER_STATUS_SUCCESS) {
-    set_error("cusolverDnDsyevd failed");
-    return SHRK_ECUDA;
+  {
+    LaunchScope ls("matrix_eigh", s);
+    if (cusolverDnDsyevd(H->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)p,
+                         (double*)a, (int)p, (double*)w, (double*)work, lwork, (int*)info) !=
+        CUSOLVER_STATUS_SUCCESS) {
+      set_error("cusolverDnDsyevd failed");
+      return SHRK_ECUDA;
+    }
   }
-  add_launches(1);
   int h_info = 0;
   w_host.resize(p);
   SHRK_CUDA(cudaMemcpyAsync(w_host.data(), w, sizeof(double) * p, cudaMemcpyDeviceToHost, s));
@@ -337,10 +369,40 @@ shrk_status clean_sorted(const std::vector<int>& cols, const std::vector<double>
                               cudaMemcpyHostToDevice, s));
     SHRK_CUDA(cudaMemcpyAsync(d_cols, act.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
   }
-  spiked_reconstruct_kernel<<<rows_grid(P, 256), 256, 0, s>>>((const double*)e, P, d_cols,
-                                                              d_scales, k, d_bulk, (double*)out);
-  SHRK_CUDA(cudaGetLastError());
-  add_launches(1);
+  if (k <= SMALL_K) {
+    LaunchScope ls("matrix_reconstruct", s);
+    spiked_reconstruct_kernel<<<rows_grid(P, 256), 256, 0, s>>>((const double*)e, P, d_cols,
+                                                                d_scales, k, d_bulk, (double*)out);
+    SHRK_CUDA(cudaGetLastError());
+  } else {
+    // many active directions: the rank-k update as a DGEMM, Sigma = B G^T
+    Handles* H = nullptr;
+    SHRK_TRY(handles(s, &H));
+    void* gb = nullptr;
+    SHRK_TRY(scratch_get(SLOT_TMP, sizeof(double) * 2 * P * k, &gb));
+    double* G = (double*)gb;
+    double* B = G + P * k;
+    {
+      LaunchScope ls("matrix_reconstruct", s);
+      gather_scaled_kernel<<<dim3(nblocks(P, 256), (unsigned)k), 256, 0, s>>>(
+          (const double*)e, P, d_cols, d_scales, G, B);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    {
+      LaunchScope ls("matrix_gemm", s);
+      const double one = 1.0, zero = 0.0;
+      if (cublasDgemm(H->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)p, (int)p, k, &one, B, (int)p, G,
+                      (int)p, &zero, (double*)out, (int)p) != CUBLAS_STATUS_SUCCESS) {
+        set_error("cublasDgemm failed");
+        return SHRK_ECUDA;
+      }
+    }
+    {
+      LaunchScope ls("matrix_reconstruct", s);
+      finish_spiked_kernel<<<rows_grid(P, 256), 256, 0, s>>>((double*)out, P, d_bulk);
+      SHRK_CUDA(cudaGetLastError());
+    }
+  }
   double* result = (double*)out;
   if (renorm) {
     void* out2 = nullptr;
@@ -386,20 +448,28 @@ shrk_status precision_sorted(const std::vector<int>& cols, const std::vector<dou
   SHRK_TRY(scratch_get(SLOT_TMP, sizeof(double) * P * P, &b));
   SHRK_TRY(scratch_get(SLOT_OUT, sizeof(double) * P * P, &out));
   SHRK_CUDA(cudaMemcpyAsync(small, w_col.data(), sizeof(double) * p, cudaMemcpyHostToDevice, s));
-  scale_columns_kernel<<<rows_grid(P, 256), 256, 0, s>>>((const double*)e, P,
-                                                         (const double*)small, (double*)b);
-  SHRK_CUDA(cudaGetLastError());
-  // Omega = B E^T (column-major; symmetric, so also the row-major result)
-  const double one = 1.0, zero = 0.0;
-  if (cublasDgemm(H->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)p, (int)p, (int)p, &one,
-                  (const double*)b, (int)p, (const double*)e, (int)p, &zero, (double*)out,
-                  (int)p) != CUBLAS_STATUS_SUCCESS) {
-    set_error("cublasDgemm failed");
-    return SHRK_ECUDA;
+  {
+    LaunchScope ls("matrix_reconstruct", s);
+    scale_columns_kernel<<<rows_grid(P, 256), 256, 0, s>>>((const double*)e, P,
+                                                           (const double*)small, (double*)b);
+    SHRK_CUDA(cudaGetLastError());
   }
-  symmetrize_kernel<<<rows_grid(P, 256), 256, 0, s>>>((double*)out, P);
-  SHRK_CUDA(cudaGetLastError());
-  add_launches(3);
+  {
+    // Omega = B E^T (column-major; symmetric, so also the row-major result)
+    LaunchScope ls("matrix_gemm", s);
+    const double one = 1.0, zero = 0.0;
+    if (cublasDgemm(H->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)p, (int)p, (int)p, &one,
+                    (const double*)b, (int)p, (const double*)e, (int)p, &zero, (double*)out,
+                    (int)p) != CUBLAS_STATUS_SUCCESS) {
+      set_error("cublasDgemm failed");
+      return SHRK_ECUDA;
+    }
+  }
+  {
+    LaunchScope ls("matrix_reconstruct", s);
+    symmetrize_kernel<<<rows_grid(P, 256), 256, 0, s>>>((double*)out, P);
+    SHRK_CUDA(cudaGetLastError());
+  }
   SHRK_CUDA(cudaMemcpyAsync(prec, out, sizeof(double) * P * P, cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
   if (evecs) SHRK_TRY(download_columns(cols, P, evecs, s));

@@ -78,6 +78,21 @@ def test_same_eigensystem_matches_oracle_tightly(rk, oracle):
         assert g["smoothing"] == r["smoothing"]
 
 
+@pytest.mark.parametrize("p", [100, 300])
+def test_few_spikes_reference_order_kernel(rk, oracle, p):
+    """A bulk in [0.5, 1.5] plus spikes 10, 20, 30 in a random basis: 3-4
+    active directions, summed by the kernel in the reference's order."""
+    ev = np.concatenate([np.sort(0.5 + np.random.default_rng(1).uniform(0, 1, p - 3)),
+                         [10.0, 20.0, 30.0]])
+    q, _ = np.linalg.qr(np.random.default_rng(2).standard_normal((p, p)))
+    q = np.ascontiguousarray(q)
+    got = rk.clean_eigensystem(q, ev, 0.1)
+    ref = oracle.clean_eigensystem(q, ev, 0.1)
+    assert 0 < np.sum(ref["overlaps"] > 0) <= 16
+    assert close(got["covariance"], ref["covariance"], 1e-12)
+    np.testing.assert_allclose(got["overlaps"], ref["overlaps"], rtol=1e-10)
+
+
 def test_large_spiked_matrix(rk, oracle):
     """p = 1500 with three factors: GPU end to end vs the oracle's cleaning of
     LAPACK's eigensystem of the same matrix."""
@@ -92,7 +107,9 @@ def test_large_spiked_matrix(rk, oracle):
     ref = oracle.clean_eigensystem(v, w, c)
     assert close(got["covariance"], ref["covariance"], 1e-9)
     np.testing.assert_allclose(got["eigenvalues"], ref["eigenvalues"], rtol=1e-9)
-    assert np.sum(got["overlaps"] > 0) == np.sum(ref["overlaps"] > 0) >= 3
+    # the trace rescale lifts the whole cleaned bulk above sigma^2 (1 + sqrt(c)):
+    # every direction is active and the rank-k update is the DGEMM path
+    assert np.sum(got["overlaps"] > 0) == np.sum(ref["overlaps"] > 0) > 16
     ev, _ = rk.symmetric_eigh(cov)
     np.testing.assert_allclose(ev, w, rtol=1e-10, atol=1e-12 * w[-1])
 
