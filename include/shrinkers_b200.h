@@ -42,9 +42,12 @@ typedef enum {
 /* Method identifiers: same names and order as StieltjesMethod
  * (src/config.rs:19-89).  Exact family (NAIVE .. BLOCKED_HYBRID) -> GPU exact
  * kernels; CHEBCODE* -> GPU treecode with the same ChebPreset; NUFFT -> GPU
- * coarse-grid NUFFT; AUTO/SPEED_AUTO/ACCURACY_AUTO -> resolved exactly as
- * config::resolve_auto_method.  ADAPTIVE, FFT5/3/2, TREECODE, EWALD, DST and
- * HODLR return SHRK_ENOTIMPL (no CPU fallback). */
+ * coarse-grid NUFFT; FFT5/3/2 -> GPU fft5 grid convolution; ADAPTIVE / DST ->
+ * its real part with the windowed (or exact) imaginary part;
+ * AUTO/SPEED_AUTO/ACCURACY_AUTO -> resolved exactly as
+ * config::resolve_auto_method.  At all points TREECODE, EWALD and HODLR
+ * return SHRK_ENOTIMPL (no CPU fallback); at query points they are the exact
+ * per-point sum, as in the reference (mod.rs:265-287). */
 typedef enum {
   SHRK_M_NAIVE = 0, SHRK_M_AUTOVEC, SHRK_M_BLOCKED, SHRK_M_BLOCKED_AUTOVEC,
   SHRK_M_BLOCKED_TILED, SHRK_M_BLOCKED_WINDOWED, SHRK_M_BLOCKED_HYBRID,
@@ -199,6 +202,17 @@ shrk_status shrk_stieltjes_scaled_ray(const double* ev, size_t p, double scale, 
                                       double* raw_im);
 shrk_status shrk_stieltjes_scaled_ray_dev(const double* d_ev, size_t p, double scale,
                                           double* d_re, double* d_im, void* stream);
+
+/* Dyadic Chebyshev FMM (no reference counterpart: the crate's ChebCode is a
+ * treecode, reproduced by the chebcode methods): S(ev_i)/p at every
+ * eigenvalue, input order, from P2M / M2M / M2L / L2L / L2P on a dyadic tree
+ * with leaves of at most 48 eigenvalues and the leaf plus its neighbours
+ * summed directly in FP64.  order = Chebyshev points per box, 4..16; the
+ * error vs the exact sums falls from ~1e-9 (10) to FP64 round-off (16). */
+shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order, double* out_re,
+                               double* out_im);
+shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int order,
+                                   double* d_re, double* d_im, void* stream);
 
 /* fft5.rs:568-590 compute_all_stieltjes_fft5_with_options: RAW sums (not
  * scaled by 1/p) at every eigenvalue from the fft5 grid convolution with the

@@ -35,7 +35,7 @@ __all__ = [
     "stieltjes_scaled_ray", "chebcode_evaluate_many", "stieltjes_fft5_with_options",
     "clean_correlation_matrix", "clean_covariance_matrix", "estimate_precision_matrix",
     "clean_eigensystem", "precision_from_eigensystem", "renormalize_to_unit_diagonal",
-    "symmetric_eigh",
+    "symmetric_eigh", "stieltjes_fmm",
 ]
 
 _D = C.POINTER(C.c_double)
@@ -413,6 +413,23 @@ def stieltjes_scaled_ray(eigenvalues, scale):
     re, im = np.empty(ev.size), np.empty(ev.size)
     _native.check(_lib().shrk_stieltjes_scaled_ray(_dp(ev), ev.size, s, _dp(re), _dp(im)),
                   "stieltjes_scaled_ray")
+    return {"real": re, "imag": im}
+
+
+def stieltjes_fmm(eigenvalues, eta=INFERRED, order=16):
+    """The dyadic Chebyshev FMM (no reference counterpart; the reference's
+    ChebCode treecode is method="chebcode*"): S(ev_i)/p at every eigenvalue
+    as {"real", "imag"}.  order = Chebyshev points per box in [4, 16]; the
+    error vs the exact sums goes from ~1e-9 (10) to FP64 round-off (16)."""
+    ev = _owned_f64_vec(eigenvalues, "eigenvalues")
+    _require_finite(ev, "eigenvalues")
+    if ev.size == 0:
+        raise ValueError("eigenvalues must be non-empty")
+    e = _inferred_f64(eta, "eta")
+    e = 0.1 / math.sqrt(ev.size) if e is None else _require_positive_finite(e, "eta")
+    re, im = np.empty(ev.size), np.empty(ev.size)
+    _native.check(_lib().shrk_stieltjes_fmm(_dp(ev), ev.size, e, int(order), _dp(re), _dp(im)),
+                  "stieltjes_fmm")
     return {"real": re, "imag": im}
 
 

@@ -40,7 +40,7 @@ struct DeviceState {
   bool init = false;
   int sms = 0;
   cudaStream_t stream = nullptr;
-  Scratch slots[40];
+  Scratch slots[48];
   int* err = nullptr;
 };
 
@@ -178,7 +178,7 @@ static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
 // 12/13/14/22/23 batched path (its cached graph reads 12, 13, 14 and 22, so
 // no other path may write them), 15 probe sink, 16..21 treecode,
 // 24 FFT-grid stencil weights, 25..31 (see the kernel files), 32..38 the
-// matrix front-end (matrix.cu).
+// matrix front-end (matrix.cu), 39..45 the dyadic FMM (fmm.cu).
 
 static bool is_fft5_family(int m) {
   return m == SHRK_M_FFT5 || m == SHRK_M_FFT3 || m == SHRK_M_FFT2;
@@ -881,6 +881,39 @@ shrk_status shrk_ledoit_wolf_shrinkage(const double* ev, size_t p, double c, int
   Guard g;
   SHRK_TRY(g.st);
   return lw_device(ev, p, c, method, precision, parallelism, eta, xi);
+}
+
+static shrk_status check_fmm(size_t p, double eta, int order) {
+  if (p == 0) return einval("eigenvalues must be non-empty");
+  if (p > (size_t)INT32_MAX) return einval("fmm: at most 2^31 - 1 eigenvalues");
+  if (!(std::isfinite(eta) && eta > 0.0)) return einval("eta must be a positive finite number");
+  if (order < 4 || order > 16) return einval("fmm: the expansion order must be in [4, 16]");
+  return SHRK_OK;
+}
+
+shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int order,
+                                   double* d_re, double* d_im, void* stream) {
+  SHRK_TRY(check_fmm(p, eta, order));
+  Guard g;
+  SHRK_TRY(g.st);
+  return fmm_all(d_ev, (int64_t)p, eta, order, d_re, d_im, (cudaStream_t)stream);
+}
+
+shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order, double* out_re,
+                               double* out_im) {
+  SHRK_TRY(check_fmm(p, eta, order));
+  Guard g;
+  SHRK_TRY(g.st);
+  cudaStream_t s = g_cur->stream;
+  void* dev = nullptr;
+  SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
+  void* out = nullptr;
+  SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
+  SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  SHRK_TRY(fmm_all((const double*)dev, (int64_t)p, eta, order, (double*)out, (double*)out + p, s));
+  SHRK_TRY(d2h(out_re, out, sizeof(double) * p, s));
+  SHRK_TRY(d2h(out_im, (double*)out + p, sizeof(double) * p, s));
+  return check_device_error(s);
 }
 
 shrk_status shrk_stieltjes_scaled_ray_dev(const double* d_ev, size_t p, double scale,

@@ -1,0 +1,532 @@
+// Dyadic Chebyshev FMM for the Stieltjes sums S(x_t) = sum_j 1/((x_t - s_j) - i eta)
+// at every source (all points), on sm_100a.
+//
+// No reference counterpart: the crate's ChebCode (src/stieltjes/chebcode.rs)
+// is a treecode -- node expansions evaluated directly at each query (M2P) --
+// and is reproduced bit for bit by chebcode.cu.  This is the dual-tree
+// variant with P2M / M2M / M2L / L2L / L2P on a dyadic tree, where the
+// kernel's translation invariance makes every M2L matrix depend only on the
+// level and the box offset, so the far field is a batch of small dense
+// contractions with shared matrices.  Its accuracy class is set by the
+// expansion order n (measured against the exact sums).
+//
+// Tree: the spectrum's range [a, a + W) is cut into 2^l boxes at level l;
+// the leaf level L is the coarsest at which no box holds more than
+// FMM_OCC sources (at most FMM_LMAX).  Only boxes that hold sources exist:
+// the leaves are the runs of equal leaf keys of the sorted sources, and the
+// boxes of level l are the runs of leaf keys >> (L - l), numbered level after
+// level by one scan over (level, leaf) flags.
+//
+// Expansions (n Chebyshev points of the first kind tau_j on [-1, 1],
+// barycentric weights lambda_j): the multipole of a box is the vector of
+// Lagrange-basis sums W_j = sum_{s in box} l_j((s - c)/(h/2)); a child's
+// vector moves to its parent through the fixed matrices T_side[j][k] =
+// l_j(side/2 + tau_k/2); M2L from source box A to target box B at offset
+// o = key_B - key_A (|o| in {2, 3}: the children of the parent's neighbours
+// that do not touch B) is L_B[i] += sum_j W_A[j] / ((h/2)(2o + tau_i - tau_j) - i eta);
+// L2L applies T_side^T; L2P interpolates L at the target; the leaf and its
+// two neighbours are summed directly in FP64.
+#include "common.cuh"
+#include "internal.h"
+
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+namespace shrk {
+
+namespace {
+
+constexpr int FMM_MAXN = 16;
+constexpr int FMM_LMAX = 22;
+constexpr int FMM_OCC = 48;
+
+// scratch slots 39..45 (see the slot map in capi.cu)
+constexpr int SLOT_KEYS = 39;    // per source: leaf key, run flag / leaf index
+constexpr int SLOT_LEAF = 40;    // leaves: key, first source
+constexpr int SLOT_LVL = 41;     // (level, leaf) flags -> global box ids
+constexpr int SLOT_BOX = 42;     // boxes: key, first leaf, level
+constexpr int SLOT_EXP = 43;     // expansions W, Lre, Lim
+constexpr int SLOT_TAB = 44;     // tables: tau, lambda, T_left, T_right, M2L
+constexpr int SLOT_TMP = 45;     // CUB temporaries, small host-read values
+
+struct FmmGeom {
+  double a, W;       // domain [a, a + W)
+  int L;             // leaf level
+  int n;             // expansion order
+  double eta;
+};
+
+__device__ __forceinline__ int key_at(double s, double a, double W, int l) {
+  const double u = (s - a) / W;
+  long long k = (long long)(u * (double)(1LL << l));
+  const long long top = (1LL << l) - 1;
+  return (int)(k < 0 ? 0 : (k > top ? top : k));
+}
+
+// Bit l of *mask: some FMM_OCC + 1 consecutive sorted sources share a box of
+// level l (the level is too coarse).
+__global__ void level_probe_kernel(const double* __restrict__ s, int64_t ns, double a, double W,
+                                   unsigned* __restrict__ mask) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j + FMM_OCC >= ns) return;
+  const double x0 = s[j], x1 = s[j + FMM_OCC];
+  unsigned bits = 0;
+  for (int l = 2; l <= FMM_LMAX; ++l)
+    if (key_at(x0, a, W, l) == key_at(x1, a, W, l)) bits |= 1u << l;
+  if (bits) atomicOr(mask, bits);
+}
+
+__global__ void leaf_flags_kernel(const double* __restrict__ s, int64_t ns, FmmGeom g,
+                                  int* __restrict__ key, int* __restrict__ flag) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const int k = key_at(s[j], g.a, g.W, g.L);
+  key[j] = k;
+  flag[j] = (j == 0 || key_at(s[j - 1], g.a, g.W, g.L) != k) ? 1 : 0;
+}
+
+// incl = inclusive scan of the run flags: leaf index of source j = incl[j] - 1.
+__global__ void leaf_compact_kernel(const int* __restrict__ key, const int* __restrict__ flag,
+                                    const int* __restrict__ incl, int64_t ns,
+                                    int* __restrict__ leaf_key, int* __restrict__ leaf_start) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  if (flag[j]) {
+    leaf_key[incl[j] - 1] = key[j];
+    leaf_start[incl[j] - 1] = (int)j;
+  }
+  if (j == ns - 1) leaf_start[incl[j]] = (int)ns;
+}
+
+// Flags over (level l in [2, L], leaf k): leaf k starts a box of level l.
+__global__ void level_flags_kernel(const int* __restrict__ leaf_key, int nl, int L,
+                                   int* __restrict__ flag) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)(L - 1) * nl;
+  if (t >= total) return;
+  const int l = 2 + (int)(t / nl), k = (int)(t % nl), sh = L - l;
+  flag[t] = (k == 0 || (leaf_key[k] >> sh) != (leaf_key[k - 1] >> sh)) ? 1 : 0;
+}
+
+// Box table from the inclusive scan `id` of the level flags (box id of leaf
+// k's ancestor at level l = id[(l-2) nl + k] - 1).
+__global__ void box_info_kernel(const int* __restrict__ leaf_key, int nl, int L,
+                                const int* __restrict__ flag, const int* __restrict__ id,
+                                int* __restrict__ box_key, int* __restrict__ box_leaf,
+                                unsigned char* __restrict__ box_level) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)(L - 1) * nl;
+  if (t >= total || !flag[t]) return;
+  const int l = 2 + (int)(t / nl), k = (int)(t % nl);
+  const int b = id[t] - 1;
+  box_key[b] = leaf_key[k] >> (L - l);
+  box_leaf[b] = k;
+  box_level[b] = (unsigned char)l;
+}
+
+__global__ void level_ends_kernel(const int* __restrict__ id, int nl, int L, int* __restrict__ off) {
+  // off[l - 2] = first box id of level l; off[L - 1] = total
+  const int t = threadIdx.x;
+  if (t == 0) off[0] = 0;
+  if (t < L - 1) off[t + 1] = id[(int64_t)t * nl + nl - 1];
+}
+
+struct Tabs {
+  const double* tau;
+  const double* lam;
+  const double* TL;   // [j][k] = l_j(-1/2 + tau_k/2)
+  const double* TR;   // [j][k] = l_j(+1/2 + tau_k/2)
+  const double* Mre;  // [l][oi][i][j], oi: o = -3, -2, 2, 3
+  const double* Mim;
+};
+
+// Lane j < n holds tau_j / lambda_j; returns l_j(x) for this lane (0 beyond n).
+__device__ __forceinline__ double lagrange_lane(double x, double tj, double lj, int n, int lane) {
+  const double d = x - tj;
+  const unsigned hit = __ballot_sync(0xffffffffu, lane < n && d == 0.0);
+  if (hit) return lane == __ffs(hit) - 1 ? 1.0 : 0.0;
+  const double q = lane < n ? lj / d : 0.0;
+  double sum = q;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  return q / sum;
+}
+
+// P2M: one warp per leaf, lane j accumulates W_j.
+__global__ void p2m_kernel(const double* __restrict__ s, const int* __restrict__ leaf_key,
+                           const int* __restrict__ leaf_start, int nl, FmmGeom g, Tabs tb,
+                           int64_t leaf_box0, double* __restrict__ Wm) {
+  const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (k >= nl) return;
+  const int n = g.n;
+  const double tj = lane < n ? tb.tau[lane] : 0.0, lj = lane < n ? tb.lam[lane] : 0.0;
+  const double h = g.W / (double)(1LL << g.L);
+  const double c = g.a + ((double)leaf_key[k] + 0.5) * h, hh = 0.5 * h;
+  double w = 0.0;
+  for (int j = leaf_start[k]; j < leaf_start[k + 1]; ++j) w += lagrange_lane((s[j] - c) / hh, tj, lj, n, lane);
+  if (lane < n) Wm[(leaf_box0 + k) * FMM_MAXN + lane] = w;
+}
+
+// M2M for level l: one warp per box, lane i = parent node i.
+__global__ void m2m_kernel(int64_t b0, int64_t b1, int64_t c0, int64_t c1,
+                           const int* __restrict__ box_key, const int* __restrict__ box_leaf,
+                           const int* __restrict__ id, int nl, int l, int n, Tabs tb,
+                           double* __restrict__ Wm) {
+  const int64_t b = b0 + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (b >= b1) return;
+  const int64_t first = id[(int64_t)(l + 1 - 2) * nl + box_leaf[b]] - 1;
+  double acc = 0.0;
+  for (int64_t ch = first; ch < c1 && ch < first + 2; ++ch) {
+    if ((box_key[ch] >> 1) != box_key[b]) break;
+    const double* T = (box_key[ch] & 1) ? tb.TR : tb.TL;
+    const double wc = lane < n ? Wm[ch * FMM_MAXN + lane] : 0.0;
+    for (int kk = 0; kk < n; ++kk) {
+      const double v = __shfl_sync(0xffffffffu, wc, kk);
+      if (lane < n) acc = fma(T[lane * n + kk], v, acc);
+    }
+  }
+  (void)c0;
+  if (lane < n) Wm[b * FMM_MAXN + lane] = acc;
+}
+
+__device__ __forceinline__ int64_t find_key(const int* __restrict__ keys, int64_t lo, int64_t hi,
+                                            int key) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (keys[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// M2L for every box of level >= 2: one warp per target box.
+__global__ void m2l_kernel(int64_t nbox, const int* __restrict__ box_key,
+                           const unsigned char* __restrict__ box_level,
+                           const int* __restrict__ off, int n, Tabs tb,
+                           const double* __restrict__ Wm, double* __restrict__ Lre,
+                           double* __restrict__ Lim) {
+  const int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (b >= nbox) return;
+  const int l = box_level[b], kb = box_key[b];
+  const int64_t lo = off[l - 2], hi = off[l - 1];
+  const int odd = kb & 1;
+  double re = 0.0, im = 0.0;
+  for (int q = 0; q < 3; ++q) {
+    // even kb: sources at kb-2, kb+2, kb+3 (o = 2, -2, -3); odd: kb-3, kb-2, kb+2
+    const int o = odd ? (q == 0 ? 3 : (q == 1 ? 2 : -2)) : (q == 0 ? 2 : (q == 1 ? -2 : -3));
+    const int ka = kb - o;
+    if (ka < 0) continue;
+    const int64_t a = find_key(box_key, lo, hi, ka);
+    if (a >= hi || box_key[a] != ka) continue;
+    const int oi = o == -3 ? 0 : (o == -2 ? 1 : (o == 2 ? 2 : 3));
+    const double* mr = tb.Mre + (((int64_t)l * 4 + oi) * n + lane) * n;
+    const double* mi = tb.Mim + (((int64_t)l * 4 + oi) * n + lane) * n;
+    const double wa = lane < n ? Wm[a * FMM_MAXN + lane] : 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double v = __shfl_sync(0xffffffffu, wa, j);
+      if (lane < n) {
+        re = fma(mr[j], v, re);
+        im = fma(mi[j], v, im);
+      }
+    }
+  }
+  if (lane < n) {
+    Lre[b * FMM_MAXN + lane] = re;
+    Lim[b * FMM_MAXN + lane] = im;
+  }
+}
+
+// L2L from level l to l+1: one warp per child box.
+__global__ void l2l_kernel(int64_t c0, int64_t c1, const int* __restrict__ box_key,
+                           const int* __restrict__ box_leaf, const int* __restrict__ id, int nl,
+                           int l, int n, Tabs tb, double* __restrict__ Lre,
+                           double* __restrict__ Lim) {
+  const int64_t c = c0 + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= c1) return;
+  const int64_t par = id[(int64_t)(l - 2) * nl + box_leaf[c]] - 1;
+  const double* T = (box_key[c] & 1) ? tb.TR : tb.TL;
+  const double pr = lane < n ? Lre[par * FMM_MAXN + lane] : 0.0;
+  const double pi = lane < n ? Lim[par * FMM_MAXN + lane] : 0.0;
+  double re = 0.0, im = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double vr = __shfl_sync(0xffffffffu, pr, i), vi = __shfl_sync(0xffffffffu, pi, i);
+    if (lane < n) {
+      const double t = T[i * n + lane];
+      re = fma(t, vr, re);
+      im = fma(t, vi, im);
+    }
+  }
+  if (lane < n) {
+    Lre[c * FMM_MAXN + lane] += re;
+    Lim[c * FMM_MAXN + lane] += im;
+  }
+}
+
+// L2P + near field: one thread per (sorted) target.
+__global__ void l2p_near_kernel(const double* __restrict__ s, int64_t ns,
+                                const int* __restrict__ leaf_of, const int* __restrict__ leaf_key,
+                                const int* __restrict__ leaf_start, int nl, FmmGeom g, Tabs tb,
+                                int64_t leaf_box0, const double* __restrict__ Lre,
+                                const double* __restrict__ Lim, const int* __restrict__ perm,
+                                double scale, double* __restrict__ out_re,
+                                double* __restrict__ out_im) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const int n = g.n;
+  const double x = s[t];
+  const int k = leaf_of[t] - 1, key = leaf_key[k];  // leaf_of: inclusive run count
+  const double h = g.W / (double)(1LL << g.L);
+  const double c = g.a + ((double)key + 0.5) * h;
+  const double xp = (x - c) / (0.5 * h);
+  // barycentric interpolation of the local expansion
+  double num_r = 0.0, num_i = 0.0, den = 0.0;
+  int hit = -1;
+  const double* lr = Lre + (leaf_box0 + k) * FMM_MAXN;
+  const double* li = Lim + (leaf_box0 + k) * FMM_MAXN;
+  for (int i = 0; i < n; ++i) {
+    const double d = xp - tb.tau[i];
+    if (d == 0.0) {
+      hit = i;
+      break;
+    }
+    const double q = tb.lam[i] / d;
+    num_r = fma(q, lr[i], num_r);
+    num_i = fma(q, li[i], num_i);
+    den += q;
+  }
+  double re, im;
+  if (hit >= 0) {
+    re = lr[hit];
+    im = li[hit];
+  } else {
+    re = num_r / den;
+    im = num_i / den;
+  }
+  // near field: this leaf and the adjacent ones
+  const int ka = (k > 0 && leaf_key[k - 1] == key - 1) ? k - 1 : k;
+  const int kz = (k + 1 < nl && leaf_key[k + 1] == key + 1) ? k + 1 : k;
+  const double eta = g.eta, eta2 = eta * eta;
+  double nr = 0.0, ni = 0.0;
+  for (int j = leaf_start[ka]; j < leaf_start[kz + 1]; ++j) {
+    const double d = x - s[j];
+    const double inv = 1.0 / fma(d, d, eta2);
+    nr = fma(d, inv, nr);
+    ni += inv;
+  }
+  re += nr;
+  im += eta * ni;
+  const int64_t o = perm ? perm[t] : t;
+  out_re[o] = re * scale;
+  out_im[o] = im * scale;
+}
+
+unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// Host tables: first-kind Chebyshev points, barycentric weights, M2M and
+// M2L matrices (double precision, computed here once per call).
+void host_tables(int n, int L, double W, double eta, std::vector<double>& tab) {
+  std::vector<double> tau(n), lam(n);
+  for (int j = 0; j < n; ++j) {
+    const double th = M_PI * (2.0 * j + 1.0) / (2.0 * n);
+    tau[j] = std::cos(th);
+    lam[j] = ((j & 1) ? -1.0 : 1.0) * std::sin(th);
+  }
+  auto lag = [&](double x, int j) {
+    for (int k = 0; k < n; ++k)
+      if (x == tau[k]) return k == j ? 1.0 : 0.0;
+    double den = 0.0;
+    for (int k = 0; k < n; ++k) den += lam[k] / (x - tau[k]);
+    return (lam[j] / (x - tau[j])) / den;
+  };
+  const size_t nn = (size_t)n * n, nm = (size_t)(FMM_LMAX + 1) * 4 * nn;
+  tab.assign(2 * n + 2 * nn + 2 * nm, 0.0);
+  double* T = tab.data();
+  std::copy(tau.begin(), tau.end(), T);
+  std::copy(lam.begin(), lam.end(), T + n);
+  double* TL = T + 2 * n;
+  double* TR = TL + nn;
+  for (int j = 0; j < n; ++j)
+    for (int k = 0; k < n; ++k) {
+      TL[j * n + k] = lag(-0.5 + 0.5 * tau[k], j);
+      TR[j * n + k] = lag(0.5 + 0.5 * tau[k], j);
+    }
+  double* Mre = TR + nn;
+  double* Mim = Mre + nm;
+  const int offs[4] = {-3, -2, 2, 3};
+  for (int l = 2; l <= L; ++l) {
+    const double hh = 0.5 * W / (double)(1LL << l);
+    for (int oi = 0; oi < 4; ++oi)
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) {
+          const double d = hh * (2.0 * offs[oi] + tau[i] - tau[j]);
+          const double den = d * d + eta * eta;
+          const size_t q = (((size_t)l * 4 + oi) * n + i) * n + j;
+          Mre[q] = d / den;  // 1/(d - i eta) = (d + i eta)/(d^2 + eta^2)
+          Mim[q] = eta / den;
+        }
+  }
+}
+
+}  // namespace
+
+shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, double* d_re, double* d_im,
+                    cudaStream_t s) {
+  if (p <= 0) return SHRK_OK;
+  const double* ds = nullptr;
+  const int* perm = nullptr;
+  SHRK_TRY(sorted_sources_perm(d_ev, p, &ds, &perm, s));
+  double ends[2];
+  SHRK_CUDA(cudaMemcpyAsync(&ends[0], ds, sizeof(double), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaMemcpyAsync(&ends[1], ds + p - 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+  void* tmp = nullptr;
+  SHRK_TRY(scratch_get(SLOT_TMP, 4096, &tmp));
+  unsigned* d_mask = (unsigned*)tmp;
+  SHRK_CUDA(cudaMemsetAsync(d_mask, 0, sizeof(unsigned), s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  FmmGeom g;
+  g.a = ends[0];
+  g.W = (ends[1] - ends[0]) * (1.0 + 0x1p-20);
+  if (!(g.W > 0.0) || !std::isfinite(g.W)) g.W = 1.0;
+  g.n = n;
+  g.eta = eta;
+  // leaf level: the coarsest with at most FMM_OCC sources per box
+  {
+    LaunchScope ls("fmm_build", s);
+    level_probe_kernel<<<blocks(p, 256), 256, 0, s>>>(ds, p, g.a, g.W, d_mask);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  unsigned mask = 0;
+  SHRK_CUDA(cudaMemcpyAsync(&mask, d_mask, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  g.L = FMM_LMAX;
+  for (int l = 2; l <= FMM_LMAX; ++l)
+    if (!((mask >> l) & 1u)) {
+      g.L = l;
+      break;
+    }
+  const int L = g.L;
+  // leaves
+  void* kw = nullptr;
+  SHRK_TRY(scratch_get(SLOT_KEYS, sizeof(int) * 3 * (size_t)p + 256, &kw));
+  int* key = (int*)kw;
+  int* flag = key + p;
+  int* incl = flag + p;  // becomes the leaf index per source
+  size_t cub_bytes = 0;
+  SHRK_CUDA(cub::DeviceScan::InclusiveSum(nullptr, cub_bytes, flag, incl, (int)p, s));
+  void* lw = nullptr;
+  SHRK_TRY(scratch_get(SLOT_LEAF, sizeof(int) * (2 * (size_t)p + 2), &lw));
+  int* leaf_key = (int*)lw;
+  int* leaf_start = leaf_key + p;
+  void* cubt = nullptr;
+  {
+    LaunchScope ls("fmm_build", s);
+    leaf_flags_kernel<<<blocks(p, 256), 256, 0, s>>>(ds, p, g, key, flag);
+    SHRK_CUDA(cudaGetLastError());
+    SHRK_TRY(scratch_get(SLOT_TMP, 4096 + cub_bytes, &tmp));
+    cubt = (char*)tmp + 4096;
+    SHRK_CUDA(cub::DeviceScan::InclusiveSum(cubt, cub_bytes, flag, incl, (int)p, s));
+    leaf_compact_kernel<<<blocks(p, 256), 256, 0, s>>>(key, flag, incl, p, leaf_key, leaf_start);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  int nl = 0;
+  SHRK_CUDA(cudaMemcpyAsync(&nl, incl + p - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  // boxes of levels 2..L
+  const int64_t nlev = (int64_t)(L - 1) * nl;
+  void* vw = nullptr;
+  SHRK_TRY(scratch_get(SLOT_LVL, sizeof(int) * (2 * (size_t)nlev + 64), &vw));
+  int* lflag = (int*)vw;
+  int* lid = lflag + nlev;
+  int* d_off = lid + nlev;  // L entries
+  size_t cub2 = 0;
+  SHRK_CUDA(cub::DeviceScan::InclusiveSum(nullptr, cub2, lflag, lid, (int)nlev, s));
+  SHRK_TRY(scratch_get(SLOT_TMP, 4096 + std::max(cub_bytes, cub2), &tmp));
+  cubt = (char*)tmp + 4096;
+  {
+    LaunchScope ls("fmm_build", s);
+    level_flags_kernel<<<blocks(nlev, 256), 256, 0, s>>>(leaf_key, nl, L, lflag);
+    SHRK_CUDA(cudaGetLastError());
+    SHRK_CUDA(cub::DeviceScan::InclusiveSum(cubt, cub2, lflag, lid, (int)nlev, s));
+    level_ends_kernel<<<1, 32, 0, s>>>(lid, nl, L, d_off);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  std::vector<int> off(L);
+  SHRK_CUDA(cudaMemcpyAsync(off.data(), d_off, sizeof(int) * L, cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  const int64_t nbox = off[L - 1];
+  // off[l - 2] = first box of level l, off[l - 1] = one past it
+  void* bw = nullptr;
+  SHRK_TRY(scratch_get(SLOT_BOX, (sizeof(int) * 2 + 1) * (size_t)nbox + 64, &bw));
+  int* box_key = (int*)bw;
+  int* box_leaf = box_key + nbox;
+  unsigned char* box_level = (unsigned char*)(box_leaf + nbox);
+  void* ew = nullptr;
+  SHRK_TRY(scratch_get(SLOT_EXP, sizeof(double) * 3 * FMM_MAXN * (size_t)nbox, &ew));
+  double* Wm = (double*)ew;
+  double* Lre = Wm + FMM_MAXN * nbox;
+  double* Lim = Lre + FMM_MAXN * nbox;
+  std::vector<double> htab;
+  host_tables(n, L, g.W, eta, htab);
+  void* tw = nullptr;
+  SHRK_TRY(scratch_get(SLOT_TAB, sizeof(double) * htab.size(), &tw));
+  SHRK_CUDA(cudaMemcpyAsync(tw, htab.data(), sizeof(double) * htab.size(), cudaMemcpyHostToDevice,
+                            s));
+  const size_t nn = (size_t)n * n, nm = (size_t)(FMM_LMAX + 1) * 4 * nn;
+  Tabs tb;
+  tb.tau = (const double*)tw;
+  tb.lam = tb.tau + n;
+  tb.TL = tb.lam + n;
+  tb.TR = tb.TL + nn;
+  tb.Mre = tb.TR + nn;
+  tb.Mim = tb.Mre + nm;
+  {
+    LaunchScope ls("fmm_build", s);
+    box_info_kernel<<<blocks(nlev, 256), 256, 0, s>>>(leaf_key, nl, L, lflag, lid, box_key,
+                                                     box_leaf, box_level);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  const int64_t leaf_box0 = off[L - 2];
+  {
+    LaunchScope ls("fmm_p2m", s);
+    p2m_kernel<<<blocks((int64_t)nl * 32, 256), 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb,
+                                                             leaf_box0, Wm);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  for (int l = L - 1; l >= 2; --l) {
+    const int64_t b0 = off[l - 2], b1 = off[l - 1], c0 = off[l - 1], c1 = off[l];
+    LaunchScope ls("fmm_m2m", s);
+    m2m_kernel<<<blocks((b1 - b0) * 32, 256), 256, 0, s>>>(b0, b1, c0, c1, box_key, box_leaf, lid,
+                                                          nl, l, n, tb, Wm);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  {
+    LaunchScope ls("fmm_m2l", s);
+    m2l_kernel<<<blocks(nbox * 32, 256), 256, 0, s>>>(nbox, box_key, box_level, d_off, n, tb, Wm,
+                                                      Lre, Lim);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  for (int l = 2; l < L; ++l) {
+    const int64_t c0 = off[l - 1], c1 = off[l];
+    LaunchScope ls("fmm_l2l", s);
+    l2l_kernel<<<blocks((c1 - c0) * 32, 256), 256, 0, s>>>(c0, c1, box_key, box_leaf, lid, nl, l,
+                                                          n, tb, Lre, Lim);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  {
+    LaunchScope ls("fmm_l2p_near", s);
+    l2p_near_kernel<<<blocks(p, 128), 128, 0, s>>>(ds, p, incl, leaf_key, leaf_start, nl, g, tb,
+                                                   leaf_box0, Lre, Lim, perm, 1.0 / (double)p,
+                                                   d_re, d_im);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  return SHRK_OK;
+}
+
+}  // namespace shrk

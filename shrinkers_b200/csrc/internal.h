@@ -149,6 +149,11 @@ struct LibScope {
   LibScope& operator=(const LibScope&) = delete;
 };
 
+// Dyadic Chebyshev FMM (fmm.cu): S(ev_t)/p at every eigenvalue, in the
+// caller's order, expansion order n in [4, 16].
+shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, double* d_re, double* d_im,
+                    cudaStream_t s);
+
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);
 
