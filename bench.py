@@ -50,13 +50,14 @@ def parse():
                     help="spectrum size (default: the workload's own size)")
     ap.add_argument("--workload", default="exact",
                     choices=["exact", "adjoint", "batched", "chebcode_fast", "chebcode",
-                             "chebcode_xtreme", "nufft", "fft5", "clean"],
+                             "chebcode_xtreme", "nufft", "fft5", "clean", "fmm"],
                     help="exact (default, the headline): all-points exact transform at p=1M; "
                          "adjoint: the adjoint kernel at p=20000; batched: 4096 uneven "
                          "spectra; chebcode*/nufft/fft5: the method at p=1M on the spiked "
                          "spectrum; clean: clean_covariance_matrix of a p=2048 3-factor "
                          "sample covariance")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
+    ap.add_argument("--fmm-order", type=int, default=16, help="fmm workload: expansion order")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target duration of one CPU baseline sample")
@@ -438,14 +439,23 @@ def run_path(args, world, rank, local):
         ev = torch.from_numpy(ev_h).to(dev)
         xr = torch.empty(p, dtype=torch.float64, device=dev)
         xi = torch.empty_like(xr)
-        mid = METHOD_IDS[wl]
+        mid = METHOD_IDS.get(wl, -1)
         units = float(p) * p
         family = {"nufft": b"nufft_splat", "fft5": b"fft5_fft",
                   "chebcode_fast": b"cheb_eval_f32"}.get(wl, b"cheb_eval_f64")
         desc = (f"{wl} all-points transform (tree build / grid included), MP(c=0.1)+20 spikes "
                 f"in [3,50] p={p}, eta=1/sqrt(p)")
 
+        if wl == "fmm":
+            family = b"fmm_l2p_near"
+            desc = (f"fmm (order {args.fmm_order}) all-points transform (tree build included), "
+                    f"MP(c=0.1)+20 spikes in [3,50] p={p}, eta=1/sqrt(p)")
+
         def step():
+            if wl == "fmm":
+                _native.check(L.shrk_stieltjes_fmm_dev(ev.data_ptr(), p, eta, args.fmm_order,
+                                                       xr.data_ptr(), xi.data_ptr(), sp))
+                return
             _native.check(L.shrk_stieltjes_all_dev(ev.data_ptr(), p, eta, mid, 0, float("nan"),
                                                    0, xr.data_ptr(), xi.data_ptr(), sp))
         evp = torch.from_numpy(ev_h).pin_memory()
@@ -453,6 +463,10 @@ def run_path(args, world, rank, local):
         ip = torch.empty(p, dtype=torch.float64).pin_memory()
 
         def e2e():
+            if wl == "fmm":
+                _native.check(L.shrk_stieltjes_fmm(dptr(evp), p, eta, args.fmm_order, dptr(rp),
+                                                   dptr(ip)))
+                return
             _native.check(L.shrk_stieltjes_all(dptr(evp), p, eta, mid, 0, float("nan"), 0,
                                                dptr(rp), dptr(ip)))
         io = (8 * p, 16 * p)
@@ -463,6 +477,8 @@ def run_path(args, world, rank, local):
                 O.nufft_points(ev_h, ev_h, eta, parallel=True)
             elif wl == "fft5":  # the reference's fft5 runs sequentially (fft5.rs:589)
                 O.fft5_points(ev_h, ev_h, eta)
+            elif wl == "fmm":  # no CPU FMM: the reference's accurate treecode preset
+                O.chebcode_points(ev_h, ev_h, eta, 0.25, 11, 16, False, parallel=True)
             else:
                 th, nn_, leaf, f32 = CHEB_PRESETS[wl]
                 O.chebcode_points(ev_h, ev_h, eta, th, nn_, leaf, f32, parallel=True)
@@ -497,6 +513,11 @@ def run_path(args, world, rank, local):
     kn, kms = C.c_int64(), C.c_double()
     L.shrk_timing_read(family, C.byref(kn), C.byref(kms))
     fams = {}
+    if wl == "fmm":
+        for f in (b"fmm_build", b"fmm_p2m", b"fmm_m2m", b"fmm_m2l", b"fmm_l2l", b"fmm_l2p_near"):
+            n_, ms_ = C.c_int64(), C.c_double()
+            L.shrk_timing_read(f, C.byref(n_), C.byref(ms_))
+            fams[f.decode()] = (n_.value, ms_.value)
     if wl == "fft5":  # the dominant launch family of the pipeline
         for f in FFT5_FAMILIES:
             n_, ms_ = C.c_int64(), C.c_double()
@@ -565,6 +586,10 @@ def run_path(args, world, rank, local):
                     "frac": ach / _measured_hbm(), "traffic": None, "kernel": fam,
                     "kernel_ms": k_s * 1e3, "grid_cells": m, "basis": basis,
                     "families_ms": {k: v[1] / max(1, args.steps) for k, v in fams.items()}}
+        if wl == "fmm" and fams:
+            roof = {"bound": None, "kernel": "fmm (all families)",
+                    "families_ms": {k: v[1] / max(1, args.steps) for k, v in fams.items()},
+                    "basis": "no single dominant kernel bound reported; see families_ms"}
         rate, sample = cpu()
         cpu_line = {"value": rate, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
                     "sample": sample}

@@ -31,6 +31,7 @@
 
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -143,129 +144,194 @@ struct Tabs {
   const double* Mim;
 };
 
-// Lane j < n holds tau_j / lambda_j; returns l_j(x) for this lane (0 beyond n).
-__device__ __forceinline__ double lagrange_lane(double x, double tj, double lj, int n, int lane) {
-  const double d = x - tj;
-  const unsigned hit = __ballot_sync(0xffffffffu, lane < n && d == 0.0);
-  if (hit) return lane == __ffs(hit) - 1 ? 1.0 : 0.0;
-  const double q = lane < n ? lj / d : 0.0;
-  double sum = q;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-  return q / sum;
-}
-
-// P2M: one warp per leaf, lane j accumulates W_j.
+// P2M: one warp per leaf; lanes take the leaf's sources in turn, each
+// accumulating the n Lagrange-basis values of its sources, and a fixed
+// butterfly adds the lanes (deterministic).
+template <int N>
 __global__ void p2m_kernel(const double* __restrict__ s, const int* __restrict__ leaf_key,
                            const int* __restrict__ leaf_start, int nl, FmmGeom g, Tabs tb,
                            int64_t leaf_box0, double* __restrict__ Wm) {
   const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (k >= nl) return;
-  const int n = g.n;
-  const double tj = lane < n ? tb.tau[lane] : 0.0, lj = lane < n ? tb.lam[lane] : 0.0;
+  double tau[N], lam[N], acc[N];
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    tau[j] = tb.tau[j];
+    lam[j] = tb.lam[j];
+    acc[j] = 0.0;
+  }
   const double h = g.W / (double)(1LL << g.L);
   const double c = g.a + ((double)leaf_key[k] + 0.5) * h, hh = 0.5 * h;
-  double w = 0.0;
-  for (int j = leaf_start[k]; j < leaf_start[k + 1]; ++j) w += lagrange_lane((s[j] - c) / hh, tj, lj, n, lane);
-  if (lane < n) Wm[(leaf_box0 + k) * FMM_MAXN + lane] = w;
-}
-
-// M2M for level l: one warp per box, lane i = parent node i.
-__global__ void m2m_kernel(int64_t b0, int64_t b1, int64_t c0, int64_t c1,
-                           const int* __restrict__ box_key, const int* __restrict__ box_leaf,
-                           const int* __restrict__ id, int nl, int l, int n, Tabs tb,
-                           double* __restrict__ Wm) {
-  const int64_t b = b0 + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (b >= b1) return;
-  const int64_t first = id[(int64_t)(l + 1 - 2) * nl + box_leaf[b]] - 1;
-  double acc = 0.0;
-  for (int64_t ch = first; ch < c1 && ch < first + 2; ++ch) {
-    if ((box_key[ch] >> 1) != box_key[b]) break;
-    const double* T = (box_key[ch] & 1) ? tb.TR : tb.TL;
-    const double wc = lane < n ? Wm[ch * FMM_MAXN + lane] : 0.0;
-    for (int kk = 0; kk < n; ++kk) {
-      const double v = __shfl_sync(0xffffffffu, wc, kk);
-      if (lane < n) acc = fma(T[lane * n + kk], v, acc);
+  for (int j = leaf_start[k] + lane; j < leaf_start[k + 1]; j += 32) {
+    const double x = (s[j] - c) / hh;
+    double q[N], den = 0.0;
+    int hit = -1;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const double d = x - tau[i];
+      if (d == 0.0) hit = i;
+      q[i] = lam[i] / d;
+      den += q[i];
+    }
+    if (hit >= 0) {
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+        if (i == hit) acc[i] += 1.0;
+    } else {
+      const double r = 1.0 / den;
+#pragma unroll
+      for (int i = 0; i < N; ++i) acc[i] = fma(q[i], r, acc[i]);
     }
   }
-  (void)c0;
-  if (lane < n) Wm[b * FMM_MAXN + lane] = acc;
-}
-
-__device__ __forceinline__ int64_t find_key(const int* __restrict__ keys, int64_t lo, int64_t hi,
-                                            int key) {
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (keys[mid] < key) lo = mid + 1;
-    else hi = mid;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    double v = acc[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == i) Wm[(leaf_box0 + k) * FMM_MAXN + i] = v;
   }
-  return lo;
 }
 
-// M2L for every box of level >= 2: one warp per target box.
-__global__ void m2l_kernel(int64_t nbox, const int* __restrict__ box_key,
-                           const unsigned char* __restrict__ box_level,
-                           const int* __restrict__ off, int n, Tabs tb,
-                           const double* __restrict__ Wm, double* __restrict__ Lre,
-                           double* __restrict__ Lim) {
-  const int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (b >= nbox) return;
-  const int l = box_level[b], kb = box_key[b];
-  const int64_t lo = off[l - 2], hi = off[l - 1];
-  const int odd = kb & 1;
-  double re = 0.0, im = 0.0;
-  for (int q = 0; q < 3; ++q) {
-    // even kb: sources at kb-2, kb+2, kb+3 (o = 2, -2, -3); odd: kb-3, kb-2, kb+2
-    const int o = odd ? (q == 0 ? 3 : (q == 1 ? 2 : -2)) : (q == 0 ? 2 : (q == 1 ? -2 : -3));
-    const int ka = kb - o;
-    if (ka < 0) continue;
-    const int64_t a = find_key(box_key, lo, hi, ka);
-    if (a >= hi || box_key[a] != ka) continue;
-    const int oi = o == -3 ? 0 : (o == -2 ? 1 : (o == 2 ? 2 : 3));
-    const double* mr = tb.Mre + (((int64_t)l * 4 + oi) * n + lane) * n;
-    const double* mi = tb.Mim + (((int64_t)l * 4 + oi) * n + lane) * n;
-    const double wa = lane < n ? Wm[a * FMM_MAXN + lane] : 0.0;
-    for (int j = 0; j < n; ++j) {
-      const double v = __shfl_sync(0xffffffffu, wa, j);
-      if (lane < n) {
-        re = fma(mr[j], v, re);
-        im = fma(mi[j], v, im);
+// The expansion kernels below give each box a half-warp (lane i of the half
+// = node i, n <= 16): warp w of a level takes boxes 2w and 2w + 1, warps
+// striding over the level; the loop exit is uniform across the warp.
+
+// M2M for level l: parent box b gets T_side W_child from each child.
+__global__ void __launch_bounds__(256) m2m_kernel(int64_t b0, int64_t b1, int64_t c1,
+                                                  const int* __restrict__ box_key,
+                                                  const int* __restrict__ box_leaf,
+                                                  const int* __restrict__ id, int nl, int l, int n,
+                                                  Tabs tb, double* __restrict__ Wm) {
+  __shared__ double sT[2 * FMM_MAXN * (FMM_MAXN + 1)];  // [side][j][k], padded rows
+  const int rs = n | 1;
+  for (int t = threadIdx.x; t < 2 * n * n; t += blockDim.x) {
+    const int side = t / (n * n), r = (t / n) % n, col = t % n;
+    sT[(side * n + r) * rs + col] = (side ? tb.TR : tb.TL)[r * n + col];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 15;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+    if (b0 + 2 * w >= b1) break;
+    const int64_t b = b0 + 2 * w + ((threadIdx.x >> 4) & 1);
+    const bool live = b < b1;
+    double acc = 0.0;
+    int64_t first = live ? id[(int64_t)(l + 1 - 2) * nl + box_leaf[b]] - 1 : 0;
+    const int kb = live ? box_key[b] : 0;
+    for (int q = 0; q < 2; ++q) {
+      const int64_t ch = first + q;
+      const bool has = live && ch < c1 && (box_key[ch] >> 1) == kb;
+      const double* T = sT + ((has && (box_key[ch] & 1)) ? n * rs : 0);
+      const double wc = (has && lane < n) ? Wm[ch * FMM_MAXN + lane] : 0.0;
+      for (int kk = 0; kk < n; ++kk) {
+        const double v = __shfl_sync(0xffffffffu, wc, kk, 16);
+        if (has && lane < n) acc = fma(T[lane * rs + kk], v, acc);
       }
     }
-  }
-  if (lane < n) {
-    Lre[b * FMM_MAXN + lane] = re;
-    Lim[b * FMM_MAXN + lane] = im;
+    if (live && lane < n) Wm[b * FMM_MAXN + lane] = acc;
   }
 }
 
-// L2L from level l to l+1: one warp per child box.
-__global__ void l2l_kernel(int64_t c0, int64_t c1, const int* __restrict__ box_key,
-                           const int* __restrict__ box_leaf, const int* __restrict__ id, int nl,
-                           int l, int n, Tabs tb, double* __restrict__ Lre,
-                           double* __restrict__ Lim) {
-  const int64_t c = c0 + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (c >= c1) return;
-  const int64_t par = id[(int64_t)(l - 2) * nl + box_leaf[c]] - 1;
-  const double* T = (box_key[c] & 1) ? tb.TR : tb.TL;
-  const double pr = lane < n ? Lre[par * FMM_MAXN + lane] : 0.0;
-  const double pi = lane < n ? Lim[par * FMM_MAXN + lane] : 0.0;
-  double re = 0.0, im = 0.0;
-  for (int i = 0; i < n; ++i) {
-    const double vr = __shfl_sync(0xffffffffu, pr, i), vi = __shfl_sync(0xffffffffu, pi, i);
-    if (lane < n) {
-      const double t = T[i * n + lane];
-      re = fma(t, vr, re);
-      im = fma(t, vi, im);
+// M2L for the boxes [b0, b1) of level l: the level's four n x n complex
+// matrices are staged in shared memory once per CTA.
+__global__ void __launch_bounds__(256) m2l_kernel(int64_t b0, int64_t b1, int l,
+                                                  const int* __restrict__ box_key, int n, Tabs tb,
+                                                  const double* __restrict__ Wm,
+                                                  double* __restrict__ Lre,
+                                                  double* __restrict__ Lim) {
+  // rows padded to an odd number of doubles: lane i's row starts on its own
+  // bank pair
+  __shared__ double sre[4 * FMM_MAXN * (FMM_MAXN + 1)], sim[4 * FMM_MAXN * (FMM_MAXN + 1)];
+  const int nn4 = 4 * n * n, rs = n | 1;
+  const double* mr = tb.Mre + (int64_t)l * nn4;
+  const double* mi = tb.Mim + (int64_t)l * nn4;
+  for (int t = threadIdx.x; t < nn4; t += blockDim.x) {
+    const int row = t / n, col = t % n;
+    sre[row * rs + col] = mr[t];
+    sim[row * rs + col] = mi[t];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 15;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+    if (b0 + 2 * w >= b1) break;
+    const int64_t b = b0 + 2 * w + ((threadIdx.x >> 4) & 1);
+    const bool live = b < b1;
+    const int kb = live ? box_key[b] : 0;
+    const int odd = kb & 1;
+    double re = 0.0, im = 0.0;
+    for (int q = 0; q < 3; ++q) {
+      // even kb: sources at kb-2, kb+2, kb+3 (o = 2, -2, -3); odd: kb-3, kb-2, kb+2
+      const int o = odd ? (q == 0 ? 3 : (q == 1 ? 2 : -2)) : (q == 0 ? 2 : (q == 1 ? -2 : -3));
+      const int ka = kb - o;
+      // keys of a level are sorted and distinct: a box at key offset
+      // |o| <= 3 sits within three positions of b
+      int64_t a = -1;
+      if (live && ka >= 0) {
+#pragma unroll
+        for (int t = 1; t <= 3; ++t) {
+          const int64_t f = o > 0 ? b - t : b + t;
+          if (a < 0 && f >= b0 && f < b1 && box_key[f] == ka) a = f;
+        }
+      }
+      const int oi = o == -3 ? 0 : (o == -2 ? 1 : (o == 2 ? 2 : 3));
+      const double* rr = sre + (oi * n + lane) * rs;
+      const double* ri = sim + (oi * n + lane) * rs;
+      const double wa = (a >= 0 && lane < n) ? Wm[a * FMM_MAXN + lane] : 0.0;
+      for (int j = 0; j < n; ++j) {
+        const double v = __shfl_sync(0xffffffffu, wa, j, 16);
+        if (a >= 0 && lane < n) {
+          re = fma(rr[j], v, re);
+          im = fma(ri[j], v, im);
+        }
+      }
+    }
+    if (live && lane < n) {
+      Lre[b * FMM_MAXN + lane] = re;
+      Lim[b * FMM_MAXN + lane] = im;
     }
   }
-  if (lane < n) {
-    Lre[c * FMM_MAXN + lane] += re;
-    Lim[c * FMM_MAXN + lane] += im;
+}
+
+// L2L from level l to l+1: child box c gets T_side^T L_parent.
+__global__ void __launch_bounds__(256) l2l_kernel(int64_t c0, int64_t c1,
+                                                  const int* __restrict__ box_key,
+                                                  const int* __restrict__ box_leaf,
+                                                  const int* __restrict__ id, int nl, int l, int n,
+                                                  Tabs tb, double* __restrict__ Lre,
+                                                  double* __restrict__ Lim) {
+  __shared__ double sT[2 * FMM_MAXN * (FMM_MAXN + 1)];  // [side][i][k], padded rows
+  const int rs = n | 1;
+  for (int t = threadIdx.x; t < 2 * n * n; t += blockDim.x) {
+    const int side = t / (n * n), r = (t / n) % n, col = t % n;
+    sT[(side * n + r) * rs + col] = (side ? tb.TR : tb.TL)[r * n + col];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 15;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+    if (c0 + 2 * w >= c1) break;
+    const int64_t c = c0 + 2 * w + ((threadIdx.x >> 4) & 1);
+    const bool live = c < c1;
+    const int64_t par = live ? id[(int64_t)(l - 2) * nl + box_leaf[c]] - 1 : 0;
+    const double* T = sT + ((live && (box_key[c] & 1)) ? n * rs : 0);
+    const double pr = (live && lane < n) ? Lre[par * FMM_MAXN + lane] : 0.0;
+    const double pi = (live && lane < n) ? Lim[par * FMM_MAXN + lane] : 0.0;
+    double re = 0.0, im = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double vr = __shfl_sync(0xffffffffu, pr, i, 16);
+      const double vi = __shfl_sync(0xffffffffu, pi, i, 16);
+      if (live && lane < n) {
+        const double t = T[i * rs + lane];
+        re = fma(t, vr, re);
+        im = fma(t, vi, im);
+      }
+    }
+    if (live && lane < n) {
+      Lre[c * FMM_MAXN + lane] += re;
+      Lim[c * FMM_MAXN + lane] += im;
+    }
   }
 }
 
@@ -328,6 +394,13 @@ __global__ void l2p_near_kernel(const double* __restrict__ s, int64_t ns,
 }
 
 unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// CTAs of 8 warps for nb boxes at two boxes per warp, at most 4 per SM (the
+// kernels stride).
+unsigned half_grid(int64_t nb) {
+  const int64_t need = (nb + 15) / 16;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, 148 * 4));
+}
 
 // Host tables: first-kind Chebyshev points, barycentric weights, M2M and
 // M2L matrices (double precision, computed here once per call).
@@ -495,29 +568,54 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, double* d_
   const int64_t leaf_box0 = off[L - 2];
   {
     LaunchScope ls("fmm_p2m", s);
-    p2m_kernel<<<blocks((int64_t)nl * 32, 256), 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb,
-                                                             leaf_box0, Wm);
-    SHRK_CUDA(cudaGetLastError());
-  }
-  for (int l = L - 1; l >= 2; --l) {
-    const int64_t b0 = off[l - 2], b1 = off[l - 1], c0 = off[l - 1], c1 = off[l];
-    LaunchScope ls("fmm_m2m", s);
-    m2m_kernel<<<blocks((b1 - b0) * 32, 256), 256, 0, s>>>(b0, b1, c0, c1, box_key, box_leaf, lid,
-                                                          nl, l, n, tb, Wm);
+    const unsigned nb = blocks((int64_t)nl * 32, 256);
+    switch (n) {
+      case 4: p2m_kernel<4><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 5: p2m_kernel<5><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 6: p2m_kernel<6><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 7: p2m_kernel<7><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 8: p2m_kernel<8><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 9: p2m_kernel<9><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 10: p2m_kernel<10><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 11: p2m_kernel<11><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 12: p2m_kernel<12><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 13: p2m_kernel<13><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 14: p2m_kernel<14><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 15: p2m_kernel<15><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      default: p2m_kernel<16><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+    }
     SHRK_CUDA(cudaGetLastError());
   }
   {
-    LaunchScope ls("fmm_m2l", s);
-    m2l_kernel<<<blocks(nbox * 32, 256), 256, 0, s>>>(nbox, box_key, box_level, d_off, n, tb, Wm,
-                                                      Lre, Lim);
-    SHRK_CUDA(cudaGetLastError());
+    LaunchScope ls("fmm_m2m", s);
+    for (int l = L - 1; l >= 2; --l) {
+      const int64_t b0 = off[l - 2], b1 = off[l - 1], c0 = off[l - 1], c1 = off[l];
+      (void)c0;
+      m2m_kernel<<<half_grid(b1 - b0), 256, 0, s>>>(b0, b1, c1, box_key, box_leaf, lid, nl, l, n,
+                                                    tb, Wm);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    add_launches(L - 3);
   }
-  for (int l = 2; l < L; ++l) {
-    const int64_t c0 = off[l - 1], c1 = off[l];
+  {
+    LaunchScope ls("fmm_m2l", s);
+    for (int l = 2; l <= L; ++l) {
+      const int64_t b0 = off[l - 2], b1 = off[l - 1];
+      if (b1 > b0)
+        m2l_kernel<<<half_grid(b1 - b0), 256, 0, s>>>(b0, b1, l, box_key, n, tb, Wm, Lre, Lim);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    add_launches(L - 2);
+  }
+  {
     LaunchScope ls("fmm_l2l", s);
-    l2l_kernel<<<blocks((c1 - c0) * 32, 256), 256, 0, s>>>(c0, c1, box_key, box_leaf, lid, nl, l,
-                                                          n, tb, Lre, Lim);
-    SHRK_CUDA(cudaGetLastError());
+    for (int l = 2; l < L; ++l) {
+      const int64_t c0 = off[l - 1], c1 = off[l];
+      l2l_kernel<<<half_grid(c1 - c0), 256, 0, s>>>(c0, c1, box_key, box_leaf, lid, nl, l, n, tb,
+                                                    Lre, Lim);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    add_launches(L - 3);
   }
   {
     LaunchScope ls("fmm_l2p_near", s);
