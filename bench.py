@@ -58,6 +58,8 @@ def parse():
                          "sample covariance")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
     ap.add_argument("--fmm-order", type=int, default=16, help="fmm workload: expansion order")
+    ap.add_argument("--fmm-m2l", type=int, default=0, choices=[0, 1],
+                    help="fmm workload: 0 = FP64 M2L, 1 = tensor-core M2L (TF32 x3)")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target duration of one CPU baseline sample")
@@ -448,13 +450,15 @@ def run_path(args, world, rank, local):
 
         if wl == "fmm":
             family = b"fmm_l2p_near"
-            desc = (f"fmm (order {args.fmm_order}) all-points transform (tree build included), "
+            desc = (f"fmm (order {args.fmm_order}, M2L {'tensor cores TF32x3' if args.fmm_m2l else 'FP64'}) "
+                    f"all-points transform (tree build included), "
                     f"MP(c=0.1)+20 spikes in [3,50] p={p}, eta=1/sqrt(p)")
 
         def step():
             if wl == "fmm":
                 _native.check(L.shrk_stieltjes_fmm_dev(ev.data_ptr(), p, eta, args.fmm_order,
-                                                       xr.data_ptr(), xi.data_ptr(), sp))
+                                                       args.fmm_m2l, xr.data_ptr(), xi.data_ptr(),
+                                                       sp))
                 return
             _native.check(L.shrk_stieltjes_all_dev(ev.data_ptr(), p, eta, mid, 0, float("nan"),
                                                    0, xr.data_ptr(), xi.data_ptr(), sp))
@@ -464,8 +468,8 @@ def run_path(args, world, rank, local):
 
         def e2e():
             if wl == "fmm":
-                _native.check(L.shrk_stieltjes_fmm(dptr(evp), p, eta, args.fmm_order, dptr(rp),
-                                                   dptr(ip)))
+                _native.check(L.shrk_stieltjes_fmm(dptr(evp), p, eta, args.fmm_order,
+                                                   args.fmm_m2l, dptr(rp), dptr(ip)))
                 return
             _native.check(L.shrk_stieltjes_all(dptr(evp), p, eta, mid, 0, float("nan"), 0,
                                                dptr(rp), dptr(ip)))
@@ -514,7 +518,8 @@ def run_path(args, world, rank, local):
     L.shrk_timing_read(family, C.byref(kn), C.byref(kms))
     fams = {}
     if wl == "fmm":
-        for f in (b"fmm_build", b"fmm_p2m", b"fmm_m2m", b"fmm_m2l", b"fmm_l2l", b"fmm_l2p_near"):
+        for f in (b"fmm_build", b"fmm_p2m", b"fmm_m2m", b"fmm_m2l", b"fmm_m2l_tc", b"fmm_l2l",
+                  b"fmm_l2p_near"):
             n_, ms_ = C.c_int64(), C.c_double()
             L.shrk_timing_read(f, C.byref(n_), C.byref(ms_))
             fams[f.decode()] = (n_.value, ms_.value)

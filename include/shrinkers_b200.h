@@ -208,10 +208,12 @@ shrk_status shrk_stieltjes_scaled_ray_dev(const double* d_ev, size_t p, double s
  * eigenvalue, input order, from P2M / M2M / M2L / L2L / L2P on a dyadic tree
  * with leaves of at most 48 eigenvalues and the leaf plus its neighbours
  * summed directly in FP64.  order = Chebyshev points per box, 4..16; the
- * error vs the exact sums falls from ~1e-9 (10) to FP64 round-off (16). */
-shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order, double* out_re,
-                               double* out_im);
-shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int order,
+ * error vs the exact sums falls from ~1e-9 (10) to FP64 round-off (16).
+ * m2l = 0: every stage in FP64; m2l = 1: the M2L stage on the tensor cores
+ * (tcgen05, TF32 x3 products accumulated in FP32, ~1e-7 relative). */
+shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order, int m2l,
+                               double* out_re, double* out_im);
+shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int order, int m2l,
                                    double* d_re, double* d_im, void* stream);
 
 /* fft5.rs:568-590 compute_all_stieltjes_fft5_with_options: RAW sums (not

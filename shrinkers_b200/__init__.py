@@ -416,11 +416,15 @@ def stieltjes_scaled_ray(eigenvalues, scale):
     return {"real": re, "imag": im}
 
 
-def stieltjes_fmm(eigenvalues, eta=INFERRED, order=16):
+def stieltjes_fmm(eigenvalues, eta=INFERRED, order=16, m2l="fp64"):
     """The dyadic Chebyshev FMM (no reference counterpart; the reference's
     ChebCode treecode is method="chebcode*"): S(ev_i)/p at every eigenvalue
     as {"real", "imag"}.  order = Chebyshev points per box in [4, 16]; the
-    error vs the exact sums goes from ~1e-9 (10) to FP64 round-off (16)."""
+    error vs the exact sums goes from ~1e-9 (10) to FP64 round-off (16).
+    m2l="tf32x3" runs the M2L stage on the tensor cores (~1e-7 relative)."""
+    modes = {"fp64": 0, "tf32x3": 1}
+    if m2l not in modes:
+        raise ValueError(f"unknown m2l mode {m2l!r} (expected 'fp64' or 'tf32x3')")
     ev = _owned_f64_vec(eigenvalues, "eigenvalues")
     _require_finite(ev, "eigenvalues")
     if ev.size == 0:
@@ -428,8 +432,8 @@ def stieltjes_fmm(eigenvalues, eta=INFERRED, order=16):
     e = _inferred_f64(eta, "eta")
     e = 0.1 / math.sqrt(ev.size) if e is None else _require_positive_finite(e, "eta")
     re, im = np.empty(ev.size), np.empty(ev.size)
-    _native.check(_lib().shrk_stieltjes_fmm(_dp(ev), ev.size, e, int(order), _dp(re), _dp(im)),
-                  "stieltjes_fmm")
+    _native.check(_lib().shrk_stieltjes_fmm(_dp(ev), ev.size, e, int(order), modes[m2l], _dp(re),
+                                            _dp(im)), "stieltjes_fmm")
     return {"real": re, "imag": im}
 
 

@@ -51,8 +51,8 @@ SIGNATURES = {
     "shrk_chebcode_evaluate_many_dev": (_ST, [_P, _SZ, _P, _SZ, C.c_int, _P, _P, _P]),
     "shrk_stieltjes_scaled_ray": (_ST, [_D, _SZ, C.c_double, _D, _D]),
     "shrk_stieltjes_scaled_ray_dev": (_ST, [_P, _SZ, C.c_double, _P, _P, _P]),
-    "shrk_stieltjes_fmm": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D]),
-    "shrk_stieltjes_fmm_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, _P, _P, _P]),
+    "shrk_stieltjes_fmm": (_ST, [_D, _SZ, C.c_double, C.c_int, C.c_int, _D, _D]),
+    "shrk_stieltjes_fmm_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, C.c_int, _P, _P, _P]),
     "shrk_stieltjes_fft5_with_options": (_ST, [_D, _SZ, C.c_double, C.c_int, _SZ, C.c_double, C.c_double, _D, _D]),
     "shrk_stieltjes_fft5_with_options_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, _SZ, C.c_double, C.c_double, _P, _P, _P]),
     "shrk_inverse_nonlinear_shrinkage": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),

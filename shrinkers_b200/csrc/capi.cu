@@ -891,17 +891,19 @@ static shrk_status check_fmm(size_t p, double eta, int order) {
   return SHRK_OK;
 }
 
-shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int order,
+shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int order, int m2l,
                                    double* d_re, double* d_im, void* stream) {
   SHRK_TRY(check_fmm(p, eta, order));
+  if (m2l != 0 && m2l != 1) return einval("fmm: m2l must be 0 (FP64) or 1 (tensor cores, TF32 x3)");
   Guard g;
   SHRK_TRY(g.st);
-  return fmm_all(d_ev, (int64_t)p, eta, order, d_re, d_im, (cudaStream_t)stream);
+  return fmm_all(d_ev, (int64_t)p, eta, order, m2l, d_re, d_im, (cudaStream_t)stream);
 }
 
-shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order, double* out_re,
-                               double* out_im) {
+shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order, int m2l,
+                               double* out_re, double* out_im) {
   SHRK_TRY(check_fmm(p, eta, order));
+  if (m2l != 0 && m2l != 1) return einval("fmm: m2l must be 0 (FP64) or 1 (tensor cores, TF32 x3)");
   Guard g;
   SHRK_TRY(g.st);
   cudaStream_t s = g_cur->stream;
@@ -910,7 +912,8 @@ shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
-  SHRK_TRY(fmm_all((const double*)dev, (int64_t)p, eta, order, (double*)out, (double*)out + p, s));
+  SHRK_TRY(fmm_all((const double*)dev, (int64_t)p, eta, order, m2l, (double*)out,
+                   (double*)out + p, s));
   SHRK_TRY(d2h(out_re, out, sizeof(double) * p, s));
   SHRK_TRY(d2h(out_im, (double*)out + p, sizeof(double) * p, s));
   return check_device_error(s);

@@ -34,7 +34,7 @@ struct Scratch {
   void* ptr = nullptr;
   size_t bytes = 0;
 };
-shrk_status scratch_get(int slot, size_t bytes, void** out);  // slot in [0, 40)
+shrk_status scratch_get(int slot, size_t bytes, void** out);  // slot in [0, 48)
 int* device_error_word();  // zeroed per call by the launchers that use it
 int sm_count();
 cudaStream_t library_stream();

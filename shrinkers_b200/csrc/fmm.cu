@@ -294,6 +294,226 @@ __global__ void __launch_bounds__(256) m2l_kernel(int64_t b0, int64_t b1, int l,
   }
 }
 
+// ------------------------------------------------ tensor-core M2L --
+// The M2L of one level as a GEMM on the 5th-generation tensor cores: a CTA
+// of 128 threads owns 128 target boxes (one per thread) and computes
+//   D[b][c] = sum_k A[b][k] B[c][k],   k = offset slot * 16 + source node j,
+// A[b][.] = the multipoles of b's interaction partners (zero where a slot is
+// empty), B[c][.] = row c mod 16 of the four M2L matrices (real part for
+// c < 16, imaginary part above), i.e. M = 128, N = 32, K = 64, as
+// tcgen05.mma kind::tf32 with FP32 accumulation in tensor memory, each
+// product split as hi*hi + hi*lo + lo*hi (TF32 x3).  Operands sit in shared
+// memory in the K-major no-swizzle layout: 16-byte chunks (4 values) of
+// chunk column kc and row r at chunk index kc*R + r (R = rows of the tile),
+// so 8-row groups are 128 bytes apart and K chunks R*16 bytes apart.
+constexpr int TC_M = 128, TC_N = 32, TC_K = 64;
+constexpr uint32_t TC_IDESC = (1u << 4)           // D: F32
+                              | (2u << 7)         // A: TF32
+                              | (2u << 10)        // B: TF32
+                              | ((uint32_t)(TC_N >> 3) << 17)
+                              | ((uint32_t)(TC_M >> 4) << 24);  // K-major A and B
+// A tile's interaction partners lie within 3 boxes of it: the multipoles of
+// that window (TC_WIN rows, split into TF32 hi/lo, rows padded to TC_WS
+// floats so that row-strided float4 reads do not conflict) and its keys are
+// staged with coalesced loads before A is assembled in shared memory.
+constexpr int TC_WIN = TC_M + 6, TC_WS = 20;
+constexpr int TC_OS = FMM_MAXN + 1;  // output staging row stride (doubles)
+constexpr int TC_SMEM = 2 * TC_M * TC_K * 4 + 2 * TC_N * TC_K * 4 + 2 * TC_WIN * TC_WS * 4 +
+                        TC_WIN * 4 + 256;
+static_assert(2 * TC_M * TC_OS * 8 <= 2 * TC_M * TC_K * 4, "output staging reuses A");
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+
+__device__ __forceinline__ void tf32_split(double x, float& hi, float& lo) {
+  const float f = (float)x;
+  hi = __uint_as_float(__float_as_uint(f) & 0xFFFFE000u);
+  lo = f - hi;
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+
+__global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, int l,
+                                                      const int* __restrict__ box_key, int n,
+                                                      Tabs tb, const double* __restrict__ Wm,
+                                                      double* __restrict__ Lre,
+                                                      double* __restrict__ Lim,
+                                                      int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  float4* Ahi = reinterpret_cast<float4*>(tsm);
+  float4* Alo = Ahi + TC_M * TC_K / 4;
+  float4* Bhi = Alo + TC_M * TC_K / 4;
+  float4* Blo = Bhi + TC_N * TC_K / 4;
+  float* Whi = reinterpret_cast<float*>(Blo + TC_N * TC_K / 4);
+  float* Wlo = Whi + TC_WIN * TC_WS;
+  int* skey = reinterpret_cast<int*>(Wlo + TC_WIN * TC_WS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(skey + TC_WIN + (TC_WIN & 1));
+  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  double* Ore = reinterpret_cast<double*>(tsm);  // after the MMAs: [row][TC_OS]
+  double* Oim = Ore + TC_M * TC_OS;
+  const int t = threadIdx.x, warp = t >> 5;
+
+  // TMEM: 32 columns (the F32 accumulator of N = 32), held for all tiles
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(taddr_slot)),
+                 "r"(32u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  // B (the level's matrices), built once per CTA: row c, chunk kc
+  const double* mr = tb.Mre + (int64_t)l * 4 * n * n;
+  const double* mi = tb.Mim + (int64_t)l * 4 * n * n;
+  for (int q = t; q < TC_N * (TC_K / 4); q += TC_M) {
+    const int c = q / (TC_K / 4), kc = q % (TC_K / 4);
+    const int i = c & 15, oi = kc / 4;
+    const double* src = (c < 16 ? mr : mi) + ((int64_t)oi * n + i) * n;
+    float h[4], lo[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int j = (kc % 4) * 4 + e;
+      const double v = (i < n && j < n) ? src[j] : 0.0;
+      tf32_split(v, h[e], lo[e]);
+    }
+    Bhi[kc * TC_N + c] = make_float4(h[0], h[1], h[2], h[3]);
+    Blo[kc * TC_N + c] = make_float4(lo[0], lo[1], lo[2], lo[3]);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *taddr_slot;
+  bool ok = true;
+  uint32_t phase = 0;
+
+  for (int64_t tile = blockIdx.x; b0 + tile * TC_M < b1 && ok; tile += gridDim.x) {
+    const int64_t tb0 = b0 + tile * TC_M;
+    const int64_t r0 = tb0 - 3 > b0 ? tb0 - 3 : b0;
+    const int64_t r1 = tb0 + TC_M + 3 < b1 ? tb0 + TC_M + 3 : b1;
+    const int rows = (int)(r1 - r0);
+    for (int q = t; q < rows * FMM_MAXN; q += TC_M) {
+      const int r = q / FMM_MAXN, j = q % FMM_MAXN;
+      const double w = j < n ? Wm[(r0 + r) * FMM_MAXN + j] : 0.0;
+      float h, lo;
+      tf32_split(w, h, lo);
+      Whi[r * TC_WS + j] = h;
+      Wlo[r * TC_WS + j] = lo;
+    }
+    for (int r = t; r < rows; r += TC_M) skey[r] = box_key[r0 + r];
+    __syncthreads();
+    // A: row t = target box b, slot oi = offset o in {-3, -2, 2, 3}
+    const int64_t b = tb0 + t;
+    const bool live = b < b1;
+    const int kb = live ? skey[b - r0] : 0;
+    for (int oi = 0; oi < 4; ++oi) {
+      const int o = oi == 0 ? -3 : (oi == 1 ? -2 : (oi == 2 ? 2 : 3));
+      // even kb: partners at o = 2, -2, -3; odd kb: o = 3, 2, -2
+      const bool inlist = (kb & 1) ? (o != -3) : (o != 3);
+      const int ka = kb - o;
+      int ar = -1;  // the partner's row in the window
+      if (live && inlist && ka >= 0) {
+#pragma unroll
+        for (int q = 1; q <= 3; ++q) {
+          const int64_t f = o > 0 ? b - q : b + q;
+          if (ar < 0 && f >= b0 && f < b1 && skey[f - r0] == ka) ar = (int)(f - r0);
+        }
+      }
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      const float4* wh = reinterpret_cast<const float4*>(Whi + (ar < 0 ? 0 : ar) * TC_WS);
+      const float4* wl = reinterpret_cast<const float4*>(Wlo + (ar < 0 ? 0 : ar) * TC_WS);
+#pragma unroll
+      for (int c4 = 0; c4 < 4; ++c4) {
+        const int kc = oi * 4 + c4;
+        Ahi[kc * TC_M + t] = ar < 0 ? z : wh[c4];
+        Alo[kc * TC_M + t] = ar < 0 ? z : wl[c4];
+      }
+    }
+    fence_proxy_async();  // generic-proxy writes -> tensor-core (async proxy) reads
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (t == 0) {
+      const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo);
+      const uint32_t b_hi = smem_u32(Bhi), b_lo = smem_u32(Blo);
+      constexpr uint32_t ALBO = TC_M * 16, BLBO = TC_N * 16, SBO = 128;
+      for (int st = 0; st < TC_K / 8; ++st) {  // K = 8 per instruction = 2 chunks
+        const uint32_t ao = st * 2 * TC_M * 16, bo = st * 2 * TC_N * 16;
+        umma_tf32(tmem, umma_desc(a_hi + ao, ALBO, SBO), umma_desc(b_hi + bo, BLBO, SBO),
+                  st > 0 ? 1u : 0u);
+        umma_tf32(tmem, umma_desc(a_hi + ao, ALBO, SBO), umma_desc(b_lo + bo, BLBO, SBO), 1u);
+        umma_tf32(tmem, umma_desc(a_lo + ao, ALBO, SBO), umma_desc(b_hi + bo, BLBO, SBO), 1u);
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(bar))
+          : "memory");
+    }
+    const bool done = mbar_wait(bar, phase);
+    if (!done) {
+      atomicExch(err, DEV_ERR_TIMEOUT);
+      mbar_wait(bar, phase, 200000000LL);  // the MMAs may still be in flight
+    }
+    phase ^= 1u;
+    ok = __syncthreads_and(done) != 0;  // tcgen05.ld below is warp-collective
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+          "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+          "%28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+            "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+            "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+            "=r"(v[31])
+          : "r"(tmem + ((uint32_t)(warp * 32) << 16))
+          : "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      // A is no longer read (the MMAs completed): stage the rows there
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        Ore[t * TC_OS + i] = (double)__uint_as_float(v[i]);
+        Oim[t * TC_OS + i] = (double)__uint_as_float(v[16 + i]);
+      }
+    }
+    __syncthreads();
+    if (ok) {
+      const int live_rows = (int)(b1 - tb0 < TC_M ? b1 - tb0 : TC_M);
+      for (int q = t; q < live_rows * FMM_MAXN; q += TC_M) {
+        const int r = q / FMM_MAXN, i = q % FMM_MAXN;
+        if (i < n) {
+          Lre[tb0 * FMM_MAXN + q] = Ore[r * TC_OS + i];
+          Lim[tb0 * FMM_MAXN + q] = Oim[r * TC_OS + i];
+        }
+      }
+    }
+    // the next tile rewrites A and the accumulator only after every thread
+    // has read its row; a timeout anywhere ends the loop for the whole CTA
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    ok = __syncthreads_and(ok) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u)
+                 : "memory");
+  }
+}
+
 // L2L from level l to l+1: child box c gets T_side^T L_parent.
 __global__ void __launch_bounds__(256) l2l_kernel(int64_t c0, int64_t c1,
                                                   const int* __restrict__ box_key,
@@ -449,8 +669,8 @@ void host_tables(int n, int L, double W, double eta, std::vector<double>& tab) {
 
 }  // namespace
 
-shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, double* d_re, double* d_im,
-                    cudaStream_t s) {
+shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc, double* d_re,
+                    double* d_im, cudaStream_t s) {
   if (p <= 0) return SHRK_OK;
   const double* ds = nullptr;
   const int* perm = nullptr;
@@ -597,7 +817,26 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, double* d_
     }
     add_launches(L - 3);
   }
-  {
+  if (m2l_tc) {
+    static bool opted[64] = {false};
+    int dev = 0;
+    SHRK_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && !opted[dev]) {
+      SHRK_CUDA(cudaFuncSetAttribute(m2l_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TC_SMEM));
+      opted[dev] = true;
+    }
+    LaunchScope ls("fmm_m2l_tc", s);
+    for (int l = 2; l <= L; ++l) {
+      const int64_t b0 = off[l - 2], b1 = off[l - 1];
+      if (b1 > b0)
+        m2l_tc_kernel<<<(unsigned)std::min<int64_t>(blocks(b1 - b0, TC_M), 2 * 148), TC_M,
+                        TC_SMEM, s>>>(b0, b1, l, box_key, n, tb, Wm, Lre, Lim,
+                                      device_error_word());
+      SHRK_CUDA(cudaGetLastError());
+    }
+    add_launches(L - 2);
+  } else {
     LaunchScope ls("fmm_m2l", s);
     for (int l = 2; l <= L; ++l) {
       const int64_t b0 = off[l - 2], b1 = off[l - 1];

@@ -150,9 +150,10 @@ struct LibScope {
 };
 
 // Dyadic Chebyshev FMM (fmm.cu): S(ev_t)/p at every eigenvalue, in the
-// caller's order, expansion order n in [4, 16].
-shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, double* d_re, double* d_im,
-                    cudaStream_t s);
+// caller's order, expansion order n in [4, 16]; m2l_tc: M2L on the tensor
+// cores (TF32 x3) instead of FP64.
+shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc, double* d_re,
+                    double* d_im, cudaStream_t s);
 
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);

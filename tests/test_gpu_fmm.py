@@ -20,11 +20,11 @@ _D = C.POINTER(C.c_double)
 BARS = {10: 1e-8, 12: 5e-10, 16: 1e-12}
 
 
-def fmm(ev, eta, order):
+def fmm(ev, eta, order, m2l=0):
     L = _native.load()
     ev = np.ascontiguousarray(ev, dtype=np.float64)
     re, im = np.empty(ev.size), np.empty(ev.size)
-    _native.check(L.shrk_stieltjes_fmm(ev.ctypes.data_as(_D), ev.size, eta, order,
+    _native.check(L.shrk_stieltjes_fmm(ev.ctypes.data_as(_D), ev.size, eta, order, m2l,
                                        re.ctypes.data_as(_D), im.ctypes.data_as(_D)))
     return re, im
 
@@ -89,3 +89,20 @@ def test_unsorted_input_and_python_api(rk, oracle):
     np.testing.assert_array_equal(out["real"], re)
     with pytest.raises(ValueError, match="order"):
         rk.stieltjes_fmm(ev, eta=eta, order=3)
+
+
+@pytest.mark.parametrize("p", [3000, 200_000])
+def test_tensor_core_m2l(oracle, p):
+    """M2L on the tensor cores (TF32 x3, FP32 accumulation): the same
+    expansions, error ~1e-7 of the far field against the FP64 M2L."""
+    ev = spectra.config5(p)
+    eta = 1.0 / math.sqrt(p)
+    r64, i64 = fmm(ev, eta, 16)
+    rtc, itc = fmm(ev, eta, 16, m2l=1)
+    err = rel(rtc, itc, r64, i64)
+    assert np.all(np.isfinite(rtc)) and np.all(np.isfinite(itc))
+    assert np.median(err) < 2e-6, np.median(err)
+    assert err.max() < 1e-4, err.max()
+    if p <= 3000:
+        ore, oim = oracle.compute_all(ev, eta, "blocked")
+        assert np.median(rel(rtc, itc, ore, oim)) < 2e-6
