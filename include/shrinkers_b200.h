@@ -347,6 +347,11 @@ int64_t shrk_launch_count(void);
  * second, one FMA = one op) for FP32 and FP64: the roofline denominators of
  * the exact kernels.  Runs two short probe kernels. */
 shrk_status shrk_measure_pipe_rates(double* fp32_ops_per_s, double* fp64_ops_per_s);
+/* Mean relative error of the FP32 MUFU reciprocal (rcp.approx.ftz.f32) of
+ * the current device over every mantissa of [1, 2): plain and weighted 1/m
+ * (log-uniform).  The mixed-precision pair kernel removes the log-uniform
+ * mean from its FP32 far-field partials; this probe re-measures it. */
+shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean);
 
 #ifdef __cplusplus
 }

@@ -77,6 +77,7 @@ SIGNATURES = {
     "shrk_timing_read": (_ST, [C.c_char_p, _I64, _D]),
     "shrk_launch_count": (C.c_int64, []),
     "shrk_measure_pipe_rates": (_ST, [_D, _D]),
+    "shrk_measure_rcp_bias": (_ST, [_D, _D]),
 }
 
 _lib = None

@@ -1208,4 +1208,11 @@ shrk_status shrk_measure_pipe_rates(double* fp32, double* fp64) {
   return measure_pipe_rates(fp32, fp64);
 }
 
+shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean) {
+  Guard g;
+  SHRK_TRY(g.st);
+  if (!uniform_mean || !log_mean) return einval("null output pointer");
+  return measure_rcp_bias(uniform_mean, log_mean);
+}
+
 }  // extern "C"

@@ -157,5 +157,6 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
 
 double mixed_near_k();
 shrk_status measure_pipe_rates(double* fp32, double* fp64);
+shrk_status measure_rcp_bias(double* uniform_mean, double* log_mean);
 
 }  // namespace shrk

@@ -62,7 +62,7 @@ __device__ __forceinline__ bool pair_item(const PairItem& a, PairStage& st, uint
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double eta = a.eta, eta2 = eta * eta;
   const float eta2f = (float)eta2;
-  const u64 ETA2 = pk2(eta2f, eta2f), ONE = pk2(1.0f, 1.0f);
+  const u64 ETA2 = pk2(eta2f, eta2f);
 
   const int64_t wbase = a.tile0 + (int64_t)warp * WT;
   const double x0 = a.tgt[a.tile0];
@@ -167,7 +167,7 @@ __device__ __forceinline__ bool pair_item(const PairItem& a, PairStage& st, uint
           TL[kk] = pk2((float)(o0 - (double)h0), (float)(o1 - (double)h1));
         }
         const float4* sp = &st.sm4[sub / 2];
-        const u64 ETA2_ = ETA2, ONE_ = ONE;
+        const u64 ETA2_ = ETA2;
         for (int j = 0; j < SUB / 2; j += FOLD / 2) {
           u64 RE[R2], IV[R2];
 #pragma unroll
@@ -178,18 +178,20 @@ __device__ __forceinline__ bool pair_item(const PairItem& a, PairStage& st, uint
             const u64 SM = pk2(s4.x, s4.y), DL = pk2(s4.z, s4.w);
 #pragma unroll
             for (int kk = 0; kk < R2; ++kk)
-              pairs32x4(SM, DL, TH[kk], TL[kk], ETA2_, ONE_, RE[kk], IV[kk]);
+              pairs32x4(SM, DL, TH[kk], TL[kk], ETA2_, RE[kk], IV[kk]);
           }
-          // FP32 partials of FOLD sources are folded into FP64 (negated).
+          // FP32 partials of FOLD sources are folded into FP64 (negated),
+          // with the reciprocal's mean error taken out.
+          constexpr double CORR = 1.0 - RCP32_BIAS;
 #pragma unroll
           for (int kk = 0; kk < R2; ++kk) {
             float r0, r1, v0, v1;
             upk2(RE[kk], r0, r1);
             upk2(IV[kk], v0, v1);
-            re64[2 * kk] -= (double)r0;
-            re64[2 * kk + 1] -= (double)r1;
-            iv64[2 * kk] -= (double)v0;
-            iv64[2 * kk + 1] -= (double)v1;
+            re64[2 * kk] = fma(-(double)r0, CORR, re64[2 * kk]);
+            re64[2 * kk + 1] = fma(-(double)r1, CORR, re64[2 * kk + 1]);
+            iv64[2 * kk] = fma(-(double)v0, CORR, iv64[2 * kk]);
+            iv64[2 * kk + 1] = fma(-(double)v1, CORR, iv64[2 * kk + 1]);
           }
         }
       } else {

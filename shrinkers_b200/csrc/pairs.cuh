@@ -112,6 +112,16 @@ __device__ __forceinline__ u64 fmul2(u64 a, u64 b) {
   return d;
 }
 
+// Mean relative error of the MUFU reciprocal (rcp.approx.ftz.f32) on
+// sm_100, measured over every mantissa of [1, 2) with the log-uniform weight
+// 1/m (shrk_measure_rcp_bias): r_mufu = (1/a)(1 + RCP32_BIAS) on average.
+// A far field of ~1e6 terms of one sign would carry this offset coherently,
+// so the FP64 fold scales each FP32 partial by (1 - RCP32_BIAS) instead of
+// refining every reciprocal with a Newton step (two packed FMAs per four
+// pairs); the remaining error of a seed (<= 1 ulp, zero mean) averages out
+// over the sum like the rounding of a refined reciprocal.
+constexpr double RCP32_BIAS = 3.7e-9;
+
 // Four FP32 far-field pairs: two targets (the packed lanes) x two sources
 // s1, s2 of one 256-source block with centre cb.
 //   TH + TL = x - cb   (TH = float(x - cb), TL = the rounding remainder)
@@ -124,14 +134,14 @@ __device__ __forceinline__ u64 fmul2(u64 a, u64 b) {
 // one rounding at ulp(d) depends on each source's low bits, so the
 // separation errors of different pairs are independent.
 // One reciprocal serves both sources:
-//   e_k = d_k^2 + eta^2,  r = 1/(e1 e2) (MUFU seed + one Newton step, which
-//   removes the seed's nonzero mean error),
+//   e_k = d_k^2 + eta^2,  r = 1/(e1 e2) (MUFU, its mean error removed at the
+//   fold: RCP32_BIAS),
 //   d1/e1 + d2/e2 = (d1 e2 + d2 e1) r,   1/e1 + 1/e2 = (e1 + e2) r.
 // r is carried negated (NR = -r) so the packed pipe needs no negation:
 // RE and IVN accumulate -sum d/e and -sum 1/e.  The caller keeps e1 e2
 // inside the FP32 normal range (block span <= 1e9, gap >= 1e-9).
-__device__ __forceinline__ void pairs32x4(u64 SM, u64 DL, u64 TH, u64 TL, u64 ETA2, u64 ONE,
-                                          u64& RE, u64& IVN) {
+__device__ __forceinline__ void pairs32x4(u64 SM, u64 DL, u64 TH, u64 TL, u64 ETA2, u64& RE,
+                                          u64& IVN) {
   const u64 D1 = fsub2(TH, fsub2(SM, TL));
   const u64 D2 = fadd2(D1, DL);
   const u64 E1 = ffma2(D1, D1, ETA2);
@@ -139,9 +149,7 @@ __device__ __forceinline__ void pairs32x4(u64 SM, u64 DL, u64 TH, u64 TL, u64 ET
   const u64 P = fmul2(E1, E2);
   float a0, a1;
   upk2(P, a0, a1);
-  const u64 NR0 = pk2(rcp_f32(-a0), rcp_f32(-a1));
-  const u64 E = ffma2(P, NR0, ONE);   // 1 - P r
-  const u64 NR = ffma2(NR0, E, NR0);  // -(r + r e)
+  const u64 NR = pk2(rcp_f32(-a0), rcp_f32(-a1));
   const u64 NUM = ffma2(D1, E2, fmul2(D2, E1));
   RE = ffma2(NUM, NR, RE);
   IVN = ffma2(fadd2(E1, E2), NR, IVN);

@@ -1,9 +1,12 @@
 // Pipe-rate probes: measured FP32 and FP64 FMA lane-op rates of the current
-// device, the denominators of the exact kernels' roofline fractions.  Each
+// device, the denominators of the exact kernels' roofline fractions; and the
+// mean error of the MUFU reciprocal that the mixed kernel corrects for.  Each
 // thread runs independent dependency chains of FMAs whose operands stay in
 // registers, sized so that issue (not latency) limits the rate.
 #include "common.cuh"
 #include "internal.h"
+
+#include <vector>
 
 namespace shrk {
 namespace {
@@ -45,7 +48,57 @@ shrk_status rate(double* out, cudaStream_t s) {
   return SHRK_OK;
 }
 
+// Relative error of the MUFU reciprocal over every mantissa of [1, 2):
+// a = 1 + k 2^-23, rel = r a - 1 (the product of two floats is exact in
+// FP64).  Per block: the plain sum of rel, the sum of rel / a and the sum of
+// 1 / a (the log-uniform weight), reduced in a fixed order.
+constexpr int BIAS_PER = 16, BIAS_NT = 256, BIAS_BLOCKS = (1 << 23) / (BIAS_NT * BIAS_PER);
+
+__global__ void __launch_bounds__(BIAS_NT) rcp_bias_kernel(double* part) {
+  __shared__ double red[3][BIAS_NT];
+  double su = 0.0, sl = 0.0, wl = 0.0;
+  for (int i = 0; i < BIAS_PER; ++i) {
+    const uint32_t k = (uint32_t)(blockIdx.x * BIAS_NT + threadIdx.x) * BIAS_PER + i;
+    const float a = __uint_as_float(0x3F800000u | k);
+    const float r = -rcp_f32(-a);  // the negated form the pair kernel uses
+    const double rel = (double)r * (double)a - 1.0;
+    su += rel;
+    sl += rel / (double)a;
+    wl += 1.0 / (double)a;
+  }
+  red[0][threadIdx.x] = su;
+  red[1][threadIdx.x] = sl;
+  red[2][threadIdx.x] = wl;
+  __syncthreads();
+  for (int h = BIAS_NT / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+      for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) part[blockIdx.x * 3 + threadIdx.x] = red[threadIdx.x][0];
+}
+
 }  // namespace
+
+shrk_status measure_rcp_bias(double* uniform_mean, double* log_mean) {
+  cudaStream_t s = library_stream();
+  void* part = nullptr;
+  SHRK_TRY(scratch_get(15, (size_t)BIAS_BLOCKS * 3 * sizeof(double), &part));
+  rcp_bias_kernel<<<BIAS_BLOCKS, BIAS_NT, 0, s>>>((double*)part);
+  SHRK_CUDA(cudaGetLastError());
+  std::vector<double> h((size_t)BIAS_BLOCKS * 3);
+  SHRK_CUDA(cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  double su = 0.0, sl = 0.0, wl = 0.0;
+  for (int b = 0; b < BIAS_BLOCKS; ++b) {
+    su += h[b * 3];
+    sl += h[b * 3 + 1];
+    wl += h[b * 3 + 2];
+  }
+  *uniform_mean = su / (double)(1 << 23);
+  *log_mean = sl / wl;
+  return SHRK_OK;
+}
 
 shrk_status measure_pipe_rates(double* fp32, double* fp64) {
   cudaStream_t s = library_stream();

@@ -162,6 +162,19 @@ def test_mixed_precision_error_vs_truth(oracle, p, median_bar):
     assert np.max(err) <= 1e-6, np.max(err)
 
 
+def test_rcp_bias_probe_matches_the_correction():
+    """The mixed kernel takes the MUFU reciprocal's mean relative error
+    (+3.7e-9 with the log-uniform weight over the mantissas) out of its FP32
+    far-field partials instead of refining each reciprocal; the probe
+    re-measures that mean on this device over all 2^23 mantissas."""
+    L = _native.load()
+    uni, logm = C.c_double(), C.c_double()
+    _native.check(L.shrk_measure_rcp_bias(C.byref(uni), C.byref(logm)))
+    assert abs(logm.value - 3.7e-9) < 0.5e-9, (uni.value, logm.value)
+    with pytest.raises(ValueError):
+        _native.check(L.shrk_measure_rcp_bias(None, C.byref(logm)))
+
+
 def test_cutoff_windowed_matches_oracle(oracle):
     """mod.rs:998-1033: with a cutoff the exact family runs the windowed sums."""
     p = 8000
