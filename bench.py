@@ -518,8 +518,8 @@ def run_path(args, world, rank, local):
     L.shrk_timing_read(family, C.byref(kn), C.byref(kms))
     fams = {}
     if wl == "fmm":
-        for f in (b"fmm_build", b"fmm_p2m", b"fmm_m2m", b"fmm_m2l", b"fmm_m2l_tc", b"fmm_l2l",
-                  b"fmm_l2p_near"):
+        for f in (b"fmm_build", b"fmm_p2m", b"fmm_m2m", b"fmm_top", b"fmm_down", b"fmm_m2l_tc",
+                  b"fmm_l2l", b"fmm_l2p_near"):
             n_, ms_ = C.c_int64(), C.c_double()
             L.shrk_timing_read(f, C.byref(n_), C.byref(ms_))
             fams[f.decode()] = (n_.value, ms_.value)

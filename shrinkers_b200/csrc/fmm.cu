@@ -197,53 +197,21 @@ __global__ void p2m_kernel(const double* __restrict__ s, const int* __restrict__
 // = node i, n <= 16): warp w of a level takes boxes 2w and 2w + 1, warps
 // striding over the level; the loop exit is uniform across the warp.
 
-// M2M for level l: parent box b gets T_side W_child from each child.
-__global__ void __launch_bounds__(256) m2m_kernel(int64_t b0, int64_t b1, int64_t c1,
-                                                  const int* __restrict__ box_key,
-                                                  const int* __restrict__ box_leaf,
-                                                  const int* __restrict__ id, int nl, int l, int n,
-                                                  Tabs tb, double* __restrict__ Wm) {
-  __shared__ double sT[2 * FMM_MAXN * (FMM_MAXN + 1)];  // [side][j][k], padded rows
-  const int rs = n | 1;
+// Shared-memory tables, rows padded to an odd number of doubles so that lane
+// i's row starts on its own bank pair.
+constexpr int FMM_RS = FMM_MAXN + 1;
+
+__device__ __forceinline__ void load_side_tables(double* sT, const Tabs& tb, int n) {
+  const int rs = n | 1;  // [side][j][k]
   for (int t = threadIdx.x; t < 2 * n * n; t += blockDim.x) {
     const int side = t / (n * n), r = (t / n) % n, col = t % n;
     sT[(side * n + r) * rs + col] = (side ? tb.TR : tb.TL)[r * n + col];
   }
-  __syncthreads();
-  const int lane = threadIdx.x & 15;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
-    if (b0 + 2 * w >= b1) break;
-    const int64_t b = b0 + 2 * w + ((threadIdx.x >> 4) & 1);
-    const bool live = b < b1;
-    double acc = 0.0;
-    int64_t first = live ? id[(int64_t)(l + 1 - 2) * nl + box_leaf[b]] - 1 : 0;
-    const int kb = live ? box_key[b] : 0;
-    for (int q = 0; q < 2; ++q) {
-      const int64_t ch = first + q;
-      const bool has = live && ch < c1 && (box_key[ch] >> 1) == kb;
-      const double* T = sT + ((has && (box_key[ch] & 1)) ? n * rs : 0);
-      const double wc = (has && lane < n) ? Wm[ch * FMM_MAXN + lane] : 0.0;
-      for (int kk = 0; kk < n; ++kk) {
-        const double v = __shfl_sync(0xffffffffu, wc, kk, 16);
-        if (has && lane < n) acc = fma(T[lane * rs + kk], v, acc);
-      }
-    }
-    if (live && lane < n) Wm[b * FMM_MAXN + lane] = acc;
-  }
 }
 
-// M2L for the boxes [b0, b1) of level l: the level's four n x n complex
-// matrices are staged in shared memory once per CTA.
-__global__ void __launch_bounds__(256) m2l_kernel(int64_t b0, int64_t b1, int l,
-                                                  const int* __restrict__ box_key, int n, Tabs tb,
-                                                  const double* __restrict__ Wm,
-                                                  double* __restrict__ Lre,
-                                                  double* __restrict__ Lim) {
-  // rows padded to an odd number of doubles: lane i's row starts on its own
-  // bank pair
-  __shared__ double sre[4 * FMM_MAXN * (FMM_MAXN + 1)], sim[4 * FMM_MAXN * (FMM_MAXN + 1)];
-  const int nn4 = 4 * n * n, rs = n | 1;
+__device__ __forceinline__ void load_m2l_tables(double* sre, double* sim, const Tabs& tb, int l,
+                                                int n) {
+  const int nn4 = 4 * n * n, rs = n | 1;  // [oi][i][j]
   const double* mr = tb.Mre + (int64_t)l * nn4;
   const double* mi = tb.Mim + (int64_t)l * nn4;
   for (int t = threadIdx.x; t < nn4; t += blockDim.x) {
@@ -251,6 +219,105 @@ __global__ void __launch_bounds__(256) m2l_kernel(int64_t b0, int64_t b1, int l,
     sre[row * rs + col] = mr[t];
     sim[row * rs + col] = mi[t];
   }
+}
+
+// Per-box bodies, half a warp per box (lane = node).  Every lane of the warp
+// calls them together (they shuffle); `live` masks the arithmetic.  The
+// expansion arrays are plain pointers: the fused top-of-tree kernel reads
+// what it wrote at the previous level.
+
+// M2M: parent b (level l) gets T_side W_child from each child (level l+1,
+// boxes before c1).
+__device__ __forceinline__ double m2m_box(int64_t b, bool live, int64_t c1, const int* box_key,
+                                          const int* box_leaf, const int* id, int nl, int l,
+                                          int n, const double* sT, const double* Wm, int lane) {
+  const int rs = n | 1;
+  double acc = 0.0;
+  const int64_t first = live ? id[(int64_t)(l + 1 - 2) * nl + box_leaf[b]] - 1 : 0;
+  const int kb = live ? box_key[b] : 0;
+  for (int q = 0; q < 2; ++q) {
+    const int64_t ch = first + q;
+    const bool has = live && ch < c1 && (box_key[ch] >> 1) == kb;
+    const double* T = sT + ((has && (box_key[ch] & 1)) ? n * rs : 0);
+    const double wc = (has && lane < n) ? Wm[ch * FMM_MAXN + lane] : 0.0;
+    for (int kk = 0; kk < n; ++kk) {
+      const double v = __shfl_sync(0xffffffffu, wc, kk, 16);
+      if (has && lane < n) acc = fma(T[lane * rs + kk], v, acc);
+    }
+  }
+  return acc;
+}
+
+// M2L: box b of level l (boxes [b0, b1)) from its three interaction
+// partners, with the level's four matrices in shared memory.
+__device__ __forceinline__ void m2l_box(int64_t b, bool live, int64_t b0, int64_t b1,
+                                        const int* box_key, int n, const double* sre,
+                                        const double* sim, const double* Wm, int lane,
+                                        double& re, double& im) {
+  const int rs = n | 1;
+  const int kb = live ? box_key[b] : 0;
+  const int odd = kb & 1;
+  re = 0.0;
+  im = 0.0;
+  for (int q = 0; q < 3; ++q) {
+    // even kb: sources at kb-2, kb+2, kb+3 (o = 2, -2, -3); odd: kb-3, kb-2, kb+2
+    const int o = odd ? (q == 0 ? 3 : (q == 1 ? 2 : -2)) : (q == 0 ? 2 : (q == 1 ? -2 : -3));
+    const int ka = kb - o;
+    // keys of a level are sorted and distinct: a box at key offset |o| <= 3
+    // sits within three positions of b
+    int64_t a = -1;
+    if (live && ka >= 0) {
+#pragma unroll
+      for (int t = 1; t <= 3; ++t) {
+        const int64_t f = o > 0 ? b - t : b + t;
+        if (a < 0 && f >= b0 && f < b1 && box_key[f] == ka) a = f;
+      }
+    }
+    const int oi = o == -3 ? 0 : (o == -2 ? 1 : (o == 2 ? 2 : 3));
+    const double* rr = sre + (oi * n + lane) * rs;
+    const double* ri = sim + (oi * n + lane) * rs;
+    const double wa = (a >= 0 && lane < n) ? Wm[a * FMM_MAXN + lane] : 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double v = __shfl_sync(0xffffffffu, wa, j, 16);
+      if (a >= 0 && lane < n) {
+        re = fma(rr[j], v, re);
+        im = fma(ri[j], v, im);
+      }
+    }
+  }
+}
+
+// L2L: child c (level l + 1) gets T_side^T L_parent (parent at level l).
+__device__ __forceinline__ void l2l_box(int64_t c, bool live, const int* box_key,
+                                        const int* box_leaf, const int* id, int nl, int l, int n,
+                                        const double* sT, const double* Lre, const double* Lim,
+                                        int lane, double& re, double& im) {
+  const int rs = n | 1;
+  const int64_t par = live ? id[(int64_t)(l - 2) * nl + box_leaf[c]] - 1 : 0;
+  const double* T = sT + ((live && (box_key[c] & 1)) ? n * rs : 0);
+  const double pr = (live && lane < n) ? Lre[par * FMM_MAXN + lane] : 0.0;
+  const double pi = (live && lane < n) ? Lim[par * FMM_MAXN + lane] : 0.0;
+  re = 0.0;
+  im = 0.0;
+  for (int i = 0; i < n; ++i) {
+    const double vr = __shfl_sync(0xffffffffu, pr, i, 16);
+    const double vi = __shfl_sync(0xffffffffu, pi, i, 16);
+    if (live && lane < n) {
+      const double t = T[i * rs + lane];
+      re = fma(t, vr, re);
+      im = fma(t, vi, im);
+    }
+  }
+}
+
+// M2M for level l: parent box b gets T_side W_child from each child.
+__global__ void __launch_bounds__(256) m2m_kernel(int64_t b0, int64_t b1, int64_t c1,
+                                                  const int* __restrict__ box_key,
+                                                  const int* __restrict__ box_leaf,
+                                                  const int* __restrict__ id, int nl, int l, int n,
+                                                  Tabs tb, double* __restrict__ Wm) {
+  __shared__ double sT[2 * FMM_MAXN * FMM_RS];
+  load_side_tables(sT, tb, n);
   __syncthreads();
   const int lane = threadIdx.x & 15;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -258,39 +325,94 @@ __global__ void __launch_bounds__(256) m2l_kernel(int64_t b0, int64_t b1, int l,
     if (b0 + 2 * w >= b1) break;
     const int64_t b = b0 + 2 * w + ((threadIdx.x >> 4) & 1);
     const bool live = b < b1;
-    const int kb = live ? box_key[b] : 0;
-    const int odd = kb & 1;
-    double re = 0.0, im = 0.0;
-    for (int q = 0; q < 3; ++q) {
-      // even kb: sources at kb-2, kb+2, kb+3 (o = 2, -2, -3); odd: kb-3, kb-2, kb+2
-      const int o = odd ? (q == 0 ? 3 : (q == 1 ? 2 : -2)) : (q == 0 ? 2 : (q == 1 ? -2 : -3));
-      const int ka = kb - o;
-      // keys of a level are sorted and distinct: a box at key offset
-      // |o| <= 3 sits within three positions of b
-      int64_t a = -1;
-      if (live && ka >= 0) {
-#pragma unroll
-        for (int t = 1; t <= 3; ++t) {
-          const int64_t f = o > 0 ? b - t : b + t;
-          if (a < 0 && f >= b0 && f < b1 && box_key[f] == ka) a = f;
-        }
-      }
-      const int oi = o == -3 ? 0 : (o == -2 ? 1 : (o == 2 ? 2 : 3));
-      const double* rr = sre + (oi * n + lane) * rs;
-      const double* ri = sim + (oi * n + lane) * rs;
-      const double wa = (a >= 0 && lane < n) ? Wm[a * FMM_MAXN + lane] : 0.0;
-      for (int j = 0; j < n; ++j) {
-        const double v = __shfl_sync(0xffffffffu, wa, j, 16);
-        if (a >= 0 && lane < n) {
-          re = fma(rr[j], v, re);
-          im = fma(ri[j], v, im);
-        }
-      }
-    }
+    const double acc = m2m_box(b, live, c1, box_key, box_leaf, id, nl, l, n, sT, Wm, lane);
+    if (live && lane < n) Wm[b * FMM_MAXN + lane] = acc;
+  }
+}
+
+// Downward pass of level l (boxes [b0, b1)), M2L and L2L in one launch:
+// L_b = M2L(partners) + T^T L_parent (the parent's L is complete: levels run
+// in order).  Level 2 has no parent term.
+__global__ void __launch_bounds__(256) down_kernel(int64_t b0, int64_t b1, int l,
+                                                   const int* __restrict__ box_key,
+                                                   const int* __restrict__ box_leaf,
+                                                   const int* __restrict__ id, int nl, int n,
+                                                   Tabs tb, const double* __restrict__ Wm,
+                                                   double* __restrict__ Lre,
+                                                   double* __restrict__ Lim) {
+  __shared__ double sre[4 * FMM_MAXN * FMM_RS], sim[4 * FMM_MAXN * FMM_RS];
+  __shared__ double sT[2 * FMM_MAXN * FMM_RS];
+  load_m2l_tables(sre, sim, tb, l, n);
+  load_side_tables(sT, tb, n);
+  __syncthreads();
+  const int lane = threadIdx.x & 15;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+    if (b0 + 2 * w >= b1) break;
+    const int64_t b = b0 + 2 * w + ((threadIdx.x >> 4) & 1);
+    const bool live = b < b1;
+    double re, im, pr = 0.0, pi = 0.0;
+    m2l_box(b, live, b0, b1, box_key, n, sre, sim, Wm, lane, re, im);
+    if (l > 2) l2l_box(b, live, box_key, box_leaf, id, nl, l - 1, n, sT, Lre, Lim, lane, pr, pi);
     if (live && lane < n) {
-      Lre[b * FMM_MAXN + lane] = re;
-      Lim[b * FMM_MAXN + lane] = im;
+      Lre[b * FMM_MAXN + lane] = re + pr;
+      Lim[b * FMM_MAXN + lane] = im + pi;
     }
+  }
+}
+
+// The top of the tree in one CTA: levels 2..K hold at most FMM_TOP_BOXES
+// boxes each, too few to fill the GPU, so one launch per level would cost
+// more than its work.  Given W at level K, the CTA runs M2M up to level 2,
+// then M2L + L2L down to level K, with a block barrier between levels (the
+// writes of one level are visible to every thread of the CTA at the next).
+// With tensor-core M2L the levels up to K still take this FP64 M2L.
+constexpr int FMM_TOP_BOXES = 128;
+constexpr int FMM_TOP_NT = 1024;
+
+struct LevelOffs {
+  int64_t o[FMM_LMAX];  // o[l - 2] = first box of level l, o[l - 1] = one past it
+};
+
+__global__ void __launch_bounds__(FMM_TOP_NT) top_kernel(LevelOffs off, int K,
+                                                         const int* __restrict__ box_key,
+                                                         const int* __restrict__ box_leaf,
+                                                         const int* __restrict__ id, int nl,
+                                                         int n, Tabs tb, double* Wm, double* Lre,
+                                                         double* Lim) {
+  __shared__ double sre[4 * FMM_MAXN * FMM_RS], sim[4 * FMM_MAXN * FMM_RS];
+  __shared__ double sT[2 * FMM_MAXN * FMM_RS];
+  load_side_tables(sT, tb, n);
+  __syncthreads();
+  const int lane = threadIdx.x & 15, half = (threadIdx.x >> 4) & 1;
+  const int warp = threadIdx.x >> 5, nw = FMM_TOP_NT / 32;
+  for (int l = K - 1; l >= 2; --l) {
+    const int64_t b0 = off.o[l - 2], b1 = off.o[l - 1], c1 = off.o[l];
+    for (int64_t w = warp; b0 + 2 * w < b1; w += nw) {
+      const int64_t b = b0 + 2 * w + half;
+      const bool live = b < b1;
+      const double acc = m2m_box(b, live, c1, box_key, box_leaf, id, nl, l, n, sT, Wm, lane);
+      if (live && lane < n) Wm[b * FMM_MAXN + lane] = acc;
+    }
+    __syncthreads();
+  }
+  for (int l = 2; l <= K; ++l) {
+    load_m2l_tables(sre, sim, tb, l, n);
+    __syncthreads();
+    const int64_t b0 = off.o[l - 2], b1 = off.o[l - 1];
+    for (int64_t w = warp; b0 + 2 * w < b1; w += nw) {
+      const int64_t b = b0 + 2 * w + half;
+      const bool live = b < b1;
+      double re, im, pr = 0.0, pi = 0.0;
+      m2l_box(b, live, b0, b1, box_key, n, sre, sim, Wm, lane, re, im);
+      if (l > 2)
+        l2l_box(b, live, box_key, box_leaf, id, nl, l - 1, n, sT, Lre, Lim, lane, pr, pi);
+      if (live && lane < n) {
+        Lre[b * FMM_MAXN + lane] = re + pr;
+        Lim[b * FMM_MAXN + lane] = im + pi;
+      }
+    }
+    __syncthreads();  // this level's L before the next level's L2L; tables reloaded
   }
 }
 
@@ -514,19 +636,16 @@ __global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, in
   }
 }
 
-// L2L from level l to l+1: child box c gets T_side^T L_parent.
+// L2L from level l to l+1: child box c gets T_side^T L_parent (added to the
+// child's M2L result).
 __global__ void __launch_bounds__(256) l2l_kernel(int64_t c0, int64_t c1,
                                                   const int* __restrict__ box_key,
                                                   const int* __restrict__ box_leaf,
                                                   const int* __restrict__ id, int nl, int l, int n,
                                                   Tabs tb, double* __restrict__ Lre,
                                                   double* __restrict__ Lim) {
-  __shared__ double sT[2 * FMM_MAXN * (FMM_MAXN + 1)];  // [side][i][k], padded rows
-  const int rs = n | 1;
-  for (int t = threadIdx.x; t < 2 * n * n; t += blockDim.x) {
-    const int side = t / (n * n), r = (t / n) % n, col = t % n;
-    sT[(side * n + r) * rs + col] = (side ? tb.TR : tb.TL)[r * n + col];
-  }
+  __shared__ double sT[2 * FMM_MAXN * FMM_RS];
+  load_side_tables(sT, tb, n);
   __syncthreads();
   const int lane = threadIdx.x & 15;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -534,20 +653,8 @@ __global__ void __launch_bounds__(256) l2l_kernel(int64_t c0, int64_t c1,
     if (c0 + 2 * w >= c1) break;
     const int64_t c = c0 + 2 * w + ((threadIdx.x >> 4) & 1);
     const bool live = c < c1;
-    const int64_t par = live ? id[(int64_t)(l - 2) * nl + box_leaf[c]] - 1 : 0;
-    const double* T = sT + ((live && (box_key[c] & 1)) ? n * rs : 0);
-    const double pr = (live && lane < n) ? Lre[par * FMM_MAXN + lane] : 0.0;
-    const double pi = (live && lane < n) ? Lim[par * FMM_MAXN + lane] : 0.0;
-    double re = 0.0, im = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double vr = __shfl_sync(0xffffffffu, pr, i, 16);
-      const double vi = __shfl_sync(0xffffffffu, pi, i, 16);
-      if (live && lane < n) {
-        const double t = T[i * rs + lane];
-        re = fma(t, vr, re);
-        im = fma(t, vi, im);
-      }
-    }
+    double re, im;
+    l2l_box(c, live, box_key, box_leaf, id, nl, l, n, sT, Lre, Lim, lane, re, im);
     if (live && lane < n) {
       Lre[c * FMM_MAXN + lane] += re;
       Lim[c * FMM_MAXN + lane] += im;
@@ -806,18 +913,32 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
     }
     SHRK_CUDA(cudaGetLastError());
   }
-  {
+  // K: the deepest level with at most FMM_TOP_BOXES boxes (box counts grow
+  // with the level); levels 2..K run in the single-CTA top kernel.
+  int K = 2;
+  while (K < L && off[K - 1] - off[K - 2] <= FMM_TOP_BOXES) ++K;
+  if (off[K - 1] - off[K - 2] > FMM_TOP_BOXES && K > 2) --K;
+  if (L - 1 >= K) {
     LaunchScope ls("fmm_m2m", s);
-    for (int l = L - 1; l >= 2; --l) {
-      const int64_t b0 = off[l - 2], b1 = off[l - 1], c0 = off[l - 1], c1 = off[l];
-      (void)c0;
+    for (int l = L - 1; l >= K; --l) {
+      const int64_t b0 = off[l - 2], b1 = off[l - 1], c1 = off[l];
       m2m_kernel<<<half_grid(b1 - b0), 256, 0, s>>>(b0, b1, c1, box_key, box_leaf, lid, nl, l, n,
                                                     tb, Wm);
       SHRK_CUDA(cudaGetLastError());
     }
-    add_launches(L - 3);
+    add_launches(L - 1 - K);
   }
-  if (m2l_tc) {
+  {
+    LevelOffs lo{};
+    for (int l = 2; l <= L; ++l) {
+      lo.o[l - 2] = off[l - 2];
+      lo.o[l - 1] = off[l - 1];
+    }
+    LaunchScope ls("fmm_top", s);
+    top_kernel<<<1, FMM_TOP_NT, 0, s>>>(lo, K, box_key, box_leaf, lid, nl, n, tb, Wm, Lre, Lim);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  if (L > K && m2l_tc) {
     static bool opted[64] = {false};
     int dev = 0;
     SHRK_CUDA(cudaGetDevice(&dev));
@@ -826,35 +947,34 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
                                      TC_SMEM));
       opted[dev] = true;
     }
-    LaunchScope ls("fmm_m2l_tc", s);
-    for (int l = 2; l <= L; ++l) {
-      const int64_t b0 = off[l - 2], b1 = off[l - 1];
-      if (b1 > b0)
+    {
+      LaunchScope ls("fmm_m2l_tc", s);
+      for (int l = K + 1; l <= L; ++l) {
+        const int64_t b0 = off[l - 2], b1 = off[l - 1];
         m2l_tc_kernel<<<(unsigned)std::min<int64_t>(blocks(b1 - b0, TC_M), 2 * 148), TC_M,
                         TC_SMEM, s>>>(b0, b1, l, box_key, n, tb, Wm, Lre, Lim,
                                       device_error_word());
-      SHRK_CUDA(cudaGetLastError());
+        SHRK_CUDA(cudaGetLastError());
+      }
+      add_launches(L - K - 1);
     }
-    add_launches(L - 2);
-  } else {
-    LaunchScope ls("fmm_m2l", s);
-    for (int l = 2; l <= L; ++l) {
-      const int64_t b0 = off[l - 2], b1 = off[l - 1];
-      if (b1 > b0)
-        m2l_kernel<<<half_grid(b1 - b0), 256, 0, s>>>(b0, b1, l, box_key, n, tb, Wm, Lre, Lim);
-      SHRK_CUDA(cudaGetLastError());
-    }
-    add_launches(L - 2);
-  }
-  {
     LaunchScope ls("fmm_l2l", s);
-    for (int l = 2; l < L; ++l) {
+    for (int l = K; l < L; ++l) {
       const int64_t c0 = off[l - 1], c1 = off[l];
       l2l_kernel<<<half_grid(c1 - c0), 256, 0, s>>>(c0, c1, box_key, box_leaf, lid, nl, l, n, tb,
                                                     Lre, Lim);
       SHRK_CUDA(cudaGetLastError());
     }
-    add_launches(L - 3);
+    add_launches(L - K - 1);
+  } else if (L > K) {
+    LaunchScope ls("fmm_down", s);
+    for (int l = K + 1; l <= L; ++l) {
+      const int64_t b0 = off[l - 2], b1 = off[l - 1];
+      down_kernel<<<half_grid(b1 - b0), 256, 0, s>>>(b0, b1, l, box_key, box_leaf, lid, nl, n, tb,
+                                                     Wm, Lre, Lim);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    add_launches(L - K - 1);
   }
   {
     LaunchScope ls("fmm_l2p_near", s);
