@@ -80,13 +80,26 @@ __global__ void level_probe_kernel(const double* __restrict__ s, int64_t ns, dou
   if (bits) atomicOr(mask, bits);
 }
 
-__global__ void leaf_flags_kernel(const double* __restrict__ s, int64_t ns, FmmGeom g,
-                                  int* __restrict__ key, int* __restrict__ flag) {
+// The leaf level: the coarsest level l >= 2 whose bit is clear in the probe
+// mask (FMM_LMAX when none is).
+__host__ __device__ __forceinline__ int leaf_level(unsigned mask) {
+  for (int l = 2; l <= FMM_LMAX; ++l)
+    if (!((mask >> l) & 1u)) return l;
+  return FMM_LMAX;
+}
+
+// Leaf key of every source and the start of each run of equal keys; the leaf
+// level comes from the probe mask on the device, so the host reads the mask
+// back together with the leaf count.
+__global__ void leaf_flags_kernel(const double* __restrict__ s, int64_t ns, double a, double W,
+                                  const unsigned* __restrict__ mask, int* __restrict__ key,
+                                  int* __restrict__ flag) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ns) return;
-  const int k = key_at(s[j], g.a, g.W, g.L);
+  const int L = leaf_level(*mask);
+  const int k = key_at(s[j], a, W, L);
   key[j] = k;
-  flag[j] = (j == 0 || key_at(s[j - 1], g.a, g.W, g.L) != k) ? 1 : 0;
+  flag[j] = (j == 0 || key_at(s[j - 1], a, W, L) != k) ? 1 : 0;
 }
 
 // incl = inclusive scan of the run flags: leaf index of source j = incl[j] - 1.
@@ -145,22 +158,28 @@ struct Tabs {
 };
 
 // P2M: one warp per leaf; lanes take the leaf's sources in turn, each
-// accumulating the n Lagrange-basis values of its sources, and a fixed
-// butterfly adds the lanes (deterministic).
+// accumulating the n Lagrange-basis values of its sources (barycentric form,
+// reciprocals by rcp_f64, within an ulp), and a fixed reduce-scatter adds
+// the lanes: 16 shuffles leave the total of node i on lanes 2i and 2i + 1
+// (deterministic).  The node tables sit in shared memory (broadcast reads).
 template <int N>
-__global__ void p2m_kernel(const double* __restrict__ s, const int* __restrict__ leaf_key,
-                           const int* __restrict__ leaf_start, int nl, FmmGeom g, Tabs tb,
-                           int64_t leaf_box0, double* __restrict__ Wm) {
+__global__ void __launch_bounds__(256) p2m_kernel(const double* __restrict__ s,
+                                                  const int* __restrict__ leaf_key,
+                                                  const int* __restrict__ leaf_start, int nl,
+                                                  FmmGeom g, Tabs tb, int64_t leaf_box0,
+                                                  double* __restrict__ Wm) {
+  __shared__ double stau[N], slam[N];
+  if (threadIdx.x < N) {
+    stau[threadIdx.x] = tb.tau[threadIdx.x];
+    slam[threadIdx.x] = tb.lam[threadIdx.x];
+  }
+  __syncthreads();
   const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (k >= nl) return;
-  double tau[N], lam[N], acc[N];
+  if (k >= nl) return;  // whole warps leave together
+  double v[16];
 #pragma unroll
-  for (int j = 0; j < N; ++j) {
-    tau[j] = tb.tau[j];
-    lam[j] = tb.lam[j];
-    acc[j] = 0.0;
-  }
+  for (int i = 0; i < 16; ++i) v[i] = 0.0;
   const double h = g.W / (double)(1LL << g.L);
   const double c = g.a + ((double)leaf_key[k] + 0.5) * h, hh = 0.5 * h;
   for (int j = leaf_start[k] + lane; j < leaf_start[k + 1]; j += 32) {
@@ -169,28 +188,37 @@ __global__ void p2m_kernel(const double* __restrict__ s, const int* __restrict__
     int hit = -1;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const double d = x - tau[i];
+      const double d = x - stau[i];
       if (d == 0.0) hit = i;
-      q[i] = lam[i] / d;
+      q[i] = slam[i] * rcp_f64(d);  // |d| >= one ulp of x unless it is 0
       den += q[i];
     }
     if (hit >= 0) {
 #pragma unroll
       for (int i = 0; i < N; ++i)
-        if (i == hit) acc[i] += 1.0;
+        if (i == hit) v[i] += 1.0;
     } else {
-      const double r = 1.0 / den;
+      const double r = rcp_f64(den);
 #pragma unroll
-      for (int i = 0; i < N; ++i) acc[i] = fma(q[i], r, acc[i]);
+      for (int i = 0; i < N; ++i) v[i] = fma(q[i], r, v[i]);
     }
   }
+  // reduce-scatter: at the step of width m (8, 4, 2, 1) and lane bit b, a
+  // lane keeps the upper or lower m of its 2m partial totals and adds the
+  // partner's copy of them
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    double v = acc[i];
+  for (int m = 8, o = 16; m >= 1; m >>= 1, o >>= 1) {
+    const bool up = (lane & o) != 0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == i) Wm[(leaf_box0 + k) * FMM_MAXN + i] = v;
+    for (int i = 0; i < m; ++i) {
+      const double send = up ? v[i] : v[m + i];
+      const double keep = up ? v[m + i] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
   }
+  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+  const int node = lane >> 1;
+  if (!(lane & 1) && node < N) Wm[(leaf_box0 + k) * FMM_MAXN + node] = v[0];
 }
 
 // The expansion kernels below give each box a half-warp (lane i of the half
@@ -729,9 +757,10 @@ unsigned half_grid(int64_t nb) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, 148 * 4));
 }
 
-// Host tables: first-kind Chebyshev points, barycentric weights, M2M and
-// M2L matrices (double precision, computed here once per call).
-void host_tables(int n, int L, double W, double eta, std::vector<double>& tab) {
+// Host tables: first-kind Chebyshev points, barycentric weights and the
+// M2M / L2L matrices (double precision, computed here once per call; the
+// M2L matrices are made on the device by m2l_tables_kernel).
+void host_tables(int n, std::vector<double>& tab) {
   std::vector<double> tau(n), lam(n);
   for (int j = 0; j < n; ++j) {
     const double th = M_PI * (2.0 * j + 1.0) / (2.0 * n);
@@ -745,8 +774,8 @@ void host_tables(int n, int L, double W, double eta, std::vector<double>& tab) {
     for (int k = 0; k < n; ++k) den += lam[k] / (x - tau[k]);
     return (lam[j] / (x - tau[j])) / den;
   };
-  const size_t nn = (size_t)n * n, nm = (size_t)(FMM_LMAX + 1) * 4 * nn;
-  tab.assign(2 * n + 2 * nn + 2 * nm, 0.0);
+  const size_t nn = (size_t)n * n;
+  tab.assign(2 * n + 2 * nn, 0.0);
   double* T = tab.data();
   std::copy(tau.begin(), tau.end(), T);
   std::copy(lam.begin(), lam.end(), T + n);
@@ -757,21 +786,26 @@ void host_tables(int n, int L, double W, double eta, std::vector<double>& tab) {
       TL[j * n + k] = lag(-0.5 + 0.5 * tau[k], j);
       TR[j * n + k] = lag(0.5 + 0.5 * tau[k], j);
     }
-  double* Mre = TR + nn;
-  double* Mim = Mre + nm;
-  const int offs[4] = {-3, -2, 2, 3};
-  for (int l = 2; l <= L; ++l) {
-    const double hh = 0.5 * W / (double)(1LL << l);
-    for (int oi = 0; oi < 4; ++oi)
-      for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) {
-          const double d = hh * (2.0 * offs[oi] + tau[i] - tau[j]);
-          const double den = d * d + eta * eta;
-          const size_t q = (((size_t)l * 4 + oi) * n + i) * n + j;
-          Mre[q] = d / den;  // 1/(d - i eta) = (d + i eta)/(d^2 + eta^2)
-          Mim[q] = eta / den;
-        }
-  }
+}
+
+// The M2L matrices of levels 2..L on the device (the host uploads only the
+// node tables): Mre + i Mim [l][oi][i][j] = 1/(d - i eta) = (d + i eta) /
+// (d^2 + eta^2), d = (h_l / 2)(2 o + tau_i - tau_j), h_l = W / 2^l.
+__global__ void m2l_tables_kernel(const double* __restrict__ tau, int n, int L, double W,
+                                  double eta, double* __restrict__ Mre,
+                                  double* __restrict__ Mim) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t per = 4LL * n * n;
+  if (t >= (int64_t)(L - 1) * per) return;
+  const int l = 2 + (int)(t / per), r = (int)(t % per);
+  const int oi = r / (n * n), i = (r / n) % n, j = r % n;
+  const int o = oi == 0 ? -3 : (oi == 1 ? -2 : (oi == 2 ? 2 : 3));
+  const double hh = 0.5 * W / (double)(1LL << l);
+  const double d = hh * (2.0 * o + tau[i] - tau[j]);
+  const double den = d * d + eta * eta;
+  const int64_t q = (((int64_t)l * 4 + oi) * n + i) * n + j;
+  Mre[q] = d / den;
+  Mim[q] = eta / den;
 }
 
 }  // namespace
@@ -781,38 +815,17 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
   if (p <= 0) return SHRK_OK;
   const double* ds = nullptr;
   const int* perm = nullptr;
-  SHRK_TRY(sorted_sources_perm(d_ev, p, &ds, &perm, s));
   double ends[2];
-  SHRK_CUDA(cudaMemcpyAsync(&ends[0], ds, sizeof(double), cudaMemcpyDeviceToHost, s));
-  SHRK_CUDA(cudaMemcpyAsync(&ends[1], ds + p - 1, sizeof(double), cudaMemcpyDeviceToHost, s));
-  void* tmp = nullptr;
-  SHRK_TRY(scratch_get(SLOT_TMP, 4096, &tmp));
-  unsigned* d_mask = (unsigned*)tmp;
-  SHRK_CUDA(cudaMemsetAsync(d_mask, 0, sizeof(unsigned), s));
-  SHRK_CUDA(cudaStreamSynchronize(s));
+  SHRK_TRY(sorted_sources_perm(d_ev, p, &ds, &perm, s, &ends[0], &ends[1]));
   FmmGeom g;
   g.a = ends[0];
   g.W = (ends[1] - ends[0]) * (1.0 + 0x1p-20);
   if (!(g.W > 0.0) || !std::isfinite(g.W)) g.W = 1.0;
   g.n = n;
   g.eta = eta;
-  // leaf level: the coarsest with at most FMM_OCC sources per box
-  {
-    LaunchScope ls("fmm_build", s);
-    level_probe_kernel<<<blocks(p, 256), 256, 0, s>>>(ds, p, g.a, g.W, d_mask);
-    SHRK_CUDA(cudaGetLastError());
-  }
-  unsigned mask = 0;
-  SHRK_CUDA(cudaMemcpyAsync(&mask, d_mask, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-  SHRK_CUDA(cudaStreamSynchronize(s));
-  g.L = FMM_LMAX;
-  for (int l = 2; l <= FMM_LMAX; ++l)
-    if (!((mask >> l) & 1u)) {
-      g.L = l;
-      break;
-    }
-  const int L = g.L;
-  // leaves
+  // leaves: keys at the leaf level (the coarsest with at most FMM_OCC
+  // sources per box, found by the probe) and their runs; one read-back for
+  // the probe mask and the leaf count
   void* kw = nullptr;
   SHRK_TRY(scratch_get(SLOT_KEYS, sizeof(int) * 3 * (size_t)p + 256, &kw));
   int* key = (int*)kw;
@@ -824,20 +837,29 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
   SHRK_TRY(scratch_get(SLOT_LEAF, sizeof(int) * (2 * (size_t)p + 2), &lw));
   int* leaf_key = (int*)lw;
   int* leaf_start = leaf_key + p;
-  void* cubt = nullptr;
+  void* tmp = nullptr;
+  SHRK_TRY(scratch_get(SLOT_TMP, 4096 + cub_bytes, &tmp));
+  unsigned* d_mask = (unsigned*)tmp;
+  void* cubt = (char*)tmp + 4096;
+  SHRK_CUDA(cudaMemsetAsync(d_mask, 0, sizeof(unsigned), s));
   {
     LaunchScope ls("fmm_build", s);
-    leaf_flags_kernel<<<blocks(p, 256), 256, 0, s>>>(ds, p, g, key, flag);
+    level_probe_kernel<<<blocks(p, 256), 256, 0, s>>>(ds, p, g.a, g.W, d_mask);
     SHRK_CUDA(cudaGetLastError());
-    SHRK_TRY(scratch_get(SLOT_TMP, 4096 + cub_bytes, &tmp));
-    cubt = (char*)tmp + 4096;
+    leaf_flags_kernel<<<blocks(p, 256), 256, 0, s>>>(ds, p, g.a, g.W, d_mask, key, flag);
+    SHRK_CUDA(cudaGetLastError());
     SHRK_CUDA(cub::DeviceScan::InclusiveSum(cubt, cub_bytes, flag, incl, (int)p, s));
     leaf_compact_kernel<<<blocks(p, 256), 256, 0, s>>>(key, flag, incl, p, leaf_key, leaf_start);
     SHRK_CUDA(cudaGetLastError());
+    add_launches(4);  // five kernels, the scan's two included
   }
+  unsigned mask = 0;
   int nl = 0;
+  SHRK_CUDA(cudaMemcpyAsync(&mask, d_mask, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaMemcpyAsync(&nl, incl + p - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
+  g.L = leaf_level(mask);
+  const int L = g.L;
   // boxes of levels 2..L
   const int64_t nlev = (int64_t)(L - 1) * nl;
   void* vw = nullptr;
@@ -873,12 +895,12 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
   double* Lre = Wm + FMM_MAXN * nbox;
   double* Lim = Lre + FMM_MAXN * nbox;
   std::vector<double> htab;
-  host_tables(n, L, g.W, eta, htab);
+  host_tables(n, htab);
+  const size_t nn = (size_t)n * n, nm = (size_t)(FMM_LMAX + 1) * 4 * nn;
   void* tw = nullptr;
-  SHRK_TRY(scratch_get(SLOT_TAB, sizeof(double) * htab.size(), &tw));
+  SHRK_TRY(scratch_get(SLOT_TAB, sizeof(double) * (htab.size() + 2 * nm), &tw));
   SHRK_CUDA(cudaMemcpyAsync(tw, htab.data(), sizeof(double) * htab.size(), cudaMemcpyHostToDevice,
                             s));
-  const size_t nn = (size_t)n * n, nm = (size_t)(FMM_LMAX + 1) * 4 * nn;
   Tabs tb;
   tb.tau = (const double*)tw;
   tb.lam = tb.tau + n;
@@ -886,6 +908,14 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
   tb.TR = tb.TL + nn;
   tb.Mre = tb.TR + nn;
   tb.Mim = tb.Mre + nm;
+  {
+    LaunchScope ls("fmm_build", s);
+    const int64_t nt = (int64_t)(L - 1) * 4 * n * n;
+    m2l_tables_kernel<<<blocks(nt, 256), 256, 0, s>>>(tb.tau, n, L, g.W, eta,
+                                                      const_cast<double*>(tb.Mre),
+                                                      const_cast<double*>(tb.Mim));
+    SHRK_CUDA(cudaGetLastError());
+  }
   {
     LaunchScope ls("fmm_build", s);
     box_info_kernel<<<blocks(nlev, 256), 256, 0, s>>>(leaf_key, nl, L, lflag, lid, box_key,

@@ -118,9 +118,12 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
 shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sorted,
                            double* first, double* last, cudaStream_t s);
 // The same, plus the permutation: d_sorted[i] = d_src[perm[i]]; *d_perm is
-// null when d_src is already sorted (the identity).
+// null when d_src is already sorted (the identity).  With lo / hi given,
+// also the smallest and largest source (no extra read-back for sorted
+// input).
 shrk_status sorted_sources_perm(const double* d_src, int64_t ns, const double** d_sorted,
-                                const int** d_perm, cudaStream_t s);
+                                const int** d_perm, cudaStream_t s, double* lo = nullptr,
+                                double* hi = nullptr);
 
 // Treecode adjoint (chebcode.cu): the gradient of shrk_stieltjes_adjoint
 // with every source sum evaluated by the ChebCode tree of preset `prm`.

@@ -78,13 +78,15 @@ shrk_status sorted_sources(const double* d_src, int64_t ns, const double** d_sor
 // As sorted_sources, with the source index of every sorted entry (scratch
 // slot 29 holds the identity and the permutation).
 shrk_status sorted_sources_perm(const double* d_src, int64_t ns, const double** d_sorted,
-                                const int** d_perm, cudaStream_t s) {
+                                const int** d_perm, cudaStream_t s, double* lo, double* hi) {
   bool sorted = true;
   double first = 0.0, last = 0.0;
   SHRK_TRY(check_sorted(d_src, ns, &sorted, &first, &last, s));
   *d_perm = nullptr;
   if (sorted) {
     *d_sorted = d_src;
+    if (lo) *lo = first;
+    if (hi) *hi = last;
     return SHRK_OK;
   }
   void* pv = nullptr;
@@ -108,6 +110,15 @@ shrk_status sorted_sources_perm(const double* d_src, int64_t ns, const double** 
   }
   *d_sorted = (const double*)out;
   *d_perm = perm;
+  if (lo || hi) {
+    double ends[2];
+    SHRK_CUDA(cudaMemcpyAsync(&ends[0], out, sizeof(double), cudaMemcpyDeviceToHost, s));
+    SHRK_CUDA(cudaMemcpyAsync(&ends[1], (const double*)out + (ns - 1), sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    SHRK_CUDA(cudaStreamSynchronize(s));
+    if (lo) *lo = ends[0];
+    if (hi) *hi = ends[1];
+  }
   return SHRK_OK;
 }
 
