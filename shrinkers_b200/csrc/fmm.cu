@@ -690,7 +690,8 @@ __global__ void __launch_bounds__(256) l2l_kernel(int64_t c0, int64_t c1,
   }
 }
 
-// L2P + near field: one thread per (sorted) target.
+// L2P + near field: one thread per (sorted) target; reciprocals by rcp_f64
+// (within an ulp).
 __global__ void l2p_near_kernel(const double* __restrict__ s, int64_t ns,
                                 const int* __restrict__ leaf_of, const int* __restrict__ leaf_key,
                                 const int* __restrict__ leaf_start, int nl, FmmGeom g, Tabs tb,
@@ -717,7 +718,7 @@ __global__ void l2p_near_kernel(const double* __restrict__ s, int64_t ns,
       hit = i;
       break;
     }
-    const double q = tb.lam[i] / d;
+    const double q = tb.lam[i] * rcp_f64(d);  // |d| >= one ulp of xp
     num_r = fma(q, lr[i], num_r);
     num_i = fma(q, li[i], num_i);
     den += q;
@@ -727,8 +728,9 @@ __global__ void l2p_near_kernel(const double* __restrict__ s, int64_t ns,
     re = lr[hit];
     im = li[hit];
   } else {
-    re = num_r / den;
-    im = num_i / den;
+    const double r = rcp_f64(den);
+    re = num_r * r;
+    im = num_i * r;
   }
   // near field: this leaf and the adjacent ones
   const int ka = (k > 0 && leaf_key[k - 1] == key - 1) ? k - 1 : k;
@@ -737,7 +739,7 @@ __global__ void l2p_near_kernel(const double* __restrict__ s, int64_t ns,
   double nr = 0.0, ni = 0.0;
   for (int j = leaf_start[ka]; j < leaf_start[kz + 1]; ++j) {
     const double d = x - s[j];
-    const double inv = 1.0 / fma(d, d, eta2);
+    const double inv = rcp_f64(fma(d, d, eta2));
     nr = fma(d, inv, nr);
     ni += inv;
   }
