@@ -360,32 +360,106 @@ __global__ void __launch_bounds__(256) m2m_kernel(int64_t b0, int64_t b1, int64_
 
 // Downward pass of level l (boxes [b0, b1)), M2L and L2L in one launch:
 // L_b = M2L(partners) + T^T L_parent (the parent's L is complete: levels run
-// in order).  Level 2 has no parent term.
-__global__ void __launch_bounds__(256) down_kernel(int64_t b0, int64_t b1, int l,
-                                                   const int* __restrict__ box_key,
-                                                   const int* __restrict__ box_leaf,
-                                                   const int* __restrict__ id, int nl, int n,
-                                                   Tabs tb, const double* __restrict__ Wm,
-                                                   double* __restrict__ Lre,
-                                                   double* __restrict__ Lim) {
-  __shared__ double sre[4 * FMM_MAXN * FMM_RS], sim[4 * FMM_MAXN * FMM_RS];
-  __shared__ double sT[2 * FMM_MAXN * FMM_RS];
-  load_m2l_tables(sre, sim, tb, l, n);
-  load_side_tables(sT, tb, n);
-  __syncthreads();
-  const int lane = threadIdx.x & 15;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
-    if (b0 + 2 * w >= b1) break;
-    const int64_t b = b0 + 2 * w + ((threadIdx.x >> 4) & 1);
-    const bool live = b < b1;
-    double re, im, pr = 0.0, pi = 0.0;
-    m2l_box(b, live, b0, b1, box_key, n, sre, sim, Wm, lane, re, im);
-    if (l > 2) l2l_box(b, live, box_key, box_leaf, id, nl, l - 1, n, sT, Lre, Lim, lane, pr, pi);
-    if (live && lane < n) {
-      Lre[b * FMM_MAXN + lane] = re + pr;
-      Lim[b * FMM_MAXN + lane] = im + pi;
+// in order; level 2 has no parent term).  A CTA takes tiles of DT_BOXES
+// consecutive boxes; their partners lie within 3 positions, so the tile's
+// multipole window and keys are staged in shared memory with coalesced
+// loads.  Thread (box, g) computes nodes 4g..4g+3 of its box: 8 independent
+// FP64 accumulators, operands read as shared-memory broadcasts.  The table
+// blocks of the four offsets (and of the two sides) are padded by one double
+// so that the offsets and sides met within a warp fall in different banks.
+constexpr int DT_BOXES = 64, DT_NT = 256, DT_WIN = DT_BOXES + 6;
+constexpr int DT_MS = FMM_MAXN * FMM_RS + 1;  // one offset's (or side's) block
+
+__global__ void __launch_bounds__(DT_NT) down_kernel(int64_t b0, int64_t b1, int l,
+                                                     const int* __restrict__ box_key,
+                                                     const int* __restrict__ box_leaf,
+                                                     const int* __restrict__ id, int nl, int n,
+                                                     Tabs tb, const double* __restrict__ Wm,
+                                                     double* __restrict__ Lre,
+                                                     double* __restrict__ Lim) {
+  __shared__ double sre[4 * DT_MS], sim[4 * DT_MS], sT[2 * DT_MS];
+  __shared__ double sW[DT_WIN * FMM_RS];
+  __shared__ int skey[DT_WIN];
+  {
+    const int nn = n * n;
+    const double* mr = tb.Mre + (int64_t)l * 4 * nn;
+    const double* mi = tb.Mim + (int64_t)l * 4 * nn;
+    for (int t = threadIdx.x; t < 4 * nn; t += DT_NT) {
+      const int oi = t / nn, i = (t / n) % n, j = t % n;
+      sre[oi * DT_MS + i * FMM_RS + j] = mr[t];
+      sim[oi * DT_MS + i * FMM_RS + j] = mi[t];
     }
+    for (int t = threadIdx.x; t < 2 * nn; t += DT_NT) {
+      const int side = t / nn, i = (t / n) % n, j = t % n;
+      sT[side * DT_MS + i * FMM_RS + j] = (side ? tb.TR : tb.TL)[i * n + j];
+    }
+  }
+  const int bl = threadIdx.x >> 2, g4 = (threadIdx.x & 3) * 4;
+  for (int64_t tile = blockIdx.x; b0 + tile * DT_BOXES < b1; tile += gridDim.x) {
+    const int64_t tb0 = b0 + tile * DT_BOXES;
+    const int64_t r0 = tb0 - 3 > b0 ? tb0 - 3 : b0;
+    const int64_t r1 = tb0 + DT_BOXES + 3 < b1 ? tb0 + DT_BOXES + 3 : b1;
+    const int rows = (int)(r1 - r0);
+    __syncthreads();  // the previous tile is done with sW / skey (and tables loaded)
+    for (int q = threadIdx.x; q < rows * FMM_MAXN; q += DT_NT) {
+      const int r = q / FMM_MAXN, j = q % FMM_MAXN;
+      sW[r * FMM_RS + j] = j < n ? Wm[(r0 + r) * FMM_MAXN + j] : 0.0;
+    }
+    for (int r = threadIdx.x; r < rows; r += DT_NT) skey[r] = box_key[r0 + r];
+    __syncthreads();
+    const int64_t b = tb0 + bl;
+    if (b >= b1) continue;
+    double re[4] = {0.0, 0.0, 0.0, 0.0}, im[4] = {0.0, 0.0, 0.0, 0.0};
+    const int kb = skey[b - r0];
+    const int odd = kb & 1;
+    for (int q = 0; q < 3; ++q) {
+      // even kb: sources at kb-2, kb+2, kb+3 (o = 2, -2, -3); odd: kb-3, kb-2, kb+2
+      const int o = odd ? (q == 0 ? 3 : (q == 1 ? 2 : -2)) : (q == 0 ? 2 : (q == 1 ? -2 : -3));
+      const int ka = kb - o;
+      int ar = -1;  // the partner's row in the window
+      if (ka >= 0) {
+#pragma unroll
+        for (int t = 1; t <= 3; ++t) {
+          const int64_t f = o > 0 ? b - t : b + t;
+          if (ar < 0 && f >= b0 && f < b1 && skey[f - r0] == ka) ar = (int)(f - r0);
+        }
+      }
+      if (ar < 0) continue;
+      const int oi = o == -3 ? 0 : (o == -2 ? 1 : (o == 2 ? 2 : 3));
+      const double* w = sW + ar * FMM_RS;
+      const double* mr = sre + oi * DT_MS + g4 * FMM_RS;
+      const double* mi = sim + oi * DT_MS + g4 * FMM_RS;
+      for (int j = 0; j < n; ++j) {
+        const double v = w[j];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          re[u] = fma(mr[u * FMM_RS + j], v, re[u]);
+          im[u] = fma(mi[u * FMM_RS + j], v, im[u]);
+        }
+      }
+    }
+    if (l > 2) {
+      // L2L: child node v = g4 + u gets sum_i T_side[i][v] L_parent[i]
+      const int64_t par = id[(int64_t)(l - 1 - 2) * nl + box_leaf[b]] - 1;
+      const double* T = sT + (kb & 1) * DT_MS + g4;
+      const double* pr = Lre + par * FMM_MAXN;
+      const double* pi = Lim + par * FMM_MAXN;
+      for (int i = 0; i < n; ++i) {
+        const double vr = pr[i], vi = pi[i];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double t = T[i * FMM_RS + u];
+          re[u] = fma(t, vr, re[u]);
+          im[u] = fma(t, vi, im[u]);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (g4 + u < n) {
+        Lre[b * FMM_MAXN + g4 + u] = re[u];
+        Lim[b * FMM_MAXN + g4 + u] = im[u];
+      }
   }
 }
 
@@ -1002,8 +1076,8 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
     LaunchScope ls("fmm_down", s);
     for (int l = K + 1; l <= L; ++l) {
       const int64_t b0 = off[l - 2], b1 = off[l - 1];
-      down_kernel<<<half_grid(b1 - b0), 256, 0, s>>>(b0, b1, l, box_key, box_leaf, lid, nl, n, tb,
-                                                     Wm, Lre, Lim);
+      down_kernel<<<(unsigned)std::min<int64_t>(blocks(b1 - b0, DT_BOXES), 148 * 4), DT_NT, 0,
+                    s>>>(b0, b1, l, box_key, box_leaf, lid, nl, n, tb, Wm, Lre, Lim);
       SHRK_CUDA(cudaGetLastError());
     }
     add_launches(L - K - 1);
