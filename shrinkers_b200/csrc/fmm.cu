@@ -363,22 +363,29 @@ __global__ void __launch_bounds__(256) m2m_kernel(int64_t b0, int64_t b1, int64_
 // in order; level 2 has no parent term).  A CTA takes tiles of DT_BOXES
 // consecutive boxes; their partners lie within 3 positions, so the tile's
 // multipole window and keys are staged in shared memory with coalesced
-// loads.  Thread (box, g) computes nodes 4g..4g+3 of its box: 8 independent
-// FP64 accumulators, operands read as shared-memory broadcasts.  The table
-// blocks of the four offsets (and of the two sides) are padded by one double
-// so that the offsets and sides met within a warp fall in different banks.
+// loads.  Thread (box, g) computes nodes g, g+4, g+8, g+12 of its box: 8
+// independent FP64 accumulators.  The kernel is bound by shared-memory
+// wavefronts, so the M2L matrices are stored as {re, im} pairs (one 16-byte
+// load feeds two FMAs) and the window is read two nodes at a time.  Strides
+// (in 16-byte units: rows 17, offset blocks 276 = 4 mod 8; window rows 18
+// doubles; side blocks 276 doubles) put the 8 distinct addresses a warp
+// reads at once -- 4 node rows x the 2 offsets of even and odd boxes, or x
+// the 2 sides -- in 8 different bank groups.
 constexpr int DT_BOXES = 64, DT_NT = 256, DT_WIN = DT_BOXES + 6;
-constexpr int DT_MS = FMM_MAXN * FMM_RS + 1;  // one offset's (or side's) block
+constexpr int DT_RS = FMM_MAXN + 1;        // matrix row stride (entries)
+constexpr int DT_MS = FMM_MAXN * DT_RS + 4;  // offset / side block stride
+constexpr int DT_WS = FMM_MAXN + 2;        // window row stride (doubles)
 
-__global__ void __launch_bounds__(DT_NT) down_kernel(int64_t b0, int64_t b1, int l,
+__global__ void __launch_bounds__(DT_NT, 2) down_kernel(int64_t b0, int64_t b1, int l,
                                                      const int* __restrict__ box_key,
                                                      const int* __restrict__ box_leaf,
                                                      const int* __restrict__ id, int nl, int n,
                                                      Tabs tb, const double* __restrict__ Wm,
                                                      double* __restrict__ Lre,
                                                      double* __restrict__ Lim) {
-  __shared__ double sre[4 * DT_MS], sim[4 * DT_MS], sT[2 * DT_MS];
-  __shared__ double sW[DT_WIN * FMM_RS];
+  __shared__ double2 sM[4 * DT_MS];  // [oi][i][j] = {re, im}
+  __shared__ double sT[2 * DT_MS];   // [side][i][v]
+  __shared__ __align__(16) double sW[DT_WIN * DT_WS];
   __shared__ int skey[DT_WIN];
   {
     const int nn = n * n;
@@ -386,15 +393,15 @@ __global__ void __launch_bounds__(DT_NT) down_kernel(int64_t b0, int64_t b1, int
     const double* mi = tb.Mim + (int64_t)l * 4 * nn;
     for (int t = threadIdx.x; t < 4 * nn; t += DT_NT) {
       const int oi = t / nn, i = (t / n) % n, j = t % n;
-      sre[oi * DT_MS + i * FMM_RS + j] = mr[t];
-      sim[oi * DT_MS + i * FMM_RS + j] = mi[t];
+      sM[oi * DT_MS + i * DT_RS + j] = make_double2(mr[t], mi[t]);
     }
     for (int t = threadIdx.x; t < 2 * nn; t += DT_NT) {
       const int side = t / nn, i = (t / n) % n, j = t % n;
-      sT[side * DT_MS + i * FMM_RS + j] = (side ? tb.TR : tb.TL)[i * n + j];
+      sT[side * DT_MS + i * DT_RS + j] = (side ? tb.TR : tb.TL)[i * n + j];
     }
   }
-  const int bl = threadIdx.x >> 2, g4 = (threadIdx.x & 3) * 4;
+  const int bl = threadIdx.x >> 2, g = threadIdx.x & 3;
+  const int ne = (n + 1) & ~1;  // nodes read in pairs; the window is zero above n
   for (int64_t tile = blockIdx.x; b0 + tile * DT_BOXES < b1; tile += gridDim.x) {
     const int64_t tb0 = b0 + tile * DT_BOXES;
     const int64_t r0 = tb0 - 3 > b0 ? tb0 - 3 : b0;
@@ -403,7 +410,7 @@ __global__ void __launch_bounds__(DT_NT) down_kernel(int64_t b0, int64_t b1, int
     __syncthreads();  // the previous tile is done with sW / skey (and tables loaded)
     for (int q = threadIdx.x; q < rows * FMM_MAXN; q += DT_NT) {
       const int r = q / FMM_MAXN, j = q % FMM_MAXN;
-      sW[r * FMM_RS + j] = j < n ? Wm[(r0 + r) * FMM_MAXN + j] : 0.0;
+      sW[r * DT_WS + j] = j < n ? Wm[(r0 + r) * FMM_MAXN + j] : 0.0;
     }
     for (int r = threadIdx.x; r < rows; r += DT_NT) skey[r] = box_key[r0 + r];
     __syncthreads();
@@ -426,29 +433,29 @@ __global__ void __launch_bounds__(DT_NT) down_kernel(int64_t b0, int64_t b1, int
       }
       if (ar < 0) continue;
       const int oi = o == -3 ? 0 : (o == -2 ? 1 : (o == 2 ? 2 : 3));
-      const double* w = sW + ar * FMM_RS;
-      const double* mr = sre + oi * DT_MS + g4 * FMM_RS;
-      const double* mi = sim + oi * DT_MS + g4 * FMM_RS;
-      for (int j = 0; j < n; ++j) {
-        const double v = w[j];
+      const double2* w2 = reinterpret_cast<const double2*>(sW + ar * DT_WS);
+      const double2* m = sM + oi * DT_MS + g * DT_RS;
+      for (int j = 0; j < ne; j += 2) {
+        const double2 v = w2[j >> 1];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          re[u] = fma(mr[u * FMM_RS + j], v, re[u]);
-          im[u] = fma(mi[u * FMM_RS + j], v, im[u]);
+          const double2 c0 = m[4 * u * DT_RS + j], c1 = m[4 * u * DT_RS + j + 1];
+          re[u] = fma(c1.x, v.y, fma(c0.x, v.x, re[u]));
+          im[u] = fma(c1.y, v.y, fma(c0.y, v.x, im[u]));
         }
       }
     }
     if (l > 2) {
-      // L2L: child node v = g4 + u gets sum_i T_side[i][v] L_parent[i]
+      // L2L: child node v gets sum_i T_side[i][v] L_parent[i]
       const int64_t par = id[(int64_t)(l - 1 - 2) * nl + box_leaf[b]] - 1;
-      const double* T = sT + (kb & 1) * DT_MS + g4;
+      const double* T = sT + (kb & 1) * DT_MS + g;
       const double* pr = Lre + par * FMM_MAXN;
       const double* pi = Lim + par * FMM_MAXN;
       for (int i = 0; i < n; ++i) {
         const double vr = pr[i], vi = pi[i];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const double t = T[i * FMM_RS + u];
+          const double t = T[i * DT_RS + 4 * u];
           re[u] = fma(t, vr, re[u]);
           im[u] = fma(t, vi, im[u]);
         }
@@ -456,9 +463,9 @@ __global__ void __launch_bounds__(DT_NT) down_kernel(int64_t b0, int64_t b1, int
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u)
-      if (g4 + u < n) {
-        Lre[b * FMM_MAXN + g4 + u] = re[u];
-        Lim[b * FMM_MAXN + g4 + u] = im[u];
+      if (g + 4 * u < n) {
+        Lre[b * FMM_MAXN + g + 4 * u] = re[u];
+        Lim[b * FMM_MAXN + g + 4 * u] = im[u];
       }
   }
 }
