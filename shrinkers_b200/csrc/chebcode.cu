@@ -234,6 +234,10 @@ struct DevTreeF64 {
   int n;
 };
 
+// Up to this many queries the evaluation takes a warp per query (a thread per
+// query leaves most of the GPU idle and each traversal serial).
+constexpr int64_t CHEB_WARP_NQ = 16384;
+
 struct EvalArgs {
   const double* q;
   int64_t nq;
@@ -270,10 +274,59 @@ __device__ __forceinline__ void leaf_sum(const double* xs, int64_t len, double x
   li_out = li;
 }
 
-// chebcode.rs:607-711 contribution_f64.
+// The same leaf sum with a warp per query (every lane holds the same x):
+// lane l computes the terms of sources base + l in parallel, then every lane
+// adds them in the sequential order through shuffles -- the two chains of
+// the F64x2 schedule, their sum, then the odd tail -- so the result equals
+// leaf_sum bit for bit.  Used when there are too few queries to fill the GPU
+// with one thread each (the reciprocals dominate, the ordered adds are cheap).
+__device__ __forceinline__ void leaf_sum_warp(const double* xs, int64_t len, double x,
+                                              double eta2, int lane, double& lr_out,
+                                              double& li_out) {
+  double ar0 = 0.0, ar1 = 0.0, ai0 = 0.0, ai1 = 0.0, tr = 0.0, ti = 0.0;
+  const int64_t pair_end = len & ~(int64_t)1;
+  for (int64_t base = 0; base < len; base += 32) {
+    const int64_t k = base + lane;
+    double vr = 0.0, vi = 0.0;
+    if (k < len) {
+      const double d = x - xs[k];
+      const double inv = __drcp_rn(eta2 + d * d);  // = d * d + eta2 for the tail
+      vr = d * inv;
+      vi = inv;
+    }
+    const int cnt = (int)min((int64_t)32, len - base);
+    for (int j = 0; j < cnt; ++j) {
+      const double r = __shfl_sync(0xffffffffu, vr, j), i = __shfl_sync(0xffffffffu, vi, j);
+      const int64_t kk = base + j;
+      if (kk >= pair_end) {
+        tr = r;
+        ti = i;
+      } else if (kk & 1) {
+        ar1 = ar1 + r;
+        ai1 = ai1 + i;
+      } else {
+        ar0 = ar0 + r;
+        ai0 = ai0 + i;
+      }
+    }
+  }
+  double lr = ar0 + ar1, li = ai0 + ai1;
+  if (len & 1) {
+    lr += tr;
+    li += ti;
+  }
+  lr_out = lr;
+  li_out = li;
+}
+
+// chebcode.rs:607-711 contribution_f64.  WARP: a warp per query (all lanes
+// walk the same nodes; leaf sums by leaf_sum_warp; lane 0 stores).
+template <bool WARP>
 __global__ void __launch_bounds__(128) cheb_eval_f64(const EvalArgs a) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.nq) return;
+  const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = WARP ? gt >> 5 : gt;
+  const int lane = WARP ? (int)(threadIdx.x & 31) : 0;
+  if (t >= a.nq) return;  // WARP: whole warps leave together
   const DevTreeF64& T = a.t;
   const int n = T.n;
   const double x = a.q[t], eta = a.eta, eta2 = eta * eta;
@@ -287,7 +340,8 @@ __global__ void __launch_bounds__(128) cheb_eval_f64(const EvalArgs a) {
     if (rt < 0) {
       double lr, li;
       const int64_t l0 = T.lo_idx[node];
-      leaf_sum(a.sorted + l0, T.hi_idx[node] - l0, x, eta2, lr, li);
+      if (WARP) leaf_sum_warp(a.sorted + l0, T.hi_idx[node] - l0, x, eta2, lane, lr, li);
+      else leaf_sum(a.sorted + l0, T.hi_idx[node] - l0, x, eta2, lr, li);
       re += lr;
       im += eta * li;
       continue;
@@ -327,13 +381,16 @@ __global__ void __launch_bounds__(128) cheb_eval_f64(const EvalArgs a) {
       stack[top++] = node + 1;
     }
   }
-  epi_store(a.epi, t, x, re, im);
+  if (lane == 0) epi_store(a.epi, t, x, re, im);
 }
 
-// chebcode.rs:722-828 contribution_fast32.
+// chebcode.rs:722-828 contribution_fast32.  WARP as cheb_eval_f64.
+template <bool WARP>
 __global__ void __launch_bounds__(128) cheb_eval_f32(const EvalArgs a) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.nq) return;
+  const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = WARP ? gt >> 5 : gt;
+  const int lane = WARP ? (int)(threadIdx.x & 31) : 0;
+  if (t >= a.nq) return;  // WARP: whole warps leave together
   const int n = a.t.n;
   const double lambda = a.q[t], eta = a.eta, eta2d = eta * eta;
   const float x = (float)lambda, e32 = (float)eta, eta2 = e32 * e32;
@@ -347,7 +404,11 @@ __global__ void __launch_bounds__(128) cheb_eval_f32(const EvalArgs a) {
     const NodeF32 nd = a.nf[node];
     if (nd.right < 0) {
       double lr, li;
-      leaf_sum(a.sorted + nd.lo_idx, (int64_t)(nd.hi_idx - nd.lo_idx), lambda, eta2d, lr, li);
+      if (WARP)
+        leaf_sum_warp(a.sorted + nd.lo_idx, (int64_t)(nd.hi_idx - nd.lo_idx), lambda, eta2d,
+                      lane, lr, li);
+      else
+        leaf_sum(a.sorted + nd.lo_idx, (int64_t)(nd.hi_idx - nd.lo_idx), lambda, eta2d, lr, li);
       leaf_re += lr;
       leaf_im += eta * li;
       continue;
@@ -394,7 +455,7 @@ __global__ void __launch_bounds__(128) cheb_eval_f32(const EvalArgs a) {
   }
   const float hr = (fre[0] + fre[1]) + (fre[2] + fre[3]);
   const float hi = (fim[0] + fim[1]) + (fim[2] + fim[3]);
-  epi_store(a.epi, t, lambda, leaf_re + (double)hr, leaf_im + eta * (double)hi);
+  if (lane == 0) epi_store(a.epi, t, lambda, leaf_re + (double)hr, leaf_im + eta * (double)hi);
 }
 
 __global__ void tree_init_kernel(BuildArrays b, int64_t ns) {
@@ -787,7 +848,8 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     a.t.nodes = f.nodes;
     a.t.w = f.w;
     LaunchScope ls("cheb_eval_f64", s);
-    cheb_eval_f64<<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
+    if (nq <= CHEB_WARP_NQ) cheb_eval_f64<true><<<(unsigned)((nq * 32 + 127) / 128), 128, 0, s>>>(a);
+    else cheb_eval_f64<false><<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   } else {
     void* q = nullptr;
@@ -803,7 +865,8 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     a.nf = nf;
     a.panel = panel;
     LaunchScope ls("cheb_eval_f32", s);
-    cheb_eval_f32<<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
+    if (nq <= CHEB_WARP_NQ) cheb_eval_f32<true><<<(unsigned)((nq * 32 + 127) / 128), 128, 0, s>>>(a);
+    else cheb_eval_f32<false><<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   }
   return SHRK_OK;

@@ -58,7 +58,8 @@ template <bool MIXED, int R>
 __device__ __forceinline__ bool pair_item(const PairItem& a, PairStage& st, uint32_t& phase,
                                           uint32_t& pending) {
   constexpr int NT = PAIR_NT, CH = PAIR_CH, FOLD = PAIR_FOLD;
-  constexpr int WT = 32 * R, R2 = R / 2;
+  static_assert(!MIXED || R % 2 == 0, "the packed far field takes targets in pairs");
+  constexpr int WT = 32 * R, R2 = R / 2 > 0 ? R / 2 : 1;  // R2: packed pairs (MIXED only)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double eta = a.eta, eta2 = eta * eta;
   const float eta2f = (float)eta2;

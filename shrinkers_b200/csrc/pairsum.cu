@@ -47,6 +47,8 @@ constexpr int NT = PAIR_NT;
 constexpr int CH = PAIR_CH;
 constexpr int R_F64 = 4;
 constexpr int R_MIXED = SHRK_R_MIXED;
+constexpr int R_SMALL_F64 = 1;    // targets per thread below one full tile
+constexpr int R_SMALL_MIXED = 2;  // the packed far field takes target pairs
 
 double g_near_k = SHRK_NEAR_K;
 
@@ -60,7 +62,7 @@ struct PairArgs {
   double near_dist;
   int64_t n_tiles;
   int n_splits;
-  int64_t split_len;       // multiple of CH
+  int64_t split_len;       // multiple of CH (of SUB below one full tile)
   double* part_re;         // [n_splits][nt]
   double* part_im;
   int* err;
@@ -200,8 +202,15 @@ shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src
     return SHRK_EINVAL;
   }
   const bool mixed = (precision == SHRK_PREC_MIXED);
-  const int R = mixed ? R_MIXED : R_F64;
-  const SplitPlan pl = plan_splits(nt, ns, NT * R, CH, mixed ? SHRK_MIXED_CTAS : 2);
+  // Fewer targets than one full tile (a query grid, a small spectrum): the
+  // 4-target tiles would leave most of each thread's work on padding and the
+  // 1024-source splits would put the whole sum on a few CTAs, so such calls
+  // take R_SMALL targets per thread and splits of SUB sources (plain loads,
+  // still aligned to the mixed kernel's source blocks).
+  const bool small = nt < (int64_t)NT * (mixed ? R_MIXED : R_F64);
+  const int R = small ? (mixed ? R_SMALL_MIXED : R_SMALL_F64) : (mixed ? R_MIXED : R_F64);
+  const SplitPlan pl =
+      plan_splits(nt, ns, NT * R, small ? SUB : CH, mixed ? SHRK_MIXED_CTAS : 2);
   void* part = nullptr;
   SHRK_TRY(scratch_get(0, sizeof(double) * 2 * (size_t)pl.n_splits * (size_t)nt, &part));
   double2* bounds = nullptr;
@@ -229,7 +238,9 @@ shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src
   a.use_tma = ((uintptr_t)d_src % 16 == 0) ? 1 : 0;
   {
     LaunchScope ls(mixed ? "pair_sum_mixed" : "pair_sum_f64", s);
-    if (mixed) pair_sum_kernel<true, R_MIXED><<<pl.grid, NT, 0, s>>>(a);
+    if (mixed && small) pair_sum_kernel<true, R_SMALL_MIXED><<<pl.grid, NT, 0, s>>>(a);
+    else if (mixed) pair_sum_kernel<true, R_MIXED><<<pl.grid, NT, 0, s>>>(a);
+    else if (small) pair_sum_kernel<false, R_SMALL_F64><<<pl.grid, NT, 0, s>>>(a);
     else pair_sum_kernel<false, R_F64><<<pl.grid, NT, 0, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   }
