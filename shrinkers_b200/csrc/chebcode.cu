@@ -142,10 +142,9 @@ struct FlatTree {
   double* w;      // [nn][n]
 };
 
-__global__ void tree_fill_kernel(const double* __restrict__ sorted, BuildArrays b, int nn,
-                                 FlatTree f, ChebConsts k, double theta_sq) {
-  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= nn) return;
+__device__ __forceinline__ void tree_fill_node(const double* __restrict__ sorted,
+                                               const BuildArrays& b, int i, const FlatTree& f,
+                                               const ChebConsts& k, double theta_sq) {
   const int idx = b.pre[i];
   const int64_t lo_idx = b.blo[i], hi_idx = b.bhi[i];
   const double lo = sorted[lo_idx], hi = sorted[hi_idx - 1];
@@ -158,6 +157,114 @@ __global__ void tree_fill_kernel(const double* __restrict__ sorted, BuildArrays 
   f.right[idx] = b.lc[i] < 0 ? -1 : b.pre[b.rc[i]];
   const double c = 0.5 * (lo + hi), l = 0.5 * (hi - lo);
   for (int j = 0; j < k.n; ++j) f.nodes[(int64_t)idx * k.n + j] = c + l * k.sm1[j];
+}
+
+__global__ void tree_fill_kernel(const double* __restrict__ sorted, BuildArrays b, int nn,
+                                 FlatTree f, ChebConsts k, double theta_sq) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= nn) return;
+  tree_fill_node(sorted, b, i, f, k, theta_sq);
+}
+
+// The topology of a small tree in one CTA (no launch or read-back per
+// level): splits level by level with a barrier between levels, subtree sizes
+// bottom-up, pre-order indices top-down, the flat arrays.  A warp splits a
+// node: its upper_bound of mid probes 32 evenly spaced positions per step
+// (the range shrinks 33-fold), then scans the last <= 32 -- the same index as
+// tree_split_node's binary search, so the tree is identical.  The levels
+// table is left for the host to read once.
+__device__ __forceinline__ void tree_split_node_warp(const double* __restrict__ sorted,
+                                                     BuildArrays b, int i, int depth,
+                                                     int64_t leaf_cap, int lane) {
+  const int64_t lo_idx = b.blo[i], hi_idx = b.bhi[i];
+  if (hi_idx - lo_idx <= leaf_cap || depth >= MAX_TREE_DEPTH) {
+    if (lane == 0) b.lc[i] = b.rc[i] = -1;
+    return;
+  }
+  const double lo = sorted[lo_idx], hi = sorted[hi_idx - 1];
+  const double mid = lo + 0.5 * (hi - lo);
+  // invariant: sorted[< a] <= mid, sorted[>= e] > mid (or e = hi_idx)
+  int64_t a = lo_idx, e = hi_idx;
+  while (e - a > 32) {
+    const int64_t span = e - a;
+    const int64_t pos = a + span * (lane + 1) / 33;  // strictly increasing, in [a, e)
+    const unsigned gt = __ballot_sync(0xffffffffu, mid < sorted[pos]);
+    if (gt) {
+      const int f = __ffs(gt) - 1;  // first probe above mid
+      const int64_t pf = a + span * (f + 1) / 33, pprev = a + span * f / 33;
+      if (f > 0) a = pprev + 1;  // probe f - 1 was <= mid
+      e = pf;
+    } else {
+      a = a + span * 32 / 33 + 1;
+    }
+  }
+  const unsigned gt = __ballot_sync(0xffffffffu, a + lane < e && mid < sorted[a + lane]);
+  int64_t split = gt ? a + (__ffs(gt) - 1) : e;
+  if (split == lo_idx || split == hi_idx) split = (lo_idx + hi_idx) / 2;
+  if (lane == 0) {
+    const int slot = atomicAdd(b.counter, 2);
+    b.blo[slot] = lo_idx;
+    b.bhi[slot] = split;
+    b.blo[slot + 1] = split;
+    b.bhi[slot + 1] = hi_idx;
+    b.lc[i] = slot;
+    b.rc[i] = slot + 1;
+  }
+}
+
+constexpr int TOPO_NT = 1024;
+// Trees of at most this many leaf-capacities of sources (ns / leaf_cap) are
+// built by tree_topology_cta_kernel: a few hundred to ~2 000 nodes, where one
+// CTA beats two launches per level (a query-grid tree, a small spectrum).
+constexpr int64_t SMALL_TREE_LEAVES = 512;
+
+__global__ void __launch_bounds__(TOPO_NT) tree_topology_cta_kernel(
+    const double* __restrict__ sorted, BuildArrays b, int64_t ns, int64_t leaf_cap, FlatTree f,
+    ChebConsts k, double theta_sq) {
+  constexpr int NLEV = MAX_TREE_DEPTH + 2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = TOPO_NT / 32;
+  if (tid == 0) {
+    b.blo[0] = 0;
+    b.bhi[0] = ns;
+    b.pre[0] = 0;
+    *b.counter = 1;
+    b.levels[0] = 0;
+    b.levels[1] = 1;
+  }
+  __syncthreads();
+  int last = NLEV - 1;  // first empty level
+  for (int depth = 0; depth < NLEV - 1; ++depth) {
+    const int begin = b.levels[2 * depth], end = b.levels[2 * depth + 1];
+    if (begin == end) {
+      last = depth;
+      break;
+    }
+    for (int i = begin + warp; i < end; i += nw)
+      tree_split_node_warp(sorted, b, i, depth, leaf_cap, lane);
+    __syncthreads();
+    if (tid == 0) {
+      b.levels[2 * depth + 2] = end;
+      b.levels[2 * depth + 3] = *b.counter;
+    }
+    __syncthreads();
+  }
+  for (int L = last - 1; L >= 0; --L) {
+    const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
+    for (int i = begin + tid; i < end; i += TOPO_NT)
+      b.size[i] = b.lc[i] < 0 ? 1 : 1 + b.size[b.lc[i]] + b.size[b.rc[i]];
+    __syncthreads();
+  }
+  for (int L = 0; L < last; ++L) {
+    const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
+    for (int i = begin + tid; i < end; i += TOPO_NT)
+      if (b.lc[i] >= 0) {
+        b.pre[b.lc[i]] = b.pre[i] + 1;
+        b.pre[b.rc[i]] = b.pre[i] + 1 + b.size[b.lc[i]];
+      }
+    __syncthreads();
+  }
+  const int nn = b.levels[2 * last - 1];
+  for (int i = tid; i < nn; i += TOPO_NT) tree_fill_node(sorted, b, i, f, k, theta_sq);
 }
 
 // chebcode.rs:309-337 barycentric_row, one warp wide: lane j < n owns node j
@@ -540,6 +647,49 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   b.counter = (int*)(b.pre + cap);
   b.levels = b.counter + 8;
   constexpr int BS = 256;
+  if (ns / std::max<int64_t>(prm.leaf_cap, 1) <= SMALL_TREE_LEAVES) {
+    // small tree: the whole topology in one CTA, one read-back of the levels
+    // (the flat arrays are sized for the 2 ns node bound)
+    void* q = nullptr;
+    SHRK_TRY(scratch_get(TREE_SLOTS + 0, sizeof(double) * 3 * (size_t)cap, &q));
+    f.lo = (double*)q;
+    f.hi = f.lo + cap;
+    f.accept_hw = f.hi + cap;
+    SHRK_TRY(scratch_get(TREE_SLOTS + 1, sizeof(int64_t) * 2 * (size_t)cap, &q));
+    f.lo_idx = (int64_t*)q;
+    f.hi_idx = f.lo_idx + cap;
+    SHRK_TRY(scratch_get(TREE_SLOTS + 2, sizeof(int32_t) * (size_t)cap, &q));
+    f.right = (int32_t*)q;
+    SHRK_TRY(scratch_get(TREE_SLOTS + 3, sizeof(double) * 2 * (size_t)cap * prm.n, &q));
+    f.nodes = (double*)q;
+    f.w = f.nodes + (size_t)cap * prm.n;
+    {
+      LaunchScope ls("cheb_build", s);
+      tree_topology_cta_kernel<<<1, TOPO_NT, 0, s>>>(d_sorted, b, ns, (int64_t)prm.leaf_cap, f, k,
+                                                     prm.theta * prm.theta);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    int h_lev[2 * NLEV];
+    SHRK_CUDA(cudaMemcpyAsync(h_lev, b.levels, sizeof(h_lev), cudaMemcpyDeviceToHost, s));
+    SHRK_CUDA(cudaStreamSynchronize(s));
+    int last = NLEV - 1;
+    for (int L = 1; L < NLEV; ++L)
+      if (h_lev[2 * L] == h_lev[2 * L + 1]) {
+        last = L;
+        break;
+      }
+    std::vector<int> lb, le;
+    for (int L = 0; L < last; ++L) {
+      lb.push_back(h_lev[2 * L]);
+      le.push_back(h_lev[2 * L + 1]);
+    }
+    tb.nn = le.back();
+    tb.lb = lb;
+    tb.le = le;
+    tb.b = b;
+    tb.k = k;
+    return tree_weights(tb, d_sorted, nullptr, f.w, s);
+  }
   {
     LaunchScope ls("cheb_build", s);
     tree_init_kernel<<<1, 1, 0, s>>>(b, ns);
