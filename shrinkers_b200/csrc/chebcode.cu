@@ -213,6 +213,71 @@ __device__ __forceinline__ void tree_split_node_warp(const double* __restrict__ 
 }
 
 constexpr int TOPO_NT = 1024;
+
+// M2M of a small tree in one CTA (tree_small_m2m_kernel).  A barycentric row
+// (chebcode.rs:309-337) is split into its parallel part -- the hit node or
+// the n quotients q_j = lam_j / (x - t_j), their sum in order,
+// m = mass * (1 / sum) -- one row per thread, and its accumulation
+// w_j = fma(m, q_j, w_j) (w_hit += mass on a hit), one thread per (node, j)
+// over an internal node's rows in the reference's order: the left then the
+// right child's masses in node order, zero masses skipped.  These are the
+// operations of bary_row_warp, so the weights are identical.
+struct SmallBuild {
+  int* row_hit;     // per row: node index hit exactly, or -1
+  double* row_m;    // per row: m (or the mass on a hit)
+  double* row_q;    // per row: q_j, j < n
+  int64_t rows_cap; // rows per level for M2M (>= 2 n x the nodes of any level)
+  int* err;
+  NodeF32* nf;      // f32 mirror (null: none)
+  float* panel;
+};
+
+__device__ __forceinline__ void bary_row_parts(double x, const double* t, const double* lam, int n,
+                                               double mass, int* hit_out, double* m_out,
+                                               double* q_out) {
+  int hit = -1;
+  for (int j = 0; j < n; ++j)
+    if (hit < 0 && x - t[j] == 0.0) hit = j;
+  *hit_out = hit;
+  if (hit >= 0) {
+    *m_out = mass;
+    return;
+  }
+  double sum = 0.0;
+  for (int j = 0; j < n; ++j) {
+    const double q = lam[j] / (x - t[j]);
+    q_out[j] = q;
+    sum += q;
+  }
+  *m_out = mass * (1.0 / sum);
+}
+
+__device__ __forceinline__ double bary_row_apply(int hit, double m, double qj, int j, double w) {
+  if (hit == -2) return w;  // skipped row (zero mass)
+  if (hit >= 0) return hit == j ? w + m : w;
+  return fma(m, qj, w);
+}
+
+// Node j's weight over rows [r0, r1) in order; the rows' loads are issued
+// eight at a time ahead of the dependent fma chain.
+__device__ __forceinline__ double bary_rows_accumulate(const SmallBuild& sb, int64_t r0, int64_t r1,
+                                                       int n, int j) {
+  double w = 0.0;
+  for (int64_t r = r0; r < r1; r += 8) {
+    int h[8];
+    double m[8], qj[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const bool in = r + u < r1;
+      h[u] = in ? sb.row_hit[r + u] : -2;
+      m[u] = in ? sb.row_m[r + u] : 0.0;
+      qj[u] = in && h[u] == -1 ? sb.row_q[(r + u) * n + j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) w = bary_row_apply(h[u], m[u], qj[u], j, w);
+  }
+  return w;
+}
 // Trees of at most this many leaf-capacities of sources (ns / leaf_cap) are
 // built by tree_topology_cta_kernel: a few hundred to ~2 000 nodes, where one
 // CTA beats two launches per level (a query-grid tree, a small spectrum).
@@ -267,6 +332,62 @@ __global__ void __launch_bounds__(TOPO_NT) tree_topology_cta_kernel(
   for (int i = tid; i < nn; i += TOPO_NT) tree_fill_node(sorted, b, i, f, k, theta_sq);
 }
 
+// M2M and the f32 mirror of a small tree in one CTA, after tree_p2m_grid_kernel
+// (levels read on the device).
+__global__ void __launch_bounds__(TOPO_NT) tree_small_m2m_kernel(BuildArrays b, FlatTree f,
+                                                                 ChebConsts k, SmallBuild sb) {
+  constexpr int NLEV = MAX_TREE_DEPTH + 2;
+  const int tid = threadIdx.x;
+  int last = NLEV - 1;  // first empty level
+  for (int L = 1; L < NLEV; ++L)
+    if (b.levels[2 * L] == b.levels[2 * L + 1]) {
+      last = L;
+      break;
+    }
+  const int nn = b.levels[2 * last - 1];
+  const int n = k.n;
+  // M2M, deepest internal level first; rows (node, child c, child node ti)
+  for (int L = last - 2; L >= 0; --L) {
+    const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
+    const int64_t nrows = (int64_t)(end - begin) * 2 * n;
+    if (nrows > sb.rows_cap) {  // excluded by the host's size rule; never drop rows
+      if (tid == 0) atomicExch(sb.err, DEV_ERR_BOUNDS);
+      return;
+    }
+    for (int64_t r = tid; r < nrows; r += TOPO_NT) {
+      const int i = begin + (int)(r / (2 * n)), c = (int)((r / n) % 2), ti = (int)(r % n);
+      if (b.lc[i] < 0) continue;
+      const int kid = b.pre[c ? b.rc[i] : b.lc[i]];
+      const double m = f.w[(int64_t)kid * n + ti];
+      if (m == 0.0) {
+        sb.row_hit[r] = -2;  // skipped
+        continue;
+      }
+      bary_row_parts(f.nodes[(int64_t)kid * n + ti], f.nodes + (int64_t)b.pre[i] * n, k.lam, n,
+                     m, &sb.row_hit[r], &sb.row_m[r], sb.row_q + r * n);
+    }
+    __syncthreads();
+    for (int t = tid; t < (end - begin) * n; t += TOPO_NT) {
+      const int i = begin + t / n, j = t % n;
+      if (b.lc[i] < 0) continue;
+      const int64_t r0 = (int64_t)(i - begin) * 2 * n;
+      f.w[(int64_t)b.pre[i] * n + j] = bary_rows_accumulate(sb, r0, r0 + 2 * n, n, j);
+    }
+    __syncthreads();
+  }
+  if (sb.nf) {
+    for (int i = tid; i < nn; i += TOPO_NT) {
+      sb.nf[i] = {(float)f.lo[i], (float)f.hi[i], (float)f.accept_hw[i], (uint32_t)f.lo_idx[i],
+                  (uint32_t)f.hi_idx[i], f.right[i]};
+      for (int j = 0; j < n; ++j) {
+        sb.panel[(int64_t)i * 2 * n + j] = (float)f.nodes[(int64_t)i * n + j];
+        sb.panel[(int64_t)i * 2 * n + n + j] = (float)f.w[(int64_t)i * n + j];
+      }
+    }
+  }
+}
+
+
 // chebcode.rs:309-337 barycentric_row, one warp wide: lane j < n owns node j
 // and its weight w.  The n divisions run in parallel; s is summed in the
 // sequential order (q_0 + q_1) + q_2 + ... through shuffles, an exact hit goes
@@ -290,12 +411,10 @@ __device__ __forceinline__ void bary_row_warp(double x, double t, double lam, in
 
 // P2M, one warp per leaf.  charges: per sorted source (null = unit masses,
 // the reference's P2M); wout: the node-weight array [nn][n] to fill.
-__global__ void tree_p2m_kernel(const double* __restrict__ sorted,
-                                const double* __restrict__ charges, BuildArrays b, int nn,
-                                FlatTree f, double* wout, ChebConsts k) {
-  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (i >= nn || b.lc[i] >= 0) return;  // whole warps leave together
+__device__ __forceinline__ void p2m_leaf(const double* __restrict__ sorted,
+                                         const double* __restrict__ charges, const BuildArrays& b,
+                                         int i, int lane, const FlatTree& f, double* wout,
+                                         const ChebConsts& k) {
   const int idx = b.pre[i];
   const int n = k.n;
   const double t = lane < n ? f.nodes[(int64_t)idx * n + lane] : 0.0;
@@ -304,6 +423,26 @@ __global__ void tree_p2m_kernel(const double* __restrict__ sorted,
   for (int64_t q = b.blo[i]; q < b.bhi[i]; ++q)
     bary_row_warp(sorted[q], t, lam, n, lane, w, charges ? charges[q] : 1.0);
   if (lane < n) wout[(int64_t)idx * n + lane] = w;
+}
+
+__global__ void tree_p2m_kernel(const double* __restrict__ sorted,
+                                const double* __restrict__ charges, BuildArrays b, int nn,
+                                FlatTree f, double* wout, ChebConsts k) {
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= nn || b.lc[i] >= 0) return;  // whole warps leave together
+  p2m_leaf(sorted, charges, b, i, lane, f, wout, k);
+}
+
+// The same over a fixed grid, the node count read on the device (the
+// breadth-first slot counter of a finished build), so no read-back is needed.
+__global__ void tree_p2m_grid_kernel(const double* __restrict__ sorted, BuildArrays b, FlatTree f,
+                                     double* wout, ChebConsts k) {
+  const int nn = *b.counter;
+  const int lane = threadIdx.x & 31;
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < nn; i += nw)
+    if (b.lc[i] < 0) p2m_leaf(sorted, nullptr, b, i, lane, f, wout, k);  // warp-uniform
 }
 
 // M2M, one warp per internal node of a level: the left then the right
@@ -966,6 +1105,86 @@ size_t grid_leaf_cap(size_t n, size_t p, size_t nq, size_t preset_leaf) {
   return std::min(std::max(r, preset_leaf), hi);
 }
 
+// The forward evaluation's tree for a small spectrum with no read-back: the
+// topology in one CTA, P2M over a fixed grid (the node count read on the
+// device), M2M and the f32 mirror in one CTA.  ns / leaf_cap <=
+// SMALL_TREE_LEAVES, so a level holds at most 2 * SMALL_TREE_LEAVES nodes
+// (each internal node holds more than leaf_cap sources); scratch slot 46
+// holds the M2M rows of one level.
+static bool fused_build_ok(int64_t ns, const ChebParams& prm) {
+  return ns / std::max<int64_t>(prm.leaf_cap, 1) <= SMALL_TREE_LEAVES;
+}
+
+static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const ChebParams& prm,
+                                    FlatTree& f, NodeF32** nf, float** panel, cudaStream_t s) {
+  const int64_t cap = std::max<int64_t>(2 * ns, 2);
+  const int n = prm.n;
+  ChebConsts k;
+  k.n = n;
+  for (int j = 0; j < n; ++j) {
+    k.sm1[j] = std::cos((double)j * M_PI / (double)(n - 1));
+    const double sign = (j % 2 == 0) ? 1.0 : -1.0;
+    k.lam[j] = (j == 0 || j == n - 1) ? 0.5 * sign : sign;
+  }
+  constexpr int NLEV = MAX_TREE_DEPTH + 2;
+  void* p64 = nullptr;
+  void* p32 = nullptr;
+  SHRK_TRY(scratch_get(25, sizeof(int64_t) * 2 * (size_t)cap, &p64));
+  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (4 * (size_t)cap + 8 + 2 * NLEV), &p32));
+  BuildArrays b;
+  b.blo = (int64_t*)p64;
+  b.bhi = b.blo + cap;
+  b.lc = (int32_t*)p32;
+  b.rc = b.lc + cap;
+  b.size = b.rc + cap;
+  b.pre = b.size + cap;
+  b.counter = (int*)(b.pre + cap);
+  b.levels = b.counter + 8;
+  void* q = nullptr;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 0, sizeof(double) * 3 * (size_t)cap, &q));
+  f.lo = (double*)q;
+  f.hi = f.lo + cap;
+  f.accept_hw = f.hi + cap;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 1, sizeof(int64_t) * 2 * (size_t)cap, &q));
+  f.lo_idx = (int64_t*)q;
+  f.hi_idx = f.lo_idx + cap;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 2, sizeof(int32_t) * (size_t)cap, &q));
+  f.right = (int32_t*)q;
+  SHRK_TRY(scratch_get(TREE_SLOTS + 3, sizeof(double) * 2 * (size_t)cap * n, &q));
+  f.nodes = (double*)q;
+  f.w = f.nodes + (size_t)cap * n;
+  SmallBuild sb;
+  sb.rows_cap = 2 * SMALL_TREE_LEAVES * 2 * n;
+  const int64_t rows = sb.rows_cap;
+  SHRK_TRY(scratch_get(46, (sizeof(double) * (n + 1) + sizeof(int)) * (size_t)rows + 64, &q));
+  sb.row_m = (double*)q;
+  sb.row_q = sb.row_m + rows;
+  sb.row_hit = (int*)(sb.row_q + rows * n);
+  sb.err = device_error_word();
+  sb.nf = nullptr;
+  sb.panel = nullptr;
+  if (prm.f32) {
+    SHRK_TRY(scratch_get(TREE_SLOTS + 4, sizeof(NodeF32) * (size_t)cap, &q));
+    sb.nf = (NodeF32*)q;
+    SHRK_TRY(scratch_get(TREE_SLOTS + 5, sizeof(float) * 2 * (size_t)cap * n, &q));
+    sb.panel = (float*)q;
+  }
+  {
+    LaunchScope ls("cheb_build", s);
+    tree_topology_cta_kernel<<<1, TOPO_NT, 0, s>>>(d_sorted, b, ns, (int64_t)prm.leaf_cap, f, k,
+                                                   prm.theta * prm.theta);
+    SHRK_CUDA(cudaGetLastError());
+    tree_p2m_grid_kernel<<<sm_count() * 4, 128, 0, s>>>(d_sorted, b, f, f.w, k);
+    SHRK_CUDA(cudaGetLastError());
+    tree_small_m2m_kernel<<<1, TOPO_NT, 0, s>>>(b, f, k, sb);
+    SHRK_CUDA(cudaGetLastError());
+    add_launches(2);
+  }
+  *nf = sb.nf;
+  *panel = sb.panel;
+  return SHRK_OK;
+}
+
 shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorted_src, int64_t ns,
                             double eta, const ChebParams& prm, const Epilogue& epi,
                             cudaStream_t s) {
@@ -975,7 +1194,11 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     return SHRK_EINVAL;
   }
   TreeBuild tb;
-  SHRK_TRY(build_tree_gpu(d_sorted_src, ns, prm, tb, s));
+  NodeF32* fused_nf = nullptr;
+  float* fused_panel = nullptr;
+  const bool fused = fused_build_ok(ns, prm);
+  if (fused) SHRK_TRY(build_tree_fused(d_sorted_src, ns, prm, tb.f, &fused_nf, &fused_panel, s));
+  else SHRK_TRY(build_tree_gpu(d_sorted_src, ns, prm, tb, s));
   const FlatTree& f = tb.f;
   const int nn = tb.nn;
   EvalArgs a;
@@ -1002,12 +1225,14 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     else cheb_eval_f64<false><<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   } else {
-    void* q = nullptr;
-    SHRK_TRY(scratch_get(TREE_SLOTS + 4, sizeof(NodeF32) * (size_t)nn, &q));
-    NodeF32* nf = (NodeF32*)q;
-    SHRK_TRY(scratch_get(TREE_SLOTS + 5, sizeof(float) * 2 * (size_t)nn * prm.n, &q));
-    float* panel = (float*)q;
-    {
+    NodeF32* nf = fused_nf;
+    float* panel = fused_panel;
+    if (!fused) {
+      void* q = nullptr;
+      SHRK_TRY(scratch_get(TREE_SLOTS + 4, sizeof(NodeF32) * (size_t)nn, &q));
+      nf = (NodeF32*)q;
+      SHRK_TRY(scratch_get(TREE_SLOTS + 5, sizeof(float) * 2 * (size_t)nn * prm.n, &q));
+      panel = (float*)q;
       LaunchScope ls("cheb_build", s);
       tree_f32_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(f, nn, prm.n, nf, panel);
       SHRK_CUDA(cudaGetLastError());
