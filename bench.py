@@ -50,7 +50,7 @@ def parse():
                     help="spectrum size (default: the workload's own size)")
     ap.add_argument("--workload", default="exact",
                     choices=["exact", "adjoint", "batched", "chebcode_fast", "chebcode",
-                             "chebcode_xtreme", "nufft", "fft5", "clean", "fmm"],
+                             "chebcode_xtreme", "nufft", "fft5", "clean", "fmm", "deconv"],
                     help="exact (default, the headline): all-points exact transform at p=1M; "
                          "adjoint: the adjoint kernel at p=20000; batched: 4096 uneven "
                          "spectra; chebcode*/nufft/fft5: the method at p=1M on the spiked "
@@ -861,11 +861,91 @@ def run_clean(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_deconv(args, world, rank, local):
+    """deconvolve_spiked (hybrid.rs:96-138: BEMA spike detection, inverse BBP,
+    El Karoui deconvolution of the bulk on a 200-point grid with the default
+    `auto` method, which the reference resolves to chebcode_fast up to
+    p = 50 000) through the Python API with host arrays -- the path has no
+    device form, so value and e2e both include the copies.  MP(c = 0.25) bulk
+    + 3 spikes in [4, 12].  A step = one call at --p; the line also times
+    p = 10 000 / 20 000 / 50 000, the sizes the reference publishes.  The CPU
+    baseline is the oracle's restatement of the same call on all host cores."""
+    import ctypes as C
+    import torch
+    import shrinkers_b200 as rk
+    from shrinkers_b200 import _native, spectra
+    from oracle import oracle as O
+
+    torch.cuda.set_device(local)
+    L = _native.load()
+    p = args.p
+    c = 0.25
+    spec = lambda n: spectra.mp_with_spikes(n, c, 3, 4.0, 12.0, seed=n + rank)
+    ev = spec(p)
+    step = lambda: rk.deconvolve_spiked(ev, c)
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    n0 = int(L.shrk_launch_count())
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    clk = clocks.stop()
+    launches = int(L.shrk_launch_count()) - n0
+    sizes = {}
+    for n in (10_000, 20_000, 50_000):
+        e = spec(n)
+        for _ in range(5):
+            rk.deconvolve_spiked(e, c)
+        reps = 200
+        t1 = time.perf_counter()
+        for _ in range(reps):
+            rk.deconvolve_spiked(e, c)
+        sizes[str(n)] = (time.perf_counter() - t1) * 1e3 / reps
+    cpu_line = None
+    if rank == 0 and not args.no_extras:
+        O.deconvolve_spiked(ev, c, parallel=True)
+        reps, t1 = 0, time.perf_counter()
+        while time.perf_counter() - t1 < 2.0:
+            O.deconvolve_spiked(ev, c, parallel=True)
+            reps += 1
+        dt = (time.perf_counter() - t1) / reps
+        cpu_line = {"value": 1.0 / dt, "unit": "calls/s", "cores": os.cpu_count(), "kind": "port",
+                    "sample": f"{reps} full calls at p={p} (auto -> chebcode_fast grid, "
+                              f"parallel route), {dt * 1e3:.3f} ms each"}
+    if rank != 0:
+        return
+    rate = world * 1e3 / ms
+    line = {
+        "metric": "deconvolve_spiked calls/s (host arrays)", "value": rate, "unit": "calls/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"deconvolve_spiked(ev, c=0.25), p={p}, n_points=200, method auto, "
+                               "MP(c=0.25) + 3 spikes in [4, 12]",
+                   "p": p, "parallelism": f"{world} GPU(s), one call stream per GPU",
+                   "value_basis": "Python API with host arrays (no device form)",
+                   "l2": "inputs of 8p bytes copied in every step"},
+        "roofline": None,
+        "ms_by_p": sizes,
+        "reference_published_ms_m1max": {"10000": 0.244, "20000": 0.368, "50000": 0.779},
+        "cpu_baseline": cpu_line,
+        "e2e": {"value": rate, "unit": "calls/s", "h2d_bytes_per_step": 8 * p + 8 * 200,
+                "d2h_bytes_per_step": 48 * 200, "ms_per_step": ms},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args.gpus)
     if args.p is None:
-        args.p = {"adjoint": 20_000, "clean": 2048}.get(args.workload, 1_000_000)
+        args.p = {"adjoint": 20_000, "clean": 2048, "deconv": 50_000}.get(args.workload, 1_000_000)
     if args.impl == "reference":
         if args.workload != "exact":
             if rank == 0:
@@ -877,6 +957,9 @@ def main():
         return
     if args.workload == "clean":
         run_clean(args, world, rank, local)
+        return
+    if args.workload == "deconv":
+        run_deconv(args, world, rank, local)
         return
     if args.workload != "exact":
         run_path(args, world, rank, local)

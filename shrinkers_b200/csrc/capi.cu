@@ -335,7 +335,10 @@ static void bema(const double* sorted, size_t p, double gamma, double margin, Sp
 static void detect_debias_split(const double* ev, size_t p, double gamma, double margin,
                                 SpikeSplit& s) {
   s.sorted.assign(ev, ev + p);
-  std::stable_sort(s.sorted.begin(), s.sorted.end());
+  // spectra usually arrive sorted: an O(p) check skips the O(p log p) sort
+  // (equal doubles are indistinguishable, so either way gives the same array)
+  if (!std::is_sorted(s.sorted.begin(), s.sorted.end()))
+    std::stable_sort(s.sorted.begin(), s.sorted.end());
   bema(s.sorted.data(), p, gamma, margin, s);
   s.spikes.clear();
   s.spike_sample.clear();
