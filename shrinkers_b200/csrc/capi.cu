@@ -178,8 +178,7 @@ static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s)
 // 12/13/14/22/23 batched path (its cached graph reads 12, 13, 14 and 22, so
 // no other path may write them), 15 probe sink, 16..21 treecode,
 // 24 FFT-grid stencil weights, 25..31 (see the kernel files), 32..38 the
-// matrix front-end (matrix.cu), 39..45 the dyadic FMM (fmm.cu), 46 the
-// fused small treecode build's barycentric rows (chebcode.cu).
+// matrix front-end (matrix.cu), 39..45 the dyadic FMM (fmm.cu).
 
 static bool is_fft5_family(int m) {
   return m == SHRK_M_FFT5 || m == SHRK_M_FFT3 || m == SHRK_M_FFT2;

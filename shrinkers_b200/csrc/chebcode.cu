@@ -73,6 +73,8 @@ struct BuildArrays {
   int32_t* pre;  // pre-order index
   int* counter;  // next free BFS slot
   int* levels;   // level L = BFS slots [levels[2L], levels[2L+1])
+  int32_t* parent;  // small builds: parent slot (-1 at the root)
+  int32_t* arrive;  // small builds: children finished per node
 };
 
 __device__ __forceinline__ void tree_split_node(const double* __restrict__ sorted, BuildArrays b,
@@ -213,77 +215,12 @@ __device__ __forceinline__ void tree_split_node_warp(const double* __restrict__ 
 }
 
 constexpr int TOPO_NT = 1024;
-
-// M2M of a small tree in one CTA (tree_small_m2m_kernel).  A barycentric row
-// (chebcode.rs:309-337) is split into its parallel part -- the hit node or
-// the n quotients q_j = lam_j / (x - t_j), their sum in order,
-// m = mass * (1 / sum) -- one row per thread, and its accumulation
-// w_j = fma(m, q_j, w_j) (w_hit += mass on a hit), one thread per (node, j)
-// over an internal node's rows in the reference's order: the left then the
-// right child's masses in node order, zero masses skipped.  These are the
-// operations of bary_row_warp, so the weights are identical.
-struct SmallBuild {
-  int* row_hit;     // per row: node index hit exactly, or -1
-  double* row_m;    // per row: m (or the mass on a hit)
-  double* row_q;    // per row: q_j, j < n
-  int64_t rows_cap; // rows per level for M2M (>= 2 n x the nodes of any level)
-  int* err;
-  NodeF32* nf;      // f32 mirror (null: none)
-  float* panel;
-};
-
-__device__ __forceinline__ void bary_row_parts(double x, const double* t, const double* lam, int n,
-                                               double mass, int* hit_out, double* m_out,
-                                               double* q_out) {
-  int hit = -1;
-  for (int j = 0; j < n; ++j)
-    if (hit < 0 && x - t[j] == 0.0) hit = j;
-  *hit_out = hit;
-  if (hit >= 0) {
-    *m_out = mass;
-    return;
-  }
-  double sum = 0.0;
-  for (int j = 0; j < n; ++j) {
-    const double q = lam[j] / (x - t[j]);
-    q_out[j] = q;
-    sum += q;
-  }
-  *m_out = mass * (1.0 / sum);
-}
-
-__device__ __forceinline__ double bary_row_apply(int hit, double m, double qj, int j, double w) {
-  if (hit == -2) return w;  // skipped row (zero mass)
-  if (hit >= 0) return hit == j ? w + m : w;
-  return fma(m, qj, w);
-}
-
-// Node j's weight over rows [r0, r1) in order; the rows' loads are issued
-// eight at a time ahead of the dependent fma chain.
-__device__ __forceinline__ double bary_rows_accumulate(const SmallBuild& sb, int64_t r0, int64_t r1,
-                                                       int n, int j) {
-  double w = 0.0;
-  for (int64_t r = r0; r < r1; r += 8) {
-    int h[8];
-    double m[8], qj[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const bool in = r + u < r1;
-      h[u] = in ? sb.row_hit[r + u] : -2;
-      m[u] = in ? sb.row_m[r + u] : 0.0;
-      qj[u] = in && h[u] == -1 ? sb.row_q[(r + u) * n + j] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) w = bary_row_apply(h[u], m[u], qj[u], j, w);
-  }
-  return w;
-}
 // Trees of at most this many leaf-capacities of sources (ns / leaf_cap) are
 // built by tree_topology_cta_kernel: a few hundred to ~2 000 nodes, where one
 // CTA beats two launches per level (a query-grid tree, a small spectrum).
 constexpr int64_t SMALL_TREE_LEAVES = 512;
 
-__global__ void __launch_bounds__(TOPO_NT) tree_topology_cta_kernel(
+__global__ void __launch_bounds__(TOPO_NT, 1) tree_topology_cta_kernel(
     const double* __restrict__ sorted, BuildArrays b, int64_t ns, int64_t leaf_cap, FlatTree f,
     ChebConsts k, double theta_sq) {
   constexpr int NLEV = MAX_TREE_DEPTH + 2;
@@ -321,151 +258,197 @@ __global__ void __launch_bounds__(TOPO_NT) tree_topology_cta_kernel(
   }
   for (int L = 0; L < last; ++L) {
     const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
-    for (int i = begin + tid; i < end; i += TOPO_NT)
+    for (int i = begin + tid; i < end; i += TOPO_NT) {
+      b.arrive[i] = 0;
+      if (L == 0) b.parent[i] = -1;
       if (b.lc[i] >= 0) {
         b.pre[b.lc[i]] = b.pre[i] + 1;
         b.pre[b.rc[i]] = b.pre[i] + 1 + b.size[b.lc[i]];
+        b.parent[b.lc[i]] = i;
+        b.parent[b.rc[i]] = i;
       }
+    }
     __syncthreads();
   }
   const int nn = b.levels[2 * last - 1];
   for (int i = tid; i < nn; i += TOPO_NT) tree_fill_node(sorted, b, i, f, k, theta_sq);
 }
 
-// M2M and the f32 mirror of a small tree in one CTA, after tree_p2m_grid_kernel
-// (levels read on the device).
-__global__ void __launch_bounds__(TOPO_NT) tree_small_m2m_kernel(BuildArrays b, FlatTree f,
-                                                                 ChebConsts k, SmallBuild sb) {
-  constexpr int NLEV = MAX_TREE_DEPTH + 2;
-  const int tid = threadIdx.x;
-  int last = NLEV - 1;  // first empty level
-  for (int L = 1; L < NLEV; ++L)
-    if (b.levels[2 * L] == b.levels[2 * L + 1]) {
-      last = L;
-      break;
-    }
-  const int nn = b.levels[2 * last - 1];
-  const int n = k.n;
-  // M2M, deepest internal level first; rows (node, child c, child node ti)
-  for (int L = last - 2; L >= 0; --L) {
-    const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
-    const int64_t nrows = (int64_t)(end - begin) * 2 * n;
-    if (nrows > sb.rows_cap) {  // excluded by the host's size rule; never drop rows
-      if (tid == 0) atomicExch(sb.err, DEV_ERR_BOUNDS);
-      return;
-    }
-    for (int64_t r = tid; r < nrows; r += TOPO_NT) {
-      const int i = begin + (int)(r / (2 * n)), c = (int)((r / n) % 2), ti = (int)(r % n);
-      if (b.lc[i] < 0) continue;
-      const int kid = b.pre[c ? b.rc[i] : b.lc[i]];
-      const double m = f.w[(int64_t)kid * n + ti];
-      if (m == 0.0) {
-        sb.row_hit[r] = -2;  // skipped
-        continue;
-      }
-      bary_row_parts(f.nodes[(int64_t)kid * n + ti], f.nodes + (int64_t)b.pre[i] * n, k.lam, n,
-                     m, &sb.row_hit[r], &sb.row_m[r], sb.row_q + r * n);
-    }
-    __syncthreads();
-    for (int t = tid; t < (end - begin) * n; t += TOPO_NT) {
-      const int i = begin + t / n, j = t % n;
-      if (b.lc[i] < 0) continue;
-      const int64_t r0 = (int64_t)(i - begin) * 2 * n;
-      f.w[(int64_t)b.pre[i] * n + j] = bary_rows_accumulate(sb, r0, r0 + 2 * n, n, j);
-    }
-    __syncthreads();
-  }
-  if (sb.nf) {
-    for (int i = tid; i < nn; i += TOPO_NT) {
-      sb.nf[i] = {(float)f.lo[i], (float)f.hi[i], (float)f.accept_hw[i], (uint32_t)f.lo_idx[i],
-                  (uint32_t)f.hi_idx[i], f.right[i]};
+// Up to 32 barycentric rows at once, one warp: lane r computes row r's
+// parallel part (the first node hit exactly, or the quotients
+// q_j = lam_j / (x - t_j) into the warp's shared tile, their sum in order and
+// m = mass * (1 / sum)); then lane j < n adds the rows in order,
+// w_j = fma(m_r, q_rj, w_j) (w_j + mass_r on a hit at j).  These are the
+// operations of chebcode.rs:309-337 barycentric_row (IEEE divisions, the
+// sum in node order, the first exact hit taking the whole mass, a fused
+// update) applied row after row, so w is the sequential result bit for bit;
+// the divisions of 32 rows run in parallel.  Invalid rows (zero masses, the
+// tail of a batch) are skipped.
+constexpr int ROW_RS = MAX_N + 1;  // shared tile row stride (doubles)
+constexpr int WEIGHT_NT = 128;     // threads per block of the weight kernels
+
+struct RowTile {
+  double q[32 * ROW_RS];
+  double t[MAX_N];
+  double lam[MAX_N];
+};
+
+__device__ __forceinline__ void bary_rows_batch(double x, double mass, bool valid, int cnt, int n,
+                                                int lane, RowTile& rt, double& w) {
+  int hit = -2;
+  double m = 0.0;
+  if (valid) {
+    hit = -1;
+    for (int j = 0; j < n; ++j)
+      if (hit < 0 && x - rt.t[j] == 0.0) hit = j;
+    if (hit >= 0) {
+      m = mass;
+    } else {
+      double sum = 0.0;
       for (int j = 0; j < n; ++j) {
-        sb.panel[(int64_t)i * 2 * n + j] = (float)f.nodes[(int64_t)i * n + j];
-        sb.panel[(int64_t)i * 2 * n + n + j] = (float)f.w[(int64_t)i * n + j];
+        const double q = rt.lam[j] / (x - rt.t[j]);
+        rt.q[lane * ROW_RS + j] = q;
+        sum += q;
+      }
+      m = mass * (1.0 / sum);
+    }
+  }
+  __syncwarp();
+  for (int r = 0; r < cnt; ++r) {
+    const int h = __shfl_sync(0xffffffffu, hit, r);
+    const double mr = __shfl_sync(0xffffffffu, m, r);
+    if (lane < n && h != -2) {
+      if (h >= 0) {
+        if (h == lane) w = w + mr;
+      } else {
+        w = fma(mr, rt.q[r * ROW_RS + lane], w);
       }
     }
   }
+  __syncwarp();  // the tile is rewritten by the next batch
 }
 
-
-// chebcode.rs:309-337 barycentric_row, one warp wide: lane j < n owns node j
-// and its weight w.  The n divisions run in parallel; s is summed in the
-// sequential order (q_0 + q_1) + q_2 + ... through shuffles, an exact hit goes
-// to the first node with d == 0 (as the sequential loop's break does), and
-// each weight takes the same fma -- the result equals the sequential row bit
-// for bit.
-__device__ __forceinline__ void bary_row_warp(double x, double t, double lam, int n, int lane,
-                                              double& w, double mass) {
-  const double d = x - t;
-  const unsigned hit = __ballot_sync(0xffffffffu, lane < n && d == 0.0);
-  if (hit) {
-    if (lane == __ffs(hit) - 1) w += mass;
-    return;
+__device__ __forceinline__ void row_tile_node(RowTile& rt, const FlatTree& f, int idx, int n,
+                                              const ChebConsts& k, int lane) {
+  if (lane < n) {
+    rt.t[lane] = f.nodes[(int64_t)idx * n + lane];
+    rt.lam[lane] = k.lam[lane];
   }
-  const double q = lane < n ? lam / d : 0.0;
-  double sum = 0.0;
-  for (int j = 0; j < n; ++j) sum += __shfl_sync(0xffffffffu, q, j);
-  const double m = mass * (1.0 / sum);
-  if (lane < n) w = fma(m, q, w);
+  __syncwarp();
 }
 
-// P2M, one warp per leaf.  charges: per sorted source (null = unit masses,
-// the reference's P2M); wout: the node-weight array [nn][n] to fill.
+// P2M, one warp per leaf, its sources 32 at a time in index order.  charges:
+// per sorted source (null = unit masses, the reference's P2M); wout: the
+// node-weight array [nn][n] to fill.
 __device__ __forceinline__ void p2m_leaf(const double* __restrict__ sorted,
                                          const double* __restrict__ charges, const BuildArrays& b,
                                          int i, int lane, const FlatTree& f, double* wout,
-                                         const ChebConsts& k) {
+                                         const ChebConsts& k, RowTile& rt) {
   const int idx = b.pre[i];
   const int n = k.n;
-  const double t = lane < n ? f.nodes[(int64_t)idx * n + lane] : 0.0;
-  const double lam = lane < n ? k.lam[lane] : 0.0;
+  row_tile_node(rt, f, idx, n, k, lane);
   double w = 0.0;
-  for (int64_t q = b.blo[i]; q < b.bhi[i]; ++q)
-    bary_row_warp(sorted[q], t, lam, n, lane, w, charges ? charges[q] : 1.0);
+  const int64_t q1 = b.bhi[i];
+  for (int64_t q0 = b.blo[i]; q0 < q1; q0 += 32) {
+    const int cnt = (int)min((int64_t)32, q1 - q0);
+    const bool in = lane < cnt;
+    const double x = in ? sorted[q0 + lane] : 0.0;
+    const double mass = in ? (charges ? charges[q0 + lane] : 1.0) : 0.0;
+    bary_rows_batch(x, mass, in, cnt, n, lane, rt, w);
+  }
   if (lane < n) wout[(int64_t)idx * n + lane] = w;
 }
 
-__global__ void tree_p2m_kernel(const double* __restrict__ sorted,
-                                const double* __restrict__ charges, BuildArrays b, int nn,
-                                FlatTree f, double* wout, ChebConsts k) {
+__global__ void __launch_bounds__(WEIGHT_NT) tree_p2m_kernel(const double* __restrict__ sorted,
+                                                             const double* __restrict__ charges,
+                                                             BuildArrays b, int nn, FlatTree f,
+                                                             double* wout, ChebConsts k) {
+  __shared__ RowTile tiles[WEIGHT_NT / 32];
   const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (i >= nn || b.lc[i] >= 0) return;  // whole warps leave together
-  p2m_leaf(sorted, charges, b, i, lane, f, wout, k);
+  p2m_leaf(sorted, charges, b, i, lane, f, wout, k, tiles[threadIdx.x >> 5]);
 }
 
-// The same over a fixed grid, the node count read on the device (the
-// breadth-first slot counter of a finished build), so no read-back is needed.
-__global__ void tree_p2m_grid_kernel(const double* __restrict__ sorted, BuildArrays b, FlatTree f,
-                                     double* wout, ChebConsts k) {
+// M2M of node i: rows (child c, child node ti), the left child first, in
+// node order, zero masses skipped (2 n <= 32 rows, one batch).  cg: read the
+// children's weights past L1 (they may come from another SM in this launch).
+__device__ __forceinline__ void m2m_node(const BuildArrays& b, int i, int lane, const FlatTree& f,
+                                         double* wts, const ChebConsts& k, bool cg, RowTile& rt) {
+  const int idx = b.pre[i];
+  const int n = k.n;
+  row_tile_node(rt, f, idx, n, k, lane);
+  double x = 0.0, mass = 0.0;
+  if (lane < 2 * n) {
+    const int kid = b.pre[lane < n ? b.lc[i] : b.rc[i]], ti = lane % n;
+    const double* mp = wts + (int64_t)kid * n + ti;
+    mass = cg ? __ldcg(mp) : *mp;
+    x = f.nodes[(int64_t)kid * n + ti];
+  }
+  double w = 0.0;
+  bary_rows_batch(x, mass, lane < 2 * n && mass != 0.0, 2 * n, n, lane, rt, w);
+  if (lane < n) wts[(int64_t)idx * n + lane] = w;
+}
+
+__global__ void __launch_bounds__(WEIGHT_NT) tree_m2m_kernel(BuildArrays b, int begin, int end,
+                                                             FlatTree f, double* wts,
+                                                             ChebConsts k) {
+  __shared__ RowTile tiles[WEIGHT_NT / 32];
+  const int i = begin + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= end || b.lc[i] < 0) return;  // whole warps leave together
+  m2m_node(b, i, lane, f, wts, k, false, tiles[threadIdx.x >> 5]);
+}
+
+__device__ __forceinline__ void mirror_f32(const FlatTree& f, int idx, int n, int lane,
+                                           NodeF32* nf, float* panel) {
+  if (lane == 0)
+    nf[idx] = {(float)f.lo[idx], (float)f.hi[idx], (float)f.accept_hw[idx],
+               (uint32_t)f.lo_idx[idx], (uint32_t)f.hi_idx[idx], f.right[idx]};
+  if (lane < n) {
+    panel[(int64_t)idx * 2 * n + lane] = (float)f.nodes[(int64_t)idx * n + lane];
+    panel[(int64_t)idx * 2 * n + n + lane] = (float)__ldcg(f.w + (int64_t)idx * n + lane);
+  }
+}
+
+// P2M and M2M of a small tree in one launch over a fixed grid, with no
+// read-back (the node count is the breadth-first slot counter): a warp
+// fills a leaf, then climbs -- it fences its weights and counts itself in at
+// the parent; the warp that brings the count to two (the last child done)
+// merges the parent (m2m_node, children's weights read past L1) and goes on
+// up, the other stops.  No warp waits on another.  Each node's f32 mirror
+// entry is written once its weights are final (nf null: none).
+__global__ void __launch_bounds__(WEIGHT_NT, 1) tree_p2m_grid_kernel(
+    const double* __restrict__ sorted, BuildArrays b, FlatTree f, double* wout, ChebConsts k,
+    NodeF32* nf, float* panel) {
+  __shared__ RowTile tiles[WEIGHT_NT / 32];
+  RowTile& rt = tiles[threadIdx.x >> 5];
   const int nn = *b.counter;
   const int lane = threadIdx.x & 31;
   const int nw = (int)((gridDim.x * blockDim.x) >> 5);
-  for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < nn; i += nw)
-    if (b.lc[i] < 0) p2m_leaf(sorted, nullptr, b, i, lane, f, wout, k);  // warp-uniform
+  for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < nn; i += nw) {
+    if (b.lc[i] >= 0) continue;  // warp-uniform
+    p2m_leaf(sorted, nullptr, b, i, lane, f, wout, k, rt);
+    if (nf) mirror_f32(f, b.pre[i], k.n, lane, nf, panel);
+    for (int node = i;;) {
+      const int par = b.parent[node];
+      if (par < 0) break;
+      __threadfence();  // this node's weights before the count
+      int seen = 0;
+      if (lane == 0) seen = atomicAdd(&b.arrive[par], 1);
+      seen = __shfl_sync(0xffffffffu, seen, 0);
+      if (seen == 0) break;  // the sibling's warp merges the parent
+      __threadfence();
+      m2m_node(b, par, lane, f, wout, k, true, rt);
+      if (nf) mirror_f32(f, b.pre[par], k.n, lane, nf, panel);
+      node = par;
+    }
+  }
 }
 
 // M2M, one warp per internal node of a level: the left then the right
 // child's node masses, in node order.
-__global__ void tree_m2m_kernel(BuildArrays b, int begin, int end, FlatTree f, double* wts,
-                                ChebConsts k) {
-  const int i = begin + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (i >= end || b.lc[i] < 0) return;  // whole warps leave together
-  const int idx = b.pre[i];
-  const int n = k.n;
-  const double t = lane < n ? f.nodes[(int64_t)idx * n + lane] : 0.0;
-  const double lam = lane < n ? k.lam[lane] : 0.0;
-  double w = 0.0;
-  const int kids[2] = {b.pre[b.lc[i]], b.pre[b.rc[i]]};
-  for (int c = 0; c < 2; ++c)
-    for (int ti = 0; ti < n; ++ti) {
-      const double m = wts[(int64_t)kids[c] * n + ti];
-      if (m == 0.0) continue;
-      bary_row_warp(f.nodes[(int64_t)kids[c] * n + ti], t, lam, n, lane, w, m);
-    }
-  if (lane < n) wts[(int64_t)idx * n + lane] = w;
-}
+
 
 // ----------------------------------------------------------- device --
 struct DevTreeF64 {
@@ -741,12 +724,12 @@ struct TreeBuild {
 // wout: P2M at the leaves, then M2M from the deepest internal level up.
 shrk_status tree_weights(const TreeBuild& tb, const double* d_sorted, const double* charges,
                          double* wout, cudaStream_t s) {
-  tree_p2m_kernel<<<blocks_for((int64_t)tb.nn * 32, 128), 128, 0, s>>>(d_sorted, charges, tb.b,
+  tree_p2m_kernel<<<blocks_for((int64_t)tb.nn * 32, WEIGHT_NT), WEIGHT_NT, 0, s>>>(d_sorted, charges, tb.b,
                                                                        tb.nn, tb.f, wout, tb.k);
   SHRK_CUDA(cudaGetLastError());
   const int levels = (int)tb.lb.size();
   for (int L = levels - 2; L >= 0; --L) {
-    tree_m2m_kernel<<<blocks_for((int64_t)(tb.le[L] - tb.lb[L]) * 32, 128), 128, 0, s>>>(
+    tree_m2m_kernel<<<blocks_for((int64_t)(tb.le[L] - tb.lb[L]) * 32, WEIGHT_NT), WEIGHT_NT, 0, s>>>(
         tb.b, tb.lb[L], tb.le[L], tb.f, wout, tb.k);
     SHRK_CUDA(cudaGetLastError());
   }
@@ -775,7 +758,7 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   void* p32 = nullptr;
   SHRK_TRY(scratch_get(25, sizeof(int64_t) * 2 * (size_t)cap, &p64));
   constexpr int NLEV = MAX_TREE_DEPTH + 2;  // levels 0..48 split, level 49 is empty
-  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (4 * (size_t)cap + 8 + 2 * NLEV), &p32));
+  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (6 * (size_t)cap + 8 + 2 * NLEV), &p32));
   BuildArrays b;
   b.blo = (int64_t*)p64;
   b.bhi = b.blo + cap;
@@ -785,6 +768,8 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   b.pre = b.size + cap;
   b.counter = (int*)(b.pre + cap);
   b.levels = b.counter + 8;
+  b.parent = b.levels + 2 * NLEV;
+  b.arrive = b.parent + cap;
   constexpr int BS = 256;
   if (ns / std::max<int64_t>(prm.leaf_cap, 1) <= SMALL_TREE_LEAVES) {
     // small tree: the whole topology in one CTA, one read-back of the levels
@@ -1105,12 +1090,10 @@ size_t grid_leaf_cap(size_t n, size_t p, size_t nq, size_t preset_leaf) {
   return std::min(std::max(r, preset_leaf), hi);
 }
 
-// The forward evaluation's tree for a small spectrum with no read-back: the
-// topology in one CTA, P2M over a fixed grid (the node count read on the
-// device), M2M and the f32 mirror in one CTA.  ns / leaf_cap <=
-// SMALL_TREE_LEAVES, so a level holds at most 2 * SMALL_TREE_LEAVES nodes
-// (each internal node holds more than leaf_cap sources); scratch slot 46
-// holds the M2M rows of one level.
+// The forward evaluation's tree for a small spectrum (ns / leaf_cap <=
+// SMALL_TREE_LEAVES) with no read-back: the topology in one CTA, then P2M,
+// M2M and the f32 mirror in one launch over a fixed grid
+// (tree_p2m_grid_kernel).
 static bool fused_build_ok(int64_t ns, const ChebParams& prm) {
   return ns / std::max<int64_t>(prm.leaf_cap, 1) <= SMALL_TREE_LEAVES;
 }
@@ -1130,7 +1113,7 @@ static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const Ch
   void* p64 = nullptr;
   void* p32 = nullptr;
   SHRK_TRY(scratch_get(25, sizeof(int64_t) * 2 * (size_t)cap, &p64));
-  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (4 * (size_t)cap + 8 + 2 * NLEV), &p32));
+  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (6 * (size_t)cap + 8 + 2 * NLEV), &p32));
   BuildArrays b;
   b.blo = (int64_t*)p64;
   b.bhi = b.blo + cap;
@@ -1140,6 +1123,8 @@ static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const Ch
   b.pre = b.size + cap;
   b.counter = (int*)(b.pre + cap);
   b.levels = b.counter + 8;
+  b.parent = b.levels + 2 * NLEV;
+  b.arrive = b.parent + cap;
   void* q = nullptr;
   SHRK_TRY(scratch_get(TREE_SLOTS + 0, sizeof(double) * 3 * (size_t)cap, &q));
   f.lo = (double*)q;
@@ -1153,35 +1138,26 @@ static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const Ch
   SHRK_TRY(scratch_get(TREE_SLOTS + 3, sizeof(double) * 2 * (size_t)cap * n, &q));
   f.nodes = (double*)q;
   f.w = f.nodes + (size_t)cap * n;
-  SmallBuild sb;
-  sb.rows_cap = 2 * SMALL_TREE_LEAVES * 2 * n;
-  const int64_t rows = sb.rows_cap;
-  SHRK_TRY(scratch_get(46, (sizeof(double) * (n + 1) + sizeof(int)) * (size_t)rows + 64, &q));
-  sb.row_m = (double*)q;
-  sb.row_q = sb.row_m + rows;
-  sb.row_hit = (int*)(sb.row_q + rows * n);
-  sb.err = device_error_word();
-  sb.nf = nullptr;
-  sb.panel = nullptr;
+  NodeF32* mirror = nullptr;
+  float* mpanel = nullptr;
   if (prm.f32) {
     SHRK_TRY(scratch_get(TREE_SLOTS + 4, sizeof(NodeF32) * (size_t)cap, &q));
-    sb.nf = (NodeF32*)q;
+    mirror = (NodeF32*)q;
     SHRK_TRY(scratch_get(TREE_SLOTS + 5, sizeof(float) * 2 * (size_t)cap * n, &q));
-    sb.panel = (float*)q;
+    mpanel = (float*)q;
   }
   {
     LaunchScope ls("cheb_build", s);
     tree_topology_cta_kernel<<<1, TOPO_NT, 0, s>>>(d_sorted, b, ns, (int64_t)prm.leaf_cap, f, k,
                                                    prm.theta * prm.theta);
     SHRK_CUDA(cudaGetLastError());
-    tree_p2m_grid_kernel<<<sm_count() * 4, 128, 0, s>>>(d_sorted, b, f, f.w, k);
+    tree_p2m_grid_kernel<<<sm_count() * 4, WEIGHT_NT, 0, s>>>(d_sorted, b, f, f.w, k, mirror,
+                                                              mpanel);
     SHRK_CUDA(cudaGetLastError());
-    tree_small_m2m_kernel<<<1, TOPO_NT, 0, s>>>(b, f, k, sb);
-    SHRK_CUDA(cudaGetLastError());
-    add_launches(2);
+    add_launches(1);
   }
-  *nf = sb.nf;
-  *panel = sb.panel;
+  *nf = mirror;
+  *panel = mpanel;
   return SHRK_OK;
 }
 
