@@ -18,6 +18,8 @@
 #include "epilogue.cuh"
 #include "internal.h"
 
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -73,8 +75,11 @@ struct BuildArrays {
   int32_t* pre;  // pre-order index
   int* counter;  // next free BFS slot
   int* levels;   // level L = BFS slots [levels[2L], levels[2L+1])
-  int32_t* parent;  // small builds: parent slot (-1 at the root)
-  int32_t* arrive;  // small builds: children finished per node
+  int32_t* parent;  // parent slot (-1 at the root)
+  int32_t* arrive;  // children finished per node (the climbing P2M/M2M)
+  int32_t* dep;     // depth
+  int32_t* rturn;   // right turns on the path from the root
+  int32_t* leafpre; // [ns + 1]: leaf starts, then their exclusive prefix count
 };
 
 __device__ __forceinline__ void tree_split_node(const double* __restrict__ sorted, BuildArrays b,
@@ -101,36 +106,53 @@ __device__ __forceinline__ void tree_split_node(const double* __restrict__ sorte
   b.bhi[slot + 1] = hi_idx;
   b.lc[i] = slot;
   b.rc[i] = slot + 1;
+  b.parent[slot] = b.parent[slot + 1] = i;
+  b.dep[slot] = b.dep[slot + 1] = depth + 1;
+  b.rturn[slot] = b.rturn[i];
+  b.rturn[slot + 1] = b.rturn[i] + 1;
 }
 
 // Splits the nodes of level `depth` (its slot range read from b.levels, so
-// successive levels launch without host round trips).
+// successive levels launch without host round trips).  The last CTA to
+// finish (a ticket taken after a fence) records the next level: exactly the
+// children allocated while splitting this one.
 __global__ void tree_split_kernel(const double* __restrict__ sorted, BuildArrays b, int depth,
                                   int64_t leaf_cap) {
   const int begin = b.levels[2 * depth], end = b.levels[2 * depth + 1];
   for (int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x); i < end;
        i += (int)(gridDim.x * blockDim.x))
     tree_split_node(sorted, b, i, depth, leaf_cap);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned ticket = atomicAdd(reinterpret_cast<unsigned*>(b.counter + 1), 1u);
+    if (ticket == gridDim.x - 1) {
+      __threadfence();
+      b.levels[2 * depth + 2] = end;
+      b.levels[2 * depth + 3] = atomicAdd(b.counter, 0);
+      b.counter[1] = 0;  // the next level's launch counts again from zero
+    }
+  }
 }
 
-// The next level holds exactly the children allocated while splitting this one.
-__global__ void tree_level_advance_kernel(BuildArrays b, int depth) {
-  b.levels[2 * depth + 2] = b.levels[2 * depth + 1];
-  b.levels[2 * depth + 3] = *b.counter;
+// Subtree sizes and pre-order indices without a level loop.  The tree is
+// full (every internal node has two children), so a node over sources
+// [lo, hi) with L leaves has 2 L - 1 nodes, and in pre-order it follows its
+// ancestors and, for each right turn on its path, the whole left subtree it
+// turned away from; those subtrees hold exactly the leaves before lo:
+//   size = 2 L - 1,   pre = depth + 2 * (leaves before lo) - right turns,
+// with leaf counts from an exclusive prefix sum of the leaves' start flags.
+__global__ void tree_leaf_flags_kernel(BuildArrays b, int nn) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i < nn && b.lc[i] < 0) b.leafpre[b.blo[i]] = 1;
 }
 
-
-__global__ void tree_size_kernel(BuildArrays b, int begin, int end) {
-  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= end) return;
-  b.size[i] = b.lc[i] < 0 ? 1 : 1 + b.size[b.lc[i]] + b.size[b.rc[i]];
-}
-
-__global__ void tree_pre_kernel(BuildArrays b, int begin, int end) {
-  const int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (i >= end || b.lc[i] < 0) return;
-  b.pre[b.lc[i]] = b.pre[i] + 1;
-  b.pre[b.rc[i]] = b.pre[i] + 1 + b.size[b.lc[i]];
+__global__ void tree_order_kernel(BuildArrays b, int nn, const int* __restrict__ prefix) {
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= nn) return;
+  const int before = prefix[b.blo[i]];
+  b.size[i] = 2 * (prefix[b.bhi[i]] - before) - 1;
+  b.pre[i] = b.dep[i] + 2 * before - b.rturn[i];
 }
 
 struct FlatTree {
@@ -691,6 +713,10 @@ __global__ void tree_init_kernel(BuildArrays b, int64_t ns) {
   b.blo[0] = 0;
   b.bhi[0] = ns;
   b.pre[0] = 0;
+  b.parent[0] = -1;
+  b.dep[0] = 0;
+  b.rturn[0] = 0;
+  b.counter[1] = 0;
   *b.counter = 1;
   b.levels[0] = 0;
   b.levels[1] = 1;
@@ -758,7 +784,8 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   void* p32 = nullptr;
   SHRK_TRY(scratch_get(25, sizeof(int64_t) * 2 * (size_t)cap, &p64));
   constexpr int NLEV = MAX_TREE_DEPTH + 2;  // levels 0..48 split, level 49 is empty
-  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (6 * (size_t)cap + 8 + 2 * NLEV), &p32));
+  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (8 * (size_t)cap + (size_t)ns + 2 + 8 + 2 * NLEV),
+                       &p32));
   BuildArrays b;
   b.blo = (int64_t*)p64;
   b.bhi = b.blo + cap;
@@ -770,6 +797,9 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   b.levels = b.counter + 8;
   b.parent = b.levels + 2 * NLEV;
   b.arrive = b.parent + cap;
+  b.dep = b.arrive + cap;
+  b.rturn = b.dep + cap;
+  b.leafpre = b.rturn + cap;
   constexpr int BS = 256;
   if (ns / std::max<int64_t>(prm.leaf_cap, 1) <= SMALL_TREE_LEAVES) {
     // small tree: the whole topology in one CTA, one read-back of the levels
@@ -820,20 +850,23 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
     SHRK_CUDA(cudaGetLastError());
   }
   // 1. split, level by level (each level's children fill the next slots);
-  //    levels run in batches of 8 with one read-back of the level table per
-  //    batch to see whether a level came out empty.
+  //    levels run in batches with one read-back of the level table per batch
+  //    to see whether a level came out empty: the first batch covers the
+  //    depth a balanced tree would need plus a margin, later ones 8 levels.
   const int split_grid = std::max(1, sm_count() * 4);
   int h_lev[2 * NLEV];
   int last = -1;  // first empty level
+  const int64_t leaves_est = std::max<int64_t>(ns / std::max<int64_t>(prm.leaf_cap, 1), 1);
+  int batch = 8;
+  while ((int64_t{1} << (batch - 8)) < leaves_est && batch < NLEV - 1) ++batch;
   for (int L0 = 0; last < 0;) {
-    const int L1 = std::min(L0 + 8, NLEV - 1);
+    const int L1 = std::min(L0 + batch, NLEV - 1);
+    batch = 8;
     for (int L = L0; L < L1; ++L) {
       tree_split_kernel<<<split_grid, BS, 0, s>>>(d_sorted, b, L, (int64_t)prm.leaf_cap);
       SHRK_CUDA(cudaGetLastError());
-      tree_level_advance_kernel<<<1, 1, 0, s>>>(b, L);
-      SHRK_CUDA(cudaGetLastError());
     }
-    add_launches(2 * (L1 - L0));
+    add_launches(L1 - L0);
     SHRK_CUDA(cudaMemcpyAsync(h_lev, b.levels, sizeof(h_lev), cudaMemcpyDeviceToHost, s));
     SHRK_CUDA(cudaStreamSynchronize(s));
     for (int L = L0 + 1; L <= L1; ++L)
@@ -850,17 +883,24 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
     le.push_back(h_lev[2 * L + 1]);
   }
   const int nn = le.back();
-  const int levels = (int)lb.size();
-  // 2. subtree sizes bottom-up, pre-order indices top-down
-  for (int L = levels - 1; L >= 0; --L) {
-    tree_size_kernel<<<blocks_for(le[L] - lb[L], BS), BS, 0, s>>>(b, lb[L], le[L]);
+  // 2. subtree sizes and pre-order indices from the leaves' start flags
+  //    (tree_order_kernel); the arrival counters hold the prefix meanwhile
+  {
+    LaunchScope ls("cheb_build", s);
+    SHRK_CUDA(cudaMemsetAsync(b.leafpre, 0, sizeof(int32_t) * ((size_t)ns + 1), s));
+    tree_leaf_flags_kernel<<<blocks_for(nn, BS), BS, 0, s>>>(b, nn);
     SHRK_CUDA(cudaGetLastError());
-  }
-  for (int L = 0; L < levels; ++L) {
-    tree_pre_kernel<<<blocks_for(le[L] - lb[L], BS), BS, 0, s>>>(b, lb[L], le[L]);
+    size_t temp_bytes = 0;
+    SHRK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, b.leafpre, b.arrive,
+                                            (int)(ns + 1), s));
+    void* temp = nullptr;
+    SHRK_TRY(scratch_get(28, std::max<size_t>(temp_bytes, 256), &temp));
+    SHRK_CUDA(cub::DeviceScan::ExclusiveSum(temp, temp_bytes, b.leafpre, b.arrive,
+                                            (int)(ns + 1), s));
+    tree_order_kernel<<<blocks_for(nn, BS), BS, 0, s>>>(b, nn, b.arrive);
     SHRK_CUDA(cudaGetLastError());
+    add_launches(3);  // flags, the scan's two kernels, order
   }
-  add_launches(2 * levels);
   // 3. flat arrays
   void* q = nullptr;
   SHRK_TRY(scratch_get(TREE_SLOTS + 0, sizeof(double) * 3 * (size_t)nn, &q));
@@ -884,7 +924,9 @@ shrk_status build_tree_gpu(const double* d_sorted, int64_t ns, const ChebParams&
   tb.le = le;
   tb.b = b;
   tb.k = k;
-  // 4. P2M at the leaves; 5. M2M from the deepest internal level up
+  // 4. P2M at the leaves; 5. M2M from the deepest internal level up (a
+  //    level-parallel launch per level: at this size the climbing form of
+  //    the small trees was measured 2.3x slower)
   return tree_weights(tb, d_sorted, nullptr, f.w, s);
 }
 
@@ -1113,7 +1155,8 @@ static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const Ch
   void* p64 = nullptr;
   void* p32 = nullptr;
   SHRK_TRY(scratch_get(25, sizeof(int64_t) * 2 * (size_t)cap, &p64));
-  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (6 * (size_t)cap + 8 + 2 * NLEV), &p32));
+  SHRK_TRY(scratch_get(26, sizeof(int32_t) * (8 * (size_t)cap + (size_t)ns + 2 + 8 + 2 * NLEV),
+                       &p32));
   BuildArrays b;
   b.blo = (int64_t*)p64;
   b.bhi = b.blo + cap;
@@ -1125,6 +1168,9 @@ static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const Ch
   b.levels = b.counter + 8;
   b.parent = b.levels + 2 * NLEV;
   b.arrive = b.parent + cap;
+  b.dep = b.arrive + cap;
+  b.rturn = b.dep + cap;
+  b.leafpre = b.rturn + cap;
   void* q = nullptr;
   SHRK_TRY(scratch_get(TREE_SLOTS + 0, sizeof(double) * 3 * (size_t)cap, &q));
   f.lo = (double*)q;
