@@ -217,7 +217,7 @@ def test_f32_precision_matches_oracle(oracle):
 
 
 def test_full_size_properties():
-    """p = 1e6 (BASELINE scale-up workload): size-independent checks.
+    """p = 1e6 (the exact scale-up workload, MP(c=0.5)): size-independent checks.
     * antisymmetry: sum_i Re S(lambda_i) = 0 up to rounding;
     * MIXED vs FP64 on the device: median relative difference <= 1e-9;
     * a sample of targets against the double-double truth on the host."""
