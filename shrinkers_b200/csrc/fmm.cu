@@ -550,7 +550,7 @@ constexpr uint32_t TC_IDESC = (1u << 4)           // D: F32
 constexpr int TC_WIN = TC_M + 6, TC_WS = 20;
 constexpr int TC_OS = FMM_MAXN + 1;  // output staging row stride (doubles)
 constexpr int TC_SMEM = 2 * TC_M * TC_K * 4 + 2 * TC_N * TC_K * 4 + 2 * TC_WIN * TC_WS * 4 +
-                        TC_WIN * 4 + 256;
+                        TC_WIN * 4 + 2 * FMM_MAXN * FMM_RS * 8 + TC_M * 4 + 256;
 static_assert(2 * TC_M * TC_OS * 8 <= 2 * TC_M * TC_K * 4, "output staging reuses A");
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -574,8 +574,14 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint6
       : "memory");
 }
 
+//
+// The level's L2L rides in the epilogue: each box adds T_side^T L_parent
+// (summed from zero in node order, then added, as l2l_box), so a level takes
+// one launch; the parent level is complete (levels run in order).
 __global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, int l,
-                                                      const int* __restrict__ box_key, int n,
+                                                      const int* __restrict__ box_key,
+                                                      const int* __restrict__ box_leaf,
+                                                      const int* __restrict__ id, int nl, int n,
                                                       Tabs tb, const double* __restrict__ Wm,
                                                       double* __restrict__ Lre,
                                                       double* __restrict__ Lim,
@@ -588,7 +594,9 @@ __global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, in
   float* Whi = reinterpret_cast<float*>(Blo + TC_N * TC_K / 4);
   float* Wlo = Whi + TC_WIN * TC_WS;
   int* skey = reinterpret_cast<int*>(Wlo + TC_WIN * TC_WS);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(skey + TC_WIN + (TC_WIN & 1));
+  double* sT = reinterpret_cast<double*>(skey + TC_WIN + (TC_WIN & 1));  // [side][i][v]
+  int* spar = reinterpret_cast<int*>(sT + 2 * FMM_MAXN * FMM_RS);  // 2 parent + side per row
+  uint64_t* bar = reinterpret_cast<uint64_t*>(spar + TC_M);
   uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(bar + 1);
   double* Ore = reinterpret_cast<double*>(tsm);  // after the MMAs: [row][TC_OS]
   double* Oim = Ore + TC_M * TC_OS;
@@ -623,6 +631,7 @@ __global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, in
     Bhi[kc * TC_N + c] = make_float4(h[0], h[1], h[2], h[3]);
     Blo[kc * TC_N + c] = make_float4(lo[0], lo[1], lo[2], lo[3]);
   }
+  load_side_tables(sT, tb, n);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -649,6 +658,7 @@ __global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, in
     const int64_t b = tb0 + t;
     const bool live = b < b1;
     const int kb = live ? skey[b - r0] : 0;
+    spar[t] = live ? 2 * (id[(int64_t)(l - 1 - 2) * nl + box_leaf[b]] - 1) + (kb & 1) : 0;
     for (int oi = 0; oi < 4; ++oi) {
       const int o = oi == 0 ? -3 : (oi == 1 ? -2 : (oi == 2 ? 2 : 3));
       // even kb: partners at o = 2, -2, -3; odd kb: o = 3, 2, -2
@@ -715,11 +725,28 @@ __global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, in
           : "r"(tmem + ((uint32_t)(warp * 32) << 16))
           : "memory");
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      // A is no longer read (the MMAs completed): stage the rows there
+      // A is no longer read (the MMAs completed): stage the rows there, each
+      // plus its L2L term (this thread's box: its parent's row in registers)
+      double lpr[FMM_MAXN], lpi[FMM_MAXN];
+      const int64_t par = spar[t] >> 1;
+      const double* T = sT + (spar[t] & 1) * n * (n | 1);
+#pragma unroll
+      for (int i = 0; i < FMM_MAXN; ++i) {
+        lpr[i] = (live && i < n) ? Lre[par * FMM_MAXN + i] : 0.0;
+        lpi[i] = (live && i < n) ? Lim[par * FMM_MAXN + i] : 0.0;
+      }
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        Ore[t * TC_OS + i] = (double)__uint_as_float(v[i]);
-        Oim[t * TC_OS + i] = (double)__uint_as_float(v[16 + i]);
+        double are = 0.0, aim = 0.0;
+#pragma unroll
+        for (int k = 0; k < FMM_MAXN; ++k)
+          if (k < n) {
+            const double tk = T[k * (n | 1) + i];
+            are = fma(tk, lpr[k], are);
+            aim = fma(tk, lpi[k], aim);
+          }
+        Ore[t * TC_OS + i] = (double)__uint_as_float(v[i]) + are;
+        Oim[t * TC_OS + i] = (double)__uint_as_float(v[16 + i]) + aim;
       }
     }
     __syncthreads();
@@ -742,32 +769,6 @@ __global__ void __launch_bounds__(TC_M) m2l_tc_kernel(int64_t b0, int64_t b1, in
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32u)
                  : "memory");
-  }
-}
-
-// L2L from level l to l+1: child box c gets T_side^T L_parent (added to the
-// child's M2L result).
-__global__ void __launch_bounds__(256) l2l_kernel(int64_t c0, int64_t c1,
-                                                  const int* __restrict__ box_key,
-                                                  const int* __restrict__ box_leaf,
-                                                  const int* __restrict__ id, int nl, int l, int n,
-                                                  Tabs tb, double* __restrict__ Lre,
-                                                  double* __restrict__ Lim) {
-  __shared__ double sT[2 * FMM_MAXN * FMM_RS];
-  load_side_tables(sT, tb, n);
-  __syncthreads();
-  const int lane = threadIdx.x & 15;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
-    if (c0 + 2 * w >= c1) break;
-    const int64_t c = c0 + 2 * w + ((threadIdx.x >> 4) & 1);
-    const bool live = c < c1;
-    double re, im;
-    l2l_box(c, live, box_key, box_leaf, id, nl, l, n, sT, Lre, Lim, lane, re, im);
-    if (live && lane < n) {
-      Lre[c * FMM_MAXN + lane] += re;
-      Lim[c * FMM_MAXN + lane] += im;
-    }
   }
 }
 
@@ -1060,22 +1061,12 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
                                      TC_SMEM));
       opted[dev] = true;
     }
-    {
-      LaunchScope ls("fmm_m2l_tc", s);
-      for (int l = K + 1; l <= L; ++l) {
-        const int64_t b0 = off[l - 2], b1 = off[l - 1];
-        m2l_tc_kernel<<<(unsigned)std::min<int64_t>(blocks(b1 - b0, TC_M), 2 * 148), TC_M,
-                        TC_SMEM, s>>>(b0, b1, l, box_key, n, tb, Wm, Lre, Lim,
-                                      device_error_word());
-        SHRK_CUDA(cudaGetLastError());
-      }
-      add_launches(L - K - 1);
-    }
-    LaunchScope ls("fmm_l2l", s);
-    for (int l = K; l < L; ++l) {
-      const int64_t c0 = off[l - 1], c1 = off[l];
-      l2l_kernel<<<half_grid(c1 - c0), 256, 0, s>>>(c0, c1, box_key, box_leaf, lid, nl, l, n, tb,
-                                                    Lre, Lim);
+    LaunchScope ls("fmm_m2l_tc", s);
+    for (int l = K + 1; l <= L; ++l) {
+      const int64_t b0 = off[l - 2], b1 = off[l - 1];
+      m2l_tc_kernel<<<(unsigned)std::min<int64_t>(blocks(b1 - b0, TC_M), 2 * 148), TC_M, TC_SMEM,
+                      s>>>(b0, b1, l, box_key, box_leaf, lid, nl, n, tb, Wm, Lre, Lim,
+                           device_error_word());
       SHRK_CUDA(cudaGetLastError());
     }
     add_launches(L - K - 1);
