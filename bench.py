@@ -665,6 +665,7 @@ def secondary(args, L, dev, ev, ev_h, eta, p, stream):
     out["fp64_ms"] = timed(lambda: run(0, r64, i64), 2)
     out["mixed_ms"] = timed(lambda: run(1, rmx, imx), 3)
     out["mixed_speedup_vs_fp64"] = out["fp64_ms"] / out["mixed_ms"]
+    torch.cuda.synchronize()  # results read back only after every launch has finished
     a64 = torch.complex(r64, i64)
     amx = torch.complex(rmx, imx)
     rel = (torch.abs(amx - a64) / torch.abs(a64)).cpu().numpy()
@@ -741,6 +742,7 @@ def secondary(args, L, dev, ev, ev_h, eta, p, stream):
     x5r = torch.empty(p5, dtype=torch.float64, device=dev)
     x5i = torch.empty_like(x5r)
     run(0, x5r, x5i, ev5, p5, e5)
+    torch.cuda.synchronize()
     ex5 = torch.complex(x5r, x5i)
     for name, mid in [("chebcode_fast", 14), ("chebcode", 13), ("chebcode_xtreme", 15),
                       ("nufft", 11)]:
@@ -749,6 +751,7 @@ def secondary(args, L, dev, ev, ev_h, eta, p, stream):
                                                    x5r.data_ptr(), x5i.data_ptr(),
                                                    stream.cuda_stream))
         ms = timed(call, 5)
+        torch.cuda.synchronize()
         rel = torch.abs(torch.complex(x5r, x5i) - ex5) / torch.abs(ex5)
         out[f"p1m_{name}_ms"] = ms
         out[f"p1m_{name}_rel_err_median"] = float(rel.median())
