@@ -202,15 +202,19 @@ shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src
     return SHRK_EINVAL;
   }
   const bool mixed = (precision == SHRK_PREC_MIXED);
-  // Fewer targets than one full tile (a query grid, a small spectrum): the
-  // 4-target tiles would leave most of each thread's work on padding and the
+  // Fewer targets than one full tile (a query grid), or a sum whose full-tile
+  // plan has fewer items than the GPU holds CTAs (a small spectrum): the
+  // 4-target tiles would leave most of each thread's work on padding or the
   // 1024-source splits would put the whole sum on a few CTAs, so such calls
   // take R_SMALL targets per thread and splits of SUB sources (plain loads,
   // still aligned to the mixed kernel's source blocks).
-  const bool small = nt < (int64_t)NT * (mixed ? R_MIXED : R_F64);
-  const int R = small ? (mixed ? R_SMALL_MIXED : R_SMALL_F64) : (mixed ? R_MIXED : R_F64);
-  const SplitPlan pl =
-      plan_splits(nt, ns, NT * R, small ? SUB : CH, mixed ? SHRK_MIXED_CTAS : 2);
+  const int Rbig = mixed ? R_MIXED : R_F64;
+  const int cps = mixed ? SHRK_MIXED_CTAS : 2;
+  const SplitPlan big = plan_splits(nt, ns, NT * Rbig, CH, cps);
+  const bool small =
+      nt < (int64_t)NT * Rbig || big.n_tiles * big.n_splits < (int64_t)sm_count() * cps;
+  const int R = small ? (mixed ? R_SMALL_MIXED : R_SMALL_F64) : Rbig;
+  const SplitPlan pl = small ? plan_splits(nt, ns, NT * R, SUB, cps) : big;
   void* part = nullptr;
   SHRK_TRY(scratch_get(0, sizeof(double) * 2 * (size_t)pl.n_splits * (size_t)nt, &part));
   double2* bounds = nullptr;
