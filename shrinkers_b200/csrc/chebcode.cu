@@ -112,6 +112,52 @@ __device__ __forceinline__ void tree_split_node(const double* __restrict__ sorte
   b.rturn[slot + 1] = b.rturn[i] + 1;
 }
 
+// A warp splits a node: its upper_bound of mid probes 32 evenly spaced
+// positions per step (the range shrinks 33-fold), then scans the last
+// <= 32 -- the index tree_split_node's binary search finds.
+__device__ __forceinline__ void tree_split_node_warp(const double* __restrict__ sorted,
+                                                     BuildArrays b, int i, int depth,
+                                                     int64_t leaf_cap, int lane) {
+  const int64_t lo_idx = b.blo[i], hi_idx = b.bhi[i];
+  if (hi_idx - lo_idx <= leaf_cap || depth >= MAX_TREE_DEPTH) {
+    if (lane == 0) b.lc[i] = b.rc[i] = -1;
+    return;
+  }
+  const double lo = sorted[lo_idx], hi = sorted[hi_idx - 1];
+  const double mid = lo + 0.5 * (hi - lo);
+  // invariant: sorted[< a] <= mid, sorted[>= e] > mid (or e = hi_idx)
+  int64_t a = lo_idx, e = hi_idx;
+  while (e - a > 32) {
+    const int64_t span = e - a;
+    const int64_t pos = a + span * (lane + 1) / 33;  // strictly increasing, in [a, e)
+    const unsigned gt = __ballot_sync(0xffffffffu, mid < sorted[pos]);
+    if (gt) {
+      const int f = __ffs(gt) - 1;  // first probe above mid
+      const int64_t pf = a + span * (f + 1) / 33, pprev = a + span * f / 33;
+      if (f > 0) a = pprev + 1;  // probe f - 1 was <= mid
+      e = pf;
+    } else {
+      a = a + span * 32 / 33 + 1;
+    }
+  }
+  const unsigned gt = __ballot_sync(0xffffffffu, a + lane < e && mid < sorted[a + lane]);
+  int64_t split = gt ? a + (__ffs(gt) - 1) : e;
+  if (split == lo_idx || split == hi_idx) split = (lo_idx + hi_idx) / 2;
+  if (lane == 0) {
+    const int slot = atomicAdd(b.counter, 2);
+    b.blo[slot] = lo_idx;
+    b.bhi[slot] = split;
+    b.blo[slot + 1] = split;
+    b.bhi[slot + 1] = hi_idx;
+    b.lc[i] = slot;
+    b.rc[i] = slot + 1;
+    b.parent[slot] = b.parent[slot + 1] = i;
+    b.dep[slot] = b.dep[slot + 1] = depth + 1;
+    b.rturn[slot] = b.rturn[i];
+    b.rturn[slot + 1] = b.rturn[i] + 1;
+  }
+}
+
 // Splits the nodes of level `depth` (its slot range read from b.levels, so
 // successive levels launch without host round trips).  The last CTA to
 // finish (a ticket taken after a fence) records the next level: exactly the
@@ -119,9 +165,17 @@ __device__ __forceinline__ void tree_split_node(const double* __restrict__ sorte
 __global__ void tree_split_kernel(const double* __restrict__ sorted, BuildArrays b, int depth,
                                   int64_t leaf_cap) {
   const int begin = b.levels[2 * depth], end = b.levels[2 * depth + 1];
-  for (int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x); i < end;
-       i += (int)(gridDim.x * blockDim.x))
-    tree_split_node(sorted, b, i, depth, leaf_cap);
+  const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+  if (end - begin <= nw) {
+    // few nodes (the upper levels, long ranges): a warp per node
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (begin + w < end) tree_split_node_warp(sorted, b, begin + w, depth, leaf_cap,
+                                              threadIdx.x & 31);
+  } else {
+    for (int i = begin + (int)(blockIdx.x * blockDim.x + threadIdx.x); i < end;
+         i += (int)(gridDim.x * blockDim.x))
+      tree_split_node(sorted, b, i, depth, leaf_cap);
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -197,45 +251,6 @@ __global__ void tree_fill_kernel(const double* __restrict__ sorted, BuildArrays 
 // (the range shrinks 33-fold), then scans the last <= 32 -- the same index as
 // tree_split_node's binary search, so the tree is identical.  The levels
 // table is left for the host to read once.
-__device__ __forceinline__ void tree_split_node_warp(const double* __restrict__ sorted,
-                                                     BuildArrays b, int i, int depth,
-                                                     int64_t leaf_cap, int lane) {
-  const int64_t lo_idx = b.blo[i], hi_idx = b.bhi[i];
-  if (hi_idx - lo_idx <= leaf_cap || depth >= MAX_TREE_DEPTH) {
-    if (lane == 0) b.lc[i] = b.rc[i] = -1;
-    return;
-  }
-  const double lo = sorted[lo_idx], hi = sorted[hi_idx - 1];
-  const double mid = lo + 0.5 * (hi - lo);
-  // invariant: sorted[< a] <= mid, sorted[>= e] > mid (or e = hi_idx)
-  int64_t a = lo_idx, e = hi_idx;
-  while (e - a > 32) {
-    const int64_t span = e - a;
-    const int64_t pos = a + span * (lane + 1) / 33;  // strictly increasing, in [a, e)
-    const unsigned gt = __ballot_sync(0xffffffffu, mid < sorted[pos]);
-    if (gt) {
-      const int f = __ffs(gt) - 1;  // first probe above mid
-      const int64_t pf = a + span * (f + 1) / 33, pprev = a + span * f / 33;
-      if (f > 0) a = pprev + 1;  // probe f - 1 was <= mid
-      e = pf;
-    } else {
-      a = a + span * 32 / 33 + 1;
-    }
-  }
-  const unsigned gt = __ballot_sync(0xffffffffu, a + lane < e && mid < sorted[a + lane]);
-  int64_t split = gt ? a + (__ffs(gt) - 1) : e;
-  if (split == lo_idx || split == hi_idx) split = (lo_idx + hi_idx) / 2;
-  if (lane == 0) {
-    const int slot = atomicAdd(b.counter, 2);
-    b.blo[slot] = lo_idx;
-    b.bhi[slot] = split;
-    b.blo[slot + 1] = split;
-    b.bhi[slot + 1] = hi_idx;
-    b.lc[i] = slot;
-    b.rc[i] = slot + 1;
-  }
-}
-
 constexpr int TOPO_NT = 1024;
 // Trees of at most this many leaf-capacities of sources (ns / leaf_cap) are
 // built by tree_topology_cta_kernel: a few hundred to ~2 000 nodes, where one
@@ -251,6 +266,9 @@ __global__ void __launch_bounds__(TOPO_NT, 1) tree_topology_cta_kernel(
     b.blo[0] = 0;
     b.bhi[0] = ns;
     b.pre[0] = 0;
+    b.parent[0] = -1;
+    b.dep[0] = 0;
+    b.rturn[0] = 0;
     *b.counter = 1;
     b.levels[0] = 0;
     b.levels[1] = 1;
