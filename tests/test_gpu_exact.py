@@ -144,11 +144,14 @@ def test_at_points_matches_oracle(oracle, nq, p):
     assert np.max(rel_err_pointwise(re, im, o_re, o_im)) < 1e-12
 
 
-@pytest.mark.parametrize("p,median_bar", [(1000, 1e-9), (20000, 2e-9), (50000, 1e-9)])
+@pytest.mark.parametrize("p,median_bar", [(1000, 1e-9), (4099, 2e-9), (12347, 2e-9),
+                                          (20000, 2e-9), (50000, 1e-9)])
 def test_mixed_precision_error_vs_truth(oracle, p, median_bar):
     """Median relative error of m vs the double-double truth: <= 1e-9 at the
-    workload sizes (p = 5e4, 1e6); at p = 2e4 the far field has fewer terms
-    to average and the bar is 2e-9."""
+    workload sizes (p = 5e4, 1e6); between them the far field has fewer terms
+    to average and the bar is 2e-9.  p = 1000 runs the one-partial-tile
+    decomposition, 4099 and 12347 the under-filled-plan one (two targets per
+    thread, 256-source splits), 2e4 and up the full tiles."""
     ev = spectra.config2(p)
     eta = 1.0 / math.sqrt(p)
     re, im = gpu_all(ev, eta, precision=MIXED)
