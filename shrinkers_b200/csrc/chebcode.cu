@@ -46,15 +46,17 @@ struct NodeF32 {
 //      mid, or the index midpoint when one side would be empty,
 //      chebcode.rs:347-388); children take slots from an atomic counter and
 //      are linked explicitly, so slot order does not matter;
-//   2. subtree sizes bottom-up, pre-order indices top-down (node, left
-//      subtree, right subtree -- the reference's flat layout);
+//   2. subtree sizes and pre-order indices (node, left subtree, right
+//      subtree -- the reference's flat layout): from a scan of the leaves'
+//      start flags for large trees, level by level in one CTA for small ones;
 //   3. flat arrays at the pre-order indices: bounds, acceptance radius,
 //      Chebyshev nodes c + l cos(j pi/(n-1)) (set_node_positions 268-278);
-//   4. P2M: one thread per leaf adds the barycentric rows of its sources in
-//      index order (fill_leaves 401-460);
-//   5. M2M: level by level from the deepest, one thread per internal node
-//      merges the left then the right child's node masses
-//      (merge_all_weights 474-506).
+//   4. P2M: a warp per leaf adds the barycentric rows of its sources in
+//      index order (fill_leaves 401-460), 32 rows per step;
+//   5. M2M: from the deepest level up, a warp per internal node merges the
+//      left then the right child's node masses (merge_all_weights 474-506)
+//      -- a launch per level for large trees, the P2M warps climbing from
+//      their leaves for small ones.
 // Every weight is accumulated in the reference's order with the same
 // operations (IEEE division, fused fma where it uses mul_add), so the tree is
 // identical to the sequential build.
