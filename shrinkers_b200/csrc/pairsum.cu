@@ -19,9 +19,10 @@
 //
 // MIXED (R = 4): a source block of 256 whose interval lies at least
 // max(K*eta, 1e-9) from all of the warp's targets is summed in FP32 on the
-// packed f32x2 pipe -- two targets x two sources per step, one unbiased
+// packed f32x2 pipe -- two targets x two sources per step, one MUFU
 // reciprocal per two sources (pairs32x4 in pairs.cuh), FP32 partials folded
-// into FP64 every 16 sources.  Every other pair (the near field, where the
+// into FP64 every 16 sources with the reciprocal's measured mean error taken
+// out at the fold.  Every other pair (the near field, where the
 // terms are large and d cancels) is summed in FP64, as are all reductions.
 #include "common.cuh"
 #include "epilogue.cuh"
