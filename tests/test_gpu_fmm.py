@@ -91,6 +91,22 @@ def test_unsorted_input_and_python_api(rk, oracle):
         rk.stieltjes_fmm(ev, eta=eta, order=3)
 
 
+@pytest.mark.parametrize("order", [10, 12])
+def test_tensor_core_m2l_lower_orders(order):
+    """The tensor-core M2L with its L2L epilogue at orders below 16 (padded
+    operands, n x n side matrices): the same ~1e-6 class against the FP64
+    M2L of the same order."""
+    p = 50_000
+    ev = spectra.config5(p)
+    eta = 1.0 / math.sqrt(p)
+    r64, i64 = fmm(ev, eta, order)
+    rtc, itc = fmm(ev, eta, order, m2l=1)
+    err = rel(rtc, itc, r64, i64)
+    assert np.all(np.isfinite(rtc)) and np.all(np.isfinite(itc))
+    assert np.median(err) < 2e-6, np.median(err)
+    assert err.max() < 1e-4, err.max()
+
+
 @pytest.mark.parametrize("p", [20_000, 200_000])
 def test_tensor_core_m2l(oracle, p):
     """M2L on the tensor cores (TF32 x3, FP32 accumulation): the same
