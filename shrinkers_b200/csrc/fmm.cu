@@ -162,8 +162,12 @@ struct Tabs {
 // reciprocals by rcp_f64, within an ulp), and a fixed reduce-scatter adds
 // the lanes: 16 shuffles leave the total of node i on lanes 2i and 2i + 1
 // (deterministic).  The node tables sit in shared memory (broadcast reads).
+// 128-thread blocks: at ~150 registers three fit per SM (one 256-thread
+// block did), and the kernel is bound by how many leaf warps stay resident.
+constexpr int P2M_NT = 128;
+
 template <int N>
-__global__ void __launch_bounds__(256) p2m_kernel(const double* __restrict__ s,
+__global__ void __launch_bounds__(P2M_NT) p2m_kernel(const double* __restrict__ s,
                                                   const int* __restrict__ leaf_key,
                                                   const int* __restrict__ leaf_start, int nl,
                                                   FmmGeom g, Tabs tb, int64_t leaf_box0,
@@ -1009,21 +1013,21 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
   const int64_t leaf_box0 = off[L - 2];
   {
     LaunchScope ls("fmm_p2m", s);
-    const unsigned nb = blocks((int64_t)nl * 32, 256);
+    const unsigned nb = blocks((int64_t)nl * 32, P2M_NT);
     switch (n) {
-      case 4: p2m_kernel<4><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 5: p2m_kernel<5><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 6: p2m_kernel<6><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 7: p2m_kernel<7><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 8: p2m_kernel<8><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 9: p2m_kernel<9><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 10: p2m_kernel<10><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 11: p2m_kernel<11><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 12: p2m_kernel<12><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 13: p2m_kernel<13><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 14: p2m_kernel<14><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      case 15: p2m_kernel<15><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
-      default: p2m_kernel<16><<<nb, 256, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 4: p2m_kernel<4><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 5: p2m_kernel<5><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 6: p2m_kernel<6><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 7: p2m_kernel<7><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 8: p2m_kernel<8><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 9: p2m_kernel<9><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 10: p2m_kernel<10><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 11: p2m_kernel<11><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 12: p2m_kernel<12><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 13: p2m_kernel<13><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 14: p2m_kernel<14><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      case 15: p2m_kernel<15><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
+      default: p2m_kernel<16><<<nb, P2M_NT, 0, s>>>(ds, leaf_key, leaf_start, nl, g, tb, leaf_box0, Wm); break;
     }
     SHRK_CUDA(cudaGetLastError());
   }
