@@ -130,24 +130,46 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ reference --
-def cpu_baseline_sample(ev, eta, seconds):
+def cpu_isa():
+    """x86-64-v3 build of the restatement when the host runs it (hardware
+    FMA, as the reference's published native builds have), else the v2 one."""
+    from oracle import oracle as O
+
+    return "v3" if O.host_has_v3() else "v2"
+
+
+def cpu_baseline_sample(ev, eta, seconds, shape="block", isa=None):
     """Time the reference's parallel all-points route (C++ restatement of
-    cacheblock.rs:1454-1513, every host thread) on a target sample sized to
-    about `seconds` of work; returns pairs/s and the sample description."""
+    cacheblock.rs:1286-1513 in its loop shape: 32-target blocks x source
+    quads, every host thread) on a target sample sized to about `seconds`
+    of work; returns pairs/s, the sample size, its time and the threads."""
     from oracle import oracle as O
 
     O.build()
+    isa = isa or cpu_isa()
     p = ev.size
-    probe = min(p, 64)
+    probe = min(p, 256)
     t0 = time.perf_counter()
-    O.tiled_targets(ev[:probe], ev, eta)
+    O.tiled_targets(ev[:probe], ev, eta, shape, isa)
     rate = probe * p / max(time.perf_counter() - t0, 1e-6)
     n = int(min(p, max(probe, rate * seconds / p)))
     idx = np.linspace(0, p - 1, n).astype(np.int64)
     t0 = time.perf_counter()
-    O.tiled_targets(ev[idx], ev, eta)
+    O.tiled_targets(ev[idx], ev, eta, shape, isa)
     dt = time.perf_counter() - t0
     return n * p / dt, n, dt, O.num_threads()
+
+
+def cpu_variants(ev, eta, seconds=2.0):
+    """Short timings of the restatement's other forms (pairs/s): the
+    reference's x86 build target (x86-64-v2, fma() out of line) and one
+    accumulation chain per target.  All forms give the same sums."""
+    out = {}
+    for shape, isa in [("block", "v2"), ("target", "v2"), ("target", cpu_isa())]:
+        key = f"{shape}_{isa}"
+        if key not in out:
+            out[key] = cpu_baseline_sample(ev, eta, seconds, shape, isa)[0]
+    return out
 
 
 def run_reference(args, world, rank):
@@ -167,15 +189,20 @@ def run_reference(args, world, rank):
     value = float(np.median(vals))
     n, dt = samples[-1]
     ms = p * p / value * 1e3
+    isa = cpu_isa()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"exact all-points transform, MP(c=0.5) p={p}, eta=1/sqrt(p)",
-                   "p": p, "route": "reference parallel all-points route (tiled full square)"},
+                   "p": p, "route": "reference parallel all-points route (tiled full square, "
+                                    "32-target blocks x source quads)", "isa": f"x86-64-{isa}"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{n} targets x {p} sources per step ({dt:.1f} s); "
-                                   "ms_per_step extrapolated to all p targets"},
+                         "sample": f"{n} targets x {p} sources per step ({dt:.1f} s), "
+                                   f"x86-64-{isa} build; ms_per_step extrapolated to all p "
+                                   "targets",
+                         "per_core": value / cores,
+                         "variants": cpu_variants(ev, eta)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -303,7 +330,10 @@ def run_ours(args, world, rank, local):
         cpu_rate, n, dt, cores = cpu_baseline_sample(ev_h, eta, args.cpu_seconds)
         cpu = {"value": cpu_rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{n} of {p} targets x {p} sources, {dt:.1f} s, reference parallel "
-                         "route restated in C++ (OpenMP)"}
+                         "route restated in C++ in its loop shape (32-target blocks x source "
+                         f"quads, OpenMP), x86-64-{cpu_isa()} build",
+               "per_core": cpu_rate / cores,
+               "variants": cpu_variants(ev_h, eta)}
 
     if pg:
         pg.barrier()

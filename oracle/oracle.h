@@ -44,6 +44,8 @@ void tiled_span_no_cutoff(const double* targets, size_t nt, const double* ev, si
 void tiled_one_target_pub(double t, const double* ev, size_t p, double eta, double eta_sq,
                           double* r, double* i);
 void tiled_parallel(const double* ev, size_t p, double eta, double* re, double* im);
+void tiled_blocks_parallel(const double* targets, size_t nt, const double* ev, size_t p,
+                           double eta, double* re, double* im);
 void blocked_at_points(const double* q, size_t nq, const double* ev, size_t p, double eta,
                        double cutoff, double* re, double* im);
 void windowed(const double* ev, size_t p, double eta, double cut, double* re, double* im);

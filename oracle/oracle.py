@@ -17,6 +17,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _SO = os.path.join(_HERE, "_build", "liboracle.so")
+# The same sources built for x86-64-v3 (hardware FMA, AVX2): identical
+# results, used only to time the CPU baseline on an FMA-capable host.
+_SO_V3 = os.path.join(_HERE, "_build", "liboracle_v3.so")
 
 # Method identifiers: declaration order of StieltjesMethod (src/config.rs:19-89).
 METHODS = [
@@ -36,19 +39,34 @@ _SZ = C.c_size_t
 
 def build(force: bool = False) -> str:
     """Compile the oracle with its Makefile (idempotent)."""
-    if force or not os.path.exists(_SO):
+    if force or not (os.path.exists(_SO) and os.path.exists(_SO_V3)):
         subprocess.run(["make", "-C", _HERE, "-s"], check=True)
     return _SO
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
+def host_has_v3() -> bool:
+    """True when this host's CPU runs x86-64-v3 code (AVX2 + FMA + BMI2)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((ln for ln in f if ln.startswith("flags")), "").split()
+    except OSError:
+        return False
+    return all(x in flags for x in ("avx2", "fma", "bmi2", "movbe"))
+
+
+def lib_v3():
+    """The x86-64-v3 build (same symbols, same results)."""
+    return lib(_SO_V3)
+
+
+def lib(path=None):
+    path = path or _SO
+    if path not in _libs:
         build()
-        L = C.CDLL(_SO)
+        L = C.CDLL(path)
         sig = {
             "orc_resolve_auto_method": (C.c_int, [C.c_int, C.c_int, _SZ]),
             "orc_grid_appropriate": (C.c_int, [C.c_int, _SZ, _SZ]),
@@ -62,6 +80,7 @@ def lib():
             "orc_compute_all": (C.c_int, [_D, _SZ, C.c_double, C.c_int, C.c_double, C.c_int, _D, _D]),
             "orc_compute_at_points": (C.c_int, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, C.c_double, C.c_int, _D, _D]),
             "orc_tiled_targets": (None, [_D, _SZ, _D, _SZ, C.c_double, _D, _D]),
+            "orc_tiled_targets_blocked": (None, [_D, _SZ, _D, _SZ, C.c_double, _D, _D]),
             "orc_all_f32": (None, [_F, _SZ, C.c_float, _F, _F]),
             "orc_with_deriv": (None, [_D, _SZ, C.c_double, _D, _D, _D, _D]),
             "orc_truth_points": (None, [_D, _SZ, _D, _SZ, C.c_double, _D, _D]),
@@ -104,8 +123,8 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def _d(a):
@@ -167,11 +186,18 @@ def tiled_full_square(ev, eta):
     return re, im
 
 
-def tiled_targets(targets, ev, eta):
-    """Parallel all-points route of the reference for a subset of targets (raw)."""
+def tiled_targets(targets, ev, eta, shape="block", isa="v2"):
+    """Parallel all-points route of the reference for a subset of targets (raw).
+
+    shape "block": the reference's loop shape (32-target blocks x source
+    quads, cacheblock.rs:1286-1424); "target": one accumulation chain per
+    target.  Both give the same sums bit for bit.  isa "v3" runs the
+    x86-64-v3 build (same results)."""
     t, ev = _arr(targets), _arr(ev)
     re, im = np.empty_like(t), np.empty_like(t)
-    lib().orc_tiled_targets(_d(t), t.size, _d(ev), ev.size, eta, _d(re), _d(im))
+    L = lib_v3() if isa == "v3" else lib()
+    f = L.orc_tiled_targets_blocked if shape == "block" else L.orc_tiled_targets
+    f(_d(t), t.size, _d(ev), ev.size, eta, _d(re), _d(im))
     return re, im
 
 

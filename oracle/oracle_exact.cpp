@@ -229,6 +229,78 @@ void tiled_one_target_pub(double t, const double* ev, size_t p, double eta, doub
   tiled_one_target(t, ev, p, eta, eta_sq, r, i);
 }
 
+// cacheblock.rs:1286-1424 with the reference's loop shape as well as its
+// order: a block of TILED_BS targets (cacheblock.rs:1433) advances together
+// over each quad of sources, four sources per target per step.  Each target
+// still meets its sources in ascending order, so the sums are those of
+// tiled_one_target bit for bit; the block's 32 accumulation chains and their
+// divisions are independent, which is where the reference's speed comes
+// from (the compiler vectorises the target loop when the ISA has FMA).
+// Positions past nb repeat the first target and are discarded.
+static const size_t TILED_BS = 32;
+
+static void tiled_block(const double* t, size_t nb, const double* ev, size_t p, double eta,
+                        double eta_sq, double* re, double* im) {
+  double x[TILED_BS], ar[TILED_BS], ai[TILED_BS];
+  for (size_t k = 0; k < TILED_BS; ++k) {
+    x[k] = t[k < nb ? k : 0];
+    ar[k] = 0.0;
+    ai[k] = 0.0;
+  }
+  size_t j = 0;
+  for (; j + 4 <= p; j += 4) {
+    const double l0 = ev[j], l1 = ev[j + 1], l2 = ev[j + 2], l3 = ev[j + 3];
+    for (size_t k = 0; k < TILED_BS; ++k) {
+      double r = ar[k], i = ai[k];
+      const double d0 = x[k] - l0;
+      const double v0 = 1.0 / std::fma(d0, d0, eta_sq);
+      r = std::fma(d0, v0, r);
+      i = std::fma(eta, v0, i);
+      const double d1 = x[k] - l1;
+      const double v1 = 1.0 / std::fma(d1, d1, eta_sq);
+      r = std::fma(d1, v1, r);
+      i = std::fma(eta, v1, i);
+      const double d2 = x[k] - l2;
+      const double v2 = 1.0 / std::fma(d2, d2, eta_sq);
+      r = std::fma(d2, v2, r);
+      i = std::fma(eta, v2, i);
+      const double d3 = x[k] - l3;
+      const double v3 = 1.0 / std::fma(d3, d3, eta_sq);
+      r = std::fma(d3, v3, r);
+      i = std::fma(eta, v3, i);
+      ar[k] = r;
+      ai[k] = i;
+    }
+  }
+  for (; j < p; ++j) {  // cacheblock.rs:1406-1423, the 1-3 trailing sources
+    const double lj = ev[j];
+    for (size_t k = 0; k < TILED_BS; ++k) {
+      const double d = x[k] - lj;
+      const double v = 1.0 / std::fma(d, d, eta_sq);
+      ar[k] = std::fma(d, v, ar[k]);
+      ai[k] = std::fma(eta, v, ai[k]);
+    }
+  }
+  for (size_t k = 0; k < nb; ++k) {
+    re[k] = ar[k];
+    im[k] = ai[k];
+  }
+}
+
+// cacheblock.rs:1454-1513 over blocks of TILED_BS targets on every host
+// thread (raw sums at `targets`).
+void tiled_blocks_parallel(const double* targets, size_t nt, const double* ev, size_t p,
+                           double eta, double* re, double* im) {
+  const double eta_sq = eta * eta;
+  const long nblk = (long)((nt + TILED_BS - 1) / TILED_BS);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long b = 0; b < nblk; ++b) {
+    const size_t t0 = (size_t)b * TILED_BS;
+    const size_t nb = std::min(TILED_BS, nt - t0);
+    tiled_block(targets + t0, nb, ev, p, eta, eta_sq, re + t0, im + t0);
+  }
+}
+
 // cacheblock.rs:1255-1278 tiled_span_no_cutoff (bs only groups targets).
 void tiled_span_no_cutoff(const double* targets, size_t nt, const double* ev, size_t p,
                           size_t /*bs*/, double eta, double* re, double* im) {
@@ -241,14 +313,9 @@ void tiled_span_no_cutoff(const double* targets, size_t nt, const double* ev, si
 }
 
 // cacheblock.rs:1454-1513: disjoint target spans over all host threads.
+// Same sums as tiled_one_target per target, taken in the block loop shape.
 void tiled_parallel(const double* ev, size_t p, double eta, double* re, double* im) {
-  const double eta_sq = eta * eta;
-#pragma omp parallel for schedule(dynamic, 32)
-  for (long k = 0; k < (long)p; ++k) {
-    re[k] = 0.0;
-    im[k] = 0.0;
-    tiled_one_target(ev[k], ev, p, eta, eta_sq, &re[k], &im[k]);
-  }
+  tiled_blocks_parallel(ev, p, ev, p, eta, re, im);
 }
 
 // cacheblock.rs:167-224 + at_points_inner_loop 236-437.  Per query the
@@ -655,5 +722,12 @@ void orc_tiled_targets(const double* targets, size_t nt, const double* ev, size_
     im[k] = 0.0;
     orc::tiled_one_target_pub(targets[k], ev, p, eta, eta_sq, &re[k], &im[k]);
   }
+}
+
+// The same sums in the reference's block loop shape (32 targets x source
+// quads, cacheblock.rs:1286-1424), the fast form of the route for timing.
+void orc_tiled_targets_blocked(const double* targets, size_t nt, const double* ev, size_t p,
+                               double eta, double* re, double* im) {
+  orc::tiled_blocks_parallel(targets, nt, ev, p, eta, re, im);
 }
 }

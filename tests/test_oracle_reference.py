@@ -132,6 +132,22 @@ def test_tiled_parallel_matches_sequential(oracle, p):
     assert np.max((np.abs(p_re - s_re) + np.abs(p_im - s_im)) / scale) < 1e-12
 
 
+@pytest.mark.parametrize("nt,p", [(1, 5), (31, 1001), (33, 2002), (100, 4003), (64, 4000)])
+def test_tiled_block_shape_is_bit_identical(oracle, nt, p):
+    """The block-shaped route (32-target blocks x source quads, the
+    reference's loop shape) gives every target the same sums as one chain
+    per target, in both ISA builds: ragged blocks and p % 4 tails included."""
+    ev = spectra.log_spectrum(p)
+    eta = 1.0 / np.sqrt(p)
+    t = ev[np.linspace(0, p - 1, nt).astype(np.int64)]
+    base = oracle.tiled_targets(t, ev, eta, "target", "v2")
+    isas = ["v2", "v3"] if oracle.host_has_v3() else ["v2"]
+    for shape in ["block", "target"]:
+        for isa in isas:
+            re, im = oracle.tiled_targets(t, ev, eta, shape, isa)
+            assert np.array_equal(re, base[0]) and np.array_equal(im, base[1]), (shape, isa)
+
+
 def test_with_deriv_matches_finite_difference(oracle):
     """autovec.rs:115-148."""
     p = 300
