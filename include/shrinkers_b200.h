@@ -5,11 +5,11 @@
  * (alexisrosuel/shrinkers).  Every entry point below names the reference
  * function it replaces (path:line inside the crate).  Plain pointers and
  * sizes only; no allocation is visible to the caller (device scratch is
- * cached per device inside the library); every function returns a status
- * code and never aborts.  Host-pointer entry points copy the inputs to the
- * device, run on a library-owned stream and copy the outputs back; `_dev`
- * entry points take device pointers and a cudaStream_t (as void*; NULL = the
- * legacy default stream) and are
+ * cached per device and stream inside the library); every function returns
+ * a status code and never aborts.  Host-pointer entry points copy the inputs
+ * to the device, run on a library-owned stream of the calling thread and
+ * copy the outputs back; `_dev` entry points take device pointers and a
+ * cudaStream_t (as void*; NULL = the legacy default stream) and are
  * stream-ordered (no host synchronisation unless stated).
  *
  * Conventions (identical to the reference):
@@ -75,6 +75,27 @@ size_t shrk_last_error(char* buf, size_t len);
 const char* shrk_version(void);
 /* Number of visible CUDA devices (0 when none); never fails. */
 int shrk_device_count(void);
+
+/* ------------------------------------------------ streams and state -- */
+/* Concurrency: calls are thread-safe.  Host-pointer entry points run on a
+ * stream of the calling host thread's own; `_dev` entry points on the
+ * stream they are given.  The library keeps its device scratch per (device,
+ * stream) -- per (device, host thread) for host-pointer calls -- so calls on
+ * different streams, from one host thread or several, run concurrently on
+ * the GPU; calls on one stream share scratch and run in stream order (the
+ * library serialises their host-side setup).
+ *
+ * shrk_stream_check: waits for `stream` (NULL = the legacy default stream)
+ * and reads and clears the device-side error word of the calls issued on
+ * it: SHRK_ETIMEOUT if a bounded device-side wait of an earlier `_dev` call
+ * on that stream gave up (its outputs are then unspecified), else SHRK_OK.
+ * Host-pointer entry points do this themselves before returning. */
+shrk_status shrk_stream_check(void* stream);
+/* Frees the device scratch and caches the library holds for calls on
+ * `stream` on the current device (after waiting for the stream); call it
+ * before destroying a stream the library was used with.  A later call on
+ * the stream allocates afresh. */
+shrk_status shrk_stream_release(void* stream);
 
 /* ---------------------------------------------------- method policy -- */
 /* python.rs:321-350 parse_method (all aliases).  SHRK_EINVAL on unknown. */
@@ -333,25 +354,6 @@ shrk_status shrk_deconvolve_spiked(const double* ev, size_t p, double c, size_t 
                                    int parallelism, double cutoff_ratio, size_t* k,
                                    double* spikes, double* spike_sample, double* bulk_edge,
                                    double* sigma2, double* out7);
-
-/* ------------------------------------------------------- profiling -- */
-/* Per-kernel CUDA-event timing of the library's own launches (off by
- * default).  shrk_timing_read returns the number of launches of the kernel
- * family `name` since the last reset and their summed duration (ms). */
-void shrk_timing_enable(int on);
-void shrk_timing_reset(void);
-shrk_status shrk_timing_read(const char* name, int64_t* launches, double* total_ms);
-/* Number of kernels the library launched since the last reset. */
-int64_t shrk_launch_count(void);
-/* Measured FMA issue rates of the current device (lane-operations per
- * second, one FMA = one op) for FP32 and FP64: the roofline denominators of
- * the exact kernels.  Runs two short probe kernels. */
-shrk_status shrk_measure_pipe_rates(double* fp32_ops_per_s, double* fp64_ops_per_s);
-/* Mean relative error of the FP32 MUFU reciprocal (rcp.approx.ftz.f32) of
- * the current device over every mantissa of [1, 2): plain and weighted 1/m
- * (log-uniform).  The mixed-precision pair kernel removes the log-uniform
- * mean from its FP32 far-field partials; this probe re-measures it. */
-shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean);
 
 #ifdef __cplusplus
 }

@@ -23,7 +23,8 @@ _SZ = C.c_size_t
 _ST = C.c_int
 _P = C.c_void_p
 
-# name -> (restype, argtypes).  Must list every symbol of include/shrinkers_b200.h.
+# name -> (restype, argtypes).  Must list every symbol of include/shrinkers_b200.h and
+# include/shrinkers_b200_diag.h.
 SIGNATURES = {
     "shrk_last_error": (_SZ, [C.c_char_p, _SZ]),
     "shrk_version": (C.c_char_p, []),
@@ -33,6 +34,8 @@ SIGNATURES = {
     "shrk_resolve_auto_method": (C.c_int, [C.c_int, C.c_int, _SZ]),
     "shrk_grid_appropriate": (C.c_int, [C.c_int, _SZ, _SZ]),
     "shrk_mixed_near_k": (C.c_double, []),
+    "shrk_stream_check": (_ST, [_P]),
+    "shrk_stream_release": (_ST, [_P]),
     "shrk_stieltjes_all": (_ST, [_D, _SZ, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, _D, _D]),
     "shrk_stieltjes_all_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, _P, _P, _P]),
     "shrk_stieltjes_all_f32": (_ST, [_F, _SZ, C.c_float, C.c_int, C.c_double, _F, _F]),
@@ -78,6 +81,7 @@ SIGNATURES = {
     "shrk_launch_count": (C.c_int64, []),
     "shrk_measure_pipe_rates": (_ST, [_D, _D]),
     "shrk_measure_rcp_bias": (_ST, [_D, _D]),
+    "shrk_diag_set_wait_limit": (C.c_longlong, [C.c_longlong]),
 }
 
 _lib = None

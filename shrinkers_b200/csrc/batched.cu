@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace shrk {
@@ -106,6 +107,7 @@ __global__ void __launch_bounds__(PAIR_NT, B_CTAS) batched_kernel(const BatchArg
     it.out_im = a.part_im + d.part_base + (int64_t)w.split * d.p;
     it.err = a.err;
     it.use_tma = ((uintptr_t)(it.src + it.s0) & 15u) == 0;
+    it.wait_cycles = WAIT_CYCLES_DEFAULT;
     const bool ok = d.R == 4 ? pair_item<MIXED, 4>(it, st, phase, pending)
                              : pair_item<MIXED, 2>(it, st, phase, pending);
     if (!ok) return;
@@ -149,6 +151,7 @@ struct Tune {
 constexpr int kMaxDev = 64;
 constexpr int64_t kMaxSpectrum = 1LL << 24;
 Tune g_tune[kMaxDev][2];
+std::mutex g_tune_mu[kMaxDev];  // guards g_tune[dev] (and its autotuning run)
 
 struct Plan {
   std::vector<SpecDesc> spec;
@@ -294,7 +297,8 @@ shrk_status enqueue(const Plan& pl, const DevBuffers& b, const double* d_ev, con
 
 int kernels_per_call(int precision) { return precision == SHRK_PREC_MIXED ? 3 : 2; }
 
-// One cached graph per device: the last plan.
+// One cached graph per call context (it reads that context's scratch slots):
+// the last plan.
 struct GraphCache {
   bool valid = false;
   std::vector<int64_t> offsets;
@@ -303,8 +307,10 @@ struct GraphCache {
   const void* ptrs[10] = {};
   PlanShape shape;
   cudaGraphExec_t exec = nullptr;
+  ~GraphCache() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
 };
-GraphCache g_graph[kMaxDev];
 
 int current_device() {
   int d = 0;
@@ -383,6 +389,7 @@ shrk_status batched_tune(int precision, bool force, int* table, cudaStream_t s) 
     set_error("device ordinal out of range");
     return SHRK_EINVAL;
   }
+  std::lock_guard<std::mutex> lk(g_tune_mu[dev]);
   Tune& t = g_tune[dev][precision];
   if (force || !t.tuned) SHRK_TRY(autotune(precision, t, s));
   if (table)
@@ -433,22 +440,27 @@ shrk_status batched(const double* d_ev, const int64_t* d_offsets, const int64_t*
     set_error("device ordinal out of range");
     return SHRK_EINVAL;
   }
-  Tune& t = g_tune[dev][precision];
-  if (!t.tuned) {
-    // SHRK_BATCHED_AUTOTUNE=0: keep the default table (plans, and so the
-    // split summation order, then do not depend on timing).
-    const char* env = std::getenv("SHRK_BATCHED_AUTOTUNE");
-    if (env && std::strcmp(env, "0") == 0) {
-      default_tune(t);
-      t.tuned = true;
-    } else {
-      SHRK_TRY(autotune(precision, t, s));
+  Tune t;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu[dev]);
+    Tune& tt = g_tune[dev][precision];
+    if (!tt.tuned) {
+      // SHRK_BATCHED_AUTOTUNE=0: keep the default table (plans, and so the
+      // split summation order, then do not depend on timing).
+      const char* env = std::getenv("SHRK_BATCHED_AUTOTUNE");
+      if (env && std::strcmp(env, "0") == 0) {
+        default_tune(tt);
+        tt.tuned = true;
+      } else {
+        SHRK_TRY(autotune(precision, tt, s));
+      }
     }
+    t = tt;
   }
 
   // Replay the cached graph when the plan (offsets, precision, tuning) and
   // every buffer it references are unchanged.
-  GraphCache& gc = g_graph[dev];
+  GraphCache& gc = ctx_state<GraphCache>(EXT_BATCHED_GRAPH);
   DevBuffers b;
   if (gc.valid && gc.precision == precision && gc.tune_version == t.version &&
       (int64_t)gc.offsets.size() == n + 1 &&

@@ -5,6 +5,7 @@
 // fftgrid.cu, chebcode.cu and batched.cu; there is no CPU fallback.
 #include "common.cuh"
 #include "internal.h"
+#include "../../include/shrinkers_b200_diag.h"
 
 #include <algorithm>
 #include <atomic>
@@ -13,6 +14,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -35,38 +37,136 @@ static shrk_status einval(const std::string& msg) {
   return SHRK_EINVAL;
 }
 
-// ------------------------------------------------------ device state --
-struct DeviceState {
-  bool init = false;
+// ---------------------------------------------------------- contexts --
+// A context holds what one stream of calls needs: the scratch slots, the
+// device error word and the modules' per-context caches (FFT tables, the
+// batched path's CUDA graph, the matrix path's handles).  Calls on one
+// context are serialised by its mutex (they share the scratch); calls on
+// different contexts run concurrently.  Host-pointer entry points use one
+// context per host thread and device, with a stream of its own; `_dev`
+// entry points use one context per (device, stream) they are given, so calls
+// on different streams never share scratch.
+constexpr int kExtSlots = 8;
+
+struct Context {
+  std::recursive_mutex mu;
+  int dev = 0;
   int sms = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // the stream of a host-thread context (owned)
+  bool host = false;
+  bool in_use = true;             // host-thread contexts: false once their thread exited
+  uintptr_t key = 0;              // `_dev` contexts: the stream handle
   Scratch slots[48];
   int* err = nullptr;
+  void* ext[kExtSlots] = {};
+  void (*ext_del[kExtSlots])(void*) = {};
+  // source_hint of the running host-pointer call
+  const double* hint_dev = nullptr;
+  int64_t hint_n = 0;
+  bool hint_sorted = false;
+  double hint_first = 0.0, hint_last = 0.0, hint_min = 0.0, hint_max = 0.0;
 };
 
-static std::mutex g_mu;  // serialises library calls (state + scratch reuse)
-static std::map<int, DeviceState> g_dev;
+static std::mutex g_ctx_mu;  // guards the registries below, not the contexts
+static std::map<std::pair<int, uintptr_t>, Context*> g_stream_ctx;
+static std::vector<Context*> g_host_ctx;
+static thread_local Context* t_cur = nullptr;  // the context of the running call
 
-static shrk_status current_state(DeviceState** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  DeviceState& st = g_dev[dev];
-  if (!st.init) {
-    SHRK_CUDA(cudaDeviceGetAttribute(&st.sms, cudaDevAttrMultiProcessorCount, dev));
-    SHRK_CUDA(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
-    SHRK_CUDA(cudaMalloc(&st.err, sizeof(int)));
-    SHRK_CUDA(cudaMemset(st.err, 0, sizeof(int)));
-    st.init = true;
+// The calling thread's host contexts; on thread exit they become free for
+// the next thread that needs one on that device (no CUDA call at exit).
+struct ThreadContexts {
+  std::map<int, Context*> by_dev;
+  ~ThreadContexts() {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    for (auto& kv : by_dev) kv.second->in_use = false;
   }
-  *out = &st;
+};
+static thread_local ThreadContexts t_host;
+
+static shrk_status init_context(Context* c, int dev, bool host) {
+  c->dev = dev;
+  c->host = host;
+  SHRK_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, dev));
+  if (host) SHRK_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  SHRK_CUDA(cudaMalloc(&c->err, sizeof(int)));
+  SHRK_CUDA(cudaMemset(c->err, 0, sizeof(int)));
   return SHRK_OK;
 }
 
-static DeviceState* g_cur = nullptr;  // valid while g_mu is held
+static shrk_status host_context(Context** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  auto it = t_host.by_dev.find(dev);
+  if (it != t_host.by_dev.end()) {
+    *out = it->second;
+    return SHRK_OK;
+  }
+  Context* c = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    for (Context* x : g_host_ctx)
+      if (!x->in_use && x->dev == dev) {
+        x->in_use = true;
+        c = x;
+        break;
+      }
+  }
+  if (!c) {
+    std::unique_ptr<Context> n(new Context());
+    SHRK_TRY(init_context(n.get(), dev, true));
+    c = n.release();
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    g_host_ctx.push_back(c);
+  }
+  t_host.by_dev[dev] = c;
+  *out = c;
+  return SHRK_OK;
+}
+
+static shrk_status stream_context(const void* stream, Context** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  const auto key = std::make_pair(dev, (uintptr_t)stream);
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = g_stream_ctx.find(key);
+    if (it != g_stream_ctx.end()) {
+      *out = it->second;
+      return SHRK_OK;
+    }
+  }
+  std::unique_ptr<Context> n(new Context());
+  n->key = (uintptr_t)stream;
+  SHRK_TRY(init_context(n.get(), dev, false));
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  auto ins = g_stream_ctx.emplace(key, n.get());
+  if (ins.second) {
+    *out = n.release();
+  } else {  // another thread registered it first
+    cudaFree(n->err);
+    *out = ins.first->second;
+  }
+  return SHRK_OK;
+}
+
+// Frees everything a context holds on the device (its mutex held).
+static void release_context_memory(Context* c) {
+  for (auto& sl : c->slots) {
+    if (sl.ptr) cudaFree(sl.ptr);
+    sl.ptr = nullptr;
+    sl.bytes = 0;
+  }
+  for (int k = 0; k < kExtSlots; ++k) {
+    if (c->ext[k] && c->ext_del[k]) c->ext_del[k](c->ext[k]);
+    c->ext[k] = nullptr;
+    c->ext_del[k] = nullptr;
+  }
+}
 
 shrk_status scratch_get(int slot, size_t bytes, void** out) {
-  Scratch& s = g_cur->slots[slot];
+  Scratch& s = t_cur->slots[slot];
   if (s.bytes < bytes) {
     if (s.ptr) {
       cudaError_t e = cudaFree(s.ptr);
@@ -83,16 +183,56 @@ shrk_status scratch_get(int slot, size_t bytes, void** out) {
   return SHRK_OK;
 }
 
-int* device_error_word() { return g_cur->err; }
-int sm_count() { return g_cur ? g_cur->sms : 148; }
-cudaStream_t library_stream() { return g_cur->stream; }
+void* ctx_ext(int k, void* (*make)(), void (*del)(void*)) {
+  Context* c = t_cur;
+  if (!c->ext[k]) {
+    c->ext[k] = make();
+    c->ext_del[k] = del;
+  }
+  return c->ext[k];
+}
 
-shrk_status check_device_error(cudaStream_t s) {
+void set_source_hint(const double* d_src, const double* h_src, int64_t n) {
+  Context* c = t_cur;
+  if (!c || n <= 0) return;
+  bool sorted = true;
+  double mn = h_src[0], mx = h_src[0];
+  for (int64_t i = 1; i < n; ++i) {
+    if (!(h_src[i - 1] <= h_src[i])) sorted = false;
+    mn = std::min(mn, h_src[i]);
+    mx = std::max(mx, h_src[i]);
+  }
+  c->hint_dev = d_src;
+  c->hint_n = n;
+  c->hint_sorted = sorted;
+  c->hint_first = h_src[0];
+  c->hint_last = h_src[n - 1];
+  c->hint_min = mn;
+  c->hint_max = mx;
+}
+
+bool source_hint(const double* d_src, int64_t n, bool* sorted, double* first, double* last,
+                 double* lo, double* hi) {
+  Context* c = t_cur;
+  if (!c || c->hint_dev != d_src || c->hint_n != n || !d_src) return false;
+  *sorted = c->hint_sorted;
+  *first = c->hint_first;
+  *last = c->hint_last;
+  if (lo) *lo = c->hint_min;
+  if (hi) *hi = c->hint_max;
+  return true;
+}
+
+int* device_error_word() { return t_cur->err; }
+int sm_count() { return t_cur ? t_cur->sms : 148; }
+cudaStream_t library_stream() { return t_cur->stream; }
+
+static shrk_status check_error_word(Context* c, cudaStream_t s) {
   int h = 0;
-  SHRK_CUDA(cudaMemcpyAsync(&h, g_cur->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
   if (h != DEV_ERR_NONE) {
-    SHRK_CUDA(cudaMemsetAsync(g_cur->err, 0, sizeof(int), s));
+    SHRK_CUDA(cudaMemsetAsync(c->err, 0, sizeof(int), s));
     SHRK_CUDA(cudaStreamSynchronize(s));
     if (h == DEV_ERR_TIMEOUT) {
       set_error("a bounded device-side wait gave up (timeout)");
@@ -104,9 +244,12 @@ shrk_status check_device_error(cudaStream_t s) {
   return SHRK_OK;
 }
 
+shrk_status check_device_error(cudaStream_t s) { return check_error_word(t_cur, s); }
+
 // ------------------------------------------------------------ timing --
 static std::atomic<int64_t> g_launches{0};
-static bool g_timing = false;
+static std::atomic<bool> g_timing{false};
+static std::mutex g_timing_mu;  // guards g_timed
 struct TimedLaunch { std::string family; cudaEvent_t a, b; };
 static std::vector<TimedLaunch> g_timed;
 
@@ -123,6 +266,7 @@ LaunchScope::LaunchScope(const char* fam, cudaStream_t s) : family(fam), stream(
 LaunchScope::~LaunchScope() {
   if (start) {
     cudaEventRecord(stop, stream);
+    std::lock_guard<std::mutex> lk(g_timing_mu);
     g_timed.push_back({family, start, stop});
   }
 }
@@ -358,8 +502,7 @@ static void detect_debias_split(const double* ev, size_t p, double gamma, double
 // Ledoit-Wolf xi on the device for host ev (estimation.rs:75-90).
 static shrk_status lw_device(const double* ev, size_t p, double c, int method, int precision,
                              int parallelism, double eta, double* xi) {
-  DeviceState* st = g_cur;
-  cudaStream_t s = st->stream;
+  cudaStream_t s = t_cur->stream;
   int m = resolve(method, parallelism, p);
   if (std::isnan(eta)) eta = 0.4 / std::sqrt((double)p);  // mod.rs:150-153
   void* dev = nullptr;
@@ -367,6 +510,7 @@ static shrk_status lw_device(const double* ev, size_t p, double c, int method, i
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * p, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   Epilogue epi;
   epi.mode = EPI_LW;
   epi.scale = 1.0 / (double)p;
@@ -383,7 +527,7 @@ static shrk_status deconv_device(const double* ev, size_t p, double c, size_t n_
                                  double lmin, double lmax, int method, int precision,
                                  int parallelism, double cutoff, double* out7) {
   if (p == 0) return SHRK_OK;
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   double eta_val = std::isnan(eta) ? 0.1 / std::sqrt((double)p) : eta;
   double mn = INFINITY, mx = -INFINITY;
   for (size_t i = 0; i < p; ++i) {
@@ -408,6 +552,7 @@ static shrk_status deconv_device(const double* ev, size_t p, double c, size_t n_
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 6 * n_points, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   SHRK_TRY(h2d(dq, grid, sizeof(double) * n_points, s));
   Epilogue epi;
   epi.mode = EPI_MP;
@@ -421,19 +566,55 @@ static shrk_status deconv_device(const double* ev, size_t p, double c, size_t n_
   return check_device_error(s);
 }
 
+// Selects and locks the context of a call for its lifetime: Guard() the
+// calling thread's host context (host-pointer entry points), Guard(stream)
+// the context of (current device, stream) (`_dev` entry points).  Nested
+// calls on the same context are allowed (the mutex is recursive); the
+// previous context is restored on exit.
 struct Guard {
-  std::lock_guard<std::mutex> lk;
+  Context* prev = t_cur;
+  Context* ctx = nullptr;
   shrk_status st;
-  Guard() : lk(g_mu) { st = current_state(&g_cur); }
+  std::unique_lock<std::recursive_mutex> lk;
+  Guard() { st = host_context(&ctx); enter(); }
+  explicit Guard(const void* stream) { st = stream_context(stream, &ctx); enter(); }
+  ~Guard() { t_cur = prev; }
+  Guard(const Guard&) = delete;
+  Guard& operator=(const Guard&) = delete;
+
+ private:
+  void enter() {
+    if (st != SHRK_OK) return;
+    lk = std::unique_lock<std::recursive_mutex>(ctx->mu);
+    t_cur = ctx;
+    ctx->hint_dev = nullptr;  // a hint never outlives the call that set it
+  }
 };
 
+// lib_enter / lib_exit: the host context of the calling thread, as a stack
+// of (previous context, entered context) pairs.
+static thread_local std::vector<std::pair<Context*, Context*>> t_lib_stack;
+
 shrk_status lib_enter(cudaStream_t* stream) {
-  g_mu.lock();
-  shrk_status st = current_state(&g_cur);
-  *stream = st == SHRK_OK ? g_cur->stream : nullptr;
-  return st;
+  Context* c = nullptr;
+  shrk_status st = host_context(&c);
+  if (st != SHRK_OK) c = nullptr;
+  t_lib_stack.emplace_back(t_cur, c);
+  *stream = nullptr;
+  if (!c) return st;
+  c->mu.lock();
+  t_cur = c;
+  *stream = c->stream;
+  return SHRK_OK;
 }
-void lib_exit() { g_mu.unlock(); }
+
+void lib_exit() {
+  if (t_lib_stack.empty()) return;
+  const auto top = t_lib_stack.back();
+  t_lib_stack.pop_back();
+  if (top.second) top.second->mu.unlock();
+  t_cur = top.first;
+}
 
 }  // namespace shrk
 
@@ -540,7 +721,7 @@ shrk_status shrk_stieltjes_all_dev(const double* d_ev, size_t p, double eta, int
                                    double* d_im, void* stream) {
   SHRK_TRY(check_common(p, eta, method, precision));
   SHRK_TRY(check_cutoff(cutoff));
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
   int m = resolve(method, parallelism, p);
@@ -559,13 +740,14 @@ shrk_status shrk_stieltjes_all(const double* ev, size_t p, double eta, int metho
   SHRK_TRY(check_cutoff(cutoff));
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   int m = resolve(method, parallelism, p);
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   Epilogue epi;
   epi.mode = EPI_SUMS;
   epi.scale = 1.0 / (double)p;
@@ -599,7 +781,7 @@ shrk_status shrk_stieltjes_all_f32(const float* ev, size_t p, float eta, int met
   }
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(float) * p, &dev));
   void* out = nullptr;
@@ -618,7 +800,7 @@ shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const dou
   SHRK_TRY(check_common(p, eta, method, precision));
   SHRK_TRY(check_cutoff(cutoff));
   if (nq == 0) return SHRK_OK;
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
   const bool par = parallelism == SHRK_PAR_PARALLEL;
@@ -641,7 +823,7 @@ shrk_status shrk_stieltjes_at_points(const double* q, size_t nq, const double* e
   if (nq == 0) return SHRK_OK;
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   const bool par = parallelism == SHRK_PAR_PARALLEL;
   int m = method;
   if (is_auto(m)) m = shrk_grid_appropriate(shrk_resolve_auto_method(m, par, p), p, nq);
@@ -652,6 +834,7 @@ shrk_status shrk_stieltjes_at_points(const double* q, size_t nq, const double* e
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 2 * nq, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   SHRK_TRY(h2d(dq, q, sizeof(double) * nq, s));
   Epilogue epi;
   epi.mode = EPI_SUMS;
@@ -670,12 +853,13 @@ shrk_status shrk_stieltjes_with_deriv(const double* ev, size_t p, double eta, do
   SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, SHRK_PREC_F64));
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 4 * p, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   double* o = (double*)out;
   SHRK_TRY(with_deriv((const double*)dev, (int64_t)p, eta, o, o + p, o + 2 * p, o + 3 * p, s));
   SHRK_TRY(d2h(re, o, sizeof(double) * p, s));
@@ -691,7 +875,7 @@ shrk_status shrk_stieltjes_batched_dev(const double* d_ev, const int64_t* d_offs
   if (n_spectra == 0) return SHRK_OK;
   if (precision != SHRK_PREC_F64 && precision != SHRK_PREC_MIXED)
     return einval("unknown precision id");
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
   return batched(d_ev, d_offsets, nullptr, (int64_t)n_spectra, d_eta, precision, d_re, d_im, s);
@@ -712,7 +896,7 @@ shrk_status shrk_stieltjes_batched(const double* ev, const int64_t* offsets, siz
   const size_t total = (size_t)offsets[n_spectra];
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * total, &dev));
   void* out = nullptr;
@@ -736,17 +920,17 @@ shrk_status shrk_batched_autotune(int precision, int force, int32_t* table) {
   Guard g;
   SHRK_TRY(g.st);
   int t[16];
-  SHRK_TRY(batched_tune(precision, force != 0, t, g_cur->stream));
+  SHRK_TRY(batched_tune(precision, force != 0, t, t_cur->stream));
   if (table)
     for (int i = 0; i < 16; ++i) table[i] = t[i];
-  return check_device_error(g_cur->stream);
+  return check_device_error(t_cur->stream);
 }
 
 shrk_status shrk_stieltjes_adjoint_dev(const double* d_ev, size_t p, double eta,
                                        const double* d_gre, const double* d_gim, int precision,
                                        double* d_grad, void* stream) {
   SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, precision));
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
   return adjoint(d_ev, (int64_t)p, eta, d_gre, d_gim, precision, d_grad, s);
@@ -766,7 +950,7 @@ shrk_status shrk_chebcode_evaluate_many_dev(const double* d_ev, size_t p, const 
   if (n_eta == 0) return SHRK_OK;
   ChebParams prm;
   SHRK_TRY(check_cheb_method(method, &prm));
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   return chebcode_evaluate_many(d_ev, (int64_t)p, d_etas, (int64_t)n_eta, prm, d_re, d_im,
                                 (cudaStream_t)stream);
@@ -784,13 +968,14 @@ shrk_status shrk_chebcode_evaluate_many(const double* ev, size_t p, const double
   SHRK_TRY(check_cheb_method(method, &prm));
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * (p + n_eta), &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p * n_eta, &out));
   double* d = (double*)dev;
   SHRK_TRY(h2d(d, ev, sizeof(double) * p, s));
+  set_source_hint(d, ev, (int64_t)p);
   SHRK_TRY(h2d(d + p, etas, sizeof(double) * n_eta, s));
   double* o = (double*)out;
   SHRK_TRY(chebcode_evaluate_many(d, (int64_t)p, d + p, (int64_t)n_eta, prm, o, o + p * n_eta,
@@ -806,7 +991,7 @@ shrk_status shrk_stieltjes_adjoint_treecode_dev(const double* d_ev, size_t p, do
   SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, SHRK_PREC_F64));
   ChebParams prm;
   SHRK_TRY(check_cheb_method(method, &prm));
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   cudaStream_t s = (cudaStream_t)stream;  // null = the legacy default stream
   return chebcode_adjoint(d_ev, (int64_t)p, eta, d_gre, d_gim, prm, d_grad, s);
@@ -820,13 +1005,14 @@ shrk_status shrk_stieltjes_adjoint_treecode(const double* ev, size_t p, double e
   SHRK_TRY(check_cheb_method(method, &prm));
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * 3 * p, &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * p, &out));
   double* d = (double*)dev;
   SHRK_TRY(h2d(d, ev, sizeof(double) * p, s));
+  set_source_hint(d, ev, (int64_t)p);
   SHRK_TRY(h2d(d + p, g_re, sizeof(double) * p, s));
   SHRK_TRY(h2d(d + 2 * p, g_im, sizeof(double) * p, s));
   SHRK_TRY(chebcode_adjoint(d, (int64_t)p, eta, d + p, d + 2 * p, prm, (double*)out, s));
@@ -839,13 +1025,14 @@ shrk_status shrk_stieltjes_adjoint(const double* ev, size_t p, double eta, const
   SHRK_TRY(check_common(p, eta, SHRK_M_BLOCKED, precision));
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * 3 * p, &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * p, &out));
   double* d = (double*)dev;
   SHRK_TRY(h2d(d, ev, sizeof(double) * p, s));
+  set_source_hint(d, ev, (int64_t)p);
   SHRK_TRY(h2d(d + p, g_re, sizeof(double) * p, s));
   SHRK_TRY(h2d(d + 2 * p, g_im, sizeof(double) * p, s));
   SHRK_TRY(adjoint(d, (int64_t)p, eta, d + p, d + 2 * p, precision, (double*)out, s));
@@ -898,7 +1085,7 @@ shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int
                                    double* d_re, double* d_im, void* stream) {
   SHRK_TRY(check_fmm(p, eta, order));
   if (m2l != 0 && m2l != 1) return einval("fmm: m2l must be 0 (FP64) or 1 (tensor cores, TF32 x3)");
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   return fmm_all(d_ev, (int64_t)p, eta, order, m2l, d_re, d_im, (cudaStream_t)stream);
 }
@@ -909,12 +1096,13 @@ shrk_status shrk_stieltjes_fmm(const double* ev, size_t p, double eta, int order
   if (m2l != 0 && m2l != 1) return einval("fmm: m2l must be 0 (FP64) or 1 (tensor cores, TF32 x3)");
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   SHRK_TRY(fmm_all((const double*)dev, (int64_t)p, eta, order, m2l, (double*)out,
                    (double*)out + p, s));
   SHRK_TRY(d2h(out_re, out, sizeof(double) * p, s));
@@ -927,7 +1115,7 @@ shrk_status shrk_stieltjes_scaled_ray_dev(const double* d_ev, size_t p, double s
   if (p == 0) return einval("eigenvalues must be non-empty");
   if (!(std::isfinite(scale) && scale > 0.0))
     return einval("scale must be a positive finite number");
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   return scaled_ray_sums(d_ev, (int64_t)p, scale, d_re, d_im, (cudaStream_t)stream);
 }
@@ -939,12 +1127,13 @@ shrk_status shrk_stieltjes_scaled_ray(const double* ev, size_t p, double scale, 
     return einval("scale must be a positive finite number");
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   SHRK_TRY(scaled_ray_sums((const double*)dev, (int64_t)p, scale, (double*)out,
                            (double*)out + p, s));
   SHRK_TRY(d2h(raw_re, out, sizeof(double) * p, s));
@@ -968,7 +1157,7 @@ shrk_status shrk_stieltjes_fft5_with_options_dev(const double* d_ev, size_t p, d
                                                  double pad_eta_mult, double pad_range_frac,
                                                  double* d_re, double* d_im, void* stream) {
   SHRK_TRY(check_fft5_opts(p, eta, order, pad_eta_mult, pad_range_frac));
-  Guard g;
+  Guard g(stream);
   SHRK_TRY(g.st);
   cudaStream_t s = (cudaStream_t)stream;
   const double* ds = nullptr;
@@ -994,12 +1183,13 @@ shrk_status shrk_stieltjes_fft5_with_options(const double* ev, size_t p, double 
   SHRK_TRY(check_fft5_opts(p, eta, order, pad_eta_mult, pad_range_frac));
   Guard g;
   SHRK_TRY(g.st);
-  cudaStream_t s = g_cur->stream;
+  cudaStream_t s = t_cur->stream;
   void* dev = nullptr;
   SHRK_TRY(scratch_get(3, sizeof(double) * p, &dev));
   void* out = nullptr;
   SHRK_TRY(scratch_get(4, sizeof(double) * 2 * p, &out));
   SHRK_TRY(h2d(dev, ev, sizeof(double) * p, s));
+  set_source_hint((const double*)dev, ev, (int64_t)p);
   const double* ds = nullptr;
   double first = 0.0, last = 0.0;
   SHRK_TRY(sorted_sources((const double*)dev, (int64_t)p, &ds, &first, &last, s));
@@ -1169,14 +1359,40 @@ shrk_status shrk_deconvolve_spiked(const double* ev, size_t p, double c, size_t 
                        precision, parallelism, cutoff, out7);
 }
 
-// ------------------------------------------------------- profiling --
-void shrk_timing_enable(int on) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  g_timing = on != 0;
+// --------------------------------------------------------- streams --
+shrk_status shrk_stream_check(void* stream) {
+  Guard g(stream);
+  SHRK_TRY(g.st);
+  return check_error_word(g.ctx, (cudaStream_t)stream);
 }
 
+shrk_status shrk_stream_release(void* stream) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  Context* c = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = g_stream_ctx.find(std::make_pair(dev, (uintptr_t)stream));
+    if (it == g_stream_ctx.end()) return SHRK_OK;
+    c = it->second;
+    g_stream_ctx.erase(it);
+  }
+  // No call can enter the context any more; wait for the one that may run.
+  std::lock_guard<std::recursive_mutex> lk(c->mu);
+  e = cudaStreamSynchronize((cudaStream_t)stream);
+  release_context_memory(c);
+  if (c->err) cudaFree(c->err);
+  c->err = nullptr;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize(release)");
+  return SHRK_OK;
+}
+
+// ------------------------------------------------------- profiling --
+void shrk_timing_enable(int on) { g_timing = on != 0; }
+
 void shrk_timing_reset(void) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_timing_mu);
   for (auto& t : g_timed) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
@@ -1186,7 +1402,7 @@ void shrk_timing_reset(void) {
 }
 
 shrk_status shrk_timing_read(const char* name, int64_t* launches, double* total_ms) {
-  std::lock_guard<std::mutex> lk(g_mu);
+  std::lock_guard<std::mutex> lk(g_timing_mu);
   int64_t n = 0;
   double ms = 0.0;
   for (auto& t : g_timed) {
@@ -1217,5 +1433,7 @@ shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean) {
   if (!uniform_mean || !log_mean) return einval("null output pointer");
   return measure_rcp_bias(uniform_mean, log_mean);
 }
+
+long long shrk_diag_set_wait_limit(long long cycles) { return set_wait_cycles(cycles); }
 
 }  // extern "C"

@@ -35,7 +35,27 @@ struct Scratch {
   size_t bytes = 0;
 };
 shrk_status scratch_get(int slot, size_t bytes, void** out);  // slot in [0, 48)
-int* device_error_word();  // zeroed per call by the launchers that use it
+// Per-context module state: the object in slot k (a CtxExt) of the running
+// call's context, made by `make` on first use and deleted by `del` when the
+// context is released.  Contexts are never shared by concurrent calls.
+enum CtxExt : int { EXT_FFT_TABLES = 0, EXT_BATCHED_GRAPH = 1, EXT_MATRIX_HANDLES = 2 };
+void* ctx_ext(int k, void* (*make)(), void (*del)(void*));
+template <typename T>
+T& ctx_state(int k) {
+  return *static_cast<T*>(
+      ctx_ext(k, []() -> void* { return new T(); }, [](void* q) { delete static_cast<T*>(q); }));
+}
+int* device_error_word();  // the running call's context; cleared when a host call reads it
+
+// Host-side facts about a source array a host-pointer entry point has just
+// uploaded (sortedness, first and last entry in the caller's order), so the
+// methods that need sorted sources skip the device check and its read-back.
+// Valid for the running call only (cleared when a host-pointer call enters).
+void set_source_hint(const double* d_src, const double* h_src, int64_t n);
+// lo / hi (optional): the smallest and largest entry.  NaN input makes the
+// array unsorted (the comparison v[i-1] <= v[i] fails), as on the device.
+bool source_hint(const double* d_src, int64_t n, bool* sorted, double* first, double* last,
+                 double* lo = nullptr, double* hi = nullptr);
 int sm_count();
 cudaStream_t library_stream();
 
@@ -98,10 +118,16 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// Default budget of a bounded wait: 2e9 clock cycles, about a second.
+constexpr long long WAIT_CYCLES_DEFAULT = 2000000000LL;
+
 // Bounded wait on an mbarrier phase: gives up after `max_cycles` clock
-// cycles (about a second at the default limit) and returns false.
+// cycles (about a second at the default limit) and returns false.  A budget
+// of zero or less gives up at once without looking at the barrier (the
+// failure path's test setting).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
-                                          long long max_cycles = 2000000000LL) {
+                                          long long max_cycles = WAIT_CYCLES_DEFAULT) {
+  if (max_cycles <= 0) return false;
   const uint32_t addr = smem_u32(bar);
   const long long t0 = clock64();
   while (true) {

@@ -35,6 +35,7 @@
 
 #include <cub/cub.cuh>
 
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <string>
@@ -566,7 +567,8 @@ __global__ void even_kernel_spectrum(double* ke, int64_t m, double ke0, double r
   ke[k] = ke0 * pow(r, (double)kk);
 }
 
-// Constant tables, cached per (device, m) and (device, m, dx, eta).
+// Constant tables, cached per call context for the last m and (m, dx, eta);
+// written and read on the context's stream.
 struct Tables {
   double2* tw = nullptr;
   int64_t tw_m = 0;
@@ -574,16 +576,16 @@ struct Tables {
   int64_t ke_cap = 0;
   int64_t ke_m = 0;
   double ke_dx = 0.0, ke_eta = 0.0;
+  ~Tables() {
+    if (tw) cudaFree(tw);
+    if (ke) cudaFree(ke);
+  }
 };
-std::map<int, Tables> g_tables;
 
 unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 shrk_status ensure_tables(int64_t m, double dx, double eta, cudaStream_t s, Tables** out) {
-  int dev = 0;
-  SHRK_CUDA(cudaGetDevice(&dev));
-  Tables& T = g_tables[dev];
-  bool made = false;
+  Tables& T = ctx_state<Tables>(EXT_FFT_TABLES);
   if (T.tw_m != m) {
     if (T.tw) SHRK_CUDA(cudaFree(T.tw));
     T.tw = nullptr;
@@ -592,7 +594,6 @@ shrk_status ensure_tables(int64_t m, double dx, double eta, cudaStream_t s, Tabl
     twiddle_kernel<<<blocks_for(m, 256), 256, 0, s>>>(T.tw, m);
     SHRK_CUDA(cudaGetLastError());
     T.tw_m = m;
-    made = true;
   }
   if (T.ke_m != m || T.ke_dx != dx || T.ke_eta != eta) {
     if (T.ke_cap < m) {
@@ -608,10 +609,7 @@ shrk_status ensure_tables(int64_t m, double dx, double eta, cudaStream_t s, Tabl
     T.ke_m = m;
     T.ke_dx = dx;
     T.ke_eta = eta;
-    made = true;
   }
-  // Tables may be read later from another stream.
-  if (made) SHRK_CUDA(cudaStreamSynchronize(s));
   *out = &T;
   return SHRK_OK;
 }
@@ -646,14 +644,14 @@ shrk_status fft(double2* buf, double2* tmp, int64_t m, const double2* tw, double
   }
   const int bits = ilog2(m);
   const int m1 = 1 << ((bits + 1) / 2), m2 = 1 << (bits / 2);
-  static bool opted[64] = {false};
+  static std::atomic<bool> opted[64];
   int dev = 0;
   SHRK_CUDA(cudaGetDevice(&dev));
-  if (dev < 64 && !opted[dev]) {
+  if (dev < 0 || dev >= 64 || !opted[dev].load()) {
     const int big = (int)pass_smem(FFT_MAXL, 1);
     SHRK_CUDA(cudaFuncSetAttribute(fft_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     SHRK_CUDA(cudaFuncSetAttribute(fft_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    opted[dev] = true;
+    if (dev >= 0 && dev < 64) opted[dev] = true;
   }
   {
     const int G = rows_per_cta(m1, m2);

@@ -27,6 +27,8 @@
 // L2L applies T_side^T; L2P interpolates L at the target; the leaf and its
 // two neighbours are summed directly in FP64.
 #include "common.cuh"
+
+#include <atomic>
 #include "internal.h"
 
 #include <cub/cub.cuh>
@@ -1057,13 +1059,13 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
     SHRK_CUDA(cudaGetLastError());
   }
   if (L > K && m2l_tc) {
-    static bool opted[64] = {false};
+    static std::atomic<bool> opted[64];
     int dev = 0;
     SHRK_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && !opted[dev]) {
+    if (dev < 0 || dev >= 64 || !opted[dev].load()) {
       SHRK_CUDA(cudaFuncSetAttribute(m2l_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      TC_SMEM));
-      opted[dev] = true;
+      if (dev >= 0 && dev < 64) opted[dev] = true;
     }
     LaunchScope ls("fmm_m2l_tc", s);
     for (int l = K + 1; l <= L; ++l) {

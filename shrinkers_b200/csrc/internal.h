@@ -159,6 +159,9 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
                     double* d_im, cudaStream_t s);
 
 double mixed_near_k();
+// Sets the bulk-copy wait budget of the exact pair kernels (cycles; negative
+// = the default) and returns the previous one.
+long long set_wait_cycles(long long cycles);
 shrk_status measure_pipe_rates(double* fp32, double* fp64);
 shrk_status measure_rcp_bias(double* uniform_mean, double* log_mean);
 

@@ -41,9 +41,6 @@ namespace shrk {
 
 namespace {
 
-// Held for the whole of a matrix call: the eigenvectors stay in SLOT_E while
-// the library lock is released around the shrinkage calls.
-std::mutex g_matrix_mu;
 
 constexpr int SLOT_E = 32;      // eigenvectors, column-major p x p
 constexpr int SLOT_W = 33;      // eigenvalues / small vectors
@@ -57,16 +54,19 @@ constexpr int SLOT_TMP = 38;    // p x p staging (input, scaled columns)
 // spiked_reconstruct_kernel in the reference's order; beyond, by a DGEMM.
 constexpr int SMALL_K = 16;
 
+// Library handles of the running call's context (a handle is not shared
+// by concurrent calls).
 struct Handles {
   cusolverDnHandle_t sol = nullptr;
   cublasHandle_t blas = nullptr;
+  ~Handles() {
+    if (sol) cusolverDnDestroy(sol);
+    if (blas) cublasDestroy(blas);
+  }
 };
-std::map<int, Handles> g_handles;
 
 shrk_status handles(cudaStream_t s, Handles** out) {
-  int dev = 0;
-  SHRK_CUDA(cudaGetDevice(&dev));
-  Handles& h = g_handles[dev];
+  Handles& h = ctx_state<Handles>(EXT_MATRIX_HANDLES);
   if (!h.sol && cusolverDnCreate(&h.sol) != CUSOLVER_STATUS_SUCCESS) {
     h.sol = nullptr;
     set_error("cusolverDnCreate failed");
@@ -509,7 +509,6 @@ extern "C" {
 
 shrk_status shrk_symmetric_eigh(const double* matrix, size_t p, double* eigenvalues,
                                 double* eigenvectors) {
-  std::lock_guard<std::mutex> lk(g_matrix_mu);
   SHRK_TRY(check_matrix_args(matrix, p, 1.0));
   std::vector<int> cols;
   std::vector<double> sorted;
@@ -528,7 +527,6 @@ shrk_status shrk_clean_eigensystem(const double* eigenvectors, const double* eig
                                    size_t p, double c, double* covariance,
                                    double* sorted_eigenvectors, double* rie_eigenvalues,
                                    double* overlaps, double* sigma2) {
-  std::lock_guard<std::mutex> lk(g_matrix_mu);
   SHRK_TRY(check_matrix_args(eigenvectors, p, c));
   std::vector<int> cols = descending(eigenvalues, p);
   std::vector<double> sorted(p);
@@ -546,7 +544,6 @@ shrk_status shrk_clean_covariance_matrix(const double* matrix, size_t p, double 
                                          int renormalize, double* covariance,
                                          double* eigenvectors, double* rie_eigenvalues,
                                          double* overlaps, double* sigma2) {
-  std::lock_guard<std::mutex> lk(g_matrix_mu);
   SHRK_TRY(check_matrix_args(matrix, p, c));
   std::vector<int> cols;
   std::vector<double> sorted;
@@ -556,7 +553,6 @@ shrk_status shrk_clean_covariance_matrix(const double* matrix, size_t p, double 
 }
 
 shrk_status shrk_renormalize_to_unit_diagonal(const double* matrix, size_t p, double* out) {
-  std::lock_guard<std::mutex> lk(g_matrix_mu);
   SHRK_TRY(check_matrix_args(matrix, p, 1.0));
   LibScope L;
   SHRK_TRY(L.st);
@@ -585,7 +581,6 @@ shrk_status shrk_precision_from_eigensystem(const double* eigenvectors, const do
                                             size_t p, double c, int method, double* precision,
                                             double* sorted_eigenvectors, double* precision_ev,
                                             double* covariance_ev, double* smoothing) {
-  std::lock_guard<std::mutex> lk(g_matrix_mu);
   SHRK_TRY(check_matrix_args(eigenvectors, p, c));
   std::vector<int> cols = descending(eigenvalues, p);
   std::vector<double> sorted(p);
@@ -603,7 +598,6 @@ shrk_status shrk_estimate_precision_matrix(const double* matrix, size_t p, doubl
                                            double* precision, double* eigenvectors,
                                            double* precision_ev, double* covariance_ev,
                                            double* smoothing) {
-  std::lock_guard<std::mutex> lk(g_matrix_mu);
   SHRK_TRY(check_matrix_args(matrix, p, c));
   std::vector<int> cols;
   std::vector<double> sorted;

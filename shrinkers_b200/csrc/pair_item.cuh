@@ -40,6 +40,7 @@ struct PairItem {
   double* out_im;
   int* err;
   bool use_tma;             // src + s0 is 16-byte aligned
+  long long wait_cycles;    // budget of each bulk-copy wait (clock cycles)
 };
 
 __device__ __forceinline__ void pair_stage_init(PairStage& st) {
@@ -114,9 +115,11 @@ __device__ __forceinline__ bool pair_item(const PairItem& a, PairStage& st, uint
     const int len = (int)min((int64_t)CH, s1 - cs);
     bool ok = true;
     if (chunk_is_tma(k)) {
-      ok = mbar_wait(&st.bar[b], (phase >> b) & 1u);
-      phase ^= 1u << b;
-      pending &= ~(1u << b);
+      ok = mbar_wait(&st.bar[b], (phase >> b) & 1u, a.wait_cycles);
+      if (ok) {  // a copy that did not land stays pending for the drain below
+        phase ^= 1u << b;
+        pending &= ~(1u << b);
+      }
     } else {
       for (int i = tid; i < len; i += NT) st.sbuf[b][i] = a.src[cs + i];
     }

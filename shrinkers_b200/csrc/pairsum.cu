@@ -31,6 +31,7 @@
 #include "pairs.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 
 namespace shrk {
@@ -52,6 +53,9 @@ constexpr int R_SMALL_F64 = 1;    // targets per thread below one full tile
 constexpr int R_SMALL_MIXED = 2;  // the packed far field takes target pairs
 
 double g_near_k = SHRK_NEAR_K;
+// Budget of the pair kernels' bulk-copy waits (clock cycles); changed only by
+// shrk_diag_set_wait_limit to exercise the timeout path.
+std::atomic<long long> g_wait_cycles{WAIT_CYCLES_DEFAULT};
 
 struct PairArgs {
   const double* tgt;
@@ -68,6 +72,7 @@ struct PairArgs {
   double* part_im;
   int* err;
   int use_tma;
+  long long wait_cycles;   // budget of each bulk-copy wait
 };
 
 template <bool MIXED, int R>
@@ -94,6 +99,7 @@ __global__ void __launch_bounds__(NT, MIXED ? SHRK_MIXED_CTAS : 2) pair_sum_kern
     it.out_im = a.part_im + (int64_t)split * a.nt;
     it.err = a.err;
     it.use_tma = a.use_tma != 0;
+    it.wait_cycles = a.wait_cycles;
     if (!pair_item<MIXED, R>(it, st, phase, pending)) return;
   }
 }
@@ -165,6 +171,10 @@ __global__ void reduce_kernel(const ReduceArgs a) {
 }  // namespace
 
 double mixed_near_k() { return g_near_k; }
+
+long long set_wait_cycles(long long cycles) {
+  return g_wait_cycles.exchange(cycles < 0 ? WAIT_CYCLES_DEFAULT : cycles);
+}
 
 SplitPlan plan_splits(int64_t nt, int64_t ns, int tile, int chunk, int ctas_per_sm) {
   SplitPlan pl;
@@ -241,6 +251,7 @@ shrk_status exact_pair_sums(const double* d_tgt, int64_t nt, const double* d_src
   a.part_im = (double*)part + (size_t)pl.n_splits * nt;
   a.err = device_error_word();
   a.use_tma = ((uintptr_t)d_src % 16 == 0) ? 1 : 0;
+  a.wait_cycles = g_wait_cycles.load();
   {
     LaunchScope ls(mixed ? "pair_sum_mixed" : "pair_sum_f64", s);
     if (mixed && small) pair_sum_kernel<true, R_SMALL_MIXED><<<pl.grid, NT, 0, s>>>(a);
@@ -350,6 +361,7 @@ shrk_status exact_pair_sums_fixed(const double* d_tgt, int64_t nt, const double*
   a.part_im = part + (size_t)n_splits * nt;
   a.err = err;
   a.use_tma = ((uintptr_t)d_src % 16 == 0) ? 1 : 0;
+  a.wait_cycles = g_wait_cycles.load();
   if (mixed) pair_sum_kernel<true, R_MIXED><<<grid, NT, 0, s>>>(a);
   else pair_sum_kernel<false, R_F64><<<grid, NT, 0, s>>>(a);
   SHRK_CUDA(cudaGetLastError());

@@ -1,8 +1,9 @@
 // Sources in ascending order on the device, for the methods that need them
 // (the treecode builds over the sorted spectrum, chebcode.rs:1088-1097; the
 // NUFFT splat gathers contiguous source runs per grid cell).  Sortedness is
-// checked on the device; only unsorted input is sorted (CUB radix sort into
-// library scratch).  The first and last entries IN THE CALLER'S ORDER are
+// checked on the device (or taken from the host check of a host-pointer
+// call's upload); only unsorted input is sorted (CUB radix sort into library
+// scratch).  The first and last entries IN THE CALLER'S ORDER are
 // returned too: the NUFFT takes its grid bounds from them (nufft.rs:139-146).
 #include "common.cuh"
 #include "internal.h"
@@ -26,6 +27,14 @@ __global__ void iota_kernel(int* v, int64_t n) {
 // first / last entries, read back with one synchronisation.
 shrk_status check_sorted(const double* d_src, int64_t ns, bool* sorted, double* first,
                          double* last, cudaStream_t s) {
+  // A host-pointer call has checked its upload on the host already.
+  if (source_hint(d_src, ns, sorted, first, last)) {
+    if (!*sorted && ns > (int64_t)INT32_MAX) {
+      set_error("unsorted input larger than 2^31 values: sort it before the call");
+      return SHRK_EINVAL;
+    }
+    return SHRK_OK;
+  }
   void* f = nullptr;
   SHRK_TRY(scratch_get(27, 256, &f));
   int* flag = (int*)f;
@@ -110,6 +119,9 @@ shrk_status sorted_sources_perm(const double* d_src, int64_t ns, const double** 
   }
   *d_sorted = (const double*)out;
   *d_perm = perm;
+  bool hs = false;
+  double hf = 0.0, hl = 0.0;
+  if ((lo || hi) && source_hint(d_src, ns, &hs, &hf, &hl, lo, hi)) return SHRK_OK;
   if (lo || hi) {
     double ends[2];
     SHRK_CUDA(cudaMemcpyAsync(&ends[0], out, sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -1,12 +1,13 @@
 """C ABI and host logic, CPU only (no compute call reaches a GPU here).
 
 * libshrinkers_b200.so loads and exports every function that
-  include/shrinkers_b200.h declares, and the Python binding covers them all;
+  include/*.h declares, and the Python binding covers them all;
 * the host-side policy (parse_method, auto resolution, grid redirect) and the
   host estimators (BEMA, inverse BBP, shrinkage factor) agree with the oracle;
 * the Python boundary raises the reference's errors before touching a GPU.
 """
 import ctypes as C
+import glob
 import os
 import re
 
@@ -19,7 +20,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def header_functions():
-    text = open(os.path.join(ROOT, "include", "shrinkers_b200.h")).read()
+    text = ""
+    for h in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))):
+        text += open(h).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(shrk_[a-z0-9_]+)\s*\(", text)))
 

@@ -95,18 +95,25 @@ def test_nufft_alias_and_grid_redirect(rk):
     np.testing.assert_array_equal(a["real"], b["real"])
 
 
-def test_nufft_full_size(oracle):
-    """p = 1e6 MP + 20 spikes (the treecode/NUFFT workload): GPU vs oracle and
-    the NUFFT's error vs the exact sums on a target sample."""
+@pytest.mark.parametrize("eta_rule", ["1/sqrtp", "1e-4"])
+def test_nufft_full_size(oracle, eta_rule):
+    """p = 1e6 MP + 20 spikes (the treecode/NUFFT workload) at both of its
+    etas: GPU vs oracle (same grid policy, so the same grid of 65 536 cells)
+    within 1e-10 of the largest value, and the NUFFT's error vs the exact
+    sums on a target sample.  The reference's grid cap (65 536 cells over a
+    range of ~50) makes the cell ~2e-3 wide, coarse against either eta:
+    that error class is the reference's, recorded here, not a GPU defect."""
     p = 1_000_000
     ev = spectra.config3(p)
-    eta = 1.0 / math.sqrt(p)
+    eta = 1.0 / math.sqrt(p) if eta_rule == "1/sqrtp" else 1e-4
     re, im = gpu_nufft_all(ev, eta)
     o_re, o_im = oracle.nufft_points(ev, ev, eta, parallel=True)
     scale = max(np.max(np.abs(o_re)), np.max(np.abs(o_im)))
-    assert np.max(np.abs(re * p - o_re)) < 1e-9 * scale
+    assert np.max(np.abs(re * p - o_re)) < 1e-10 * scale
+    assert np.max(np.abs(im * p - o_im)) < 1e-10 * scale
     idx = np.random.default_rng(1).choice(p, 32, replace=False)
     t_re, t_im = oracle.truth_points(ev[idx], ev, eta)
     err = np.hypot(re[idx] * p - t_re, im[idx] * p - t_im) / np.hypot(t_re, t_im)
-    # documented behaviour: the 65,536-cell cap dominates this error class
-    assert np.median(err) < 5e-2
+    assert np.all(np.isfinite(err))
+    if eta_rule == "1/sqrtp":
+        assert np.median(err) < 5e-2
