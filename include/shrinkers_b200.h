@@ -180,6 +180,11 @@ shrk_status shrk_stieltjes_batched_dev(const double* d_ev, const int64_t* d_offs
  * force != 0.  Spectra of the batched entry points hold at most 16 777 216
  * values each. */
 shrk_status shrk_batched_autotune(int precision, int force, int32_t* table);
+/* Installs a (R, SL) table of the layout shrk_batched_autotune returns, for
+ * `precision` on the current device, e.g. one saved from an earlier process
+ * so that no call pays for tuning; R in {2, 4}, SL in {1024, 2048, 4096,
+ * 8192}, else SHRK_EINVAL.  Later batched calls plan with it. */
+shrk_status shrk_batched_set_tune(int precision, const int32_t* table);
 
 /* Adjoint of m(z_j) = (1/p) sum_i 1/(ev_i - z_j), z_j = ev_j + i*eta (the
  * -conj(S)/p convention; no reference counterpart).  Given cotangents
@@ -257,7 +262,8 @@ shrk_status shrk_stieltjes_fft5_with_options_dev(const double* d_ev, size_t p, d
 
 /* --------------------------------------------------- matrix front-end -- */
 /* Matrices are row-major p x p (p <= 46340), eigenvectors are their
- * columns.  The eigendecomposition is cuSOLVER's syevd on the device (the
+ * columns.  The eigendecomposition is this library's own on the device
+ * (Householder tridiagonalisation, multisection, inverse iteration; the
  * reference's symmetric_eigh, pipeline/mod.rs:502-585, is a Jacobi
  * iteration; eigenvector signs are arbitrary in both).  Output pointers
  * marked "may be NULL" are skipped when NULL. */

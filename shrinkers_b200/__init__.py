@@ -686,7 +686,7 @@ def renormalize_to_unit_diagonal(matrix):
 
 
 def symmetric_eigh(matrix):
-    """pipeline/mod.rs:502-585 symmetric_eigh on the GPU (cuSOLVER syevd):
+    """pipeline/mod.rs:502-585 symmetric_eigh on the GPU (this library's eigensolver):
     (ascending eigenvalues, eigenvectors as columns)."""
     a = _owned_symmetric_matrix(matrix, "matrix")
     p = a.shape[0]

@@ -17,8 +17,6 @@ NVCC_FLAGS = [
     "--fmad=false",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
     "-shared", "-cudart", "static",
-    # the matrix front-end's eigensolver and GEMM (library calls)
-    "-lcusolver", "-lcublas",
 ]
 
 

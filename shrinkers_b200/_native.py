@@ -46,6 +46,7 @@ SIGNATURES = {
     "shrk_stieltjes_batched": (_ST, [_D, _I64, _SZ, _D, C.c_int, _D, _D]),
     "shrk_stieltjes_batched_dev": (_ST, [_P, _P, _SZ, _P, C.c_int, _P, _P, _P]),
     "shrk_batched_autotune": (_ST, [C.c_int, C.c_int, C.POINTER(C.c_int32)]),
+    "shrk_batched_set_tune": (_ST, [C.c_int, C.POINTER(C.c_int32)]),
     "shrk_stieltjes_adjoint": (_ST, [_D, _SZ, C.c_double, _D, _D, C.c_int, _D]),
     "shrk_stieltjes_adjoint_dev": (_ST, [_P, _SZ, C.c_double, _P, _P, C.c_int, _P, _P]),
     "shrk_stieltjes_adjoint_treecode": (_ST, [_D, _SZ, C.c_double, _D, _D, C.c_int, _D]),

@@ -23,7 +23,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <iterator>
 #include <mutex>
+#include <string>
 #include <vector>
 
 namespace shrk {
@@ -382,6 +384,33 @@ shrk_status autotune(int precision, Tune& t, cudaStream_t s) {
 }
 
 }  // namespace
+
+shrk_status batched_set_tune(int precision, const int* table) {
+  const int dev = current_device();
+  if (dev < 0 || dev >= kMaxDev) {
+    set_error("device ordinal out of range");
+    return SHRK_EINVAL;
+  }
+  for (int b = 0; b < NB; ++b) {
+    const int R = table[2 * b], SL = table[2 * b + 1];
+    const bool r_ok = std::find(std::begin(TUNE_R), std::end(TUNE_R), R) != std::end(TUNE_R);
+    const bool s_ok = std::find(std::begin(TUNE_SL), std::end(TUNE_SL), SL) != std::end(TUNE_SL);
+    if (!r_ok || !s_ok) {
+      set_error("batched tuning table: R must be 2 or 4 and SL one of 1024, 2048, 4096, 8192 "
+                "(bucket " + std::to_string(b) + ")");
+      return SHRK_EINVAL;
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu[dev]);
+  Tune& t = g_tune[dev][precision];
+  for (int b = 0; b < NB; ++b) {
+    t.R[b] = table[2 * b];
+    t.SL[b] = table[2 * b + 1];
+  }
+  t.tuned = true;
+  t.version += 1;
+  return SHRK_OK;
+}
 
 shrk_status batched_tune(int precision, bool force, int* table, cudaStream_t s) {
   const int dev = current_device();

@@ -56,10 +56,18 @@ struct Context {
   bool host = false;
   bool in_use = true;             // host-thread contexts: false once their thread exited
   uintptr_t key = 0;              // `_dev` contexts: the stream handle
-  Scratch slots[48];
+  Scratch slots[64];
   int* err = nullptr;
   void* ext[kExtSlots] = {};
   void (*ext_del[kExtSlots])(void*) = {};
+  // Host-pointer calls: pinned staging of their host<->device copies (grow-
+  // only; sized at call entry from the previous call's needs) and the
+  // device->host copies waiting for the call's one synchronisation.
+  char* stage = nullptr;
+  size_t stage_bytes = 0, stage_used = 0, stage_want = 0;
+  bool stage_busy = false;  // copies from/to the stage may still be in flight
+  struct PendingCopy { void* dst; size_t off, bytes; };
+  std::vector<PendingCopy> pending;
   // source_hint of the running host-pointer call
   const double* hint_dev = nullptr;
   int64_t hint_n = 0;
@@ -229,8 +237,16 @@ cudaStream_t library_stream() { return t_cur->stream; }
 
 static shrk_status check_error_word(Context* c, cudaStream_t s) {
   int h = 0;
-  SHRK_CUDA(cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  char* st = (c->host && s == c->stream && c->stage && c->stage_used + 256 <= c->stage_bytes)
+                 ? c->stage + c->stage_used
+                 : nullptr;
+  SHRK_CUDA(cudaMemcpyAsync(st ? (void*)st : (void*)&h, c->err, sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
+  c->stage_busy = false;
+  if (st) std::memcpy(&h, st, sizeof(int));
+  for (const auto& q : c->pending) std::memcpy(q.dst, c->stage + q.off, q.bytes);
+  c->pending.clear();
   if (h != DEV_ERR_NONE) {
     SHRK_CUDA(cudaMemsetAsync(c->err, 0, sizeof(int), s));
     SHRK_CUDA(cudaStreamSynchronize(s));
@@ -307,12 +323,68 @@ static shrk_status not_impl(int m) {
   return SHRK_ENOTIMPL;
 }
 
+// Host<->device copies of the host-pointer entry points, staged through the
+// context's pinned buffer: an upload is a host memcpy into the stage plus an
+// asynchronous copy; a download is an asynchronous copy into the stage that
+// check_device_error completes (one synchronisation per call, shared with
+// the error-word read).  A copy that does not fit the stage goes direct
+// (pageable) and the stage grows before the next call.
+static char* stage_take(Context* c, size_t bytes, size_t* off) {
+  const size_t al = (bytes + 255) & ~(size_t)255;
+  c->stage_want += al;
+  if (!c->stage || c->stage_used + al > c->stage_bytes) return nullptr;
+  *off = c->stage_used;
+  c->stage_used += al;
+  c->stage_busy = true;
+  return c->stage + *off;
+}
+
 static shrk_status h2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
-  SHRK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+  Context* c = t_cur;
+  size_t off = 0;
+  char* st = (c && c->host && s == c->stream) ? stage_take(c, bytes, &off) : nullptr;
+  if (st) {
+    std::memcpy(st, src, bytes);
+    SHRK_CUDA(cudaMemcpyAsync(dst, st, bytes, cudaMemcpyHostToDevice, s));
+  } else {
+    SHRK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+  }
   return SHRK_OK;
 }
+
 static shrk_status d2h(void* dst, const void* src, size_t bytes, cudaStream_t s) {
-  SHRK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+  Context* c = t_cur;
+  size_t off = 0;
+  char* st = (c && c->host && s == c->stream) ? stage_take(c, bytes, &off) : nullptr;
+  if (st) {
+    SHRK_CUDA(cudaMemcpyAsync(st, src, bytes, cudaMemcpyDeviceToHost, s));
+    c->pending.push_back({dst, off, bytes});
+  } else {
+    SHRK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+  }
+  return SHRK_OK;
+}
+
+// At the entry of a host-pointer call: settle what an earlier call that
+// returned early may have left in flight, and size the stage.
+static shrk_status stage_begin(Context* c) {
+  if (c->stage_busy) {
+    SHRK_CUDA(cudaStreamSynchronize(c->stream));
+    c->stage_busy = false;
+  }
+  c->pending.clear();
+  constexpr size_t kStageMax = (size_t)64 << 20;
+  const size_t want = std::min(std::max(c->stage_want, (size_t)1 << 16), kStageMax);
+  if (want > c->stage_bytes) {
+    if (c->stage) cudaFreeHost(c->stage);
+    c->stage = nullptr;
+    c->stage_bytes = 0;
+    const size_t grow = std::min(std::max(want, 2 * c->stage_bytes), kStageMax);
+    if (cudaMallocHost((void**)&c->stage, grow) == cudaSuccess) c->stage_bytes = grow;
+    else cudaGetLastError();  // no pinned memory: the copies go direct
+  }
+  c->stage_used = 0;
+  c->stage_want = 0;
   return SHRK_OK;
 }
 
@@ -588,6 +660,8 @@ struct Guard {
     lk = std::unique_lock<std::recursive_mutex>(ctx->mu);
     t_cur = ctx;
     ctx->hint_dev = nullptr;  // a hint never outlives the call that set it
+    // the outermost host-pointer call on this context owns the stage
+    if (ctx->host && prev != ctx) st = stage_begin(ctx);
   }
 };
 
@@ -924,6 +998,15 @@ shrk_status shrk_batched_autotune(int precision, int force, int32_t* table) {
   if (table)
     for (int i = 0; i < 16; ++i) table[i] = t[i];
   return check_device_error(t_cur->stream);
+}
+
+shrk_status shrk_batched_set_tune(int precision, const int32_t* table) {
+  if (precision != SHRK_PREC_F64 && precision != SHRK_PREC_MIXED)
+    return einval("unknown precision id");
+  if (!table) return einval("null table");
+  int t[16];
+  for (int i = 0; i < 16; ++i) t[i] = table[i];
+  return batched_set_tune(precision, t);
 }
 
 shrk_status shrk_stieltjes_adjoint_dev(const double* d_ev, size_t p, double eta,

@@ -34,11 +34,11 @@ struct Scratch {
   void* ptr = nullptr;
   size_t bytes = 0;
 };
-shrk_status scratch_get(int slot, size_t bytes, void** out);  // slot in [0, 48)
+shrk_status scratch_get(int slot, size_t bytes, void** out);  // slot in [0, 64)
 // Per-context module state: the object in slot k (a CtxExt) of the running
 // call's context, made by `make` on first use and deleted by `del` when the
 // context is released.  Contexts are never shared by concurrent calls.
-enum CtxExt : int { EXT_FFT_TABLES = 0, EXT_BATCHED_GRAPH = 1, EXT_MATRIX_HANDLES = 2 };
+enum CtxExt : int { EXT_FFT_TABLES = 0, EXT_BATCHED_GRAPH = 1 };
 void* ctx_ext(int k, void* (*make)(), void (*del)(void*));
 template <typename T>
 T& ctx_state(int k) {

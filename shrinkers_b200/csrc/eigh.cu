@@ -1,0 +1,698 @@
+// Dense symmetric eigendecomposition and FP64 GEMM on sm_100a, for the matrix
+// front-end (src/pipeline/mod.rs:502-585 symmetric_eigh; the reference runs a
+// cyclic Jacobi iteration, and its docs name LAPACK's dsyevd as the fast
+// path).  Written for the GPU instead of restating Jacobi:
+//
+//   1. tridiagonalisation  Householder reflections H_j = I - beta_j v_j v_j^T,
+//                          one cooperative persistent kernel: every warp owns
+//                          columns of the (full, symmetric, column-major)
+//                          trailing matrix; per column j one grid barrier
+//                          after the symmetric product p = beta A22 v and one
+//                          after the rank-2 update A22 -= v w^T + w v^T,
+//                          w = p - (beta/2)(p^T v) v.  The reflectors stay in
+//                          the strict lower part of A (v_{j+1} and beta_j
+//                          aside), as in LAPACK's dsytrd.
+//   2. eigenvalues         the tridiagonal T splits where an off-diagonal is
+//                          negligible; each eigenvalue of each unreduced block
+//                          by 32-way multisection on Sturm counts, one warp
+//                          per eigenvalue.
+//   3. eigenvectors of T   inverse iteration (LU with partial pivoting,
+//                          three solves from a fixed pseudo-random start),
+//                          one thread per cluster of eigenvalues closer than
+//                          CLUSTER_TOL ||T||, modified Gram-Schmidt inside a
+//                          cluster; then one Newton-Schulz step
+//                          Z <- Z (3I - Z^T Z)/2 on the whole basis, which
+//                          takes the remaining O(eps ||T|| / gap) overlaps
+//                          of close eigenvectors to rounding level.
+//   4. back-transformation U = H_0 ... H_{p-3} Z in blocks of NB reflectors,
+//                          each (I - Y T Y^T) in compact WY form (three
+//                          GEMMs).
+//
+// The GEMM (dgemm) is a plain FP64 tiled kernel: 64 x 64 outputs per CTA of
+// 256 threads, 4 x 4 per thread, k staged 16 at a time in shared memory.
+#include "common.cuh"
+#include "internal.h"
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <string>
+#include <vector>
+
+namespace shrk {
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+// ------------------------------------------------------------------ GEMM --
+constexpr int GT = 64;   // output tile
+constexpr int GK = 16;   // k per shared-memory stage
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, double alpha,
+                                                    const double* __restrict__ A, int64_t lda,
+                                                    const double* __restrict__ B, int64_t ldb,
+                                                    double beta, double* __restrict__ C,
+                                                    int64_t ldc) {
+  __shared__ double As[GK][GT + 1];  // As[kk][i] = op(A)[i0 + i, k0 + kk]
+  __shared__ double Bs[GK][GT + 1];  // Bs[kk][j] = op(B)[k0 + kk, j0 + j]
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = blockIdx.x * GT, j0 = blockIdx.y * GT;
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+  for (int k0 = 0; k0 < k; k0 += GK) {
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int t = threadIdx.x + it * 256;
+      int i, kk;
+      if (!TA) { i = t & 63; kk = t >> 6; }   // A(i, kk) contiguous in i
+      else { kk = t & 15; i = t >> 4; }       // A(kk, i) contiguous in kk
+      const int gi = i0 + i, gk = k0 + kk;
+      double v = 0.0;
+      if (gi < m && gk < k) v = !TA ? A[gi + (int64_t)gk * lda] : A[gk + (int64_t)gi * lda];
+      As[kk][i] = v;
+    }
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int t = threadIdx.x + it * 256;
+      int j, kk;
+      if (!TB) { kk = t & 15; j = t >> 4; }   // B(kk, j) contiguous in kk
+      else { j = t & 63; kk = t >> 6; }       // B(j, kk) contiguous in j
+      const int gj = j0 + j, gk = k0 + kk;
+      double v = 0.0;
+      if (gj < n && gk < k) v = !TB ? B[gk + (int64_t)gj * ldb] : B[gj + (int64_t)gk * ldb];
+      Bs[kk][j] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) a[r] = As[kk][tx + 16 * r];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) b[c] = Bs[kk][ty + 16 * c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int gj = j0 + ty + 16 * c;
+    if (gj >= n) continue;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int gi = i0 + tx + 16 * r;
+      if (gi >= m) continue;
+      double* cp = C + gi + (int64_t)gj * ldc;
+      *cp = beta == 0.0 ? alpha * acc[r][c] : fma(alpha, acc[r][c], beta * *cp);
+    }
+  }
+}
+
+// -------------------------------------------------------- tridiagonalise --
+struct TriArgs {
+  double* A;        // p x p column-major, symmetric (both triangles)
+  int64_t p;
+  double* d;        // [p] diagonal of T
+  double* e;        // [p] off-diagonal of T (e[j] couples j and j+1)
+  double* vhead;    // [p] first entry v_{j+1} of reflector j
+  double* beta;     // [p] beta_j (0: no reflection)
+  double* pv;       // [p] p = beta A22 v
+  double* part;     // [gridDim.x] per-block partial sums of p^T v
+  double* scal;     // [2] norm^2 and first entry of the next column below the diagonal
+};
+
+constexpr int TRI_NT = 512;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Norm^2 and first entry of A[c+1 .. p-1, c] by one warp; lane 0 writes them
+// (and the final diagonal entry d[c]).
+__device__ __forceinline__ void column_tail(const TriArgs& a, int64_t c, int lane) {
+  const int64_t p = a.p;
+  const double* col = a.A + c * p;
+  double s = 0.0;
+  for (int64_t k = c + 1 + lane; k < p; k += 32) s += col[k] * col[k];
+  s = warp_sum(s);
+  if (lane == 0) {
+    a.scal[0] = s;
+    a.scal[1] = c + 1 < p ? col[c + 1] : 0.0;
+    a.d[c] = col[c];
+  }
+}
+
+__global__ void __launch_bounds__(TRI_NT, 1) tridiag_kernel(const TriArgs a) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double s_red[TRI_NT / 32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  constexpr int WPB = TRI_NT / 32;
+  const int64_t gw = (int64_t)blockIdx.x * WPB + wib;  // global warp: owns columns gw mod nw
+  const int64_t nw = (int64_t)gridDim.x * WPB;
+  const int64_t p = a.p;
+  double* A = a.A;
+  if (gw == 0) column_tail(a, 0, lane);
+  grid.sync();
+  for (int64_t j = 0; j + 2 < p; ++j) {
+    // the reflector of column j, from the norm its owner left in scal
+    const double norm2 = a.scal[0], x0 = a.scal[1];
+    const double sig = norm2 - x0 * x0;
+    double beta = 0.0, v0 = x0;
+    if (sig > 0.0) {
+      const double nrm = sqrt(norm2);
+      const double alpha = x0 >= 0.0 ? -nrm : nrm;
+      v0 = x0 - alpha;
+      beta = 2.0 / (sig + v0 * v0);
+      if (gw == 0 && lane == 0) a.e[j] = alpha;
+    } else if (gw == 0 && lane == 0) {
+      a.e[j] = x0;  // already reduced: H_j = I
+    }
+    if (gw == 0 && lane == 0) {
+      a.vhead[j] = v0;
+      a.beta[j] = beta;
+    }
+    const double* vcol = A + j * p;  // v_k = vcol[k] for k >= j + 2
+    const int64_t k0 = j + 1;
+    // (1) p = beta A22 v over the owned columns, and p^T v
+    double dot = 0.0;
+    if (beta != 0.0) {
+      int64_t c = k0 + ((gw - k0) % nw + nw) % nw;
+      for (; c < p; c += nw) {
+        const double* col = A + c * p;
+        double s = 0.0;
+        for (int64_t k = k0 + lane; k < p; k += 32) {
+          const double vk = k == k0 ? v0 : vcol[k];
+          s = fma(col[k], vk, s);
+        }
+        s = warp_sum(s) * beta;
+        if (lane == 0) a.pv[c] = s;
+        dot = fma(s, c == k0 ? v0 : vcol[c], dot);
+      }
+    }
+    if (lane == 0) s_red[wib] = dot;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < WPB; ++w) t += s_red[w];
+      a.part[blockIdx.x] = t;
+    }
+    grid.sync();
+    // (2) A22 -= v w^T + w v^T, w = p - (beta/2)(p^T v) v, by owned columns;
+    // the owner of column j+1 then measures the next column
+    if (beta != 0.0) {
+      double g = 0.0;
+      for (int b = lane; b < (int)gridDim.x; b += 32) g += a.part[b];
+      const double K = 0.5 * beta * warp_sum(g);
+      int64_t c = k0 + ((gw - k0) % nw + nw) % nw;
+      for (; c < p; c += nw) {
+        double* col = A + c * p;
+        const double vc = c == k0 ? v0 : vcol[c];
+        const double wc = a.pv[c] - K * vc;
+        for (int64_t k = k0 + lane; k < p; k += 32) {
+          const double vk = k == k0 ? v0 : vcol[k];
+          const double wk = a.pv[k] - K * vk;
+          col[k] = col[k] - (vk * wc + wk * vc);
+        }
+      }
+    }
+    if (gw == k0 % nw) {
+      __syncwarp();
+      column_tail(a, k0, lane);
+    }
+    grid.sync();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (p >= 2) a.e[p - 2] = a.scal[1];
+    a.d[p - 1] = A[(p - 1) + (p - 1) * p];
+    if (p == 1) a.d[0] = A[0];
+  }
+}
+
+// ------------------------------------------------------------ bisection --
+// Slot k: the kloc-th smallest eigenvalue of the unreduced block [b0, b1)
+// of T, searched in the block's Gershgorin interval [lo, hi].
+struct EigSlot {
+  int b0, b1, kloc, pad;
+  double lo, hi;
+};
+
+// Number of eigenvalues of T[b0:b1) below x (negative pivots of the LDL^T
+// factorisation of T - x I; a pivot smaller than pivmin counts as -pivmin).
+__device__ __forceinline__ int sturm(const double* __restrict__ d, const double* __restrict__ e2,
+                                     int b0, int b1, double x, double pivmin) {
+  double q = d[b0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int cnt = q < 0.0;
+  for (int i = b0 + 1; i < b1; ++i) {
+    q = (d[i] - x) - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += q < 0.0;
+  }
+  return cnt;
+}
+
+__global__ void __launch_bounds__(256) bisect_kernel(const double* __restrict__ d,
+                                                     const double* __restrict__ e2,
+                                                     const EigSlot* __restrict__ slots, int n,
+                                                     double pivmin, double* __restrict__ lam) {
+  const int k = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (k >= n) return;
+  const EigSlot sl = slots[k];
+  double lo = sl.lo, hi = sl.hi;
+  const double eps = 2.220446049250313e-16;
+  for (int it = 0; it < 64; ++it) {
+    if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + pivmin) break;
+    const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
+    const bool above = sturm(d, e2, sl.b0, sl.b1, x, pivmin) > sl.kloc;
+    const unsigned m = __ballot_sync(0xffffffffu, above);
+    const double nlo = m == 0u ? __shfl_sync(0xffffffffu, x, 31)
+                               : (__ffs(m) == 1 ? lo : __shfl_sync(0xffffffffu, x, __ffs(m) - 2));
+    const double nhi = m == 0u ? hi : __shfl_sync(0xffffffffu, x, __ffs(m) - 1);
+    if (!(nlo > lo || nhi < hi)) break;  // no representable progress
+    lo = nlo;
+    hi = nhi;
+  }
+  if (lane == 0) lam[k] = 0.5 * (lo + hi);
+}
+
+// ------------------------------------------------------ inverse iteration --
+// Cluster c: slots [s0, s0 + ns) of the unreduced block [b0, b1).
+struct Cluster {
+  int s0, ns, b0, b1;
+};
+
+// Deterministic start vector entry (hash of slot and row), in [-1, 1).
+__device__ __forceinline__ double start_entry(int slot, int i) {
+  uint64_t h = (uint64_t)(uint32_t)slot * 0x9E3779B97F4A7C15ull ^ (uint64_t)(uint32_t)i * 0xC2B2AE3D27D4EB4Full;
+  h ^= h >> 31;
+  h *= 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 29;
+  return (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// One thread per cluster.  Workspace (interleaved by thread, so a warp's
+// accesses to the same row coalesce): u0, u1, u2 of U and the right-hand
+// side / solution x, rows relative to the block start.  Eigenvector of slot
+// s goes to Zt[s + i p] (row s of Z^T) for i in [b0, b1).
+__global__ void __launch_bounds__(128) inverse_iteration_kernel(
+    const double* __restrict__ d, const double* __restrict__ e, const double* __restrict__ lam,
+    const Cluster* __restrict__ cl, int ncl, int64_t p, double tnorm, double* __restrict__ ws,
+    double* __restrict__ Zt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncl) return;
+  const Cluster c = cl[t];
+  const int64_t stride = (int64_t)ncl;
+  double* u0 = ws;
+  double* u1 = ws + stride * p;
+  double* u2 = ws + 2 * stride * p;
+  double* x = ws + 3 * stride * p;
+#define W(arr, i) arr[(int64_t)(i) * stride + t]
+  const int n = c.b1 - c.b0;
+  const double small = 2.220446049250313e-16 * tnorm + 1e-300;
+  for (int q = 0; q < c.ns; ++q) {
+    const int slot = c.s0 + q;
+    const double l = lam[slot];
+    for (int i = 0; i < n; ++i) W(x, i) = start_entry(slot, i);
+    for (int iter = 0; iter < 3; ++iter) {
+      // factor T - l I with partial pivoting, eliminating the right-hand side
+      double diag = d[c.b0] - l;
+      double sup = n > 1 ? e[c.b0] : 0.0;
+      double rhs = W(x, 0);
+      for (int i = 0; i + 1 < n; ++i) {
+        const double sub = e[c.b0 + i];
+        const double nd = d[c.b0 + i + 1] - l;
+        const double ns = i + 2 < n ? e[c.b0 + i + 1] : 0.0;
+        const double rn = W(x, i + 1);
+        if (fabs(diag) >= fabs(sub)) {
+          const double m = diag != 0.0 ? sub / diag : 0.0;
+          W(u0, i) = diag;
+          W(u1, i) = sup;
+          W(u2, i) = 0.0;
+          W(x, i) = rhs;
+          diag = nd - m * sup;
+          sup = ns;
+          rhs = rn - m * rhs;
+        } else {
+          const double m = diag / sub;
+          W(u0, i) = sub;
+          W(u1, i) = nd;
+          W(u2, i) = ns;
+          W(x, i) = rn;
+          diag = sup - m * nd;
+          sup = -m * ns;
+          rhs = rhs - m * rn;
+        }
+      }
+      W(u0, n - 1) = diag;
+      W(x, n - 1) = rhs;
+      // back substitution, tiny pivots replaced by eps ||T||
+      double nrm2 = 0.0, x1 = 0.0, x2 = 0.0;
+      for (int i = n - 1; i >= 0; --i) {
+        double piv = W(u0, i);
+        if (fabs(piv) < small) piv = piv < 0.0 ? -small : small;
+        double s = W(x, i);
+        if (i + 1 < n) s -= W(u1, i) * x1;
+        if (i + 2 < n) s -= W(u2, i) * x2;
+        const double xi = s / piv;
+        W(x, i) = xi;
+        nrm2 += xi * xi;
+        x2 = x1;
+        x1 = xi;
+      }
+      double inv = 1.0 / sqrt(nrm2);
+      for (int i = 0; i < n; ++i) W(x, i) *= inv;
+      // modified Gram-Schmidt against the cluster's earlier vectors
+      for (int r = 0; r < q; ++r) {
+        const double* zr = Zt + (c.s0 + r);
+        double dt = 0.0;
+        for (int i = 0; i < n; ++i) dt += zr[(int64_t)(c.b0 + i) * p] * W(x, i);
+        nrm2 = 0.0;
+        for (int i = 0; i < n; ++i) {
+          const double xi = W(x, i) - dt * zr[(int64_t)(c.b0 + i) * p];
+          W(x, i) = xi;
+          nrm2 += xi * xi;
+        }
+        inv = 1.0 / sqrt(nrm2);
+        for (int i = 0; i < n; ++i) W(x, i) *= inv;
+      }
+    }
+    for (int i = 0; i < n; ++i) Zt[slot + (int64_t)(c.b0 + i) * p] = W(x, i);
+  }
+#undef W
+}
+
+// M = 1.5 I - 0.5 G (Newton-Schulz step for the polar factor).
+__global__ void ns_matrix_kernel(double* __restrict__ g, int64_t p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y;
+  if (i >= p) return;
+  const double v = g[i + j * p];
+  g[i + j * p] = (i == j ? 1.5 : 0.0) - 0.5 * v;
+}
+
+// Y[r, jj] = v_{j0+jj}[j0+1+r] (rows of the block's reach, zero above the
+// reflector's first entry), n = p - j0 - 1 rows, nb columns.
+__global__ void build_y_kernel(const double* __restrict__ A, const double* __restrict__ vhead,
+                               int64_t p, int64_t j0, int nb, double* __restrict__ Y) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int jj = blockIdx.y;
+  const int64_t n = p - j0 - 1;
+  if (r >= n) return;
+  const int64_t j = j0 + jj;
+  const int64_t row = j0 + 1 + r;
+  double v = 0.0;
+  if (row == j + 1) v = vhead[j];
+  else if (row > j + 1) v = A[row + j * p];
+  Y[r + (int64_t)jj * n] = v;
+}
+
+// T of the compact WY form, H_{j0} ... H_{j0+nb-1} = I - Y T Y^T (forward,
+// columnwise): T[jj][jj] = beta, T[0:jj, jj] = -beta T[0:jj, 0:jj] S[0:jj, jj]
+// with S = Y^T Y.  One CTA; nb <= 64.
+__global__ void wy_t_kernel(const double* __restrict__ S, const double* __restrict__ beta,
+                            int64_t j0, int nb, double* __restrict__ T) {
+  __shared__ double t[64 * 64];
+  __shared__ double col[64];
+  for (int i = threadIdx.x; i < nb * nb; i += blockDim.x) t[i] = 0.0;
+  __syncthreads();
+  for (int jj = 0; jj < nb; ++jj) {
+    const double b = beta[j0 + jj];
+    const int r = threadIdx.x;
+    if (r < jj) {
+      double s = 0.0;
+      for (int q = r; q < jj; ++q) s += t[r + q * nb] * S[q + jj * nb];
+      col[r] = -b * s;
+    }
+    __syncthreads();
+    if (r < jj) t[r + jj * nb] = col[r];
+    if (r == 0) t[jj + jj * nb] = b;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < nb * nb; i += blockDim.x) T[i] = t[i];
+}
+
+// out[:, k] = U[:, perm[k]]
+__global__ void permute_columns_kernel(const double* __restrict__ U, int64_t p,
+                                       const int* __restrict__ perm, double* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t k = blockIdx.y;
+  if (i < p) out[i + k * p] = U[i + (int64_t)perm[k] * p];
+}
+
+// Column-major transpose: out[j + i p] = in[i + j p].
+__global__ void transpose_sq_kernel(const double* __restrict__ in, int64_t p,
+                                    double* __restrict__ out) {
+  __shared__ double tile[32][33];
+  const int64_t i0 = (int64_t)blockIdx.x * 32, j0 = (int64_t)blockIdx.y * 32;
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int64_t i = i0 + threadIdx.x, j = j0 + dy;
+    if (i < p && j < p) tile[dy][threadIdx.x] = in[i + j * p];
+  }
+  __syncthreads();
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int64_t j = j0 + threadIdx.x, i = i0 + dy;
+    if (i < p && j < p) out[j + i * p] = tile[threadIdx.x][dy];
+  }
+}
+
+// A = the lower triangle mirrored (the eigensolver reads the lower triangle).
+__global__ void mirror_lower_kernel(double* __restrict__ A, int64_t p) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y;
+  if (i < j && j < p) A[i + j * p] = A[j + i * p];
+}
+
+unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+constexpr int NB = 32;                 // reflectors per WY block
+constexpr double CLUSTER_TOL = 1e-8;   // eigenvalues closer than this x ||T||: one cluster
+
+// Scratch slots 46..52 belong to this file.
+constexpr int SLOT_U = 46, SLOT_Z = 47, SLOT_G = 48, SLOT_SMALL = 49, SLOT_WS = 50,
+              SLOT_WY = 51, SLOT_META = 52;
+
+}  // namespace
+
+shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+                  int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                  cudaStream_t s) {
+  if (m <= 0 || n <= 0) return SHRK_OK;
+  if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX) {
+    set_error("dgemm: dimensions must be below 2^31");
+    return SHRK_EINVAL;
+  }
+  const dim3 grid(cdiv(m, GT), cdiv(n, GT));
+  LaunchScope ls("dgemm", s);
+  if (!ta && !tb) dgemm_kernel<false, false><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
+  else if (!ta && tb) dgemm_kernel<false, true><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
+  else if (ta && !tb) dgemm_kernel<true, false><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
+  else dgemm_kernel<true, true><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
+  SHRK_CUDA(cudaGetLastError());
+  return SHRK_OK;
+}
+
+shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaStream_t s) {
+  w_host.assign((size_t)p, 0.0);
+  if (p <= 0) return SHRK_OK;
+  const int64_t P2 = p * p;
+  void *small = nullptr, *zt = nullptr, *u = nullptr;
+  // small: d, e, e2, vhead, beta, pv, scal (+2), part (<= 4096), lam, perm
+  SHRK_TRY(scratch_get(SLOT_SMALL, sizeof(double) * (8 * (size_t)p + 4096 + 16), &small));
+  double* d = (double*)small;
+  double* e = d + p;
+  double* e2 = e + p;
+  double* vhead = e2 + p;
+  double* beta = vhead + p;
+  double* pv = beta + p;
+  double* lam = pv + p;
+  int* perm = (int*)(lam + p);  // p ints in the room of p/2 doubles (8p doubles reserved)
+  double* scal = lam + 2 * p;
+  double* part = scal + 16;
+  SHRK_TRY(scratch_get(SLOT_Z, sizeof(double) * (size_t)P2, &zt));
+  SHRK_TRY(scratch_get(SLOT_U, sizeof(double) * (size_t)P2, &u));
+  double* Zt = (double*)zt;
+  double* U = (double*)u;
+
+  // 0. symmetric input from its lower triangle
+  {
+    LaunchScope ls("eigh_tridiag", s);
+    mirror_lower_kernel<<<dim3(cdiv(p, 256), (unsigned)p), 256, 0, s>>>(A, p);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  // 1. tridiagonalisation (cooperative: all CTAs resident)
+  {
+    int dev = 0, sms = 0, per_sm = 0;
+    SHRK_CUDA(cudaGetDevice(&dev));
+    SHRK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SHRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tridiag_kernel, TRI_NT, 0));
+    if (per_sm < 1) {
+      set_error("eigensolver: the tridiagonalisation kernel cannot be resident");
+      return SHRK_ECUDA;
+    }
+    const int blocks = std::min(sms, 4096);
+    TriArgs ta{A, p, d, e, vhead, beta, pv, part, scal};
+    void* args[] = {&ta};
+    LaunchScope ls("eigh_tridiag", s);
+    SHRK_CUDA(cudaLaunchCooperativeKernel((const void*)tridiag_kernel, dim3(blocks), dim3(TRI_NT),
+                                          args, 0, s));
+  }
+  // 2. split T, Gershgorin bounds per block, eigenvalue slots (host; O(p))
+  std::vector<double> hd(p), he(std::max<int64_t>(p - 1, 1), 0.0);
+  SHRK_CUDA(cudaMemcpyAsync(hd.data(), d, sizeof(double) * p, cudaMemcpyDeviceToHost, s));
+  if (p > 1)
+    SHRK_CUDA(cudaMemcpyAsync(he.data(), e, sizeof(double) * (p - 1), cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  const double eps = 2.220446049250313e-16;
+  double tnorm = 0.0;
+  for (int64_t i = 0; i < p; ++i) {
+    const double r = (i > 0 ? std::fabs(he[i - 1]) : 0.0) + (i + 1 < p ? std::fabs(he[i]) : 0.0);
+    tnorm = std::max(tnorm, std::fabs(hd[i]) + r);
+  }
+  if (!(tnorm > 0.0)) tnorm = 1.0;
+  if (!std::isfinite(tnorm)) {
+    set_error("symmetric eigendecomposition: the matrix has non-finite entries");
+    return SHRK_EINVAL;
+  }
+  // negligible off-diagonals split T (dstebz's relative criterion)
+  std::vector<double> he2(std::max<int64_t>(p - 1, 1), 0.0);
+  std::vector<int> bstart{0};
+  for (int64_t i = 0; i + 1 < p; ++i) {
+    const double t2 = he[i] * he[i];
+    if (t2 <= eps * eps * std::fabs(hd[i] * hd[i + 1]) + 1e-300) {
+      he[i] = 0.0;
+      bstart.push_back((int)(i + 1));
+    }
+    he2[i] = he[i] * he[i];
+  }
+  bstart.push_back((int)p);
+  const double pivmin = 1e-300 * std::max(1.0, tnorm * tnorm);
+  std::vector<EigSlot> hslots(p);
+  for (size_t b = 0; b + 1 < bstart.size(); ++b) {
+    const int b0 = bstart[b], b1 = bstart[b + 1];
+    double lo = INFINITY, hi = -INFINITY;
+    for (int i = b0; i < b1; ++i) {
+      const double r = (i > b0 ? std::fabs(he[i - 1]) : 0.0) + (i + 1 < b1 ? std::fabs(he[i]) : 0.0);
+      lo = std::min(lo, hd[i] - r);
+      hi = std::max(hi, hd[i] + r);
+    }
+    const double pad = 2.0 * eps * tnorm + 2.0 * pivmin;
+    for (int i = b0; i < b1; ++i) hslots[i] = EigSlot{b0, b1, i - b0, 0, lo - pad, hi + pad};
+  }
+  void* meta = nullptr;
+  SHRK_TRY(scratch_get(SLOT_META, sizeof(EigSlot) * (size_t)p + sizeof(Cluster) * (size_t)p + 256,
+                       &meta));
+  EigSlot* dslots = (EigSlot*)meta;
+  Cluster* dcl = (Cluster*)(dslots + p);
+  SHRK_CUDA(cudaMemcpyAsync(e, he.data(), sizeof(double) * std::max<int64_t>(p - 1, 0),
+                            cudaMemcpyHostToDevice, s));
+  SHRK_CUDA(cudaMemcpyAsync(e2, he2.data(), sizeof(double) * std::max<int64_t>(p - 1, 0),
+                            cudaMemcpyHostToDevice, s));
+  SHRK_CUDA(cudaMemcpyAsync(dslots, hslots.data(), sizeof(EigSlot) * p, cudaMemcpyHostToDevice, s));
+  {
+    LaunchScope ls("eigh_bisect", s);
+    bisect_kernel<<<cdiv(p * 32, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  // 3. clusters of close eigenvalues inside each block (host), inverse iteration
+  std::vector<double> hl(p);
+  SHRK_CUDA(cudaMemcpyAsync(hl.data(), lam, sizeof(double) * p, cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  std::vector<Cluster> hcl;
+  for (size_t b = 0; b + 1 < bstart.size(); ++b) {
+    const int b0 = bstart[b], b1 = bstart[b + 1];
+    int k = b0;
+    while (k < b1) {
+      int g = k + 1;
+      while (g < b1 && hl[g] - hl[g - 1] < CLUSTER_TOL * tnorm) ++g;
+      hcl.push_back(Cluster{k, g - k, b0, b1});
+      k = g;
+    }
+  }
+  const int ncl = (int)hcl.size();
+  SHRK_CUDA(cudaMemcpyAsync(dcl, hcl.data(), sizeof(Cluster) * ncl, cudaMemcpyHostToDevice, s));
+  void* ws = nullptr;
+  SHRK_TRY(scratch_get(SLOT_WS, sizeof(double) * 4 * (size_t)ncl * (size_t)p, &ws));
+  SHRK_CUDA(cudaMemsetAsync(Zt, 0, sizeof(double) * (size_t)P2, s));
+  {
+    LaunchScope ls("eigh_inverse_iteration", s);
+    inverse_iteration_kernel<<<cdiv(ncl, 128), 128, 0, s>>>(d, e, lam, dcl, ncl, p, tnorm,
+                                                            (double*)ws, Zt);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  // one Newton-Schulz step on the basis: Z <- Z (3I - Z^T Z)/2, in the
+  // transposed storage Zt: G = Zt Zt^T, Zt <- M Zt
+  void* gbuf = nullptr;
+  SHRK_TRY(scratch_get(SLOT_G, sizeof(double) * (size_t)P2, &gbuf));
+  double* G = (double*)gbuf;
+  SHRK_TRY(dgemm(false, true, p, p, p, 1.0, Zt, p, Zt, p, 0.0, G, p, s));
+  {
+    LaunchScope ls("eigh_orthogonalise", s);
+    ns_matrix_kernel<<<dim3(cdiv(p, 256), (unsigned)p), 256, 0, s>>>(G, p);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  SHRK_TRY(dgemm(false, false, p, p, p, 1.0, G, p, Zt, p, 0.0, U, p, s));  // U = (Z M)^T
+  {
+    LaunchScope ls("eigh_orthogonalise", s);
+    transpose_sq_kernel<<<dim3(cdiv(p, 32), cdiv(p, 32)), dim3(32, 8), 0, s>>>(U, p, Zt);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  double* Zc = Zt;  // now Z, column-major
+  // 4. back-transformation Zc <- H_0 ... H_{p-3} Zc, blocks from the last
+  const int64_t nref = std::max<int64_t>(p - 2, 0);
+  if (nref > 0) {
+    void* wy = nullptr;
+    SHRK_TRY(scratch_get(SLOT_WY, sizeof(double) * ((size_t)p * NB * 3 + 2 * NB * NB), &wy));
+    double* Y = (double*)wy;
+    double* W = Y + (size_t)p * NB;
+    double* W2 = W + (size_t)p * NB;
+    double* S = W2 + (size_t)p * NB;
+    double* T = S + NB * NB;
+    for (int64_t j0 = ((nref - 1) / NB) * NB; j0 >= 0; j0 -= NB) {
+      const int nb = (int)std::min<int64_t>(NB, nref - j0);
+      const int64_t n = p - j0 - 1;
+      {
+        LaunchScope ls("eigh_back_transform", s);
+        build_y_kernel<<<dim3(cdiv(n, 256), (unsigned)nb), 256, 0, s>>>(A, vhead, p, j0, nb, Y);
+        SHRK_CUDA(cudaGetLastError());
+      }
+      SHRK_TRY(dgemm(true, false, nb, nb, n, 1.0, Y, n, Y, n, 0.0, S, nb, s));
+      {
+        LaunchScope ls("eigh_back_transform", s);
+        wy_t_kernel<<<1, 64, 0, s>>>(S, beta, j0, nb, T);
+        SHRK_CUDA(cudaGetLastError());
+      }
+      double* Zs = Zc + (j0 + 1);  // rows j0+1 .. p-1 of Zc (leading dimension p)
+      SHRK_TRY(dgemm(true, false, nb, p, n, 1.0, Y, n, Zs, p, 0.0, W, nb, s));     // W = Y^T Zs
+      SHRK_TRY(dgemm(false, false, nb, p, nb, 1.0, T, nb, W, nb, 0.0, W2, nb, s));  // W2 = T W
+      SHRK_TRY(dgemm(false, false, n, p, nb, -1.0, Y, n, W2, nb, 1.0, Zs, p, s));   // Zs -= Y W2
+    }
+  }
+  // ascending eigenvalues; eigenvector columns in that order, into A
+  std::vector<int> hperm(p);
+  std::iota(hperm.begin(), hperm.end(), 0);
+  std::stable_sort(hperm.begin(), hperm.end(), [&](int x, int y) { return hl[x] < hl[y]; });
+  for (int64_t k = 0; k < p; ++k) w_host[k] = hl[hperm[k]];
+  SHRK_CUDA(cudaMemcpyAsync(perm, hperm.data(), sizeof(int) * p, cudaMemcpyHostToDevice, s));
+  {
+    LaunchScope ls("eigh_back_transform", s);
+    permute_columns_kernel<<<dim3(cdiv(p, 256), (unsigned)p), 256, 0, s>>>(Zc, p, perm, A);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  SHRK_CUDA(cudaStreamSynchronize(s));
+  return SHRK_OK;
+}
+
+}  // namespace shrk

@@ -9,16 +9,17 @@
 // the NUFFT policy of src/stieltjes/nufft.rs (33-126, entry points 164-220).
 // Pipeline (all FP64), stencil width N = 2/4/6/8 a template parameter:
 //
-//   1. weights      one thread per source: stencil cell i0 = floor((v-lo)/dx)
-//                   and the N Lagrange weights of t = pos - i0.
-//   2. runs         the last source of each run of equal cells marks it;
-//                   an exclusive max-scan turns the marks into first[key] =
-//                   the first source with cell >= key.
-//   3. gather+pack  one thread per grid cell adds the weights of its sources
+//   1. runs         a source's stencil cell is i0 = floor((v-lo)/dx); the
+//                   sources are sorted, so the cells are too, and one thread
+//                   per cell key bisects for first[key] = the first source
+//                   with cell >= key.
+//   2. gather+pack  one thread per grid cell adds the weights of its sources
 //                   (at most 32) run by run in ascending source order -- the
 //                   order of the reference's sequential splat, so these
 //                   densities are the same sums, without atomics -- and
-//                   queues denser cells for one warp (or one CTA) each.
+//                   queues denser cells for one warp (or one CTA) each.  The
+//                   N Lagrange weights of t = pos - i0 are recomputed where
+//                   they are added (sources come from L2; no weight array).
 //                   packed[c] = density[c] + i x_c/(x_c^2 + eta^2).
 //   4. fft          four-step FFT m = m1*m2 (m1, m2 <= 2048): column FFTs of
 //                   length m1 in shared memory with the inter-pass twiddle,
@@ -33,7 +34,7 @@
 #include "epilogue.cuh"
 #include "internal.h"
 
-#include <cub/cub.cuh>
+#include <cooperative_groups.h>
 
 #include <atomic>
 #include <cmath>
@@ -41,6 +42,8 @@
 #include <string>
 
 namespace shrk {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -114,8 +117,6 @@ struct GridArgs {
   int rev;            // 1: visit the sources in descending order (dx < 0)
   double lo, dx, eta;
   int64_t m;
-  int* cell;          // per visited source: stencil cell, clamped to [-N, m + N]
-  double* w;          // per visited source: the N stencil weights, SoA [N][ns]
   double2* packed;
 };
 
@@ -126,21 +127,38 @@ __device__ __forceinline__ int clamped_cell(const GridArgs& a, int64_t j, double
   return (int)(i0 < -N ? -N : (i0 > a.m + N ? a.m + N : i0));
 }
 
-// Per source: stencil cell and weights (fft5.rs:175-185).  The visiting order
-// makes cell[] non-decreasing; the last source of each run of equal cells
-// also records last[cell - k_lo] = its index + 1 (k_lo = -N - 1).
-template <int N>
-__global__ void splat_weights_kernel(const GridArgs a, int* __restrict__ last) {
-  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.ns) return;
-  double t, t_next;
-  const int ci = clamped_cell<N>(a, j, &t);
+// Stencil weight k of visited source j (fft5.rs:136-164, 175-185): the same
+// arithmetic as the k-th entry of lagrange<N>, recomputed where it is summed
+// (k is a compile-time constant at every call, so only that weight's
+// operations remain).  Sources are read through L2; no weight array.
+template <int N, int K>
+__device__ __forceinline__ double weight_of(const GridArgs& a, int64_t j) {
+  double t;
+  (void)clamped_cell<N>(a, j, &t);
   double w[N];
   lagrange<N>(t, w);
-  a.cell[j] = ci;
-#pragma unroll
-  for (int k = 0; k < N; ++k) a.w[(int64_t)k * a.ns + j] = w[k];
-  if (j == a.ns - 1 || clamped_cell<N>(a, j + 1, &t_next) != ci) last[ci + N + 1] = (int)(j + 1);
+  return w[K];
+}
+
+// first[key + N + 1] for every key in [-N - 1, m + N]: the number of visited
+// sources whose clamped stencil cell is below key.  Visiting order makes the
+// cells non-decreasing, so this is a lower bound found by bisection (the same
+// cell computation as everywhere else, so the same runs).
+template <int N>
+__global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n_keys,
+                            int* __restrict__ n_dense) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < 2) n_dense[idx] = 0;  // the dense-cell queues start empty
+  if (idx >= n_keys) return;
+  const int key = (int)(idx - N - 1);
+  int64_t lo = 0, hi = a.ns;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    double t;
+    if (clamped_cell<N>(a, mid, &t) < key) lo = mid + 1;
+    else hi = mid;
+  }
+  first[idx] = (int)lo;
 }
 
 constexpr int DENSE_MIN = 32;    // sources above which a cell gets a whole warp
@@ -151,11 +169,6 @@ struct GatherArgs {
   const int* first;  // first[key + N + 1] = #sources with cell < key, key in [-N-1, m+N]
   int* dense;        // cells left for pack_dense_kernel: [0, m) warp queue, [m, 2m) CTA queue
   int* n_dense;      // the two queue lengths
-};
-
-// Exclusive max-scan operator: first[key] = max over cells below key of last[].
-struct MaxOp {
-  __device__ __forceinline__ int operator()(int x, int y) const { return x > y ? x : y; }
 };
 
 // Steps 1+pack: the density of cell c is the sum of weight k over the run of
@@ -171,6 +184,19 @@ __device__ __forceinline__ void pack_cell(const GridArgs& a, int64_t c, double d
   const double x = sd * a.dx;
   const double denom = x * x + a.eta * a.eta;
   a.packed[c] = make_double2(dens, x / denom);
+}
+
+// dens += weight K of every source of the run of cell c + N/2 - 1 - K, for
+// K = KK .. 0 in that order: the runs in ascending cell order, each run in
+// ascending source order (the sequential splat's order).
+template <int N, int KK>
+__device__ __forceinline__ void run_sums(const GridArgs& a, const int* first, int64_t c,
+                                         double& dens) {
+  if constexpr (KK >= 0) {
+    const int64_t e = c + N / 2 - 1 - KK;
+    for (int64_t j = first[e], j1 = first[e + 1]; j < j1; ++j) dens += weight_of<N, KK>(a, j);
+    run_sums<N, KK - 1>(a, first, c, dens);
+  }
 }
 
 template <int N>
@@ -189,23 +215,21 @@ __global__ void __launch_bounds__(256) pack_sparse_kernel(const GatherArgs ga) {
       ga.dense[q * m + atomicAdd(ga.n_dense + q, 1)] = (int)c;
       return;
     }
-#pragma unroll
-    for (int k = N - 1; k >= 0; --k) {
-      const int64_t e = c + H - 1 - k;
-      const double* wk = a.w + (int64_t)k * a.ns;
-      for (int64_t j = first[e], j1 = first[e + 1]; j < j1; ++j) dens += wk[j];
-    }
+    run_sums<N, N - 1>(a, first, c, dens);
   } else {
     // edge cell: every slot whose clamped index lands here, sources then slots
     const int64_t j0 = (c == 0) ? 0 : first[m - 1 - H];
     const int64_t j1 = (c == 0) ? first[H] : a.ns;
     for (int64_t j = j0; j < j1; ++j) {
-      const int i0 = a.cell[j];
+      double t;
+      const int i0 = clamped_cell<N>(a, j, &t);
+      double w[N];
+      lagrange<N>(t, w);
 #pragma unroll
       for (int k = 0; k < N; ++k) {
         int64_t cell = (int64_t)i0 - H + 1 + k;
         cell = cell < 0 ? 0 : (cell > m - 1 ? m - 1 : cell);
-        if (cell == c) dens += a.w[(int64_t)k * a.ns + j];
+        if (cell == c) dens += w[k];
       }
     }
   }
@@ -218,18 +242,22 @@ __global__ void __launch_bounds__(256) pack_sparse_kernel(const GatherArgs ga) {
 // striding the runs, a butterfly at the end.  Deterministic, not the
 // sequential order; CTAs and warps stride the queues, whose lengths are read
 // on the device.
+template <int N, int KK>
+__device__ __forceinline__ void strided_run_sums(const GridArgs& a, const int* first, int c, int t,
+                                                 int nt, double& dens) {
+  if constexpr (KK >= 0) {
+    const int e = c + N / 2 - 1 - KK;  // the run of cell e feeds slot KK
+    const int64_t j1 = first[e + 1];
+    for (int64_t j = first[e] + t; j < j1; j += nt) dens += weight_of<N, KK>(a, j);
+    strided_run_sums<N, KK - 1>(a, first, c, t, nt, dens);
+  }
+}
+
 template <int N>
 __device__ __forceinline__ double window_sum(const GatherArgs& ga, const int* first, int c,
                                              int t, int nt) {
-  constexpr int H = N / 2;
   double dens = 0.0;
-#pragma unroll
-  for (int k = N - 1; k >= 0; --k) {
-    const int e = c + H - 1 - k;  // the run of cell e feeds slot k
-    const double* wk = ga.g.w + (int64_t)k * ga.g.ns;
-    const int64_t j1 = first[e + 1];
-    for (int64_t j = first[e] + t; j < j1; j += nt) dens += wk[j];
-  }
+  strided_run_sums<N, N - 1>(ga.g, first, c, t, nt, dens);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) dens += __shfl_xor_sync(0xffffffffu, dens, o);
   return dens;
@@ -515,6 +543,190 @@ __global__ void spectral_kernel(const double2* __restrict__ C, const double* __r
   out[k] = make_double2(ih_re - rh.y, ih_im + rh.x);
 }
 
+// ------------------------------------------- fused grid transform (cluster) --
+// For grids of FUSED_MIN_M .. FUSED_MAX_M cells (every NUFFT grid, and the
+// fft5 grids of small spectra) the whole frequency-domain step -- forward
+// four-step FFT, the spectral product, inverse four-step FFT -- runs in ONE
+// launch: a cluster of FC CTAs holds the grid in shared memory (m/FC complex
+// values per CTA, ~148 KB at m = 65 536) and exchanges it through distributed
+// shared memory instead of global memory between the passes.
+//
+//   forward, m = m1 m2:   rows = columns n2 of x[m2 n1 + n2]; CTA r owns n2 in
+//                         [r G1, (r+1) G1), G1 = m2/FC; length-m1 FFTs, then
+//                         the twiddle W^{n2 k1}.
+//   transpose (DSMEM)     CTA r takes rows k1 in [r G2, (r+1) G2), G2 = m1/FC;
+//                         length-m2 FFTs give X[k1 + m1 k2].
+//   spectral (DSMEM)      out[k] from X[k] and X[m-k] (the partner row lives in
+//                         another CTA), written in place after a cluster
+//                         barrier.
+//   inverse, m = m2 m1:   input index k = k1 + m1 k2 = m1 n1' + n2' with
+//                         n2' = k1: the rows each CTA holds are already the
+//                         inverse's first-pass columns; length-m2 FFTs and
+//                         the twiddle W^{+k1 k1'}.
+//   transpose (DSMEM)     rows k1' in [r G1, (r+1) G1); length-m1 FFTs give
+//                         the grid at k1' + m2 k2', stored to global memory.
+//
+// Every phase holds exactly m/FC values per CTA, 8 per thread, so the same
+// row_fft serves all four transforms (the stage twiddles of the four
+// (length, sign) pairs sit in shared memory).  A value moves between CTAs
+// through registers: all threads read their remote values, a cluster barrier
+// makes sure every CTA has read, then each writes its own shared memory.
+constexpr int FC = 8;                   // CTAs per cluster (portable size)
+constexpr int64_t FUSED_MIN_M = 2048;
+constexpr int64_t FUSED_MAX_M = 65536;  // 1024 threads x 8 values x FC
+
+struct FusedArgs {
+  const double2* packed;  // [m] density + i x/(x^2 + eta^2)
+  double2* grid;          // [m] unnormalised inverse transform of the product
+  const double2* tw;      // [m] (cos, sin)(2 pi j/m)
+  const double* ke;       // [m] even-kernel spectrum
+  int m1, m2;             // forward factorisation m = m1 m2 (powers of two)
+  int64_t m;
+};
+
+__host__ __device__ __forceinline__ int row_pad(int L) { return L + (L >> 3) + 1; }
+
+__host__ __device__ __forceinline__ size_t fused_smem_bytes(int m1, int m2) {
+  const int G1 = m2 / FC, G2 = m1 / FC;
+  const int a = G1 * row_pad(m1), b = G2 * row_pad(m2);
+  return sizeof(double2) * ((size_t)(a > b ? a : b) + 2 * (size_t)m1 + 2 * (size_t)m2);
+}
+
+// Spectral product of fftplan.rs:43-76 for one k (as spectral_kernel).
+__device__ __forceinline__ double2 spectral_at(double2 ck, double2 cn, double kev) {
+  const double2 cnc = make_double2(cn.x, -cn.y);
+  const double2 s = make_double2(ck.x + cnc.x, ck.y + cnc.y);
+  const double2 df = make_double2(ck.x - cnc.x, ck.y - cnc.y);
+  const double2 D = make_double2(0.5 * s.x, 0.5 * s.y);
+  const double2 K = make_double2(0.5 * df.y, -0.5 * df.x);  // (-0.5 i) * df
+  const double ih_re = D.x * kev, ih_im = D.y * kev;
+  const double2 rh = cmul(D, K);
+  return make_double2(ih_re - rh.y, ih_im + rh.x);
+}
+
+__global__ void __cluster_dims__(FC, 1, 1) __launch_bounds__(1024, 1)
+    grid_transform_cluster(const FusedArgs a) {
+  extern __shared__ double2 fsm[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int r = (int)cl.block_rank();
+  const int tid = threadIdx.x, nt = blockDim.x;  // nt = m / (8 FC)
+  const int m1 = a.m1, m2 = a.m2;
+  const int64_t m = a.m;
+  const int G1 = m2 / FC, G2 = m1 / FC;
+  const int lg1 = __ffs(G1) - 1, lg2 = __ffs(G2) - 1, lm1 = __ffs(m1) - 1;
+  const int P1 = row_pad(m1), P2 = row_pad(m2);
+  const int da = G1 * P1, db = G2 * P2;
+  double2* data = fsm;
+  double2* tw_f1 = fsm + (da > db ? da : db);  // (m1, -), (m2, -), (m2, +), (m1, +)
+  double2* tw_f2 = tw_f1 + m1;
+  double2* tw_i1 = tw_f2 + m2;
+  double2* tw_i2 = tw_i1 + m2;
+  load_stage_twiddles(tw_f1, a.tw, m1, m, -1.0);
+  load_stage_twiddles(tw_f2, a.tw, m2, m, -1.0);
+  load_stage_twiddles(tw_i1, a.tw, m2, m, +1.0);
+  load_stage_twiddles(tw_i2, a.tw, m1, m, +1.0);
+  double2 v[8];
+
+  // forward pass 1: rows g = columns n2 = r G1 + g, element n1 at padi(n1)
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    const int g = e & (G1 - 1), n1 = e >> lg1;
+    v[it] = a.packed[(int64_t)m2 * n1 + r * G1 + g];
+  }
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    data[(e & (G1 - 1)) * P1 + padi(e >> lg1)] = v[it];
+  }
+  __syncthreads();
+  row_fft(data + (tid / (m1 >> 3)) * P1, tw_f1, m1, tid % (m1 >> 3), -1.0);
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {  // twiddle W^{-n2 k1}
+    const int e = tid + it * nt;
+    const int g = e & (G1 - 1), k1 = e >> lg1;
+    const double2 w = a.tw[((int64_t)(r * G1 + g) * k1) & (m - 1)];
+    double2* x = &data[g * P1 + padi(k1)];
+    *x = cmul(*x, make_double2(w.x, -w.y));
+  }
+  cl.sync();
+
+  // transpose: rows k1 = r G2 + g2 over n2; (k1, n2) is in CTA n2 / G1
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    const int g2 = e & (G2 - 1), n2 = e >> lg2;
+    const double2* rem = cl.map_shared_rank(data, n2 >> lg1);
+    v[it] = rem[(n2 & (G1 - 1)) * P1 + padi(r * G2 + g2)];
+  }
+  cl.sync();
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    data[(e & (G2 - 1)) * P2 + padi(e >> lg2)] = v[it];
+  }
+  __syncthreads();
+  row_fft(data + (tid / (m2 >> 3)) * P2, tw_f2, m2, tid % (m2 >> 3), -1.0);
+  cl.sync();  // X[k1 + m1 k2] complete in every CTA
+
+  // spectral product: partner X[m - k] from the CTA holding row (m - k) mod m1
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    const int g2 = e & (G2 - 1), k2 = e >> lg2;
+    const int64_t k = (int64_t)(r * G2 + g2) + (int64_t)m1 * k2;
+    const int64_t kp = (m - k) & (m - 1);
+    const int kp1 = (int)(kp & (m1 - 1)), kp2 = (int)(kp >> lm1);
+    const double2* rem = cl.map_shared_rank(data, kp1 >> lg2);
+    v[it] = spectral_at(data[g2 * P2 + padi(k2)], rem[(kp1 & (G2 - 1)) * P2 + padi(kp2)],
+                        a.ke[k]);
+  }
+  cl.sync();
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    data[(e & (G2 - 1)) * P2 + padi(e >> lg2)] = v[it];
+  }
+  __syncthreads();
+
+  // inverse pass 1 on the same rows (n2' = k1), length m2, twiddle W^{+k1 k1'}
+  row_fft(data + (tid / (m2 >> 3)) * P2, tw_i1, m2, tid % (m2 >> 3), +1.0);
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    const int g2 = e & (G2 - 1), k1p = e >> lg2;
+    const double2 w = a.tw[((int64_t)(r * G2 + g2) * k1p) & (m - 1)];
+    double2* x = &data[g2 * P2 + padi(k1p)];
+    *x = cmul(*x, w);
+  }
+  cl.sync();
+
+  // transpose: rows k1' = r G1 + g3 over n2' = k1; (k1', k1) is in CTA k1 / G2
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    const int g3 = e & (G1 - 1), k1 = e >> lg1;
+    const double2* rem = cl.map_shared_rank(data, k1 >> lg2);
+    v[it] = rem[(k1 & (G2 - 1)) * P2 + padi(r * G1 + g3)];
+  }
+  cl.sync();  // last remote read: no CTA leaves while another still reads it
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    data[(e & (G1 - 1)) * P1 + padi(e >> lg1)] = v[it];
+  }
+  __syncthreads();
+  row_fft(data + (tid / (m1 >> 3)) * P1, tw_i2, m1, tid % (m1 >> 3), +1.0);
+
+  // the grid at k1' + m2 k2'
+#pragma unroll
+  for (int it = 0; it < 8; ++it) {
+    const int e = tid + it * nt;
+    const int g3 = e & (G1 - 1), k2p = e >> lg1;
+    a.grid[(int64_t)(r * G1 + g3) + (int64_t)m2 * k2p] = data[g3 * P1 + padi(k2p)];
+  }
+}
+
 struct InterpArgs {
   const double* q;
   int64_t nq;
@@ -670,6 +882,43 @@ shrk_status fft(double2* buf, double2* tmp, int64_t m, const double2* tw, double
   return SHRK_OK;
 }
 
+// The frequency-domain step of a grid of FUSED_MIN_M .. FUSED_MAX_M cells in
+// one cluster launch (A -> B).  *done is false when the device cannot place
+// the cluster (then the caller runs the multi-pass transform).
+shrk_status fused_transform(const double2* A, double2* B, int64_t m, const Tables* T,
+                            const char* family, cudaStream_t s, bool* done) {
+  *done = false;
+  const int bits = ilog2(m);
+  const int m1 = 1 << ((bits + 1) / 2), m2 = 1 << (bits / 2);
+  const size_t smem = fused_smem_bytes(m1, m2);
+  static std::atomic<int> usable[64];  // 0 unknown, 1 yes, -1 no
+  int dev = 0;
+  SHRK_CUDA(cudaGetDevice(&dev));
+  const bool known = dev >= 0 && dev < 64;
+  if (!known || usable[dev].load() == 0) {
+    SHRK_CUDA(cudaFuncSetAttribute(grid_transform_cluster,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)fused_smem_bytes(256, 256)));
+    cudaLaunchConfig_t cfg = {};  // the cluster size is the kernel's compile-time one
+    cfg.gridDim = dim3(FC);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = fused_smem_bytes(256, 256);
+    int clusters = 0;
+    const cudaError_t e =
+        cudaOccupancyMaxActiveClusters(&clusters, grid_transform_cluster, &cfg);
+    if (e != cudaSuccess) cudaGetLastError();
+    if (known) usable[dev] = (e == cudaSuccess && clusters >= 1) ? 1 : -1;
+    if (!(e == cudaSuccess && clusters >= 1)) return SHRK_OK;
+  }
+  if (usable[dev].load() < 0) return SHRK_OK;
+  FusedArgs fa{A, B, T->tw, T->ke, m1, m2, m};
+  LaunchScope ls(family, s);
+  grid_transform_cluster<<<FC, (unsigned)(m / (8 * FC)), smem, s>>>(fa);
+  SHRK_CUDA(cudaGetLastError());
+  *done = true;
+  return SHRK_OK;
+}
+
 // One grid: stencil width, size, origin and spacing, and the launch families
 // its kernels are timed under.
 struct GridPlan {
@@ -693,37 +942,20 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   double2* A = (double2*)w;
   double2* B = A + m;
   double2* Tmp = B + m;
-  // slot 24: weights [N][ns] | cells [ns] | last [K] | first [K] | queues [2m] |
-  // queue lengths [2] | scan temporaries, K = m + 2N + 2 keys from -N - 1.
+  // slot 24: first [K] | queues [2m] | queue lengths [2], K = m + 2N + 2 keys
+  // from -N - 1.
   const int64_t n_keys = m + 2 * N + 2;
-  size_t scan_bytes = 0;
-  SHRK_CUDA(cub::DeviceScan::ExclusiveScan(nullptr, scan_bytes, (const int*)nullptr,
-                                           (int*)nullptr, MaxOp(), 0, (int)n_keys, s));
-  const size_t head = sizeof(double) * N * (size_t)ns +
-                      sizeof(int) * ((size_t)ns + 2 * n_keys + 2 * m + 2);
-  const size_t head_al = (head + 255) & ~(size_t)255;
   void* sw = nullptr;
-  SHRK_TRY(scratch_get(24, head_al + scan_bytes, &sw));
-  double* wts = (double*)sw;
-  int* cell = (int*)(wts + (int64_t)N * ns);
-  int* last = cell + ns;
-  int* first = last + n_keys;
+  SHRK_TRY(scratch_get(24, sizeof(int) * ((size_t)n_keys + 2 * (size_t)m + 2), &sw));
+  int* first = (int*)sw;
   int* dense = first + n_keys;
   int* n_dense = dense + 2 * m;
-  void* scan_tmp = (char*)sw + head_al;
-  GridArgs ga{d_src, ns, g.dx < 0.0 ? 1 : 0, g.lo, g.dx, eta, m, cell, wts, A};
+  GridArgs ga{d_src, ns, g.dx < 0.0 ? 1 : 0, g.lo, g.dx, eta, m, A};
   GatherArgs gg{ga, first, dense, n_dense};
-  SHRK_CUDA(cudaMemsetAsync(last, 0, sizeof(int) * n_keys, s));
-  SHRK_CUDA(cudaMemsetAsync(n_dense, 0, 2 * sizeof(int), s));
   {
     LaunchScope ls(g.fam_splat, s);
-    splat_weights_kernel<N><<<blocks_for(ns, 256), 256, 0, s>>>(ga, last);
+    keys_kernel<N><<<blocks_for(n_keys, 256), 256, 0, s>>>(ga, first, n_keys, n_dense);
     SHRK_CUDA(cudaGetLastError());
-  }
-  {
-    LaunchScope ls(g.fam_splat, s);
-    SHRK_CUDA(cub::DeviceScan::ExclusiveScan(scan_tmp, scan_bytes, (const int*)last, first,
-                                             MaxOp(), 0, (int)n_keys, s));
   }
   {
     LaunchScope ls(g.fam_splat, s);
@@ -736,13 +968,17 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
     pack_dense_kernel<N><<<nb, 256, 0, s>>>(gg);
     SHRK_CUDA(cudaGetLastError());
   }
-  SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, g.fam_fft, s));
-  {
-    LaunchScope ls(g.fam_spectral, s);
-    spectral_kernel<<<blocks_for(m, 256), 256, 0, s>>>(A, T->ke, B, m);
-    SHRK_CUDA(cudaGetLastError());
+  bool fused = false;
+  if (m >= FUSED_MIN_M && m <= FUSED_MAX_M) SHRK_TRY(fused_transform(A, B, m, T, g.fam_fft, s, &fused));
+  if (!fused) {
+    SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, g.fam_fft, s));
+    {
+      LaunchScope ls(g.fam_spectral, s);
+      spectral_kernel<<<blocks_for(m, 256), 256, 0, s>>>(A, T->ke, B, m);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    SHRK_TRY(fft(B, Tmp, m, T->tw, +1.0, g.fam_fft, s));
   }
-  SHRK_TRY(fft(B, Tmp, m, T->tw, +1.0, g.fam_fft, s));
   InterpArgs ia{d_q, nq, B, m, g.lo, g.dx, 1.0 / (double)m, epi};
   {
     LaunchScope ls(g.fam_interp, s);

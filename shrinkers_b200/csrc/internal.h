@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/shrinkers_b200.h"
 
@@ -73,6 +74,9 @@ shrk_status batched(const double* d_ev, const int64_t* d_offsets, const int64_t*
 // not run yet, or if force) and writes (R, SL) for the 8 p-buckets into
 // table[16] (may be null).
 shrk_status batched_tune(int precision, bool force, int* table, cudaStream_t s);
+// Installs a table of the same layout (e.g. one saved from an earlier
+// process) for `precision` on the current device.
+shrk_status batched_set_tune(int precision, const int* table);
 
 // Epilogue over precomputed raw sums (n targets), same arithmetic as the
 // fused reduction of exact_pair_sums.
@@ -157,6 +161,16 @@ struct LibScope {
 // cores (TF32 x3) instead of FP64.
 shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc, double* d_re,
                     double* d_im, cudaStream_t s);
+
+// FP64 GEMM (eigh.cu): C = alpha op(A) op(B) + beta C, column-major,
+// op = transpose when ta / tb.
+shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
+                  int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
+                  cudaStream_t s);
+// Symmetric eigendecomposition of A (p x p column-major, lower triangle
+// read; overwritten by the eigenvectors, column j for the j-th smallest
+// eigenvalue); the eigenvalues ascending to w_host.  Synchronises s.
+shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaStream_t s);
 
 double mixed_near_k();
 // Sets the bulk-copy wait budget of the exact pair kernels (cycles; negative

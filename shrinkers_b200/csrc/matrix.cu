@@ -8,26 +8,24 @@
 // symmetric_eigh 502-585; and compute_angular_overlaps
 // (src/eigenvector_overlaps/overlaps.rs:26-46).
 //
-// The O(p^3) symmetric eigendecomposition is a library call (cuSOLVER
-// syevd; the reference's own docs point to LAPACK's dsyevd as the fast
-// path, its Jacobi iteration being the fallback).  The spectrum goes through
+// The O(p^3) symmetric eigendecomposition is this library's own (eigh.cu:
+// Householder tridiagonalisation, multisection, inverse iteration, WY
+// back-transformation; the reference runs a Jacobi iteration and its docs
+// point to LAPACK's dsyevd as the fast path).  The spectrum goes through
 // this library's RIE and inverse-shrinkage paths; the per-eigenvalue host
 // arithmetic (noise level, overlaps, bulk level) follows the reference's
 // order.  The reconstructions run on the device: the spiked covariance
 // d I + sum_t s_t v_t v_t^T over the k directions with a positive overlap --
-// an FP64 kernel in the reference's operation order for k <= 16, a cuBLAS
-// DGEMM (a plain library GEMM) above, since the overlap is positive for
-// every cleaned eigenvalue beyond sigma^2 (1 + sqrt(c)) and k can reach a
-// fair share of p -- and the precision matrix U diag(w) U^T as a DGEMM.
+// an FP64 kernel in the reference's operation order for k <= 16, the FP64
+// GEMM of eigh.cu above, since the overlap is positive for every cleaned
+// eigenvalue beyond sigma^2 (1 + sqrt(c)) and k can reach a fair share of
+// p -- and the precision matrix U diag(w) U^T by the same GEMM.
 //
 // Layouts: caller matrices are row-major p x p with eigenvectors as columns;
-// the device keeps the eigenvector matrix column-major (column j contiguous),
-// as syevd writes it.  Scratch slots 32..38 belong to this file.
+// the device keeps the eigenvector matrix column-major (column j contiguous).
+// Scratch slots 32..38 belong to this file.
 #include "common.cuh"
 #include "internal.h"
-
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -44,7 +42,6 @@ namespace {
 
 constexpr int SLOT_E = 32;      // eigenvectors, column-major p x p
 constexpr int SLOT_W = 33;      // eigenvalues / small vectors
-constexpr int SLOT_WORK = 34;   // syevd workspace
 constexpr int SLOT_IDX = 35;    // column indices, scales, flags
 constexpr int SLOT_OUT = 36;    // p x p result
 constexpr int SLOT_OUT2 = 37;   // p x p result (renormalised / eigenvectors)
@@ -53,38 +50,6 @@ constexpr int SLOT_TMP = 38;    // p x p staging (input, scaled columns)
 // Up to this many active directions the spiked covariance is summed by
 // spiked_reconstruct_kernel in the reference's order; beyond, by a DGEMM.
 constexpr int SMALL_K = 16;
-
-// Library handles of the running call's context (a handle is not shared
-// by concurrent calls).
-struct Handles {
-  cusolverDnHandle_t sol = nullptr;
-  cublasHandle_t blas = nullptr;
-  ~Handles() {
-    if (sol) cusolverDnDestroy(sol);
-    if (blas) cublasDestroy(blas);
-  }
-};
-
-shrk_status handles(cudaStream_t s, Handles** out) {
-  Handles& h = ctx_state<Handles>(EXT_MATRIX_HANDLES);
-  if (!h.sol && cusolverDnCreate(&h.sol) != CUSOLVER_STATUS_SUCCESS) {
-    h.sol = nullptr;
-    set_error("cusolverDnCreate failed");
-    return SHRK_ECUDA;
-  }
-  if (!h.blas && cublasCreate(&h.blas) != CUBLAS_STATUS_SUCCESS) {
-    h.blas = nullptr;
-    set_error("cublasCreate failed");
-    return SHRK_ECUDA;
-  }
-  if (cusolverDnSetStream(h.sol, s) != CUSOLVER_STATUS_SUCCESS ||
-      cublasSetStream(h.blas, s) != CUBLAS_STATUS_SUCCESS) {
-    set_error("cuSOLVER/cuBLAS stream binding failed");
-    return SHRK_ECUDA;
-  }
-  *out = &h;
-  return SHRK_OK;
-}
 
 unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
@@ -212,44 +177,13 @@ __global__ void symmetrize_kernel(double* __restrict__ m, int64_t p) {
 dim3 rows_grid(int64_t p, int t) { return dim3(nblocks(p, t), (unsigned)p); }
 dim3 tiles_grid(int64_t p) { return dim3(nblocks(p, 32), nblocks(p, 32)); }
 
-// syevd of the symmetric matrix in slot SLOT_E (overwritten by its
-// eigenvectors, column-major); ascending eigenvalues to the host.
-shrk_status syevd(int64_t p, std::vector<double>& w_host, cudaStream_t s) {
-  Handles* H = nullptr;
-  SHRK_TRY(handles(s, &H));
-  void *a = nullptr, *w = nullptr, *info = nullptr;
+// Eigendecomposition of the symmetric matrix in slot SLOT_E (its lower
+// triangle; overwritten by the eigenvectors, column-major, column j for the
+// j-th smallest eigenvalue); ascending eigenvalues to the host (eigh.cu).
+shrk_status eigh_sorted_slot(int64_t p, std::vector<double>& w_host, cudaStream_t s) {
+  void* a = nullptr;
   SHRK_TRY(scratch_get(SLOT_E, sizeof(double) * p * p, &a));
-  SHRK_TRY(scratch_get(SLOT_W, sizeof(double) * p, &w));
-  int lwork = 0;
-  if (cusolverDnDsyevd_bufferSize(H->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
-                                  (int)p, (double*)a, (int)p, (double*)w, &lwork) !=
-      CUSOLVER_STATUS_SUCCESS) {
-    set_error("cusolverDnDsyevd_bufferSize failed");
-    return SHRK_ECUDA;
-  }
-  void* work = nullptr;
-  SHRK_TRY(scratch_get(SLOT_WORK, sizeof(double) * (size_t)lwork + sizeof(int) + 256, &work));
-  info = (char*)work + sizeof(double) * (size_t)lwork;
-  {
-    LaunchScope ls("matrix_eigh", s);
-    if (cusolverDnDsyevd(H->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)p,
-                         (double*)a, (int)p, (double*)w, (double*)work, lwork, (int*)info) !=
-        CUSOLVER_STATUS_SUCCESS) {
-      set_error("cusolverDnDsyevd failed");
-      return SHRK_ECUDA;
-    }
-  }
-  int h_info = 0;
-  w_host.resize(p);
-  SHRK_CUDA(cudaMemcpyAsync(w_host.data(), w, sizeof(double) * p, cudaMemcpyDeviceToHost, s));
-  SHRK_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s));
-  SHRK_CUDA(cudaStreamSynchronize(s));
-  if (h_info != 0) {
-    set_error("symmetric eigendecomposition did not converge (syevd info " +
-              std::to_string(h_info) + ")");
-    return SHRK_ECUDA;
-  }
-  return SHRK_OK;
+  return eigh_device((double*)a, p, w_host, s);
 }
 
 shrk_status check_matrix_args(const void* m, size_t p, double c) {
@@ -375,9 +309,7 @@ shrk_status clean_sorted(const std::vector<int>& cols, const std::vector<double>
                                                                 d_scales, k, d_bulk, (double*)out);
     SHRK_CUDA(cudaGetLastError());
   } else {
-    // many active directions: the rank-k update as a DGEMM, Sigma = B G^T
-    Handles* H = nullptr;
-    SHRK_TRY(handles(s, &H));
+    // many active directions: the rank-k update as a GEMM, Sigma = B G^T
     void* gb = nullptr;
     SHRK_TRY(scratch_get(SLOT_TMP, sizeof(double) * 2 * P * k, &gb));
     double* G = (double*)gb;
@@ -388,15 +320,7 @@ shrk_status clean_sorted(const std::vector<int>& cols, const std::vector<double>
           (const double*)e, P, d_cols, d_scales, G, B);
       SHRK_CUDA(cudaGetLastError());
     }
-    {
-      LaunchScope ls("matrix_gemm", s);
-      const double one = 1.0, zero = 0.0;
-      if (cublasDgemm(H->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)p, (int)p, k, &one, B, (int)p, G,
-                      (int)p, &zero, (double*)out, (int)p) != CUBLAS_STATUS_SUCCESS) {
-        set_error("cublasDgemm failed");
-        return SHRK_ECUDA;
-      }
-    }
+    SHRK_TRY(dgemm(false, true, P, P, k, 1.0, B, P, G, P, 0.0, (double*)out, P, s));
     {
       LaunchScope ls("matrix_reconstruct", s);
       finish_spiked_kernel<<<rows_grid(P, 256), 256, 0, s>>>((double*)out, P, d_bulk);
@@ -439,8 +363,6 @@ shrk_status precision_sorted(const std::vector<int>& cols, const std::vector<dou
   LibScope L;
   SHRK_TRY(L.st);
   cudaStream_t s = L.stream;
-  Handles* H = nullptr;
-  SHRK_TRY(handles(s, &H));
   const int64_t P = (int64_t)p;
   void *e = nullptr, *small = nullptr, *b = nullptr, *out = nullptr;
   SHRK_TRY(scratch_get(SLOT_E, sizeof(double) * P * P, &e));
@@ -454,17 +376,9 @@ shrk_status precision_sorted(const std::vector<int>& cols, const std::vector<dou
                                                            (const double*)small, (double*)b);
     SHRK_CUDA(cudaGetLastError());
   }
-  {
-    // Omega = B E^T (column-major; symmetric, so also the row-major result)
-    LaunchScope ls("matrix_gemm", s);
-    const double one = 1.0, zero = 0.0;
-    if (cublasDgemm(H->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)p, (int)p, (int)p, &one,
-                    (const double*)b, (int)p, (const double*)e, (int)p, &zero, (double*)out,
-                    (int)p) != CUBLAS_STATUS_SUCCESS) {
-      set_error("cublasDgemm failed");
-      return SHRK_ECUDA;
-    }
-  }
+  // Omega = B E^T (column-major; symmetric, so also the row-major result)
+  SHRK_TRY(dgemm(false, true, P, P, P, 1.0, (const double*)b, P, (const double*)e, P, 0.0,
+                 (double*)out, P, s));
   {
     LaunchScope ls("matrix_reconstruct", s);
     symmetrize_kernel<<<rows_grid(P, 256), 256, 0, s>>>((double*)out, P);
@@ -490,10 +404,10 @@ shrk_status eigh_sorted(const double* m, int64_t p, std::vector<int>& cols,
   SHRK_TRY(scratch_get(SLOT_E, sizeof(double) * p * p, &a));
   SHRK_CUDA(cudaMemcpyAsync(a, m, sizeof(double) * p * p, cudaMemcpyHostToDevice, s));
   std::vector<double> w;
-  SHRK_TRY(syevd(p, w, s));
+  SHRK_TRY(eigh_sorted_slot(p, w, s));
   cols.resize(p);
   sorted.resize(p);
-  for (int64_t i = 0; i < p; ++i) {  // syevd is ascending: reverse it
+  for (int64_t i = 0; i < p; ++i) {  // ascending: reverse it
     cols[i] = (int)(p - 1 - i);
     sorted[i] = w[p - 1 - i];
   }

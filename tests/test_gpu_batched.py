@@ -147,6 +147,33 @@ def test_autotuner_table_and_retune():
         assert np.max(_rel_pointwise(c, d, a, b)) <= 1e-12
 
 
+def test_set_tune_installs_a_saved_table():
+    """A table saved from one run (or written by hand) installs without
+    tuning; plans then follow it (here every bucket forced to R = 2 and
+    SL = 1024, then to R = 4, SL = 8192), and results stay within the FP64
+    bar; out-of-range entries are rejected."""
+    L = _native.load()
+    arrs = _ragged([300, 2500, 9000, 17000], seed=8)
+    etas = [1.0 / math.sqrt(a.size) for a in arrs]
+    saved = (C.c_int32 * 16)()
+    _native.check(L.shrk_batched_autotune(F64, 0, saved), "batched_autotune")
+    ref = _batched_host(arrs, etas, F64)
+    try:
+        for r, sl in ((2, 1024), (4, 8192)):
+            t = (C.c_int32 * 16)(*([r, sl] * 8))
+            _native.check(L.shrk_batched_set_tune(F64, t), "batched_set_tune")
+            got = (C.c_int32 * 16)()
+            _native.check(L.shrk_batched_autotune(F64, 0, got), "batched_autotune")
+            assert list(got) == [r, sl] * 8
+            for (a, b), (c, d) in zip(ref, _batched_host(arrs, etas, F64)):
+                assert np.max(_rel_pointwise(c, d, a, b)) <= 1e-12
+        bad = (C.c_int32 * 16)(*([3, 1024] * 8))
+        assert L.shrk_batched_set_tune(F64, bad) == 1
+        assert "R must be 2 or 4" in _native.last_error()
+    finally:
+        _native.check(L.shrk_batched_set_tune(F64, saved), "batched_set_tune")
+
+
 def test_python_api_batched_matches_single():
     arrs = _ragged([100, 2000, 5000], seed=7)
     out = rk.stieltjes_transform_batched(arrs, precision="f64")

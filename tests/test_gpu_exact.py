@@ -102,7 +102,7 @@ def test_unsorted_large_matches_sorted(oracle):
         r2, i2 = gpu_all(ev[order], eta, precision=MIXED)
         err = np.hypot(r2 - o_re[np.argsort(perm)][order], i2 - o_im[np.argsort(perm)][order])
         err /= np.hypot(o_re[np.argsort(perm)][order], o_im[np.argsort(perm)][order])
-        assert np.median(err) <= 1e-9 and np.max(err) <= 1e-6
+        assert np.median(err) <= 1e-9 and np.max(err) <= 1e-7
 
 
 @pytest.mark.parametrize("method", ["naive", "autovec", "blocked", "blocked_autovec",
@@ -162,7 +162,7 @@ def test_mixed_precision_error_vs_truth(oracle, p, median_bar):
     t_re, t_im = oracle.truth_points(ev[idx], ev, eta)
     err = np.hypot(re[idx] - t_re / p, im[idx] - t_im / p) / np.hypot(t_re / p, t_im / p)
     assert np.median(err) <= median_bar, np.median(err)
-    assert np.max(err) <= 1e-6, np.max(err)
+    assert np.max(err) <= 3e-8, np.max(err)  # measured 4.6e-9 .. 8.0e-9
 
 
 def test_rcp_bias_probe_matches_the_correction():

@@ -104,7 +104,7 @@ def test_tensor_core_m2l_lower_orders(order):
     err = rel(rtc, itc, r64, i64)
     assert np.all(np.isfinite(rtc)) and np.all(np.isfinite(itc))
     assert np.median(err) < 2e-6, np.median(err)
-    assert err.max() < 1e-4, err.max()
+    assert err.max() < 5e-6, err.max()  # measured 1.2-1.5e-6
 
 
 @pytest.mark.parametrize("p", [20_000, 200_000])
@@ -130,7 +130,7 @@ def test_tensor_core_m2l(oracle, p):
     err = rel(rtc, itc, r64, i64)
     assert np.all(np.isfinite(rtc)) and np.all(np.isfinite(itc))
     assert np.median(err) < 2e-6, np.median(err)
-    assert err.max() < 1e-4, err.max()
+    assert err.max() < 5e-6, err.max()  # measured 1.2-1.5e-6
     if p <= 20_000:
         ore, oim = oracle.compute_all(ev, eta, "blocked", parallel=True)
         assert np.median(rel(rtc, itc, ore, oim)) < 2e-6
