@@ -596,13 +596,36 @@ def run_path(args, world, rank, local):
                     "basis": f"{ops:g} pipe lane-ops per pair evaluation; peak = measured FMA "
                              "lane-op rate of this GPU"}
         elif wl == "nufft" and kn.value:
-            m = 65536
-            alg = 8 * p + 4 * 16 * m  # splat: read sources, write the grid
-            roof = {"bound": "hbm", "achieved": alg / k_s / 1e9,
-                    "peak": _measured_hbm(), "unit": "GB/s",
-                    "frac": alg / k_s / 1e9 / _measured_hbm(), "traffic": None,
-                    "kernel": "nufft_splat", "kernel_ms": k_s * 1e3,
-                    "basis": "splat: 8 B per source read + 64 B per grid cell written"}
+            m = O.nufft_grid_size(float(ev_h[-1] - ev_h[0]), eta)
+            # every launch family of the call; the roofline is the splat's
+            # (its HBM GB/s is the figure asked for), the call's total
+            # algorithmic bytes and rate are given beside it
+            alg_fam = {"nufft_splat": (8 * p + 16 * m, "8 B per source read + 16 B per "
+                                       "grid cell written"),
+                       "nufft_fft": (32 * m, "the grid read and written once (one cluster "
+                                     "launch: FFT, spectral product, inverse FFT on chip)"),
+                       "nufft_spectral": (40 * m, "16+8 B per cell read, 16 B written"),
+                       "nufft_interp": (24 * p + 16 * m, "8 B per query read, 16 B written, "
+                                        "the grid read once")}
+            for f in alg_fam:
+                n_, ms_ = C.c_int64(), C.c_double()
+                L.shrk_timing_read(f.encode(), C.byref(n_), C.byref(ms_))
+                fams[f] = (n_.value, ms_.value)
+            alg, basis = alg_fam["nufft_splat"]
+            ach = alg / k_s / 1e9
+            tr = None
+            tpath = os.path.join(ROOT, "profiles", "traffic.json")
+            if os.path.exists(tpath):
+                tr = json.load(open(tpath)).get("nufft_splat")
+            total_alg = sum(v[0] for k_, v in alg_fam.items() if fams[k_][0])
+            roof = {"bound": "hbm", "achieved": ach, "peak": _measured_hbm(), "unit": "GB/s",
+                    "frac": ach / _measured_hbm(), "traffic": tr, "kernel": "nufft_splat",
+                    "kernel_ms": k_s * 1e3, "grid_cells": m,
+                    "basis": "splat family (cell keys + gather/pack launches): " + basis
+                             + ", per step",
+                    "families_ms": {k_: v[1] / max(1, args.steps) for k_, v in fams.items()},
+                    "call_algorithmic_bytes": total_alg,
+                    "call_gbs": total_alg / (ms * 1e-3) / 1e9}
         elif wl == "fft5" and kn.value:
             m = O.fft5_grid_size(ev_h, eta)
             fam = family.decode()

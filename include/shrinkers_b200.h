@@ -45,9 +45,12 @@ typedef enum {
  * coarse-grid NUFFT; FFT5/3/2 -> GPU fft5 grid convolution; ADAPTIVE / DST ->
  * its real part with the windowed (or exact) imaginary part;
  * AUTO/SPEED_AUTO/ACCURACY_AUTO -> resolved exactly as
- * config::resolve_auto_method.  At all points TREECODE, EWALD and HODLR
- * return SHRK_ENOTIMPL (no CPU fallback); at query points they are the exact
- * per-point sum, as in the reference (mod.rs:265-287). */
+ * config::resolve_auto_method.  At all points TREECODE ("fmm") runs the
+ * dyadic Chebyshev FMM (order 16, M2L on the tensor cores, ~1e-6 relative;
+ * the reference's multipole treecode is pinned at 1e-3, treecode.rs:357-393),
+ * EWALD and HODLR return SHRK_ENOTIMPL (no CPU fallback); at query points
+ * all three are the exact per-point sum, as in the reference
+ * (mod.rs:265-287). */
 typedef enum {
   SHRK_M_NAIVE = 0, SHRK_M_AUTOVEC, SHRK_M_BLOCKED, SHRK_M_BLOCKED_AUTOVEC,
   SHRK_M_BLOCKED_TILED, SHRK_M_BLOCKED_WINDOWED, SHRK_M_BLOCKED_HYBRID,
@@ -141,7 +144,9 @@ shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const dou
  *     larger sizes return SHRK_EINVAL with a message naming the limit.
  *   - The first call on each device does a one-time setup (it looks up the
  *     array's device address, which may also load the module onto the
- *     device); make that first call before any stream capture.
+ *     device); make that first call before any stream capture.  The address
+ *     is kept for the life of the process: do not use this entry point on a
+ *     device after cudaDeviceReset (the module may then load elsewhere).
  *   - Every call on a device shares the array.  Calls that overlap -- on
  *     different streams, or enqueued concurrently from several host threads
  *     -- race on it and corrupt each other's results; serialise them (for

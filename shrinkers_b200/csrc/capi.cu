@@ -476,6 +476,20 @@ static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* 
     }
     return apply_epilogue(d_tgt, rre, rim, nt, epi, s);
   }
+  if (all_points && method == SHRK_M_TREECODE) {
+    // StieltjesMethod::TreeCode ("fmm", mod.rs:646-655: a multipole treecode,
+    // theta 0.5, order 6, accuracy pinned at 1e-3, treecode.rs:357-393): the
+    // dyadic Chebyshev FMM of fmm.cu, order 16, M2L on the tensor cores
+    // (TF32 x3, ~1e-6 of |S|).  fmm_all writes S/p in the caller's order.
+    void* raw = nullptr;
+    SHRK_TRY(scratch_get(7, sizeof(double) * 2 * nt, &raw));
+    double* rre = (double*)raw;
+    double* rim = rre + nt;
+    SHRK_TRY(fmm_all(d_src, ns, eta, 16, 1, rre, rim, s));
+    Epilogue e2 = epi;
+    e2.scale = epi.scale * (double)ns;  // the values are already S/p
+    return apply_epilogue(d_tgt, rre, rim, nt, e2, s);
+  }
   if (method == SHRK_M_NUFFT || is_cheb(method)) {
     const double* ds = nullptr;
     double first = 0.0, last = 0.0;

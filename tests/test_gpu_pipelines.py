@@ -93,6 +93,39 @@ def test_mixed_precision_c1(rk, oracle, c1):
 def test_out_of_scope_methods_fail_loudly(rk, c1):
     """All-points methods without a GPU kernel raise instead of falling back
     to the CPU (at query points they are the exact per-point sum)."""
-    for method in ["treecode", "fmm", "ewald", "hodlr"]:
+    for method in ["ewald", "hodlr"]:
         with pytest.raises(NotImplementedError, match="no GPU implementation"):
             rk.stieltjes_transform(c1, method=method)
+
+
+def test_treecode_method_runs_the_fmm(rk, oracle):
+    """method "fmm" / "treecode" (StieltjesMethod::TreeCode) at all points is
+    the GPU's dyadic Chebyshev FMM.  The reference's own tests of its
+    multipole treecode, restated: treecode.rs:303-329 (p = 1500 log spectrum,
+    eta = 0.15, raw sums within 0.5 of autovec) and treecode.rs:357-393
+    (p = 512, eta = 0.1/sqrt(p), max relative error of each part below
+    1e-3, floor 1e-12); plus the FMM's own class at a size whose levels
+    reach the tensor-core M2L (p = 2e4: median below 2e-6 of |S|)."""
+    p = 1500
+    ev = spectra.log_spectrum(p)
+    a = rk.stieltjes_transform(ev, eta=0.15, method="fmm")
+    b = rk.stieltjes_transform(ev, eta=0.15, method="treecode")
+    np.testing.assert_array_equal(a["real"], b["real"])
+    for i in range(100):
+        r, m = oracle.autovec_sum(ev[i], ev, 0.15)
+        assert abs(a["real"][i] * p - r) < 0.5 and abs(a["imag"][i] * p - m) < 0.5
+    p = 512
+    ev = spectra.log_spectrum(p)
+    eta = 0.1 / math.sqrt(p)
+    t = rk.stieltjes_transform(ev, eta=eta, method="fmm")
+    e_re, e_im = oracle.compute_at_points(ev, ev, eta, "naive")
+    err_r = np.abs(t["real"] * p - e_re) / np.maximum(np.abs(e_re), 1e-12)
+    err_i = np.abs(t["imag"] * p - e_im) / np.maximum(np.abs(e_im), 1e-12)
+    assert err_r.max() < 1e-3 and err_i.max() < 1e-3
+    p = 20000
+    ev = spectra.config5(p)
+    eta = 1.0 / math.sqrt(p)
+    t = rk.stieltjes_transform(ev, eta=eta, method="fmm")
+    o_re, o_im = oracle.compute_all(ev, eta, "blocked", parallel=True)
+    err = np.hypot(t["real"] - o_re, t["imag"] - o_im) / np.hypot(o_re, o_im)
+    assert np.median(err) < 2e-6 and err.max() < 5e-6
