@@ -318,8 +318,17 @@ def run_ours(args, world, rank, local):
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
             traffic = json.load(open(tpath)).get(kname.decode())
+        mufu = None
+        if prec == 1:  # one MUFU reciprocal per two far-field pairs
+            rr = C.c_double()
+            _native.check(L.shrk_measure_rcp_rate(C.byref(rr)))
+            mufu = {"achieved": 0.5 * p * p / k_avg_s / 1e12, "peak": rr.value / 1e12,
+                    "unit": "T rcp/s", "frac": 0.5 * p * p / k_avg_s / rr.value,
+                    "basis": "0.5 MUFU reciprocal per pair (the FP64 near field, ~1 % of the "
+                             "pairs here, counted as far) / measured rcp.approx.f32 rate"}
         roof = {"bound": "fp32" if prec == 1 else "fp64", "achieved": achieved / 1e12,
                 "peak": peak / 1e12, "unit": "Tops/s", "frac": achieved / peak,
+                "xu_pipe": mufu,
                 "traffic": traffic, "kernel": kname.decode(),
                 "kernel_ms": k_avg_s * 1e3, "kernel_launches": kn.value,
                 "basis": (f"{ops_per_pair:g} pipe lane-ops per pair evaluation x p^2 pairs per "
@@ -602,8 +611,8 @@ def run_path(args, world, rank, local):
             # algorithmic bytes and rate are given beside it
             alg_fam = {"nufft_splat": (8 * p + 16 * m, "8 B per source read + 16 B per "
                                        "grid cell written"),
-                       "nufft_fft": (32 * m, "the grid read and written once (one cluster "
-                                     "launch: FFT, spectral product, inverse FFT on chip)"),
+                       "nufft_fft": (128 * m, "two transforms of two four-step passes: "
+                                     "16 B per cell read + 16 B written per pass"),
                        "nufft_spectral": (40 * m, "16+8 B per cell read, 16 B written"),
                        "nufft_interp": (24 * p + 16 * m, "8 B per query read, 16 B written, "
                                         "the grid read once")}
@@ -928,7 +937,8 @@ def run_deconv(args, world, rank, local):
     p = 50 000) through the Python API with host arrays -- the path has no
     device form, so value and e2e both include the copies.  MP(c = 0.25) bulk
     + 3 spikes in [4, 12].  A step = one call at --p; the line also times
-    p = 10 000 / 20 000 / 50 000, the sizes the reference publishes.  The CPU
+    p = 1 000 / 10 000 / 20 000 / 50 000, the sizes the reference publishes
+    (docs/internals.md:236-238, 557-564).  The CPU
     baseline is the oracle's restatement of the same call on all host cores."""
     import ctypes as C
     import torch
@@ -957,7 +967,7 @@ def run_deconv(args, world, rank, local):
     clk = clocks.stop()
     launches = int(L.shrk_launch_count()) - n0
     sizes = {}
-    for n in (10_000, 20_000, 50_000):
+    for n in (1_000, 10_000, 20_000, 50_000):
         e = spec(n)
         for _ in range(5):
             rk.deconvolve_spiked(e, c)
@@ -992,7 +1002,8 @@ def run_deconv(args, world, rank, local):
                    "l2": "inputs of 8p bytes copied in every step"},
         "roofline": None,
         "ms_by_p": sizes,
-        "reference_published_ms_m1max": {"10000": 0.244, "20000": 0.368, "50000": 0.779},
+        "reference_published_ms_m1max": {"1000": 0.0632, "10000": 0.244, "20000": 0.368,
+                                          "50000": 0.779},
         "cpu_baseline": cpu_line,
         "e2e": {"value": rate, "unit": "calls/s", "h2d_bytes_per_step": 8 * p + 8 * 200,
                 "d2h_bytes_per_step": 48 * 200, "ms_per_step": ms},

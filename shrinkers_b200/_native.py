@@ -83,6 +83,7 @@ SIGNATURES = {
     "shrk_measure_pipe_rates": (_ST, [_D, _D]),
     "shrk_measure_rcp_bias": (_ST, [_D, _D]),
     "shrk_diag_set_wait_limit": (C.c_longlong, [C.c_longlong]),
+    "shrk_measure_rcp_rate": (_ST, [_D]),
 }
 
 _lib = None

@@ -323,13 +323,19 @@ static shrk_status not_impl(int m) {
   return SHRK_ENOTIMPL;
 }
 
-// Host<->device copies of the host-pointer entry points, staged through the
-// context's pinned buffer: an upload is a host memcpy into the stage plus an
-// asynchronous copy; a download is an asynchronous copy into the stage that
-// check_device_error completes (one synchronisation per call, shared with
-// the error-word read).  A copy that does not fit the stage goes direct
-// (pageable) and the stage grows before the next call.
+// Host<->device copies of the host-pointer entry points.  Small ones (at
+// most 1 MiB) are staged through the context's pinned buffer: an upload is a
+// host memcpy into the stage plus an asynchronous copy; a download is an
+// asynchronous copy into the stage that check_device_error completes (one
+// synchronisation per call, shared with the error-word read).  Larger copies,
+// and small ones that do not fit the stage (it grows before the next call),
+// go direct.
 static char* stage_take(Context* c, size_t bytes, size_t* off) {
+  // Large copies go direct: the DMA engine reads pinned user memory at full
+  // speed and the driver stages pageable memory itself; an extra host copy
+  // only pays for small, latency-bound transfers.
+  constexpr size_t kStageCopyMax = (size_t)1 << 20;
+  if (bytes > kStageCopyMax) return nullptr;
   const size_t al = (bytes + 255) & ~(size_t)255;
   c->stage_want += al;
   if (!c->stage || c->stage_used + al > c->stage_bytes) return nullptr;
@@ -373,7 +379,7 @@ static shrk_status stage_begin(Context* c) {
     c->stage_busy = false;
   }
   c->pending.clear();
-  constexpr size_t kStageMax = (size_t)64 << 20;
+  constexpr size_t kStageMax = (size_t)8 << 20;
   const size_t want = std::min(std::max(c->stage_want, (size_t)1 << 16), kStageMax);
   if (want > c->stage_bytes) {
     if (c->stage) cudaFreeHost(c->stage);
@@ -1532,5 +1538,12 @@ shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean) {
 }
 
 long long shrk_diag_set_wait_limit(long long cycles) { return set_wait_cycles(cycles); }
+
+shrk_status shrk_measure_rcp_rate(double* rcp_per_s) {
+  Guard g;
+  SHRK_TRY(g.st);
+  if (!rcp_per_s) return einval("null output pointer");
+  return measure_rcp_rate(rcp_per_s);
+}
 
 }  // extern "C"

@@ -37,6 +37,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -240,6 +242,173 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag_kernel(const TriArgs a) {
   }
 }
 
+
+// The same reduction with ONE grid barrier per column.  Phase j applies
+// reflector j to the trailing columns and, in the same pass over each
+// column, forms the next product p_{j+1} = beta_{j+1} A^{(j+1)} v_{j+1}.
+// That needs v_{j+1} at the start of the phase: every CTA derives it itself
+// from the stale column j+1 and the previous phase's p_j (w = p_j - K v_j),
+// bit-identically in every CTA (same reads, same reduction order), into its
+// own buffer.  Column j+1 is then never written: reflector j+1 goes to row
+// j+1 of the upper triangle (a part no later phase reads), and only rows
+// >= j+2 of the trailing columns are updated.  p and the partial sums of
+// p^T v alternate between two buffers.
+struct Tri1Args {
+  double* A;       // p x p column-major, symmetric (both triangles)
+  int64_t p;
+  double* d;
+  double* e;
+  double* vhead;   // [p] reflector heads
+  double* beta;    // [p]
+  double* pv;      // [2][p]
+  double* part;    // [2][gridDim.x]
+  double* vb;      // [gridDim.x][2][p] per-CTA reflector copies
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  v = warp_sum(v);
+  __syncthreads();  // red may still be read from the previous call
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  const int nw = blockDim.x >> 5;
+  for (int w = 0; w < nw; ++w) t += red[w];
+  return t;
+}
+
+// Reflector of x = v[k0 .. p): on return v[k0] holds the head x0 - alpha and
+// the rest is x; beta = 0 (and alpha = x0) when x is already reduced.
+__device__ __forceinline__ void make_reflector(double* v, int64_t k0, int64_t p, double* red,
+                                               double& beta, double& alpha) {
+  double s = 0.0;
+  for (int64_t k = k0 + threadIdx.x; k < p; k += blockDim.x) s += v[k] * v[k];
+  const double norm2 = block_sum(s, red);
+  const double x0 = v[k0];
+  const double sig = norm2 - x0 * x0;
+  double head = x0;
+  beta = 0.0;
+  alpha = x0;
+  if (sig > 0.0) {
+    const double nrm = sqrt(norm2);
+    alpha = x0 >= 0.0 ? -nrm : nrm;
+    head = x0 - alpha;
+    beta = 2.0 / (sig + head * head);
+  }
+  __syncthreads();  // every thread has read v[k0]
+  if (threadIdx.x == 0) v[k0] = head;
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double red[TRI_NT / 32];
+  const int lane = threadIdx.x & 31;
+  constexpr int WPB = TRI_NT / 32;
+  const int64_t gw = (int64_t)blockIdx.x * WPB + (threadIdx.x >> 5);
+  const int64_t nw = (int64_t)gridDim.x * WPB;
+  const int64_t G = gridDim.x;
+  const int64_t p = a.p;
+  double* A = a.A;
+  const bool lead = blockIdx.x == 0;
+  if (p < 3) {
+    if (lead && threadIdx.x == 0) {
+      a.d[0] = A[0];
+      if (p == 2) {
+        a.e[0] = A[1];
+        a.d[1] = A[3];
+      }
+    }
+    return;
+  }
+  double* vb = a.vb + (int64_t)blockIdx.x * 2 * p;
+  // prologue: reflector 0 from column 0, p_0 over the columns c >= 1
+  double* vcur = vb;
+  for (int64_t k = 1 + threadIdx.x; k < p; k += blockDim.x) vcur[k] = A[k];
+  double bcur = 0.0, alpha = 0.0;
+  make_reflector(vcur, 1, p, red, bcur, alpha);
+  if (lead) {
+    if (threadIdx.x == 0) {
+      a.d[0] = A[0];
+      a.e[0] = alpha;
+      a.vhead[0] = vcur[1];
+      a.beta[0] = bcur;
+    }
+    for (int64_t k = 2 + threadIdx.x; k < p; k += blockDim.x) A[k * p] = vcur[k];  // row 0
+  }
+  {
+    double dot = 0.0;
+    if (bcur != 0.0)
+      for (int64_t c = 1 + ((gw - 1) % nw + nw) % nw; c < p; c += nw) {
+        const double* col = A + c * p;
+        double s = 0.0;
+        for (int64_t k = 1 + lane; k < p; k += 32) s = fma(col[k], vcur[k], s);
+        s = warp_sum(s) * bcur;
+        if (lane == 0) a.pv[c] = s;
+        dot = fma(s, vcur[c], dot);
+      }
+    const double t = block_sum(lane == 0 ? dot : 0.0, red);
+    if (threadIdx.x == 0) a.part[blockIdx.x] = t;
+  }
+  grid.sync();
+  for (int64_t j = 0; j + 2 < p; ++j) {
+    const int par = (int)(j & 1), nxt = par ^ 1;
+    vcur = vb + par * p;
+    double* vnext = vb + nxt * p;
+    const double* pj = a.pv + par * p;
+    const double g = block_sum(threadIdx.x < G ? a.part[par * G + threadIdx.x] : 0.0, red);
+    const double K = 0.5 * bcur * g;
+    const bool upd = bcur != 0.0;
+    const int64_t k1 = j + 1, k2 = j + 2;
+    const double vj1 = vcur[k1], wj1 = upd ? pj[k1] - K * vj1 : 0.0;
+    // column j+1 of A^{(j+1)}, rows >= j+2, and its diagonal entry
+    for (int64_t k = k2 + threadIdx.x; k < p; k += blockDim.x) {
+      const double vk = vcur[k], wk = upd ? pj[k] - K * vk : 0.0;
+      vnext[k] = A[k + k1 * p] - (vk * wj1 + wk * vj1);
+    }
+    const double dnew = A[k1 + k1 * p] - 2.0 * vj1 * wj1;
+    double bnext = 0.0;
+    if (k1 + 2 < p) {
+      make_reflector(vnext, k2, p, red, bnext, alpha);
+      if (lead) {
+        if (threadIdx.x == 0) {
+          a.d[k1] = dnew;
+          a.e[k1] = alpha;
+          a.vhead[k1] = vnext[k2];
+          a.beta[k1] = bnext;
+        }
+        for (int64_t k = k2 + 1 + threadIdx.x; k < p; k += blockDim.x) A[k1 + k * p] = vnext[k];
+      }
+    } else {  // the last 2 x 2 block: no further reflector
+      __syncthreads();
+      if (lead && threadIdx.x == 0) {
+        a.d[k1] = dnew;
+        a.e[k1] = vnext[k2];
+      }
+    }
+    // trailing columns: update rows >= j+2 and form p_{j+1} from the new values
+    double dot = 0.0;
+    for (int64_t c = k2 + ((gw - k2) % nw + nw) % nw; c < p; c += nw) {
+      double* col = A + c * p;
+      const double vc = vcur[c], wc = upd ? pj[c] - K * vc : 0.0;
+      double s = 0.0;
+      for (int64_t k = k2 + lane; k < p; k += 32) {
+        const double vk = vcur[k], wk = upd ? pj[k] - K * vk : 0.0;
+        const double x = col[k] - (vk * wc + wk * vc);
+        col[k] = x;
+        s = fma(x, vnext[k], s);
+      }
+      s = warp_sum(s) * bnext;
+      if (lane == 0 && bnext != 0.0) a.pv[nxt * p + c] = s;
+      dot = fma(s, vnext[c], dot);
+    }
+    const double t = block_sum(lane == 0 ? dot : 0.0, red);
+    if (threadIdx.x == 0) a.part[nxt * G + blockIdx.x] = t;
+    bcur = bnext;
+    grid.sync();
+  }
+  if (lead && threadIdx.x == 0) a.d[p - 1] = A[(p - 1) + (p - 1) * p];
+}
+
 // ------------------------------------------------------------ bisection --
 // Slot k: the kloc-th smallest eigenvalue of the unreduced block [b0, b1)
 // of T, searched in the block's Gershgorin interval [lo, hi].
@@ -404,9 +573,12 @@ __global__ void ns_matrix_kernel(double* __restrict__ g, int64_t p) {
 }
 
 // Y[r, jj] = v_{j0+jj}[j0+1+r] (rows of the block's reach, zero above the
-// reflector's first entry), n = p - j0 - 1 rows, nb columns.
+// reflector's first entry), n = p - j0 - 1 rows, nb columns.  Reflector j
+// sits below the diagonal in column j (rowstore 0) or right of it in row j
+// (rowstore 1), its head in vhead[j].
 __global__ void build_y_kernel(const double* __restrict__ A, const double* __restrict__ vhead,
-                               int64_t p, int64_t j0, int nb, double* __restrict__ Y) {
+                               int64_t p, int64_t j0, int nb, int rowstore,
+                               double* __restrict__ Y) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y;
   const int64_t n = p - j0 - 1;
@@ -415,7 +587,7 @@ __global__ void build_y_kernel(const double* __restrict__ A, const double* __res
   const int64_t row = j0 + 1 + r;
   double v = 0.0;
   if (row == j + 1) v = vhead[j];
-  else if (row > j + 1) v = A[row + j * p];
+  else if (row > j + 1) v = rowstore ? A[j + row * p] : A[row + j * p];
   Y[r + (int64_t)jj * n] = v;
 }
 
@@ -478,11 +650,16 @@ __global__ void mirror_lower_kernel(double* __restrict__ A, int64_t p) {
 unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 constexpr int NB = 32;                 // reflectors per WY block
-constexpr double CLUSTER_TOL = 1e-8;   // eigenvalues closer than this x ||T||: one cluster
+// Eigenvalues closer than CLUSTER_TOL ||T|| (numerically equal) share one
+// thread and are orthogonalised by Gram-Schmidt during inverse iteration;
+// every other pair is left to inverse iteration, whose vectors then overlap
+// by about eps ||T|| / gap, and to the Newton-Schulz steps (each squares
+// the overlap), as many as the smallest such gap needs.
+constexpr double CLUSTER_TOL = 1e-12;
 
-// Scratch slots 46..52 belong to this file.
+// Scratch slots 46..53 belong to this file.
 constexpr int SLOT_U = 46, SLOT_Z = 47, SLOT_G = 48, SLOT_SMALL = 49, SLOT_WS = 50,
-              SLOT_WY = 51, SLOT_META = 52;
+              SLOT_WY = 51, SLOT_META = 52, SLOT_VB = 53;
 
 }  // namespace
 
@@ -532,22 +709,39 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
     mirror_lower_kernel<<<dim3(cdiv(p, 256), (unsigned)p), 256, 0, s>>>(A, p);
     SHRK_CUDA(cudaGetLastError());
   }
-  // 1. tridiagonalisation (cooperative: all CTAs resident)
+  // 1. tridiagonalisation (cooperative: all CTAs resident); one grid barrier
+  // per column (tridiag1_kernel, reflectors in the upper triangle) unless
+  // SHRK_EIGH_TRIDIAG=2 selects the two-barrier form
+  const char* tri_env = std::getenv("SHRK_EIGH_TRIDIAG");
+  const int rowstore = (tri_env && std::strcmp(tri_env, "2") == 0) ? 0 : 1;
   {
     int dev = 0, sms = 0, per_sm = 0;
     SHRK_CUDA(cudaGetDevice(&dev));
     SHRK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    SHRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tridiag_kernel, TRI_NT, 0));
+    SHRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, rowstore ? (const void*)tridiag1_kernel : (const void*)tridiag_kernel, TRI_NT, 0));
     if (per_sm < 1) {
       set_error("eigensolver: the tridiagonalisation kernel cannot be resident");
       return SHRK_ECUDA;
     }
-    const int blocks = std::min(sms, 4096);
-    TriArgs ta{A, p, d, e, vhead, beta, pv, part, scal};
-    void* args[] = {&ta};
-    LaunchScope ls("eigh_tridiag", s);
-    SHRK_CUDA(cudaLaunchCooperativeKernel((const void*)tridiag_kernel, dim3(blocks), dim3(TRI_NT),
-                                          args, 0, s));
+    const int blocks = std::min(sms, 2048);
+    if (rowstore) {
+      void* vbuf = nullptr;
+      SHRK_TRY(scratch_get(SLOT_VB, sizeof(double) * ((size_t)blocks * 2 * (size_t)p + 2 * (size_t)p + 2 * (size_t)blocks), &vbuf));
+      double* vbd = (double*)vbuf;
+      Tri1Args ta{A, p, d, e, vhead, beta, vbd + (size_t)blocks * 2 * p,
+                  vbd + (size_t)blocks * 2 * p + 2 * p, vbd};
+      void* args[] = {&ta};
+      LaunchScope ls("eigh_tridiag", s);
+      SHRK_CUDA(cudaLaunchCooperativeKernel((const void*)tridiag1_kernel, dim3(blocks),
+                                            dim3(TRI_NT), args, 0, s));
+    } else {
+      TriArgs ta{A, p, d, e, vhead, beta, pv, part, scal};
+      void* args[] = {&ta};
+      LaunchScope ls("eigh_tridiag", s);
+      SHRK_CUDA(cudaLaunchCooperativeKernel((const void*)tridiag_kernel, dim3(blocks),
+                                            dim3(TRI_NT), args, 0, s));
+    }
   }
   // 2. split T, Gershgorin bounds per block, eigenvalue slots (host; O(p))
   std::vector<double> hd(p), he(std::max<int64_t>(p - 1, 1), 0.0);
@@ -566,12 +760,17 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
     set_error("symmetric eigendecomposition: the matrix has non-finite entries");
     return SHRK_EINVAL;
   }
-  // negligible off-diagonals split T (dstebz's relative criterion)
+  // negligible off-diagonals split T: relative to their diagonal neighbours
+  // (dstebz's criterion) or below eps ||T|| (setting them to zero moves no
+  // eigenvalue by more than the tridiagonalisation's own backward error;
+  // without it a block of rounding noise -- the null space of a low-rank
+  // matrix -- would stay one huge cluster)
   std::vector<double> he2(std::max<int64_t>(p - 1, 1), 0.0);
   std::vector<int> bstart{0};
   for (int64_t i = 0; i + 1 < p; ++i) {
     const double t2 = he[i] * he[i];
-    if (t2 <= eps * eps * std::fabs(hd[i] * hd[i + 1]) + 1e-300) {
+    if (t2 <= eps * eps * std::fabs(hd[i] * hd[i + 1]) + 1e-300 ||
+        std::fabs(he[i]) <= eps * tnorm) {
       he[i] = 0.0;
       bstart.push_back((int)(i + 1));
     }
@@ -611,6 +810,7 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
   SHRK_CUDA(cudaMemcpyAsync(hl.data(), lam, sizeof(double) * p, cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
   std::vector<Cluster> hcl;
+  double min_gap = INFINITY;  // smallest gap inside a block between clusters
   for (size_t b = 0; b + 1 < bstart.size(); ++b) {
     const int b0 = bstart[b], b1 = bstart[b + 1];
     int k = b0;
@@ -618,9 +818,14 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
       int g = k + 1;
       while (g < b1 && hl[g] - hl[g - 1] < CLUSTER_TOL * tnorm) ++g;
       hcl.push_back(Cluster{k, g - k, b0, b1});
+      if (g < b1) min_gap = std::min(min_gap, hl[g] - hl[g - 1]);
       k = g;
     }
   }
+  // expected overlap of distinct inverse-iteration vectors, and the
+  // Newton-Schulz steps that take it below rounding (e -> ~1.5 e^2)
+  const double overlap = min_gap < INFINITY ? 8.0 * eps * tnorm / min_gap : 0.0;
+  const int ns_steps = overlap <= 1e-15 ? 0 : (overlap <= 1e-7 ? 1 : 2);
   const int ncl = (int)hcl.size();
   SHRK_CUDA(cudaMemcpyAsync(dcl, hcl.data(), sizeof(Cluster) * ncl, cudaMemcpyHostToDevice, s));
   void* ws = nullptr;
@@ -632,24 +837,29 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
                                                             (double*)ws, Zt);
     SHRK_CUDA(cudaGetLastError());
   }
-  // one Newton-Schulz step on the basis: Z <- Z (3I - Z^T Z)/2, in the
+  // Newton-Schulz steps on the basis: Z <- Z (3I - Z^T Z)/2, in the
   // transposed storage Zt: G = Zt Zt^T, Zt <- M Zt
   void* gbuf = nullptr;
   SHRK_TRY(scratch_get(SLOT_G, sizeof(double) * (size_t)P2, &gbuf));
   double* G = (double*)gbuf;
-  SHRK_TRY(dgemm(false, true, p, p, p, 1.0, Zt, p, Zt, p, 0.0, G, p, s));
+  double* zcur = Zt;  // current Z^T
+  double* other = U;
+  for (int it = 0; it < ns_steps; ++it) {
+    SHRK_TRY(dgemm(false, true, p, p, p, 1.0, zcur, p, zcur, p, 0.0, G, p, s));
+    {
+      LaunchScope ls("eigh_orthogonalise", s);
+      ns_matrix_kernel<<<dim3(cdiv(p, 256), (unsigned)p), 256, 0, s>>>(G, p);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    SHRK_TRY(dgemm(false, false, p, p, p, 1.0, G, p, zcur, p, 0.0, other, p, s));  // (Z M)^T
+    std::swap(zcur, other);
+  }
   {
     LaunchScope ls("eigh_orthogonalise", s);
-    ns_matrix_kernel<<<dim3(cdiv(p, 256), (unsigned)p), 256, 0, s>>>(G, p);
+    transpose_sq_kernel<<<dim3(cdiv(p, 32), cdiv(p, 32)), dim3(32, 8), 0, s>>>(zcur, p, other);
     SHRK_CUDA(cudaGetLastError());
   }
-  SHRK_TRY(dgemm(false, false, p, p, p, 1.0, G, p, Zt, p, 0.0, U, p, s));  // U = (Z M)^T
-  {
-    LaunchScope ls("eigh_orthogonalise", s);
-    transpose_sq_kernel<<<dim3(cdiv(p, 32), cdiv(p, 32)), dim3(32, 8), 0, s>>>(U, p, Zt);
-    SHRK_CUDA(cudaGetLastError());
-  }
-  double* Zc = Zt;  // now Z, column-major
+  double* Zc = other;  // Z, column-major
   // 4. back-transformation Zc <- H_0 ... H_{p-3} Zc, blocks from the last
   const int64_t nref = std::max<int64_t>(p - 2, 0);
   if (nref > 0) {
@@ -665,7 +875,8 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
       const int64_t n = p - j0 - 1;
       {
         LaunchScope ls("eigh_back_transform", s);
-        build_y_kernel<<<dim3(cdiv(n, 256), (unsigned)nb), 256, 0, s>>>(A, vhead, p, j0, nb, Y);
+        build_y_kernel<<<dim3(cdiv(n, 256), (unsigned)nb), 256, 0, s>>>(A, vhead, p, j0, nb,
+                                                                        rowstore, Y);
         SHRK_CUDA(cudaGetLastError());
       }
       SHRK_TRY(dgemm(true, false, nb, nb, n, 1.0, Y, n, Y, n, 0.0, S, nb, s));

@@ -34,16 +34,12 @@
 #include "epilogue.cuh"
 #include "internal.h"
 
-#include <cooperative_groups.h>
-
 #include <atomic>
 #include <cmath>
 #include <map>
 #include <string>
 
 namespace shrk {
-
-namespace cg = cooperative_groups;
 
 namespace {
 
@@ -543,190 +539,6 @@ __global__ void spectral_kernel(const double2* __restrict__ C, const double* __r
   out[k] = make_double2(ih_re - rh.y, ih_im + rh.x);
 }
 
-// ------------------------------------------- fused grid transform (cluster) --
-// For grids of FUSED_MIN_M .. FUSED_MAX_M cells (every NUFFT grid, and the
-// fft5 grids of small spectra) the whole frequency-domain step -- forward
-// four-step FFT, the spectral product, inverse four-step FFT -- runs in ONE
-// launch: a cluster of FC CTAs holds the grid in shared memory (m/FC complex
-// values per CTA, ~148 KB at m = 65 536) and exchanges it through distributed
-// shared memory instead of global memory between the passes.
-//
-//   forward, m = m1 m2:   rows = columns n2 of x[m2 n1 + n2]; CTA r owns n2 in
-//                         [r G1, (r+1) G1), G1 = m2/FC; length-m1 FFTs, then
-//                         the twiddle W^{n2 k1}.
-//   transpose (DSMEM)     CTA r takes rows k1 in [r G2, (r+1) G2), G2 = m1/FC;
-//                         length-m2 FFTs give X[k1 + m1 k2].
-//   spectral (DSMEM)      out[k] from X[k] and X[m-k] (the partner row lives in
-//                         another CTA), written in place after a cluster
-//                         barrier.
-//   inverse, m = m2 m1:   input index k = k1 + m1 k2 = m1 n1' + n2' with
-//                         n2' = k1: the rows each CTA holds are already the
-//                         inverse's first-pass columns; length-m2 FFTs and
-//                         the twiddle W^{+k1 k1'}.
-//   transpose (DSMEM)     rows k1' in [r G1, (r+1) G1); length-m1 FFTs give
-//                         the grid at k1' + m2 k2', stored to global memory.
-//
-// Every phase holds exactly m/FC values per CTA, 8 per thread, so the same
-// row_fft serves all four transforms (the stage twiddles of the four
-// (length, sign) pairs sit in shared memory).  A value moves between CTAs
-// through registers: all threads read their remote values, a cluster barrier
-// makes sure every CTA has read, then each writes its own shared memory.
-constexpr int FC = 8;                   // CTAs per cluster (portable size)
-constexpr int64_t FUSED_MIN_M = 2048;
-constexpr int64_t FUSED_MAX_M = 65536;  // 1024 threads x 8 values x FC
-
-struct FusedArgs {
-  const double2* packed;  // [m] density + i x/(x^2 + eta^2)
-  double2* grid;          // [m] unnormalised inverse transform of the product
-  const double2* tw;      // [m] (cos, sin)(2 pi j/m)
-  const double* ke;       // [m] even-kernel spectrum
-  int m1, m2;             // forward factorisation m = m1 m2 (powers of two)
-  int64_t m;
-};
-
-__host__ __device__ __forceinline__ int row_pad(int L) { return L + (L >> 3) + 1; }
-
-__host__ __device__ __forceinline__ size_t fused_smem_bytes(int m1, int m2) {
-  const int G1 = m2 / FC, G2 = m1 / FC;
-  const int a = G1 * row_pad(m1), b = G2 * row_pad(m2);
-  return sizeof(double2) * ((size_t)(a > b ? a : b) + 2 * (size_t)m1 + 2 * (size_t)m2);
-}
-
-// Spectral product of fftplan.rs:43-76 for one k (as spectral_kernel).
-__device__ __forceinline__ double2 spectral_at(double2 ck, double2 cn, double kev) {
-  const double2 cnc = make_double2(cn.x, -cn.y);
-  const double2 s = make_double2(ck.x + cnc.x, ck.y + cnc.y);
-  const double2 df = make_double2(ck.x - cnc.x, ck.y - cnc.y);
-  const double2 D = make_double2(0.5 * s.x, 0.5 * s.y);
-  const double2 K = make_double2(0.5 * df.y, -0.5 * df.x);  // (-0.5 i) * df
-  const double ih_re = D.x * kev, ih_im = D.y * kev;
-  const double2 rh = cmul(D, K);
-  return make_double2(ih_re - rh.y, ih_im + rh.x);
-}
-
-__global__ void __cluster_dims__(FC, 1, 1) __launch_bounds__(1024, 1)
-    grid_transform_cluster(const FusedArgs a) {
-  extern __shared__ double2 fsm[];
-  cg::cluster_group cl = cg::this_cluster();
-  const int r = (int)cl.block_rank();
-  const int tid = threadIdx.x, nt = blockDim.x;  // nt = m / (8 FC)
-  const int m1 = a.m1, m2 = a.m2;
-  const int64_t m = a.m;
-  const int G1 = m2 / FC, G2 = m1 / FC;
-  const int lg1 = __ffs(G1) - 1, lg2 = __ffs(G2) - 1, lm1 = __ffs(m1) - 1;
-  const int P1 = row_pad(m1), P2 = row_pad(m2);
-  const int da = G1 * P1, db = G2 * P2;
-  double2* data = fsm;
-  double2* tw_f1 = fsm + (da > db ? da : db);  // (m1, -), (m2, -), (m2, +), (m1, +)
-  double2* tw_f2 = tw_f1 + m1;
-  double2* tw_i1 = tw_f2 + m2;
-  double2* tw_i2 = tw_i1 + m2;
-  load_stage_twiddles(tw_f1, a.tw, m1, m, -1.0);
-  load_stage_twiddles(tw_f2, a.tw, m2, m, -1.0);
-  load_stage_twiddles(tw_i1, a.tw, m2, m, +1.0);
-  load_stage_twiddles(tw_i2, a.tw, m1, m, +1.0);
-  double2 v[8];
-
-  // forward pass 1: rows g = columns n2 = r G1 + g, element n1 at padi(n1)
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    const int g = e & (G1 - 1), n1 = e >> lg1;
-    v[it] = a.packed[(int64_t)m2 * n1 + r * G1 + g];
-  }
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    data[(e & (G1 - 1)) * P1 + padi(e >> lg1)] = v[it];
-  }
-  __syncthreads();
-  row_fft(data + (tid / (m1 >> 3)) * P1, tw_f1, m1, tid % (m1 >> 3), -1.0);
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {  // twiddle W^{-n2 k1}
-    const int e = tid + it * nt;
-    const int g = e & (G1 - 1), k1 = e >> lg1;
-    const double2 w = a.tw[((int64_t)(r * G1 + g) * k1) & (m - 1)];
-    double2* x = &data[g * P1 + padi(k1)];
-    *x = cmul(*x, make_double2(w.x, -w.y));
-  }
-  cl.sync();
-
-  // transpose: rows k1 = r G2 + g2 over n2; (k1, n2) is in CTA n2 / G1
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    const int g2 = e & (G2 - 1), n2 = e >> lg2;
-    const double2* rem = cl.map_shared_rank(data, n2 >> lg1);
-    v[it] = rem[(n2 & (G1 - 1)) * P1 + padi(r * G2 + g2)];
-  }
-  cl.sync();
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    data[(e & (G2 - 1)) * P2 + padi(e >> lg2)] = v[it];
-  }
-  __syncthreads();
-  row_fft(data + (tid / (m2 >> 3)) * P2, tw_f2, m2, tid % (m2 >> 3), -1.0);
-  cl.sync();  // X[k1 + m1 k2] complete in every CTA
-
-  // spectral product: partner X[m - k] from the CTA holding row (m - k) mod m1
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    const int g2 = e & (G2 - 1), k2 = e >> lg2;
-    const int64_t k = (int64_t)(r * G2 + g2) + (int64_t)m1 * k2;
-    const int64_t kp = (m - k) & (m - 1);
-    const int kp1 = (int)(kp & (m1 - 1)), kp2 = (int)(kp >> lm1);
-    const double2* rem = cl.map_shared_rank(data, kp1 >> lg2);
-    v[it] = spectral_at(data[g2 * P2 + padi(k2)], rem[(kp1 & (G2 - 1)) * P2 + padi(kp2)],
-                        a.ke[k]);
-  }
-  cl.sync();
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    data[(e & (G2 - 1)) * P2 + padi(e >> lg2)] = v[it];
-  }
-  __syncthreads();
-
-  // inverse pass 1 on the same rows (n2' = k1), length m2, twiddle W^{+k1 k1'}
-  row_fft(data + (tid / (m2 >> 3)) * P2, tw_i1, m2, tid % (m2 >> 3), +1.0);
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    const int g2 = e & (G2 - 1), k1p = e >> lg2;
-    const double2 w = a.tw[((int64_t)(r * G2 + g2) * k1p) & (m - 1)];
-    double2* x = &data[g2 * P2 + padi(k1p)];
-    *x = cmul(*x, w);
-  }
-  cl.sync();
-
-  // transpose: rows k1' = r G1 + g3 over n2' = k1; (k1', k1) is in CTA k1 / G2
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    const int g3 = e & (G1 - 1), k1 = e >> lg1;
-    const double2* rem = cl.map_shared_rank(data, k1 >> lg2);
-    v[it] = rem[(k1 & (G2 - 1)) * P2 + padi(r * G1 + g3)];
-  }
-  cl.sync();  // last remote read: no CTA leaves while another still reads it
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    data[(e & (G1 - 1)) * P1 + padi(e >> lg1)] = v[it];
-  }
-  __syncthreads();
-  row_fft(data + (tid / (m1 >> 3)) * P1, tw_i2, m1, tid % (m1 >> 3), +1.0);
-
-  // the grid at k1' + m2 k2'
-#pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    const int e = tid + it * nt;
-    const int g3 = e & (G1 - 1), k2p = e >> lg1;
-    a.grid[(int64_t)(r * G1 + g3) + (int64_t)m2 * k2p] = data[g3 * P1 + padi(k2p)];
-  }
-}
-
 struct InterpArgs {
   const double* q;
   int64_t nq;
@@ -882,43 +694,6 @@ shrk_status fft(double2* buf, double2* tmp, int64_t m, const double2* tw, double
   return SHRK_OK;
 }
 
-// The frequency-domain step of a grid of FUSED_MIN_M .. FUSED_MAX_M cells in
-// one cluster launch (A -> B).  *done is false when the device cannot place
-// the cluster (then the caller runs the multi-pass transform).
-shrk_status fused_transform(const double2* A, double2* B, int64_t m, const Tables* T,
-                            const char* family, cudaStream_t s, bool* done) {
-  *done = false;
-  const int bits = ilog2(m);
-  const int m1 = 1 << ((bits + 1) / 2), m2 = 1 << (bits / 2);
-  const size_t smem = fused_smem_bytes(m1, m2);
-  static std::atomic<int> usable[64];  // 0 unknown, 1 yes, -1 no
-  int dev = 0;
-  SHRK_CUDA(cudaGetDevice(&dev));
-  const bool known = dev >= 0 && dev < 64;
-  if (!known || usable[dev].load() == 0) {
-    SHRK_CUDA(cudaFuncSetAttribute(grid_transform_cluster,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)fused_smem_bytes(256, 256)));
-    cudaLaunchConfig_t cfg = {};  // the cluster size is the kernel's compile-time one
-    cfg.gridDim = dim3(FC);
-    cfg.blockDim = dim3(1024);
-    cfg.dynamicSmemBytes = fused_smem_bytes(256, 256);
-    int clusters = 0;
-    const cudaError_t e =
-        cudaOccupancyMaxActiveClusters(&clusters, grid_transform_cluster, &cfg);
-    if (e != cudaSuccess) cudaGetLastError();
-    if (known) usable[dev] = (e == cudaSuccess && clusters >= 1) ? 1 : -1;
-    if (!(e == cudaSuccess && clusters >= 1)) return SHRK_OK;
-  }
-  if (usable[dev].load() < 0) return SHRK_OK;
-  FusedArgs fa{A, B, T->tw, T->ke, m1, m2, m};
-  LaunchScope ls(family, s);
-  grid_transform_cluster<<<FC, (unsigned)(m / (8 * FC)), smem, s>>>(fa);
-  SHRK_CUDA(cudaGetLastError());
-  *done = true;
-  return SHRK_OK;
-}
-
 // One grid: stencil width, size, origin and spacing, and the launch families
 // its kernels are timed under.
 struct GridPlan {
@@ -968,17 +743,13 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
     pack_dense_kernel<N><<<nb, 256, 0, s>>>(gg);
     SHRK_CUDA(cudaGetLastError());
   }
-  bool fused = false;
-  if (m >= FUSED_MIN_M && m <= FUSED_MAX_M) SHRK_TRY(fused_transform(A, B, m, T, g.fam_fft, s, &fused));
-  if (!fused) {
-    SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, g.fam_fft, s));
-    {
-      LaunchScope ls(g.fam_spectral, s);
-      spectral_kernel<<<blocks_for(m, 256), 256, 0, s>>>(A, T->ke, B, m);
-      SHRK_CUDA(cudaGetLastError());
-    }
-    SHRK_TRY(fft(B, Tmp, m, T->tw, +1.0, g.fam_fft, s));
+  SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, g.fam_fft, s));
+  {
+    LaunchScope ls(g.fam_spectral, s);
+    spectral_kernel<<<blocks_for(m, 256), 256, 0, s>>>(A, T->ke, B, m);
+    SHRK_CUDA(cudaGetLastError());
   }
+  SHRK_TRY(fft(B, Tmp, m, T->tw, +1.0, g.fam_fft, s));
   InterpArgs ia{d_q, nq, B, m, g.lo, g.dx, 1.0 / (double)m, epi};
   {
     LaunchScope ls(g.fam_interp, s);

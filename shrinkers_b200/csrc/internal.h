@@ -177,6 +177,7 @@ double mixed_near_k();
 // = the default) and returns the previous one.
 long long set_wait_cycles(long long cycles);
 shrk_status measure_pipe_rates(double* fp32, double* fp64);
+shrk_status measure_rcp_rate(double* per_s);
 shrk_status measure_rcp_bias(double* uniform_mean, double* log_mean);
 
 }  // namespace shrk
