@@ -53,12 +53,17 @@ namespace {
 constexpr int GT = 64;   // output tile
 constexpr int GK = 16;   // k per shared-memory stage
 
+// Split-K: CTA z of gridDim.z sums k in [z kz, (z+1) kz) and, when the grid
+// has several, writes alpha times its partial product to its own m x n slab
+// of C (ldc = m, beta = 0); dgemm then adds the slabs in a fixed order.
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, double alpha,
+__global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, int kz, double alpha,
                                                     const double* __restrict__ A, int64_t lda,
                                                     const double* __restrict__ B, int64_t ldb,
                                                     double beta, double* __restrict__ C,
                                                     int64_t ldc) {
+  const int kb = blockIdx.z * kz, ke = min(k, kb + kz);
+  if (gridDim.z > 1) C += (int64_t)blockIdx.z * m * n;
   __shared__ double As[GK][GT + 1];  // As[kk][i] = op(A)[i0 + i, k0 + kk]
   __shared__ double Bs[GK][GT + 1];  // Bs[kk][j] = op(B)[k0 + kk, j0 + j]
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -68,7 +73,7 @@ __global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, double 
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-  for (int k0 = 0; k0 < k; k0 += GK) {
+  for (int k0 = kb; k0 < ke; k0 += GK) {
 #pragma unroll
     for (int it = 0; it < 4; ++it) {
       const int t = threadIdx.x + it * 256;
@@ -77,7 +82,7 @@ __global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, double 
       else { kk = t & 15; i = t >> 4; }       // A(kk, i) contiguous in kk
       const int gi = i0 + i, gk = k0 + kk;
       double v = 0.0;
-      if (gi < m && gk < k) v = !TA ? A[gi + (int64_t)gk * lda] : A[gk + (int64_t)gi * lda];
+      if (gi < m && gk < ke) v = !TA ? A[gi + (int64_t)gk * lda] : A[gk + (int64_t)gi * lda];
       As[kk][i] = v;
     }
 #pragma unroll
@@ -88,7 +93,7 @@ __global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, double 
       else { j = t & 63; kk = t >> 6; }       // B(j, kk) contiguous in j
       const int gj = j0 + j, gk = k0 + kk;
       double v = 0.0;
-      if (gj < n && gk < k) v = !TB ? B[gk + (int64_t)gj * ldb] : B[gj + (int64_t)gk * ldb];
+      if (gj < n && gk < ke) v = !TB ? B[gk + (int64_t)gj * ldb] : B[gj + (int64_t)gk * ldb];
       Bs[kk][j] = v;
     }
     __syncthreads();
@@ -118,6 +123,116 @@ __global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, double 
       *cp = beta == 0.0 ? alpha * acc[r][c] : fma(alpha, acc[r][c], beta * *cp);
     }
   }
+}
+
+// The large-problem form: 128 x 128 outputs per CTA of 256 threads, 8 x 8
+// per thread (64 independent FMA chains), k staged 8 at a time, two stages
+// in flight (the next stage's global loads are issued before this stage's
+// FMAs).
+constexpr int GT2 = 128, GK2 = 8;
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256, 1) dgemm_big_kernel(int m, int n, int k, int kz,
+                                                           double alpha,
+                                                           const double* __restrict__ A,
+                                                           int64_t lda,
+                                                           const double* __restrict__ B,
+                                                           int64_t ldb, double beta,
+                                                           double* __restrict__ C,
+                                                           int64_t ldc) {
+  __shared__ double As[2][GK2][GT2 + 2];  // As[kk][i] = op(A)[i0 + i, k0 + kk]
+  __shared__ double Bs[2][GK2][GT2 + 2];  // Bs[kk][j] = op(B)[k0 + kk, j0 + j]
+  const int kb = blockIdx.z * kz, ke = min(k, kb + kz);
+  if (gridDim.z > 1) C += (int64_t)blockIdx.z * m * n;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = blockIdx.x * GT2, j0 = blockIdx.y * GT2;
+  double acc[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
+  double ra[4], rb[4];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int t = threadIdx.x + it * 256;
+      int i, kk;
+      if (!TA) { i = t & 127; kk = t >> 7; }  // A(i, kk) contiguous in i
+      else { kk = t & 7; i = t >> 3; }        // A(kk, i) contiguous in kk
+      const int gi = i0 + i, gk = k0 + kk;
+      ra[it] = (gi < m && gk < ke) ? (!TA ? A[gi + (int64_t)gk * lda] : A[gk + (int64_t)gi * lda])
+                                   : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int t = threadIdx.x + it * 256;
+      int j, kk;
+      if (!TB) { kk = t & 7; j = t >> 3; }    // B(kk, j) contiguous in kk
+      else { j = t & 127; kk = t >> 7; }      // B(j, kk) contiguous in j
+      const int gj = j0 + j, gk = k0 + kk;
+      rb[it] = (gj < n && gk < ke) ? (!TB ? B[gk + (int64_t)gj * ldb] : B[gj + (int64_t)gk * ldb])
+                                   : 0.0;
+    }
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+      const int t = threadIdx.x + it * 256;
+      if (!TA) As[buf][t >> 7][t & 127] = ra[it];
+      else As[buf][t & 7][t >> 3] = ra[it];
+      if (!TB) Bs[buf][t & 7][t >> 3] = rb[it];
+      else Bs[buf][t >> 7][t & 127] = rb[it];
+    }
+  };
+  fetch(kb);
+  stash(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = kb; k0 < ke; k0 += GK2) {
+    const bool more = k0 + GK2 < ke;
+    if (more) fetch(k0 + GK2);
+#pragma unroll
+    for (int kk = 0; kk < GK2; ++kk) {
+      double a[8], b[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) a[r] = As[buf][kk][tx + 16 * r];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) b[c] = Bs[buf][kk][ty + 16 * c];
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+    if (more) {
+      stash(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int gj = j0 + ty + 16 * c;
+    if (gj >= n) continue;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int gi = i0 + tx + 16 * r;
+      if (gi >= m) continue;
+      double* cp = C + gi + (int64_t)gj * ldc;
+      *cp = beta == 0.0 ? alpha * acc[r][c] : fma(alpha, acc[r][c], beta * *cp);
+    }
+  }
+}
+
+// C = sum_z slab[z] + beta C, the split-K slabs added in order.
+__global__ void dgemm_reduce_kernel(const double* __restrict__ ws, int splits, int m, int n,
+                                    double beta, double* __restrict__ C, int64_t ldc) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)m * n) return;
+  const int64_t i = idx % m, j = idx / m;
+  double t = 0.0;
+  for (int z = 0; z < splits; ++z) t += ws[(int64_t)z * m * n + idx];
+  double* cp = C + i + j * ldc;
+  *cp = beta == 0.0 ? t : t + beta * *cp;
 }
 
 // -------------------------------------------------------- tridiagonalise --
@@ -649,7 +764,7 @@ __global__ void mirror_lower_kernel(double* __restrict__ A, int64_t p) {
 
 unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
-constexpr int NB = 32;                 // reflectors per WY block
+constexpr int NB = 64;                 // reflectors per WY block (wy_t_kernel: <= 64)
 // Eigenvalues closer than CLUSTER_TOL ||T|| (numerically equal) share one
 // thread and are orthogonalised by Gram-Schmidt during inverse iteration;
 // every other pair is left to inverse iteration, whose vectors then overlap
@@ -657,11 +772,21 @@ constexpr int NB = 32;                 // reflectors per WY block
 // the overlap), as many as the smallest such gap needs.
 constexpr double CLUSTER_TOL = 1e-12;
 
-// Scratch slots 46..53 belong to this file.
+// Scratch slots 46..54 belong to this file.
 constexpr int SLOT_U = 46, SLOT_Z = 47, SLOT_G = 48, SLOT_SMALL = 49, SLOT_WS = 50,
-              SLOT_WY = 51, SLOT_META = 52, SLOT_VB = 53;
+              SLOT_WY = 51, SLOT_META = 52, SLOT_VB = 53, SLOT_SPLITK = 54;
 
 }  // namespace
+
+template <bool TA, bool TB>
+static void launch_gemm(bool big, dim3 grid, int m, int n, int k, int kz, double alpha,
+                        const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
+                        double* C, int64_t ldc, cudaStream_t s) {
+  if (big)
+    dgemm_big_kernel<TA, TB><<<grid, 256, 0, s>>>(m, n, k, kz, alpha, A, lda, B, ldb, beta, C, ldc);
+  else
+    dgemm_kernel<TA, TB><<<grid, 256, 0, s>>>(m, n, k, kz, alpha, A, lda, B, ldb, beta, C, ldc);
+}
 
 shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
                   int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
@@ -671,13 +796,39 @@ shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alph
     set_error("dgemm: dimensions must be below 2^31");
     return SHRK_EINVAL;
   }
-  const dim3 grid(cdiv(m, GT), cdiv(n, GT));
-  LaunchScope ls("dgemm", s);
-  if (!ta && !tb) dgemm_kernel<false, false><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
-  else if (!ta && tb) dgemm_kernel<false, true><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
-  else if (ta && !tb) dgemm_kernel<true, false><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
-  else dgemm_kernel<true, true><<<grid, 256, 0, s>>>((int)m, (int)n, (int)k, alpha, A, lda, B, ldb, beta, C, ldc);
-  SHRK_CUDA(cudaGetLastError());
+  const bool big = m >= GT2 && n >= GT2 && k >= 64;
+  const int tile = big ? GT2 : GT;
+  const int64_t tiles = (int64_t)cdiv(m, tile) * cdiv(n, tile);
+  // too few output tiles to fill the GPU and a long k: split k
+  const int64_t want = 2LL * sm_count();
+  int splits = 1;
+  if (tiles < want && k >= 512)
+    splits = (int)std::min<int64_t>({(want + tiles - 1) / tiles, k / 256, 16});
+  double* out = C;
+  int64_t ldo = ldc;
+  double b = beta;
+  if (splits > 1) {
+    void* ws = nullptr;
+    SHRK_TRY(scratch_get(SLOT_SPLITK, sizeof(double) * (size_t)splits * (size_t)m * (size_t)n, &ws));
+    out = (double*)ws;
+    ldo = m;
+    b = 0.0;
+  }
+  const int kz = (int)((k + splits - 1) / splits);
+  const dim3 grid(cdiv(m, tile), cdiv(n, tile), (unsigned)splits);
+  {
+    LaunchScope ls("dgemm", s);
+    if (!ta && !tb) launch_gemm<false, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
+    else if (!ta && tb) launch_gemm<false, true>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
+    else if (ta && !tb) launch_gemm<true, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
+    else launch_gemm<true, true>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  if (splits > 1) {
+    LaunchScope ls("dgemm", s);
+    dgemm_reduce_kernel<<<cdiv(m * n, 256), 256, 0, s>>>(out, splits, (int)m, (int)n, beta, C, ldc);
+    SHRK_CUDA(cudaGetLastError());
+  }
   return SHRK_OK;
 }
 
