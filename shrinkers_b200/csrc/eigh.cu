@@ -476,9 +476,28 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
     const int64_t k1 = j + 1, k2 = j + 2;
     const double vj1 = vcur[k1], wj1 = upd ? pj[k1] - K * vj1 : 0.0;
     // column j+1 of A^{(j+1)}, rows >= j+2, and its diagonal entry
-    for (int64_t k = k2 + threadIdx.x; k < p; k += blockDim.x) {
-      const double vk = vcur[k], wk = upd ? pj[k] - K * vk : 0.0;
-      vnext[k] = A[k + k1 * p] - (vk * wj1 + wk * vj1);
+    {
+      const double* colj1 = A + k1 * p;
+      const int64_t bd = blockDim.x;
+      int64_t k = k2 + threadIdx.x;
+      for (; k + 3 * bd < p; k += 4 * bd) {
+        double av[4], vv[4], qv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          av[u] = colj1[k + u * bd];
+          vv[u] = vcur[k + u * bd];
+          qv[u] = pj[k + u * bd];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double wk = upd ? qv[u] - K * vv[u] : 0.0;
+          vnext[k + u * bd] = av[u] - (vv[u] * wj1 + wk * vj1);
+        }
+      }
+      for (; k < p; k += bd) {
+        const double vk = vcur[k], wk = upd ? pj[k] - K * vk : 0.0;
+        vnext[k] = colj1[k] - (vk * wj1 + wk * vj1);
+      }
     }
     const double dnew = A[k1 + k1 * p] - 2.0 * vj1 * wj1;
     double bnext = 0.0;
@@ -506,7 +525,27 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
       double* col = A + c * p;
       const double vc = vcur[c], wc = upd ? pj[c] - K * vc : 0.0;
       double s = 0.0;
-      for (int64_t k = k2 + lane; k < p; k += 32) {
+      int64_t k = k2 + lane;
+      // four rows per lane per step, every load issued before any store
+      // (the stores to col could alias the loads for all the compiler knows)
+      for (; k + 96 < p; k += 128) {
+        double av[4], vv[4], qv[4], nv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          av[u] = col[k + 32 * u];
+          vv[u] = vcur[k + 32 * u];
+          qv[u] = pj[k + 32 * u];
+          nv[u] = vnext[k + 32 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double wk = upd ? qv[u] - K * vv[u] : 0.0;
+          const double x = av[u] - (vv[u] * wc + wk * vc);
+          col[k + 32 * u] = x;
+          s = fma(x, nv[u], s);
+        }
+      }
+      for (; k < p; k += 32) {
         const double vk = vcur[k], wk = upd ? pj[k] - K * vk : 0.0;
         const double x = col[k] - (vk * wc + wk * vc);
         col[k] = x;
