@@ -141,10 +141,8 @@ __device__ __forceinline__ double weight_of(const GridArgs& a, int64_t j) {
 // cells non-decreasing, so this is a lower bound found by bisection (the same
 // cell computation as everywhere else, so the same runs).
 template <int N>
-__global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n_keys,
-                            int* __restrict__ n_dense) {
+__global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n_keys) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx < 2) n_dense[idx] = 0;  // the dense-cell queues start empty
   if (idx >= n_keys) return;
   const int key = (int)(idx - N - 1);
   int64_t lo = 0, hi = a.ns;
@@ -157,23 +155,80 @@ __global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n
   first[idx] = (int)lo;
 }
 
-constexpr int DENSE_MIN = 32;    // sources above which a cell gets a whole warp
-constexpr int CTA_MIN = 2048;    // ... and above which it gets a whole CTA
+constexpr int DENSE_MIN = 32;   // cells with more sources take their density from run sums
+constexpr int RUN_CTA = 256;    // runs with more sources get a whole CTA for their sums
 
-struct GatherArgs {
-  GridArgs g;
-  const int* first;  // first[key + N + 1] = #sources with cell < key, key in [-N-1, m+N]
-  int* dense;        // cells left for pack_dense_kernel: [0, m) warp queue, [m, 2m) CTA queue
-  int* n_dense;      // the two queue lengths
-};
+// Run sums: S[(e + N + 1) N + k] = the sum of stencil weight k over the run
+// of sources whose cell is e.  Each source's N weights are computed once.
+// Blocks below small_blocks give a run of at most RUN_CTA sources one thread
+// (ascending source order); the others stride over the keys and give every
+// longer run one CTA (threads stride the run, partials added in a fixed
+// order).  first has n_keys + 1 entries (the last is ns).
+template <int N>
+__global__ void __launch_bounds__(256) run_sums_kernel(const GridArgs a,
+                                                       const int* __restrict__ first,
+                                                       int64_t n_keys, int small_blocks,
+                                                       double* __restrict__ S) {
+  if ((int)blockIdx.x < small_blocks) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n_keys) return;
+    const int64_t j0 = first[idx], j1 = first[idx + 1];
+    if (j1 - j0 > RUN_CTA) return;
+    double acc[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) acc[k] = 0.0;
+    for (int64_t j = j0; j < j1; ++j) {
+      double t, w[N];
+      (void)clamped_cell<N>(a, j, &t);
+      lagrange<N>(t, w);
+#pragma unroll
+      for (int k = 0; k < N; ++k) acc[k] += w[k];
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) S[idx * N + k] = acc[k];
+    return;
+  }
+  __shared__ double red[8][N];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (int64_t idx = (int64_t)blockIdx.x - small_blocks; idx < n_keys;
+       idx += (int64_t)gridDim.x - small_blocks) {
+    const int64_t j0 = first[idx], j1 = first[idx + 1];
+    if (j1 - j0 <= RUN_CTA) continue;  // uniform across the CTA
+    double acc[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) acc[k] = 0.0;
+    for (int64_t j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
+      double t, w[N];
+      (void)clamped_cell<N>(a, j, &t);
+      lagrange<N>(t, w);
+#pragma unroll
+      for (int k = 0; k < N; ++k) acc[k] += w[k];
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double v = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[wib][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < N) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+      S[idx * N + threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
 
-// Steps 1+pack: the density of cell c is the sum of weight k over the run of
-// sources with i0 = c + N/2 - 1 - k, for k = N-1 .. 0 (fft5.rs:175-185): the
-// runs in ascending cell order, i.e. the sources in ascending order -- the
-// order of the reference's sequential splat.  The two edge cells also collect
-// every clamped slot.  One thread per cell adds at most DENSE_MIN sources and
-// queues denser cells for pack_dense_kernel.  packed[c] = density[c] +
-// i x_c/(x_c^2 + eta^2) (fft5.rs:364-376).
+// The density of cell c is the sum of weight k over the run of sources with
+// cell c + N/2 - 1 - k, k = N-1 .. 0 (fft5.rs:175-185).  A cell with at most
+// DENSE_MIN sources adds them one by one, runs in ascending cell order and
+// each run in ascending source order -- the order of the reference's
+// sequential splat, so these densities are the same sums, without atomics;
+// a denser cell adds the N run sums in that run order (deterministic, not the
+// sequential order).  The two edge cells also collect every clamped slot.
+// packed[c] = density[c] + i x_c/(x_c^2 + eta^2) (fft5.rs:364-376).
 __device__ __forceinline__ void pack_cell(const GridArgs& a, int64_t c, double dens) {
   const int64_t half = a.m / 2;
   const double sd = (c <= half) ? (double)c : (double)c - (double)a.m;
@@ -183,8 +238,7 @@ __device__ __forceinline__ void pack_cell(const GridArgs& a, int64_t c, double d
 }
 
 // dens += weight K of every source of the run of cell c + N/2 - 1 - K, for
-// K = KK .. 0 in that order: the runs in ascending cell order, each run in
-// ascending source order (the sequential splat's order).
+// K = KK .. 0 in that order.
 template <int N, int KK>
 __device__ __forceinline__ void run_sums(const GridArgs& a, const int* first, int64_t c,
                                          double& dens) {
@@ -196,22 +250,22 @@ __device__ __forceinline__ void run_sums(const GridArgs& a, const int* first, in
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) pack_sparse_kernel(const GatherArgs ga) {
+__global__ void __launch_bounds__(256) pack_kernel(const GridArgs a, const int* __restrict__ first_all,
+                                                   const double* __restrict__ S) {
   constexpr int H = N / 2;
-  const GridArgs& a = ga.g;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t m = a.m;
   if (c >= m) return;
-  const int* first = ga.first + N + 1;  // first[key] for key >= -N - 1
+  const int* first = first_all + N + 1;  // first[key] for key >= -N - 1
   double dens = 0.0;
   if (c > 0 && c < m - 1) {
     const int cnt = first[c + H] - first[c - H];
     if (cnt > DENSE_MIN) {
-      const int q = cnt > CTA_MIN ? 1 : 0;
-      ga.dense[q * m + atomicAdd(ga.n_dense + q, 1)] = (int)c;
-      return;
+#pragma unroll
+      for (int k = N - 1; k >= 0; --k) dens += S[(c + H - 1 - k + N + 1) * N + k];
+    } else {
+      run_sums<N, N - 1>(a, first, c, dens);
     }
-    run_sums<N, N - 1>(a, first, c, dens);
   } else {
     // edge cell: every slot whose clamped index lands here, sources then slots
     const int64_t j0 = (c == 0) ? 0 : first[m - 1 - H];
@@ -230,61 +284,6 @@ __global__ void __launch_bounds__(256) pack_sparse_kernel(const GatherArgs ga) {
     }
   }
   pack_cell(a, c, dens);
-}
-
-// The queued cells.  Cells of the CTA queue get one CTA each: threads stride
-// each run and the partial sums are added in a fixed order (warp butterflies,
-// then the warps in order).  Cells of the warp queue get one warp each, lanes
-// striding the runs, a butterfly at the end.  Deterministic, not the
-// sequential order; CTAs and warps stride the queues, whose lengths are read
-// on the device.
-template <int N, int KK>
-__device__ __forceinline__ void strided_run_sums(const GridArgs& a, const int* first, int c, int t,
-                                                 int nt, double& dens) {
-  if constexpr (KK >= 0) {
-    const int e = c + N / 2 - 1 - KK;  // the run of cell e feeds slot KK
-    const int64_t j1 = first[e + 1];
-    for (int64_t j = first[e] + t; j < j1; j += nt) dens += weight_of<N, KK>(a, j);
-    strided_run_sums<N, KK - 1>(a, first, c, t, nt, dens);
-  }
-}
-
-template <int N>
-__device__ __forceinline__ double window_sum(const GatherArgs& ga, const int* first, int c,
-                                             int t, int nt) {
-  double dens = 0.0;
-  strided_run_sums<N, N - 1>(ga.g, first, c, t, nt, dens);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) dens += __shfl_xor_sync(0xffffffffu, dens, o);
-  return dens;
-}
-
-template <int N>
-__global__ void __launch_bounds__(256) pack_dense_kernel(const GatherArgs ga) {
-  __shared__ double s_part[8];
-  const int* first = ga.first + N + 1;
-  const int64_t m = ga.g.m;
-  const int n_cta = ga.n_dense[1];
-  for (int i = blockIdx.x; i < n_cta; i += gridDim.x) {
-    const int c = ga.dense[m + i];
-    const double d = window_sum<N>(ga, first, c, threadIdx.x, blockDim.x);
-    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = d;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
-      pack_cell(ga.g, c, t);
-    }
-    __syncthreads();
-  }
-  const int n_warp = ga.n_dense[0];
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_warp; i += warps) {
-    const int c = ga.dense[i];
-    const double d = window_sum<N>(ga, first, c, lane, 32);
-    if (lane == 0) pack_cell(ga.g, c, d);
-  }
 }
 
 // ---------------------------------------------------------------- FFT --
@@ -717,30 +716,29 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   double2* A = (double2*)w;
   double2* B = A + m;
   double2* Tmp = B + m;
-  // slot 24: first [K] | queues [2m] | queue lengths [2], K = m + 2N + 2 keys
-  // from -N - 1.
+  // slot 24: first [K + 1] | run sums [K][N], K = m + 2N + 2 keys from -N - 1
   const int64_t n_keys = m + 2 * N + 2;
+  const size_t first_bytes = ((sizeof(int) * ((size_t)n_keys + 1)) + 255) & ~(size_t)255;
   void* sw = nullptr;
-  SHRK_TRY(scratch_get(24, sizeof(int) * ((size_t)n_keys + 2 * (size_t)m + 2), &sw));
+  SHRK_TRY(scratch_get(24, first_bytes + sizeof(double) * N * (size_t)n_keys, &sw));
   int* first = (int*)sw;
-  int* dense = first + n_keys;
-  int* n_dense = dense + 2 * m;
+  double* runs = (double*)((char*)sw + first_bytes);
   GridArgs ga{d_src, ns, g.dx < 0.0 ? 1 : 0, g.lo, g.dx, eta, m, A};
-  GatherArgs gg{ga, first, dense, n_dense};
   {
     LaunchScope ls(g.fam_splat, s);
-    keys_kernel<N><<<blocks_for(n_keys, 256), 256, 0, s>>>(ga, first, n_keys, n_dense);
+    keys_kernel<N><<<blocks_for(n_keys + 1, 256), 256, 0, s>>>(ga, first, n_keys + 1);
     SHRK_CUDA(cudaGetLastError());
   }
   {
     LaunchScope ls(g.fam_splat, s);
-    pack_sparse_kernel<N><<<blocks_for(m, 256), 256, 0, s>>>(gg);
+    const int small_blocks = (int)blocks_for(n_keys, 256);
+    run_sums_kernel<N><<<small_blocks + sm_count() * 4, 256, 0, s>>>(ga, first, n_keys,
+                                                                       small_blocks, runs);
     SHRK_CUDA(cudaGetLastError());
   }
   {
     LaunchScope ls(g.fam_splat, s);
-    const unsigned nb = (unsigned)std::min<int64_t>(m, 148 * 16);
-    pack_dense_kernel<N><<<nb, 256, 0, s>>>(gg);
+    pack_kernel<N><<<blocks_for(m, 256), 256, 0, s>>>(ga, first, runs);
     SHRK_CUDA(cudaGetLastError());
   }
   SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, g.fam_fft, s));
