@@ -156,7 +156,7 @@ __global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n
 }
 
 constexpr int DENSE_MIN = 32;   // cells with more sources take their density from run sums
-constexpr int RUN_CTA = 256;    // runs with more sources get a whole CTA for their sums
+constexpr int RUN_CTA = 32;     // runs with more sources get a whole CTA for their sums
 
 // Run sums: S[(e + N + 1) N + k] = the sum of stencil weight k over the run
 // of sources whose cell is e.  Each source's N weights are computed once.
