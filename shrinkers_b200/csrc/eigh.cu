@@ -526,19 +526,19 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
       const double vc = vcur[c], wc = upd ? pj[c] - K * vc : 0.0;
       double s = 0.0;
       int64_t k = k2 + lane;
-      // four rows per lane per step, every load issued before any store
+      // eight rows per lane per step, every load issued before any store
       // (the stores to col could alias the loads for all the compiler knows)
-      for (; k + 96 < p; k += 128) {
-        double av[4], vv[4], qv[4], nv[4];
+      for (; k + 224 < p; k += 256) {
+        double av[8], vv[8], qv[8], nv[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 8; ++u) {
           av[u] = col[k + 32 * u];
           vv[u] = vcur[k + 32 * u];
           qv[u] = pj[k + 32 * u];
           nv[u] = vnext[k + 32 * u];
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < 8; ++u) {
           const double wk = upd ? qv[u] - K * vv[u] : 0.0;
           const double x = av[u] - (vv[u] * wc + wk * vc);
           col[k + 32 * u] = x;
