@@ -179,11 +179,13 @@ shrk_status shrk_stieltjes_batched_dev(const double* d_ev, const int64_t* d_offs
  * p-bucket [2^8,2^9), ..., [2^14,2^15), [2^15,inf) it times every candidate
  * (targets per thread R in {2,4}, source split SL in {1024,...,8192}) on a
  * synthetic batch of that bucket and keeps the fastest; table receives
- * (R, SL) per bucket, 16 ints.  Runs once per device and precision (the
- * first batched call runs it implicitly, unless the environment variable
- * SHRK_BATCHED_AUTOTUNE=0 selects the fixed default table), again when
- * force != 0.  Spectra of the batched entry points hold at most 16 777 216
- * values each. */
+ * (R, SL) per bucket, 16 ints.  Batched calls plan with a table the
+ * autotuner chose on a B200 until this runs (with force != 0, or force == 0
+ * before any batched call on the device) or shrk_batched_set_tune installs
+ * another; with the environment variable SHRK_BATCHED_AUTOTUNE=1 the first
+ * batched call tunes instead.  With force == 0 on a device that already has
+ * a table, table receives it without tuning.  Spectra of the batched entry
+ * points hold at most 16 777 216 values each. */
 shrk_status shrk_batched_autotune(int precision, int force, int32_t* table);
 /* Installs a (R, SL) table of the layout shrk_batched_autotune returns, for
  * `precision` on the current device, e.g. one saved from an earlier process

@@ -167,10 +167,17 @@ int bucket_of(int64_t p) {
   return std::min(std::max(b, 8), 15) - 8;
 }
 
-void default_tune(Tune& t) {
+// The table the autotuner chose on a B200 (one run, per precision), used
+// until a call tunes or installs another: (R, SL) per p-bucket.
+constexpr int kDefaultR[2][NB] = {{2, 4, 2, 4, 4, 4, 4, 4}, {2, 4, 2, 4, 2, 2, 2, 2}};
+constexpr int kDefaultSL[2][NB] = {{1024, 1024, 2048, 2048, 1024, 2048, 8192, 8192},
+                                   {1024, 1024, 2048, 4096, 4096, 2048, 4096, 8192}};
+
+void default_tune(Tune& t, int precision) {
+  const int q = precision == SHRK_PREC_MIXED ? 1 : 0;
   for (int b = 0; b < NB; ++b) {
-    t.R[b] = b < 2 ? 2 : 4;
-    t.SL[b] = 4096;
+    t.R[b] = kDefaultR[q][b];
+    t.SL[b] = kDefaultSL[q][b];
   }
 }
 
@@ -345,7 +352,7 @@ shrk_status time_config(const Plan& pl, const double* d_ev, const double* d_eta,
 // (p = 1.5 * 2^b, about 4M targets and at most 5e9 pairs) is timed for every
 // (R, SL) candidate; the fastest is kept.
 shrk_status autotune(int precision, Tune& t, cudaStream_t s) {
-  default_tune(t);
+  default_tune(t, precision);
   for (int b = 0; b < NB; ++b) {
     const int64_t p = 3LL << (b + 7);
     const int64_t n = std::max<int64_t>(1, std::min<int64_t>((1LL << 22) / p,
@@ -474,14 +481,15 @@ shrk_status batched(const double* d_ev, const int64_t* d_offsets, const int64_t*
     std::lock_guard<std::mutex> lk(g_tune_mu[dev]);
     Tune& tt = g_tune[dev][precision];
     if (!tt.tuned) {
-      // SHRK_BATCHED_AUTOTUNE=0: keep the default table (plans, and so the
-      // split summation order, then do not depend on timing).
+      // The B200 table by default; SHRK_BATCHED_AUTOTUNE=1 tunes on this
+      // device at the first call instead (plans, and so the split summation
+      // order, then depend on timing).
       const char* env = std::getenv("SHRK_BATCHED_AUTOTUNE");
-      if (env && std::strcmp(env, "0") == 0) {
-        default_tune(tt);
-        tt.tuned = true;
-      } else {
+      if (env && std::strcmp(env, "1") == 0) {
         SHRK_TRY(autotune(precision, tt, s));
+      } else {
+        default_tune(tt, precision);
+        tt.tuned = true;
       }
     }
     t = tt;
