@@ -136,64 +136,82 @@ __device__ __forceinline__ double weight_of(const GridArgs& a, int64_t j) {
   return w[K];
 }
 
-// first[key + N + 1] for every key in [-N - 1, m + N]: the number of visited
-// sources whose clamped stencil cell is below key.  Visiting order makes the
-// cells non-decreasing, so this is a lower bound found by bisection (the same
-// cell computation as everywhere else, so the same runs).
+// first[key + N + 1] for every key in [-N - 1, m + N + 1]: the number of
+// visited sources whose clamped stencil cell is below key.  Visiting order
+// makes the cells non-decreasing, so this is a lower bound found by
+// bisection (the same cell computation as everywhere else, so the same runs).
 template <int N>
-__global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n_keys) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_keys) return;
-  const int key = (int)(idx - N - 1);
-  int64_t lo = 0, hi = a.ns;
+__device__ __forceinline__ int64_t lower_key(const GridArgs& a, int key, int64_t lo, int64_t hi) {
   while (lo < hi) {
     const int64_t mid = (lo + hi) >> 1;
     double t;
     if (clamped_cell<N>(a, mid, &t) < key) lo = mid + 1;
     else hi = mid;
   }
-  first[idx] = (int)lo;
+  return lo;
 }
 
 constexpr int DENSE_MIN = 32;   // cells with more sources take their density from run sums
 constexpr int RUN_CTA = 32;     // runs with more sources get a whole CTA for their sums
 
-// Run sums: S[(e + N + 1) N + k] = the sum of stencil weight k over the run
-// of sources whose cell is e.  Each source's N weights are computed once.
-// Blocks below small_blocks give a run of at most RUN_CTA sources one thread
-// (ascending source order); the others stride over the keys and give every
-// longer run one CTA (threads stride the run, partials added in a fixed
-// order).  first has n_keys + 1 entries (the last is ns).
+// Keys and run sums.  The thread of key e finds first[e] by bisection and
+// the end of its run by a galloping search from there (one probe for an empty
+// run); then S[(e + N + 1) N + k], the sum of stencil weight k over the run,
+// computing each source's N weights once in ascending source order -- or,
+// for a run of more than RUN_CTA sources, appends e to the list that
+// long_runs_kernel gives a CTA each (*n_long is zero on entry).
 template <int N>
-__global__ void __launch_bounds__(256) run_sums_kernel(const GridArgs a,
-                                                       const int* __restrict__ first,
-                                                       int64_t n_keys, int small_blocks,
-                                                       double* __restrict__ S) {
-  if ((int)blockIdx.x < small_blocks) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n_keys) return;
-    const int64_t j0 = first[idx], j1 = first[idx + 1];
-    if (j1 - j0 > RUN_CTA) return;
-    double acc[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) acc[k] = 0.0;
-    for (int64_t j = j0; j < j1; ++j) {
-      double t, w[N];
-      (void)clamped_cell<N>(a, j, &t);
-      lagrange<N>(t, w);
-#pragma unroll
-      for (int k = 0; k < N; ++k) acc[k] += w[k];
-    }
-#pragma unroll
-    for (int k = 0; k < N; ++k) S[idx * N + k] = acc[k];
+__global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n_keys,
+                            double* __restrict__ S, int* __restrict__ long_runs,
+                            int* __restrict__ n_long) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx > n_keys) return;
+  const int key = (int)(idx - N - 1);
+  const int64_t j0 = lower_key<N>(a, key, 0, a.ns);
+  first[idx] = (int)j0;
+  if (idx == n_keys) return;  // the closing entry (= ns)
+  // end of the run: the first source whose cell is at least key + 1
+  int64_t lo = j0, step = 1, hi = j0;
+  double t;
+  while (hi < a.ns && clamped_cell<N>(a, hi, &t) < key + 1) {
+    lo = hi + 1;
+    hi = j0 + step;
+    step *= 2;
+  }
+  const int64_t j1 = lower_key<N>(a, key + 1, lo, hi < a.ns ? hi : a.ns);
+  if (j1 - j0 > RUN_CTA) {
+    long_runs[atomicAdd(n_long, 1)] = (int)idx;
     return;
   }
+  double acc[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) acc[k] = 0.0;
+  for (int64_t j = j0; j < j1; ++j) {
+    double w[N];
+    (void)clamped_cell<N>(a, j, &t);
+    lagrange<N>(t, w);
+#pragma unroll
+    for (int k = 0; k < N; ++k) acc[k] += w[k];
+  }
+#pragma unroll
+  for (int k = 0; k < N; ++k) S[idx * N + k] = acc[k];
+}
+
+// Run sums of the long runs, one CTA each (threads stride the run, partials
+// added in a fixed order).  The list order varies from call to call; each
+// run's sum does not.
+template <int N>
+__global__ void __launch_bounds__(256) long_runs_kernel(const GridArgs a,
+                                                        const int* __restrict__ first,
+                                                        const int* __restrict__ long_runs,
+                                                        const int* __restrict__ n_long,
+                                                        double* __restrict__ S) {
   __shared__ double red[8][N];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  for (int64_t idx = (int64_t)blockIdx.x - small_blocks; idx < n_keys;
-       idx += (int64_t)gridDim.x - small_blocks) {
+  const int nl = *n_long;
+  for (int r = blockIdx.x; r < nl; r += gridDim.x) {
+    const int64_t idx = long_runs[r];
     const int64_t j0 = first[idx], j1 = first[idx + 1];
-    if (j1 - j0 <= RUN_CTA) continue;  // uniform across the CTA
     double acc[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) acc[k] = 0.0;
@@ -213,9 +231,9 @@ __global__ void __launch_bounds__(256) run_sums_kernel(const GridArgs a,
     }
     __syncthreads();
     if (threadIdx.x < N) {
-      double t = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
-      S[idx * N + threadIdx.x] = t;
+      double tt = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tt += red[w][threadIdx.x];
+      S[idx * N + threadIdx.x] = tt;
     }
     __syncthreads();
   }
@@ -716,24 +734,27 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   double2* A = (double2*)w;
   double2* B = A + m;
   double2* Tmp = B + m;
-  // slot 24: first [K + 1] | run sums [K][N], K = m + 2N + 2 keys from -N - 1
+  // slot 24: first [K + 1] | long-run list [K] + its length | run sums [K][N],
+  // K = m + 2N + 2 keys from -N - 1
   const int64_t n_keys = m + 2 * N + 2;
-  const size_t first_bytes = ((sizeof(int) * ((size_t)n_keys + 1)) + 255) & ~(size_t)255;
+  const size_t first_bytes = ((sizeof(int) * (2 * (size_t)n_keys + 2)) + 255) & ~(size_t)255;
   void* sw = nullptr;
   SHRK_TRY(scratch_get(24, first_bytes + sizeof(double) * N * (size_t)n_keys, &sw));
   int* first = (int*)sw;
+  int* long_runs = first + n_keys + 1;
+  int* n_long = long_runs + n_keys;
   double* runs = (double*)((char*)sw + first_bytes);
   GridArgs ga{d_src, ns, g.dx < 0.0 ? 1 : 0, g.lo, g.dx, eta, m, A};
+  SHRK_CUDA(cudaMemsetAsync(n_long, 0, sizeof(int), s));
   {
     LaunchScope ls(g.fam_splat, s);
-    keys_kernel<N><<<blocks_for(n_keys + 1, 256), 256, 0, s>>>(ga, first, n_keys + 1);
+    keys_kernel<N><<<blocks_for(n_keys + 1, 256), 256, 0, s>>>(ga, first, n_keys, runs, long_runs,
+                                                              n_long);
     SHRK_CUDA(cudaGetLastError());
   }
   {
     LaunchScope ls(g.fam_splat, s);
-    const int small_blocks = (int)blocks_for(n_keys, 256);
-    run_sums_kernel<N><<<small_blocks + sm_count() * 4, 256, 0, s>>>(ga, first, n_keys,
-                                                                       small_blocks, runs);
+    long_runs_kernel<N><<<sm_count() * 4, 256, 0, s>>>(ga, first, long_runs, n_long, runs);
     SHRK_CUDA(cudaGetLastError());
   }
   {
