@@ -621,6 +621,7 @@ def run_path(args, world, rank, local):
                 L.shrk_timing_read(f.encode(), C.byref(n_), C.byref(ms_))
                 fams[f] = (n_.value, ms_.value)
             alg, basis = alg_fam["nufft_splat"]
+            k_s = fams["nufft_splat"][1] / max(1, args.steps) * 1e-3  # the family, per step
             ach = alg / k_s / 1e9
             tr = None
             tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -630,8 +631,9 @@ def run_path(args, world, rank, local):
             roof = {"bound": "hbm", "achieved": ach, "peak": _measured_hbm(), "unit": "GB/s",
                     "frac": ach / _measured_hbm(), "traffic": tr, "kernel": "nufft_splat",
                     "kernel_ms": k_s * 1e3, "grid_cells": m,
-                    "basis": "splat family (cell keys + gather/pack launches): " + basis
-                             + ", per step",
+                    "basis": "splat family (keys + short-run sums, long-run sums, pack: three "
+                             "launches) per step: " + basis + "; traffic = DRAM bytes of those "
+                             "launches per step (ncu at p = 2^24, scaled by the source count)",
                     "families_ms": {k_: v[1] / max(1, args.steps) for k_, v in fams.items()},
                     "call_algorithmic_bytes": total_alg,
                     "call_gbs": total_alg / (ms * 1e-3) / 1e9}
