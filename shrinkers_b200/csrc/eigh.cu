@@ -630,7 +630,7 @@ __device__ __forceinline__ double start_entry(int slot, int i) {
 // accesses to the same row coalesce): u0, u1, u2 of U and the right-hand
 // side / solution x, rows relative to the block start.  Eigenvector of slot
 // s goes to Zt[s + i p] (row s of Z^T) for i in [b0, b1).
-__global__ void __launch_bounds__(128) inverse_iteration_kernel(
+__global__ void __launch_bounds__(64) inverse_iteration_kernel(
     const double* __restrict__ d, const double* __restrict__ e, const double* __restrict__ lam,
     const Cluster* __restrict__ cl, int ncl, int64_t p, double tnorm, double* __restrict__ ws,
     double* __restrict__ Zt) {
@@ -645,74 +645,108 @@ __global__ void __launch_bounds__(128) inverse_iteration_kernel(
 #define W(arr, i) arr[(int64_t)(i) * stride + t]
   const int n = c.b1 - c.b0;
   const double small = 2.220446049250313e-16 * tnorm + 1e-300;
+  constexpr int CH = 8;  // rows whose loads are issued together (a row's loads
+                         // would otherwise wait behind the previous row's stores)
   for (int q = 0; q < c.ns; ++q) {
     const int slot = c.s0 + q;
     const double l = lam[slot];
     for (int i = 0; i < n; ++i) W(x, i) = start_entry(slot, i);
+    double scale = 1.0;  // x in memory times scale is the current vector
     for (int iter = 0; iter < 3; ++iter) {
       // factor T - l I with partial pivoting, eliminating the right-hand side
       double diag = d[c.b0] - l;
       double sup = n > 1 ? e[c.b0] : 0.0;
-      double rhs = W(x, 0);
-      for (int i = 0; i + 1 < n; ++i) {
-        const double sub = e[c.b0 + i];
-        const double nd = d[c.b0 + i + 1] - l;
-        const double ns = i + 2 < n ? e[c.b0 + i + 1] : 0.0;
-        const double rn = W(x, i + 1);
-        if (fabs(diag) >= fabs(sub)) {
-          const double m = diag != 0.0 ? sub / diag : 0.0;
-          W(u0, i) = diag;
-          W(u1, i) = sup;
-          W(u2, i) = 0.0;
-          W(x, i) = rhs;
-          diag = nd - m * sup;
-          sup = ns;
-          rhs = rn - m * rhs;
-        } else {
-          const double m = diag / sub;
-          W(u0, i) = sub;
-          W(u1, i) = nd;
-          W(u2, i) = ns;
-          W(x, i) = rn;
-          diag = sup - m * nd;
-          sup = -m * ns;
-          rhs = rhs - m * rn;
+      double rhs = W(x, 0) * scale;
+      for (int i0 = 0; i0 + 1 < n; i0 += CH) {
+        double rnv[CH], subv[CH], ndv[CH], nsv[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int i = i0 + u;
+          const bool ok = i + 1 < n;
+          rnv[u] = ok ? W(x, i + 1) * scale : 0.0;
+          subv[u] = ok ? e[c.b0 + i] : 0.0;
+          ndv[u] = ok ? d[c.b0 + i + 1] - l : 0.0;
+          nsv[u] = i + 2 < n ? e[c.b0 + i + 1] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int i = i0 + u;
+          if (i + 1 >= n) break;
+          const double sub = subv[u], nd = ndv[u], ns = nsv[u], rn = rnv[u];
+          if (fabs(diag) >= fabs(sub)) {
+            const double m = diag != 0.0 ? sub / diag : 0.0;
+            W(u0, i) = diag;
+            W(u1, i) = sup;
+            W(u2, i) = 0.0;
+            W(x, i) = rhs;
+            diag = nd - m * sup;
+            sup = ns;
+            rhs = rn - m * rhs;
+          } else {
+            const double m = diag / sub;
+            W(u0, i) = sub;
+            W(u1, i) = nd;
+            W(u2, i) = ns;
+            W(x, i) = rn;
+            diag = sup - m * nd;
+            sup = -m * ns;
+            rhs = rhs - m * rn;
+          }
         }
       }
       W(u0, n - 1) = diag;
       W(x, n - 1) = rhs;
       // back substitution, tiny pivots replaced by eps ||T||
       double nrm2 = 0.0, x1 = 0.0, x2 = 0.0;
-      for (int i = n - 1; i >= 0; --i) {
-        double piv = W(u0, i);
-        if (fabs(piv) < small) piv = piv < 0.0 ? -small : small;
-        double s = W(x, i);
-        if (i + 1 < n) s -= W(u1, i) * x1;
-        if (i + 2 < n) s -= W(u2, i) * x2;
-        const double xi = s / piv;
-        W(x, i) = xi;
-        nrm2 += xi * xi;
-        x2 = x1;
-        x1 = xi;
-      }
-      double inv = 1.0 / sqrt(nrm2);
-      for (int i = 0; i < n; ++i) W(x, i) *= inv;
-      // modified Gram-Schmidt against the cluster's earlier vectors
-      for (int r = 0; r < q; ++r) {
-        const double* zr = Zt + (c.s0 + r);
-        double dt = 0.0;
-        for (int i = 0; i < n; ++i) dt += zr[(int64_t)(c.b0 + i) * p] * W(x, i);
-        nrm2 = 0.0;
-        for (int i = 0; i < n; ++i) {
-          const double xi = W(x, i) - dt * zr[(int64_t)(c.b0 + i) * p];
+      for (int i0 = n - 1; i0 >= 0; i0 -= CH) {
+        double p0[CH], p1[CH], p2[CH], xv[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int i = i0 - u;
+          const bool ok = i >= 0;
+          p0[u] = ok ? W(u0, i) : 1.0;
+          p1[u] = ok ? W(u1, i) : 0.0;
+          p2[u] = ok ? W(u2, i) : 0.0;
+          xv[u] = ok ? W(x, i) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+          const int i = i0 - u;
+          if (i < 0) break;
+          double piv = p0[u];
+          if (fabs(piv) < small) piv = piv < 0.0 ? -small : small;
+          double sv = xv[u];
+          if (i + 1 < n) sv -= p1[u] * x1;
+          if (i + 2 < n) sv -= p2[u] * x2;
+          const double xi = sv / piv;
           W(x, i) = xi;
           nrm2 += xi * xi;
+          x2 = x1;
+          x1 = xi;
         }
-        inv = 1.0 / sqrt(nrm2);
-        for (int i = 0; i < n; ++i) W(x, i) *= inv;
+      }
+      scale = 1.0 / sqrt(nrm2);
+      if (q > 0) {
+        // modified Gram-Schmidt against the cluster's earlier vectors (on the
+        // normalised vector; rare: numerically equal eigenvalues only)
+        for (int i = 0; i < n; ++i) W(x, i) *= scale;
+        scale = 1.0;
+        for (int r = 0; r < q; ++r) {
+          const double* zr = Zt + (c.s0 + r);
+          double dt = 0.0;
+          for (int i = 0; i < n; ++i) dt += zr[(int64_t)(c.b0 + i) * p] * W(x, i);
+          nrm2 = 0.0;
+          for (int i = 0; i < n; ++i) {
+            const double xi = W(x, i) - dt * zr[(int64_t)(c.b0 + i) * p];
+            W(x, i) = xi;
+            nrm2 += xi * xi;
+          }
+          const double inv = 1.0 / sqrt(nrm2);
+          for (int i = 0; i < n; ++i) W(x, i) *= inv;
+        }
       }
     }
-    for (int i = 0; i < n; ++i) Zt[slot + (int64_t)(c.b0 + i) * p] = W(x, i);
+    for (int i = 0; i < n; ++i) Zt[slot + (int64_t)(c.b0 + i) * p] = W(x, i) * scale;
   }
 #undef W
 }
@@ -1023,7 +1057,7 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
   SHRK_CUDA(cudaMemsetAsync(Zt, 0, sizeof(double) * (size_t)P2, s));
   {
     LaunchScope ls("eigh_inverse_iteration", s);
-    inverse_iteration_kernel<<<cdiv(ncl, 128), 128, 0, s>>>(d, e, lam, dcl, ncl, p, tnorm,
+    inverse_iteration_kernel<<<cdiv(ncl, 64), 64, 0, s>>>(d, e, lam, dcl, ncl, p, tnorm,
                                                             (double*)ws, Zt);
     SHRK_CUDA(cudaGetLastError());
   }
