@@ -765,8 +765,8 @@ __global__ void ns_matrix_kernel(double* __restrict__ g, int64_t p) {
 // sits below the diagonal in column j (rowstore 0) or right of it in row j
 // (rowstore 1), its head in vhead[j].
 __global__ void build_y_kernel(const double* __restrict__ A, const double* __restrict__ vhead,
-                               int64_t p, int64_t j0, int nb, int rowstore,
-                               double* __restrict__ Y) {
+                               const double* __restrict__ beta, int64_t p, int64_t j0, int nb,
+                               int rowstore, double* __restrict__ Y) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int jj = blockIdx.y;
   const int64_t n = p - j0 - 1;
@@ -774,34 +774,43 @@ __global__ void build_y_kernel(const double* __restrict__ A, const double* __res
   const int64_t j = j0 + jj;
   const int64_t row = j0 + 1 + r;
   double v = 0.0;
-  if (row == j + 1) v = vhead[j];
+  if (beta[j] == 0.0) v = 0.0;  // no reflection: a zero column of Y
+  else if (row == j + 1) v = vhead[j];
   else if (row > j + 1) v = rowstore ? A[j + row * p] : A[row + j * p];
   Y[r + (int64_t)jj * n] = v;
 }
 
-// T of the compact WY form, H_{j0} ... H_{j0+nb-1} = I - Y T Y^T (forward,
-// columnwise): T[jj][jj] = beta, T[0:jj, jj] = -beta T[0:jj, 0:jj] S[0:jj, jj]
-// with S = Y^T Y.  One CTA; nb <= 64.
+// T of the compact WY form, H_{j0} ... H_{j0+nb-1} = I - Y T Y^T (forward),
+// from T^{-1} = triu(S, 1) + diag(1 / beta), S = Y^T Y (the inverse of T is
+// the strictly upper part of Y^T Y plus the reflectors' v^T v / 2 on the
+// diagonal): thread j solves for column j of T by back substitution, all
+// columns at once (a reflector with beta = 0 has a zero column in Y and a
+// unit diagonal here).  One CTA of nb <= 64 threads.
 __global__ void wy_t_kernel(const double* __restrict__ S, const double* __restrict__ beta,
                             int64_t j0, int nb, double* __restrict__ T) {
-  __shared__ double t[64 * 64];
-  __shared__ double col[64];
-  for (int i = threadIdx.x; i < nb * nb; i += blockDim.x) t[i] = 0.0;
-  __syncthreads();
-  for (int jj = 0; jj < nb; ++jj) {
-    const double b = beta[j0 + jj];
-    const int r = threadIdx.x;
-    if (r < jj) {
-      double s = 0.0;
-      for (int q = r; q < jj; ++q) s += t[r + q * nb] * S[q + jj * nb];
-      col[r] = -b * s;
-    }
-    __syncthreads();
-    if (r < jj) t[r + jj * nb] = col[r];
-    if (r == 0) t[jj + jj * nb] = b;
-    __syncthreads();
+  __shared__ double u[64][65];   // u[i][k] = T^{-1}[i][k]
+  double tc[64];                 // this thread's column of T (local memory)
+  const int j = threadIdx.x;
+  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+    const int i = idx % nb, k = idx / nb;
+    double v = 0.0;
+    if (i < k) v = S[i + k * nb];
+    else if (i == k) v = beta[j0 + i] != 0.0 ? 1.0 / beta[j0 + i] : 1.0;
+    u[i][k] = v;
   }
-  for (int i = threadIdx.x; i < nb * nb; i += blockDim.x) T[i] = t[i];
+  __syncthreads();
+  if (j < nb) {
+    for (int i = nb - 1; i >= 0; --i) {
+      double t = 0.0;
+      if (i <= j) {
+        double acc = i == j ? 1.0 : 0.0;
+        for (int k = i + 1; k <= j; ++k) acc -= u[i][k] * tc[k];
+        t = acc / u[i][i];
+      }
+      tc[i] = t;
+    }
+    for (int i = 0; i < nb; ++i) T[i + j * nb] = tc[i];
+  }
 }
 
 // out[:, k] = U[:, perm[k]]
@@ -1099,8 +1108,8 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
       const int64_t n = p - j0 - 1;
       {
         LaunchScope ls("eigh_back_transform", s);
-        build_y_kernel<<<dim3(cdiv(n, 256), (unsigned)nb), 256, 0, s>>>(A, vhead, p, j0, nb,
-                                                                        rowstore, Y);
+        build_y_kernel<<<dim3(cdiv(n, 256), (unsigned)nb), 256, 0, s>>>(A, vhead, beta, p, j0,
+                                                                        nb, rowstore, Y);
         SHRK_CUDA(cudaGetLastError());
       }
       SHRK_TRY(dgemm(true, false, nb, nb, n, 1.0, Y, n, Y, n, 0.0, S, nb, s));

@@ -49,7 +49,14 @@ shrk_status rate(double* out, cudaStream_t s) {
 }
 
 // MUFU (XU pipe) reciprocal issue rate: eight independent chains of
-// rcp.approx.ftz.f32 per thread (x <-> 1/x, no denormals).
+// rcp.approx.ftz.f32 per thread (x <-> 1/x, no denormals).  The instruction
+// is volatile here so that none of the chain is folded away.
+__device__ __forceinline__ float rcp_issue(float a) {
+  float r;
+  asm volatile("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+  return r;
+}
+
 __global__ void __launch_bounds__(256) rcp_rate_kernel(int iters, float seed, float* sink) {
   float x[8];
 #pragma unroll
@@ -58,7 +65,7 @@ __global__ void __launch_bounds__(256) rcp_rate_kernel(int iters, float seed, fl
 #pragma unroll
     for (int r = 0; r < 16; ++r)
 #pragma unroll
-      for (int k = 0; k < 8; ++k) x[k] = rcp_f32(x[k]);
+      for (int k = 0; k < 8; ++k) x[k] = rcp_issue(x[k]);
   }
   float s = ((x[0] + x[1]) + (x[2] + x[3])) + ((x[4] + x[5]) + (x[6] + x[7]));
   if (s == -1.2345f) sink[0] = s;  // never true; keeps the chains live
@@ -125,8 +132,10 @@ shrk_status measure_rcp_rate(double* per_s) {
   SHRK_CUDA(cudaEventCreate(&e0));
   SHRK_CUDA(cudaEventCreate(&e1));
   rcp_rate_kernel<<<blocks, 256, 0, s>>>(32, 1.5f, (float*)sink);  // warm-up
+  SHRK_CUDA(cudaGetLastError());
   SHRK_CUDA(cudaEventRecord(e0, s));
   rcp_rate_kernel<<<blocks, 256, 0, s>>>(iters, 1.5f, (float*)sink);
+  SHRK_CUDA(cudaGetLastError());
   SHRK_CUDA(cudaEventRecord(e1, s));
   SHRK_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;
