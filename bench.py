@@ -320,12 +320,15 @@ def run_ours(args, world, rank, local):
             traffic = json.load(open(tpath)).get(kname.decode())
         mufu = None
         if prec == 1:  # one MUFU reciprocal per two far-field pairs
-            rr = C.c_double()
-            _native.check(L.shrk_measure_rcp_rate(C.byref(rr)))
-            mufu = {"achieved": 0.5 * p * p / k_avg_s / 1e12, "peak": rr.value / 1e12,
-                    "unit": "T rcp/s", "frac": 0.5 * p * p / k_avg_s / rr.value,
+            mhz = clk.get("sm_mhz")
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            rr = 16.0 * sms * mhz * 1e6 if mhz else None
+            mufu = {"achieved": 0.5 * p * p / k_avg_s / 1e12,
+                    "peak": rr / 1e12 if rr else None, "unit": "T rcp/s",
+                    "frac": 0.5 * p * p / k_avg_s / rr if rr else None,
                     "basis": "0.5 MUFU reciprocal per pair (the FP64 near field, ~1 % of the "
-                             "pairs here, counted as far) / measured rcp.approx.f32 rate"}
+                             "pairs here, counted as far) / nominal 16 reciprocals per clock "
+                             "per SM x SMs x the SM clock nvidia-smi reports"}
         roof = {"bound": "fp32" if prec == 1 else "fp64", "achieved": achieved / 1e12,
                 "peak": peak / 1e12, "unit": "Tops/s", "frac": achieved / peak,
                 "xu_pipe": mufu,

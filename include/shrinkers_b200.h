@@ -134,6 +134,23 @@ shrk_status shrk_stieltjes_at_points_dev(const double* d_q, size_t nq, const dou
                                          size_t p, double eta, int method, int precision,
                                          double cutoff_ratio, int parallelism, double* d_re,
                                          double* d_im, void* stream);
+/* A target shard of shrk_stieltjes_all_dev (all_points = 1) or of
+ * shrk_stieltjes_at_points_dev (all_points = 0), for a call split over
+ * several GPUs by targets with the spectrum replicated: the values at
+ * d_tgt[0..nt) computed with the policies of the whole call.  all_points:
+ * d_tgt points into d_ev (a slice of the spectrum), nq_total = p, outputs
+ * S/p.  At points: nq_total = the whole call's query count, which sets the
+ * treecode's grid leaf capacity (mod.rs:475-489) and the auto method's grid
+ * rule, so every shard uses the tree of the whole call; raw sums.  The
+ * treecode and grid methods evaluate each target independently of the
+ * others, so the shards assemble into the single call's values bit for bit;
+ * the exact methods' split reductions depend on the launch shape (1e-13).
+ * The "treecode" method's all-points form (the FMM) evaluates every point
+ * and keeps the slice. */
+shrk_status shrk_stieltjes_shard_dev(const double* d_tgt, size_t nt, size_t nq_total,
+                                     int all_points, const double* d_ev, size_t p, double eta,
+                                     int method, int precision, double cutoff_ratio,
+                                     int parallelism, double* d_re, double* d_im, void* stream);
 /* Allocation-free form of shrk_stieltjes_at_points_dev for the exact method
  * (no counterpart in the reference): the same RAW sums, FP64 or MIXED, with
  * every device temporary taken from one static array of
@@ -256,8 +273,10 @@ shrk_status shrk_stieltjes_fmm_dev(const double* d_ev, size_t p, double eta, int
  * m_override = forced grid size, 0 for the rule dx <= eta/8, m >= 8p, at
  * most 2^20; pad = max(pad_eta_mult*eta, pad_range_frac*raw_range) (defaults
  * 1000 and 0.75).  The first and last entries bound the grid, as in the
- * reference (ascending input expected).  SHRK_ENOTIMPL when the grid size is
- * not a power of two no larger than 2^22. */
+ * reference (ascending input expected).  Any grid size up to 2^21, or a power
+ * of two up to 2^22 (rustfft plans any length, fftplan.rs:21-28; here a size
+ * that is not a power of two runs Bluestein's chirp-z form over the
+ * power-of-two transform); SHRK_ENOTIMPL above that. */
 shrk_status shrk_stieltjes_fft5_with_options(const double* ev, size_t p, double eta, int order,
                                              size_t m_override, double pad_eta_mult,
                                              double pad_range_frac, double* raw_re,
@@ -266,6 +285,32 @@ shrk_status shrk_stieltjes_fft5_with_options_dev(const double* d_ev, size_t p, d
                                                  int order, size_t m_override,
                                                  double pad_eta_mult, double pad_range_frac,
                                                  double* d_re, double* d_im, void* stream);
+
+/* The NUFFT (nufft.rs:164-220) in its two stages, for a point-sharded
+ * transform over several GPUs (no reference counterpart: the reference runs
+ * in one process).  The splat is linear in the sources, so ranks that splat
+ * disjoint shards of one spectrum onto the same grid and sum their densities
+ * (one all-reduce of m <= 65 536 doubles) hold the density of the whole
+ * spectrum; each then evaluates its own queries.
+ *
+ * shrk_nufft_grid: the grid of nufft.rs:106-126 (with the padding of
+ * fft5.rs:339-361) for a spectrum whose first and last entries, in the
+ * caller's order, are first / last: m cells from lo, spacing dx (negative
+ * for descending input).  Host only.
+ * shrk_nufft_density_dev: the order-4 density of ns sources (any order;
+ * sorted on the device when needed) on the grid (m, lo, dx) into
+ * d_density[m]; ns = 0 gives zeros.
+ * shrk_nufft_eval_dev: the packed convolution of d_density with the kernel
+ * pair, and RAW sums at nq device queries.
+ * Splatting every source of a spectrum and evaluating gives the same values,
+ * bit for bit, as shrk_stieltjes_at_points_dev with the nufft method. */
+shrk_status shrk_nufft_grid(double first, double last, double eta, int64_t* m, double* lo,
+                            double* dx);
+shrk_status shrk_nufft_density_dev(const double* d_src, size_t ns, int64_t m, double lo,
+                                   double dx, double* d_density, void* stream);
+shrk_status shrk_nufft_eval_dev(const double* d_density, int64_t m, double lo, double dx,
+                                double eta, const double* d_q, size_t nq, double* d_re,
+                                double* d_im, void* stream);
 
 /* --------------------------------------------------- matrix front-end -- */
 /* Matrices are row-major p x p (p <= 46340), eigenvectors are their

@@ -36,10 +36,6 @@ shrk_status shrk_measure_pipe_rates(double* fp32_ops_per_s, double* fp64_ops_per
  * (log-uniform).  The mixed-precision pair kernel removes the log-uniform
  * mean from its FP32 far-field partials; this probe re-measures it. */
 shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean);
-/* Measured issue rate of the FP32 MUFU reciprocal (rcp.approx.ftz.f32) of
- * the current device, reciprocals per second: the denominator of the mixed
- * kernel's XU-pipe share (it issues one reciprocal per two far pairs). */
-shrk_status shrk_measure_rcp_rate(double* rcp_per_s);
 /* Budget, in GPU clock cycles, of every bulk-copy wait of the exact pair
  * kernels launched after this call (shrk_stieltjes_all / _at_points with an
  * exact method, their _dev forms, shrk_stieltjes_at_points_noalloc); returns

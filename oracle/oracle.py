@@ -94,6 +94,11 @@ def lib(path=None):
             "orc_nufft_points": (None, [_D, _SZ, _D, _SZ, C.c_double, C.c_int, _D, _D]),
             "orc_nufft_grid": (_SZ, [_D, _SZ, C.c_double, _D, _D, _D, _D]),
             "orc_fft": (None, [_D, _SZ, C.c_int]),
+            "orc_nufft_geometry": (None, [C.c_double, C.c_double, C.c_double, C.POINTER(_SZ),
+                                          _D, _D]),
+            "orc_grid_density": (None, [_D, _SZ, _SZ, C.c_double, C.c_double, C.c_int, _D]),
+            "orc_grid_eval": (None, [_D, _SZ, C.c_double, C.c_double, C.c_double, C.c_int, _D,
+                                     _SZ, _D, _D]),
             "orc_lagrange4": (None, [C.c_double, _D]),
             "orc_lagrange": (None, [C.c_int, C.c_double, _D]),
             "orc_fft5_grid_size": (_SZ, [C.c_double, C.c_double, _SZ, C.c_double, C.c_double, C.c_double]),
@@ -330,6 +335,32 @@ def nufft_grid(ev, eta):
                 dx=dx.value)
 
 
+def nufft_geometry(first, last, eta):
+    """nufft.rs:106-126: (m, lo, dx) of the grid of a spectrum whose first
+    and last entries are first / last."""
+    m, lo, dx = _SZ(), C.c_double(), C.c_double()
+    lib().orc_nufft_geometry(float(first), float(last), float(eta), C.byref(m), C.byref(lo),
+                             C.byref(dx))
+    return int(m.value), lo.value, dx.value
+
+
+def grid_density(ev, m, lo, dx, order=4):
+    """The sequential order-N splat of ev on the grid (m, lo, dx)."""
+    ev = _arr(ev)
+    out = np.empty(int(m))
+    lib().orc_grid_density(_d(ev), ev.size, int(m), float(lo), float(dx), int(order), _d(out))
+    return out
+
+
+def grid_eval(density, m, lo, dx, eta, q, order=4):
+    """Convolution of a grid density and interpolation at q: RAW sums."""
+    density, q = _arr(density), _arr(q)
+    re, im = np.empty_like(q), np.empty_like(q)
+    lib().orc_grid_eval(_d(density), int(m), float(lo), float(dx), float(eta), int(order), _d(q),
+                        q.size, _d(re), _d(im))
+    return re, im
+
+
 # ------------------------------------------------------------------- fft5 --
 def fft5_grid_size(ev, eta, pad_eta_mult=1000.0, pad_range_frac=0.75):
     ev = _arr(ev)
@@ -344,7 +375,7 @@ def fft5_points(q, ev, eta, order=8, m=None, pad_eta_mult=1000.0, pad_range_frac
     st = lib().orc_fft5_points(_d(q), q.size, _d(ev), ev.size, eta, int(order), int(m or 0),
                                pad_eta_mult, pad_range_frac, _d(re), _d(im))
     if st:
-        raise ValueError("fft5 oracle: the grid size must be a power of two")
+        raise ValueError(f"fft5 oracle: status {st}")
     return re, im
 
 

@@ -120,6 +120,36 @@ void fft_radix2(cplx* a, size_t m, int sign) {
   }
 }
 
+// Any-length DFT for grids that are not a power of two (rustfft plans any
+// length, fftplan.rs:21-28): the direct sum, one output per iteration, with
+// the twiddle index n k reduced modulo m exactly in integers so that every
+// factor is a correctly rounded cos/sin of 2 pi j/m.  Every output is one
+// sequential sum, so the threads do not change the result.  O(m^2): the
+// grids the tests force this way are at most a few 10^4 points.
+void dft_any(cplx* a, size_t m, int sign) {
+  if ((m & (m - 1)) == 0) {
+    fft_radix2(a, m, sign);
+    return;
+  }
+  std::vector<cplx> tw(m), out(m);
+  for (size_t j = 0; j < m; ++j) {
+    const double ang = 2.0 * M_PI * (double)j / (double)m;
+    tw[j] = cplx(std::cos(ang), sign * std::sin(ang));
+  }
+#pragma omp parallel for schedule(static)
+  for (long long k = 0; k < (long long)m; ++k) {
+    cplx acc(0.0, 0.0);
+    size_t idx = 0;
+    for (size_t n = 0; n < m; ++n) {
+      acc += a[n] * tw[idx];
+      idx += (size_t)k;
+      if (idx >= m) idx -= m;
+    }
+    out[(size_t)k] = acc;
+  }
+  std::copy(out.begin(), out.end(), a);
+}
+
 struct Grid { std::vector<cplx> out; double lo, dx; size_t m; };
 
 // fft5.rs:213-249 Fft5Options.
@@ -148,9 +178,12 @@ size_t fft5_grid_size(double lo_raw, double hi_raw, size_t p, double eta, double
   return std::max(next_pow2(min_grid), (size_t)2);
 }
 
+static void convolve_density(const double* density, size_t m, double lo, double dx, double eta,
+                             Grid& G);
+
 // fft5.rs:325-432 fft_convolution: grid (lo, dx, m) from the first/last
 // entries, order-N splat, packed forward FFT, analytic even kernel, packed
-// product, inverse FFT.  m must be a power of two (the radix-2 restatement).
+// product, inverse FFT (radix-2 for powers of two, the direct DFT otherwise).
 static void convolution(const double* ev, size_t p, double eta, const Opts& o, size_t m,
                         bool parallel, Grid& G) {
   double lo_raw = ev[0], hi_raw = ev[p - 1];
@@ -159,7 +192,6 @@ static void convolution(const double* ev, size_t p, double eta, const Opts& o, s
   double lo = lo_raw - pad, hi = hi_raw + pad;
   double range = hi - lo;
   double dx = range / (double)m;
-  size_t half = m / 2;
 
   std::vector<double> density(m, 0.0);
   if (parallel && p >= 4096) {  // fft5.rs:259-292 per-worker buffers + reduce
@@ -178,6 +210,14 @@ static void convolution(const double* ev, size_t p, double eta, const Opts& o, s
     splat_chunk(ev, 0, p, density.data(), m, lo, dx, o.order);
   }
 
+  convolve_density(density.data(), m, lo, dx, eta, G);
+}
+
+// fft5.rs:364-432: the density packed with the odd kernel, forward FFT,
+// analytic even kernel, packed product, inverse FFT, on the grid (m, lo, dx).
+static void convolve_density(const double* density, size_t m, double lo, double dx, double eta,
+                             Grid& G) {
+  const size_t half = m / 2;
   std::vector<cplx> packed(m);
   const double mf = (double)m;
   for (size_t i = 0; i < m; ++i) {
@@ -186,7 +226,7 @@ static void convolution(const double* ev, size_t p, double eta, const Opts& o, s
     double denom = x * x + eta * eta;
     packed[i] = cplx(density[i], x / denom);
   }
-  fft_radix2(packed.data(), m, -1);
+  dft_any(packed.data(), m, -1);
   // fftplan.rs:43-54 unpack_packed_real_pair
   std::vector<cplx> D(m), K(m);
   for (size_t k = 0; k < m; ++k) {
@@ -212,7 +252,7 @@ static void convolution(const double* ev, size_t p, double eta, const Opts& o, s
     cplx rh = d * K[k];
     G.out[k] = cplx(ih_re - rh.imag(), ih_im + rh.real());
   }
-  fft_radix2(G.out.data(), m, +1);
+  dft_any(G.out.data(), m, +1);
   G.lo = lo;
   G.dx = dx;
   G.m = m;
@@ -264,8 +304,8 @@ void nufft_points(const double* q, size_t nq, const double* ev, size_t p, double
 }
 
 // fft5.rs:559-625 compute_all_stieltjes_fft5_with_options /
-// compute_stieltjes_fft_at_points (raw sums, sequential).  Returns 0, or 4
-// when the grid size is not a power of two.
+// compute_stieltjes_fft_at_points (raw sums, sequential splat and
+// interpolation).  Returns 0.
 int fft5_points(const double* q, size_t nq, const double* ev, size_t p, double eta, int order,
                 size_t m_override, double pad_eta_mult, double pad_range_frac, double* re,
                 double* im) {
@@ -274,7 +314,6 @@ int fft5_points(const double* q, size_t nq, const double* ev, size_t p, double e
   const size_t m = m_override ? std::max(m_override, (size_t)2)
                               : fft5_grid_size(ev[0], ev[p - 1], p, eta, pad_eta_mult,
                                                pad_range_frac);
-  if ((m & (m - 1)) != 0) return 4;
   Grid G;
   convolution(ev, p, eta, o, m, false, G);
   interpolate(G, q, nq, order, false, re, im);
@@ -316,8 +355,35 @@ size_t orc_nufft_grid(const double* ev, size_t p, double eta, double* density_ou
   return G.m;
 }
 
+// The NUFFT grid of a spectrum with first/last entries first/last
+// (nufft.rs:106-126 with the padding of fft5.rs:339-361).
+void orc_nufft_geometry(double first, double last, double eta, size_t* m, double* lo,
+                        double* dx) {
+  const double raw_range = last - first;
+  *m = std::max(nufft_grid_size(raw_range, eta), (size_t)2);
+  const double pad = std::max(PAD_ETA_MULT * eta, PAD_RANGE_FRAC * raw_range);
+  *lo = first - pad;
+  *dx = ((last + pad) - *lo) / (double)*m;
+}
+
+// The two stages of the grid convolution apart, on a given grid: the
+// sequential order-N splat of p sources (fft5.rs:295-318), and the
+// convolution of a density plus interpolation at nq points (raw sums).
+void orc_grid_density(const double* ev, size_t p, size_t m, double lo, double dx, int order,
+                      double* density) {
+  std::fill(density, density + m, 0.0);
+  splat_chunk(ev, 0, p, density, m, lo, dx, order);
+}
+
+void orc_grid_eval(const double* density, size_t m, double lo, double dx, double eta, int order,
+                   const double* q, size_t nq, double* re, double* im) {
+  Grid G;
+  convolve_density(density, m, lo, dx, eta, G);
+  interpolate(G, q, nq, order, false, re, im);
+}
+
 void orc_fft(double* interleaved, size_t m, int sign) {
-  fft_radix2(reinterpret_cast<std::complex<double>*>(interleaved), m, sign);
+  dft_any(reinterpret_cast<std::complex<double>*>(interleaved), m, sign);
 }
 
 void orc_lagrange4(double t, double* w) { lagrange_weights<4>(t, w); }

@@ -445,7 +445,8 @@ def stieltjes_fft5_with_options(eigenvalues, eta, order="heptic", grid_size=None
     """compute_all_stieltjes_fft5_with_options (fft5.rs:568-590): RAW sums at
     every eigenvalue from the fft5 grid convolution, as {"real", "imag"}.
     order: "linear" / "cubic" / "quintic" / "heptic" (or 2/4/6/8 nodes);
-    grid_size: a forced power-of-two grid (None = dx <= eta/8, m >= 8p);
+    grid_size: a forced grid of any length up to 2^21, or a power of two up
+    to 2^22 (None = dx <= eta/8, m >= 8p);
     padding max(pad_eta_mult*eta, pad_range_frac*range).  The first and last
     entries bound the grid (ascending input expected, as in the reference)."""
     ev = _owned_f64_vec(eigenvalues, "eigenvalues")

@@ -59,6 +59,12 @@ SIGNATURES = {
     "shrk_stieltjes_fmm_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, C.c_int, _P, _P, _P]),
     "shrk_stieltjes_fft5_with_options": (_ST, [_D, _SZ, C.c_double, C.c_int, _SZ, C.c_double, C.c_double, _D, _D]),
     "shrk_stieltjes_fft5_with_options_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, _SZ, C.c_double, C.c_double, _P, _P, _P]),
+    "shrk_stieltjes_shard_dev": (_ST, [_P, _SZ, _SZ, C.c_int, _P, _SZ, C.c_double, C.c_int, C.c_int,
+                                       C.c_double, C.c_int, _P, _P, _P]),
+    "shrk_nufft_grid": (_ST, [C.c_double, C.c_double, C.c_double, _I64, _D, _D]),
+    "shrk_nufft_density_dev": (_ST, [_P, _SZ, C.c_int64, C.c_double, C.c_double, _P, _P]),
+    "shrk_nufft_eval_dev": (_ST, [_P, C.c_int64, C.c_double, C.c_double, C.c_double, _P, _SZ, _P,
+                                  _P, _P]),
     "shrk_inverse_nonlinear_shrinkage": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
     "shrk_symmetric_eigh": (_ST, [_D, _SZ, _D, _D]),
     "shrk_clean_eigensystem": (_ST, [_D, _D, _SZ, C.c_double, _D, _D, _D, _D, _D]),
@@ -83,7 +89,6 @@ SIGNATURES = {
     "shrk_measure_pipe_rates": (_ST, [_D, _D]),
     "shrk_measure_rcp_bias": (_ST, [_D, _D]),
     "shrk_diag_set_wait_limit": (C.c_longlong, [C.c_longlong]),
-    "shrk_measure_rcp_rate": (_ST, [_D]),
 }
 
 _lib = None

@@ -410,10 +410,15 @@ static bool is_fft5_family(int m) {
 // through `epi`.  The method must already be resolved.  all_points: the
 // targets are the sources (compute_all_stieltjes, mod.rs:601-790), else
 // arbitrary query points (compute_stieltjes_at_points, mod.rs:394-494).
+// A shard of a multi-GPU call passes the size of the whole call's query set
+// (nq_total, for the policies that depend on it) and, for all points, where
+// its targets start in the spectrum (tgt_offset).
 static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* d_src,
                                  int64_t ns, double eta, int method,
                                  int precision, double cutoff, const Epilogue& epi,
-                                 cudaStream_t s, bool all_points) {
+                                 cudaStream_t s, bool all_points, int64_t nq_total = -1,
+                                 int64_t tgt_offset = 0) {
+  if (nq_total < 0) nq_total = nt;
   const bool cut = !std::isnan(cutoff);
   // mod.rs:265-287: at query points, every grid method without a points
   // path of its own takes the exact per-point sum.
@@ -487,14 +492,15 @@ static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* 
     // theta 0.5, order 6, accuracy pinned at 1e-3, treecode.rs:357-393): the
     // dyadic Chebyshev FMM of fmm.cu, order 16, M2L on the tensor cores
     // (TF32 x3, ~1e-6 of |S|).  fmm_all writes S/p in the caller's order.
+    // A shard evaluates every point and keeps its slice.
     void* raw = nullptr;
-    SHRK_TRY(scratch_get(7, sizeof(double) * 2 * nt, &raw));
+    SHRK_TRY(scratch_get(7, sizeof(double) * 2 * ns, &raw));
     double* rre = (double*)raw;
-    double* rim = rre + nt;
+    double* rim = rre + ns;
     SHRK_TRY(fmm_all(d_src, ns, eta, 16, 1, rre, rim, s));
     Epilogue e2 = epi;
     e2.scale = epi.scale * (double)ns;  // the values are already S/p
-    return apply_epilogue(d_tgt, rre, rim, nt, e2, s);
+    return apply_epilogue(d_tgt, rre + tgt_offset, rim + tgt_offset, nt, e2, s);
   }
   if (method == SHRK_M_NUFFT || is_cheb(method)) {
     const double* ds = nullptr;
@@ -507,7 +513,7 @@ static shrk_status sums_dispatch(const double* d_tgt, int64_t nt, const double* 
       cheb_preset(method, &prm);
       // At arbitrary query points the leaf capacity is relaxed by the grid
       // rule (mod.rs:475-489).
-      if (!all_points) prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nt, prm.leaf_cap);
+      if (!all_points) prm.leaf_cap = (int)grid_leaf_cap(prm.n, ns, nq_total, prm.leaf_cap);
       SHRK_TRY(chebcode_points(d_tgt, nt, ds, ns, eta, prm, epi, s));
     }
     return SHRK_OK;
@@ -826,6 +832,41 @@ shrk_status shrk_stieltjes_all_dev(const double* d_ev, size_t p, double eta, int
   epi.out_im = d_im;
   return sums_dispatch(d_ev, (int64_t)p, d_ev, (int64_t)p, eta, m, precision, cutoff,
                        epi, s, true);
+}
+
+shrk_status shrk_stieltjes_shard_dev(const double* d_tgt, size_t nt, size_t nq_total,
+                                     int all_points, const double* d_ev, size_t p, double eta,
+                                     int method, int precision, double cutoff, int parallelism,
+                                     double* d_re, double* d_im, void* stream) {
+  SHRK_TRY(check_common(p, eta, method, precision));
+  SHRK_TRY(check_cutoff(cutoff));
+  if (nq_total < nt) {
+    set_error("shard: nq_total must be at least nt");
+    return SHRK_EINVAL;
+  }
+  int64_t offset = 0;
+  if (all_points) {
+    offset = (int64_t)(d_tgt - d_ev);
+    if (d_tgt < d_ev || offset > (int64_t)(p - nt) || nq_total != p) {
+      set_error("shard: all-points targets must be a slice of the spectrum, nq_total = p");
+      return SHRK_EINVAL;
+    }
+  }
+  if (nt == 0) return SHRK_OK;
+  Guard g(stream);
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;
+  const bool par = parallelism == SHRK_PAR_PARALLEL;
+  int m = method;
+  if (all_points) m = resolve(method, parallelism, p);
+  else if (is_auto(m)) m = shrk_grid_appropriate(shrk_resolve_auto_method(m, par, p), p, nq_total);
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = all_points ? 1.0 / (double)p : 1.0;
+  epi.out_re = d_re;
+  epi.out_im = d_im;
+  return sums_dispatch(d_tgt, (int64_t)nt, d_ev, (int64_t)p, eta, m, precision, cutoff, epi, s,
+                       all_points != 0, (int64_t)nq_total, offset);
 }
 
 shrk_status shrk_stieltjes_all(const double* ev, size_t p, double eta, int method, int precision,
@@ -1313,6 +1354,79 @@ shrk_status shrk_stieltjes_fft5_with_options(const double* ev, size_t p, double 
   return check_device_error(s);
 }
 
+// ------------------------------------------------ NUFFT stages apart --
+// The point-sharded NUFFT over several GPUs: every rank splats its shard of
+// the sources onto the common grid, the densities are summed (one all-reduce
+// of m <= 65 536 doubles), and every rank evaluates its shard of the queries.
+
+static shrk_status check_grid(int64_t m, double lo, double dx) {
+  if (m < 2 || m > (int64_t)1 << 22 || ((m & (m - 1)) != 0 && m > (int64_t)1 << 21)) {
+    set_error("grid: m must lie in [2, 2^22] (at most 2^21 when not a power of two)");
+    return SHRK_EINVAL;
+  }
+  if (!std::isfinite(lo) || !std::isfinite(dx) || dx == 0.0) {
+    set_error("grid: lo and dx must be finite and dx non-zero");
+    return SHRK_EINVAL;
+  }
+  return SHRK_OK;
+}
+
+shrk_status shrk_nufft_grid(double first, double last, double eta, int64_t* m, double* lo,
+                            double* dx) {
+  if (!std::isfinite(first) || !std::isfinite(last)) {
+    set_error("nufft_grid: first and last must be finite");
+    return SHRK_EINVAL;
+  }
+  if (!(std::isfinite(eta) && eta > 0.0)) {
+    set_error("eta must be a positive finite number");
+    return SHRK_EINVAL;
+  }
+  if (!m || !lo || !dx) {
+    set_error("nufft_grid: null output pointer");
+    return SHRK_EINVAL;
+  }
+  nufft_geometry(first, last, eta, m, lo, dx);
+  return SHRK_OK;
+}
+
+shrk_status shrk_nufft_density_dev(const double* d_src, size_t ns, int64_t m, double lo,
+                                   double dx, double* d_density, void* stream) {
+  SHRK_TRY(check_grid(m, lo, dx));
+  if (ns > (size_t)INT32_MAX) {
+    set_error("nufft_density: at most 2^31 - 1 sources per call");
+    return SHRK_EINVAL;
+  }
+  Guard g(stream);
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;
+  const double* ds = d_src;
+  if (ns > 0) {
+    double first = 0.0, last = 0.0;
+    SHRK_TRY(sorted_sources(d_src, (int64_t)ns, &ds, &first, &last, s));
+  }
+  return nufft_density(ds, (int64_t)ns, m, lo, dx, d_density, s);
+}
+
+shrk_status shrk_nufft_eval_dev(const double* d_density, int64_t m, double lo, double dx,
+                                double eta, const double* d_q, size_t nq, double* d_re,
+                                double* d_im, void* stream) {
+  SHRK_TRY(check_grid(m, lo, dx));
+  if (!(std::isfinite(eta) && eta > 0.0)) {
+    set_error("eta must be a positive finite number");
+    return SHRK_EINVAL;
+  }
+  if (nq == 0) return SHRK_OK;
+  Guard g(stream);
+  SHRK_TRY(g.st);
+  cudaStream_t s = (cudaStream_t)stream;
+  Epilogue epi;
+  epi.mode = EPI_SUMS;
+  epi.scale = 1.0;
+  epi.out_re = d_re;
+  epi.out_im = d_im;
+  return nufft_eval(d_density, m, lo, dx, eta, d_q, (int64_t)nq, epi, s);
+}
+
 // inverse.rs safe_reciprocal: 1/x, or the largest double for x <= 0 or
 // non-finite.
 static double safe_reciprocal(double x) {
@@ -1538,12 +1652,5 @@ shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean) {
 }
 
 long long shrk_diag_set_wait_limit(long long cycles) { return set_wait_cycles(cycles); }
-
-shrk_status shrk_measure_rcp_rate(double* rcp_per_s) {
-  Guard g;
-  SHRK_TRY(g.st);
-  if (!rcp_per_s) return einval("null output pointer");
-  return measure_rcp_rate(rcp_per_s);
-}
 
 }  // extern "C"

@@ -114,6 +114,7 @@ struct GridArgs {
   double lo, dx, eta;
   int64_t m;
   double2* packed;
+  double* dens;       // non-null: write the density alone (the splat stage)
 };
 
 template <int N>
@@ -248,6 +249,10 @@ __global__ void __launch_bounds__(256) long_runs_kernel(const GridArgs a,
 // sequential order).  The two edge cells also collect every clamped slot.
 // packed[c] = density[c] + i x_c/(x_c^2 + eta^2) (fft5.rs:364-376).
 __device__ __forceinline__ void pack_cell(const GridArgs& a, int64_t c, double dens) {
+  if (a.dens) {
+    a.dens[c] = dens;
+    return;
+  }
   const int64_t half = a.m / 2;
   const double sd = (c <= half) ? (double)c : (double)c - (double)a.m;
   const double x = sd * a.dx;
@@ -302,6 +307,13 @@ __global__ void __launch_bounds__(256) pack_kernel(const GridArgs a, const int* 
     }
   }
   pack_cell(a, c, dens);
+}
+
+// The evaluation stage's input: packed[c] from a given density (the sum of
+// the splat stages of several source sets).
+__global__ void pack_density_kernel(const GridArgs a, const double* __restrict__ density) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.m) pack_cell(a, c, density[c]);
 }
 
 // ---------------------------------------------------------------- FFT --
@@ -608,33 +620,132 @@ __global__ void even_kernel_spectrum(double* ke, int64_t m, double ke0, double r
   ke[k] = ke0 * pow(r, (double)kk);
 }
 
-// Constant tables, cached per call context for the last m and (m, dx, eta);
-// written and read on the context's stream.
+// Grids whose size m is not a power of two (a forced fft5 grid_size; the
+// reference plans any length through rustfft, fftplan.rs:21-28) take
+// Bluestein's chirp-z form over the power-of-two transform of length
+// M = next_pow2(2m - 1):  with c_j = e^{i pi j^2/m} and nk = (n^2 + k^2 -
+// (k - n)^2)/2,
+//   y_k = sum_n x_n e^{s 2 pi i nk/m} = c_k^s sum_n (x_n c_n^s) conj(c^s)_{k-n},
+// a circular convolution of length M with the chirp filter, which is
+// transformed once per m.  c^s is c for s = +1 and its conjugate for s = -1.
+
+// c_j = e^{i pi (j^2 mod 2m)/m}, j < m; j^2 is exact in 64-bit integers for
+// the m this path admits (m <= 2^21).
+__global__ void chirp_kernel(double2* c, int64_t m) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int64_t r = (j * j) % (2 * m);
+  double sn, cs;
+  sincospi((double)r / (double)m, &sn, &cs);
+  c[j] = make_double2(cs, sn);
+}
+
+// The forward transform's filter conj(c^{-1})_j = c_j on the circular index
+// range (-m, m) of length M, scaled by 1/M (a power of two: exact) so that
+// the unnormalised inverse transform of the product is the convolution.
+__global__ void chirp_filter_kernel(const double2* __restrict__ c, int64_t m, int64_t M,
+                                    double2* __restrict__ b) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= M) return;
+  const int64_t j = k < m ? k : (k > M - m ? M - k : -1);
+  const double inv = 1.0 / (double)M;
+  b[k] = j >= 0 ? make_double2(c[j].x * inv, c[j].y * inv) : make_double2(0.0, 0.0);
+}
+
+// a_n = x_n c^s_n for n < m, zero up to M.
+__global__ void chirp_in_kernel(const double2* __restrict__ x, const double2* __restrict__ c,
+                                int64_t m, int64_t M, double sign, double2* __restrict__ a) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= M) return;
+  a[k] = k < m ? cmul(x[k], make_double2(c[k].x, sign * c[k].y)) : make_double2(0.0, 0.0);
+}
+
+// a_k *= B_k for the forward transform; for the inverse the filter is the
+// conjugate chirp, whose transform is conj(B_{-k mod M}).
+__global__ void chirp_mul_kernel(double2* __restrict__ a, const double2* __restrict__ bhat,
+                                 int64_t M, int inverse) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= M) return;
+  double2 h = bhat[inverse ? (M - k) & (M - 1) : k];
+  if (inverse) h.y = -h.y;
+  a[k] = cmul(a[k], h);
+}
+
+// y_k = c^s_k a_k, k < m.
+__global__ void chirp_out_kernel(const double2* __restrict__ a, const double2* __restrict__ c,
+                                 int64_t m, double sign, double2* __restrict__ y) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  y[k] = cmul(a[k], make_double2(c[k].x, sign * c[k].y));
+}
+
+// Length of the power-of-two (or direct, below 64 points) transform that
+// serves a grid of m cells.
+int64_t transform_len(int64_t m) {
+  if (m < 64 || (m & (m - 1)) == 0) return m;
+  return (int64_t)next_pow2((size_t)(2 * m - 1));
+}
+
+// Constant tables, cached per call context for the last transform length,
+// m and (m, dx, eta); written and read on the context's stream.
 struct Tables {
-  double2* tw = nullptr;
+  double2* tw = nullptr;     // twiddles of the transform length
   int64_t tw_m = 0;
+  double2* chirp = nullptr;  // Bluestein: c_j (m) and the filter's transform (M)
+  double2* bhat = nullptr;
+  int64_t bs_m = 0, bs_cap = 0, bhat_cap = 0;
   double* ke = nullptr;
   int64_t ke_cap = 0;
   int64_t ke_m = 0;
   double ke_dx = 0.0, ke_eta = 0.0;
   ~Tables() {
     if (tw) cudaFree(tw);
+    if (chirp) cudaFree(chirp);
+    if (bhat) cudaFree(bhat);
     if (ke) cudaFree(ke);
   }
 };
 
 unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-shrk_status ensure_tables(int64_t m, double dx, double eta, cudaStream_t s, Tables** out) {
+shrk_status fft(double2* buf, double2* tmp, int64_t m, const double2* tw, double sign,
+                const char* family, cudaStream_t s);
+
+shrk_status ensure_tables(int64_t m, double dx, double eta, const char* family, cudaStream_t s,
+                          Tables** out) {
   Tables& T = ctx_state<Tables>(EXT_FFT_TABLES);
-  if (T.tw_m != m) {
+  const int64_t L = transform_len(m);
+  if (T.tw_m != L) {
     if (T.tw) SHRK_CUDA(cudaFree(T.tw));
     T.tw = nullptr;
     T.tw_m = 0;
-    SHRK_CUDA(cudaMalloc(&T.tw, sizeof(double2) * m));
-    twiddle_kernel<<<blocks_for(m, 256), 256, 0, s>>>(T.tw, m);
+    SHRK_CUDA(cudaMalloc(&T.tw, sizeof(double2) * L));
+    twiddle_kernel<<<blocks_for(L, 256), 256, 0, s>>>(T.tw, L);
     SHRK_CUDA(cudaGetLastError());
-    T.tw_m = m;
+    T.tw_m = L;
+  }
+  if (L != m && T.bs_m != m) {
+    T.bs_m = 0;
+    if (T.bs_cap < m) {
+      if (T.chirp) SHRK_CUDA(cudaFree(T.chirp));
+      T.chirp = nullptr;
+      T.bs_cap = 0;
+      SHRK_CUDA(cudaMalloc(&T.chirp, sizeof(double2) * m));
+      T.bs_cap = m;
+    }
+    if (T.bhat_cap < 2 * L) {  // the filter's transform and its scratch
+      if (T.bhat) SHRK_CUDA(cudaFree(T.bhat));
+      T.bhat = nullptr;
+      T.bhat_cap = 0;
+      SHRK_CUDA(cudaMalloc(&T.bhat, sizeof(double2) * 2 * L));
+      T.bhat_cap = 2 * L;
+    }
+    chirp_kernel<<<blocks_for(m, 256), 256, 0, s>>>(T.chirp, m);
+    SHRK_CUDA(cudaGetLastError());
+    chirp_filter_kernel<<<blocks_for(L, 256), 256, 0, s>>>(T.chirp, m, L, T.bhat);
+    SHRK_CUDA(cudaGetLastError());
+    SHRK_TRY(fft(T.bhat, T.bhat + L, L, T.tw, -1.0, family, s));
+    T.bs_m = m;
   }
   if (T.ke_m != m || T.ke_dx != dx || T.ke_eta != eta) {
     if (T.ke_cap < m) {
@@ -711,6 +822,33 @@ shrk_status fft(double2* buf, double2* tmp, int64_t m, const double2* tw, double
   return SHRK_OK;
 }
 
+// Unnormalised DFT of the m-cell grid in buf (sign -1 forward, +1 inverse):
+// the power-of-two transform in place, or Bluestein's form through the
+// M-point work buffers wa and wt.
+shrk_status dft(double2* buf, int64_t m, const Tables* T, double sign, double2* wa, double2* wt,
+                const char* family, cudaStream_t s) {
+  const int64_t M = transform_len(m);
+  if (M == m) return fft(buf, wt, m, T->tw, sign, family, s);
+  {
+    LaunchScope ls(family, s);
+    chirp_in_kernel<<<blocks_for(M, 256), 256, 0, s>>>(buf, T->chirp, m, M, sign, wa);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  SHRK_TRY(fft(wa, wt, M, T->tw, -1.0, family, s));
+  {
+    LaunchScope ls(family, s);
+    chirp_mul_kernel<<<blocks_for(M, 256), 256, 0, s>>>(wa, T->bhat, M, sign > 0.0 ? 1 : 0);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  SHRK_TRY(fft(wa, wt, M, T->tw, +1.0, family, s));
+  {
+    LaunchScope ls(family, s);
+    chirp_out_kernel<<<blocks_for(m, 256), 256, 0, s>>>(wa, T->chirp, m, sign, buf);
+    SHRK_CUDA(cudaGetLastError());
+  }
+  return SHRK_OK;
+}
+
 // One grid: stencil width, size, origin and spacing, and the launch families
 // its kernels are timed under.
 struct GridPlan {
@@ -724,16 +862,40 @@ struct GridPlan {
 };
 
 template <int N>
+shrk_status eval_grid(double2* A, double2* B, double2* Wa, double2* Wt, const Tables* T,
+                      const double* d_q, int64_t nq, const GridPlan& g, const Epilogue& epi,
+                      cudaStream_t s);
+
+// The whole grid convolution, or one of its two stages: with dens_out the
+// splat alone (the density of the sources into dens_out[m], nothing else);
+// with dens_in the evaluation alone from that density (no sources read).
+template <int N>
 shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t ns, double eta,
-                     const GridPlan& g, const Epilogue& epi, cudaStream_t s) {
+                     const GridPlan& g, const Epilogue& epi, cudaStream_t s,
+                     const double* dens_in, double* dens_out) {
   const int64_t m = g.m;
   Tables* T = nullptr;
-  SHRK_TRY(ensure_tables(m, g.dx, eta, s, &T));
+  if (!dens_out) SHRK_TRY(ensure_tables(m, g.dx, eta, g.fam_fft, s, &T));
+  // slot 11: A (packed grid) | B (product) | Wt | Wa, the last two of the
+  // transform length (Wa only for a Bluestein grid)
+  const int64_t L = transform_len(m);
   void* w = nullptr;
-  SHRK_TRY(scratch_get(11, sizeof(double2) * 3 * (size_t)m, &w));
+  SHRK_TRY(scratch_get(11, sizeof(double2) * (size_t)(2 * m + (L == m ? L : 2 * L)), &w));
   double2* A = (double2*)w;
   double2* B = A + m;
-  double2* Tmp = B + m;
+  double2* Wt = B + m;
+  double2* Wa = Wt + L;
+  GridArgs ga{d_src, ns, g.dx < 0.0 ? 1 : 0, g.lo, g.dx, eta, m, A, dens_out};
+  if (dens_in) {
+    LaunchScope ls(g.fam_splat, s);
+    pack_density_kernel<<<blocks_for(m, 256), 256, 0, s>>>(ga, dens_in);
+    SHRK_CUDA(cudaGetLastError());
+    return eval_grid<N>(A, B, Wa, Wt, T, d_q, nq, g, epi, s);
+  }
+  if (ns == 0) {  // no sources: a zero density
+    if (dens_out) SHRK_CUDA(cudaMemsetAsync(dens_out, 0, sizeof(double) * m, s));
+    return SHRK_OK;
+  }
   // slot 24: first [K + 1] | long-run list [K] + its length | run sums [K][N],
   // K = m + 2N + 2 keys from -N - 1
   const int64_t n_keys = m + 2 * N + 2;
@@ -744,7 +906,6 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   int* long_runs = first + n_keys + 1;
   int* n_long = long_runs + n_keys;
   double* runs = (double*)((char*)sw + first_bytes);
-  GridArgs ga{d_src, ns, g.dx < 0.0 ? 1 : 0, g.lo, g.dx, eta, m, A};
   SHRK_CUDA(cudaMemsetAsync(n_long, 0, sizeof(int), s));
   {
     LaunchScope ls(g.fam_splat, s);
@@ -762,13 +923,24 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
     pack_kernel<N><<<blocks_for(m, 256), 256, 0, s>>>(ga, first, runs);
     SHRK_CUDA(cudaGetLastError());
   }
-  SHRK_TRY(fft(A, Tmp, m, T->tw, -1.0, g.fam_fft, s));
+  if (dens_out) return SHRK_OK;
+  return eval_grid<N>(A, B, Wa, Wt, T, d_q, nq, g, epi, s);
+}
+
+// Forward transform of the packed grid A, spectral product into B, inverse
+// transform, interpolation at the queries with the epilogue.
+template <int N>
+shrk_status eval_grid(double2* A, double2* B, double2* Wa, double2* Wt, const Tables* T,
+                      const double* d_q, int64_t nq, const GridPlan& g, const Epilogue& epi,
+                      cudaStream_t s) {
+  const int64_t m = g.m;
+  SHRK_TRY(dft(A, m, T, -1.0, Wa, Wt, g.fam_fft, s));
   {
     LaunchScope ls(g.fam_spectral, s);
     spectral_kernel<<<blocks_for(m, 256), 256, 0, s>>>(A, T->ke, B, m);
     SHRK_CUDA(cudaGetLastError());
   }
-  SHRK_TRY(fft(B, Tmp, m, T->tw, +1.0, g.fam_fft, s));
+  SHRK_TRY(dft(B, m, T, +1.0, Wa, Wt, g.fam_fft, s));
   InterpArgs ia{d_q, nq, B, m, g.lo, g.dx, 1.0 / (double)m, epi};
   {
     LaunchScope ls(g.fam_interp, s);
@@ -779,12 +951,13 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
 }
 
 shrk_status run_grid_order(const double* d_q, int64_t nq, const double* d_src, int64_t ns,
-                           double eta, const GridPlan& g, const Epilogue& epi, cudaStream_t s) {
+                           double eta, const GridPlan& g, const Epilogue& epi, cudaStream_t s,
+                           const double* dens_in = nullptr, double* dens_out = nullptr) {
   switch (g.order) {
-    case 2: return run_grid<2>(d_q, nq, d_src, ns, eta, g, epi, s);
-    case 4: return run_grid<4>(d_q, nq, d_src, ns, eta, g, epi, s);
-    case 6: return run_grid<6>(d_q, nq, d_src, ns, eta, g, epi, s);
-    case 8: return run_grid<8>(d_q, nq, d_src, ns, eta, g, epi, s);
+    case 2: return run_grid<2>(d_q, nq, d_src, ns, eta, g, epi, s, dens_in, dens_out);
+    case 4: return run_grid<4>(d_q, nq, d_src, ns, eta, g, epi, s, dens_in, dens_out);
+    case 6: return run_grid<6>(d_q, nq, d_src, ns, eta, g, epi, s, dens_in, dens_out);
+    case 8: return run_grid<8>(d_q, nq, d_src, ns, eta, g, epi, s, dens_in, dens_out);
     default:
       set_error("fft5: the stencil order must be 2, 4, 6 or 8 nodes");
       return SHRK_EINVAL;
@@ -817,19 +990,44 @@ size_t fft5_grid_size(double lo_raw, double hi_raw, size_t p, double eta, double
   return std::max(next_pow2(min_grid), (size_t)2);
 }
 
+// fft5.rs:339-361 with the NUFFT options (m fixed by the policy).
+void nufft_geometry(double lo_raw, double hi_raw, double eta, int64_t* m, double* lo,
+                    double* dx) {
+  const double raw_range = hi_raw - lo_raw;
+  *m = (int64_t)std::max(nufft_grid_size(raw_range, eta), (size_t)2);
+  const double pad = std::max(NUFFT_PAD_ETA_MULT * eta, NUFFT_PAD_RANGE_FRAC * raw_range);
+  *lo = lo_raw - pad;
+  const double hi = hi_raw + pad;
+  *dx = (hi - *lo) / (double)*m;
+}
+
+namespace {
+GridPlan nufft_plan(int64_t m, double lo, double dx) {
+  return GridPlan{4, m, lo, dx, "nufft_splat", "nufft_fft", "nufft_spectral", "nufft_interp"};
+}
+}  // namespace
+
 shrk_status nufft_points(const double* d_q, int64_t nq, const double* d_src, int64_t ns,
                          double lo_raw, double hi_raw, double eta, const Epilogue& epi,
                          cudaStream_t s) {
   if (nq <= 0 || ns <= 0) return SHRK_OK;
-  // fft5.rs:339-361 with the NUFFT options (m fixed by the policy).
-  const double raw_range = hi_raw - lo_raw;
-  const int64_t m = (int64_t)std::max(nufft_grid_size(raw_range, eta), (size_t)2);
-  const double pad = std::max(NUFFT_PAD_ETA_MULT * eta, NUFFT_PAD_RANGE_FRAC * raw_range);
-  const double lo = lo_raw - pad, hi = hi_raw + pad;
-  const double range = hi - lo;
-  GridPlan g{4, m, lo, range / (double)m, "nufft_splat", "nufft_fft", "nufft_spectral",
-             "nufft_interp"};
-  return run_grid_order(d_q, nq, d_src, ns, eta, g, epi, s);
+  int64_t m = 0;
+  double lo = 0.0, dx = 0.0;
+  nufft_geometry(lo_raw, hi_raw, eta, &m, &lo, &dx);
+  return run_grid_order(d_q, nq, d_src, ns, eta, nufft_plan(m, lo, dx), epi, s);
+}
+
+shrk_status nufft_density(const double* d_sorted_src, int64_t ns, int64_t m, double lo, double dx,
+                          double* d_density, cudaStream_t s) {
+  return run_grid_order(nullptr, 0, d_sorted_src, ns, 0.0, nufft_plan(m, lo, dx), Epilogue{}, s,
+                        nullptr, d_density);
+}
+
+shrk_status nufft_eval(const double* d_density, int64_t m, double lo, double dx, double eta,
+                       const double* d_q, int64_t nq, const Epilogue& epi, cudaStream_t s) {
+  if (nq <= 0) return SHRK_OK;
+  return run_grid_order(d_q, nq, nullptr, 0, eta, nufft_plan(m, lo, dx), epi, s, d_density,
+                        nullptr);
 }
 
 shrk_status fft5_points(const double* d_q, int64_t nq, const double* d_src, int64_t ns,
@@ -839,9 +1037,9 @@ shrk_status fft5_points(const double* d_q, int64_t nq, const double* d_src, int6
   const size_t m = o.m_override ? std::max(o.m_override, (size_t)2)
                                 : fft5_grid_size(lo_raw, hi_raw, (size_t)ns, eta, o.pad_eta_mult,
                                                  o.pad_range_frac);
-  if ((m & (m - 1)) != 0 || m > (size_t)FFT_MAX_M) {
-    set_error("fft5: the grid size must be a power of two no larger than 2^22 (got " +
-              std::to_string(m) + ")");
+  if (m > (size_t)FFT_MAX_M || ((m & (m - 1)) != 0 && m > (size_t)FFT_MAX_M / 2)) {
+    set_error("fft5: the grid size must be at most 2^22, or 2^21 when it is not a power of "
+              "two (got " + std::to_string(m) + ")");
     return SHRK_ENOTIMPL;
   }
   const double raw_range = hi_raw - lo_raw;

@@ -91,6 +91,17 @@ shrk_status nufft_points(const double* d_q, int64_t nq, const double* d_sorted_s
                          double lo_raw, double hi_raw, double eta, const Epilogue& epi,
                          cudaStream_t s);
 size_t nufft_grid_size(double raw_range, double eta);
+// The NUFFT grid (m cells from lo, spacing dx) of a spectrum whose first and
+// last entries in the caller's order are lo_raw / hi_raw.
+void nufft_geometry(double lo_raw, double hi_raw, double eta, int64_t* m, double* lo,
+                    double* dx);
+// The NUFFT's two stages apart: the order-4 splat of ns ascending sources
+// into d_density[m] (linear in the sources), and the convolution of a
+// density with the kernel pair plus interpolation at nq queries.
+shrk_status nufft_density(const double* d_sorted_src, int64_t ns, int64_t m, double lo, double dx,
+                          double* d_density, cudaStream_t s);
+shrk_status nufft_eval(const double* d_density, int64_t m, double lo, double dx, double eta,
+                       const double* d_q, int64_t nq, const Epilogue& epi, cudaStream_t s);
 
 // fft5.rs:213-249 Fft5Options: stencil nodes (2/4/6/8), forced grid size
 // (0 = the adaptive rule dx <= eta/8, m >= 8p), padding multipliers.
@@ -101,7 +112,8 @@ struct Fft5Opts {
   double pad_range_frac = 0.75;
 };
 // fft5 grid convolution at nq points (same source contract as nufft_points);
-// SHRK_ENOTIMPL when the grid size is not a power of two <= 2^22.
+// SHRK_ENOTIMPL when the grid is larger than 2^22 cells (2^21 when the size
+// is not a power of two).
 shrk_status fft5_points(const double* d_q, int64_t nq, const double* d_sorted_src, int64_t ns,
                         double lo_raw, double hi_raw, double eta, const Fft5Opts& o,
                         const Epilogue& epi, cudaStream_t s);
@@ -177,7 +189,6 @@ double mixed_near_k();
 // = the default) and returns the previous one.
 long long set_wait_cycles(long long cycles);
 shrk_status measure_pipe_rates(double* fp32, double* fp64);
-shrk_status measure_rcp_rate(double* per_s);
 shrk_status measure_rcp_bias(double* uniform_mean, double* log_mean);
 
 }  // namespace shrk

@@ -48,29 +48,6 @@ shrk_status rate(double* out, cudaStream_t s) {
   return SHRK_OK;
 }
 
-// MUFU (XU pipe) reciprocal issue rate: eight independent chains of
-// rcp.approx.ftz.f32 per thread (x <-> 1/x, no denormals).  The instruction
-// is volatile here so that none of the chain is folded away.
-__device__ __forceinline__ float rcp_issue(float a) {
-  float r;
-  asm volatile("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
-  return r;
-}
-
-__global__ void __launch_bounds__(256) rcp_rate_kernel(int iters, float seed, float* sink) {
-  float x[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) x[k] = seed + 0.125f * (float)k + 1e-3f * (float)threadIdx.x;
-  for (int i = 0; i < iters; ++i) {
-#pragma unroll
-    for (int r = 0; r < 16; ++r)
-#pragma unroll
-      for (int k = 0; k < 8; ++k) x[k] = rcp_issue(x[k]);
-  }
-  float s = ((x[0] + x[1]) + (x[2] + x[3])) + ((x[4] + x[5]) + (x[6] + x[7]));
-  if (s == -1.2345f) sink[0] = s;  // never true; keeps the chains live
-}
-
 // Relative error of the MUFU reciprocal over every mantissa of [1, 2):
 // a = 1 + k 2^-23, rel = r a - 1 (the product of two floats is exact in
 // FP64).  Per block: the plain sum of rel, the sum of rel / a and the sum of
@@ -120,29 +97,6 @@ shrk_status measure_rcp_bias(double* uniform_mean, double* log_mean) {
   }
   *uniform_mean = su / (double)(1 << 23);
   *log_mean = sl / wl;
-  return SHRK_OK;
-}
-
-shrk_status measure_rcp_rate(double* per_s) {
-  cudaStream_t s = library_stream();
-  const int blocks = sm_count() * 8, iters = 2048;
-  void* sink = nullptr;
-  SHRK_TRY(scratch_get(15, 64, &sink));
-  cudaEvent_t e0, e1;
-  SHRK_CUDA(cudaEventCreate(&e0));
-  SHRK_CUDA(cudaEventCreate(&e1));
-  rcp_rate_kernel<<<blocks, 256, 0, s>>>(32, 1.5f, (float*)sink);  // warm-up
-  SHRK_CUDA(cudaGetLastError());
-  SHRK_CUDA(cudaEventRecord(e0, s));
-  rcp_rate_kernel<<<blocks, 256, 0, s>>>(iters, 1.5f, (float*)sink);
-  SHRK_CUDA(cudaGetLastError());
-  SHRK_CUDA(cudaEventRecord(e1, s));
-  SHRK_CUDA(cudaEventSynchronize(e1));
-  float ms = 0.f;
-  SHRK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  *per_s = (double)blocks * 256.0 * iters * 16.0 * 8.0 / (ms * 1e-3);
   return SHRK_OK;
 }
 

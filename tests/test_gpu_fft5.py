@@ -178,10 +178,38 @@ def test_forced_grid_sizes(oracle, m):
     assert close(re, im, o_re, o_im)
 
 
+@pytest.mark.parametrize("m", [3, 5, 63, 65, 100, 1000, 3000, 12345, 40000])
+def test_forced_grid_sizes_not_a_power_of_two(oracle, m):
+    """Any grid length, as rustfft plans it (fftplan.rs:21-28): the direct
+    DFT below 64 points, Bluestein's chirp-z form over the power-of-two
+    transform above (M = next_pow2(2m - 1)), against the oracle's direct
+    DFT.  Orders 4 and 8; 3 000 is the length the reference's docs force."""
+    ev = spectra.harness_spectrum(3000)
+    eta = 1.0 / math.sqrt(3000)
+    for order in (4, 8):
+        re, im = gpu_opts(ev, eta, order=order, m=m)
+        o_re, o_im = oracle.fft5_points(ev, ev, eta, order=order, m=m)
+        assert close(re, im, o_re, o_im), (m, order)
+
+
+def test_largest_bluestein_grid():
+    """m = 2^21 - 1, the largest grid that is not a power of two (M = 2^22):
+    the same sums as the neighbouring power-of-two grid to the resolution
+    change of one cell in 2^21, and finite everywhere."""
+    ev = spectra.harness_spectrum(3000)
+    eta = 1.0 / math.sqrt(3000)
+    a_re, a_im = gpu_opts(ev, eta, order=4, m=(1 << 21) - 1)
+    b_re, b_im = gpu_opts(ev, eta, order=4, m=1 << 21)
+    assert np.all(np.isfinite(a_re)) and np.all(np.isfinite(a_im))
+    assert close(a_re, a_im, b_re, b_im, tol=1e-5)
+
+
 def test_forced_grid_errors(rk):
     ev = spectra.log_spectrum(100)
-    with pytest.raises(NotImplementedError, match="power of two"):
-        rk.stieltjes_fft5_with_options(ev, 0.1, grid_size=3000)
+    with pytest.raises(NotImplementedError, match="2\\^21"):
+        rk.stieltjes_fft5_with_options(ev, 0.1, grid_size=(1 << 21) + 1)
+    with pytest.raises(NotImplementedError, match="2\\^22"):
+        rk.stieltjes_fft5_with_options(ev, 0.1, grid_size=1 << 23)
     with pytest.raises(ValueError, match="order"):
         rk.stieltjes_fft5_with_options(ev, 0.1, order="septic")
     a = rk.stieltjes_fft5_with_options(ev, 0.1, order="cubic", grid_size=16384)

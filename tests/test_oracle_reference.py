@@ -225,6 +225,17 @@ def test_fft_matches_dft(oracle):
     np.testing.assert_allclose(oracle.fft(x, +1), np.fft.ifft(x) * 256, rtol=0, atol=1e-11)
 
 
+@pytest.mark.parametrize("m", [3, 7, 100, 3000])
+def test_fft_any_length_matches_numpy(oracle, m):
+    """Lengths that are not a power of two (a forced fft5 grid_size; rustfft
+    plans any length): the oracle's direct DFT against numpy's FFT."""
+    rng = np.random.default_rng(m)
+    x = rng.standard_normal(m) + 1j * rng.standard_normal(m)
+    tol = 1e-14 * m
+    np.testing.assert_allclose(oracle.fft(x, -1), np.fft.fft(x), rtol=0, atol=tol)
+    np.testing.assert_allclose(oracle.fft(x, +1), np.fft.ifft(x) * m, rtol=0, atol=tol)
+
+
 def test_lagrange_partition_of_unity(oracle):
     """fft5.rs:774-804: every stencil width, t = s/97 for s in 0..97."""
     for t in np.linspace(0, 0.999, 17):
