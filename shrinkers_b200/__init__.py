@@ -48,7 +48,9 @@ def _lib():
 
 
 def _dp(a: np.ndarray):
-    return a.ctypes.data_as(_D)
+    """double* to a's data; the caller keeps `a` alive for the call (every
+    call site passes a named array)."""
+    return C.cast(a.ctypes.data, _D)
 
 
 # ------------------------------------------------------------ parsing --
@@ -108,8 +110,15 @@ def _require_finite(ev: np.ndarray, what: str) -> None:
 
 def _sanitize_positive(ev: np.ndarray, what: str = "eigenvalues") -> None:
     """python.rs:292-308: clamp round-off dust, reject meaningful negatives."""
-    _require_finite(ev, what)
-    scale = max(1.0, float(np.max(np.abs(ev)))) if ev.size else 1.0
+    if ev.size == 0:
+        return
+    # a finite sum means every entry is finite (a NaN or infinity makes it
+    # non-finite); only an overflowing sum needs the element-wise check
+    if not math.isfinite(float(ev.sum())):
+        _require_finite(ev, what)
+    if float(ev.min()) >= 0.0:
+        return
+    scale = max(1.0, float(np.max(np.abs(ev))))
     tol = 1e-10 * scale
     neg = np.nonzero(ev < 0.0)[0]
     for i in neg:
