@@ -202,7 +202,10 @@ void* ctx_ext(int k, void* (*make)(), void (*del)(void*)) {
 
 void set_source_hint(const double* d_src, const double* h_src, int64_t n) {
   Context* c = t_cur;
-  if (!c || n <= 0) return;
+  // Up to 16 384 values the host scan (~1 ns a value) costs less than the
+  // device check's launch and read-back; above, the device checks.
+  constexpr int64_t kHostScanMax = 16384;
+  if (!c || n <= 0 || n > kHostScanMax) return;
   bool sorted = true;
   double mn = h_src[0], mx = h_src[0];
   for (int64_t i = 1; i < n; ++i) {

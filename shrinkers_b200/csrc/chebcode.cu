@@ -153,10 +153,12 @@ __device__ __forceinline__ void tree_split_node_warp(const double* __restrict__ 
     b.bhi[slot + 1] = hi_idx;
     b.lc[i] = slot;
     b.rc[i] = slot + 1;
-    b.parent[slot] = b.parent[slot + 1] = i;
-    b.dep[slot] = b.dep[slot + 1] = depth + 1;
-    b.rturn[slot] = b.rturn[i];
-    b.rturn[slot + 1] = b.rturn[i] + 1;
+    if (b.parent) b.parent[slot] = b.parent[slot + 1] = i;  // absent in the one-CTA build
+    if (b.dep) {
+      b.dep[slot] = b.dep[slot + 1] = depth + 1;
+      b.rturn[slot] = b.rturn[i];
+      b.rturn[slot + 1] = b.rturn[i] + 1;
+    }
   }
 }
 
@@ -259,18 +261,23 @@ constexpr int TOPO_NT = 1024;
 // CTA beats two launches per level (a query-grid tree, a small spectrum).
 constexpr int64_t SMALL_TREE_LEAVES = 512;
 
-__global__ void __launch_bounds__(TOPO_NT, 1) tree_topology_cta_kernel(
-    const double* __restrict__ sorted, BuildArrays b, int64_t ns, int64_t leaf_cap, FlatTree f,
-    ChebConsts k, double theta_sq) {
+// The body, for a CTA of any size; parent, dep, rturn and arrive may be null
+// (the one-CTA build of tiny trees keeps its node arrays in shared memory and
+// needs none of them).  Returns the number of levels.
+__device__ int topology_cta(const double* __restrict__ sorted, BuildArrays b, int64_t ns,
+                            int64_t leaf_cap, FlatTree f, ChebConsts k, double theta_sq) {
   constexpr int NLEV = MAX_TREE_DEPTH + 2;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = TOPO_NT / 32;
+  const int nt = blockDim.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = nt / 32;
   if (tid == 0) {
     b.blo[0] = 0;
     b.bhi[0] = ns;
     b.pre[0] = 0;
-    b.parent[0] = -1;
-    b.dep[0] = 0;
-    b.rturn[0] = 0;
+    if (b.parent) b.parent[0] = -1;
+    if (b.dep) {
+      b.dep[0] = 0;
+      b.rturn[0] = 0;
+    }
     *b.counter = 1;
     b.levels[0] = 0;
     b.levels[1] = 1;
@@ -294,26 +301,35 @@ __global__ void __launch_bounds__(TOPO_NT, 1) tree_topology_cta_kernel(
   }
   for (int L = last - 1; L >= 0; --L) {
     const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
-    for (int i = begin + tid; i < end; i += TOPO_NT)
+    for (int i = begin + tid; i < end; i += nt)
       b.size[i] = b.lc[i] < 0 ? 1 : 1 + b.size[b.lc[i]] + b.size[b.rc[i]];
     __syncthreads();
   }
   for (int L = 0; L < last; ++L) {
     const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
-    for (int i = begin + tid; i < end; i += TOPO_NT) {
-      b.arrive[i] = 0;
-      if (L == 0) b.parent[i] = -1;
+    for (int i = begin + tid; i < end; i += nt) {
+      if (b.arrive) b.arrive[i] = 0;
+      if (b.parent && L == 0) b.parent[i] = -1;
       if (b.lc[i] >= 0) {
         b.pre[b.lc[i]] = b.pre[i] + 1;
         b.pre[b.rc[i]] = b.pre[i] + 1 + b.size[b.lc[i]];
-        b.parent[b.lc[i]] = i;
-        b.parent[b.rc[i]] = i;
+        if (b.parent) {
+          b.parent[b.lc[i]] = i;
+          b.parent[b.rc[i]] = i;
+        }
       }
     }
     __syncthreads();
   }
   const int nn = b.levels[2 * last - 1];
-  for (int i = tid; i < nn; i += TOPO_NT) tree_fill_node(sorted, b, i, f, k, theta_sq);
+  for (int i = tid; i < nn; i += nt) tree_fill_node(sorted, b, i, f, k, theta_sq);
+  return last;
+}
+
+__global__ void __launch_bounds__(TOPO_NT, 1) tree_topology_cta_kernel(
+    const double* __restrict__ sorted, BuildArrays b, int64_t ns, int64_t leaf_cap, FlatTree f,
+    ChebConsts k, double theta_sq) {
+  (void)topology_cta(sorted, b, ns, leaf_cap, f, k, theta_sq);
 }
 
 // Up to 32 barycentric rows at once, one warp: lane r computes row r's
@@ -333,6 +349,8 @@ struct RowTile {
   double q[32 * ROW_RS];
   double t[MAX_N];
   double lam[MAX_N];
+  double m[32];  // row r's scaled mass and exact-hit node (-2: no row)
+  int hit[32];
 };
 
 __device__ __forceinline__ void bary_rows_batch(double x, double mass, bool valid, int cnt, int n,
@@ -355,15 +373,30 @@ __device__ __forceinline__ void bary_rows_batch(double x, double mass, bool vali
       m = mass * (1.0 / sum);
     }
   }
+  rt.m[lane] = m;
+  rt.hit[lane] = hit;
   __syncwarp();
-  for (int r = 0; r < cnt; ++r) {
-    const int h = __shfl_sync(0xffffffffu, hit, r);
-    const double mr = __shfl_sync(0xffffffffu, m, r);
-    if (lane < n && h != -2) {
-      if (h >= 0) {
-        if (h == lane) w = w + mr;
-      } else {
-        w = fma(mr, rt.q[r * ROW_RS + lane], w);
+  // Rows in order, four at a time: their operands are loaded together (they
+  // do not depend on w), then applied one after the other.
+  for (int r0 = 0; r0 < cnt; r0 += 4) {
+    int hh[4];
+    double mm[4], qq[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = r0 + u;
+      const bool ok = r < cnt && lane < n;
+      hh[u] = ok ? rt.hit[r] : -2;
+      mm[u] = ok ? rt.m[r] : 0.0;
+      qq[u] = ok ? rt.q[r * ROW_RS + lane] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (hh[u] != -2) {
+        if (hh[u] >= 0) {
+          if (hh[u] == lane) w = w + mm[u];
+        } else {
+          w = fma(mm[u], qq[u], w);
+        }
       }
     }
   }
@@ -488,6 +521,90 @@ __global__ void __launch_bounds__(WEIGHT_NT, 1) tree_p2m_grid_kernel(
   }
 }
 
+// The whole build of a tiny tree (ns <= TINY_NS sources) in one CTA and one
+// launch: the spectrum and every node array of the topology in shared memory
+// (a tree over ns sources has at most 2 ns - 1 nodes), the flat arrays, the
+// P2M of the leaves, then the M2M level by level from the deepest with a
+// barrier between levels, and the f32 mirror.  The same device functions as
+// the multi-launch builds, node by node, so the same tree and the same
+// weights bit for bit; what goes is a launch, the per-level round trips to
+// global memory and the climbing warps' fences and arrival counters.
+constexpr int64_t TINY_NS = 2048;
+constexpr int TINY_NT = 1024;
+constexpr int TINY_TILES = 16;  // warps with a row tile (P2M / M2M)
+
+__device__ __forceinline__ unsigned dyn_smem_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+  return r;
+}
+
+__host__ __device__ size_t tiny_smem_bytes(int64_t ns) {
+  constexpr int NLEV = MAX_TREE_DEPTH + 2;
+  const size_t cap = (size_t)(2 * ns > 2 ? 2 * ns : 2);
+  return sizeof(RowTile) * TINY_TILES + sizeof(double) * (size_t)ns +
+         sizeof(int64_t) * 2 * cap + sizeof(int32_t) * (4 * cap + 8 + 2 * NLEV);
+}
+
+__global__ void __launch_bounds__(TINY_NT, 1) tree_tiny_kernel(
+    const double* __restrict__ sorted_g, int64_t ns, int64_t leaf_cap, FlatTree f, ChebConsts k,
+    double theta_sq, NodeF32* nf, float* panel, int* nn_out) {
+  extern __shared__ __align__(16) unsigned char tiny_sm[];
+  const int64_t cap = ns * 2 > 2 ? ns * 2 : 2;
+  RowTile* tiles = reinterpret_cast<RowTile*>(tiny_sm);
+  double* s_sorted = reinterpret_cast<double*>(tiles + TINY_TILES);
+  BuildArrays b;
+  b.blo = reinterpret_cast<int64_t*>(s_sorted + ns);
+  b.bhi = b.blo + cap;
+  b.lc = reinterpret_cast<int32_t*>(b.bhi + cap);
+  b.rc = b.lc + cap;
+  b.size = b.rc + cap;
+  b.pre = b.size + cap;
+  b.counter = b.pre + cap;
+  b.levels = b.counter + 8;
+  b.parent = b.arrive = b.dep = b.rturn = b.leafpre = nullptr;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int64_t i = tid; i < ns; i += blockDim.x) s_sorted[i] = sorted_g[i];
+  __syncthreads();
+  const int last = topology_cta(s_sorted, b, ns, leaf_cap, f, k, theta_sq);
+  __syncthreads();
+  const int nn = b.levels[2 * last - 1];
+  // The Chebyshev nodes and weights in the shared memory left over when the
+  // tree is small enough (typically: nn is far below its bound 2 ns - 1):
+  // the M2M chain, one level after another, then runs without an L2 round
+  // trip per level; the weights are copied out at the end.
+  const size_t used = tiny_smem_bytes(ns);
+  const size_t need = sizeof(double) * 2 * (size_t)nn * k.n;
+  FlatTree fw = f;
+  const bool in_smem = used + need <= (size_t)dyn_smem_size();
+  if (in_smem) {
+    double* sn = reinterpret_cast<double*>(tiny_sm + used);
+    for (int i = tid; i < nn * k.n; i += blockDim.x) sn[i] = f.nodes[i];
+    fw.nodes = sn;
+    fw.w = sn + (size_t)nn * k.n;
+    __syncthreads();
+  }
+  if (warp < TINY_TILES)
+    for (int i = warp; i < nn; i += TINY_TILES)
+      if (b.lc[i] < 0) p2m_leaf(s_sorted, nullptr, b, i, lane, fw, fw.w, k, tiles[warp]);
+  __syncthreads();
+  for (int L = last - 2; L >= 0; --L) {  // level last - 1 holds leaves only
+    const int begin = b.levels[2 * L], end = b.levels[2 * L + 1];
+    if (warp < TINY_TILES)
+      for (int i = begin + warp; i < end; i += TINY_TILES)
+        if (b.lc[i] >= 0) m2m_node(b, i, lane, fw, fw.w, k, !in_smem, tiles[warp]);
+    __syncthreads();
+  }
+  if (in_smem) {
+    for (int i = tid; i < nn * k.n; i += blockDim.x) f.w[i] = fw.w[i];
+    __syncthreads();
+  }
+  if (nf)
+    for (int idx = warp; idx < nn; idx += (int)(blockDim.x >> 5))
+      mirror_f32(f, idx, k.n, lane, nf, panel);
+  if (tid == 0) *nn_out = nn;
+}
+
 // M2M, one warp per internal node of a level: the left then the right
 // child's node masses, in node order.
 
@@ -519,7 +636,28 @@ struct EvalArgs {
   const float* panel;
   Epilogue epi;
   int* err;
+  // Node count (nn_dev on the device when the build kept it there, else
+  // nn_host) and the dynamic shared memory each CTA may fill with a copy of
+  // the tree's node records (0: read them from global memory).  A traversal
+  // is a chain of dependent node loads; from shared memory each costs tens
+  // of cycles instead of an L2 round trip.
+  const int* nn_dev;
+  int nn_host;
+  int stage_bytes;
 };
+
+// Staged node record of the FP64 traversal.
+struct NodeHdr64 {
+  double lo, hi, accept_hw;
+  int64_t lo_idx, hi_idx;
+  int32_t right, pad;
+};
+
+constexpr int CHEB_STAGE_BYTES = 48 * 1024;
+
+__device__ __forceinline__ int eval_node_count(const EvalArgs& a) {
+  return a.nn_dev ? *a.nn_dev : a.nn_host;
+}
 
 // Exact leaf sum, F64x2 schedule of chebcode.rs:620-649 (x86 semantics).
 __device__ __forceinline__ void leaf_sum(const double* xs, int64_t len, double x, double eta2,
@@ -566,18 +704,29 @@ __device__ __forceinline__ void leaf_sum_warp(const double* xs, int64_t len, dou
       vi = inv;
     }
     const int cnt = (int)min((int64_t)32, len - base);
-    for (int j = 0; j < cnt; ++j) {
-      const double r = __shfl_sync(0xffffffffu, vr, j), i = __shfl_sync(0xffffffffu, vi, j);
-      const int64_t kk = base + j;
-      if (kk >= pair_end) {
-        tr = r;
-        ti = i;
-      } else if (kk & 1) {
-        ar1 = ar1 + r;
-        ai1 = ai1 + i;
-      } else {
-        ar0 = ar0 + r;
-        ai0 = ai0 + i;
+    // four terms' shuffles issued together (they do not depend on the
+    // sums), then added one after the other in source order
+    for (int j0 = 0; j0 < cnt; j0 += 4) {
+      double rr[4], ii[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        rr[u] = __shfl_sync(0xffffffffu, vr, j0 + u);
+        ii[u] = __shfl_sync(0xffffffffu, vi, j0 + u);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (j0 + u >= cnt) break;
+        const int64_t kk = base + j0 + u;
+        if (kk >= pair_end) {
+          tr = rr[u];
+          ti = ii[u];
+        } else if (kk & 1) {
+          ar1 = ar1 + rr[u];
+          ai1 = ai1 + ii[u];
+        } else {
+          ar0 = ar0 + rr[u];
+          ai0 = ai0 + ii[u];
+        }
       }
     }
   }
@@ -594,12 +743,37 @@ __device__ __forceinline__ void leaf_sum_warp(const double* xs, int64_t len, dou
 // walk the same nodes; leaf sums by leaf_sum_warp; lane 0 stores).
 template <bool WARP>
 __global__ void __launch_bounds__(128) cheb_eval_f64(const EvalArgs a) {
+  extern __shared__ __align__(16) unsigned char stage_raw[];
   const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t t = WARP ? gt >> 5 : gt;
   const int lane = WARP ? (int)(threadIdx.x & 31) : 0;
-  if (t >= a.nq) return;  // WARP: whole warps leave together
   const DevTreeF64& T = a.t;
   const int n = T.n;
+  // Node records in shared memory when they fit (the same values, so the
+  // same arithmetic); the node count is uniform, so is the branch.
+  const NodeHdr64* sh = nullptr;
+  const double* s_nodes = nullptr;
+  if (a.stage_bytes > 0) {
+    const int nn = eval_node_count(a);
+    const size_t hb = (size_t)nn * sizeof(NodeHdr64), pb = (size_t)nn * 2 * n * sizeof(double);
+    if (hb <= (size_t)a.stage_bytes) {
+      NodeHdr64* h = reinterpret_cast<NodeHdr64*>(stage_raw);
+      for (int i = threadIdx.x; i < nn; i += blockDim.x)
+        h[i] = NodeHdr64{T.lo[i], T.hi[i], T.accept_hw[i], T.lo_idx[i], T.hi_idx[i], T.right[i], 0};
+      sh = h;
+      if (hb + pb <= (size_t)a.stage_bytes) {
+        double* d = reinterpret_cast<double*>(stage_raw + hb);
+        for (int i = threadIdx.x; i < nn * n; i += blockDim.x) {
+          d[i] = T.nodes[i];
+          d[nn * n + i] = T.w[i];
+        }
+        s_nodes = d;
+      }
+    }
+    __syncthreads();
+  }
+  if (t >= a.nq) return;  // WARP: whole warps leave together
+  const int nn_s = s_nodes ? eval_node_count(a) : 0;
   const double x = a.q[t], eta = a.eta, eta2 = eta * eta;
   int32_t stack[MAX_TREE_DEPTH + 2];
   int top = 0;
@@ -607,22 +781,23 @@ __global__ void __launch_bounds__(128) cheb_eval_f64(const EvalArgs a) {
   double re = 0.0, im = 0.0;
   while (top > 0) {
     const int32_t node = stack[--top];
-    const int32_t rt = T.right[node];
+    const int32_t rt = sh ? sh[node].right : T.right[node];
     if (rt < 0) {
       double lr, li;
-      const int64_t l0 = T.lo_idx[node];
-      if (WARP) leaf_sum_warp(a.sorted + l0, T.hi_idx[node] - l0, x, eta2, lane, lr, li);
-      else leaf_sum(a.sorted + l0, T.hi_idx[node] - l0, x, eta2, lr, li);
+      const int64_t l0 = sh ? sh[node].lo_idx : T.lo_idx[node];
+      const int64_t l1 = sh ? sh[node].hi_idx : T.hi_idx[node];
+      if (WARP) leaf_sum_warp(a.sorted + l0, l1 - l0, x, eta2, lane, lr, li);
+      else leaf_sum(a.sorted + l0, l1 - l0, x, eta2, lr, li);
       re += lr;
       im += eta * li;
       continue;
     }
-    const double lo = T.lo[node], hi = T.hi[node];
+    const double lo = sh ? sh[node].lo : T.lo[node], hi = sh ? sh[node].hi : T.hi[node];
     const double cl = fmax(fmax(lo - x, x - hi), 0.0);
     const double d_sq = fma(cl, cl, eta2);
-    if (T.accept_hw[node] < d_sq) {
-      const double* ts = T.nodes + (int64_t)node * n;
-      const double* ws = T.w + (int64_t)node * n;
+    if ((sh ? sh[node].accept_hw : T.accept_hw[node]) < d_sq) {
+      const double* ts = (s_nodes ? s_nodes : T.nodes) + (int64_t)node * n;
+      const double* ws = (s_nodes ? s_nodes + (int64_t)nn_s * n : T.w) + (int64_t)node * n;
       double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
       int j = 0;
       for (; j + 2 <= n; j += 2) {
@@ -658,11 +833,30 @@ __global__ void __launch_bounds__(128) cheb_eval_f64(const EvalArgs a) {
 // chebcode.rs:722-828 contribution_fast32.  WARP as cheb_eval_f64.
 template <bool WARP>
 __global__ void __launch_bounds__(128) cheb_eval_f32(const EvalArgs a) {
+  extern __shared__ __align__(16) unsigned char stage_raw[];
   const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t t = WARP ? gt >> 5 : gt;
   const int lane = WARP ? (int)(threadIdx.x & 31) : 0;
-  if (t >= a.nq) return;  // WARP: whole warps leave together
   const int n = a.t.n;
+  // Node records and panel in shared memory when they fit (see cheb_eval_f64).
+  const NodeF32* nfp = a.nf;
+  const float* panel = a.panel;
+  if (a.stage_bytes > 0) {
+    const int nn = eval_node_count(a);
+    const size_t hb = (size_t)nn * sizeof(NodeF32), pb = (size_t)nn * 2 * n * sizeof(float);
+    if (hb <= (size_t)a.stage_bytes) {
+      NodeF32* h = reinterpret_cast<NodeF32*>(stage_raw);
+      for (int i = threadIdx.x; i < nn; i += blockDim.x) h[i] = a.nf[i];
+      nfp = h;
+      if (hb + pb <= (size_t)a.stage_bytes) {
+        float* d = reinterpret_cast<float*>(stage_raw + hb);
+        for (int i = threadIdx.x; i < nn * 2 * n; i += blockDim.x) d[i] = a.panel[i];
+        panel = d;
+      }
+    }
+    __syncthreads();
+  }
+  if (t >= a.nq) return;  // WARP: whole warps leave together
   const double lambda = a.q[t], eta = a.eta, eta2d = eta * eta;
   const float x = (float)lambda, e32 = (float)eta, eta2 = e32 * e32;
   float fre[4] = {0.f, 0.f, 0.f, 0.f}, fim[4] = {0.f, 0.f, 0.f, 0.f};
@@ -672,7 +866,7 @@ __global__ void __launch_bounds__(128) cheb_eval_f32(const EvalArgs a) {
   stack[top++] = 0;
   while (top > 0) {
     const int32_t node = stack[--top];
-    const NodeF32 nd = a.nf[node];
+    const NodeF32 nd = nfp[node];
     if (nd.right < 0) {
       double lr, li;
       if (WARP)
@@ -688,7 +882,7 @@ __global__ void __launch_bounds__(128) cheb_eval_f32(const EvalArgs a) {
     const float d_sq = fmaf(cl, cl, eta2);
     const float outside = (cl == 0.0f) ? d_sq : OUTSIDE_THETA2 * d_sq;
     if (nd.accept_hw < outside) {
-      const float* ts = a.panel + (int64_t)node * 2 * n;
+      const float* ts = panel + (int64_t)node * 2 * n;
       const float* ws = ts + n;
       int j = 0;
       for (; j + 4 <= n; j += 4) {
@@ -1161,7 +1355,8 @@ static bool fused_build_ok(int64_t ns, const ChebParams& prm) {
 }
 
 static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const ChebParams& prm,
-                                    FlatTree& f, NodeF32** nf, float** panel, cudaStream_t s) {
+                                    FlatTree& f, NodeF32** nf, float** panel, const int** d_nn,
+                                    cudaStream_t s) {
   const int64_t cap = std::max<int64_t>(2 * ns, 2);
   const int n = prm.n;
   ChebConsts k;
@@ -1212,18 +1407,45 @@ static shrk_status build_tree_fused(const double* d_sorted, int64_t ns, const Ch
     SHRK_TRY(scratch_get(TREE_SLOTS + 5, sizeof(float) * 2 * (size_t)cap * n, &q));
     mpanel = (float*)q;
   }
-  {
+  if (ns <= TINY_NS && prm.leaf_cap >= 1) {
+    // all the shared memory a CTA may have: what the arrays leave over holds
+    // the nodes and weights of a small enough tree
+    static std::atomic<int> optin[64];
+    int dev = 0;
+    SHRK_CUDA(cudaGetDevice(&dev));
+    int smem = dev >= 0 && dev < 64 ? optin[dev].load() : 0;
+    if (smem == 0) {
+      SHRK_CUDA(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+      SHRK_CUDA(cudaFuncSetAttribute(tree_tiny_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     smem));
+      if (dev >= 0 && dev < 64) optin[dev] = smem;
+    }
+    if ((size_t)smem < tiny_smem_bytes(ns)) {
+      set_error("chebcode: the device has too little shared memory per block");
+      return SHRK_ECUDA;
+    }
     LaunchScope ls("cheb_build", s);
-    tree_topology_cta_kernel<<<1, TOPO_NT, 0, s>>>(d_sorted, b, ns, (int64_t)prm.leaf_cap, f, k,
-                                                   prm.theta * prm.theta);
+    tree_tiny_kernel<<<1, TINY_NT, (size_t)smem, s>>>(
+        d_sorted, ns, (int64_t)prm.leaf_cap, f, k, prm.theta * prm.theta, mirror, mpanel,
+        b.counter);
     SHRK_CUDA(cudaGetLastError());
-    tree_p2m_grid_kernel<<<sm_count() * 4, WEIGHT_NT, 0, s>>>(d_sorted, b, f, f.w, k, mirror,
-                                                              mpanel);
-    SHRK_CUDA(cudaGetLastError());
-    add_launches(1);
+  } else {
+    {
+      LaunchScope ls("cheb_build", s);
+      tree_topology_cta_kernel<<<1, TOPO_NT, 0, s>>>(d_sorted, b, ns, (int64_t)prm.leaf_cap, f,
+                                                     k, prm.theta * prm.theta);
+      SHRK_CUDA(cudaGetLastError());
+    }
+    {
+      LaunchScope ls("cheb_build_weights", s);
+      tree_p2m_grid_kernel<<<sm_count() * 4, WEIGHT_NT, 0, s>>>(d_sorted, b, f, f.w, k, mirror,
+                                                                mpanel);
+      SHRK_CUDA(cudaGetLastError());
+    }
   }
   *nf = mirror;
   *panel = mpanel;
+  *d_nn = b.counter;  // the node count, left on the device by the build
   return SHRK_OK;
 }
 
@@ -1238,8 +1460,10 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
   TreeBuild tb;
   NodeF32* fused_nf = nullptr;
   float* fused_panel = nullptr;
+  const int* d_nn = nullptr;
   const bool fused = fused_build_ok(ns, prm);
-  if (fused) SHRK_TRY(build_tree_fused(d_sorted_src, ns, prm, tb.f, &fused_nf, &fused_panel, s));
+  if (fused)
+    SHRK_TRY(build_tree_fused(d_sorted_src, ns, prm, tb.f, &fused_nf, &fused_panel, &d_nn, s));
   else SHRK_TRY(build_tree_gpu(d_sorted_src, ns, prm, tb, s));
   const FlatTree& f = tb.f;
   const int nn = tb.nn;
@@ -1253,6 +1477,15 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
   a.t.n = prm.n;
   a.nf = nullptr;
   a.panel = nullptr;
+  a.nn_dev = d_nn;
+  a.nn_host = nn;
+  // A warp (or a thread) per query, 128 threads per CTA; the CTAs copy the
+  // tree's node records into shared memory when there are few enough CTAs
+  // that the copies cost less than the L2 round trips they save.
+  const bool warp = nq <= CHEB_WARP_NQ;
+  const unsigned ctas = (unsigned)(((warp ? nq * 32 : nq) + 127) / 128);
+  a.stage_bytes = ctas <= (unsigned)(8 * sm_count()) ? CHEB_STAGE_BYTES : 0;
+  const size_t smem = (size_t)a.stage_bytes;
   if (!prm.f32) {
     a.t.lo = f.lo;
     a.t.hi = f.hi;
@@ -1263,8 +1496,8 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     a.t.nodes = f.nodes;
     a.t.w = f.w;
     LaunchScope ls("cheb_eval_f64", s);
-    if (nq <= CHEB_WARP_NQ) cheb_eval_f64<true><<<(unsigned)((nq * 32 + 127) / 128), 128, 0, s>>>(a);
-    else cheb_eval_f64<false><<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
+    if (warp) cheb_eval_f64<true><<<ctas, 128, smem, s>>>(a);
+    else cheb_eval_f64<false><<<ctas, 128, smem, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   } else {
     NodeF32* nf = fused_nf;
@@ -1282,8 +1515,8 @@ shrk_status chebcode_points(const double* d_q, int64_t nq, const double* d_sorte
     a.nf = nf;
     a.panel = panel;
     LaunchScope ls("cheb_eval_f32", s);
-    if (nq <= CHEB_WARP_NQ) cheb_eval_f32<true><<<(unsigned)((nq * 32 + 127) / 128), 128, 0, s>>>(a);
-    else cheb_eval_f32<false><<<(unsigned)((nq + 127) / 128), 128, 0, s>>>(a);
+    if (warp) cheb_eval_f32<true><<<ctas, 128, smem, s>>>(a);
+    else cheb_eval_f32<false><<<ctas, 128, smem, s>>>(a);
     SHRK_CUDA(cudaGetLastError());
   }
   return SHRK_OK;
