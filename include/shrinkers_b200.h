@@ -359,6 +359,25 @@ shrk_status shrk_estimate_precision_matrix(const double* matrix, size_t p, doubl
                                            double* precision, double* eigenvectors,
                                            double* precision_ev, double* covariance_ev,
                                            double* smoothing);
+/* Device-pointer forms of shrk_symmetric_eigh, shrk_clean_covariance_matrix
+ * and shrk_estimate_precision_matrix: the matrix and every array output on
+ * the device (the p x p outputs, and the p-vectors: eigenvalues, RIE
+ * eigenvalues, overlaps, precision_ev, covariance_ev; "may be NULL" as in
+ * the host forms), the scalar outputs (sigma2, smoothing) on the host.  The
+ * calls wait for the work queued on `stream` before reading the matrix, and
+ * `stream` waits for their outputs; they synchronise internally (the steps
+ * between the kernels are host arithmetic on the spectrum). */
+shrk_status shrk_symmetric_eigh_dev(const double* d_matrix, size_t p, double* d_eigenvalues,
+                                    double* d_eigenvectors, void* stream);
+shrk_status shrk_clean_covariance_matrix_dev(const double* d_matrix, size_t p, double c,
+                                             int renormalize, double* d_covariance,
+                                             double* d_eigenvectors, double* d_rie_eigenvalues,
+                                             double* d_overlaps, double* sigma2, void* stream);
+shrk_status shrk_estimate_precision_matrix_dev(const double* d_matrix, size_t p, double c,
+                                               int method, double* d_precision,
+                                               double* d_eigenvectors, double* d_precision_ev,
+                                               double* d_covariance_ev, double* smoothing,
+                                               void* stream);
 
 /* ------------------------------------------------------- consumers -- */
 /* deconvolution/inverse.rs:156-269 inverse_nonlinear_shrinkage (RmtConfig::new:

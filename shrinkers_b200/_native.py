@@ -67,6 +67,11 @@ SIGNATURES = {
                                   _P, _P]),
     "shrk_inverse_nonlinear_shrinkage": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
     "shrk_symmetric_eigh": (_ST, [_D, _SZ, _D, _D]),
+    "shrk_symmetric_eigh_dev": (_ST, [_P, _SZ, _P, _P, _P]),
+    "shrk_clean_covariance_matrix_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, _P, _P, _P, _P, _D,
+                                               _P]),
+    "shrk_estimate_precision_matrix_dev": (_ST, [_P, _SZ, C.c_double, C.c_int, _P, _P, _P, _P,
+                                                 _D, _P]),
     "shrk_clean_eigensystem": (_ST, [_D, _D, _SZ, C.c_double, _D, _D, _D, _D, _D]),
     "shrk_clean_covariance_matrix": (_ST, [_D, _SZ, C.c_double, C.c_int, _D, _D, _D, _D, _D]),
     "shrk_renormalize_to_unit_diagonal": (_ST, [_D, _SZ, _D]),

@@ -186,6 +186,11 @@ shrk_status eigh_sorted_slot(int64_t p, std::vector<double>& w_host, cudaStream_
   return eigh_device((double*)a, p, w_host, s);
 }
 
+shrk_status einval_matrix(const char* what) {
+  set_error(what);
+  return SHRK_EINVAL;
+}
+
 shrk_status check_matrix_args(const void* m, size_t p, double c) {
   if (!m || p == 0) {
     set_error("matrix must be non-empty");
@@ -223,20 +228,36 @@ shrk_status upload_eigenvectors(const double* v, int64_t p, cudaStream_t s) {
   return SHRK_OK;
 }
 
-// Downloads the columns `cols` of SLOT_E as a row-major matrix.
+// Downloads the columns `cols` of SLOT_E as a row-major matrix (dev_out:
+// gathered straight into the caller's device matrix).
 shrk_status download_columns(const std::vector<int>& cols, int64_t p, double* out,
-                             cudaStream_t s) {
+                             cudaStream_t s, bool dev_out = false) {
   void *a = nullptr, *idx = nullptr, *o = nullptr;
   SHRK_TRY(scratch_get(SLOT_E, sizeof(double) * p * p, &a));
   SHRK_TRY(scratch_get(SLOT_IDX, sizeof(int) * p + 256, &idx));
-  SHRK_TRY(scratch_get(SLOT_OUT2, sizeof(double) * p * p, &o));
+  if (dev_out) o = out;
+  else SHRK_TRY(scratch_get(SLOT_OUT2, sizeof(double) * p * p, &o));
   SHRK_CUDA(cudaMemcpyAsync(idx, cols.data(), sizeof(int) * p, cudaMemcpyHostToDevice, s));
   gather_columns_kernel<<<tiles_grid(p), dim3(32, 8), 0, s>>>((const double*)a, p,
                                                               (const int*)idx, (double*)o);
   SHRK_CUDA(cudaGetLastError());
   add_launches(1);
-  SHRK_CUDA(cudaMemcpyAsync(out, o, sizeof(double) * p * p, cudaMemcpyDeviceToHost, s));
+  if (!dev_out)
+    SHRK_CUDA(cudaMemcpyAsync(out, o, sizeof(double) * p * p, cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
+  return SHRK_OK;
+}
+
+// Copies p values from the host into a caller's device array (or a host
+// array, when the outputs are on the host).
+shrk_status put_vector(double* dst, const std::vector<double>& v, bool dev_out, cudaStream_t s) {
+  if (!dst) return SHRK_OK;
+  if (!dev_out) {
+    std::copy(v.begin(), v.end(), dst);
+    return SHRK_OK;
+  }
+  SHRK_CUDA(cudaMemcpyAsync(dst, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, s));
+  SHRK_CUDA(cudaStreamSynchronize(s));  // v is a local of the caller
   return SHRK_OK;
 }
 
@@ -245,7 +266,7 @@ shrk_status download_columns(const std::vector<int>& cols, int64_t p, double* ou
 // entry: the RIE call takes it itself.
 shrk_status clean_sorted(const std::vector<int>& cols, const std::vector<double>& sorted, double c,
                          int renorm, double* cov, double* evecs, double* l_rie, double* overlaps,
-                         double* sigma2) {
+                         double* sigma2, bool dev_out = false) {
   const size_t p = sorted.size();
   std::vector<double> xi(p), a2(p, 0.0);
   // RmtConfig::new(c): Blocked, Sequential, no cutoff, eta = 0.4/sqrt(p)
@@ -340,11 +361,12 @@ shrk_status clean_sorted(const std::vector<int>& cols, const std::vector<double>
     add_launches(2);
     result = (double*)out2;
   }
-  SHRK_CUDA(cudaMemcpyAsync(cov, result, sizeof(double) * P * P, cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaMemcpyAsync(cov, result, sizeof(double) * P * P,
+                            dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
-  if (evecs) SHRK_TRY(download_columns(cols, P, evecs, s));
-  if (l_rie) std::copy(xi.begin(), xi.end(), l_rie);
-  if (overlaps) std::copy(a2.begin(), a2.end(), overlaps);
+  if (evecs) SHRK_TRY(download_columns(cols, P, evecs, s, dev_out));
+  SHRK_TRY(put_vector(l_rie, xi, dev_out, s));
+  SHRK_TRY(put_vector(overlaps, a2, dev_out, s));
   if (sigma2) *sigma2 = s2;
   return check_device_error(s);
 }
@@ -352,7 +374,7 @@ shrk_status clean_sorted(const std::vector<int>& cols, const std::vector<double>
 // mod.rs:409-464 from the eigenvectors in SLOT_E; lock not held on entry.
 shrk_status precision_sorted(const std::vector<int>& cols, const std::vector<double>& sorted,
                              double c, int method, double* prec, double* evecs, double* prec_ev,
-                             double* cov_ev, double* smoothing) {
+                             double* cov_ev, double* smoothing, bool dev_out = false) {
   const size_t p = sorted.size();
   std::vector<double> pe(p), ce(p);
   double h = 0.0;
@@ -384,11 +406,12 @@ shrk_status precision_sorted(const std::vector<int>& cols, const std::vector<dou
     symmetrize_kernel<<<rows_grid(P, 256), 256, 0, s>>>((double*)out, P);
     SHRK_CUDA(cudaGetLastError());
   }
-  SHRK_CUDA(cudaMemcpyAsync(prec, out, sizeof(double) * P * P, cudaMemcpyDeviceToHost, s));
+  SHRK_CUDA(cudaMemcpyAsync(prec, out, sizeof(double) * P * P,
+                            dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
   SHRK_CUDA(cudaStreamSynchronize(s));
-  if (evecs) SHRK_TRY(download_columns(cols, P, evecs, s));
-  if (prec_ev) std::copy(pe.begin(), pe.end(), prec_ev);
-  if (cov_ev) std::copy(ce.begin(), ce.end(), cov_ev);
+  if (evecs) SHRK_TRY(download_columns(cols, P, evecs, s, dev_out));
+  SHRK_TRY(put_vector(prec_ev, pe, dev_out, s));
+  SHRK_TRY(put_vector(cov_ev, ce, dev_out, s));
   if (smoothing) *smoothing = h;
   return check_device_error(s);
 }
@@ -396,13 +419,14 @@ shrk_status precision_sorted(const std::vector<int>& cols, const std::vector<dou
 // Eigendecomposition of a caller matrix into SLOT_E; descending eigenvalues
 // and, for each, its column of SLOT_E.
 shrk_status eigh_sorted(const double* m, int64_t p, std::vector<int>& cols,
-                        std::vector<double>& sorted) {
+                        std::vector<double>& sorted, bool dev_in = false) {
   LibScope L;
   SHRK_TRY(L.st);
   cudaStream_t s = L.stream;
   void* a = nullptr;
   SHRK_TRY(scratch_get(SLOT_E, sizeof(double) * p * p, &a));
-  SHRK_CUDA(cudaMemcpyAsync(a, m, sizeof(double) * p * p, cudaMemcpyHostToDevice, s));
+  SHRK_CUDA(cudaMemcpyAsync(a, m, sizeof(double) * p * p,
+                            dev_in ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
   std::vector<double> w;
   SHRK_TRY(eigh_sorted_slot(p, w, s));
   cols.resize(p);
@@ -518,6 +542,100 @@ shrk_status shrk_estimate_precision_matrix(const double* matrix, size_t p, doubl
   SHRK_TRY(eigh_sorted(matrix, (int64_t)p, cols, sorted));
   return precision_sorted(cols, sorted, c, method, precision, eigenvectors, precision_ev,
                           covariance_ev, smoothing);
+}
+
+// Device-pointer forms.  The library runs them on its own stream for the
+// calling thread (the steps between the kernels are host arithmetic that
+// needs the spectrum on the host); they wait for the work already queued on
+// the caller's stream before reading its matrix, and the caller's stream
+// waits for their outputs.
+namespace {
+struct StreamJoin {
+  cudaStream_t caller;
+  shrk_status st = SHRK_OK;
+  explicit StreamJoin(void* stream) : caller((cudaStream_t)stream) {
+    LibScope L;
+    st = L.st;
+    if (st != SHRK_OK) return;
+    st = join(caller, L.stream);
+  }
+  // `after` waits for everything queued on `before` so far
+  static shrk_status join(cudaStream_t before, cudaStream_t after) {
+    if (before == after) return SHRK_OK;
+    cudaEvent_t ev;
+    SHRK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaEventRecord(ev, before);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(after, ev, 0);
+    cudaEventDestroy(ev);
+    if (e != cudaSuccess) {
+      set_error(std::string("CUDA: ") + cudaGetErrorString(e));
+      return SHRK_ECUDA;
+    }
+    return SHRK_OK;
+  }
+  shrk_status finish(shrk_status r) {
+    if (r != SHRK_OK) return r;
+    LibScope L;
+    SHRK_TRY(L.st);
+    return join(L.stream, caller);
+  }
+};
+}  // namespace
+
+shrk_status shrk_symmetric_eigh_dev(const double* d_matrix, size_t p, double* d_eigenvalues,
+                                    double* d_eigenvectors, void* stream) {
+  SHRK_TRY(check_matrix_args(d_matrix, p, 1.0));
+  if (!d_eigenvalues) return einval_matrix("null eigenvalue output");
+  StreamJoin J(stream);
+  SHRK_TRY(J.st);
+  std::vector<int> cols;
+  std::vector<double> sorted;
+  SHRK_TRY(eigh_sorted(d_matrix, (int64_t)p, cols, sorted, true));
+  std::vector<double> asc(sorted.rbegin(), sorted.rend());
+  shrk_status r = SHRK_OK;
+  {
+    LibScope L;
+    SHRK_TRY(L.st);
+    SHRK_TRY(put_vector(d_eigenvalues, asc, true, L.stream));
+    if (d_eigenvectors) {
+      std::vector<int> idx(p);
+      std::iota(idx.begin(), idx.end(), 0);
+      SHRK_TRY(download_columns(idx, (int64_t)p, d_eigenvectors, L.stream, true));
+    }
+    r = check_device_error(L.stream);
+  }
+  return J.finish(r);
+}
+
+shrk_status shrk_clean_covariance_matrix_dev(const double* d_matrix, size_t p, double c,
+                                             int renormalize, double* d_covariance,
+                                             double* d_eigenvectors, double* d_rie_eigenvalues,
+                                             double* d_overlaps, double* sigma2, void* stream) {
+  SHRK_TRY(check_matrix_args(d_matrix, p, c));
+  if (!d_covariance) return einval_matrix("null covariance output");
+  StreamJoin J(stream);
+  SHRK_TRY(J.st);
+  std::vector<int> cols;
+  std::vector<double> sorted;
+  SHRK_TRY(eigh_sorted(d_matrix, (int64_t)p, cols, sorted, true));
+  return J.finish(clean_sorted(cols, sorted, c, renormalize, d_covariance, d_eigenvectors,
+                               d_rie_eigenvalues, d_overlaps, sigma2, true));
+}
+
+shrk_status shrk_estimate_precision_matrix_dev(const double* d_matrix, size_t p, double c,
+                                               int method, double* d_precision,
+                                               double* d_eigenvectors, double* d_precision_ev,
+                                               double* d_covariance_ev, double* smoothing,
+                                               void* stream) {
+  SHRK_TRY(check_matrix_args(d_matrix, p, c));
+  if (!d_precision) return einval_matrix("null precision output");
+  StreamJoin J(stream);
+  SHRK_TRY(J.st);
+  std::vector<int> cols;
+  std::vector<double> sorted;
+  SHRK_TRY(eigh_sorted(d_matrix, (int64_t)p, cols, sorted, true));
+  return J.finish(precision_sorted(cols, sorted, c, method, d_precision, d_eigenvectors,
+                                   d_precision_ev, d_covariance_ev, smoothing, true));
 }
 
 }  // extern "C"

@@ -3,8 +3,9 @@ friends) against the oracle's restatement of src/pipeline/mod.rs, and the
 reference's Python tests of clean_correlation_matrix / clean_covariance_matrix
 / estimate_precision_matrix (test_python_api.py:165-470) restated.
 
-The GPU eigensolver (cuSOLVER syevd) and the reference's Jacobi iteration
-agree to rounding on the spectrum and, up to sign, on the eigenvectors; the
+The GPU eigensolver (the library's own: Householder tridiagonalisation,
+multisection, inverse iteration) and the reference's Jacobi iteration agree
+to rounding on the spectrum and, up to sign, on the eigenvectors; the
 cleaned matrices are sign-invariant.  Bars: 1e-10 relative to the largest
 entry for matrices built from different eigensolvers, 1e-12 when both sides
 start from the same eigensystem.
@@ -237,3 +238,62 @@ def test_small_and_trivial(rk, oracle):
     one = rk.clean_covariance_matrix(np.array([[2.0]]), c=0.5)
     ref = oracle.clean_matrix(np.array([[2.0]]), 0.5)
     np.testing.assert_allclose(one["covariance"], ref["covariance"], rtol=1e-12)
+
+
+def test_device_forms_match_host_forms(rk):
+    """shrk_*_dev: the matrix produced on the caller's stream just before
+    the call (the call must wait for it), outputs on the device; the same
+    values as the host forms, bit for bit."""
+    import ctypes as C
+
+    import torch
+    from shrinkers_b200 import _native
+
+    L = _native.load()
+    cov, c, _ = sample_cov(300, 1200, 21)
+    p = cov.shape[0]
+    host = rk.clean_covariance_matrix(cov, c=c)
+    prec_host = rk.estimate_precision_matrix(cov, c=c)
+    ev_host, vec_host = rk.symmetric_eigh(cov)
+    d = torch.device("cuda", 0)
+    st = torch.cuda.Stream(device=d)
+    with torch.cuda.stream(st):
+        src = torch.from_numpy(cov).to(d)
+        m = (src * 2.0) * 0.5  # queued on st right before the call
+        out = torch.empty(p, p, dtype=torch.float64, device=d)
+        vec = torch.empty_like(out)
+        rie = torch.empty(p, dtype=torch.float64, device=d)
+        ov = torch.empty_like(rie)
+        s2 = C.c_double()
+        _native.check(L.shrk_clean_covariance_matrix_dev(
+            m.data_ptr(), p, c, 0, out.data_ptr(), vec.data_ptr(), rie.data_ptr(), ov.data_ptr(),
+            C.byref(s2), st.cuda_stream), "clean_covariance_matrix_dev")
+        res = {k: v.cpu().numpy() for k, v in
+               (("covariance", out), ("eigenvectors", vec), ("eigenvalues", rie),
+                ("overlaps", ov))}
+        pe = torch.empty(p, dtype=torch.float64, device=d)
+        ce = torch.empty_like(pe)
+        om = torch.empty(p, p, dtype=torch.float64, device=d)
+        h = C.c_double()
+        _native.check(L.shrk_estimate_precision_matrix_dev(
+            m.data_ptr(), p, c, 0, om.data_ptr(), vec.data_ptr(), pe.data_ptr(), ce.data_ptr(),
+            C.byref(h), st.cuda_stream), "estimate_precision_matrix_dev")
+        prec = {"precision": om.cpu().numpy(), "eigenvectors": vec.cpu().numpy(),
+                "precision_eigenvalues": pe.cpu().numpy(),
+                "covariance_eigenvalues": ce.cpu().numpy()}
+        w = torch.empty(p, dtype=torch.float64, device=d)
+        _native.check(L.shrk_symmetric_eigh_dev(m.data_ptr(), p, w.data_ptr(), vec.data_ptr(),
+                                                st.cuda_stream), "symmetric_eigh_dev")
+        ev_dev, vec_dev = w.cpu().numpy(), vec.cpu().numpy()
+    for k in ("covariance", "eigenvectors", "eigenvalues", "overlaps"):
+        np.testing.assert_array_equal(res[k], host[k])
+    assert s2.value == host["sigma2"]
+    for k in ("precision", "eigenvectors", "precision_eigenvalues", "covariance_eigenvalues"):
+        np.testing.assert_array_equal(prec[k], prec_host[k])
+    assert h.value == prec_host["smoothing"]
+    np.testing.assert_array_equal(ev_dev, ev_host)
+    np.testing.assert_array_equal(vec_dev, vec_host)
+    # argument checks before any device work
+    assert L.shrk_clean_covariance_matrix_dev(None, p, c, 0, out.data_ptr(), None, None, None,
+                                              None, None) == _native.SHRK_EINVAL
+    assert L.shrk_symmetric_eigh_dev(m.data_ptr(), p, None, None, None) == _native.SHRK_EINVAL
