@@ -849,11 +849,15 @@ shrk_status shrk_stieltjes_shard_dev(const double* d_tgt, size_t nt, size_t nq_t
   }
   int64_t offset = 0;
   if (all_points) {
-    offset = (int64_t)(d_tgt - d_ev);
-    if (d_tgt < d_ev || offset > (int64_t)(p - nt) || nq_total != p) {
+    // the targets must be a slice of the spectrum (compared as addresses)
+    const uintptr_t t = (uintptr_t)d_tgt, e = (uintptr_t)d_ev;
+    const bool inside = t >= e && (t - e) % sizeof(double) == 0 && nt <= p &&
+                        (t - e) / sizeof(double) <= (uintptr_t)(p - nt);
+    if (!inside || nq_total != p) {
       set_error("shard: all-points targets must be a slice of the spectrum, nq_total = p");
       return SHRK_EINVAL;
     }
+    offset = (int64_t)((t - e) / sizeof(double));
   }
   if (nt == 0) return SHRK_OK;
   Guard g(stream);
