@@ -153,18 +153,32 @@ __device__ __forceinline__ int64_t lower_key(const GridArgs& a, int key, int64_t
 }
 
 constexpr int DENSE_MIN = 32;   // cells with more sources take their density from run sums
-constexpr int RUN_CTA = 32;     // runs with more sources get a whole CTA for their sums
+constexpr int RUN_CTA = 32;     // runs with more sources are summed by CTAs,
+constexpr int RUN_CHUNK = 4096; // in chunks of this many sources, a CTA each
+
+// The long runs and their chunks (keys_kernel fills them, long_runs_kernel
+// sums them): run r is key idx[r] with nch[r] chunks from the chunk list's
+// base[r]; cnt[r] counts its finished chunks; partial[g][k] holds chunk g's
+// sums.  counters[0] / [1] = runs / chunks listed (zero on entry).
+struct LongRuns {
+  int* idx;
+  int* base;
+  int* nch;
+  int* cnt;
+  int* chunk_run;  // chunk g -> its run r
+  int* counters;
+  double* partial;
+};
 
 // Keys and run sums.  The thread of key e finds first[e] by bisection and
 // the end of its run by a galloping search from there (one probe for an empty
 // run); then S[(e + N + 1) N + k], the sum of stencil weight k over the run,
 // computing each source's N weights once in ascending source order -- or,
-// for a run of more than RUN_CTA sources, appends e to the list that
-// long_runs_kernel gives a CTA each (*n_long is zero on entry).
+// for a run of more than RUN_CTA sources, lists the run and its chunks of
+// RUN_CHUNK sources for long_runs_kernel.
 template <int N>
 __global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n_keys,
-                            double* __restrict__ S, int* __restrict__ long_runs,
-                            int* __restrict__ n_long) {
+                            double* __restrict__ S, LongRuns L) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx > n_keys) return;
   const int key = (int)(idx - N - 1);
@@ -181,7 +195,14 @@ __global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n
   }
   const int64_t j1 = lower_key<N>(a, key + 1, lo, hi < a.ns ? hi : a.ns);
   if (j1 - j0 > RUN_CTA) {
-    long_runs[atomicAdd(n_long, 1)] = (int)idx;
+    const int nch = (int)((j1 - j0 + RUN_CHUNK - 1) / RUN_CHUNK);
+    const int r = atomicAdd(L.counters, 1);
+    const int base = atomicAdd(L.counters + 1, nch);
+    L.idx[r] = (int)idx;
+    L.base[r] = base;
+    L.nch[r] = nch;
+    L.cnt[r] = 0;
+    for (int c = 0; c < nch; ++c) L.chunk_run[base + c] = r;
     return;
   }
   double acc[N];
@@ -198,21 +219,28 @@ __global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n
   for (int k = 0; k < N; ++k) S[idx * N + k] = acc[k];
 }
 
-// Run sums of the long runs, one CTA each (threads stride the run, partials
-// added in a fixed order).  The list order varies from call to call; each
-// run's sum does not.
+// Run sums of the long runs: a CTA per chunk of RUN_CHUNK sources (threads
+// stride the chunk, partials added in a fixed order).  A run of one chunk
+// writes its sums directly; otherwise the CTA that finishes a run's last
+// chunk (a ticket taken after a fence) adds the run's chunk partials in
+// chunk order.  The lists' order varies from call to call; each run's sum
+// does not.
 template <int N>
 __global__ void __launch_bounds__(256) long_runs_kernel(const GridArgs a,
                                                         const int* __restrict__ first,
-                                                        const int* __restrict__ long_runs,
-                                                        const int* __restrict__ n_long,
+                                                        const LongRuns L,
                                                         double* __restrict__ S) {
   __shared__ double red[8][N];
+  __shared__ int last;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int nl = *n_long;
-  for (int r = blockIdx.x; r < nl; r += gridDim.x) {
-    const int64_t idx = long_runs[r];
-    const int64_t j0 = first[idx], j1 = first[idx + 1];
+  const int n_chunks = L.counters[1];
+  for (int g = blockIdx.x; g < n_chunks; g += gridDim.x) {
+    const int r = L.chunk_run[g];
+    const int64_t idx = L.idx[r];
+    const int nch = L.nch[r], c = g - L.base[r];
+    const int64_t r0 = first[idx], r1 = first[idx + 1];
+    const int64_t j0 = r0 + (int64_t)c * RUN_CHUNK;
+    const int64_t j1 = j0 + RUN_CHUNK < r1 ? j0 + RUN_CHUNK : r1;
     double acc[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) acc[k] = 0.0;
@@ -234,7 +262,23 @@ __global__ void __launch_bounds__(256) long_runs_kernel(const GridArgs a,
     if (threadIdx.x < N) {
       double tt = 0.0;
       for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tt += red[w][threadIdx.x];
-      S[idx * N + threadIdx.x] = tt;
+      if (nch == 1) S[idx * N + threadIdx.x] = tt;
+      else L.partial[(int64_t)g * N + threadIdx.x] = tt;
+    }
+    if (nch > 1) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();  // this chunk's partials before its ticket
+        last = atomicAdd(L.cnt + r, 1) == nch - 1;
+      }
+      __syncthreads();
+      if (last && threadIdx.x < N) {
+        __threadfence();
+        const int b0 = L.base[r];
+        double tt = 0.0;
+        for (int q = 0; q < nch; ++q) tt += __ldcg(L.partial + (int64_t)(b0 + q) * N + threadIdx.x);
+        S[idx * N + threadIdx.x] = tt;
+      }
     }
     __syncthreads();
   }
@@ -896,26 +940,36 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
     if (dens_out) SHRK_CUDA(cudaMemsetAsync(dens_out, 0, sizeof(double) * m, s));
     return SHRK_OK;
   }
-  // slot 24: first [K + 1] | long-run list [K] + its length | run sums [K][N],
-  // K = m + 2N + 2 keys from -N - 1
+  // slot 24: first [K + 1] | long runs: idx, base, nch, cnt [K] each | two
+  // counters | chunk list [C] | run sums [K][N] | chunk partials [C][N],
+  // K = m + 2N + 2 keys from -N - 1, C = ns / RUN_CHUNK + K chunks at most
+  // (a run of n > RUN_CTA sources has ceil(n / RUN_CHUNK) chunks)
   const int64_t n_keys = m + 2 * N + 2;
-  const size_t first_bytes = ((sizeof(int) * (2 * (size_t)n_keys + 2)) + 255) & ~(size_t)255;
+  const int64_t max_chunks = ns / RUN_CHUNK + n_keys;
+  const size_t int_bytes =
+      ((sizeof(int) * (5 * (size_t)n_keys + 3 + (size_t)max_chunks)) + 255) & ~(size_t)255;
   void* sw = nullptr;
-  SHRK_TRY(scratch_get(24, first_bytes + sizeof(double) * N * (size_t)n_keys, &sw));
+  SHRK_TRY(scratch_get(24, int_bytes + sizeof(double) * N * ((size_t)n_keys + (size_t)max_chunks),
+                       &sw));
   int* first = (int*)sw;
-  int* long_runs = first + n_keys + 1;
-  int* n_long = long_runs + n_keys;
-  double* runs = (double*)((char*)sw + first_bytes);
-  SHRK_CUDA(cudaMemsetAsync(n_long, 0, sizeof(int), s));
+  LongRuns lr;
+  lr.idx = first + n_keys + 1;
+  lr.base = lr.idx + n_keys;
+  lr.nch = lr.base + n_keys;
+  lr.cnt = lr.nch + n_keys;
+  lr.counters = lr.cnt + n_keys;
+  lr.chunk_run = lr.counters + 2;
+  double* runs = (double*)((char*)sw + int_bytes);
+  lr.partial = runs + (size_t)N * n_keys;
+  SHRK_CUDA(cudaMemsetAsync(lr.counters, 0, 2 * sizeof(int), s));
   {
     LaunchScope ls(g.fam_splat, s);
-    keys_kernel<N><<<blocks_for(n_keys + 1, 256), 256, 0, s>>>(ga, first, n_keys, runs, long_runs,
-                                                              n_long);
+    keys_kernel<N><<<blocks_for(n_keys + 1, 256), 256, 0, s>>>(ga, first, n_keys, runs, lr);
     SHRK_CUDA(cudaGetLastError());
   }
   {
     LaunchScope ls(g.fam_splat, s);
-    long_runs_kernel<N><<<sm_count() * 4, 256, 0, s>>>(ga, first, long_runs, n_long, runs);
+    long_runs_kernel<N><<<sm_count() * 4, 256, 0, s>>>(ga, first, lr, runs);
     SHRK_CUDA(cudaGetLastError());
   }
   {
