@@ -56,6 +56,28 @@ def test_nufft_matches_oracle(oracle, p, eta_rule):
     assert np.max(np.abs(im * p - o_im)) < 1e-10 * scale
 
 
+def test_nufft_dense_cells_in_chunks(oracle):
+    """Sources piled into a few grid cells: 150 000 of 200 000 sources in a
+    cluster narrower than a cell, so their runs span many 4 096-source
+    chunks (summed by different CTAs, then added in chunk order), beside a
+    sparse bulk; against the oracle's sequential splat, and twice the same
+    bits (the chunk order is fixed)."""
+    rng = np.random.default_rng(77)
+    bulk = rng.uniform(0.5, 3.0, 50_000)
+    cluster = 1.7 + rng.uniform(0.0, 1e-7, 150_000)
+    ev = np.sort(np.concatenate([bulk, cluster, [40.0]]))
+    p = ev.size
+    eta = 1.0 / math.sqrt(p)
+    re, im = gpu_nufft_all(ev, eta)
+    re2, im2 = gpu_nufft_all(ev, eta)
+    np.testing.assert_array_equal(re, re2)
+    np.testing.assert_array_equal(im, im2)
+    o_re, o_im = oracle.nufft_points(ev, ev, eta)
+    scale = max(np.max(np.abs(o_re)), np.max(np.abs(o_im)))
+    assert np.max(np.abs(re * p - o_re)) < 1e-10 * scale
+    assert np.max(np.abs(im * p - o_im)) < 1e-10 * scale
+
+
 def test_nufft_reference_accuracy_bars(oracle):
     """nufft.rs:252-318: rel-L2 < 1e-4 vs exact at p=8192 (all points and a
     200-point grid), eta = 1/sqrt(p)."""
