@@ -931,7 +931,8 @@ def run_clean(args, world, rank, local):
     L.shrk_timing_enable(0)
     fams = {}
     for f in (b"eigh_tridiag", b"eigh_bisect", b"eigh_inverse_iteration", b"eigh_orthogonalise",
-              b"eigh_back_transform", b"dgemm", b"matrix_reconstruct", b"pair_sum_f64",
+              b"eigh_back_transform", b"dgemm_wy_yty", b"dgemm_wy_ytz", b"dgemm_wy_tw",
+              b"dgemm_wy_update", b"dgemm", b"matrix_reconstruct", b"pair_sum_f64",
               b"split_reduce"):
         kn, kms = C.c_int64(), C.c_double()
         L.shrk_timing_read(f, C.byref(kn), C.byref(kms))

@@ -46,6 +46,13 @@ shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean);
  * SHRK_ETIMEOUT and the allocation-free call writes NaN to every output.
  * Process-wide; meant for tests. */
 long long shrk_diag_set_wait_limit(long long cycles);
+/* The library's FP64 GEMM on device pointers (column-major, as BLAS dgemm):
+ * C = alpha op(A) op(B) + beta C with op = transpose when ta / tb != 0; the
+ * kernel the eigensolver's back-transform and the matrix reconstructions
+ * use, exported to time it on its own. */
+shrk_status shrk_diag_dgemm(int ta, int tb, int64_t m, int64_t n, int64_t k, double alpha,
+                            const double* d_a, int64_t lda, const double* d_b, int64_t ldb,
+                            double beta, double* d_c, int64_t ldc, void* stream);
 
 #ifdef __cplusplus
 }

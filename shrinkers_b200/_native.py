@@ -94,6 +94,8 @@ SIGNATURES = {
     "shrk_measure_pipe_rates": (_ST, [_D, _D]),
     "shrk_measure_rcp_bias": (_ST, [_D, _D]),
     "shrk_diag_set_wait_limit": (C.c_longlong, [C.c_longlong]),
+    "shrk_diag_dgemm": (_ST, [C.c_int, C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_double, _P,
+                              C.c_int64, _P, C.c_int64, C.c_double, _P, C.c_int64, _P]),
 }
 
 _lib = None

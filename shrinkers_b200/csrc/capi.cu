@@ -1660,4 +1660,21 @@ shrk_status shrk_measure_rcp_bias(double* uniform_mean, double* log_mean) {
 
 long long shrk_diag_set_wait_limit(long long cycles) { return set_wait_cycles(cycles); }
 
+shrk_status shrk_diag_dgemm(int ta, int tb, int64_t m, int64_t n, int64_t k, double alpha,
+                            const double* d_a, int64_t lda, const double* d_b, int64_t ldb,
+                            double beta, double* d_c, int64_t ldc, void* stream) {
+  if (m < 0 || n < 0 || k < 0 || !d_c || (k > 0 && (!d_a || !d_b))) {
+    set_error("dgemm: invalid arguments");
+    return SHRK_EINVAL;
+  }
+  if (lda < (ta ? k : m) || ldb < (tb ? n : k) || ldc < m || lda < 1 || ldb < 1 || ldc < 1) {
+    set_error("dgemm: leading dimensions too small");
+    return SHRK_EINVAL;
+  }
+  Guard g(stream);
+  SHRK_TRY(g.st);
+  return dgemm(ta != 0, tb != 0, m, n, k, alpha, d_a, lda, d_b, ldb, beta, d_c, ldc,
+               (cudaStream_t)stream);
+}
+
 }  // extern "C"

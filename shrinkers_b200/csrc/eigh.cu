@@ -36,6 +36,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -125,11 +126,23 @@ __global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, int kz,
   }
 }
 
-// The large-problem form: 128 x 128 outputs per CTA of 256 threads, 8 x 8
-// per thread (64 independent FMA chains), k staged 8 at a time, two stages
-// in flight (the next stage's global loads are issued before this stage's
-// FMAs).
-constexpr int GT2 = 128, GK2 = 8;
+// The large-problem form: 128 x 128 outputs per CTA of 256 threads on the
+// FP64 tensor path (mma.sync m8n8k4 .f64; tcgen05 has no FP64 kind): each
+// warp owns a 32 x 64 block, 4 x 8 tiles of 8 x 8 with two accumulators a
+// lane; k staged 8 at a time through shared memory, two stages in flight
+// (the next stage's global loads are issued before this stage's MMAs).  Rows
+// of the staged tiles are 136 doubles apart (16 words mod 32 banks), so a
+// fragment load -- 4 k rows x 8 consecutive entries -- takes the two
+// wavefronts a 64-bit warp load needs and no more.
+constexpr int GT2 = 128, GK2 = 8, GP2 = GT2 + 8;
+
+// D = A B + D for one 8 x 8 x 4 FP64 tile: lane l holds A[l/4][l%4],
+// B[l%4][l/4] and D[l/4][2(l%4) + {0, 1}].
+__device__ __forceinline__ void mma_f64(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
 
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256, 1) dgemm_big_kernel(int m, int n, int k, int kz,
@@ -140,17 +153,19 @@ __global__ void __launch_bounds__(256, 1) dgemm_big_kernel(int m, int n, int k, 
                                                            int64_t ldb, double beta,
                                                            double* __restrict__ C,
                                                            int64_t ldc) {
-  __shared__ double As[2][GK2][GT2 + 2];  // As[kk][i] = op(A)[i0 + i, k0 + kk]
-  __shared__ double Bs[2][GK2][GT2 + 2];  // Bs[kk][j] = op(B)[k0 + kk, j0 + j]
+  __shared__ double As[2][GK2][GP2];  // As[kk][i] = op(A)[i0 + i, k0 + kk]
+  __shared__ double Bs[2][GK2][GP2];  // Bs[kk][j] = op(B)[k0 + kk, j0 + j]
   const int kb = blockIdx.z * kz, ke = min(k, kb + kz);
   if (gridDim.z > 1) C += (int64_t)blockIdx.z * m * n;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wi = (warp & 3) * 32, wj = (warp >> 2) * 64;  // the warp's block
+  const int fr = lane >> 2, fk = lane & 3;                 // fragment row / k
   const int i0 = blockIdx.x * GT2, j0 = blockIdx.y * GT2;
-  double acc[8][8];
+  double acc[4][8][2];
 #pragma unroll
-  for (int r = 0; r < 8; ++r)
+  for (int r = 0; r < 4; ++r)
 #pragma unroll
-    for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
+    for (int c = 0; c < 8; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
   double ra[4], rb[4];
   auto fetch = [&](int k0) {
 #pragma unroll
@@ -192,16 +207,16 @@ __global__ void __launch_bounds__(256, 1) dgemm_big_kernel(int m, int n, int k, 
     const bool more = k0 + GK2 < ke;
     if (more) fetch(k0 + GK2);
 #pragma unroll
-    for (int kk = 0; kk < GK2; ++kk) {
-      double a[8], b[8];
+    for (int k4 = 0; k4 < GK2; k4 += 4) {
+      double a[4], b[8];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) a[r] = As[buf][kk][tx + 16 * r];
+      for (int r = 0; r < 4; ++r) a[r] = As[buf][k4 + fk][wi + 8 * r + fr];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) b[c] = Bs[buf][kk][ty + 16 * c];
+      for (int c = 0; c < 8; ++c) b[c] = Bs[buf][k4 + fk][wj + 8 * c + fr];
 #pragma unroll
-      for (int r = 0; r < 8; ++r)
+      for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        for (int c = 0; c < 8; ++c) mma_f64(acc[r][c][0], acc[r][c][1], a[r], b[c]);
     }
     if (more) {
       stash(buf ^ 1);
@@ -211,14 +226,17 @@ __global__ void __launch_bounds__(256, 1) dgemm_big_kernel(int m, int n, int k, 
   }
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
-    const int gj = j0 + ty + 16 * c;
-    if (gj >= n) continue;
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int gi = i0 + tx + 16 * r;
-      if (gi >= m) continue;
-      double* cp = C + gi + (int64_t)gj * ldc;
-      *cp = beta == 0.0 ? alpha * acc[r][c] : fma(alpha, acc[r][c], beta * *cp);
+    for (int h = 0; h < 2; ++h) {
+      const int gj = j0 + wj + 8 * c + 2 * fk + h;
+      if (gj >= n) continue;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int gi = i0 + wi + 8 * r + fr;
+        if (gi >= m) continue;
+        double* cp = C + gi + (int64_t)gj * ldc;
+        *cp = beta == 0.0 ? alpha * acc[r][c][h] : fma(alpha, acc[r][c][h], beta * *cp);
+      }
     }
   }
 }
@@ -781,35 +799,59 @@ __global__ void build_y_kernel(const double* __restrict__ A, const double* __res
 }
 
 // T of the compact WY form, H_{j0} ... H_{j0+nb-1} = I - Y T Y^T (forward),
-// from T^{-1} = triu(S, 1) + diag(1 / beta), S = Y^T Y (the inverse of T is
-// the strictly upper part of Y^T Y plus the reflectors' v^T v / 2 on the
-// diagonal): thread j solves for column j of T by back substitution, all
-// columns at once (a reflector with beta = 0 has a zero column in Y and a
-// unit diagonal here).  One CTA of nb <= 64 threads.
-__global__ void wy_t_kernel(const double* __restrict__ S, const double* __restrict__ beta,
-                            int64_t j0, int nb, double* __restrict__ T) {
-  __shared__ double u[64][65];   // u[i][k] = T^{-1}[i][k]
-  double tc[64];                 // this thread's column of T (local memory)
-  const int j = threadIdx.x;
+// from T^{-1} = U = triu(S, 1) + diag(1 / beta), S = Y^T Y (the inverse of T
+// is the strictly upper part of Y^T Y plus the reflectors' v^T v / 2 on the
+// diagonal; a reflector with beta = 0 has a zero column in Y and a unit
+// diagonal here).  A warp per column j of T solves U x = e_j: lane l keeps
+// the running right-hand sides of rows l, l + 32, ...; from row j up, the
+// owner of row i forms x_i = r_i beta_i (1 / U_ii = beta_i exactly) and
+// every lane removes x_i's share from its rows above.  Each step is a
+// shuffle and a few FMAs, so the 128-step chain of a column takes a few
+// microseconds, all columns at once.  U lives in dynamic shared memory.
+constexpr int WY_NB = 128;
+constexpr int WY_T_WARPS = 32;  // columns per CTA
+constexpr size_t wy_t_smem() { return sizeof(double) * (WY_NB * (WY_NB + 1) + WY_NB); }
+
+__global__ void __launch_bounds__(WY_T_WARPS * 32) wy_t_kernel(const double* __restrict__ S,
+                                                              const double* __restrict__ beta,
+                                                              int64_t j0, int nb,
+                                                              double* __restrict__ T) {
+  extern __shared__ double u[];  // u[i LD + k] = U[i][k], i < k
+  constexpr int LD = WY_NB + 1, QN = WY_NB / 32;
+  double* rd = u + WY_NB * LD;   // 1 / U_ii
   for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
     const int i = idx % nb, k = idx / nb;
-    double v = 0.0;
-    if (i < k) v = S[i + k * nb];
-    else if (i == k) v = beta[j0 + i] != 0.0 ? 1.0 / beta[j0 + i] : 1.0;
-    u[i][k] = v;
+    if (i < k) u[i * LD + k] = S[i + k * nb];
   }
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    rd[i] = beta[j0 + i] != 0.0 ? beta[j0 + i] : 1.0;
   __syncthreads();
-  if (j < nb) {
-    for (int i = nb - 1; i >= 0; --i) {
-      double t = 0.0;
-      if (i <= j) {
-        double acc = i == j ? 1.0 : 0.0;
-        for (int k = i + 1; k <= j; ++k) acc -= u[i][k] * tc[k];
-        t = acc / u[i][i];
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * WY_T_WARPS + (threadIdx.x >> 5);
+  if (j >= nb) return;  // no barrier follows
+  double r[QN];
+#pragma unroll
+  for (int q = 0; q < QN; ++q) r[q] = lane + 32 * q == j ? 1.0 : 0.0;
+  for (int i = j; i >= 0; --i) {
+    const int owner = i & 31, qi = i >> 5;
+    double xi = 0.0;
+#pragma unroll
+    for (int q = 0; q < QN; ++q)
+      if (q == qi && lane == owner) {
+        xi = r[q] * rd[i];
+        r[q] = xi;  // row i is final: it now holds T[i][j]
       }
-      tc[i] = t;
+    xi = __shfl_sync(0xffffffffu, xi, owner);
+#pragma unroll
+    for (int q = 0; q < QN; ++q) {
+      const int row = lane + 32 * q;
+      if (row < i) r[q] -= u[row * LD + i] * xi;
     }
-    for (int i = 0; i < nb; ++i) T[i + j * nb] = tc[i];
+  }
+#pragma unroll
+  for (int q = 0; q < QN; ++q) {
+    const int row = lane + 32 * q;
+    if (row < nb) T[row + (int64_t)j * nb] = row <= j ? r[q] : 0.0;
   }
 }
 
@@ -846,7 +888,7 @@ __global__ void mirror_lower_kernel(double* __restrict__ A, int64_t p) {
 
 unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
-constexpr int NB = 64;                 // reflectors per WY block (wy_t_kernel: <= 64)
+constexpr int NB = WY_NB;              // reflectors per WY block
 // Eigenvalues closer than CLUSTER_TOL ||T|| (numerically equal) share one
 // thread and are orthogonalised by Gram-Schmidt during inverse iteration;
 // every other pair is left to inverse iteration, whose vectors then overlap
@@ -872,7 +914,7 @@ static void launch_gemm(bool big, dim3 grid, int m, int n, int k, int kz, double
 
 shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
                   int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
-                  cudaStream_t s) {
+                  cudaStream_t s, const char* family) {
   if (m <= 0 || n <= 0) return SHRK_OK;
   if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX) {
     set_error("dgemm: dimensions must be below 2^31");
@@ -899,7 +941,7 @@ shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alph
   const int kz = (int)((k + splits - 1) / splits);
   const dim3 grid(cdiv(m, tile), cdiv(n, tile), (unsigned)splits);
   {
-    LaunchScope ls("dgemm", s);
+    LaunchScope ls(family, s);
     if (!ta && !tb) launch_gemm<false, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
     else if (!ta && tb) launch_gemm<false, true>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
     else if (ta && !tb) launch_gemm<true, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
@@ -907,7 +949,7 @@ shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alph
     SHRK_CUDA(cudaGetLastError());
   }
   if (splits > 1) {
-    LaunchScope ls("dgemm", s);
+    LaunchScope ls(family, s);
     dgemm_reduce_kernel<<<cdiv(m * n, 256), 256, 0, s>>>(out, splits, (int)m, (int)n, beta, C, ldc);
     SHRK_CUDA(cudaGetLastError());
   }
@@ -1107,21 +1149,33 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
       const int nb = (int)std::min<int64_t>(NB, nref - j0);
       const int64_t n = p - j0 - 1;
       {
-        LaunchScope ls("eigh_back_transform", s);
+        LaunchScope ls("eigh_wy_y", s);
         build_y_kernel<<<dim3(cdiv(n, 256), (unsigned)nb), 256, 0, s>>>(A, vhead, beta, p, j0,
                                                                         nb, rowstore, Y);
         SHRK_CUDA(cudaGetLastError());
       }
-      SHRK_TRY(dgemm(true, false, nb, nb, n, 1.0, Y, n, Y, n, 0.0, S, nb, s));
+      SHRK_TRY(dgemm(true, false, nb, nb, n, 1.0, Y, n, Y, n, 0.0, S, nb, s, "dgemm_wy_yty"));
       {
-        LaunchScope ls("eigh_back_transform", s);
-        wy_t_kernel<<<1, 64, 0, s>>>(S, beta, j0, nb, T);
+        LaunchScope ls("eigh_wy_t", s);
+        static std::atomic<bool> opted[64];
+        int dv = 0;
+        SHRK_CUDA(cudaGetDevice(&dv));
+        if (dv < 0 || dv >= 64 || !opted[dv].load()) {
+          SHRK_CUDA(cudaFuncSetAttribute(wy_t_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)wy_t_smem()));
+          if (dv >= 0 && dv < 64) opted[dv] = true;
+        }
+        wy_t_kernel<<<(unsigned)cdiv(nb, WY_T_WARPS), WY_T_WARPS * 32, wy_t_smem(), s>>>(
+            S, beta, j0, nb, T);
         SHRK_CUDA(cudaGetLastError());
       }
       double* Zs = Zc + (j0 + 1);  // rows j0+1 .. p-1 of Zc (leading dimension p)
-      SHRK_TRY(dgemm(true, false, nb, p, n, 1.0, Y, n, Zs, p, 0.0, W, nb, s));     // W = Y^T Zs
-      SHRK_TRY(dgemm(false, false, nb, p, nb, 1.0, T, nb, W, nb, 0.0, W2, nb, s));  // W2 = T W
-      SHRK_TRY(dgemm(false, false, n, p, nb, -1.0, Y, n, W2, nb, 1.0, Zs, p, s));   // Zs -= Y W2
+      SHRK_TRY(dgemm(true, false, nb, p, n, 1.0, Y, n, Zs, p, 0.0, W, nb, s,
+                     "dgemm_wy_ytz"));  // W = Y^T Zs
+      SHRK_TRY(dgemm(false, false, nb, p, nb, 1.0, T, nb, W, nb, 0.0, W2, nb, s,
+                     "dgemm_wy_tw"));  // W2 = T W
+      SHRK_TRY(dgemm(false, false, n, p, nb, -1.0, Y, n, W2, nb, 1.0, Zs, p, s,
+                     "dgemm_wy_update"));  // Zs -= Y W2
     }
   }
   // ascending eigenvalues; eigenvector columns in that order, into A
