@@ -62,7 +62,8 @@ __global__ void __launch_bounds__(256) dgemm_kernel(int m, int n, int k, int kz,
                                                     const double* __restrict__ A, int64_t lda,
                                                     const double* __restrict__ B, int64_t ldb,
                                                     double beta, double* __restrict__ C,
-                                                    int64_t ldc) {
+                                                    int64_t ldc, int lower) {
+  if (lower && blockIdx.y > blockIdx.x) return;  // a tile wholly above the diagonal
   const int kb = blockIdx.z * kz, ke = min(k, kb + kz);
   if (gridDim.z > 1) C += (int64_t)blockIdx.z * m * n;
   __shared__ double As[GK][GT + 1];  // As[kk][i] = op(A)[i0 + i, k0 + kk]
@@ -152,7 +153,8 @@ __global__ void __launch_bounds__(256, 1) dgemm_big_kernel(int m, int n, int k, 
                                                            const double* __restrict__ B,
                                                            int64_t ldb, double beta,
                                                            double* __restrict__ C,
-                                                           int64_t ldc) {
+                                                           int64_t ldc, int lower) {
+  if (lower && blockIdx.y > blockIdx.x) return;  // a tile wholly above the diagonal
   __shared__ double As[2][GK2][GP2];  // As[kk][i] = op(A)[i0 + i, k0 + kk]
   __shared__ double Bs[2][GK2][GP2];  // Bs[kk][j] = op(B)[k0 + kk, j0 + j]
   const int kb = blockIdx.z * kz, ke = min(k, kb + kz);
@@ -771,11 +773,15 @@ __global__ void __launch_bounds__(64) inverse_iteration_kernel(
 
 // M = 1.5 I - 0.5 G (Newton-Schulz step for the polar factor).
 __global__ void ns_matrix_kernel(double* __restrict__ g, int64_t p) {
+  // M = (3I - G)/2 from the lower triangle of G (its upper one is not
+  // computed), written to both triangles
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t j = blockIdx.y;
-  if (i >= p) return;
+  if (i >= p || i < j) return;
   const double v = g[i + j * p];
-  g[i + j * p] = (i == j ? 1.5 : 0.0) - 0.5 * v;
+  const double mv = (i == j ? 1.5 : 0.0) - 0.5 * v;
+  g[i + j * p] = mv;
+  g[j + i * p] = mv;
 }
 
 // Y[r, jj] = v_{j0+jj}[j0+1+r] (rows of the block's reach, zero above the
@@ -905,17 +911,23 @@ constexpr int SLOT_U = 46, SLOT_Z = 47, SLOT_G = 48, SLOT_SMALL = 49, SLOT_WS = 
 template <bool TA, bool TB>
 static void launch_gemm(bool big, dim3 grid, int m, int n, int k, int kz, double alpha,
                         const double* A, int64_t lda, const double* B, int64_t ldb, double beta,
-                        double* C, int64_t ldc, cudaStream_t s) {
+                        double* C, int64_t ldc, int lower, cudaStream_t s) {
   if (big)
-    dgemm_big_kernel<TA, TB><<<grid, 256, 0, s>>>(m, n, k, kz, alpha, A, lda, B, ldb, beta, C, ldc);
+    dgemm_big_kernel<TA, TB><<<grid, 256, 0, s>>>(m, n, k, kz, alpha, A, lda, B, ldb, beta, C,
+                                                  ldc, lower);
   else
-    dgemm_kernel<TA, TB><<<grid, 256, 0, s>>>(m, n, k, kz, alpha, A, lda, B, ldb, beta, C, ldc);
+    dgemm_kernel<TA, TB><<<grid, 256, 0, s>>>(m, n, k, kz, alpha, A, lda, B, ldb, beta, C, ldc,
+                                              lower);
 }
 
 shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
                   int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
-                  cudaStream_t s, const char* family) {
+                  cudaStream_t s, const char* family, bool lower) {
   if (m <= 0 || n <= 0) return SHRK_OK;
+  if (lower && m != n) {
+    set_error("dgemm: a lower-triangle product must be square");
+    return SHRK_EINVAL;
+  }
   if (m > INT32_MAX || n > INT32_MAX || k > INT32_MAX) {
     set_error("dgemm: dimensions must be below 2^31");
     return SHRK_EINVAL;
@@ -942,10 +954,10 @@ shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alph
   const dim3 grid(cdiv(m, tile), cdiv(n, tile), (unsigned)splits);
   {
     LaunchScope ls(family, s);
-    if (!ta && !tb) launch_gemm<false, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
-    else if (!ta && tb) launch_gemm<false, true>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
-    else if (ta && !tb) launch_gemm<true, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
-    else launch_gemm<true, true>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, s);
+    if (!ta && !tb) launch_gemm<false, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, lower ? 1 : 0, s);
+    else if (!ta && tb) launch_gemm<false, true>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, lower ? 1 : 0, s);
+    else if (ta && !tb) launch_gemm<true, false>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, lower ? 1 : 0, s);
+    else launch_gemm<true, true>(big, grid, (int)m, (int)n, (int)k, kz, alpha, A, lda, B, ldb, b, out, ldo, lower ? 1 : 0, s);
     SHRK_CUDA(cudaGetLastError());
   }
   if (splits > 1) {
@@ -1120,7 +1132,9 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
   double* zcur = Zt;  // current Z^T
   double* other = U;
   for (int it = 0; it < ns_steps; ++it) {
-    SHRK_TRY(dgemm(false, true, p, p, p, 1.0, zcur, p, zcur, p, 0.0, G, p, s));
+    // G is symmetric: its lower triangle's tiles only, mirrored by the
+    // kernel that forms M
+    SHRK_TRY(dgemm(false, true, p, p, p, 1.0, zcur, p, zcur, p, 0.0, G, p, s, "dgemm", true));
     {
       LaunchScope ls("eigh_orthogonalise", s);
       ns_matrix_kernel<<<dim3(cdiv(p, 256), (unsigned)p), 256, 0, s>>>(G, p);

@@ -178,7 +178,7 @@ shrk_status fmm_all(const double* d_ev, int64_t p, double eta, int n, int m2l_tc
 // op = transpose when ta / tb.
 shrk_status dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha, const double* A,
                   int64_t lda, const double* B, int64_t ldb, double beta, double* C, int64_t ldc,
-                  cudaStream_t s, const char* family = "dgemm");
+                  cudaStream_t s, const char* family = "dgemm", bool lower = false);
 // Symmetric eigendecomposition of A (p x p column-major, lower triangle
 // read; overwritten by the eigenvectors, column j for the j-th smallest
 // eigenvalue); the eigenvalues ascending to w_host.  Synchronises s.
