@@ -606,29 +606,47 @@ __device__ __forceinline__ int sturm(const double* __restrict__ d, const double*
   return cnt;
 }
 
+// G-way multisection, G lanes per eigenvalue (32 / G eigenvalues a warp):
+// each step probes G evenly spaced points of the bracket and keeps the
+// sub-interval where the Sturm count crosses kloc (log2(G + 1) bits a step).
+// A wide G takes fewer steps (latency); a narrow one fewer Sturm counts in
+// all (each is a chain of divisions over the block), which is what bounds
+// large matrices.  Every lane stays in the loop until its warp is done (the
+// shuffles span the warp).
+template <int G>
 __global__ void __launch_bounds__(256) bisect_kernel(const double* __restrict__ d,
                                                      const double* __restrict__ e2,
                                                      const EigSlot* __restrict__ slots, int n,
                                                      double pivmin, double* __restrict__ lam) {
-  const int k = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (k >= n) return;
-  const EigSlot sl = slots[k];
+  const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = (int)(gt / G);
+  const int wl = threadIdx.x & 31, lane = wl % G, g0 = wl - lane;
+  const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << g0);
+  EigSlot sl{0, 0, 0, 0, 0.0, 0.0};
+  bool done = k >= n;
+  if (!done) sl = slots[k];
   double lo = sl.lo, hi = sl.hi;
   const double eps = 2.220446049250313e-16;
   for (int it = 0; it < 64; ++it) {
-    if (hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + pivmin) break;
-    const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
-    const bool above = sturm(d, e2, sl.b0, sl.b1, x, pivmin) > sl.kloc;
-    const unsigned m = __ballot_sync(0xffffffffu, above);
-    const double nlo = m == 0u ? __shfl_sync(0xffffffffu, x, 31)
-                               : (__ffs(m) == 1 ? lo : __shfl_sync(0xffffffffu, x, __ffs(m) - 2));
-    const double nhi = m == 0u ? hi : __shfl_sync(0xffffffffu, x, __ffs(m) - 1);
-    if (!(nlo > lo || nhi < hi)) break;  // no representable progress
-    lo = nlo;
-    hi = nhi;
+    if (!done && hi - lo <= 2.0 * eps * fmax(fabs(lo), fabs(hi)) + pivmin) done = true;
+    if (__ballot_sync(0xffffffffu, !done) == 0u) break;
+    const double x = lo + (hi - lo) * (double)(lane + 1) / (double)(G + 1);
+    const bool above = !done && sturm(d, e2, sl.b0, sl.b1, x, pivmin) > sl.kloc;
+    const unsigned m = (__ballot_sync(0xffffffffu, above) & gmask) >> g0;
+    const int f = __ffs(m);  // first probe above kloc, 1-based (0: none)
+    const double xl = __shfl_sync(0xffffffffu, x, g0 + (f == 0 ? G - 1 : (f >= 2 ? f - 2 : 0)));
+    const double xh = __shfl_sync(0xffffffffu, x, g0 + (f == 0 ? 0 : f - 1));
+    const double nlo = f == 0 ? xl : (f == 1 ? lo : xl);
+    const double nhi = f == 0 ? hi : xh;
+    if (!done) {
+      if (!(nlo > lo || nhi < hi)) done = true;  // no representable progress
+      else {
+        lo = nlo;
+        hi = nhi;
+      }
+    }
   }
-  if (lane == 0) lam[k] = 0.5 * (lo + hi);
+  if (lane == 0 && k < n) lam[k] = 0.5 * (lo + hi);
 }
 
 // ------------------------------------------------------ inverse iteration --
@@ -1089,7 +1107,13 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
   SHRK_CUDA(cudaMemcpyAsync(dslots, hslots.data(), sizeof(EigSlot) * p, cudaMemcpyHostToDevice, s));
   {
     LaunchScope ls("eigh_bisect", s);
-    bisect_kernel<<<cdiv(p * 32, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+    // 8 lanes an eigenvalue from p = 3072 (the Sturm counts' divisions bound
+    // the launch there: 8.4 against 11.8 ms at p = 4096), 32 below (the
+    // chain of divisions of each count bounds it: 3.3 against 4.2 ms at 2048)
+    if (p >= 3072)
+      bisect_kernel<8><<<cdiv(p * 8, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+    else
+      bisect_kernel<32><<<cdiv(p * 32, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
     SHRK_CUDA(cudaGetLastError());
   }
   // 3. clusters of close eigenvalues inside each block (host), inverse iteration
