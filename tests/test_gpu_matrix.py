@@ -327,3 +327,48 @@ def test_dgemm_matches_torch(ta, tb, m, n, k):
         got = C.cpu().t()
         err = (got - ref).abs().max().item()
         assert err <= 1e-12 * max(1.0, k ** 0.5) * max(1.0, ref.abs().max().item()), (beta, err)
+
+
+def _hard_matrices():
+    """Spectra that stress the eigensolver: sample covariances (one above
+    the size where the multisection narrows to 8 probes), the identity,
+    repeated and clustered eigenvalues, a rank-one update of the identity,
+    a wide dynamic range, and the Wilkinson tridiagonal (pairs of eigenvalues
+    equal to many digits)."""
+    rng = np.random.default_rng(2024)
+    out = []
+    for p, n in ((700, 2800), (3100, 12400)):
+        x = rng.standard_normal((n, p))
+        out.append((f"sample_cov_{p}", np.ascontiguousarray(x.T @ x / n)))
+    out.append(("identity_300", np.eye(300)))
+
+    def with_spectrum(name, w, seed):
+        q, _ = np.linalg.qr(np.random.default_rng(seed).standard_normal((w.size, w.size)))
+        a = (q * w) @ q.T
+        return (name, np.ascontiguousarray((a + a.T) / 2))
+
+    out.append(with_spectrum("repeated_400", np.repeat([1.0, 2.0, 5.0, 9.0], 100), 1))
+    w = np.concatenate([1.0 + 1e-13 * np.arange(40), np.linspace(2.0, 3.0, 216)])
+    out.append(with_spectrum("cluster_1e-13_256", w, 2))
+    v = rng.standard_normal(512)
+    out.append(("rank_one_512", np.ascontiguousarray(np.eye(512) + 50.0 * np.outer(v, v) / 512)))
+    out.append(with_spectrum("range_1e-8_1e4_300", np.geomspace(1e-8, 1e4, 300), 3))
+    m = 150
+    wil = np.diag(np.abs(np.arange(-m, m + 1)).astype(float)) + np.diag(np.ones(2 * m), 1) \
+        + np.diag(np.ones(2 * m), -1)
+    out.append(("wilkinson_301", np.ascontiguousarray(wil)))
+    return out
+
+
+@pytest.mark.parametrize("name,a", _hard_matrices(), ids=lambda v: v if isinstance(v, str) else "")
+def test_symmetric_eigh_hard_spectra(rk, name, a):
+    """The library's eigensolver against LAPACK (numpy): eigenvalues to
+    1e-13 of the largest, residual ||A V - V diag(w)|| and orthogonality
+    ||V^T V - I|| to 1e-12 (relative to the largest entry of A)."""
+    w, v = rk.symmetric_eigh(a)
+    w_ref = np.linalg.eigvalsh(a)
+    scale = max(np.max(np.abs(w_ref)), 1e-300)
+    assert np.max(np.abs(w - w_ref)) <= 1e-13 * scale, name
+    amax = np.max(np.abs(a))
+    assert np.max(np.abs(a @ v - v * w)) <= 1e-12 * amax, name
+    assert np.max(np.abs(v.T @ v - np.eye(a.shape[0]))) <= 1e-12, name
