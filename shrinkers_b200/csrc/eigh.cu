@@ -1126,13 +1126,25 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
   SHRK_CUDA(cudaMemcpyAsync(dslots, hslots.data(), sizeof(EigSlot) * p, cudaMemcpyHostToDevice, s));
   {
     LaunchScope ls("eigh_bisect", s);
-    // 8 lanes an eigenvalue from p = 3072 (the Sturm counts' divisions bound
-    // the launch there: 8.4 against 11.8 ms at p = 4096), 32 below (the
-    // chain of divisions of each count bounds it: 3.3 against 4.2 ms at 2048)
-    if (p >= 3072)
-      bisect_kernel<8><<<cdiv(p * 8, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
-    else
-      bisect_kernel<32><<<cdiv(p * 32, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+    // probes per eigenvalue: SHRK_EIGH_PROBES (4, 8, 16 or 32) or by size
+    int probes = p >= 3072 ? 8 : 32;
+    if (const char* pe = std::getenv("SHRK_EIGH_PROBES")) {
+      const int v = std::atoi(pe);
+      if (v == 4 || v == 8 || v == 16 || v == 32) probes = v;
+    }
+    switch (probes) {
+      case 4:
+        bisect_kernel<4><<<cdiv(p * 4, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+        break;
+      case 8:
+        bisect_kernel<8><<<cdiv(p * 8, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+        break;
+      case 16:
+        bisect_kernel<16><<<cdiv(p * 16, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+        break;
+      default:
+        bisect_kernel<32><<<cdiv(p * 32, 256), 256, 0, s>>>(d, e2, dslots, (int)p, pivmin, lam);
+    }
     SHRK_CUDA(cudaGetLastError());
   }
   // 3. clusters of close eigenvalues inside each block (host), inverse iteration
