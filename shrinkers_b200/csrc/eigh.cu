@@ -683,100 +683,177 @@ __device__ __forceinline__ double start_entry(int slot, int i) {
   return (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0;
 }
 
-// One thread per cluster.  Workspace (interleaved by thread, so a warp's
-// accesses to the same row coalesce): u0, u1, u2 of U and the right-hand
-// side / solution x, rows relative to the block start.  Eigenvector of slot
-// s goes to Zt[s + i p] (row s of Z^T) for i in [b0, b1).
-__global__ void __launch_bounds__(64) inverse_iteration_kernel(
+// One thread per cluster, a warp per CTA.  Workspace: the factorisation of
+// T - lambda I (U's off-diagonals, reciprocal pivots, multipliers, row
+// swaps) and the right-hand side / solution x, rows relative to the block
+// start, stored per warp as [row][array][lane] so that a warp's rows are
+// one contiguous range (a chunk of rows is one span of memory, prefetched
+// into L2 a few chunks ahead of its use).  Each eigenvalue is factored once
+// and its three solves replay the elimination with multiplications only.
+// Eigenvector of slot s goes to Zt[s + i p] (row s of Z^T) for i in [b0, b1).
+constexpr int II_ARRAYS = 6;  // u1, u2, 1/pivot, multiplier, swap, x
+constexpr int II_CH = 16;     // rows whose loads are issued together
+constexpr int II_AHEAD = 6;   // chunks prefetched ahead
+
+__device__ __forceinline__ void prefetch_rows(const double* base, int r0, int rows) {
+  // rows [r0, r0 + rows) of this warp's workspace, one bulk L2 prefetch
+  const unsigned bytes = (unsigned)rows * II_ARRAYS * 32 * sizeof(double);
+  const double* a = base + (int64_t)r0 * II_ARRAYS * 32;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+}
+
+constexpr int II_RS = II_ARRAYS * 32;  // doubles per workspace row of a warp
+enum { II_U1 = 0, II_U2 = 1, II_RP = 2, II_MU = 3, II_SW = 4, II_X = 5 };
+
+// One elimination step of T - lambda I with partial pivoting: rows i and
+// i + 1, where row i holds (diag, sup) after the earlier steps and row i + 1
+// is (sub, nd, ns).  r points at row i of this lane's workspace.  Branch
+// free (the lanes of a warp pivot differently); one division.
+__device__ __forceinline__ void factor_row(double* r, double sub, double nd, double ns,
+                                           double small, double rsmall, double& diag,
+                                           double& sup) {
+  const bool swp = fabs(diag) < fabs(sub);
+  const double piv = swp ? sub : diag;
+  const double num = swp ? diag : sub;
+  const double rinv = 1.0 / piv;
+  const double m = piv != 0.0 ? num * rinv : 0.0;
+  r[II_U1 * 32] = swp ? nd : sup;
+  r[II_U2 * 32] = swp ? ns : 0.0;
+  r[II_MU * 32] = m;
+  r[II_SW * 32] = swp ? 1.0 : 0.0;
+  r[II_RP * 32] = fabs(piv) < small ? (piv < 0.0 ? -rsmall : rsmall) : rinv;
+  const double nd2 = swp ? sup - m * nd : nd - m * sup;
+  sup = swp ? -m * ns : ns;
+  diag = nd2;
+}
+
+// The factorisation's row operation on the right-hand side: x(i) is final,
+// rhs carries row i + 1 (rn is the old x(i + 1)).
+__device__ __forceinline__ void forward_row(double* r, double rn, double m, double sw,
+                                            double& rhs) {
+  const bool swp = sw != 0.0;
+  const double keep = swp ? rn : rhs;
+  const double other = swp ? rhs : rn;
+  r[II_X * 32] = keep;
+  rhs = other - m * keep;
+}
+
+__global__ void __launch_bounds__(32) inverse_iteration_kernel(
     const double* __restrict__ d, const double* __restrict__ e, const double* __restrict__ lam,
     const Cluster* __restrict__ cl, int ncl, int64_t p, double tnorm, double* __restrict__ ws,
     double* __restrict__ Zt) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x;
+  const int t = blockIdx.x * 32 + lane;
   if (t >= ncl) return;
   const Cluster c = cl[t];
-  const int64_t stride = (int64_t)ncl;
-  double* u0 = ws;
-  double* u1 = ws + stride * p;
-  double* u2 = ws + 2 * stride * p;
-  double* x = ws + 3 * stride * p;
-#define W(arr, i) arr[(int64_t)(i) * stride + t]
+  double* base = ws + (int64_t)blockIdx.x * p * II_RS;
+  double* const wl = base + lane;  // row 0 of this lane
+#define W(a, i) wl[(int64_t)(i) * II_RS + (a) * 32]
+  // lane 0 prefetches for the warp; rows past p are outside the region
+  const bool pf = lane == 0;
+  auto ahead = [&](int r0) {
+    if (!pf) return;
+    const int lo = max(r0, 0);
+    const int hi = (int)((int64_t)r0 + II_CH < p ? (int64_t)r0 + II_CH : p);
+    if (hi > lo) prefetch_rows(base, lo, hi - lo);
+  };
   const int n = c.b1 - c.b0;
   const double small = 2.220446049250313e-16 * tnorm + 1e-300;
-  constexpr int CH = 8;  // rows whose loads are issued together (a row's loads
-                         // would otherwise wait behind the previous row's stores)
+  const double rsmall = 1.0 / small;
+  const double* db = d + c.b0;
+  const double* eb = e + c.b0;
+  constexpr int CH = II_CH;
   for (int q = 0; q < c.ns; ++q) {
     const int slot = c.s0 + q;
     const double l = lam[slot];
-    for (int i = 0; i < n; ++i) W(x, i) = start_entry(slot, i);
-    double scale = 1.0;  // x in memory times scale is the current vector
-    for (int iter = 0; iter < 3; ++iter) {
-      // factor T - l I with partial pivoting, eliminating the right-hand side
-      double diag = d[c.b0] - l;
-      double sup = n > 1 ? e[c.b0] : 0.0;
-      double rhs = W(x, 0) * scale;
-      for (int i0 = 0; i0 + 1 < n; i0 += CH) {
-        double rnv[CH], subv[CH], ndv[CH], nsv[CH];
+    // factor T - l I once with partial pivoting (and write the start
+    // vector); the three solves replay the elimination on their right-hand
+    // sides
+    {
+      double diag = db[0] - l;
+      double sup = n > 1 ? eb[0] : 0.0;
+      int i0 = 0;
+      for (; i0 + CH + 1 < n; i0 += CH) {  // full chunks: rows i0 + u + 2 < n
+        double subv[CH], ndv[CH], nsv[CH];
 #pragma unroll
         for (int u = 0; u < CH; ++u) {
-          const int i = i0 + u;
-          const bool ok = i + 1 < n;
-          rnv[u] = ok ? W(x, i + 1) * scale : 0.0;
-          subv[u] = ok ? e[c.b0 + i] : 0.0;
-          ndv[u] = ok ? d[c.b0 + i + 1] - l : 0.0;
-          nsv[u] = i + 2 < n ? e[c.b0 + i + 1] : 0.0;
+          subv[u] = eb[i0 + u];
+          ndv[u] = db[i0 + u + 1] - l;
+          nsv[u] = eb[i0 + u + 1];
         }
+        double* r = &W(0, i0);
 #pragma unroll
         for (int u = 0; u < CH; ++u) {
-          const int i = i0 + u;
-          if (i + 1 >= n) break;
-          const double sub = subv[u], nd = ndv[u], ns = nsv[u], rn = rnv[u];
-          if (fabs(diag) >= fabs(sub)) {
-            const double m = diag != 0.0 ? sub / diag : 0.0;
-            W(u0, i) = diag;
-            W(u1, i) = sup;
-            W(u2, i) = 0.0;
-            W(x, i) = rhs;
-            diag = nd - m * sup;
-            sup = ns;
-            rhs = rn - m * rhs;
-          } else {
-            const double m = diag / sub;
-            W(u0, i) = sub;
-            W(u1, i) = nd;
-            W(u2, i) = ns;
-            W(x, i) = rn;
-            diag = sup - m * nd;
-            sup = -m * ns;
-            rhs = rhs - m * rn;
-          }
+          factor_row(r + u * II_RS, subv[u], ndv[u], nsv[u], small, rsmall, diag, sup);
+          r[u * II_RS + II_X * 32] = start_entry(slot, i0 + u);
         }
       }
-      W(u0, n - 1) = diag;
-      W(x, n - 1) = rhs;
-      // back substitution, tiny pivots replaced by eps ||T||
-      double nrm2 = 0.0, x1 = 0.0, x2 = 0.0;
-      for (int i0 = n - 1; i0 >= 0; i0 -= CH) {
-        double p0[CH], p1[CH], p2[CH], xv[CH];
+      for (int i = i0; i + 1 < n; ++i) {
+        factor_row(&W(0, i), eb[i], db[i + 1] - l, i + 2 < n ? eb[i + 1] : 0.0, small, rsmall,
+                   diag, sup);
+        W(II_X, i) = start_entry(slot, i);
+      }
+      const double piv = diag;
+      W(II_RP, n - 1) = fabs(piv) < small ? (piv < 0.0 ? -rsmall : rsmall) : 1.0 / piv;
+      W(II_U1, n - 1) = 0.0;
+      W(II_U2, n - 1) = 0.0;
+      W(II_X, n - 1) = start_entry(slot, n - 1);
+    }
+    double scale = 1.0;  // x in memory times scale is the current vector
+    for (int iter = 0; iter < 3; ++iter) {
+      // the factorisation's row operations on the right-hand side
+      for (int k = 0; k < II_AHEAD; ++k) ahead(k * CH);
+      double rhs = W(II_X, 0) * scale;
+      {
+        int i0 = 0;
+        for (; i0 + CH < n; i0 += CH) {  // full chunks: rows i0 + u + 1 < n
+          ahead(i0 + II_AHEAD * CH);
+          double* r = &W(0, i0);
+          double rnv[CH], mv[CH], sv[CH];
 #pragma unroll
-        for (int u = 0; u < CH; ++u) {
-          const int i = i0 - u;
-          const bool ok = i >= 0;
-          p0[u] = ok ? W(u0, i) : 1.0;
-          p1[u] = ok ? W(u1, i) : 0.0;
-          p2[u] = ok ? W(u2, i) : 0.0;
-          xv[u] = ok ? W(x, i) : 0.0;
+          for (int u = 0; u < CH; ++u) {
+            rnv[u] = r[(u + 1) * II_RS + II_X * 32] * scale;
+            mv[u] = r[u * II_RS + II_MU * 32];
+            sv[u] = r[u * II_RS + II_SW * 32];
+          }
+#pragma unroll
+          for (int u = 0; u < CH; ++u) forward_row(r + u * II_RS, rnv[u], mv[u], sv[u], rhs);
         }
+        for (int i = i0; i + 1 < n; ++i) {
+          const double rn = W(II_X, i + 1) * scale;
+          forward_row(&W(0, i), rn, W(II_MU, i), W(II_SW, i), rhs);
+        }
+      }
+      W(II_X, n - 1) = rhs;
+      // back substitution (the last row's U entries are zero), chunks of
+      // rows [i0 - CH + 1, i0]
+      for (int k = 0; k < II_AHEAD; ++k) ahead(n - (k + 1) * CH);
+      double nrm2 = 0.0, x1 = 0.0, x2 = 0.0;
+      {
+        int i0 = n - 1;
+        for (; i0 - CH + 1 >= 0; i0 -= CH) {
+          ahead(i0 + 1 - (II_AHEAD + 1) * CH);
+          double* r = &W(0, i0);
+          double r0[CH], p1[CH], p2[CH], xv[CH];
 #pragma unroll
-        for (int u = 0; u < CH; ++u) {
-          const int i = i0 - u;
-          if (i < 0) break;
-          double piv = p0[u];
-          if (fabs(piv) < small) piv = piv < 0.0 ? -small : small;
-          double sv = xv[u];
-          if (i + 1 < n) sv -= p1[u] * x1;
-          if (i + 2 < n) sv -= p2[u] * x2;
-          const double xi = sv / piv;
-          W(x, i) = xi;
+          for (int u = 0; u < CH; ++u) {
+            r0[u] = r[-u * II_RS + II_RP * 32];
+            p1[u] = r[-u * II_RS + II_U1 * 32];
+            p2[u] = r[-u * II_RS + II_U2 * 32];
+            xv[u] = r[-u * II_RS + II_X * 32];
+          }
+#pragma unroll
+          for (int u = 0; u < CH; ++u) {
+            const double xi = (xv[u] - p1[u] * x1 - p2[u] * x2) * r0[u];
+            r[-u * II_RS + II_X * 32] = xi;
+            nrm2 += xi * xi;
+            x2 = x1;
+            x1 = xi;
+          }
+        }
+        for (int i = i0; i >= 0; --i) {
+          const double xi = (W(II_X, i) - W(II_U1, i) * x1 - W(II_U2, i) * x2) * W(II_RP, i);
+          W(II_X, i) = xi;
           nrm2 += xi * xi;
           x2 = x1;
           x1 = xi;
@@ -786,24 +863,24 @@ __global__ void __launch_bounds__(64) inverse_iteration_kernel(
       if (q > 0) {
         // modified Gram-Schmidt against the cluster's earlier vectors (on the
         // normalised vector; rare: numerically equal eigenvalues only)
-        for (int i = 0; i < n; ++i) W(x, i) *= scale;
+        for (int i = 0; i < n; ++i) W(II_X, i) *= scale;
         scale = 1.0;
         for (int r = 0; r < q; ++r) {
           const double* zr = Zt + (c.s0 + r);
           double dt = 0.0;
-          for (int i = 0; i < n; ++i) dt += zr[(int64_t)(c.b0 + i) * p] * W(x, i);
+          for (int i = 0; i < n; ++i) dt += zr[(int64_t)(c.b0 + i) * p] * W(II_X, i);
           nrm2 = 0.0;
           for (int i = 0; i < n; ++i) {
-            const double xi = W(x, i) - dt * zr[(int64_t)(c.b0 + i) * p];
-            W(x, i) = xi;
+            const double xi = W(II_X, i) - dt * zr[(int64_t)(c.b0 + i) * p];
+            W(II_X, i) = xi;
             nrm2 += xi * xi;
           }
           const double inv = 1.0 / sqrt(nrm2);
-          for (int i = 0; i < n; ++i) W(x, i) *= inv;
+          for (int i = 0; i < n; ++i) W(II_X, i) *= inv;
         }
       }
     }
-    for (int i = 0; i < n; ++i) Zt[slot + (int64_t)(c.b0 + i) * p] = W(x, i) * scale;
+    for (int i = 0; i < n; ++i) Zt[slot + (int64_t)(c.b0 + i) * p] = W(II_X, i) * scale;
   }
 #undef W
 }
@@ -1172,11 +1249,13 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
   const int ncl = (int)hcl.size();
   SHRK_CUDA(cudaMemcpyAsync(dcl, hcl.data(), sizeof(Cluster) * ncl, cudaMemcpyHostToDevice, s));
   void* ws = nullptr;
-  SHRK_TRY(scratch_get(SLOT_WS, sizeof(double) * 4 * (size_t)ncl * (size_t)p, &ws));
+  // per warp of clusters: p rows of II_ARRAYS x 32 doubles
+  SHRK_TRY(scratch_get(SLOT_WS,
+                       sizeof(double) * II_ARRAYS * 32 * (size_t)cdiv(ncl, 32) * (size_t)p, &ws));
   SHRK_CUDA(cudaMemsetAsync(Zt, 0, sizeof(double) * (size_t)P2, s));
   {
     LaunchScope ls("eigh_inverse_iteration", s);
-    inverse_iteration_kernel<<<cdiv(ncl, 64), 64, 0, s>>>(d, e, lam, dcl, ncl, p, tnorm,
+    inverse_iteration_kernel<<<cdiv(ncl, 32), 32, 0, s>>>(d, e, lam, dcl, ncl, p, tnorm,
                                                             (double*)ws, Zt);
     SHRK_CUDA(cudaGetLastError());
   }
