@@ -397,8 +397,13 @@ struct Tri1Args {
   double* beta;    // [p]
   double* pv;      // [2][p]
   double* part;    // [2][gridDim.x]
-  double* vb;      // [gridDim.x][2][p] per-CTA reflector copies
+  double* vb;      // [gridDim.x][2][p] per-CTA reflector copies (global form)
+  double* wb;      // [gridDim.x][p] per-CTA w = p_j - K v_j (global form)
 };
+
+// The per-CTA vectors (two reflectors and w, 3 p doubles) live in shared
+// memory up to this many bytes, else in global memory.
+constexpr size_t TRI1_SMEM_MAX = 200 * 1024;
 
 __device__ __forceinline__ double block_sum(double v, double* red) {
   v = warp_sum(v);
@@ -434,9 +439,11 @@ __device__ __forceinline__ void make_reflector(double* v, int64_t k0, int64_t p,
   __syncthreads();
 }
 
+template <bool SH>
 __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double red[TRI_NT / 32];
+  extern __shared__ double tri_sh[];
   const int lane = threadIdx.x & 31;
   constexpr int WPB = TRI_NT / 32;
   const int64_t gw = (int64_t)blockIdx.x * WPB + (threadIdx.x >> 5);
@@ -455,7 +462,10 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
     }
     return;
   }
-  double* vb = a.vb + (int64_t)blockIdx.x * 2 * p;
+  // the reflectors v_j, v_{j+1} and w_j = p_j - K v_j for the rows >= j+2,
+  // read by every warp of the CTA for every trailing column
+  double* vb = SH ? tri_sh : a.vb + (int64_t)blockIdx.x * 2 * p;
+  double* wv = SH ? tri_sh + 2 * p : a.wb + (int64_t)blockIdx.x * p;
   // prologue: reflector 0 from column 0, p_0 over the columns c >= 1
   double* vcur = vb;
   for (int64_t k = 1 + threadIdx.x; k < p; k += blockDim.x) vcur[k] = A[k];
@@ -511,11 +521,13 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const double wk = upd ? qv[u] - K * vv[u] : 0.0;
+          wv[k + u * bd] = wk;
           vnext[k + u * bd] = av[u] - (vv[u] * wj1 + wk * vj1);
         }
       }
       for (; k < p; k += bd) {
         const double vk = vcur[k], wk = upd ? pj[k] - K * vk : 0.0;
+        wv[k] = wk;
         vnext[k] = colj1[k] - (vk * wj1 + wk * vj1);
       }
     }
@@ -543,7 +555,7 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
     double dot = 0.0;
     for (int64_t c = k2 + ((gw - k2) % nw + nw) % nw; c < p; c += nw) {
       double* col = A + c * p;
-      const double vc = vcur[c], wc = upd ? pj[c] - K * vc : 0.0;
+      const double vc = vcur[c], wc = wv[c];
       double s = 0.0;
       int64_t k = k2 + lane;
       // eight rows per lane per step, every load issued before any store
@@ -554,20 +566,18 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
         for (int u = 0; u < 8; ++u) {
           av[u] = col[k + 32 * u];
           vv[u] = vcur[k + 32 * u];
-          qv[u] = pj[k + 32 * u];
+          qv[u] = wv[k + 32 * u];
           nv[u] = vnext[k + 32 * u];
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          const double wk = upd ? qv[u] - K * vv[u] : 0.0;
-          const double x = av[u] - (vv[u] * wc + wk * vc);
+          const double x = av[u] - (vv[u] * wc + qv[u] * vc);
           col[k + 32 * u] = x;
           s = fma(x, nv[u], s);
         }
       }
       for (; k < p; k += 32) {
-        const double vk = vcur[k], wk = upd ? pj[k] - K * vk : 0.0;
-        const double x = col[k] - (vk * wc + wk * vc);
+        const double x = col[k] - (vcur[k] * wc + wv[k] * vc);
         col[k] = x;
         s = fma(x, vnext[k], s);
       }
@@ -1119,23 +1129,38 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
     int dev = 0, sms = 0, per_sm = 0;
     SHRK_CUDA(cudaGetDevice(&dev));
     SHRK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // one-barrier form: the per-CTA vectors in shared memory when they fit
+    // (SHRK_EIGH_TRI1_GLOBAL=1 keeps them in global memory at any size)
+    const size_t sh_bytes = sizeof(double) * 3 * (size_t)p;
+    const char* glob_env = std::getenv("SHRK_EIGH_TRI1_GLOBAL");
+    const bool sh = sh_bytes <= TRI1_SMEM_MAX && !(glob_env && std::strcmp(glob_env, "1") == 0);
+    const void* tri1 = sh ? (const void*)tridiag1_kernel<true> : (const void*)tridiag1_kernel<false>;
+    const size_t dyn = rowstore && sh ? sh_bytes : 0;
+    if (dyn > 0)
+      SHRK_CUDA(cudaFuncSetAttribute(tri1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     SHRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, rowstore ? (const void*)tridiag1_kernel : (const void*)tridiag_kernel, TRI_NT, 0));
+        &per_sm, rowstore ? tri1 : (const void*)tridiag_kernel, TRI_NT, dyn));
     if (per_sm < 1) {
       set_error("eigensolver: the tridiagonalisation kernel cannot be resident");
       return SHRK_ECUDA;
     }
     const int blocks = std::min(sms, 2048);
     if (rowstore) {
+      // p_j [2][p] and the partial sums [2][blocks]; the per-CTA vectors
+      // [blocks][3][p] only when they are not in shared memory
+      const size_t per_cta = sh ? 0 : (size_t)blocks * 3 * (size_t)p;
       void* vbuf = nullptr;
-      SHRK_TRY(scratch_get(SLOT_VB, sizeof(double) * ((size_t)blocks * 2 * (size_t)p + 2 * (size_t)p + 2 * (size_t)blocks), &vbuf));
+      SHRK_TRY(scratch_get(SLOT_VB, sizeof(double) * (per_cta + 2 * (size_t)p + 2 * (size_t)blocks),
+                           &vbuf));
       double* vbd = (double*)vbuf;
-      Tri1Args ta{A, p, d, e, vhead, beta, vbd + (size_t)blocks * 2 * p,
-                  vbd + (size_t)blocks * 2 * p + 2 * p, vbd};
+      Tri1Args ta{A,          p,
+                  d,          e,
+                  vhead,      beta,
+                  vbd + per_cta, vbd + per_cta + 2 * p,
+                  sh ? nullptr : vbd, sh ? nullptr : vbd + (size_t)blocks * 2 * p};
       void* args[] = {&ta};
       LaunchScope ls("eigh_tridiag", s);
-      SHRK_CUDA(cudaLaunchCooperativeKernel((const void*)tridiag1_kernel, dim3(blocks),
-                                            dim3(TRI_NT), args, 0, s));
+      SHRK_CUDA(cudaLaunchCooperativeKernel(tri1, dim3(blocks), dim3(TRI_NT), args, dyn, s));
     } else {
       TriArgs ta{A, p, d, e, vhead, beta, pv, part, scal};
       void* args[] = {&ta};

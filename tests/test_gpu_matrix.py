@@ -372,3 +372,22 @@ def test_symmetric_eigh_hard_spectra(rk, name, a):
     amax = np.max(np.abs(a))
     assert np.max(np.abs(a @ v - v * w)) <= 1e-12 * amax, name
     assert np.max(np.abs(v.T @ v - np.eye(a.shape[0]))) <= 1e-12, name
+
+
+@pytest.mark.parametrize("form", ["shared", "global", "two_barrier"])
+def test_symmetric_eigh_tridiagonalisation_forms(rk, monkeypatch, form):
+    """The three forms of the tridiagonalisation (per-CTA vectors in shared
+    memory, the same in global memory as used above ~8 500 rows, and the
+    two-barrier form) give the same decomposition to rounding."""
+    if form == "global":
+        monkeypatch.setenv("SHRK_EIGH_TRI1_GLOBAL", "1")
+    elif form == "two_barrier":
+        monkeypatch.setenv("SHRK_EIGH_TRIDIAG", "2")
+    rng = np.random.default_rng(31)
+    x = rng.standard_normal((2000, 500))
+    a = np.ascontiguousarray(x.T @ x / 2000)
+    w, v = rk.symmetric_eigh(a)
+    w_ref = np.linalg.eigvalsh(a)
+    assert np.max(np.abs(w - w_ref)) <= 1e-13 * np.max(np.abs(w_ref))
+    assert np.max(np.abs(a @ v - v * w)) <= 1e-12 * np.max(np.abs(a))
+    assert np.max(np.abs(v.T @ v - np.eye(500))) <= 1e-12
