@@ -439,7 +439,7 @@ __device__ __forceinline__ void make_reflector(double* v, int64_t k0, int64_t p,
   __syncthreads();
 }
 
-template <bool SH>
+template <bool SH, int R = 16>
 __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
   cg::grid_group grid = cg::this_grid();
   __shared__ double red[TRI_NT / 32];
@@ -558,6 +558,25 @@ __global__ void __launch_bounds__(TRI_NT, 1) tridiag1_kernel(const Tri1Args a) {
       const double vc = vcur[c], wc = wv[c];
       double s = 0.0;
       int64_t k = k2 + lane;
+      if constexpr (SH) {
+        // R rows per lane per step (one L2 round trip), the column's loads
+        // issued before any store; the vectors come from shared memory; the
+        // ragged end is one predicated step
+        for (; k < p; k += 32 * R) {
+          double av[R];
+#pragma unroll
+          for (int u = 0; u < R; ++u) av[u] = k + 32 * u < p ? col[k + 32 * u] : 0.0;
+#pragma unroll
+          for (int u = 0; u < R; ++u) {
+            const int64_t kk = k + 32 * u;
+            if (kk < p) {
+              const double x = av[u] - (vcur[kk] * wc + wv[kk] * vc);
+              col[kk] = x;
+              s = fma(x, vnext[kk], s);
+            }
+          }
+        }
+      }
       // eight rows per lane per step, every load issued before any store
       // (the stores to col could alias the loads for all the compiler knows)
       for (; k + 224 < p; k += 256) {
@@ -1134,7 +1153,15 @@ shrk_status eigh_device(double* A, int64_t p, std::vector<double>& w_host, cudaS
     const size_t sh_bytes = sizeof(double) * 3 * (size_t)p;
     const char* glob_env = std::getenv("SHRK_EIGH_TRI1_GLOBAL");
     const bool sh = sh_bytes <= TRI1_SMEM_MAX && !(glob_env && std::strcmp(glob_env, "1") == 0);
-    const void* tri1 = sh ? (const void*)tridiag1_kernel<true> : (const void*)tridiag1_kernel<false>;
+    // rows per lane per step of the trailing update: SHRK_EIGH_TRI1_ROWS (8,
+    // 16 or 32) or by size (measured: 8 best at p = 2 048, 18.8 ms; 16 at
+    // 4 096, 87.3 ms; 32 slower at both)
+    const char* rows_env = std::getenv("SHRK_EIGH_TRI1_ROWS");
+    const int rows = rows_env ? std::atoi(rows_env) : (p >= 3072 ? 16 : 8);
+    const void* tri1 = !sh          ? (const void*)tridiag1_kernel<false>
+                       : rows == 32 ? (const void*)tridiag1_kernel<true, 32>
+                       : rows == 8  ? (const void*)tridiag1_kernel<true, 8>
+                                    : (const void*)tridiag1_kernel<true, 16>;
     const size_t dyn = rowstore && sh ? sh_bytes : 0;
     if (dyn > 0)
       SHRK_CUDA(cudaFuncSetAttribute(tri1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
