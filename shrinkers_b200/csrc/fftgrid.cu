@@ -34,8 +34,10 @@
 #include "epilogue.cuh"
 #include "internal.h"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <map>
 #include <string>
 
@@ -141,60 +143,96 @@ __device__ __forceinline__ double weight_of(const GridArgs& a, int64_t j) {
 // visited sources whose clamped stencil cell is below key.  Visiting order
 // makes the cells non-decreasing, so this is a lower bound found by
 // bisection (the same cell computation as everywhere else, so the same runs).
+// With `cells` (the clamped cell of every visited source, cells_kernel) the
+// probes compare integers instead of each dividing.
 template <int N>
-__device__ __forceinline__ int64_t lower_key(const GridArgs& a, int key, int64_t lo, int64_t hi) {
+__device__ __forceinline__ int64_t lower_key(const GridArgs& a, const int* __restrict__ cells,
+                                             int key, int64_t lo, int64_t hi) {
   while (lo < hi) {
     const int64_t mid = (lo + hi) >> 1;
     double t;
-    if (clamped_cell<N>(a, mid, &t) < key) lo = mid + 1;
+    const int c = cells ? __ldg(cells + mid) : clamped_cell<N>(a, mid, &t);
+    if (c < key) lo = mid + 1;
     else hi = mid;
   }
   return lo;
 }
 
+// cells[j] = the clamped stencil cell of visited source j: one division per
+// source, for grids with many keys, whose searches would otherwise divide at
+// every probe.
+template <int N>
+__global__ void cells_kernel(const GridArgs a, int* __restrict__ cells) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.ns; j += stride) {
+    double t;
+    cells[j] = clamped_cell<N>(a, j, &t);
+  }
+}
+
 constexpr int DENSE_MIN = 32;   // cells with more sources take their density from run sums
-constexpr int RUN_CTA = 32;     // runs with more sources are summed by CTAs,
-constexpr int RUN_CHUNK = 4096; // in chunks of this many sources, a CTA each
+constexpr int RUN_CHUNK = 4096; // long runs are summed in chunks of this many sources, a CTA each
+
+// Run lengths that decide who sums a run: at most `thread_max` sources, the
+// key's own thread; up to `warp_max`, a warp; longer runs, CTAs in chunks of
+// RUN_CHUNK.  Each run's sum depends only on its length, so it is the same
+// from call to call.
+struct RunSplit {
+  int thread_max;
+  int warp_max;
+};
 
 // The long runs and their chunks (keys_kernel fills them, long_runs_kernel
 // sums them): run r is key idx[r] with nch[r] chunks from the chunk list's
 // base[r]; cnt[r] counts its finished chunks; partial[g][k] holds chunk g's
-// sums.  counters[0] / [1] = runs / chunks listed (zero on entry).
+// sums; widx[] lists the keys of the warp-summed runs.  counters[0] / [1] /
+// [2] = runs / chunks / warp runs listed (zero on entry).
 struct LongRuns {
   int* idx;
   int* base;
   int* nch;
   int* cnt;
   int* chunk_run;  // chunk g -> its run r
+  int* widx;
   int* counters;
   double* partial;
 };
 
-// Keys and run sums.  The thread of key e finds first[e] by bisection and
-// the end of its run by a galloping search from there (one probe for an empty
-// run); then S[(e + N + 1) N + k], the sum of stencil weight k over the run,
-// computing each source's N weights once in ascending source order -- or,
-// for a run of more than RUN_CTA sources, lists the run and its chunks of
-// RUN_CHUNK sources for long_runs_kernel.
+// Keys and run sums.  A CTA of KEYS_CTA threads serves KEYS_CTA - 1
+// consecutive keys: each thread finds first[] of its key, and the end of a
+// key's run, first[] of the next key, comes from the next thread through
+// shared memory (the last thread of a CTA searches only for that, the next
+// CTA's first key), so every thread makes one search.  Then
+// S[(e + N + 1) N + k], the sum of stencil weight k over the run, computing
+// each source's N weights once in ascending source order -- or, for a longer
+// run (RunSplit), lists it for long_runs_kernel: as a warp run, or with its
+// chunks of RUN_CHUNK sources.
+constexpr int KEYS_CTA = 256;
+
 template <int N>
-__global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n_keys,
-                            double* __restrict__ S, LongRuns L) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx > n_keys) return;
+__global__ void __launch_bounds__(KEYS_CTA) keys_kernel(const GridArgs a, int* __restrict__ first,
+                                                        int64_t n_keys, double* __restrict__ S,
+                                                        LongRuns L, const int* __restrict__ cells,
+                                                        RunSplit rs) {
+  __shared__ int first_sh[KEYS_CTA];
+  const int64_t idx = (int64_t)blockIdx.x * (KEYS_CTA - 1) + threadIdx.x;
   const int key = (int)(idx - N - 1);
-  const int64_t j0 = lower_key<N>(a, key, 0, a.ns);
+  int64_t j0 = a.ns;
+  if (idx <= n_keys) j0 = lower_key<N>(a, cells, key, 0, a.ns);
+  first_sh[threadIdx.x] = (int)j0;
+  __syncthreads();
+  if (idx > n_keys || threadIdx.x == KEYS_CTA - 1) return;
   first[idx] = (int)j0;
   if (idx == n_keys) return;  // the closing entry (= ns)
-  // end of the run: the first source whose cell is at least key + 1
-  int64_t lo = j0, step = 1, hi = j0;
+  // end of the run: the first source whose cell is at least key + 1 (the
+  // next thread's key; idx < n_keys, so that thread searched)
+  const int64_t j1 = first_sh[threadIdx.x + 1];
   double t;
-  while (hi < a.ns && clamped_cell<N>(a, hi, &t) < key + 1) {
-    lo = hi + 1;
-    hi = j0 + step;
-    step *= 2;
+  if (j1 - j0 > rs.thread_max && j1 - j0 <= rs.warp_max) {
+    L.widx[atomicAdd(L.counters + 2, 1)] = (int)idx;
+    return;
   }
-  const int64_t j1 = lower_key<N>(a, key + 1, lo, hi < a.ns ? hi : a.ns);
-  if (j1 - j0 > RUN_CTA) {
+  if (j1 - j0 > rs.thread_max) {
     const int nch = (int)((j1 - j0 + RUN_CHUNK - 1) / RUN_CHUNK);
     const int r = atomicAdd(L.counters, 1);
     const int base = atomicAdd(L.counters + 1, nch);
@@ -219,12 +257,12 @@ __global__ void keys_kernel(const GridArgs a, int* __restrict__ first, int64_t n
   for (int k = 0; k < N; ++k) S[idx * N + k] = acc[k];
 }
 
-// Run sums of the long runs: a CTA per chunk of RUN_CHUNK sources (threads
-// stride the chunk, partials added in a fixed order).  A run of one chunk
-// writes its sums directly; otherwise the CTA that finishes a run's last
-// chunk (a ticket taken after a fence) adds the run's chunk partials in
-// chunk order.  The lists' order varies from call to call; each run's sum
-// does not.
+// Run sums of the longer runs.  Runs listed with chunks: a CTA per chunk of
+// RUN_CHUNK sources (threads stride the chunk, partials added in a fixed
+// order); a run of one chunk writes its sums directly, otherwise the CTA that
+// finishes a run's last chunk (a ticket taken after a fence) adds the run's
+// chunk partials in chunk order.  Then the warp runs, a warp each.  The
+// lists' order varies from call to call; each run's sum does not.
 template <int N>
 __global__ void __launch_bounds__(256) long_runs_kernel(const GridArgs a,
                                                         const int* __restrict__ first,
@@ -281,6 +319,31 @@ __global__ void __launch_bounds__(256) long_runs_kernel(const GridArgs a,
       }
     }
     __syncthreads();
+  }
+  // Warp runs: a warp per run, lanes striding it, the lanes' partials added
+  // by a fixed butterfly.
+  const int n_warp_runs = L.counters[2];
+  const int warps = (int)(blockDim.x >> 5);
+  for (int r = blockIdx.x * warps + wib; r < n_warp_runs; r += gridDim.x * warps) {
+    const int64_t idx = L.widx[r];
+    const int64_t j1 = first[idx + 1];
+    double acc[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) acc[k] = 0.0;
+    for (int64_t j = first[idx] + lane; j < j1; j += 32) {
+      double t, w[N];
+      (void)clamped_cell<N>(a, j, &t);
+      lagrange<N>(t, w);
+#pragma unroll
+      for (int k = 0; k < N; ++k) acc[k] += w[k];
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double v = acc[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == k) S[idx * N + k] = v;
+    }
   }
 }
 
@@ -910,6 +973,28 @@ shrk_status eval_grid(double2* A, double2* B, double2* Wa, double2* Wt, const Ta
                       const double* d_q, int64_t nq, const GridPlan& g, const Epilogue& epi,
                       cudaStream_t s);
 
+// Splat tuning, read once: SHRK_SPLAT_CELLS (0 / 1: the key searches on a
+// cell array off / on; default: on when the keys outnumber one wave of
+// resident threads), SHRK_SPLAT_THREAD_MAX and SHRK_SPLAT_WARP_MAX (the
+// RunSplit bounds; default 8 and 256, measured at p = 10^6 on the NUFFT's
+// 65 536-cell grid and the fft5 grid of 2^20 cells).
+struct SplatTuning {
+  int cells = -1;
+  RunSplit rs{8, 256};
+};
+
+const SplatTuning& splat_tuning() {
+  static const SplatTuning t = [] {
+    SplatTuning v;
+    if (const char* e = std::getenv("SHRK_SPLAT_CELLS")) v.cells = std::atoi(e) != 0 ? 1 : 0;
+    if (const char* e = std::getenv("SHRK_SPLAT_THREAD_MAX")) v.rs.thread_max = std::max(0, std::atoi(e));
+    if (const char* e = std::getenv("SHRK_SPLAT_WARP_MAX")) v.rs.warp_max = std::atoi(e);
+    v.rs.warp_max = std::max(v.rs.warp_max, v.rs.thread_max);
+    return v;
+  }();
+  return t;
+}
+
 // The whole grid convolution, or one of its two stages: with dens_out the
 // splat alone (the density of the sources into dens_out[m], nothing else);
 // with dens_in the evaluation alone from that density (no sources read).
@@ -940,14 +1025,19 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
     if (dens_out) SHRK_CUDA(cudaMemsetAsync(dens_out, 0, sizeof(double) * m, s));
     return SHRK_OK;
   }
-  // slot 24: first [K + 1] | long runs: idx, base, nch, cnt [K] each | two
-  // counters | chunk list [C] | run sums [K][N] | chunk partials [C][N],
-  // K = m + 2N + 2 keys from -N - 1, C = ns / RUN_CHUNK + K chunks at most
-  // (a run of n > RUN_CTA sources has ceil(n / RUN_CHUNK) chunks)
+  // slot 24: first [K + 1] | long runs: idx, base, nch, cnt, warp runs [K]
+  // each | three counters | chunk list [C] | source cells [ns] (when used) |
+  // run sums [K][N] | chunk partials [C][N], K = m + 2N + 2 keys from
+  // -N - 1, C = ns / RUN_CHUNK + K chunks at most (a chunked run of n sources
+  // has ceil(n / RUN_CHUNK))
   const int64_t n_keys = m + 2 * N + 2;
   const int64_t max_chunks = ns / RUN_CHUNK + n_keys;
+  const SplatTuning& st = splat_tuning();
+  const bool use_cells =
+      st.cells >= 0 ? st.cells != 0 : (n_keys + 1) > (int64_t)sm_count() * 2048;
   const size_t int_bytes =
-      ((sizeof(int) * (5 * (size_t)n_keys + 3 + (size_t)max_chunks)) + 255) & ~(size_t)255;
+      ((sizeof(int) * (6 * (size_t)n_keys + 4 + (size_t)max_chunks + (use_cells ? (size_t)ns : 0))) +
+       255) & ~(size_t)255;
   void* sw = nullptr;
   SHRK_TRY(scratch_get(24, int_bytes + sizeof(double) * N * ((size_t)n_keys + (size_t)max_chunks),
                        &sw));
@@ -957,14 +1047,23 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   lr.base = lr.idx + n_keys;
   lr.nch = lr.base + n_keys;
   lr.cnt = lr.nch + n_keys;
-  lr.counters = lr.cnt + n_keys;
-  lr.chunk_run = lr.counters + 2;
+  lr.widx = lr.cnt + n_keys;
+  lr.counters = lr.widx + n_keys;
+  lr.chunk_run = lr.counters + 3;
+  int* cells = use_cells ? lr.chunk_run + max_chunks : nullptr;
   double* runs = (double*)((char*)sw + int_bytes);
   lr.partial = runs + (size_t)N * n_keys;
-  SHRK_CUDA(cudaMemsetAsync(lr.counters, 0, 2 * sizeof(int), s));
+  SHRK_CUDA(cudaMemsetAsync(lr.counters, 0, 3 * sizeof(int), s));
+  if (use_cells) {
+    LaunchScope ls(g.fam_splat, s);
+    const int64_t blocks = std::min<int64_t>((ns + 255) / 256, (int64_t)sm_count() * 8);
+    cells_kernel<N><<<(unsigned)blocks, 256, 0, s>>>(ga, cells);
+    SHRK_CUDA(cudaGetLastError());
+  }
   {
     LaunchScope ls(g.fam_splat, s);
-    keys_kernel<N><<<blocks_for(n_keys + 1, 256), 256, 0, s>>>(ga, first, n_keys, runs, lr);
+    keys_kernel<N><<<blocks_for(n_keys + 1, KEYS_CTA - 1), KEYS_CTA, 0, s>>>(ga, first, n_keys,
+                                                                             runs, lr, cells, st.rs);
     SHRK_CUDA(cudaGetLastError());
   }
   {
