@@ -144,10 +144,27 @@ __device__ __forceinline__ double weight_of(const GridArgs& a, int64_t j) {
 // makes the cells non-decreasing, so this is a lower bound found by
 // bisection (the same cell computation as everywhere else, so the same runs).
 // With `cells` (the clamped cell of every visited source, cells_kernel) the
-// probes compare integers instead of each dividing.
+// probes compare integers instead of each dividing, and start on `coarse`
+// (every COARSE-th entry of cells, small enough to stay in L1): the first
+// coarse entry at least key brackets the answer within COARSE sources.
+constexpr int COARSE = 64;
+
 template <int N>
 __device__ __forceinline__ int64_t lower_key(const GridArgs& a, const int* __restrict__ cells,
-                                             int key, int64_t lo, int64_t hi) {
+                                             const int* __restrict__ coarse, int key, int64_t lo,
+                                             int64_t hi) {
+  if (cells) {
+    int64_t blo = 0, bhi = (a.ns + COARSE - 1) / COARSE;
+    while (blo < bhi) {
+      const int64_t mid = (blo + bhi) >> 1;
+      if (__ldg(coarse + mid) < key) blo = mid + 1;
+      else bhi = mid;
+    }
+    // cells[COARSE (blo - 1)] < key <= cells[COARSE blo] (or blo = the end)
+    if (blo == 0) return 0;
+    lo = COARSE * (blo - 1) + 1;
+    hi = COARSE * blo < a.ns ? COARSE * blo : a.ns;
+  }
   while (lo < hi) {
     const int64_t mid = (lo + hi) >> 1;
     double t;
@@ -162,11 +179,13 @@ __device__ __forceinline__ int64_t lower_key(const GridArgs& a, const int* __res
 // source, for grids with many keys, whose searches would otherwise divide at
 // every probe.
 template <int N>
-__global__ void cells_kernel(const GridArgs a, int* __restrict__ cells) {
+__global__ void cells_kernel(const GridArgs a, int* __restrict__ cells, int* __restrict__ coarse) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < a.ns; j += stride) {
     double t;
-    cells[j] = clamped_cell<N>(a, j, &t);
+    const int c = clamped_cell<N>(a, j, &t);
+    cells[j] = c;
+    if (j % COARSE == 0) coarse[j / COARSE] = c;
   }
 }
 
@@ -213,12 +232,13 @@ template <int N>
 __global__ void __launch_bounds__(KEYS_CTA) keys_kernel(const GridArgs a, int* __restrict__ first,
                                                         int64_t n_keys, double* __restrict__ S,
                                                         LongRuns L, const int* __restrict__ cells,
+                                                        const int* __restrict__ coarse,
                                                         RunSplit rs) {
   __shared__ int first_sh[KEYS_CTA];
   const int64_t idx = (int64_t)blockIdx.x * (KEYS_CTA - 1) + threadIdx.x;
   const int key = (int)(idx - N - 1);
   int64_t j0 = a.ns;
-  if (idx <= n_keys) j0 = lower_key<N>(a, cells, key, 0, a.ns);
+  if (idx <= n_keys) j0 = lower_key<N>(a, cells, coarse, key, 0, a.ns);
   first_sh[threadIdx.x] = (int)j0;
   __syncthreads();
   if (idx > n_keys || threadIdx.x == KEYS_CTA - 1) return;
@@ -1029,14 +1049,17 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   // each | three counters | chunk list [C] | source cells [ns] (when used) |
   // run sums [K][N] | chunk partials [C][N], K = m + 2N + 2 keys from
   // -N - 1, C = ns / RUN_CHUNK + K chunks at most (a chunked run of n sources
-  // has ceil(n / RUN_CHUNK))
+  // has ceil(n / RUN_CHUNK)); the source cells are followed by their coarse
+  // table [ceil(ns / COARSE)]
   const int64_t n_keys = m + 2 * N + 2;
   const int64_t max_chunks = ns / RUN_CHUNK + n_keys;
   const SplatTuning& st = splat_tuning();
   const bool use_cells =
       st.cells >= 0 ? st.cells != 0 : (n_keys + 1) > (int64_t)sm_count() * 2048;
+  const size_t n_coarse = (size_t)((ns + COARSE - 1) / COARSE);
   const size_t int_bytes =
-      ((sizeof(int) * (6 * (size_t)n_keys + 4 + (size_t)max_chunks + (use_cells ? (size_t)ns : 0))) +
+      ((sizeof(int) * (6 * (size_t)n_keys + 4 + (size_t)max_chunks +
+                       (use_cells ? (size_t)ns + n_coarse : 0))) +
        255) & ~(size_t)255;
   void* sw = nullptr;
   SHRK_TRY(scratch_get(24, int_bytes + sizeof(double) * N * ((size_t)n_keys + (size_t)max_chunks),
@@ -1051,19 +1074,21 @@ shrk_status run_grid(const double* d_q, int64_t nq, const double* d_src, int64_t
   lr.counters = lr.widx + n_keys;
   lr.chunk_run = lr.counters + 3;
   int* cells = use_cells ? lr.chunk_run + max_chunks : nullptr;
+  int* coarse = use_cells ? cells + ns : nullptr;
   double* runs = (double*)((char*)sw + int_bytes);
   lr.partial = runs + (size_t)N * n_keys;
   SHRK_CUDA(cudaMemsetAsync(lr.counters, 0, 3 * sizeof(int), s));
   if (use_cells) {
     LaunchScope ls(g.fam_splat, s);
     const int64_t blocks = std::min<int64_t>((ns + 255) / 256, (int64_t)sm_count() * 8);
-    cells_kernel<N><<<(unsigned)blocks, 256, 0, s>>>(ga, cells);
+    cells_kernel<N><<<(unsigned)blocks, 256, 0, s>>>(ga, cells, coarse);
     SHRK_CUDA(cudaGetLastError());
   }
   {
     LaunchScope ls(g.fam_splat, s);
     keys_kernel<N><<<blocks_for(n_keys + 1, KEYS_CTA - 1), KEYS_CTA, 0, s>>>(ga, first, n_keys,
-                                                                             runs, lr, cells, st.rs);
+                                                                             runs, lr, cells, coarse,
+                                                                             st.rs);
     SHRK_CUDA(cudaGetLastError());
   }
   {
