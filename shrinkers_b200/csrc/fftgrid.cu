@@ -12,14 +12,17 @@
 //   1. runs         a source's stencil cell is i0 = floor((v-lo)/dx); the
 //                   sources are sorted, so the cells are too, and one thread
 //                   per cell key bisects for first[key] = the first source
-//                   with cell >= key.
-//   2. gather+pack  one thread per grid cell adds the weights of its sources
+//                   with cell >= key (on an integer cell array for large
+//                   grids); each run of equal cells gets the sums of its N
+//                   stencil weights, from the key's thread, a warp or CTAs
+//                   by the run's length.
+//   2. pack         one thread per grid cell adds the weights of its sources
 //                   (at most 32) run by run in ascending source order -- the
 //                   order of the reference's sequential splat, so these
-//                   densities are the same sums, without atomics -- and
-//                   queues denser cells for one warp (or one CTA) each.  The
-//                   N Lagrange weights of t = pos - i0 are recomputed where
-//                   they are added (sources come from L2; no weight array).
+//                   densities are the same sums, without atomics; a denser
+//                   cell adds the N run sums.  The N Lagrange weights of
+//                   t = pos - i0 are recomputed where they are added
+//                   (sources come from L2; no weight array).
 //                   packed[c] = density[c] + i x_c/(x_c^2 + eta^2).
 //   4. fft          four-step FFT m = m1*m2 (m1, m2 <= 2048): column FFTs of
 //                   length m1 in shared memory with the inter-pass twiddle,
