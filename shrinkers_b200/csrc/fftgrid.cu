@@ -1134,6 +1134,11 @@ shrk_status eval_grid(double2* A, double2* B, double2* Wa, double2* Wt, const Ta
 shrk_status run_grid_order(const double* d_q, int64_t nq, const double* d_src, int64_t ns,
                            double eta, const GridPlan& g, const Epilogue& epi, cudaStream_t s,
                            const double* dens_in = nullptr, double* dens_out = nullptr) {
+  // the first-source table and the run lists index sources with 32-bit ints
+  if (ns > (int64_t)INT32_MAX) {
+    set_error("fft grid methods: at most 2^31 - 1 sources per call");
+    return SHRK_EINVAL;
+  }
   switch (g.order) {
     case 2: return run_grid<2>(d_q, nq, d_src, ns, eta, g, epi, s, dens_in, dens_out);
     case 4: return run_grid<4>(d_q, nq, d_src, ns, eta, g, epi, s, dens_in, dens_out);
