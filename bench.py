@@ -654,7 +654,7 @@ def run_path(args, world, rank, local):
             m = O.fft5_grid_size(ev_h, eta)
             fam = family.decode()
             alg_step, basis = {
-                "fft5_splat": (8 * p + 16 * m, "splat (weights + gather launches): 8 B per "
+                "fft5_splat": (8 * p + 16 * m, "splat (cell, key, run-sum and pack launches): 8 B per "
                                "source read + 16 B per grid cell written, per step"),
                 "fft5_fft": (128 * m, "two transforms of two four-step passes: 16 B per cell "
                              "read + 16 B written per pass, per step"),
